@@ -1,0 +1,220 @@
+/*
+ * lbfs_b200.h -- C ABI of the B200 (sm_100a) implementation of the LBFS-IBM
+ * time step: D3Q15 lattice-Boltzmann flux solver on an unstructured
+ * finite-volume hex mesh, immersed-boundary coupling, spring-network red blood
+ * cell membranes.
+ *
+ * The reference (CHRG-Developer/LBFS-IBM-ADE-SP) has no plugin layer: its
+ * solver entry point is the C++ method
+ *     void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh&, Solution&,
+ *         Boundary_Conditions&, external_forces&, global_variables&, domain_geometry&,
+ *         initial_conditions&, unstructured_bcs&, int mg, Solution& residual, int fmg,
+ *         post_processing&, std::vector<lagrangian_object>&)      (Solver_gpu.h:28-31)
+ * which copies the host objects into ~80 managed arrays (Solver_gpu.cu:473-655),
+ * runs the time loop (Solver_gpu.cu:749-1246) and writes the solution back.
+ * This header is what a drop-in replacement of that method binds to: the
+ * descriptors below carry exactly the arrays the reference copies (same
+ * ordering, same meaning), lbfs_create replaces the set-up block, lbfs_step
+ * replaces one iteration of the time loop, and lbfs_get_state replaces the
+ * write-back into Solution.  INTEGRATION.md shows the C++ shim.
+ *
+ * Conventions: every entry point returns an int status (LBFS_OK = 0); no C++
+ * exception crosses the boundary; all pointers in descriptors are HOST
+ * pointers owned by the caller and only read during lbfs_create; device
+ * buffers are owned by the library; a handle is not thread-safe.
+ */
+#ifndef LBFS_B200_H
+#define LBFS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define LBFS_OK 0
+#define LBFS_ERR_ARG 1          /* invalid argument or descriptor            */
+#define LBFS_ERR_CUDA 2         /* CUDA runtime error (message via lbfs_last_error) */
+#define LBFS_ERR_NOMEM 3        /* device allocation failed                  */
+#define LBFS_ERR_STATE 4        /* solution flagged non-finite / invalid      */
+#define LBFS_ERR_UNSUPPORTED 5  /* option not implemented                    */
+#define LBFS_ERR_LIMIT 6        /* size beyond a documented maximum          */
+
+/* ---- status flags (lbfs_status) ---------------------------------------- */
+#define LBFS_FLAG_NONFINITE 1u  /* NaN/Inf in the fluid state (reference: LBFS.cu:2833-2865 traps; here a flag) */
+#define LBFS_FLAG_RHO_RANGE 2u  /* rho <= 0 or rho > 1000 (same limit as LBFS.cu:2852)                       */
+#define LBFS_FLAG_IBM_RANGE 4u  /* a membrane node's IBM patch exceeded its bounding allocation            */
+
+/* ---- precision ----------------------------------------------------------- */
+#define LBFS_FP64 0             /* plain FP64: the drop-in                                   */
+#define LBFS_FP32_BULK 1        /* FP32 flux/gradient/IBM arithmetic, rho stored as rho-rho0,
+                                   FP64 reductions, FP64 node integration                     */
+
+/* ---- IBM kernels ---------------------------------------------------------- */
+#define LBFS_IBM_HAT2 2         /* 2-point hat stencil (immersed_boundary_method.cu:14-97, 947-1024) */
+#define LBFS_IBM_PESKIN4 4      /* 4-point Peskin cosine-free delta (new; no reference counterpart)  */
+
+/* Mesh arrays, in the reference's layout and order.  Sizes: nc = n_cells,
+ * nb = n_bc (boundary faces = ghost cells, ghost of bc face i is cell nc+i),
+ * nf = n_faces = n_interior + n_bc (boundary faces last).
+ * Source of every array: unstructured_mesh / gradients (Solver_gpu.cu:625-655). */
+typedef struct lbfs_mesh_desc {
+    int32_t n_cells, n_faces, n_interior, n_bc;
+    /* Axis-sorted prefix of the interior faces (x faces, then y, then z) for
+     * meshes whose interior faces are axis aligned (mesh_type 4..7, flux kernels
+     * calc_face_flux_x/_y/_z).  axis_aligned = 0 selects the general-normal
+     * reconstruction of calc_face_flux (mesh_type 3). */
+    int32_t n_face_x, n_face_y, n_face_z;
+    int32_t axis_aligned;
+    const int32_t *owner;          /* [nf]              mesh_owner              */
+    const int32_t *neighbour;      /* [nf]              mesh_neighbour (ghost index for bc faces) */
+    const double *face_area;       /* [nf]              surface_area            */
+    const double *face_normal;     /* [3*nf]            face_normal (unit)      */
+    const double *face_centroid;   /* [3*nf]            face_centroid           */
+    const double *streaming_dt;    /* [nf]              delta_t_face            */
+    const double *cell_volume;     /* [nc+nb]           cell_volume             */
+    const double *cell_centroid;   /* [3*(nc+nb)]       cell_centroid           */
+    const int32_t *gradient_stencil; /* [6*nc]          gradient_cells          */
+    const double *lhs_inverse;     /* [9*nc]  row major LHS_xx,LHS_xy,...,LHS_zz */
+    const double *rhs;             /* [18*nc] RHS_arr (6 neighbours x 3)        */
+    const int32_t *bc_rho_type;    /* [nb]    1 Dirichlet, 2 Neumann            */
+    const int32_t *bc_vel_type;    /* [nb]    1 Dirichlet, 2 Neumann, 9 duct, 10 shear */
+    const double *bc_values;       /* [4*nb]  (u, v, w, rho) = bcs_arr          */
+    /* Uniform Eulerian grid seen by the IBM stencils (Solver_gpu.cu:448, 538-544). */
+    double origin[3];              /* domain.origin_x/y/z                        */
+    double length[3];              /* domain.X/Y/Z                               */
+    double delta_x;                /* 2 * domain.dt                              */
+    double delta_h;                /* unstructured_mesh::get_delta_h()           */
+} lbfs_mesh_desc;
+
+/* Scalars of global_variables / initial_conditions used by the step. */
+typedef struct lbfs_params {
+    double visc;                /* globals.visc                                           */
+    double delta_t;             /* globals.time_marching_step (time_stepping = constant)   */
+    double gamma_inv;           /* 1 / globals.pre_conditioned_gamma                       */
+    double channel_diameter;    /* domain.Y (bc type 9)                                    */
+    double body_force[3];       /* init_conds.force_x/y/z                                  */
+    double ref_rho;             /* globals.ref_rho (residual normalisation)                */
+    double max_velocity;        /* globals.max_velocity (residual normalisation)           */
+    double rho0;                /* density offset carried by LBFS_FP32_BULK                */
+    double visc_factor_initial; /* visc_factor before the first interior-viscosity update */
+    int32_t testcase;           /* globals.testcase (8 = inviscid)                          */
+    int32_t precision;          /* LBFS_FP64 or LBFS_FP32_BULK                               */
+    int32_t ibm_stencil;        /* LBFS_IBM_HAT2 or LBFS_IBM_PESKIN4                         */
+    int32_t viscosity_period;   /* interior viscosity update when t % period == 1 (10000); 0 = never */
+} lbfs_params;
+
+/* One spring-network membrane (lagrangian_object with type == 2). */
+typedef struct lbfs_rbc_desc {
+    int32_t n_nodes, n_tris, n_springs;
+    const int32_t *tri;             /* [3*n_tris]   sorted_triIdx                         */
+    const int32_t *spring;          /* [4*n_springs] sprIdx (a, b, c, d): edge a-c, wings b, d */
+    const double *xyz_stress_free;  /* [3*n_nodes]  stress-free mesh (contour lengths, c0) */
+    const double *xyz_initial;      /* [3*n_nodes]  initial mesh (V0, A0, MAD0, angles)   */
+    double volume_modulus, local_area_modulus, global_area_modulus, shear_modulus;
+    double global_bending_modulus, local_bending_modulus, membrane_thickness, viscosity;
+    double wlc_ratio, curvature_ratio, volume_ratio, internal_viscosity_ratio, reference_length;
+    int32_t pivkin_length, sphere_reference;
+} lbfs_rbc_desc;
+
+typedef struct lbfs_solver lbfs_solver;
+
+/* Create a solver on CUDA device `device`, upload the mesh and membranes and
+ * run the membrane set-up (Solver_gpu.cu:659-735).  n_rbc may be 0.
+ * Replaces the set-up half of gpu_solver::General_Purpose_Solver_mk_i
+ * (Solver_gpu.cu:178-746). */
+int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params, const lbfs_rbc_desc *rbc, int32_t n_rbc,
+                int32_t device, lbfs_solver **out);
+int lbfs_destroy(lbfs_solver *s);
+
+/* Fluid state (primitive rho, u, v, w per interior cell), host arrays of n_cells.
+ * set_state also resets soln_t1 to the primitive state, as Solver_gpu.cu:746 does. */
+int lbfs_set_state(lbfs_solver *s, const double *rho, const double *u, const double *v, const double *w);
+int lbfs_get_state(lbfs_solver *s, double *rho, double *u, double *v, double *w);
+
+/* Advance n_steps time steps (one iteration of Solver_gpu.cu:749-1046 each).
+ * Enqueued on the solver's stream; returns without waiting. */
+int lbfs_step(lbfs_solver *s, int32_t n_steps);
+/* Same, with the per-step work replayed from a CUDA graph captured on first use. */
+int lbfs_step_graph(lbfs_solver *s, int32_t n_steps);
+int lbfs_synchronize(lbfs_solver *s);
+
+/* Use a caller stream (a cudaStream_t) instead of the solver's own. */
+int lbfs_set_stream(lbfs_solver *s, void *cuda_stream);
+
+/* Membrane node positions / velocities / forces of all membranes, host [3*total_nodes] (x,y,z per node). */
+int lbfs_get_nodes(lbfs_solver *s, int32_t which, double *out);
+int lbfs_set_nodes(lbfs_solver *s, const double *xyz);
+#define LBFS_NODES_POSITION 0
+#define LBFS_NODES_VELOCITY 1
+#define LBFS_NODES_FORCE 2
+
+/* Membrane totals, host [6*n_rbc]: V, V0, A, A0, MAD, MAD0 per membrane
+ * (lagrangian_object::total_volume ... total_MAD_0). */
+int lbfs_get_totals(lbfs_solver *s, double *out);
+/* RMS residuals of the last step, host [4]: rho, u, v, w (residuals::l2_norm_rms_moukallad). */
+int lbfs_get_residuals(lbfs_solver *s, double *out);
+
+/* Internal arrays for parity checking, copied to host.  Layouts:
+ *  LBFS_FIELD_GRADIENTS  [12*(nc+nb)]  per cell: grad rho, grad u, grad v, grad w (x,y,z each)
+ *  LBFS_FIELD_FACE_FLUX  [4*nf]        per face: (u, v, w, rho) components of res_face
+ *  LBFS_FIELD_RESIDUAL   [4*nc]        per cell: res_rho, res_u, res_v, res_w (forces included)
+ *  LBFS_FIELD_FORCE      [3*nc]        per cell: force density (body force + IBM spread)
+ *  LBFS_FIELD_T1         [4*nc]        per cell: soln_t1 (u, v, w, rho)
+ *  LBFS_FIELD_VISC       [nc]          per cell: visc_factor
+ *  LBFS_FIELD_GHOST      [4*nb]        per ghost: (u, v, w, rho)
+ *  LBFS_FIELD_SPRING     [9*total_springs] contour length, spring constant, curvature,
+ *                        curvature_0, angle_0, area_0[2], area[2]                     */
+int lbfs_get_field(lbfs_solver *s, int32_t which, double *out);
+#define LBFS_FIELD_GRADIENTS 0
+#define LBFS_FIELD_FACE_FLUX 1
+#define LBFS_FIELD_RESIDUAL 2
+#define LBFS_FIELD_FORCE 3
+#define LBFS_FIELD_T1 4
+#define LBFS_FIELD_VISC 5
+#define LBFS_FIELD_GHOST 6
+#define LBFS_FIELD_SPRING 7
+
+/* Keep the per-cell residuals of every step for lbfs_get_field(LBFS_FIELD_RESIDUAL).
+ * Off by default: it adds 32 bytes of writes per cell per step. */
+int lbfs_keep_residuals(lbfs_solver *s, int32_t on);
+
+/* Accumulated status flags (LBFS_FLAG_*) since creation; reading does not clear. */
+int lbfs_status(lbfs_solver *s, uint32_t *flags);
+/* Kernel launches issued per time step by this handle (graph or stream). */
+int lbfs_launches_per_step(lbfs_solver *s, int32_t *launches);
+/* Copy of the last error message (NUL terminated, truncated to len). */
+int lbfs_last_error(char *buf, int32_t len);
+
+/* ---- host-side set-up helpers ------------------------------------------- */
+
+/* Sizes of the uniform mesh generated for a domain X x Y x Z with streaming
+ * step dt (unstructured_mesh::create_uniform_openfoam_mesh, mesh_type 6):
+ * out[0..7] = n_cells, n_faces, n_interior, n_bc, n_face_x, n_face_y, n_face_z,
+ * n_cells + n_bc. */
+int lbfs_mesh_uniform_counts(double X, double Y, double Z, double dt, int32_t *out);
+
+/* Fill the mesh arrays of that uniform mesh (same ordering and geometry as
+ * unstructured_mesh.cpp:239-666, 1592-1692, 1963-1996 and
+ * gradients.cpp:214-315).  Output buffers must be sized from
+ * lbfs_mesh_uniform_counts; bc faces are tagged with patch ids
+ * 0 left, 1 right, 2 bottom, 3 top, 4 back, 5 front in bc_patch[nb].
+ * gradient_hybrid: 0 "LS", 1 "hybrid". */
+int lbfs_mesh_build_uniform(double X, double Y, double Z, double dt, const double *origin, double visc,
+                            double fneq_min, int32_t gradient_hybrid, int32_t *owner, int32_t *neighbour,
+                            double *face_area, double *face_normal, double *face_centroid, double *streaming_dt,
+                            double *cell_volume, double *cell_centroid, int32_t *gradient_stencil,
+                            double *lhs_inverse, double *rhs, int32_t *bc_patch, double *delta_h);
+
+/* Spring connectivity of a closed triangulated membrane, in the order the
+ * reference's Osay reader produces it (lagrangian_object.cpp:238-481).
+ * spring_out must hold 4 * capacity ints; *n_springs receives the count. */
+int lbfs_rbc_build_springs(int32_t n_nodes, int32_t n_tris, const int32_t *tri, int32_t capacity,
+                           int32_t *spring_out, int32_t *n_springs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBFS_B200_H */

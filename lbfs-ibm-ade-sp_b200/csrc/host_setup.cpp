@@ -1,0 +1,395 @@
+// Host-side set-up of the inputs the time step consumes: the uniform
+// OpenFOAM-layout hex mesh with its least-squares gradient geometry, and the
+// spring connectivity of a triangulated membrane.  These reproduce the
+// reference's orderings exactly (face order, gradient stencil order, sprIdx
+// order), because the step's results depend on them.
+//
+// Compiled with -ffp-contract=off so every multiply and add rounds on its own,
+// as the reference's host code does; the geometry is then bit-identical.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <unordered_set>
+#include <vector>
+
+#include "lbfs_b200.h"
+#include "lbfs_internal.h"
+
+namespace {
+
+struct V3 {
+    double x, y, z;
+};
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline double mag(V3 a) { return std::sqrt(std::pow(a.x, 2) + std::pow(a.y, 2) + std::pow(a.z, 2)); }
+
+struct UniformDims {
+    int nx, ny, nz;
+    double dx, dy, dz;
+    int n_cells, n_faces, n_interior, n_bc, n_fx, n_fy, n_fz;
+};
+
+// unstructured_mesh::create_uniform_openfoam_mesh, unstructured_mesh.cpp:252-401
+UniformDims uniform_dims(double X, double Y, double Z, double dt) {
+    UniformDims d;
+    d.nx = (int)std::ceil(X / dt * 0.5);
+    d.ny = (int)std::ceil(Y / dt * 0.5);
+    d.nz = (int)std::ceil(Z / dt * 0.5);
+    d.dx = X / d.nx;
+    d.dy = Y / d.ny;
+    d.dz = Z / d.nz;
+    d.n_cells = d.nx * d.ny * d.nz;
+    d.n_faces = (d.nx + 1) * d.ny * d.nz + d.nx * (d.ny + 1) * d.nz + d.nx * d.ny * (d.nz + 1);
+    d.n_interior = d.n_faces - 2 * d.ny * d.nx - 2 * d.nx * d.nz - 2 * d.ny * d.nz;
+    d.n_bc = d.n_faces - d.n_interior;
+    d.n_fx = (d.nx - 1) * d.ny * d.nz;
+    d.n_fy = d.nx * (d.ny - 1) * d.nz;
+    d.n_fz = d.nx * d.ny * (d.nz - 1);
+    return d;
+}
+
+}  // namespace
+
+extern "C" int lbfs_mesh_uniform_counts(double X, double Y, double Z, double dt, int32_t *out) {
+    if (!out || !(dt > 0) || !(X > 0) || !(Y > 0) || !(Z > 0)) return lbfs::set_error(LBFS_ERR_ARG, "bad domain");
+    UniformDims d = uniform_dims(X, Y, Z, dt);
+    if (d.nx < 2 || d.ny < 2 || d.nz < 2) return lbfs::set_error(LBFS_ERR_ARG, "mesh needs >= 2 cells per axis");
+    out[0] = d.n_cells; out[1] = d.n_faces; out[2] = d.n_interior; out[3] = d.n_bc;
+    out[4] = d.n_fx; out[5] = d.n_fy; out[6] = d.n_fz; out[7] = d.n_cells + d.n_bc;
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_mesh_build_uniform(double X, double Y, double Z, double dt, const double *origin, double visc,
+                                       double fneq_min, int32_t gradient_hybrid, int32_t *owner, int32_t *neighbour,
+                                       double *face_area, double *face_normal, double *face_centroid,
+                                       double *streaming_dt, double *cell_volume, double *cell_centroid,
+                                       int32_t *gradient_stencil, double *lhs_inverse, double *rhs, int32_t *bc_patch,
+                                       double *delta_h) {
+    int32_t cnt[8];
+    int rc = lbfs_mesh_uniform_counts(X, Y, Z, dt, cnt);
+    if (rc) return rc;
+    if (!origin || !owner || !neighbour || !face_area || !face_normal || !face_centroid || !streaming_dt ||
+        !cell_volume || !cell_centroid || !gradient_stencil || !lhs_inverse || !rhs || !bc_patch || !delta_h)
+        return lbfs::set_error(LBFS_ERR_ARG, "null output buffer");
+    UniformDims d = uniform_dims(X, Y, Z, dt);
+    const int nvx = d.nx + 1, nvy = d.ny + 1, nvz = d.nz + 1;
+    const int nc = d.n_cells, nf = d.n_faces, ni = d.n_interior, nt = nc + d.n_bc;
+
+    // Vertices are stored as float in the reference (unstructured_mesh.h:59).
+    std::vector<float> vx((size_t)nvx * nvy * nvz), vy(vx.size()), vz(vx.size());
+    {
+        size_t t = 0;
+        for (int k = 0; k < nvz; k++)
+            for (int j = 0; j < nvy; j++)
+                for (int i = 0; i < nvx; i++, t++) {
+                    vx[t] = (float)(origin[0] + i * d.dx);
+                    vy[t] = (float)(origin[1] + j * d.dy);
+                    vz[t] = (float)(origin[2] + k * d.dz);
+                }
+    }
+    // Face loop order and vertex winding: unstructured_mesh.cpp:415-664.
+    std::vector<int> fv((size_t)4 * nf);
+    int face = 0;
+    const int sxy = nvx * nvy;
+    auto put = [&](int a, int b, int c, int dd, int own, int nb) {
+        fv[4 * face] = a; fv[4 * face + 1] = b; fv[4 * face + 2] = c; fv[4 * face + 3] = dd;
+        owner[face] = own;
+        neighbour[face] = nb;
+        face++;
+    };
+    for (int k = 0; k < nvz - 1; k++)
+        for (int j = 0; j < nvy - 1; j++)
+            for (int i = 1; i < nvx - 1; i++) {
+                int a = k * sxy + j * nvx + i, b = a + nvx, c = b + sxy, dd = a + sxy;
+                int own = (i - 1) + j * d.nx + k * d.nx * d.ny;
+                put(a, b, c, dd, own, own + 1);
+            }
+    for (int k = 0; k < nvz - 1; k++)
+        for (int j = 1; j < nvy - 1; j++)
+            for (int i = 0; i < nvx - 1; i++) {
+                int a = k * sxy + j * nvx + i, b = a + sxy, c = b + 1, dd = a + 1;
+                int own = i + (j - 1) * d.nx + k * d.nx * d.ny;
+                put(a, b, c, dd, own, own + d.nx);
+            }
+    for (int k = 1; k < nvz - 1; k++)
+        for (int j = 0; j < nvy - 1; j++)
+            for (int i = 0; i < nvx - 1; i++) {
+                int a = k * sxy + j * nvx + i, b = a + 1, c = b + nvx, dd = c - 1;
+                int own = i + j * d.nx + (k - 1) * d.nx * d.ny;
+                put(a, b, c, dd, own, own + d.nx * d.ny);
+            }
+    int bci = 0;
+    for (int k = 0; k < nvz - 1; k++)
+        for (int j = 0; j < nvy - 1; j++) {  // left
+            int i = 0, a = k * sxy + j * nvx + i;
+            bc_patch[bci++] = 0;
+            put(a, a + sxy, a + nvx + sxy, a + nvx, i + j * d.nx + k * d.nx * d.ny, 0);
+        }
+    for (int k = 0; k < nvz - 1; k++)
+        for (int j = 0; j < nvy - 1; j++) {  // right
+            int i = nvx - 1, a = k * sxy + j * nvx + i, b = a + nvx;
+            bc_patch[bci++] = 1;
+            put(a, b, b + sxy, a + sxy, (i - 1) + j * d.nx + k * d.nx * d.ny, 0);
+        }
+    for (int k = 0; k < nvz - 1; k++)
+        for (int i = 0; i < nvx - 1; i++) {  // bottom
+            int j = 0, a = k * sxy + j * nvx + i;
+            bc_patch[bci++] = 2;
+            put(a, a + 1, a + sxy + 1, a + sxy, i + j * d.nx + k * d.nx * d.ny, 0);
+        }
+    for (int k = 0; k < nvz - 1; k++)
+        for (int i = 0; i < nvx - 1; i++) {  // top
+            int j = nvy - 1, a = k * sxy + j * nvx + i, b = a + sxy;
+            bc_patch[bci++] = 3;
+            put(a, b, b + 1, a + 1, i + (j - 1) * d.nx + k * d.nx * d.ny, 0);
+        }
+    for (int j = 0; j < nvy - 1; j++)
+        for (int i = 0; i < nvx - 1; i++) {  // back
+            int k = 0, a = k * sxy + j * nvx + i, b = a + nvx;
+            bc_patch[bci++] = 4;
+            put(a, b, b + 1, a + 1, i + j * d.nx + k * d.nx * d.ny, 0);
+        }
+    for (int j = 0; j < nvy - 1; j++)
+        for (int i = 0; i < nvx - 1; i++) {  // front
+            int k = nvz - 1, a = k * sxy + j * nvx + i, b = a + 1, c = b + nvx;
+            bc_patch[bci++] = 5;
+            put(a, b, c, c - 1, i + j * d.nx + (k - 1) * d.nx * d.ny, 0);
+        }
+
+    // Geometry: unstructured_mesh::generate_internal_mesh (unstructured_mesh.cpp:1592-1692),
+    // tet_volume (:1015-1040), cell_tet_area (:1170-1204), calc_face_delta_t (:1349-1446).
+    std::vector<double> cvol(nt, 0.0), csum_area(nt, 0.0), cx(nt, 0.0), cy(nt, 0.0), cz(nt, 0.0);
+    std::vector<std::vector<int>> gcells(nt), gfaces(nt);
+    const double reference_dt = visc * 3 / 1.0 / fneq_min;  // pre_conditioned_gamma = 1
+    for (int f = 0; f < nf; f++) {
+        V3 nd[4];
+        for (int q = 0; q < 4; q++) {
+            int t = fv[4 * f + q];
+            nd[q] = {(double)vx[t], (double)vy[t], (double)vz[t]};
+        }
+        for (int t = 0; t < 2; t++) {
+            V3 a = nd[0], b = sub(nd[t + 1], a), c = sub(nd[t + 2], a);
+            double vol = dot(a, cross(b, c)) / 6;
+            cvol[owner[f]] = cvol[owner[f]] + vol;
+            if (f < ni) cvol[neighbour[f]] = cvol[neighbour[f]] - vol;
+        }
+        double area_f = 0.0;
+        V3 fcen = {0, 0, 0}, fnorm = {0, 0, 0};
+        for (int t = 0; t < 2; t++) {
+            V3 a = nd[0], b = nd[t + 1], c = nd[t + 2];
+            V3 cen = {(a.x + b.x + c.x) / 3, (a.y + b.y + c.y) / 3, (a.z + b.z + c.z) / 3};
+            V3 n = cross(sub(b, a), sub(c, a));
+            double ar = 0.5 * mag(n);
+            area_f = area_f + ar;
+            double inv = 1 / ar;  // vector_var::factor divides by its argument
+            cen = {cen.x / inv, cen.y / inv, cen.z / inv};
+            fcen = add(fcen, cen);
+            fnorm = add(fnorm, n);
+        }
+        face_area[f] = area_f;
+        csum_area[owner[f]] = csum_area[owner[f]] + area_f;
+        cx[owner[f]] = cx[owner[f]] + fcen.x;
+        cy[owner[f]] = cy[owner[f]] + fcen.y;
+        cz[owner[f]] = cz[owner[f]] + fcen.z;
+        face_centroid[3 * f] = fcen.x / area_f;
+        face_centroid[3 * f + 1] = fcen.y / area_f;
+        face_centroid[3 * f + 2] = fcen.z / area_f;
+        double nm = mag(fnorm);
+        face_normal[3 * f] = fnorm.x / nm;
+        face_normal[3 * f + 1] = fnorm.y / nm;
+        face_normal[3 * f + 2] = fnorm.z / nm;
+        double face_dt = 0.5 * std::sqrt(area_f);
+        streaming_dt[f] = std::min(face_dt, reference_dt);
+        if (f > ni - 1) {
+            int g = f - ni + nc;
+            gcells[owner[f]].push_back(g);
+            gfaces[owner[f]].push_back(f);
+        } else {
+            int nb = neighbour[f];
+            csum_area[nb] = csum_area[nb] + area_f;
+            cx[nb] = cx[nb] + fcen.x;
+            cy[nb] = cy[nb] + fcen.y;
+            cz[nb] = cz[nb] + fcen.z;
+            gcells[owner[f]].push_back(nb);
+            gcells[nb].push_back(owner[f]);
+            gfaces[owner[f]].push_back(f);
+            gfaces[nb].push_back(f);
+        }
+    }
+    for (int i = 0; i < nc; i++) {
+        cx[i] = cx[i] / csum_area[i];
+        cy[i] = cy[i] / csum_area[i];
+        cz[i] = cz[i] / csum_area[i];
+    }
+    // ghost centroids: populate_ghost_cell_from_foam_face, unstructured_mesh.cpp:1963-1996
+    for (int f = ni; f < nf; f++) {
+        int g = nc + f - ni, o = owner[f];
+        double ex = (face_centroid[3 * f] - cx[o]) / 0.5;
+        double ey = (face_centroid[3 * f + 1] - cy[o]) / 0.5;
+        double ez = (face_centroid[3 * f + 2] - cz[o]) / 0.5;
+        cx[g] = cx[o] + ex;
+        cy[g] = cy[o] + ey;
+        cz[g] = cz[o] + ez;
+        neighbour[f] = g;
+    }
+    for (int i = 0; i < nt; i++) {
+        cell_volume[i] = cvol[i];
+        cell_centroid[3 * i] = cx[i];
+        cell_centroid[3 * i + 1] = cy[i];
+        cell_centroid[3 * i + 2] = cz[i];
+    }
+    double dh = std::min(d.dx, std::min(d.dy, d.dz)) * 0.5;
+    *delta_h = std::min(dh, 0.1);
+
+    // Least-squares / hybrid gradient geometry: gradients::pre_fill_LHS_and_RHS_matrix
+    // (gradients.cpp:214-315) and add_non_macrovariable_contributions (:149-211).
+    for (int i = 0; i < nc; i++) {
+        if (gcells[i].size() != 6) return lbfs::set_error(LBFS_ERR_ARG, "hex cell without 6 stencil entries");
+        double L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        double max_area = 0.0, max_disp = 0.0;
+        for (int q = 0; q < 6; q++) {
+            int i1 = gcells[i][q], f = gfaces[i][q];
+            max_area = std::max(max_area, face_area[f]);
+            double ddx = cx[i1] - cx[i], ddy = cy[i1] - cy[i], ddz = cz[i1] - cz[i];
+            max_disp = std::max(std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz), max_disp);
+        }
+        double aspect = 2 * std::fabs(max_disp) * max_area / cvol[i];
+        double beta = gradient_hybrid ? std::min(1.0, (2 / aspect)) : 1.0;
+        L[0] = L[0] + 2 * (1 - beta) * cvol[i];
+        L[4] = L[4] + 2 * (1 - beta) * cvol[i];
+        L[8] = L[8] + 2 * (1 - beta) * cvol[i];
+        for (int q = 0; q < 6; q++) {
+            int i1 = gcells[i][q], f = gfaces[i][q];
+            double fi = face_normal[3 * f], fj = face_normal[3 * f + 1], fk = face_normal[3 * f + 2];
+            double ddx = face_centroid[3 * f] - cx[i], ddy = face_centroid[3 * f + 1] - cy[i],
+                   ddz = face_centroid[3 * f + 2] - cz[i];
+            double l_norm = ddx * fi + ddy * fj + ddz * fk;
+            ddx = cx[i1] - cx[i]; ddy = cy[i1] - cy[i]; ddz = cz[i1] - cz[i];
+            double Ld = std::sqrt(std::pow(ddx, 2.0) + std::pow(ddy, 2.0) + std::pow(ddz, 2.0));
+            double s = face_area[f];
+            double L_norm = ddx * fi + ddy * fj + ddz * fk;
+            double alpha_w = std::pow(2 * l_norm / L_norm, 2.0);
+            double w = alpha_w * s / Ld;
+            L[0] = L[0] + w * ddx * ddx * beta; L[1] = L[1] + w * ddx * ddy * beta; L[2] = L[2] + w * ddx * ddz * beta;
+            L[3] = L[3] + w * ddy * ddx * beta; L[4] = L[4] + w * ddy * ddy * beta; L[5] = L[5] + w * ddy * ddz * beta;
+            L[6] = L[6] + w * ddz * ddx * beta; L[7] = L[7] + w * ddz * ddy * beta; L[8] = L[8] + w * ddz * ddz * beta;
+            double sgn = (owner[f] == i) ? 1.0 : -1.0;
+            double *R = rhs + 18 * i + 3 * q;
+            if (sgn > 0) {
+                R[0] = (beta * w * ddx + 2 * (1 - beta) * 0.5 * fi * s);
+                R[1] = (beta * w * ddy + 2 * (1 - beta) * 0.5 * fj * s);
+                R[2] = (beta * w * ddz + 2 * (1 - beta) * 0.5 * fk * s);
+            } else {
+                R[0] = (beta * w * ddx + 2 * (1 - beta) * 0.5 * fi * -1 * s);
+                R[1] = (beta * w * ddy + 2 * (1 - beta) * 0.5 * fj * -1 * s);
+                R[2] = (beta * w * ddz + 2 * (1 - beta) * 0.5 * fk * -1 * s);
+            }
+            gradient_stencil[6 * i + q] = i1;
+        }
+        // Determinant exactly as the reference forms it (gradients.cpp:282-284;
+        // its second cofactor is not the true one, which only matters on
+        // non-orthogonal meshes), then the adjugate / det.
+        double det = L[0] * (L[4] * L[8] - L[5] * L[7]) + L[1] * (L[3] * L[8] - L[5] - L[6]) +
+                     L[2] * (L[3] * L[7] - L[4] * L[6]);
+        double a = L[0], b = L[1], c = L[2], dd = L[3], e = L[4], f = L[5], g = L[6], h = L[7], k = L[8];
+        double *I = lhs_inverse + 9 * i;
+        I[0] = 1 / det * (e * k - f * h);
+        I[1] = 1 / det * (c * h - b * k);
+        I[2] = 1 / det * (b * f - c * e);
+        I[3] = 1 / det * (f * g - dd * k);
+        I[4] = 1 / det * (a * k - c * g);
+        I[5] = 1 / det * (c * dd - a * f);
+        I[6] = 1 / det * (dd * h - e * g);
+        I[7] = 1 / det * (b * g - a * h);
+        I[8] = 1 / det * (a * e - b * dd);
+    }
+    return LBFS_OK;
+}
+
+// Spring connectivity: the neighbour-ring construction, duplicate removal and
+// spring hashing of lagrangian_object::osay_mesh_read (lagrangian_object.cpp:
+// 299-481).  The ring is assembled by the same sequence of pair swaps, so the
+// (a, b, c, d) quadruples come out in the reference's order.
+extern "C" int lbfs_rbc_build_springs(int32_t n_nodes, int32_t n_tris, const int32_t *tri, int32_t capacity,
+                                      int32_t *spring_out, int32_t *n_springs) {
+    if (n_nodes <= 0 || n_tris <= 0 || !tri || !spring_out || !n_springs)
+        return lbfs::set_error(LBFS_ERR_ARG, "bad membrane arguments");
+    std::vector<std::vector<int>> ring(n_nodes);
+    std::vector<int> degree(n_nodes, 0);
+    for (int i = 0; i < 3 * n_tris; i++) {
+        if (tri[i] < 0 || tri[i] >= n_nodes) return lbfs::set_error(LBFS_ERR_ARG, "triangle index out of range");
+        degree[tri[i]]++;
+    }
+    for (int t = 0; t < n_tris; t++) {
+        int v0 = tri[3 * t], v1 = tri[3 * t + 1], v2 = tri[3 * t + 2];
+        ring[v0].push_back(v1); ring[v0].push_back(v2);
+        ring[v1].push_back(v2); ring[v1].push_back(v0);
+        ring[v2].push_back(v0); ring[v2].push_back(v1);
+    }
+    for (int i = 0; i < n_nodes; i++) {
+        std::vector<int> &r = ring[i];
+        if (r.size() < 4) return lbfs::set_error(LBFS_ERR_ARG, "node with fewer than two triangles");
+        size_t it = 1;
+        for (size_t t = 3; t < r.size(); t += 2) {
+            size_t j = it + 1;
+            while (j < r.size() && r[j] != r[it]) j++;
+            if (j == r.size()) return lbfs::set_error(LBFS_ERR_ARG, "membrane is not a closed manifold");
+            size_t num = j - it;
+            if (num % 2 == 0) {
+                if (it + num - 1 >= r.size()) return lbfs::set_error(LBFS_ERR_ARG, "membrane ring walk failed");
+                std::swap(r[it + 1], r[it + num]);
+                std::swap(r[it + 2], r[it + num - 1]);
+            } else {
+                if (it + num + 1 >= r.size()) return lbfs::set_error(LBFS_ERR_ARG, "membrane ring walk failed");
+                std::swap(r[it + 1], r[it + num]);
+                std::swap(r[it + 2], r[it + num + 1]);
+            }
+            it += 2;
+        }
+        // Remove repeated ids keeping the survivor the reference's uniquify
+        // keeps: positions sorted by value with std::sort, first of each run
+        // of equal values retained, survivors in original order.
+        std::vector<size_t> pos(r.size());
+        for (size_t q = 0; q < r.size(); q++) pos[q] = q;
+        std::sort(pos.begin(), pos.end(), [&](size_t a, size_t b) { return r[a] < r[b]; });
+        pos.erase(std::unique(pos.begin(), pos.end(), [&](size_t a, size_t b) { return r[a] == r[b]; }), pos.end());
+        std::sort(pos.begin(), pos.end());
+        std::vector<int> kept;
+        kept.reserve(pos.size());
+        for (size_t q : pos) kept.push_back(r[q]);
+        r.swap(kept);
+    }
+    long long total = 0;
+    for (int i = 0; i < n_nodes; i++) total += degree[i];
+    const int expected = (int)(total / 2);
+    if (expected > capacity) return lbfs::set_error(LBFS_ERR_LIMIT, "spring capacity too small");
+    const int factor = (int)std::ceil(std::log10((double)n_nodes));
+    std::unordered_set<long long> seen;
+    int count = 0;
+    for (int i = 0; i < n_nodes; i++) {
+        const std::vector<int> &r = ring[i];
+        const size_t m = r.size();
+        for (size_t j = 0; j < m; j++) {
+            int a = r[j], b = r[(j + 1) % m], c = r[(j + 2) % m];
+            int q[4] = {i, a, b, c};
+            std::sort(q, q + 4);
+            long long h = 0;
+            for (int t = 0; t < 4; t++) h = (long long)(h + q[t] * std::pow(10, factor * t));
+            if (seen.insert(h).second) {
+                if (count >= expected) return lbfs::set_error(LBFS_ERR_ARG, "more springs than edges");
+                spring_out[4 * count] = i;
+                spring_out[4 * count + 1] = a;
+                spring_out[4 * count + 2] = b;
+                spring_out[4 * count + 3] = c;
+                count++;
+            }
+        }
+    }
+    *n_springs = count;
+    return LBFS_OK;
+}

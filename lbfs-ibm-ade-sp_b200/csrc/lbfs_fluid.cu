@@ -1,0 +1,460 @@
+// Fluid kernels of one LBFS time step; see lbfs_fluid.cuh for the mapping to
+// the reference kernels they replace.
+#include <cuda_runtime.h>
+
+#include "lbfs_fluid.cuh"
+#include "lbfs_internal.h"
+#include "lbfs_kernels.h"
+
+namespace lbfs {
+
+// ------------------------------------------------------------------ K1 ----
+
+// Ghost-cell macros from the owner state (update_unstructured_bcs,
+// LBFS.cu:1868-1918).  Types outside {1,2} / {1,2,9,10} are rejected at
+// creation, so every branch here assigns.
+template <typename R>
+__device__ __forceinline__ Vec4<R> ghost_state(const FluidArgs<R> &a, int b, const Vec4<R> &own) {
+    const Vec4<R> bc = a.bc_val[b];
+    Vec4<R> g;
+    if (a.bc_rho_type[b] == 1) g.rho = bc.rho - (own.rho - bc.rho);
+    else g.rho = own.rho;
+    const int vt = a.bc_vel_type[b];
+    if (vt == 2) {
+        g.u = own.u; g.v = own.v; g.w = own.w;
+    } else {
+        R ut = bc.u;
+        if (vt == 9) {
+            const BcRec<R> r = a.bc_rec[b];
+            ut = (R)(16 * (double)bc.u * (a.H2 + r.gy) * (a.H2 - r.gy) * (a.H2 + r.gz) * (a.H2 - r.gz) / a.H4);
+        } else if (vt == 10) {
+            ut = a.bc_rec[b].gy * bc.u;
+        }
+        g.u = ut - (own.u - ut);
+        g.v = bc.v - (own.v - bc.v);
+        g.w = bc.w - (own.w - bc.w);
+    }
+    return g;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_cell_gradients(FluidArgs<R> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nc) return;
+    const Vec4<R> own = a.state[i];
+    R rr[3] = {0, 0, 0}, ru[3] = {0, 0, 0}, rv[3] = {0, 0, 0}, rw[3] = {0, 0, 0};
+    int st[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) st[q] = __ldg(a.stencil + 6 * i + q);
+    bool has_ghost = false;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        const int j = st[q];
+        Vec4<R> s;
+        if (j < a.nc) {
+            s = a.state[j];
+        } else {
+            s = ghost_state(a, j - a.nc, own);
+            has_ghost = true;
+        }
+        // add_LS_contributions, LBFS.cu:2051-2083
+        const R du = s.u - own.u, dv = s.v - own.v, dw = s.w - own.w, dr = s.rho - own.rho;
+        const R *R3 = a.rhs + 18 * i + 3 * q;
+        const R r0 = __ldg(R3), r1 = __ldg(R3 + 1), r2 = __ldg(R3 + 2);
+        rr[0] = rr[0] + r0 * dr; rr[1] = rr[1] + r1 * dr; rr[2] = rr[2] + r2 * dr;
+        ru[0] = ru[0] + r0 * du; ru[1] = ru[1] + r1 * du; ru[2] = ru[2] + r2 * du;
+        rv[0] = rv[0] + r0 * dv; rv[1] = rv[1] + r1 * dv; rv[2] = rv[2] + r2 * dv;
+        rw[0] = rw[0] + r0 * dw; rw[1] = rw[1] + r1 * dw; rw[2] = rw[2] + r2 * dw;
+    }
+    R L[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) L[q] = __ldg(a.lhs + 9 * i + q);
+    R g[12];
+    const R *rs[4] = {rr, ru, rv, rw};
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        g[3 * m + 0] = L[0] * rs[m][0] + L[1] * rs[m][1] + L[2] * rs[m][2];
+        g[3 * m + 1] = L[3] * rs[m][0] + L[4] * rs[m][1] + L[5] * rs[m][2];
+        g[3 * m + 2] = L[6] * rs[m][0] + L[7] * rs[m][1] + L[8] * rs[m][2];
+    }
+    R *gout = a.grad + (size_t)12 * i;
+#pragma unroll
+    for (int q = 0; q < 12; q++) gout[q] = g[q];
+    if (!has_ghost) return;
+    // Ghost states and ghost gradients of this cell's boundary faces
+    // (get_bc_gradients, LBFS.cu:1941-2044).
+    for (int q = 0; q < 6; q++) {
+        const int j = st[q];
+        if (j < a.nc) continue;
+        const int b = j - a.nc;
+        const Vec4<R> gs = ghost_state(a, b, own);
+        a.state[j] = gs;
+        const BcRec<R> r = a.bc_rec[b];
+        R gg[12];
+        const R d[4] = {gs.rho - own.rho, gs.u - own.u, gs.v - own.v, gs.w - own.w};
+        const bool dir_rho = a.bc_rho_type[b] == 1;
+        const bool dir_vel = a.bc_vel_type[b] != 2;
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const bool dirichlet = (m == 0) ? dir_rho : dir_vel;
+            if (dirichlet) {
+                gg[3 * m + 0] = d[m] / r.dmag * r.dnx;
+                gg[3 * m + 1] = d[m] / r.dmag * r.dny;
+                gg[3 * m + 2] = d[m] / r.dmag * r.dnz;
+            } else {
+                gg[3 * m + 0] = g[3 * m + 0] * r.mx;
+                gg[3 * m + 1] = g[3 * m + 1] * r.my;
+                gg[3 * m + 2] = g[3 * m + 2] * r.mz;
+            }
+        }
+        R *go = a.grad + (size_t)12 * j;
+#pragma unroll
+        for (int t = 0; t < 12; t++) go[t] = gg[t];
+    }
+}
+
+// ------------------------------------------------------------------ K2 ----
+
+struct Dir {
+    int ex, ey, ez;
+};
+__device__ __forceinline__ Dir dir_of(int k) { return {c_ex(k), c_ey(k), c_ez(k)}; }
+
+// Interface equilibrium, BGK relaxation towards the lattice equilibria and
+// the flux through the face: calculate_flux_at_interface (LBFS.cu:1462-1648)
+// and its axis-aligned forms (LBFS.cu:3648-4092).  `axis` < 0 selects the
+// general three-component form with the face normal; otherwise only the
+// directions crossing the face are formed.
+template <typename R>
+__device__ __forceinline__ Vec4<R> interface_flux(const R (&fl)[15], R rho0, R tau, R qscale, R area, int axis,
+                                                  R nx, R ny, R nz) {
+    R rho_dev = fl[0];
+#pragma unroll
+    for (int k = 1; k < 15; k++) rho_dev = rho_dev + fl[k];
+    R mx = 0, my = 0, mz = 0;
+#pragma unroll
+    for (int k = 1; k < 15; k++) {
+        const Dir e = dir_of(k);
+        if (e.ex) mx = (e.ex > 0) ? mx + fl[k] : mx - fl[k];
+        if (e.ey) my = (e.ey > 0) ? my + fl[k] : my - fl[k];
+        if (e.ez) mz = (e.ez > 0) ? mz + fl[k] : mz - fl[k];
+    }
+    const R rho_i = rho_dev + rho0;
+    const R inv = R(1) / rho_i;
+    const R ux = inv * mx, uy = inv * my, uz = inv * mz;
+    // flux tensors: F[c][m], c = face axis component (x,y,z), m = (mass, mom x, mom y, mom z)
+    R F[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+    for (int k = 1; k < 15; k++) {
+        const Dir e = dir_of(k);
+        if (axis == 0 && !e.ex) continue;
+        if (axis == 1 && !e.ey) continue;
+        if (axis == 2 && !e.ez) continue;
+        R f = feq_dev<R>(k, rho_dev, ux, uy, uz, rho0, qscale);
+        f = f - tau * (f - fl[k]);
+        const int ee[3] = {e.ex, e.ey, e.ez};
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (axis >= 0 && c != axis) continue;
+            if (!ee[c]) continue;
+            F[c][0] = (ee[c] > 0) ? F[c][0] + f : F[c][0] - f;
+#pragma unroll
+            for (int m = 0; m < 3; m++) {
+                if (!ee[m]) continue;
+                F[c][1 + m] = (ee[c] * ee[m] > 0) ? F[c][1 + m] + f : F[c][1 + m] - f;
+            }
+        }
+    }
+    Vec4<R> out;
+    if (axis >= 0) {
+        out.rho = F[axis][0] * area;
+        out.u = F[axis][1] * area;
+        out.v = F[axis][2] * area;
+        out.w = F[axis][3] * area;
+    } else {
+        out.rho = (F[0][0] * nx + F[1][0] * ny + F[2][0] * nz) * area;
+        out.u = (F[0][1] * nx + F[1][1] * ny + F[2][1] * nz) * area;
+        out.v = (F[0][2] * nx + F[1][2] * ny + F[2][2] * nz) * area;
+        out.w = (F[0][3] * nx + F[1][3] * ny + F[2][3] * nz) * area;
+    }
+    return out;
+}
+
+template <typename R> __device__ __forceinline__ void load_grad(const R *g, R (&o)[12]) {
+#pragma unroll
+    for (int t = 0; t < 12; t++) o[t] = __ldg(g + t);
+}
+
+// Axis-aligned face: populate_lattice_macros_uniform_{x,y,z} (LBFS.cu:2939-3644).
+// For direction k the lattice node sits at x_f - e_k dt; directions with
+// e_k[axis] = +1 extrapolate from the owner, -1 from the neighbour, 0 from the
+// face centre with the distance-weighted gradient.
+template <typename R, int axis>
+__device__ __forceinline__ Vec4<R> axis_face_flux(const FluidArgs<R> &a, int f) {
+    const int2 oc = __ldg(a.face_cells + f);
+    const AxisFace<R> geo = a.axis_face[f];
+    const Vec4<R> s1 = a.state[oc.x], s2 = a.state[oc.y];
+    R g1[12], g2[12];
+    load_grad(a.grad + (size_t)12 * oc.x, g1);
+    load_grad(a.grad + (size_t)12 * oc.y, g2);
+    const R dt = geo.dt, t1 = geo.t1, t2 = geo.t2;
+    const R c = t2 - t1;
+    const R wa = fabs(t2 / c), wb = fabs(t1 / c);
+    const R S1[4] = {s1.rho, s1.u, s1.v, s1.w}, S2[4] = {s2.rho, s2.u, s2.v, s2.w};
+    R pi[4], pn[4], p0[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        pi[m] = S1[m] - t1 * g1[3 * m + axis];
+        pn[m] = S2[m] - (t2 * g2[3 * m + axis]);
+        p0[m] = (pi[m] + pn[m]) * R(0.5);
+    }
+    constexpr int ob = axis == 0 ? 1 : 0;  // other axes in increasing order
+    constexpr int oc2 = axis == 2 ? 1 : 2;
+    R fl[15];
+#pragma unroll
+    for (int k = 0; k < 15; k++) {
+        const Dir e = dir_of(k);
+        const int ee[3] = {e.ex, e.ey, e.ez};
+        R L[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            R val;
+            if (ee[axis] > 0) {
+                val = pi[m] - g1[3 * m + axis] * dt;
+                if (ee[ob]) val = (ee[ob] > 0) ? val - g1[3 * m + ob] * dt : val + g1[3 * m + ob] * dt;
+                if (ee[oc2]) val = (ee[oc2] > 0) ? val - g1[3 * m + oc2] * dt : val + g1[3 * m + oc2] * dt;
+            } else if (ee[axis] < 0) {
+                val = pn[m] + g2[3 * m + axis] * dt;
+                if (ee[ob]) val = (ee[ob] > 0) ? val - g2[3 * m + ob] * dt : val + g2[3 * m + ob] * dt;
+                if (ee[oc2]) val = (ee[oc2] > 0) ? val - g2[3 * m + oc2] * dt : val + g2[3 * m + oc2] * dt;
+            } else {
+                val = p0[m];
+                if (ee[ob]) {
+                    const R gi = g1[3 * m + ob] * wa + g2[3 * m + ob] * wb;
+                    val = (ee[ob] > 0) ? val - gi * dt : val + gi * dt;
+                }
+                if (ee[oc2]) {
+                    const R gi = g1[3 * m + oc2] * wa + g2[3 * m + oc2] * wb;
+                    val = (ee[oc2] > 0) ? val - gi * dt : val + gi * dt;
+                }
+            }
+            L[m] = val;
+        }
+        fl[k] = feq_dev<R>(k, L[0], L[1], L[2], L[3], a.rho0, R(1));
+    }
+    const R vf = a.visc_factor[oc.x];
+    const R tau = (a.testcase == 8) ? R(0) : (a.visc * vf * R(3) / dt * a.gamma_inv);
+    return interface_flux<R>(fl, a.rho0, tau, R(1), geo.area, axis, 0, 0, 0);
+}
+
+// General face: populate_lattice_macros (LBFS.cu:323-936).  Faces whose
+// neighbour index is greater than n_cells take the boundary branch (the first
+// ghost, index n_cells, takes the interior branch as in the reference).
+template <typename R>
+__device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int f, bool is_bc) {
+    const int2 oc = __ldg(a.face_cells + f);
+    const GenFace<R> geo = a.gen_face[a.axis_aligned ? f - a.ni : f];
+    const Vec4<R> s1 = a.state[oc.x], s2 = a.state[oc.y];
+    R g1[12], g2[12];
+    load_grad(a.grad + (size_t)12 * oc.x, g1);
+    load_grad(a.grad + (size_t)12 * oc.y, g2);
+    const R dt = geo.dt;
+    const R S1[4] = {s1.rho, s1.u, s1.v, s1.w}, S2[4] = {s2.rho, s2.u, s2.v, s2.w};
+    R pi[4], pn[4], p0[4], g3[12];
+    if (oc.y > a.nc) {
+        const int b = oc.y - a.nc;
+        const Vec4<R> bc = a.bc_val[b];
+        const bool rd = a.bc_rho_type[b] == 1, vd = a.bc_vel_type[b] == 1;
+        const R bcv[4] = {bc.rho, bc.u, bc.v, bc.w};
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const bool dir = (m == 0) ? rd : vd;
+            p0[m] = dir ? bcv[m]
+                        : S1[m] - (geo.t1x * g2[3 * m] + geo.t1y * g2[3 * m + 1] + geo.t1z * g2[3 * m + 2]);
+            pi[m] = p0[m];
+            pn[m] = p0[m];
+        }
+#pragma unroll
+        for (int t = 0; t < 12; t++) { g3[t] = g2[t]; g1[t] = g2[t]; }
+    } else {
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            pi[m] = S1[m] - (geo.t1x * g1[3 * m] + geo.t1y * g1[3 * m + 1] + geo.t1z * g1[3 * m + 2]);
+            pn[m] = S2[m] - (geo.t2x * g2[3 * m] + geo.t2y * g2[3 * m + 1] + geo.t2z * g2[3 * m + 2]);
+            p0[m] = (pi[m] + pn[m]) * R(0.5);
+        }
+#pragma unroll
+        for (int t = 0; t < 12; t++) g3[t] = (g1[t] + g2[t]) * R(0.5);
+    }
+    // Upwind selection by the sign of n.e_k with the threshold 0.001 dt
+    // (LBFS.cu:351-352 override the sin(pi/14) arguments).
+    const R thr = R(0.001) * dt;
+    R fl[15];
+    fl[0] = feq_dev<R>(0, p0[0], p0[1], p0[2], p0[3], a.rho0, R(1));
+#pragma unroll
+    for (int k = 1; k < 15; k += 2) {
+        const Dir e = dir_of(k);
+        const R s = (k < 7) ? (e.ex ? geo.nx : (e.ey ? geo.ny : geo.nz))
+                            : (R(e.ex) * geo.nx + R(e.ey) * geo.ny + R(e.ez) * geo.nz);
+        // side of direction k and of its opposite k+1: 0 owner, 1 neighbour, 2 centre
+        const int side_k = (s > thr) ? 0 : ((s < -thr) ? 1 : 2);
+        const int side_o = (side_k == 2) ? 2 : 1 - side_k;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int kk = k + h;
+            const int side = h ? side_o : side_k;
+            const int ee[3] = {h ? -e.ex : e.ex, h ? -e.ey : e.ey, h ? -e.ez : e.ez};
+            R L[4];
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                R val = side == 0 ? pi[m] : (side == 1 ? pn[m] : p0[m]);
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    if (!ee[d]) continue;
+                    const R gd = side == 0 ? g1[3 * m + d] : (side == 1 ? g2[3 * m + d] : g3[3 * m + d]);
+                    val = (ee[d] > 0) ? val - gd * dt : val + gd * dt;
+                }
+                L[m] = val;
+            }
+            fl[kk] = feq_dev<R>(kk, L[0], L[1], L[2], L[3], a.rho0, R(1));
+        }
+    }
+    const R vf = is_bc ? R(1) : a.visc_factor[oc.x];
+    const R tau = (a.testcase == 8) ? R(0) : (a.visc * vf * R(3) / dt * a.gamma_inv);
+    return interface_flux<R>(fl, a.rho0, tau, a.gamma_inv, geo.area, -1, geo.nx, geo.ny, geo.nz);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_face_flux(FluidArgs<R> a) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= a.nf) return;
+    Vec4<R> out;
+    if (f >= a.ni) {
+        out = general_face_flux<R>(a, f, true);
+    } else if (a.axis_aligned) {
+        if (f < a.nfx) out = axis_face_flux<R, 0>(a, f);
+        else if (f < a.nfx + a.nfy) out = axis_face_flux<R, 1>(a, f);
+        else out = axis_face_flux<R, 2>(a, f);
+    } else {
+        out = general_face_flux<R>(a, f, false);
+    }
+    a.flux[f] = out;
+}
+
+// ------------------------------------------------------------------ K3 ----
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_cell_update(FluidArgs<R> a) {
+    __shared__ double sh[4][8];
+    __shared__ bool last_block;
+    double sq[4] = {0, 0, 0, 0};
+    unsigned int flag = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nc; i += gridDim.x * blockDim.x) {
+        const double vol = __ldg(a.cell_volume + i);
+        double r[4] = {0, 0, 0, 0};  // rho, u, v, w
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            const int e = __ldg(a.cell_faces + 6 * i + q);
+            const int f = (e > 0 ? e : -e) - 1;
+            const Vec4<R> fx = a.flux[f];
+            const double fv[4] = {(double)fx.rho, (double)fx.u, (double)fx.v, (double)fx.w};
+#pragma unroll
+            for (int m = 0; m < 4; m++) r[m] = (e > 0) ? r[m] + (-fv[m] / vol) : r[m] + fv[m] / vol;
+        }
+        double fx = a.force[0], fy = a.force[1], fz = a.force[2];
+        if (a.n_membranes > 0) {
+            const int ci = i % a.grid_nx, cj = (i / a.grid_nx) % a.grid_ny, ck = i / (a.grid_nx * a.grid_ny);
+            const MembraneScalars *ms = (const MembraneScalars *)a.membrane_scalars;
+            for (int m = 0; m < a.n_membranes; m++) {
+                const int px = ci - ms[m].patch_lo[0], py = cj - ms[m].patch_lo[1], pz = ck - ms[m].patch_lo[2];
+                if (ms[m].patch_cells > 0 && px >= 0 && py >= 0 && pz >= 0 && px < ms[m].patch_dim[0] &&
+                    py < ms[m].patch_dim[1] && pz < ms[m].patch_dim[2]) {
+                    const double *pf = a.patch_force + ((size_t)m * kMaxPatchCells +
+                                                        (px + ms[m].patch_dim[0] * (py + ms[m].patch_dim[1] * pz))) * 3;
+                    fx = fx + pf[0];
+                    fy = fy + pf[1];
+                    fz = fz + pf[2];
+                }
+            }
+        }
+        r[1] = r[1] + fx;
+        r[2] = r[2] + fy;
+        r[3] = r[3] + fz;
+        double4 t = a.t1[i];
+        t.w = t.w + a.delta_t * r[0];
+        t.x = t.x + a.delta_t * r[1];
+        t.y = t.y + a.delta_t * r[2];
+        t.z = t.z + a.delta_t * r[3];
+        a.t1[i] = t;
+        Vec4<R> s;
+        s.rho = (R)(t.w - (double)a.rho0);
+        s.u = (R)(t.x / t.w);
+        s.v = (R)(t.y / t.w);
+        s.w = (R)(t.z / t.w);
+        a.state[i] = s;
+        if (a.res_out) {
+            a.res_out[4 * i] = r[0]; a.res_out[4 * i + 1] = r[1];
+            a.res_out[4 * i + 2] = r[2]; a.res_out[4 * i + 3] = r[3];
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++) sq[m] = sq[m] + r[m] * r[m];
+        if (!(isfinite(t.w) && isfinite(t.x) && isfinite(t.y) && isfinite(t.z))) flag |= LBFS_FLAG_NONFINITE;
+        else if (!(t.w > 0.0) || t.w > 1000.0) flag |= LBFS_FLAG_RHO_RANGE;
+    }
+    if (flag) atomicOr(a.flags, flag);
+    // Block partial sums of the squared residuals (fixed order: warp tree, then warps in order).
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        double v = sq[m];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[m][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int m = 0; m < 4; m++) {
+            double v = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sh[m][w];
+            a.partials[4 * blockIdx.x + m] = v;
+        }
+        __threadfence();
+        const unsigned int prev = atomicAdd(a.ticket, 1u);
+        last_block = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last_block && threadIdx.x < 4) {
+        __threadfence();
+        const int m = threadIdx.x;
+        double v = 0;
+        for (int b = 0; b < (int)gridDim.x; b++) v += ((volatile double *)a.partials)[4 * b + m];
+        a.residual_sums[m] = v;
+        if (m == 0) *a.ticket = 0u;
+    }
+}
+
+// ------------------------------------------------------------ launchers ----
+
+template <typename R> int k3_grid(const FluidArgs<R> &a) {
+    int g = (a.nc + 255) / 256;
+    return g < kK3MaxBlocks ? g : kK3MaxBlocks;
+}
+
+template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStream_t s) {
+    k_cell_gradients<R><<<(a.nc + 255) / 256, 256, 0, s>>>(a);
+}
+template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s) {
+    k_face_flux<R><<<(a.nf + 127) / 128, 128, 0, s>>>(a);
+}
+template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s) {
+    k_cell_update<R><<<k3_grid(a), 256, 0, s>>>(a);
+}
+
+template void launch_fluid_gradients<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_flux<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_update<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_gradients<float>(const FluidArgs<float> &, cudaStream_t);
+template void launch_fluid_flux<float>(const FluidArgs<float> &, cudaStream_t);
+template void launch_fluid_update<float>(const FluidArgs<float> &, cudaStream_t);
+
+}  // namespace lbfs

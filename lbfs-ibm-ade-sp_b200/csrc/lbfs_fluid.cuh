@@ -1,0 +1,146 @@
+// Fluid-side kernels of one LBFS time step (sm_100a).
+//
+//   K1 cell_gradients : ghost-cell update + least-squares cell gradients +
+//                       ghost gradients, one thread per interior cell.
+//                       Replaces update_unstructured_bcs (LBFS.cu:1843-1928),
+//                       get_interior_gradients (LBFS.cu:2177-2240) and
+//                       get_bc_gradients (LBFS.cu:1933-2048).
+//   K2 face_flux      : D3Q15 reconstruction at the face lattice nodes,
+//                       equilibria, interface BGK relaxation and the face flux,
+//                       one thread per face, all in registers.  Replaces
+//                       calc_face_flux_x/_y/_z (LBFS.cu:2283-2569),
+//                       calc_face_flux (LBFS.cu:2574-2687) and calc_face_flux_bc
+//                       (LBFS.cu:2691-2810).
+//   K3 cell_update    : deterministic gather of the face fluxes of each cell,
+//                       body + IBM force, forward-Euler update of soln_t1 and
+//                       of the primitive state, residual partial sums, status
+//                       flags.  Replaces add_face_flux_to_cell (LBFS.cu:2242-2281,
+//                       8 CAS atomics per face), add (common_kernels.cu:220-233),
+//                       time_integration (LBFS.cu:2089-2172), square + total<128>
+//                       (Solver_gpu.cu:1033-1046).
+//
+// Storage type R is double (the drop-in) or float (the FP32-bulk form).  In
+// the float form the density is carried as rho' = rho - rho0 and every
+// equilibrium as f' = f - w_k rho0; the two forms are the same algebra (the
+// reconstruction and the BGK relaxation are linear in f), except that the
+// constant normal-momentum flux rho0/3 * n * area is left out, which cancels
+// exactly in the sum over the closed faces of each cell.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace lbfs {
+
+// D3Q15 velocity set (gpu_solver::populate_e_alpha, Solver_gpu.cu:1407-1445):
+//   ex = {0, 1,-1, 0, 0, 0, 0, 1,-1, 1,-1, 1,-1,-1, 1}
+//   ey = {0, 0, 0, 1,-1, 0, 0, 1,-1, 1,-1,-1, 1, 1,-1}
+//   ez = {0, 0, 0, 0, 0, 1,-1, 1,-1,-1, 1, 1,-1, 1,-1}
+// as constexpr functions so that fully unrolled loops fold every branch.
+__host__ __device__ constexpr int c_ex(int k) {
+    return (k == 1 || k == 7 || k == 9 || k == 11 || k == 14) ? 1 : ((k == 2 || k == 8 || k == 10 || k == 12 || k == 13) ? -1 : 0);
+}
+__host__ __device__ constexpr int c_ey(int k) {
+    return (k == 3 || k == 7 || k == 9 || k == 12 || k == 13) ? 1 : ((k == 4 || k == 8 || k == 10 || k == 11 || k == 14) ? -1 : 0);
+}
+__host__ __device__ constexpr int c_ez(int k) {
+    return (k == 5 || k == 7 || k == 10 || k == 11 || k == 13) ? 1 : ((k == 6 || k == 8 || k == 9 || k == 12 || k == 14) ? -1 : 0);
+}
+
+template <typename R> struct Vec4 { R u, v, w, rho; };
+
+template <typename R> __host__ __device__ constexpr R lattice_w(int k) {
+    return k == 0 ? R(2.0 / 9.0) : (k < 7 ? R(1.0 / 9.0) : R(1.0 / 72.0));
+}
+
+// Equilibrium deviation  f'_k = w_k (rho' (1 + X) + rho0 X),
+// X = 3 e.u + 4.5 (e.u)^2 - 1.5 |u|^2, with the term grouping of
+// populate_feq_lattice_explicit (LBFS.cu:1041-1354).  With rho0 = 0 it is the
+// reference's equilibrium w_k rho (1 + X) evaluated as w_k (rho (1 + X)).
+template <typename R>
+__device__ __forceinline__ R feq_dev(int k, R rho, R u, R v, R w, R rho0, R qscale) {
+    const R uu2 = u * u * qscale, vv2 = v * v * qscale, ww2 = w * w * qscale;
+    const R u2v2w2 = (uu2 + vv2 + ww2) * R(1.5);
+    const int ex = c_ex(k), ey = c_ey(k), ez = c_ez(k);
+    R X;
+    if (k == 0) {
+        X = -u2v2w2;
+    } else if (k < 7) {
+        const R comp = ex ? u : (ey ? v : w);
+        const R comp2 = ex ? uu2 : (ey ? vv2 : ww2);
+        const R s = R(ex + ey + ez);
+        X = s * R(3.0) * comp + R(4.5) * comp2 - u2v2w2;
+    } else {
+        const R uv = u * v * R(9.0) * qscale, uw = u * w * R(9.0) * qscale, vw = v * w * R(9.0) * qscale;
+        X = R(ex) * R(3.0) * u + R(ey) * R(3.0) * v + R(ez) * R(3.0) * w + R(ex * ey) * uv + R(ex * ez) * uw +
+            R(ey * ez) * vw + R(4.5) * uu2 + R(4.5) * vv2 + R(4.5) * ww2 - u2v2w2;
+    }
+    return lattice_w<R>(k) * (rho * (R(1.0) + X) + rho0 * X);
+}
+
+}  // namespace lbfs
+
+namespace lbfs {
+
+// Per-boundary-face record used by K1 (ghost state and ghost gradient).
+// d = ghost centroid - owner centroid, dmag = |d|, dn = d / dmag
+// (get_bc_gradients, LBFS.cu:1968-1979); m = 1 - |face normal| (Neumann);
+// gy, gz = ghost centroid y, z (bc types 9 and 10, LBFS.cu:1885-1913).
+template <typename R> struct BcRec {
+    R dmag, dnx, dny, dnz, mx, my, mz, gy, gz;
+};
+
+// Face geometry of an axis-aligned interior face: area, streaming dt,
+// t1 = owner centroid - face centroid and t2 = neighbour centroid - face
+// centroid along the face axis (LBFS.cu:2313-2315, 2950-2951).
+template <typename R> struct AxisFace {
+    R area, dt, t1, t2;
+};
+
+// Face geometry of a general face (boundary faces always; interior faces of
+// meshes that are not axis aligned): area, dt, unit normal, and the full
+// vectors t1 = c_owner - x_face, t2 = c_neighbour - x_face (LBFS.cu:335-337).
+template <typename R> struct GenFace {
+    R area, dt, nx, ny, nz, t1x, t1y, t1z, t2x, t2y, t2z, pad;
+};
+
+template <typename R> struct FluidArgs {
+    int nc, nf, ni, nb, nfx, nfy, nfz, axis_aligned;
+    int testcase;
+    R rho0;          // density offset of the stored state (0 in FP64)
+    R gamma_inv, visc;
+    double delta_t, H2, H4;
+    double force[3];
+    // state and gradients
+    Vec4<R> *state;              // [nc+nb]
+    R *grad;                     // [12*(nc+nb)] rho(x,y,z) u(x,y,z) v(x,y,z) w(x,y,z)
+    // K1 geometry
+    const int *stencil;          // [6*nc]
+    const R *rhs;                // [18*nc]
+    const R *lhs;                // [9*nc]
+    const int *bc_rho_type, *bc_vel_type;
+    const Vec4<R> *bc_val;       // [nb] (u, v, w, rho - rho0)
+    const BcRec<R> *bc_rec;      // [nb]
+    // K2 geometry
+    const int2 *face_cells;      // [nf] owner, neighbour
+    const AxisFace<R> *axis_face;  // [ni] when axis_aligned
+    const GenFace<R> *gen_face;  // [nb] bc faces, or [nf] when not axis aligned (indexed by face)
+    const R *visc_factor;        // [nc]
+    Vec4<R> *flux;               // [nf]
+    // K3
+    const int *cell_faces;       // [6*nc] +(f+1) owner, -(f+1) neighbour
+    const double *cell_volume;   // [nc]
+    double4 *t1;                 // [nc] (u, v, w, rho) conservative accumulator, FP64
+    double *res_out;             // [4*nc] residuals kept for parity checks (null = not stored)
+    // IBM patches (one per membrane)
+    int n_membranes, grid_nx, grid_ny;
+    const void *membrane_scalars;  // MembraneScalars[n_membranes]
+    const double *patch_force;   // [n_membranes * kMaxPatchCells * 3]
+    // reductions and flags
+    double *partials;            // [4 * gridDim of K3]
+    unsigned int *ticket;
+    double *residual_sums;       // [4] sum of squares of the last step
+    unsigned int *flags;
+};
+
+}  // namespace lbfs

@@ -1,0 +1,48 @@
+// Internal declarations shared by the host runtime and the kernels.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include "lbfs_b200.h"
+
+namespace lbfs {
+
+// Thread-local last-error text behind lbfs_last_error; returns `code`.
+int set_error(int code, const std::string &msg);
+
+// Largest membrane patch (cells of the IBM stencil's bounding box) a membrane
+// may cover; 48^3 cells covers a red cell of radius 8 cells deformed to twice
+// its diameter with the 4-point stencil margin.
+constexpr int kMaxPatchCells = 48 * 48 * 48;
+// Threads of the one-CTA-per-membrane kernel (512 leaves 128 registers per
+// thread for the spring-force derivatives).
+constexpr int kMembraneThreads = 512;
+// Largest membrane handled by one CTA (nodes; springs = 3 (nodes - 2)).
+constexpr int kMaxMembraneNodes = 16384;
+
+// D3Q15 weights and velocities, ordering of gpu_solver::populate_e_alpha
+// (Solver_gpu.cu:1407-1445).
+constexpr int kQ = 15;
+
+// Per-membrane device-side scalars (one record per membrane).
+struct MembraneScalars {
+    double V, V0, A, A0, MAD, MAD0;
+    double bbox_lo[3], bbox_hi[3];   // node coordinate bounds (interior viscosity test)
+    int patch_lo[3], patch_dim[3];   // IBM patch: first cell and extent per axis
+    int patch_cells;                 // product of patch_dim (0 when the patch overflowed)
+    int pad;
+};
+
+// Per-membrane constants (moduli) and ranges into the concatenated arrays.
+struct MembraneConst {
+    int node0, n_nodes, tri0, n_tris, spring0, n_springs;
+    int inc0;  // start of this membrane's node->(spring,slot) incidence list
+    int pad;
+    double volume_modulus, local_area_modulus, global_area_modulus, shear_modulus;
+    double global_bending_modulus, local_bending_modulus, membrane_thickness, viscosity;
+    double wlc_ratio, curvature_ratio, volume_ratio, internal_viscosity_ratio, reference_length;
+    int pivkin_length, sphere_reference;
+};
+
+}  // namespace lbfs

@@ -1,0 +1,70 @@
+// Launch wrappers shared by the runtime and the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "lbfs_fluid.cuh"
+#include "lbfs_internal.h"
+
+namespace lbfs {
+
+constexpr int kK3MaxBlocks = 148 * 8;
+
+template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStream_t s);
+template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s);
+template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s);
+
+// Membrane work modes.
+enum MembraneMode : int {
+    kModeReference = 0,  // stress-free mesh: contour lengths, spring constants, reference curvature
+    kModeInitial = 1,    // initial mesh: V0, A0, MAD0, spring_area_0, spring_angle_0
+    kModeStep = 2,       // one time step: interpolate, advect, forces, spread
+};
+
+struct MembraneArgs {
+    int n_membranes;
+    int mode;
+    int ibm_stencil;             // 2 or 4
+    double delta_t;
+    // fluid state (read) and IBM grid
+    const void *state;           // Vec4<R>[nc]
+    int state_is_float;
+    int nc, grid_nx, grid_ny, grid_nz;
+    double origin[3];
+    double delta_x;
+    // membranes
+    const MembraneConst *mc;     // [n_membranes]
+    MembraneScalars *ms;         // [n_membranes]
+    const int *tri;              // [3*total_tris]   global node ids
+    const int *spring;           // [4*total_springs] global node ids
+    const int *inc;              // node -> 4*spring + slot, CSR by node (in spring order)
+    const int *inc_start;        // [total_nodes + 1]
+    double *x, *y, *z;           // node positions [total_nodes]
+    double *vx, *vy, *vz;        // node velocities
+    double *fx, *fy, *fz;        // node forces
+    double *contour, *kspring, *curv, *curv0, *angle0, *area0, *area; // per spring (area, area0: 2 per spring)
+    double *contrib;             // [12*total_springs] per-spring node forces (scratch)
+    unsigned long long *keys;    // [total_nodes] bin keys (scratch)
+    double *patch_force;         // [n_membranes * kMaxPatchCells * 3]
+    unsigned int *flags;
+    int sort_capacity;           // power of two >= nodes of the largest membrane
+};
+
+void membrane_prepare(int sort_capacity);
+void launch_membrane(const MembraneArgs &a, cudaStream_t s);
+
+struct ViscArgs {
+    int nc, n_membranes;
+    const double *centroid;      // [3*nc]
+    const MembraneConst *mc;
+    const MembraneScalars *ms;
+    const int *tri;
+    const double *x, *y, *z;
+    double delta_h;
+    void *visc_factor;           // R[nc]
+    int visc_is_float;
+};
+
+void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s);
+
+}  // namespace lbfs

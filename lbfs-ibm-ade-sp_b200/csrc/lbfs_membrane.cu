@@ -1,0 +1,623 @@
+// Membrane side of one time step, one CTA (512 threads) per membrane:
+//
+//   P0  IBM velocity interpolation at the nodes + explicit node advection
+//       (interpolate_velocities_on_nodes, immersed_boundary_method.cu:14-97;
+//        update_node_positions, :234-264), FP64 positions.
+//   P1  triangle normals / areas / signed volumes and the membrane totals V, A
+//       (update_spring_network_tet_parameters, spring_network.cu:1186-1238, and
+//        the host sums of total<128> partials, lagrangian_object.cpp:601-630),
+//       reduced with warp shuffles in a fixed order.
+//   P2  per-spring WLC, local/global area, volume, bending, ADE (MAD) and
+//       membrane-viscosity forces (get_spring_forces_atomics,
+//       spring_network.cu:613-971), written per spring instead of 12 atomics.
+//   P3  node forces: each node sums its springs' contributions in spring order
+//       (deterministic; replaces the CAS atomics).
+//   P4  MAD = sum over the first n_nodes springs of c (A1 + A2) / 3, / A
+//       (sum_product_curvature<128> + lagrangian_object::add_MAD).
+//   P5  nodes sorted by the Eulerian cell at the base of their IBM stencil
+//       (bitonic sort of (cell, node) keys in shared memory).
+//   P6  force spreading as a per-cell segmented reduction over the sorted
+//       nodes into a dense patch around the membrane (replaces
+//       spread_forces_on_structured_grid, :947-1024, and its CAS atomics).
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "lbfs_fluid.cuh"
+#include "lbfs_internal.h"
+#include "lbfs_kernels.h"
+
+namespace lbfs {
+namespace {
+
+struct D3 {
+    double x, y, z;
+};
+__device__ __forceinline__ D3 d3(double x, double y, double z) { return {x, y, z}; }
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 operator*(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ D3 operator/(D3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 cross(D3 a, D3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ D3 tri_centroid(D3 a, D3 b, D3 c) {
+    return {(a.x + b.x + c.x) / 3, (a.y + b.y + c.y) / 3, (a.z + b.z + c.z) / 3};
+}
+
+// Deterministic block reductions: warp shuffle tree, then the warp results
+// in warp order by one thread.  `sh` holds 33 doubles.
+__device__ double block_sum(double v, double *sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += sh[w];
+        sh[32] = s;
+    }
+    __syncthreads();
+    const double r = sh[32];
+    __syncthreads();
+    return r;
+}
+__device__ double block_minmax(double v, double *sh, bool is_min) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double u = __shfl_down_sync(0xffffffffu, v, o);
+        v = is_min ? fmin(v, u) : fmax(v, u);
+    }
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = sh[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) s = is_min ? fmin(s, sh[w]) : fmax(s, sh[w]);
+        sh[32] = s;
+    }
+    __syncthreads();
+    const double r = sh[32];
+    __syncthreads();
+    return r;
+}
+__device__ int block_min_int(int v, int *sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_down_sync(0xffffffffu, v, o));
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = sh[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) s = min(s, sh[w]);
+        sh[32] = s;
+    }
+    __syncthreads();
+    const int r = sh[32];
+    __syncthreads();
+    return r;
+}
+
+// Peskin's 4-point delta, phi(r) for |r| < 2 (Peskin, Acta Numerica 2002, eq. 6.27).
+__device__ __forceinline__ double peskin4(double r) {
+    r = fabs(r);
+    if (r < 1.0) return (3.0 - 2.0 * r + sqrt(1.0 + 4.0 * r - 4.0 * r * r)) * 0.125;
+    if (r < 2.0) return (5.0 - 2.0 * r - sqrt(-7.0 + 12.0 * r - 4.0 * r * r)) * 0.125;
+    return 0.0;
+}
+
+// Stencil reference coordinates of a node (immersed_boundary_method.cu:45-58:
+// y and z are mirrored with fabs as in the reference) and the first stencil
+// cell per axis: round(r) - 1 for the 2-point hat, floor(r - 0.5) - 1 for the
+// 4-point delta.
+struct Stencil {
+    double rx, ry, rz;
+    int i0, j0, k0;
+};
+__device__ __forceinline__ Stencil node_stencil(const MembraneArgs &a, double x, double y, double z) {
+    Stencil s;
+    s.rx = (x - a.origin[0]) / a.delta_x;
+    s.ry = fabs((y - a.origin[1]) / a.delta_x);
+    s.rz = fabs((z - a.origin[2]) / a.delta_x);
+    if (a.ibm_stencil == LBFS_IBM_PESKIN4) {
+        s.i0 = (int)floor(s.rx - 0.5) - 1;
+        s.j0 = (int)floor(s.ry - 0.5) - 1;
+        s.k0 = (int)floor(s.rz - 0.5) - 1;
+    } else {
+        s.i0 = (int)round(s.rx) - 1;
+        s.j0 = (int)round(s.ry) - 1;
+        s.k0 = (int)round(s.rz) - 1;
+    }
+    return s;
+}
+__device__ __forceinline__ double stencil_weight(int stencil, double d) {
+    return stencil == LBFS_IBM_PESKIN4 ? peskin4(d) : 1 - fabs(d);
+}
+
+template <typename R>
+__device__ __forceinline__ void read_velocity(const void *state, int idx, double &u, double &v, double &w) {
+    const Vec4<R> s = ((const Vec4<R> *)state)[idx];
+    u = (double)s.u;
+    v = (double)s.v;
+    w = (double)s.w;
+}
+
+// ---- per-spring force (get_spring_forces_atomics, spring_network.cu:613-971) ----
+
+// Derivatives of the triangle normal N = (q - p) x (r - p) with respect to the
+// coordinates of p, q, r (get_d_normals, spring_network.cu:1348-1414):
+// dN[9 s + 3 c + k] = dN_k / d(node s)_c, s = 0 p, 1 q, 2 r; and the derivative
+// of the signed volume term N . centroid / 6 scaled by 6: dV[3 s + c].
+__device__ __forceinline__ void d_normals(D3 a, D3 b, D3 c, D3 normal, double *dN, double *dV) {
+    const D3 cen = tri_centroid(a, b, c);
+    dN[0] = 0.0;        dN[1] = c.z - b.z;  dN[2] = b.y - c.y;
+    dN[3] = b.z - c.z;  dN[4] = 0.0;        dN[5] = c.x - b.x;
+    dN[6] = c.y - b.y;  dN[7] = b.x - c.x;  dN[8] = 0.0;
+    dN[9] = 0.0;        dN[10] = a.z - c.z; dN[11] = c.y - a.y;
+    dN[12] = c.z - a.z; dN[13] = 0.0;       dN[14] = a.x - c.x;
+    dN[15] = a.y - c.y; dN[16] = c.x - a.x; dN[17] = 0.0;
+    dN[18] = 0.0;       dN[19] = b.z - a.z; dN[20] = a.y - b.y;
+    dN[21] = a.z - b.z; dN[22] = 0.0;       dN[23] = b.x - a.x;
+    dN[24] = b.y - a.y; dN[25] = a.x - b.x; dN[26] = 0.0;
+    normal = normal / 3.0;
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+        dV[3 * s + 0] = normal.x + dN[9 * s + 1] * cen.y + dN[9 * s + 2] * cen.z;
+        dV[3 * s + 1] = normal.y + dN[9 * s + 3] * cen.x + dN[9 * s + 5] * cen.z;
+        dV[3 * s + 2] = normal.z + dN[9 * s + 6] * cen.x + dN[9 * s + 7] * cen.y;
+    }
+}
+// Projection of dN on the unit normal (get_d_norms, spring_network.cu:1419-1428).
+__device__ __forceinline__ void d_norms(double *dn, const double *dN, double norm, D3 normal) {
+    normal = normal / norm;
+#pragma unroll
+    for (int i = 0; i < 9; i++) dn[i] = dN[3 * i] * normal.x + dN[3 * i + 1] * normal.y + dN[3 * i + 2] * normal.z;
+}
+// Merge the two triangles' 9-vectors (nodes a,b,c and c,d,a) into the 12-vector
+// over nodes (a, b, c, d) the way the reference assembles d_area / d_volume / d_angle.
+__device__ __forceinline__ void merge12(double *out, const double *t1, const double *t2) {
+#pragma unroll
+    for (int j = 0; j < 9; j++) out[j] = t1[j];
+#pragma unroll
+    for (int j = 0; j < 3; j++) out[j + 6] += t2[j];
+#pragma unroll
+    for (int j = 3; j < 6; j++) out[j + 6] = t2[j];
+#pragma unroll
+    for (int j = 6; j < 9; j++) out[j - 6] += t2[j];
+}
+
+struct SpringGeom {
+    D3 a, b, c, d, normal_a, normal_b;
+    double norm_1, norm_2, length;
+};
+
+__device__ void spring_forces(const MembraneArgs &A, const MembraneConst &mc, const MembraneScalars &ms, int s,
+                              bool initials, double sfc, double vol_coef, double area_coef, double mad_coef) {
+    const int na = A.spring[4 * s], nb = A.spring[4 * s + 1], ncn = A.spring[4 * s + 2], nd = A.spring[4 * s + 3];
+    const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]);
+    D3 c = d3(A.x[ncn], A.y[ncn], A.z[ncn]);
+    const D3 d = d3(A.x[nd], A.y[nd], A.z[nd]);
+    const D3 l = c - a;
+    double length = sqrt(dot(l, l));
+    const D3 normal_a = cross(b - a, c - a), normal_b = cross(c - a, d - a);
+    const double norm_1 = sqrt(dot(normal_a, normal_a)), norm_2 = sqrt(dot(normal_b, normal_b));
+    double dN1[27], dN2[27], dV1[9], dV2[9], dn1[9], dn2[9];
+    d_normals(a, b, c, normal_a, dN1, dV1);
+    d_normals(c, d, a, normal_b, dN2, dV2);
+    d_norms(dn1, dN1, norm_1, normal_a);
+    d_norms(dn2, dN2, norm_2, normal_b);
+    double d_area[12], d_volume[12];
+    merge12(d_area, dn1, dn2);
+#pragma unroll
+    for (int j = 0; j < 12; j++) d_area[j] *= 0.166666666666666666666666666666666666666666;
+    merge12(d_volume, dV1, dV2);
+#pragma unroll
+    for (int j = 0; j < 12; j++) d_volume[j] *= (1.0 / 18.0);
+    double cos_angle = dot(normal_a, normal_b) / (norm_1 * norm_2);
+    cos_angle = fmin(cos_angle, 1.0);
+    cos_angle = fmax(cos_angle, -1.0);
+    const D3 centroid_1 = tri_centroid(a, b, c);
+    const D3 centroid_2 = tri_centroid(a, c, d) - centroid_1;
+    const double angle_direction = dot(normal_a, centroid_2);
+    double angle = acos(cos_angle);
+    angle = ((angle_direction < 0) - (angle_direction > 0)) * angle;
+    if (initials) {
+        A.angle0[s] = angle;
+        A.area0[2 * s] = norm_1;
+        A.area0[2 * s + 1] = norm_2;
+    }
+    double d_angle_1[9], d_angle_2[9], d_angle[12];
+    {
+        const D3 h = cross(normal_a / norm_1, l / length);
+#pragma unroll
+        for (int j = 0; j < 9; j++)
+            d_angle_1[j] = -1 / norm_1 * (h.x * dN1[j * 3] + h.y * dN1[j * 3 + 1] + h.z * dN1[j * 3 + 2]);
+        const D3 h2 = cross(l / length, normal_b / norm_2);
+#pragma unroll
+        for (int j = 0; j < 9; j++)
+            d_angle_2[j] = -1 / norm_2 * (h2.x * dN2[j * 3] + h2.y * dN2[j * 3 + 1] + h2.z * dN2[j * 3 + 2]);
+    }
+    merge12(d_angle, d_angle_1, d_angle_2);
+    c = c - a;
+    length = sqrt(dot(c, c));
+    const D3 dL_ds = c / length;
+    double d_curve[12];
+#pragma unroll
+    for (int j = 0; j < 12; j++) d_curve[j] = d_angle[j] * length;
+    d_curve[0] = d_curve[0] - dL_ds.x * angle;
+    d_curve[1] = d_curve[1] - dL_ds.y * angle;
+    d_curve[2] = d_curve[2] - dL_ds.z * angle;
+    d_curve[6] = d_curve[6] + dL_ds.x * angle;
+    d_curve[7] = d_curve[7] + dL_ds.y * angle;
+    d_curve[8] = d_curve[8] + dL_ds.z * angle;
+
+    D3 fa = {0, 0, 0}, fb = {0, 0, 0}, fc = {0, 0, 0}, fd = {0, 0, 0};
+    // local + global area
+    double lac = -1 * mc.local_area_modulus * (norm_1 / A.area0[2 * s] - 1) + area_coef;
+    fb.x += lac * dn1[3]; fb.y += lac * dn1[4]; fb.z += lac * dn1[5];
+    lac = -1 * mc.local_area_modulus * (norm_2 / A.area0[2 * s + 1] - 1) + area_coef;
+    fd.x += lac * dn2[3]; fd.y += lac * dn2[4]; fd.z += lac * dn2[5];
+    // volume
+    fa.x += vol_coef * d_volume[0]; fa.y += vol_coef * d_volume[1]; fa.z += vol_coef * d_volume[2];
+    fb.x += vol_coef * d_volume[3]; fb.y += vol_coef * d_volume[4]; fb.z += vol_coef * d_volume[5];
+    fc.x += vol_coef * d_volume[6]; fc.y += vol_coef * d_volume[7]; fc.z += vol_coef * d_volume[8];
+    fd.x += vol_coef * d_volume[9]; fd.y += vol_coef * d_volume[10]; fd.z += vol_coef * d_volume[11];
+    // membrane viscosity (Osay form)
+    {
+        const D3 va = d3(A.vx[na], A.vy[na], A.vz[na]);
+        const D3 vc = d3(A.vx[ncn], A.vy[ncn], A.vz[ncn]) - va;
+        const D3 visc = dL_ds * -1 * dot(dL_ds, vc) * 4 / sqrt(3.0) * mc.viscosity;
+        fc = fc + visc;
+        fa = fa - visc;
+    }
+    // curvature and bending
+    const double spring_area_total = (norm_1 + norm_2) / 6.0;
+    A.area[2 * s] = norm_1;
+    A.area[2 * s + 1] = norm_2;
+    const double curvature = angle * length / spring_area_total;
+    A.curv[s] = curvature;
+    const double c0 = A.curv0[s];
+    const double lbc = -0.5 * mc.local_bending_modulus * (c0 - curvature) * (c0 - curvature);
+    fa.x += lbc * d_area[0]; fa.y += lbc * d_area[1]; fa.z += lbc * d_area[2];
+    fb.x += lbc * d_area[3]; fb.y += lbc * d_area[4]; fb.z += lbc * d_area[5];
+    fc.x += lbc * d_area[6]; fc.y += lbc * d_area[7]; fc.z += lbc * d_area[8];
+    fd.x += lbc * d_area[9]; fd.y += lbc * d_area[10]; fd.z += lbc * d_area[11];
+    const double cc = -1 * mc.global_bending_modulus * (curvature - c0) + mad_coef;
+    fa.x += cc * d_curve[0]; fa.y += cc * d_curve[1]; fa.z += cc * d_curve[2];
+    fb.x += cc * d_curve[3]; fb.y += cc * d_curve[4]; fb.z += cc * d_curve[5];
+    fc.x += cc * d_curve[6]; fc.y += cc * d_curve[7]; fc.z += cc * d_curve[8];
+    fd.x += cc * d_curve[9]; fd.y += cc * d_curve[10]; fd.z += cc * d_curve[11];
+    // WLC stretching
+    const double sr = length / A.contour[s];
+    const double fcoef = -1 * A.kspring[s] * ((0.25 / ((1.0 - sr) * (1.0 - sr))) - 0.25 + sr - sfc);
+    fc = fc + dL_ds * fcoef;
+    fa = fa - dL_ds * fcoef;
+    double *o = A.contrib + 12 * (size_t)s;
+    o[0] = fa.x; o[1] = fa.y; o[2] = fa.z;
+    o[3] = fb.x; o[4] = fb.y; o[5] = fb.z;
+    o[6] = fc.x; o[7] = fc.y; o[8] = fc.z;
+    o[9] = fd.x; o[10] = fd.y; o[11] = fd.z;
+}
+
+// Stress-free reference pass: get_contour_lengths (spring_network.cu:516-604)
+// with get_spring_constant / get_pivkin_spring_constant (:1600-1634), and
+// get_reference_curvatures (:389-513).
+__device__ void spring_reference(const MembraneArgs &A, const MembraneConst &mc, int s) {
+    const int na = A.spring[4 * s], nb = A.spring[4 * s + 1], ncn = A.spring[4 * s + 2], nd = A.spring[4 * s + 3];
+    const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]);
+    D3 c = d3(A.x[ncn], A.y[ncn], A.z[ncn]);
+    const D3 d = d3(A.x[nd], A.y[nd], A.z[nd]);
+    D3 l = c - a;
+    double length = sqrt(dot(l, l));
+    const double cons_wlc = (0.5 * pow(1.0 - 1 / mc.wlc_ratio, -3.0) + 1.0);
+    if (mc.pivkin_length) {
+        A.kspring[s] = ((4.0 * mc.wlc_ratio * mc.reference_length * mc.shear_modulus) / (sqrt(3.0) * cons_wlc));
+        A.contour[s] = mc.reference_length * mc.wlc_ratio;
+    } else {
+        A.kspring[s] = ((4.0 * mc.wlc_ratio * length * mc.shear_modulus) / (sqrt(3.0) * cons_wlc));
+        A.contour[s] = length * mc.wlc_ratio;
+    }
+    const D3 normal_a = cross(b - a, c - a), normal_b = cross(c - a, d - a);
+    const double norm_1 = sqrt(dot(normal_a, normal_a)), norm_2 = sqrt(dot(normal_b, normal_b));
+    double cos_angle = dot(normal_a, normal_b) / (norm_1 * norm_2);
+    cos_angle = fmin(cos_angle, 1.0);
+    cos_angle = fmax(cos_angle, -1.0);
+    const D3 centroid_1 = tri_centroid(a, b, c);
+    const D3 centroid_2 = tri_centroid(a, c, d) - centroid_1;
+    const D3 normal_ba = normal_b - normal_a;
+    const double angle_direction = dot(normal_ba, centroid_2);
+    double angle = acos(cos_angle);
+    angle = ((angle_direction > 0) - (angle_direction < 0)) * angle;
+    c = c - a;
+    length = sqrt(dot(c, c));
+    const double spring_area_total = (norm_1 + norm_2) / 6.0;
+    A.curv[s] = angle * length / spring_area_total;
+    A.area[2 * s] = norm_1;
+    A.area[2 * s + 1] = norm_2;
+    A.curv0[s] = mc.sphere_reference ? mc.curvature_ratio / 3.265483301 : 0.0;
+    A.angle0[s] = angle;
+    A.area0[2 * s] = norm_1;
+    A.area0[2 * s + 1] = norm_2;
+}
+
+template <typename R>
+__device__ void interpolate_and_advect(const MembraneArgs &A, const MembraneConst &mc) {
+    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
+        const int n = mc.node0 + ln;
+        const double x = A.x[n], y = A.y[n], z = A.z[n];
+        const Stencil st = node_stencil(A, x, y, z);
+        const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+        double vx = 0.0, vy = 0.0, vz = 0.0;
+        for (int i = st.i0; i < st.i0 + S; i++)
+            for (int j = st.j0; j < st.j0 + S; j++)
+                for (int k = st.k0; k < st.k0 + S; k++) {
+                    const int idx = i + j * A.grid_nx + k * A.grid_ny * A.grid_nx;
+                    if (idx < A.nc && idx >= 0) {
+                        const double wx = stencil_weight(A.ibm_stencil, i + 0.5 - st.rx);
+                        const double wy = stencil_weight(A.ibm_stencil, j + 0.5 - st.ry);
+                        const double wz = stencil_weight(A.ibm_stencil, k + 0.5 - st.rz);
+                        double u, v, w;
+                        read_velocity<R>(A.state, idx, u, v, w);
+                        vx += u * wx * wy * wz;
+                        vy += v * wx * wy * wz;
+                        vz += w * wx * wy * wz;
+                    }
+                }
+        A.vx[n] = vx;
+        A.vy[n] = vy;
+        A.vz[n] = vz;
+        A.x[n] = x + vx * A.delta_t;
+        A.y[n] = y + vy * A.delta_t;
+        A.z[n] = z + vz * A.delta_t;
+    }
+    __syncthreads();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kMembraneThreads) k_membrane(MembraneArgs A) {
+    extern __shared__ unsigned long long skeys[];
+    __shared__ double sh[33];
+    __shared__ int shi[33];
+    const int m = blockIdx.x;
+    const MembraneConst mc = A.mc[m];
+    MembraneScalars *ms = A.ms + m;
+
+    if (A.mode == kModeReference) {
+        for (int ls = threadIdx.x; ls < mc.n_springs; ls += blockDim.x) spring_reference(A, mc, mc.spring0 + ls);
+        return;
+    }
+    const bool initials = (A.mode == kModeInitial);
+    if (A.mode == kModeStep) {
+        if (A.state_is_float) interpolate_and_advect<float>(A, mc);
+        else interpolate_and_advect<double>(A, mc);
+    }
+    // P1: triangle totals
+    double pv = 0.0, pa = 0.0;
+    for (int lt = threadIdx.x; lt < mc.n_tris; lt += blockDim.x) {
+        const int t = mc.tri0 + lt;
+        const int na = A.tri[3 * t], nb = A.tri[3 * t + 1], nc = A.tri[3 * t + 2];
+        const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]), c = d3(A.x[nc], A.y[nc], A.z[nc]);
+        const D3 normal = cross(b - a, c - a);
+        const double area = sqrt(dot(normal, normal)) * 0.5;
+        const D3 centroid = tri_centroid(a, b, c);
+        pv += dot(normal, centroid) / 6;
+        pa += area;
+    }
+    const double V = block_sum(pv, sh);
+    const double Ar = block_sum(pa, sh);
+    double V0 = ms->V0, A0 = ms->A0;
+    if (initials) {
+        V0 = V * mc.volume_ratio;
+        A0 = Ar;
+    }
+    // P2: springs
+    const double wr = mc.wlc_ratio;
+    const double sfc = (0.25 * wr * wr / ((wr - 1.0) * (wr - 1.0)) - 0.25 + 1.0 / wr);
+    const double vol_coef = -1 * mc.volume_modulus * (V / V0 - 1.0) / 6.0;
+    const double area_coef = -1 * mc.global_area_modulus * (Ar / A0 - 1.0);
+    const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (ms->MAD - ms->MAD0) / A0;
+    for (int ls = threadIdx.x; ls < mc.n_springs; ls += blockDim.x)
+        spring_forces(A, mc, *ms, mc.spring0 + ls, initials, sfc, vol_coef, area_coef, mad_coef);
+    __syncthreads();
+    // P4: MAD over the first n_nodes springs of this membrane
+    double pm = 0.0;
+    const int n_mad = mc.n_nodes < mc.n_springs ? mc.n_nodes : mc.n_springs;
+    for (int ls = threadIdx.x; ls < n_mad; ls += blockDim.x) {
+        const int s = mc.spring0 + ls;
+        pm += A.curv[s] * (A.area[2 * s] + A.area[2 * s + 1]) * 1 / 3;
+    }
+    const double MAD = block_sum(pm, sh) / Ar;
+    if (threadIdx.x == 0) {
+        ms->V = V; ms->A = Ar; ms->MAD = MAD;
+        if (initials) { ms->V0 = V0; ms->A0 = A0; ms->MAD0 = MAD; }
+    }
+    if (A.mode != kModeStep) return;
+
+    // P3: node forces in spring order; node bounds for the interior-viscosity test
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
+        const int n = mc.node0 + ln;
+        double f[3] = {0.0, 0.0, 0.0};
+        for (int e = A.inc_start[n]; e < A.inc_start[n + 1]; e++) {
+            const int code = A.inc[e];
+            const double *o = A.contrib + 12 * (size_t)(code >> 2) + 3 * (code & 3);
+            f[0] += o[0]; f[1] += o[1]; f[2] += o[2];
+        }
+        A.fx[n] = f[0]; A.fy[n] = f[1]; A.fz[n] = f[2];
+        const double p[3] = {A.x[n], A.y[n], A.z[n]};
+        for (int c = 0; c < 3; c++) { lo[c] = fmin(lo[c], p[c]); hi[c] = fmax(hi[c], p[c]); }
+    }
+    for (int c = 0; c < 3; c++) {
+        const double l = block_minmax(lo[c], sh, true), h = block_minmax(hi[c], sh, false);
+        if (threadIdx.x == 0) { ms->bbox_lo[c] = l; ms->bbox_hi[c] = h; }
+    }
+    __syncthreads();  // node forces visible to the whole block
+
+    // P5: sort nodes by the cell at the base of their stencil
+    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+    int blo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, bhi_neg[3] = {INT32_MAX, INT32_MAX, INT32_MAX};
+    unsigned int range_flag = 0;
+    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
+        const int n = mc.node0 + ln;
+        const Stencil st = node_stencil(A, A.x[n], A.y[n], A.z[n]);
+        const int b[3] = {st.i0, st.j0, st.k0};
+        const int gn[3] = {A.grid_nx, A.grid_ny, A.grid_nz};
+        for (int c = 0; c < 3; c++) {
+            blo[c] = min(blo[c], b[c]);
+            bhi_neg[c] = min(bhi_neg[c], -b[c]);
+            if (b[c] < 0 || b[c] + S > gn[c]) range_flag = LBFS_FLAG_IBM_RANGE;
+        }
+    }
+    int plo[3], bdim[3], pdim[3];
+    for (int c = 0; c < 3; c++) {
+        plo[c] = block_min_int(blo[c], shi);
+        const int phi = -block_min_int(bhi_neg[c], shi);
+        bdim[c] = phi - plo[c] + 1;
+        pdim[c] = bdim[c] + S - 1;
+    }
+    const long long pcells = (long long)pdim[0] * pdim[1] * pdim[2];
+    const bool overflow = pcells > kMaxPatchCells || mc.n_nodes == 0;
+    if (range_flag) atomicOr(A.flags, range_flag);
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 3; c++) { ms->patch_lo[c] = plo[c]; ms->patch_dim[c] = pdim[c]; }
+        ms->patch_cells = overflow ? 0 : (int)pcells;
+        if (overflow) atomicOr(A.flags, LBFS_FLAG_IBM_RANGE);
+    }
+    if (overflow) return;
+    int npad = 1;
+    while (npad < mc.n_nodes) npad <<= 1;
+    for (int t = threadIdx.x; t < npad; t += blockDim.x) {
+        unsigned long long key = ~0ull;
+        if (t < mc.n_nodes) {
+            const int n = mc.node0 + t;
+            const Stencil st = node_stencil(A, A.x[n], A.y[n], A.z[n]);
+            const unsigned long long bin =
+                (unsigned long long)((st.i0 - plo[0]) + bdim[0] * ((st.j0 - plo[1]) + bdim[1] * (st.k0 - plo[2])));
+            key = (bin << 32) | (unsigned long long)t;
+        }
+        skeys[t] = key;
+    }
+    __syncthreads();
+    for (int size = 2; size <= npad; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int t = threadIdx.x; t < (npad >> 1); t += blockDim.x) {
+                const int i = 2 * stride * (t / stride) + (t % stride);
+                const int j = i + stride;
+                const bool up = ((i & size) == 0);
+                const unsigned long long ki = skeys[i], kj = skeys[j];
+                if ((ki > kj) == up) { skeys[i] = kj; skeys[j] = ki; }
+            }
+            __syncthreads();
+        }
+    }
+    // P6: per patch cell, sum the contributions of the nodes of the bins whose
+    // stencils cover it, bins in (z, y, x) order and nodes in node order.
+    const double inv3 = 1 / A.delta_x / A.delta_x / A.delta_x;
+    double *pf = A.patch_force + (size_t)m * kMaxPatchCells * 3;
+    for (int pc = threadIdx.x; pc < (int)pcells; pc += blockDim.x) {
+        const int px = pc % pdim[0], py = (pc / pdim[0]) % pdim[1], pz = pc / (pdim[0] * pdim[1]);
+        const int ci = plo[0] + px, cj = plo[1] + py, ck = plo[2] + pz;
+        double f[3] = {0.0, 0.0, 0.0};
+        const int bx0 = max(px - S + 1, 0), bx1 = min(px, bdim[0] - 1);
+        const int by0 = max(py - S + 1, 0), by1 = min(py, bdim[1] - 1);
+        const int bz0 = max(pz - S + 1, 0), bz1 = min(pz, bdim[2] - 1);
+        for (int bz = bz0; bz <= bz1; bz++)
+            for (int by = by0; by <= by1; by++) {
+                if (bx0 > bx1) continue;
+                const unsigned long long klo = (unsigned long long)(bx0 + bdim[0] * (by + bdim[1] * bz));
+                const unsigned long long khi = (unsigned long long)(bx1 + bdim[0] * (by + bdim[1] * bz));
+                int lo_i = 0, hi_i = mc.n_nodes;  // first sorted entry with bin >= klo
+                while (lo_i < hi_i) {
+                    const int mid = (lo_i + hi_i) >> 1;
+                    if ((skeys[mid] >> 32) < klo) lo_i = mid + 1;
+                    else hi_i = mid;
+                }
+                for (int e = lo_i; e < mc.n_nodes && (skeys[e] >> 32) <= khi; e++) {
+                    const int n = mc.node0 + (int)(skeys[e] & 0xffffffffu);
+                    const Stencil st = node_stencil(A, A.x[n], A.y[n], A.z[n]);
+                    const double wx = stencil_weight(A.ibm_stencil, ci + 0.5 - st.rx);
+                    const double wy = stencil_weight(A.ibm_stencil, cj + 0.5 - st.ry);
+                    const double wz = stencil_weight(A.ibm_stencil, ck + 0.5 - st.rz);
+                    f[0] += A.fx[n] * wx * wy * wz * inv3;
+                    f[1] += A.fy[n] * wx * wy * wz * inv3;
+                    f[2] += A.fz[n] * wx * wy * wz * inv3;
+                }
+            }
+        pf[3 * (size_t)pc] = f[0];
+        pf[3 * (size_t)pc + 1] = f[1];
+        pf[3 * (size_t)pc + 2] = f[2];
+    }
+}
+
+// ---- interior viscosity (update_interior_viscosities_plucker, immersed_boundary_method.cu:389-527) ----
+template <typename R>
+__global__ void k_interior_viscosity(ViscArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nc || i == 0) return;  // the reference skips cell 0
+    const D3 cc = d3(a.centroid[3 * i], a.centroid[3 * i + 1], a.centroid[3 * i + 2]);
+    const double pi = acos(-1.0);
+    for (int m = 0; m < a.n_membranes; m++) {
+        const MembraneScalars ms = a.ms[m];
+        const MembraneConst mc = a.mc[m];
+        const double xl = ms.bbox_lo[0] - 2 * a.delta_h, xh = ms.bbox_hi[0] + 2 * a.delta_h;
+        const double yl = ms.bbox_lo[1] - 2 * a.delta_h, yh = ms.bbox_hi[1] + 2 * a.delta_h;
+        const double zl = ms.bbox_lo[2] - 2 * a.delta_h, zh = ms.bbox_hi[2] + 2 * a.delta_h;
+        if (!(cc.x >= xl && cc.x <= xh && cc.y >= yl && cc.y <= yh && cc.z >= zl && cc.z <= zh)) continue;
+        // ray from the centroid along +x to x = xh; Plucker side tests against each triangle edge
+        const double pc0 = cc.x * cc.y - xh * cc.y, pc1 = cc.x * cc.z - xh * cc.z, pc2 = cc.x - xh;
+        int crossings = 0;
+        double min_distance = 1000000000;
+        for (int lt = 0; lt < mc.n_tris; lt++) {
+            const int t = mc.tri0 + lt;
+            const int na = a.tri[3 * t], nb = a.tri[3 * t + 1], nc = a.tri[3 * t + 2];
+            const D3 A = d3(a.x[na], a.y[na], a.z[na]), B = d3(a.x[nb], a.y[nb], a.z[nb]), C = d3(a.x[nc], a.y[nc], a.z[nc]);
+            if (A.x > cc.x && B.x > cc.x && C.x > cc.x) {
+                const D3 P[3] = {A, B, C};
+                double side[3];
+                for (int e = 0; e < 3; e++) {
+                    const D3 p = P[e], q = P[(e + 1) % 3];
+                    const double e0 = p.y * q.z - q.y * p.z, e1 = p.z - q.z, e2 = q.y - p.y;
+                    side[e] = pc0 * e1 + pc1 * e2 + pc2 * e0;
+                }
+                if ((side[0] < 0 && side[1] < 0 && side[2] < 0) || (side[0] > 0 && side[1] > 0 && side[2] > 0))
+                    crossings++;
+                min_distance = fmin(sqrt(dot(cc - A, cc - A)), min_distance);
+                min_distance = fmin(sqrt(dot(cc - B, cc - B)), min_distance);
+                min_distance = fmin(sqrt(dot(cc - C, cc - C)), min_distance);
+            }
+        }
+        const bool inside = (crossings % 2) != 0;
+        const double r = mc.internal_viscosity_ratio;
+        const double factor =
+            2.0 * fmin(0.5, (min_distance * 0.5 / a.delta_h + 1.0 / pi * sin(pi * min_distance / a.delta_h) * 0.5));
+        const double visc = inside ? (r + 1.0) + (r - 1.0) * factor : (r + 1.0) + (1.0 - r) * factor;
+        ((R *)a.visc_factor)[i] = (R)(visc * 0.5);
+    }
+}
+
+}  // namespace
+
+void membrane_prepare(int sort_capacity) {
+    const size_t smem = (size_t)(sort_capacity > 0 ? sort_capacity : 1) * sizeof(unsigned long long);
+    cudaFuncSetAttribute(k_membrane<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_membrane<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+void launch_membrane(const MembraneArgs &a, cudaStream_t s) {
+    // dynamic shared memory: one 64-bit sort key per node of the largest
+    // membrane, padded to a power of two
+    const size_t smem = (size_t)(a.sort_capacity > 0 ? a.sort_capacity : 1) * sizeof(unsigned long long);
+    if (a.state_is_float)
+        k_membrane<float><<<a.n_membranes, kMembraneThreads, smem, s>>>(a);
+    else
+        k_membrane<double><<<a.n_membranes, kMembraneThreads, smem, s>>>(a);
+}
+
+void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s) {
+    const int blocks = (a.nc + 255) / 256;
+    if (a.visc_is_float) k_interior_viscosity<float><<<blocks, 256, 0, s>>>(a);
+    else k_interior_viscosity<double><<<blocks, 256, 0, s>>>(a);
+}
+
+}  // namespace lbfs

@@ -1,0 +1,739 @@
+// Host runtime behind the C ABI of include/lbfs_b200.h.
+//
+// One handle = one solver instance on one GPU: mesh geometry and membranes are
+// uploaded once, the state stays resident in HBM, and each time step is four
+// kernels (membrane kernel on a forked stream, overlapping the gradient and
+// face-flux kernels, then the cell update), optionally replayed from a CUDA
+// graph.  This replaces gpu_solver::General_Purpose_Solver_mk_i's set-up
+// (Solver_gpu.cu:178-746) and loop body (Solver_gpu.cu:749-1046), which issue
+// 20-30 synchronising launches per step on managed memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "lbfs_b200.h"
+#include "lbfs_fluid.cuh"
+#include "lbfs_internal.h"
+#include "lbfs_kernels.h"
+
+namespace lbfs {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+}  // namespace lbfs
+
+using namespace lbfs;
+
+#define LBFS_CUDA(call)                                                                                  \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            return set_error(e_ == cudaErrorMemoryAllocation ? LBFS_ERR_NOMEM : LBFS_ERR_CUDA,           \
+                             std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+    } while (0)
+
+struct lbfs_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
+    bool own_stream = true;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    lbfs_params params{};
+    bool fp32 = false;
+    int nc = 0, nf = 0, ni = 0, nb = 0;
+    int n_membranes = 0, total_nodes = 0, total_springs = 0, total_tris = 0;
+    std::vector<void *> allocs;
+    FluidArgs<double> f64{};
+    FluidArgs<float> f32{};
+    MembraneArgs ma{};
+    ViscArgs va{};
+    double *d_centroid = nullptr;
+    double *d_res_out = nullptr;
+    bool keep_residuals = false;
+    long long t = 0;  // time-step counter (the reference's loop index)
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    int launches_per_step = 0;
+
+    template <typename T> int alloc(T **p, size_t count) {
+        void *q = nullptr;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+        if (e != cudaSuccess)
+            return set_error(LBFS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        allocs.push_back(q);
+        *p = (T *)q;
+        return LBFS_OK;
+    }
+    template <typename T> int upload(T **p, const std::vector<T> &h) {
+        int rc = alloc(p, h.size());
+        if (rc) return rc;
+        if (!h.empty()) {
+            cudaError_t e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(e));
+        }
+        return LBFS_OK;
+    }
+};
+
+namespace {
+
+template <typename R> FluidArgs<R> &fluid(lbfs_solver *s);
+template <> FluidArgs<double> &fluid<double>(lbfs_solver *s) { return s->f64; }
+template <> FluidArgs<float> &fluid<float>(lbfs_solver *s) { return s->f32; }
+
+int check_mesh(const lbfs_mesh_desc *m) {
+    if (!m) return set_error(LBFS_ERR_ARG, "mesh descriptor is null");
+    if (m->n_cells <= 0 || m->n_bc < 0 || m->n_interior < 0 || m->n_faces != m->n_interior + m->n_bc)
+        return set_error(LBFS_ERR_ARG, "inconsistent mesh sizes");
+    if (!m->owner || !m->neighbour || !m->face_area || !m->face_normal || !m->face_centroid || !m->streaming_dt ||
+        !m->cell_volume || !m->cell_centroid || !m->gradient_stencil || !m->lhs_inverse || !m->rhs ||
+        (m->n_bc > 0 && (!m->bc_rho_type || !m->bc_vel_type || !m->bc_values)))
+        return set_error(LBFS_ERR_ARG, "mesh descriptor has a null array");
+    if (m->axis_aligned && m->n_face_x + m->n_face_y + m->n_face_z != m->n_interior)
+        return set_error(LBFS_ERR_ARG, "axis-aligned face ranges do not cover the interior faces");
+    const int nt = m->n_cells + m->n_bc;
+    for (int f = 0; f < m->n_faces; f++) {
+        if (m->owner[f] < 0 || m->owner[f] >= m->n_cells || m->neighbour[f] < 0 || m->neighbour[f] >= nt)
+            return set_error(LBFS_ERR_ARG, "face cell index out of range");
+        if (f >= m->n_interior && m->neighbour[f] != m->n_cells + f - m->n_interior)
+            return set_error(LBFS_ERR_ARG, "boundary face neighbour is not its ghost cell");
+        if (!(m->streaming_dt[f] > 0) || !(m->face_area[f] > 0))
+            return set_error(LBFS_ERR_ARG, "face area and streaming dt must be positive");
+    }
+    for (int i = 0; i < 6 * m->n_cells; i++)
+        if (m->gradient_stencil[i] < 0 || m->gradient_stencil[i] >= nt)
+            return set_error(LBFS_ERR_ARG, "gradient stencil index out of range");
+    for (int b = 0; b < m->n_bc; b++) {
+        const int rt = m->bc_rho_type[b], vt = m->bc_vel_type[b];
+        if (!(rt == 1 || rt == 2) || !(vt == 1 || vt == 2 || vt == 9 || vt == 10))
+            return set_error(LBFS_ERR_UNSUPPORTED,
+                             "boundary types: rho must be 1 or 2, velocity 1, 2, 9 or 10 (the reference GPU kernels "
+                             "implement no others, LBFS.cu:1872-1918)");
+    }
+    for (int i = 0; i < m->n_cells; i++)
+        if (!(m->cell_volume[i] > 0)) return set_error(LBFS_ERR_ARG, "cell volume must be positive");
+    return LBFS_OK;
+}
+
+template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
+    FluidArgs<R> &a = fluid<R>(s);
+    const lbfs_params &p = s->params;
+    const int nc = m->n_cells, nf = m->n_faces, ni = m->n_interior, nb = m->n_bc, nt = nc + nb;
+    const double rho0 = s->fp32 ? p.rho0 : 0.0;
+    a.nc = nc; a.nf = nf; a.ni = ni; a.nb = nb;
+    a.nfx = m->n_face_x; a.nfy = m->n_face_y; a.nfz = m->n_face_z;
+    a.axis_aligned = m->axis_aligned ? 1 : 0;
+    a.testcase = p.testcase;
+    a.rho0 = (R)rho0;
+    a.gamma_inv = (R)p.gamma_inv;
+    a.visc = (R)p.visc;
+    a.delta_t = p.delta_t;
+    a.H2 = p.channel_diameter * 0.5;
+    a.H4 = p.channel_diameter * p.channel_diameter * p.channel_diameter * p.channel_diameter;
+    for (int c = 0; c < 3; c++) a.force[c] = p.body_force[c];
+    const double *cen = m->cell_centroid, *fc = m->face_centroid, *fn = m->face_normal;
+    // K1 geometry
+    std::vector<int> stencil(m->gradient_stencil, m->gradient_stencil + 6 * (size_t)nc);
+    std::vector<R> rhs(18 * (size_t)nc), lhs(9 * (size_t)nc);
+    for (size_t i = 0; i < rhs.size(); i++) rhs[i] = (R)m->rhs[i];
+    for (size_t i = 0; i < lhs.size(); i++) lhs[i] = (R)m->lhs_inverse[i];
+    std::vector<int> rt(nb), vt(nb);
+    std::vector<Vec4<R>> bcv(nb);
+    std::vector<BcRec<R>> bcr(nb);
+    for (int b = 0; b < nb; b++) {
+        rt[b] = m->bc_rho_type[b];
+        vt[b] = m->bc_vel_type[b];
+        const double *v = m->bc_values + 4 * b;
+        bcv[b] = {(R)v[0], (R)v[1], (R)v[2], (R)(v[3] - rho0)};
+        const int f = ni + b, g = nc + b, o = m->owner[f];
+        // get_bc_gradients, LBFS.cu:1968-1979
+        const double dx = cen[3 * g] - cen[3 * o], dy = cen[3 * g + 1] - cen[3 * o + 1], dz = cen[3 * g + 2] - cen[3 * o + 2];
+        const double dmag = std::sqrt(std::pow(dx, 2.0) + std::pow(dy, 2.0) + std::pow(dz, 2.0));
+        bcr[b] = {(R)dmag, (R)(dx / dmag), (R)(dy / dmag), (R)(dz / dmag), (R)(1 - std::fabs(fn[3 * f])),
+                  (R)(1 - std::fabs(fn[3 * f + 1])), (R)(1 - std::fabs(fn[3 * f + 2])), (R)cen[3 * g + 1],
+                  (R)cen[3 * g + 2]};
+    }
+    // K2 geometry
+    std::vector<int2> fcells(nf);
+    for (int f = 0; f < nf; f++) fcells[f] = make_int2(m->owner[f], m->neighbour[f]);
+    std::vector<AxisFace<R>> axf;
+    if (a.axis_aligned) {
+        axf.resize(ni);
+        for (int f = 0; f < ni; f++) {
+            const int ax = (f < a.nfx) ? 0 : ((f < a.nfx + a.nfy) ? 1 : 2);
+            const int o = m->owner[f], n = m->neighbour[f];
+            axf[f] = {(R)m->face_area[f], (R)m->streaming_dt[f], (R)(cen[3 * o + ax] - fc[3 * f + ax]),
+                      (R)(cen[3 * n + ax] - fc[3 * f + ax])};
+        }
+    }
+    const int gf0 = a.axis_aligned ? ni : 0;
+    std::vector<GenFace<R>> gen(nf - gf0);
+    for (int f = gf0; f < nf; f++) {
+        const int o = m->owner[f], n = m->neighbour[f];
+        GenFace<R> g;
+        g.area = (R)m->face_area[f];
+        g.dt = (R)m->streaming_dt[f];
+        g.nx = (R)fn[3 * f]; g.ny = (R)fn[3 * f + 1]; g.nz = (R)fn[3 * f + 2];
+        g.t1x = (R)(cen[3 * o] - fc[3 * f]); g.t1y = (R)(cen[3 * o + 1] - fc[3 * f + 1]); g.t1z = (R)(cen[3 * o + 2] - fc[3 * f + 2]);
+        g.t2x = (R)(cen[3 * n] - fc[3 * f]); g.t2y = (R)(cen[3 * n + 1] - fc[3 * f + 1]); g.t2z = (R)(cen[3 * n + 2] - fc[3 * f + 2]);
+        g.pad = 0;
+        gen[f - gf0] = g;
+    }
+    // K3: signed face list per cell, faces in increasing index order
+    std::vector<int> cf(6 * (size_t)nc, 0), cnt(nc, 0);
+    for (int f = 0; f < nf; f++) {
+        const int o = m->owner[f];
+        if (cnt[o] >= 6) return set_error(LBFS_ERR_UNSUPPORTED, "cell with more than 6 faces (hexahedra only)");
+        cf[6 * (size_t)o + cnt[o]++] = f + 1;
+        if (f < ni) {
+            const int n = m->neighbour[f];
+            if (cnt[n] >= 6) return set_error(LBFS_ERR_UNSUPPORTED, "cell with more than 6 faces (hexahedra only)");
+            cf[6 * (size_t)n + cnt[n]++] = -(f + 1);
+        }
+    }
+    for (int i = 0; i < nc; i++)
+        if (cnt[i] != 6) return set_error(LBFS_ERR_UNSUPPORTED, "cell without 6 faces (hexahedra only)");
+    std::vector<double> vol(m->cell_volume, m->cell_volume + nc);
+    std::vector<R> visc(nc, (R)p.visc_factor_initial);
+    int rc = 0;
+    int *d_stencil, *d_rt, *d_vt, *d_cf;
+    R *d_rhs, *d_lhs, *d_visc;
+    Vec4<R> *d_bcv;
+    BcRec<R> *d_bcr;
+    int2 *d_fcells;
+    AxisFace<R> *d_axf = nullptr;
+    GenFace<R> *d_gen;
+    double *d_vol;
+    if ((rc = s->upload(&d_stencil, stencil)) || (rc = s->upload(&d_rhs, rhs)) || (rc = s->upload(&d_lhs, lhs)) ||
+        (rc = s->upload(&d_rt, rt)) || (rc = s->upload(&d_vt, vt)) || (rc = s->upload(&d_bcv, bcv)) ||
+        (rc = s->upload(&d_bcr, bcr)) || (rc = s->upload(&d_fcells, fcells)) || (rc = s->upload(&d_gen, gen)) ||
+        (rc = s->upload(&d_cf, cf)) || (rc = s->upload(&d_vol, vol)) || (rc = s->upload(&d_visc, visc)))
+        return rc;
+    if (a.axis_aligned && (rc = s->upload(&d_axf, axf))) return rc;
+    a.stencil = d_stencil; a.rhs = d_rhs; a.lhs = d_lhs; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt;
+    a.bc_val = d_bcv; a.bc_rec = d_bcr; a.face_cells = d_fcells; a.axis_face = d_axf; a.gen_face = d_gen;
+    a.visc_factor = d_visc; a.cell_faces = d_cf; a.cell_volume = d_vol;
+    Vec4<R> *d_state, *d_flux;
+    R *d_grad;
+    double4 *d_t1;
+    if ((rc = s->alloc(&d_state, nt)) || (rc = s->alloc(&d_grad, 12 * (size_t)nt)) || (rc = s->alloc(&d_flux, nf)) ||
+        (rc = s->alloc(&d_t1, nc)))
+        return rc;
+    LBFS_CUDA(cudaMemset(d_state, 0, sizeof(Vec4<R>) * nt));
+    LBFS_CUDA(cudaMemset(d_grad, 0, sizeof(R) * 12 * (size_t)nt));
+    LBFS_CUDA(cudaMemset(d_flux, 0, sizeof(Vec4<R>) * nf));
+    LBFS_CUDA(cudaMemset(d_t1, 0, sizeof(double4) * nc));
+    a.state = d_state; a.grad = d_grad; a.flux = d_flux; a.t1 = d_t1;
+    double *d_partials, *d_rsum;
+    unsigned int *d_ticket, *d_flags;
+    if ((rc = s->alloc(&d_partials, 4 * (size_t)kK3MaxBlocks)) || (rc = s->alloc(&d_rsum, 4)) ||
+        (rc = s->alloc(&d_ticket, 1)) || (rc = s->alloc(&d_flags, 1)))
+        return rc;
+    LBFS_CUDA(cudaMemset(d_ticket, 0, sizeof(unsigned int)));
+    LBFS_CUDA(cudaMemset(d_flags, 0, sizeof(unsigned int)));
+    LBFS_CUDA(cudaMemset(d_rsum, 0, 4 * sizeof(double)));
+    a.partials = d_partials; a.residual_sums = d_rsum; a.ticket = d_ticket; a.flags = d_flags;
+    a.res_out = nullptr;
+    a.grid_nx = (int)(m->length[0] / m->delta_x);
+    a.grid_ny = (int)(m->length[1] / m->delta_x);
+    a.n_membranes = 0;
+    return LBFS_OK;
+}
+
+int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc *rbc, int n_rbc) {
+    const lbfs_params &p = s->params;
+    MembraneArgs &ma = s->ma;
+    ma.n_membranes = n_rbc;
+    ma.ibm_stencil = p.ibm_stencil;
+    ma.delta_t = p.delta_t;
+    ma.nc = m->n_cells;
+    ma.grid_nx = (int)(m->length[0] / m->delta_x);
+    ma.grid_ny = (int)(m->length[1] / m->delta_x);
+    ma.grid_nz = (int)(m->length[2] / m->delta_x);
+    for (int c = 0; c < 3; c++) ma.origin[c] = m->origin[c];
+    ma.delta_x = m->delta_x;
+    ma.state_is_float = s->fp32 ? 1 : 0;
+    if (n_rbc == 0) return LBFS_OK;
+    if ((long long)ma.grid_nx * ma.grid_ny * ma.grid_nz != m->n_cells)
+        return set_error(LBFS_ERR_ARG, "membranes need the lexicographic uniform grid the IBM stencils index "
+                                       "(length / delta_x cells per axis)");
+    std::vector<MembraneConst> mc(n_rbc);
+    std::vector<int> tri, spr;
+    std::vector<double> sf, init;
+    int cap = 1, maxn = 0;
+    for (int r = 0; r < n_rbc; r++) {
+        const lbfs_rbc_desc &d = rbc[r];
+        if (d.n_nodes <= 3 || d.n_tris <= 0 || d.n_springs <= 0 || !d.tri || !d.spring || !d.xyz_stress_free ||
+            !d.xyz_initial)
+            return set_error(LBFS_ERR_ARG, "bad membrane descriptor");
+        if (d.n_nodes > kMaxMembraneNodes) return set_error(LBFS_ERR_LIMIT, "membrane has more nodes than one CTA handles");
+        MembraneConst &c = mc[r];
+        c.node0 = s->total_nodes; c.n_nodes = d.n_nodes;
+        c.tri0 = s->total_tris; c.n_tris = d.n_tris;
+        c.spring0 = s->total_springs; c.n_springs = d.n_springs;
+        c.inc0 = 4 * s->total_springs;
+        c.volume_modulus = d.volume_modulus; c.local_area_modulus = d.local_area_modulus;
+        c.global_area_modulus = d.global_area_modulus; c.shear_modulus = d.shear_modulus;
+        c.global_bending_modulus = d.global_bending_modulus; c.local_bending_modulus = d.local_bending_modulus;
+        c.membrane_thickness = d.membrane_thickness; c.viscosity = d.viscosity; c.wlc_ratio = d.wlc_ratio;
+        c.curvature_ratio = d.curvature_ratio; c.volume_ratio = d.volume_ratio;
+        c.internal_viscosity_ratio = d.internal_viscosity_ratio; c.reference_length = d.reference_length;
+        c.pivkin_length = d.pivkin_length; c.sphere_reference = d.sphere_reference;
+        for (int i = 0; i < 3 * d.n_tris; i++) {
+            if (d.tri[i] < 0 || d.tri[i] >= d.n_nodes) return set_error(LBFS_ERR_ARG, "triangle index out of range");
+            tri.push_back(d.tri[i] + s->total_nodes);
+        }
+        for (int i = 0; i < 4 * d.n_springs; i++) {
+            if (d.spring[i] < 0 || d.spring[i] >= d.n_nodes) return set_error(LBFS_ERR_ARG, "spring index out of range");
+            spr.push_back(d.spring[i] + s->total_nodes);
+        }
+        sf.insert(sf.end(), d.xyz_stress_free, d.xyz_stress_free + 3 * d.n_nodes);
+        init.insert(init.end(), d.xyz_initial, d.xyz_initial + 3 * d.n_nodes);
+        s->total_nodes += d.n_nodes;
+        s->total_tris += d.n_tris;
+        s->total_springs += d.n_springs;
+        maxn = std::max(maxn, d.n_nodes);
+    }
+    while (cap < maxn) cap <<= 1;
+    ma.sort_capacity = cap;
+    membrane_prepare(cap);
+    // node -> (spring, slot) incidence in spring order
+    const int N = s->total_nodes, S = s->total_springs;
+    std::vector<int> inc_start(N + 1, 0), inc(4 * (size_t)S);
+    for (int i = 0; i < 4 * S; i++) inc_start[spr[i] + 1]++;
+    for (int n = 0; n < N; n++) inc_start[n + 1] += inc_start[n];
+    std::vector<int> fill(inc_start.begin(), inc_start.end() - 1);
+    for (int sp = 0; sp < S; sp++)
+        for (int q = 0; q < 4; q++) inc[fill[spr[4 * sp + q]]++] = 4 * sp + q;
+    std::vector<double> x(N), y(N), z(N);
+    for (int n = 0; n < N; n++) { x[n] = sf[3 * n]; y[n] = sf[3 * n + 1]; z[n] = sf[3 * n + 2]; }
+    std::vector<double> zeros_n(N, 0.0), zeros_s(S, 0.0), zeros_2s(2 * (size_t)S, 0.0);
+    std::vector<MembraneScalars> msz(n_rbc);
+    std::memset(msz.data(), 0, sizeof(MembraneScalars) * n_rbc);
+    int rc = 0;
+    MembraneConst *d_mc; MembraneScalars *d_ms; int *d_tri, *d_spr, *d_inc, *d_incs;
+    if ((rc = s->upload(&d_mc, mc)) || (rc = s->upload(&d_ms, msz)) || (rc = s->upload(&d_tri, tri)) ||
+        (rc = s->upload(&d_spr, spr)) || (rc = s->upload(&d_inc, inc)) || (rc = s->upload(&d_incs, inc_start)) ||
+        (rc = s->upload(&ma.x, x)) || (rc = s->upload(&ma.y, y)) || (rc = s->upload(&ma.z, z)) ||
+        (rc = s->upload(&ma.vx, zeros_n)) || (rc = s->upload(&ma.vy, zeros_n)) || (rc = s->upload(&ma.vz, zeros_n)) ||
+        (rc = s->upload(&ma.fx, zeros_n)) || (rc = s->upload(&ma.fy, zeros_n)) || (rc = s->upload(&ma.fz, zeros_n)) ||
+        (rc = s->upload(&ma.contour, zeros_s)) || (rc = s->upload(&ma.kspring, zeros_s)) ||
+        (rc = s->upload(&ma.curv, zeros_s)) || (rc = s->upload(&ma.curv0, zeros_s)) ||
+        (rc = s->upload(&ma.angle0, zeros_s)) || (rc = s->upload(&ma.area0, zeros_2s)) ||
+        (rc = s->upload(&ma.area, zeros_2s)) || (rc = s->alloc(&ma.contrib, 12 * (size_t)S)) ||
+        (rc = s->alloc(&ma.keys, N)) || (rc = s->alloc(&ma.patch_force, (size_t)n_rbc * kMaxPatchCells * 3)))
+        return rc;
+    ma.mc = d_mc; ma.ms = d_ms; ma.tri = d_tri; ma.spring = d_spr; ma.inc = d_inc; ma.inc_start = d_incs;
+    ma.flags = s->fp32 ? s->f32.flags : s->f64.flags;
+    ma.state = s->fp32 ? (const void *)s->f32.state : (const void *)s->f64.state;
+    // reference pass on the stress-free mesh, then the initial mesh
+    ma.mode = kModeReference;
+    launch_membrane(ma, s->stream);
+    LBFS_CUDA(cudaGetLastError());
+    for (int n = 0; n < N; n++) { x[n] = init[3 * n]; y[n] = init[3 * n + 1]; z[n] = init[3 * n + 2]; }
+    LBFS_CUDA(cudaMemcpyAsync(ma.x, x.data(), N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    LBFS_CUDA(cudaMemcpyAsync(ma.y, y.data(), N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    LBFS_CUDA(cudaMemcpyAsync(ma.z, z.data(), N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    ma.mode = kModeInitial;
+    launch_membrane(ma, s->stream);
+    LBFS_CUDA(cudaGetLastError());
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    ma.mode = kModeStep;
+    // FluidArgs see the patches
+    s->f64.n_membranes = s->f32.n_membranes = n_rbc;
+    s->f64.membrane_scalars = s->f32.membrane_scalars = d_ms;
+    s->f64.patch_force = s->f32.patch_force = ma.patch_force;
+    // interior viscosity
+    ViscArgs &va = s->va;
+    va.nc = m->n_cells; va.n_membranes = n_rbc; va.centroid = s->d_centroid; va.mc = d_mc; va.ms = d_ms;
+    va.tri = d_tri; va.x = ma.x; va.y = ma.y; va.z = ma.z; va.delta_h = m->delta_h;
+    va.visc_factor = s->fp32 ? (void *)s->f32.visc_factor : (void *)s->f64.visc_factor;
+    va.visc_is_float = s->fp32 ? 1 : 0;
+    return LBFS_OK;
+}
+
+template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *launches) {
+    FluidArgs<R> &a = fluid<R>(s);
+    int n = 0;
+    if (s->n_membranes > 0) {
+        if (visc_update) {
+            launch_membrane(s->ma, s->stream);
+            launch_interior_viscosity(s->va, s->stream);
+            launch_fluid_gradients<R>(a, s->stream);
+            launch_fluid_flux<R>(a, s->stream);
+            n += 4;
+        } else {
+            LBFS_CUDA(cudaEventRecord(s->ev_fork, s->stream));
+            LBFS_CUDA(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
+            launch_membrane(s->ma, s->stream2);
+            LBFS_CUDA(cudaEventRecord(s->ev_join, s->stream2));
+            launch_fluid_gradients<R>(a, s->stream);
+            launch_fluid_flux<R>(a, s->stream);
+            LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
+            n += 3;
+        }
+    } else {
+        launch_fluid_gradients<R>(a, s->stream);
+        launch_fluid_flux<R>(a, s->stream);
+        n += 2;
+    }
+    launch_fluid_update<R>(a, s->stream);
+    n += 1;
+    LBFS_CUDA(cudaGetLastError());
+    if (launches) *launches = n;
+    return LBFS_OK;
+}
+
+int enqueue(lbfs_solver *s, bool visc_update, int *launches) {
+    return s->fp32 ? enqueue_step<float>(s, visc_update, launches) : enqueue_step<double>(s, visc_update, launches);
+}
+
+bool visc_due(const lbfs_solver *s, long long t) {
+    return s->n_membranes > 0 && s->params.viscosity_period > 0 && t % s->params.viscosity_period == 1;
+}
+
+void free_all(lbfs_solver *s) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    for (void *p : s->allocs) cudaFree(p);
+    s->allocs.clear();
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
+    if (s->stream2) cudaStreamDestroy(s->stream2);
+    if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
+}
+
+}  // namespace
+
+extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params, const lbfs_rbc_desc *rbc,
+                           int32_t n_rbc, int32_t device, lbfs_solver **out) {
+    if (!out || !params) return set_error(LBFS_ERR_ARG, "null argument");
+    *out = nullptr;
+    int rc = check_mesh(mesh);
+    if (rc) return rc;
+    if (n_rbc < 0 || (n_rbc > 0 && !rbc)) return set_error(LBFS_ERR_ARG, "bad membrane count");
+    if (params->precision != LBFS_FP64 && params->precision != LBFS_FP32_BULK)
+        return set_error(LBFS_ERR_ARG, "precision must be LBFS_FP64 or LBFS_FP32_BULK");
+    if (params->ibm_stencil != LBFS_IBM_HAT2 && params->ibm_stencil != LBFS_IBM_PESKIN4)
+        return set_error(LBFS_ERR_ARG, "ibm_stencil must be 2 or 4");
+    if (!(params->delta_t > 0)) return set_error(LBFS_ERR_ARG, "delta_t must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_error(LBFS_ERR_CUDA, "no CUDA device: this library has no CPU path");
+    if (device < 0 || device >= ndev) return set_error(LBFS_ERR_ARG, "device index out of range");
+    lbfs_solver *s = new lbfs_solver();
+    s->device = device;
+    s->params = *params;
+    s->fp32 = params->precision == LBFS_FP32_BULK;
+    s->nc = mesh->n_cells; s->nf = mesh->n_faces; s->ni = mesh->n_interior; s->nb = mesh->n_bc;
+    s->n_membranes = n_rbc;
+    auto fail = [&](int code) { free_all(s); delete s; return code; };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(set_error(LBFS_ERR_CUDA, "cudaSetDevice failed"));
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess)
+        return fail(set_error(LBFS_ERR_CUDA, "stream/event creation failed"));
+    rc = s->fp32 ? setup_fluid<float>(s, mesh) : setup_fluid<double>(s, mesh);
+    if (rc) return fail(rc);
+    std::vector<double> centroid(mesh->cell_centroid, mesh->cell_centroid + 3 * (size_t)mesh->n_cells);
+    if ((rc = s->upload(&s->d_centroid, centroid))) return fail(rc);
+    rc = setup_membranes(s, mesh, rbc, n_rbc);
+    if (rc) return fail(rc);
+    s->launches_per_step = n_rbc > 0 ? 4 : 3;
+    *out = s;
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_destroy(lbfs_solver *s) {
+    if (!s) return LBFS_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    free_all(s);
+    delete s;
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_set_stream(lbfs_solver *s, void *stream) {
+    if (!s) return set_error(LBFS_ERR_ARG, "null handle");
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->own_stream) cudaStreamDestroy(s->stream);
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_set_state(lbfs_solver *s, const double *rho, const double *u, const double *v, const double *w) {
+    if (!s || !rho || !u || !v || !w) return set_error(LBFS_ERR_ARG, "null argument");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    const int nc = s->nc;
+    std::vector<double4> t1(nc);
+    for (int i = 0; i < nc; i++) t1[i] = make_double4(u[i], v[i], w[i], rho[i]);
+    if (s->fp32) {
+        std::vector<Vec4<float>> st(nc);
+        for (int i = 0; i < nc; i++) st[i] = {(float)u[i], (float)v[i], (float)w[i], (float)(rho[i] - s->params.rho0)};
+        LBFS_CUDA(cudaMemcpyAsync(s->f32.state, st.data(), nc * sizeof(Vec4<float>), cudaMemcpyHostToDevice, s->stream));
+        LBFS_CUDA(cudaMemcpyAsync(s->f32.t1, t1.data(), nc * sizeof(double4), cudaMemcpyHostToDevice, s->stream));
+    } else {
+        std::vector<Vec4<double>> st(nc);
+        for (int i = 0; i < nc; i++) st[i] = {u[i], v[i], w[i], rho[i]};
+        LBFS_CUDA(cudaMemcpyAsync(s->f64.state, st.data(), nc * sizeof(Vec4<double>), cudaMemcpyHostToDevice, s->stream));
+        LBFS_CUDA(cudaMemcpyAsync(s->f64.t1, t1.data(), nc * sizeof(double4), cudaMemcpyHostToDevice, s->stream));
+    }
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_get_state(lbfs_solver *s, double *rho, double *u, double *v, double *w) {
+    if (!s || !rho || !u || !v || !w) return set_error(LBFS_ERR_ARG, "null argument");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    const int nc = s->nc;
+    if (s->fp32) {
+        std::vector<Vec4<float>> st(nc);
+        LBFS_CUDA(cudaMemcpyAsync(st.data(), s->f32.state, nc * sizeof(Vec4<float>), cudaMemcpyDeviceToHost, s->stream));
+        LBFS_CUDA(cudaStreamSynchronize(s->stream));
+        for (int i = 0; i < nc; i++) {
+            rho[i] = (double)st[i].rho + s->params.rho0; u[i] = st[i].u; v[i] = st[i].v; w[i] = st[i].w;
+        }
+    } else {
+        std::vector<Vec4<double>> st(nc);
+        LBFS_CUDA(cudaMemcpyAsync(st.data(), s->f64.state, nc * sizeof(Vec4<double>), cudaMemcpyDeviceToHost, s->stream));
+        LBFS_CUDA(cudaStreamSynchronize(s->stream));
+        for (int i = 0; i < nc; i++) { rho[i] = st[i].rho; u[i] = st[i].u; v[i] = st[i].v; w[i] = st[i].w; }
+    }
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_step(lbfs_solver *s, int32_t n_steps) {
+    if (!s || n_steps < 0) return set_error(LBFS_ERR_ARG, "bad arguments");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    for (int k = 0; k < n_steps; k++) {
+        int n = 0;
+        int rc = enqueue(s, visc_due(s, s->t), &n);
+        if (rc) return rc;
+        s->t++;
+    }
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_step_graph(lbfs_solver *s, int32_t n_steps) {
+    if (!s || n_steps < 0) return set_error(LBFS_ERR_ARG, "bad arguments");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    if (!s->graph) {
+        cudaGraph_t g;
+        LBFS_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        int n = 0;
+        int rc = enqueue(s, false, &n);
+        cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        s->graph_steps = 1;
+    }
+    for (int k = 0; k < n_steps; k++) {
+        if (visc_due(s, s->t)) {
+            int rc = enqueue(s, true, nullptr);
+            if (rc) return rc;
+        } else {
+            LBFS_CUDA(cudaGraphLaunch(s->graph, s->stream));
+        }
+        s->t++;
+    }
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_synchronize(lbfs_solver *s) {
+    if (!s) return set_error(LBFS_ERR_ARG, "null handle");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_get_nodes(lbfs_solver *s, int32_t which, double *out) {
+    if (!s || !out) return set_error(LBFS_ERR_ARG, "null argument");
+    if (s->n_membranes == 0) return LBFS_OK;
+    LBFS_CUDA(cudaSetDevice(s->device));
+    double *src[3];
+    if (which == LBFS_NODES_POSITION) { src[0] = s->ma.x; src[1] = s->ma.y; src[2] = s->ma.z; }
+    else if (which == LBFS_NODES_VELOCITY) { src[0] = s->ma.vx; src[1] = s->ma.vy; src[2] = s->ma.vz; }
+    else if (which == LBFS_NODES_FORCE) { src[0] = s->ma.fx; src[1] = s->ma.fy; src[2] = s->ma.fz; }
+    else return set_error(LBFS_ERR_ARG, "unknown node array");
+    const int N = s->total_nodes;
+    std::vector<double> h(3 * (size_t)N);
+    for (int c = 0; c < 3; c++)
+        LBFS_CUDA(cudaMemcpyAsync(h.data() + (size_t)c * N, src[c], N * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    for (int n = 0; n < N; n++)
+        for (int c = 0; c < 3; c++) out[3 * n + c] = h[(size_t)c * N + n];
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_set_nodes(lbfs_solver *s, const double *xyz) {
+    if (!s || !xyz) return set_error(LBFS_ERR_ARG, "null argument");
+    if (s->n_membranes == 0) return LBFS_OK;
+    LBFS_CUDA(cudaSetDevice(s->device));
+    const int N = s->total_nodes;
+    std::vector<double> h(3 * (size_t)N);
+    for (int n = 0; n < N; n++)
+        for (int c = 0; c < 3; c++) h[(size_t)c * N + n] = xyz[3 * n + c];
+    double *dst[3] = {s->ma.x, s->ma.y, s->ma.z};
+    for (int c = 0; c < 3; c++)
+        LBFS_CUDA(cudaMemcpyAsync(dst[c], h.data() + (size_t)c * N, N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_get_totals(lbfs_solver *s, double *out) {
+    if (!s || !out) return set_error(LBFS_ERR_ARG, "null argument");
+    if (s->n_membranes == 0) return LBFS_OK;
+    LBFS_CUDA(cudaSetDevice(s->device));
+    std::vector<MembraneScalars> h(s->n_membranes);
+    LBFS_CUDA(cudaMemcpyAsync(h.data(), s->ma.ms, h.size() * sizeof(MembraneScalars), cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    for (int m = 0; m < s->n_membranes; m++) {
+        out[6 * m] = h[m].V; out[6 * m + 1] = h[m].V0; out[6 * m + 2] = h[m].A;
+        out[6 * m + 3] = h[m].A0; out[6 * m + 4] = h[m].MAD; out[6 * m + 5] = h[m].MAD0;
+    }
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_get_residuals(lbfs_solver *s, double *out) {
+    if (!s || !out) return set_error(LBFS_ERR_ARG, "null argument");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    double h[4];
+    LBFS_CUDA(cudaMemcpyAsync(h, s->fp32 ? s->f32.residual_sums : s->f64.residual_sums, sizeof(h),
+                              cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    const double ref_mom = s->params.ref_rho * s->params.max_velocity;
+    for (int k = 0; k < 4; k++) out[k] = std::sqrt(h[k] / s->nc) / (k == 0 ? s->params.ref_rho : ref_mom);
+    return LBFS_OK;
+}
+
+namespace {
+template <typename R> int copy_real(lbfs_solver *s, const R *src, size_t n, double *out) {
+    std::vector<R> h(n);
+    LBFS_CUDA(cudaMemcpyAsync(h.data(), src, n * sizeof(R), cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    for (size_t i = 0; i < n; i++) out[i] = (double)h[i];
+    return LBFS_OK;
+}
+template <typename R> int get_field_t(lbfs_solver *s, int which, double *out) {
+    FluidArgs<R> &a = fluid<R>(s);
+    const size_t nt = (size_t)s->nc + s->nb;
+    switch (which) {
+    case LBFS_FIELD_GRADIENTS: return copy_real<R>(s, a.grad, 12 * nt, out);
+    case LBFS_FIELD_FACE_FLUX: return copy_real<R>(s, (const R *)a.flux, 4 * (size_t)s->nf, out);
+    case LBFS_FIELD_RESIDUAL:
+        if (!s->d_res_out) return set_error(LBFS_ERR_STATE, "residuals are kept only after lbfs_keep_residuals(s, 1)");
+        return copy_real<double>(s, s->d_res_out, 4 * (size_t)s->nc, out);
+    case LBFS_FIELD_T1: return copy_real<double>(s, (const double *)a.t1, 4 * (size_t)s->nc, out);
+    case LBFS_FIELD_VISC: return copy_real<R>(s, a.visc_factor, (size_t)s->nc, out);
+    case LBFS_FIELD_GHOST: {
+        std::vector<double> tmp(4 * nt);
+        int rc = copy_real<R>(s, (const R *)a.state, 4 * nt, tmp.data());
+        if (rc) return rc;
+        for (int b = 0; b < s->nb; b++)
+            for (int c = 0; c < 4; c++) out[4 * b + c] = tmp[4 * ((size_t)s->nc + b) + c] + (c == 3 ? (double)a.rho0 : 0.0);
+        return LBFS_OK;
+    }
+    case LBFS_FIELD_FORCE: {
+        // body force + IBM patches, evaluated on the host from the device patches
+        const int nc = s->nc;
+        for (int i = 0; i < nc; i++) { out[3 * i] = a.force[0]; out[3 * i + 1] = a.force[1]; out[3 * i + 2] = a.force[2]; }
+        if (s->n_membranes == 0) return LBFS_OK;
+        std::vector<MembraneScalars> ms(s->n_membranes);
+        LBFS_CUDA(cudaMemcpy(ms.data(), s->ma.ms, ms.size() * sizeof(MembraneScalars), cudaMemcpyDeviceToHost));
+        std::vector<double> pf((size_t)s->n_membranes * kMaxPatchCells * 3);
+        LBFS_CUDA(cudaMemcpy(pf.data(), s->ma.patch_force, pf.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < nc; i++) {
+            const int ci = i % a.grid_nx, cj = (i / a.grid_nx) % a.grid_ny, ck = i / (a.grid_nx * a.grid_ny);
+            for (int m = 0; m < s->n_membranes; m++) {
+                const int px = ci - ms[m].patch_lo[0], py = cj - ms[m].patch_lo[1], pz = ck - ms[m].patch_lo[2];
+                if (ms[m].patch_cells > 0 && px >= 0 && py >= 0 && pz >= 0 && px < ms[m].patch_dim[0] &&
+                    py < ms[m].patch_dim[1] && pz < ms[m].patch_dim[2]) {
+                    const double *p = pf.data() + ((size_t)m * kMaxPatchCells +
+                                                    (px + ms[m].patch_dim[0] * (py + ms[m].patch_dim[1] * pz))) * 3;
+                    out[3 * i] += p[0]; out[3 * i + 1] += p[1]; out[3 * i + 2] += p[2];
+                }
+            }
+        }
+        return LBFS_OK;
+    }
+    case LBFS_FIELD_SPRING: {
+        const int S = s->total_springs;
+        if (S == 0) return LBFS_OK;
+        std::vector<double> c(S), k(S), cv(S), c0(S), a0(S), ar0(2 * (size_t)S), ar(2 * (size_t)S);
+        LBFS_CUDA(cudaMemcpy(c.data(), s->ma.contour, S * sizeof(double), cudaMemcpyDeviceToHost));
+        LBFS_CUDA(cudaMemcpy(k.data(), s->ma.kspring, S * sizeof(double), cudaMemcpyDeviceToHost));
+        LBFS_CUDA(cudaMemcpy(cv.data(), s->ma.curv, S * sizeof(double), cudaMemcpyDeviceToHost));
+        LBFS_CUDA(cudaMemcpy(c0.data(), s->ma.curv0, S * sizeof(double), cudaMemcpyDeviceToHost));
+        LBFS_CUDA(cudaMemcpy(a0.data(), s->ma.angle0, S * sizeof(double), cudaMemcpyDeviceToHost));
+        LBFS_CUDA(cudaMemcpy(ar0.data(), s->ma.area0, 2 * S * sizeof(double), cudaMemcpyDeviceToHost));
+        LBFS_CUDA(cudaMemcpy(ar.data(), s->ma.area, 2 * S * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < S; i++) {
+            double *o = out + 9 * (size_t)i;
+            o[0] = c[i]; o[1] = k[i]; o[2] = cv[i]; o[3] = c0[i]; o[4] = a0[i];
+            o[5] = ar0[2 * i]; o[6] = ar0[2 * i + 1]; o[7] = ar[2 * i]; o[8] = ar[2 * i + 1];
+        }
+        return LBFS_OK;
+    }
+    default: return set_error(LBFS_ERR_ARG, "unknown field");
+    }
+}
+}  // namespace
+
+extern "C" int lbfs_get_field(lbfs_solver *s, int32_t which, double *out) {
+    if (!s || !out) return set_error(LBFS_ERR_ARG, "null argument");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    return s->fp32 ? get_field_t<float>(s, which, out) : get_field_t<double>(s, which, out);
+}
+
+extern "C" int lbfs_keep_residuals(lbfs_solver *s, int32_t on) {
+    if (!s) return set_error(LBFS_ERR_ARG, "null handle");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    if (on && !s->d_res_out) {
+        int rc = s->alloc(&s->d_res_out, 4 * (size_t)s->nc);
+        if (rc) return rc;
+        LBFS_CUDA(cudaMemset(s->d_res_out, 0, 4 * sizeof(double) * (size_t)s->nc));
+    }
+    double *p = on ? s->d_res_out : nullptr;
+    s->f64.res_out = p;
+    s->f32.res_out = p;
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_status(lbfs_solver *s, uint32_t *flags) {
+    if (!s || !flags) return set_error(LBFS_ERR_ARG, "null argument");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    unsigned int h = 0;
+    LBFS_CUDA(cudaMemcpyAsync(&h, s->fp32 ? s->f32.flags : s->f64.flags, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    *flags = h;
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_launches_per_step(lbfs_solver *s, int32_t *launches) {
+    if (!s || !launches) return set_error(LBFS_ERR_ARG, "null argument");
+    *launches = s->launches_per_step;
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_last_error(char *buf, int32_t len) {
+    if (!buf || len <= 0) return LBFS_ERR_ARG;
+    std::snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
+    return LBFS_OK;
+}

@@ -1,0 +1,128 @@
+"""Uniform OpenFOAM-layout hex meshes and boundary tables.
+
+The mesh arrays come from lbfs_mesh_build_uniform, which reproduces
+unstructured_mesh::create_uniform_openfoam_mesh + generate_internal_mesh and
+gradients::pre_fill_LHS_and_RHS_matrix (unstructured_mesh.cpp:239-666,
+1592-1692; gradients.cpp:214-315): same face order (interior x, y, z faces,
+then the boundary patches left, right, bottom, top, back, front), same ghost
+numbering, same gradient stencil order.
+"""
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+
+PATCHES = ("left", "right", "bottom", "top", "back", "front")
+
+
+@dataclass
+class UniformMesh:
+    X: float
+    Y: float
+    Z: float
+    dt: float
+    origin: tuple
+    n_cells: int
+    n_faces: int
+    n_interior: int
+    n_bc: int
+    n_face_x: int
+    n_face_y: int
+    n_face_z: int
+    owner: np.ndarray
+    neighbour: np.ndarray
+    face_area: np.ndarray
+    face_normal: np.ndarray
+    face_centroid: np.ndarray
+    streaming_dt: np.ndarray
+    cell_volume: np.ndarray
+    cell_centroid: np.ndarray
+    gradient_stencil: np.ndarray
+    lhs_inverse: np.ndarray
+    rhs: np.ndarray
+    bc_patch: np.ndarray
+    delta_h: float
+    bc_rho_type: np.ndarray = field(default=None)
+    bc_vel_type: np.ndarray = field(default=None)
+    bc_values: np.ndarray = field(default=None)
+
+    @property
+    def shape(self):
+        """Cells per axis (nx, ny, nz); cell index = i + nx (j + ny k)."""
+        d = 2 * self.dt
+        return int(round(self.X / d)), int(round(self.Y / d)), int(round(self.Z / d))
+
+    @property
+    def delta_x(self):
+        return 2 * self.dt
+
+    def set_boundaries(self, spec):
+        """spec: {patch: (rho_type, vel_type, rho, u, v, w)} for the six patches,
+        values already scaled as after preprocessor::mach_number_factor
+        (Boundary_Conditions::assign_boundary_conditions, Boundary_Conditions.cpp:377-441)."""
+        rt = np.zeros(self.n_bc, np.int32)
+        vt = np.zeros(self.n_bc, np.int32)
+        vals = np.zeros((self.n_bc, 4), np.float64)
+        for p, name in enumerate(PATCHES):
+            rho_type, vel_type, rho, u, v, w = spec[name]
+            sel = self.bc_patch == p
+            rt[sel] = rho_type
+            vt[sel] = vel_type
+            vals[sel] = (u, v, w, rho)
+        self.bc_rho_type, self.bc_vel_type, self.bc_values = rt, vt, np.ascontiguousarray(vals)
+        return self
+
+    def desc(self):
+        """MeshDesc pointing into this object's arrays (keep the mesh alive while it is used)."""
+        if self.bc_rho_type is None:
+            raise ValueError("set_boundaries() first")
+        d = _abi.MeshDesc()
+        d.n_cells, d.n_faces, d.n_interior, d.n_bc = self.n_cells, self.n_faces, self.n_interior, self.n_bc
+        d.n_face_x, d.n_face_y, d.n_face_z = self.n_face_x, self.n_face_y, self.n_face_z
+        d.axis_aligned = 1
+        d.owner, d.neighbour = _abi.iptr(self.owner), _abi.iptr(self.neighbour)
+        d.face_area, d.face_normal = _abi.ptr(self.face_area), _abi.ptr(self.face_normal)
+        d.face_centroid, d.streaming_dt = _abi.ptr(self.face_centroid), _abi.ptr(self.streaming_dt)
+        d.cell_volume, d.cell_centroid = _abi.ptr(self.cell_volume), _abi.ptr(self.cell_centroid)
+        d.gradient_stencil = _abi.iptr(self.gradient_stencil)
+        d.lhs_inverse, d.rhs = _abi.ptr(self.lhs_inverse), _abi.ptr(self.rhs)
+        d.bc_rho_type, d.bc_vel_type = _abi.iptr(self.bc_rho_type), _abi.iptr(self.bc_vel_type)
+        d.bc_values = _abi.ptr(self.bc_values)
+        d.origin[:] = self.origin
+        d.length[:] = (self.X, self.Y, self.Z)
+        d.delta_x = self.delta_x
+        d.delta_h = self.delta_h
+        return d
+
+
+def uniform_counts(X, Y, Z, dt):
+    out = (ctypes.c_int32 * 8)()
+    _abi.check(_abi.lib().lbfs_mesh_uniform_counts(X, Y, Z, dt, out))
+    return list(out)
+
+
+def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_min=0.0, gradient="LS"):
+    """Uniform mesh of ceil(X/(2 dt)) x ceil(Y/(2 dt)) x ceil(Z/(2 dt)) cells (mesh_type 6)."""
+    nc, nf, ni, nb, nfx, nfy, nfz, nt = uniform_counts(X, Y, Z, dt)
+    owner = np.zeros(nf, np.int32)
+    neighbour = np.zeros(nf, np.int32)
+    area = np.zeros(nf)
+    normal = np.zeros((nf, 3))
+    fcen = np.zeros((nf, 3))
+    sdt = np.zeros(nf)
+    vol = np.zeros(nt)
+    ccen = np.zeros((nt, 3))
+    stencil = np.zeros((nc, 6), np.int32)
+    lhs = np.zeros((nc, 9))
+    rhs = np.zeros((nc, 6, 3))
+    patch = np.zeros(nb, np.int32)
+    dh = ctypes.c_double()
+    org = np.asarray(origin, np.float64)
+    _abi.check(_abi.lib().lbfs_mesh_build_uniform(
+        X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, 1 if gradient == "hybrid" else 0, _abi.iptr(owner),
+        _abi.iptr(neighbour), _abi.ptr(area), _abi.ptr(normal), _abi.ptr(fcen), _abi.ptr(sdt), _abi.ptr(vol),
+        _abi.ptr(ccen), _abi.iptr(stencil), _abi.ptr(lhs), _abi.ptr(rhs), _abi.iptr(patch), ctypes.byref(dh)))
+    return UniformMesh(X, Y, Z, dt, tuple(origin), nc, nf, ni, nb, nfx, nfy, nfz, owner, neighbour, area, normal,
+                       fcen, sdt, vol, ccen, stencil, lhs, rhs, patch, dh.value)

@@ -1,0 +1,150 @@
+"""Host-side mirror of the reference's GPU solver entry point.
+
+GpuSolver is the time loop of gpu_solver::General_Purpose_Solver_mk_i
+(Solver_gpu.cu:178-1275) over the C ABI: construction uploads the mesh and the
+membranes and runs the membrane set-up (Solver_gpu.cu:659-735), step() advances
+the time loop (one iteration = Solver_gpu.cu:749-1046), state() is the
+write-back into Solution.  Errors surface as LbfsError, never as exit().
+"""
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+
+
+@dataclass
+class StepParams:
+    """Scalars of global_variables / initial_conditions the step uses (values as
+    after preprocessor::mach_number_factor and global_variables::initialise)."""
+    visc: float
+    delta_t: float = 1.0
+    gamma_inv: float = 1.0
+    channel_diameter: float = 1.0
+    body_force: tuple = (0.0, 0.0, 0.0)
+    ref_rho: float = 1.0
+    max_velocity: float = 0.01
+    rho0: float = 1.0
+    visc_factor_initial: float = 1.0
+    testcase: int = 1
+    precision: int = _abi.LBFS_FP64
+    ibm_stencil: int = _abi.LBFS_IBM_HAT2
+    viscosity_period: int = 10000
+
+    def to_c(self):
+        p = _abi.Params()
+        p.visc, p.delta_t, p.gamma_inv = self.visc, self.delta_t, self.gamma_inv
+        p.channel_diameter = self.channel_diameter
+        p.body_force[:] = self.body_force
+        p.ref_rho, p.max_velocity, p.rho0 = self.ref_rho, self.max_velocity, self.rho0
+        p.visc_factor_initial = self.visc_factor_initial
+        p.testcase, p.precision, p.ibm_stencil = self.testcase, self.precision, self.ibm_stencil
+        p.viscosity_period = self.viscosity_period
+        return p
+
+
+class GpuSolver:
+    def __init__(self, mesh, params, membranes=(), device=0):
+        self.mesh = mesh
+        self.params = params
+        self.membranes = list(membranes)
+        self._mdesc = mesh.desc()
+        self._pdesc = params.to_c()
+        descs = [m.desc() for m in self.membranes]
+        self._rdesc = (_abi.RbcDesc * max(1, len(descs)))(*descs) if descs else None
+        h = ctypes.c_void_p()
+        _abi.check(_abi.lib().lbfs_create(ctypes.byref(self._mdesc), ctypes.byref(self._pdesc),
+                                          self._rdesc if self._rdesc is not None else None, len(descs), device,
+                                          ctypes.byref(h)))
+        self._h = h
+        self.n_cells = mesh.n_cells
+        self.total_nodes = sum(m.n_nodes for m in self.membranes)
+        self.total_springs = sum(len(m.springs) for m in self.membranes)
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _abi.lib().lbfs_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state ----------------------------------------------------------------
+    def set_state(self, rho, u, v, w):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (rho, u, v, w)]
+        for a in arrs:
+            if a.shape != (self.n_cells,):
+                raise ValueError("state arrays must have n_cells entries")
+        _abi.check(_abi.lib().lbfs_set_state(self._h, *[_abi.ptr(a) for a in arrs]))
+
+    def state(self):
+        out = [np.empty(self.n_cells) for _ in range(4)]
+        _abi.check(_abi.lib().lbfs_get_state(self._h, *[_abi.ptr(a) for a in out]))
+        return tuple(out)
+
+    def step(self, n=1, graph=False):
+        fn = _abi.lib().lbfs_step_graph if graph else _abi.lib().lbfs_step
+        _abi.check(fn(self._h, int(n)))
+
+    def synchronize(self):
+        _abi.check(_abi.lib().lbfs_synchronize(self._h))
+
+    # -- diagnostics ----------------------------------------------------------
+    def nodes(self, which=_abi.LBFS_NODES_POSITION):
+        out = np.zeros((self.total_nodes, 3))
+        if self.total_nodes:
+            _abi.check(_abi.lib().lbfs_get_nodes(self._h, which, _abi.ptr(out)))
+        return out
+
+    def set_nodes(self, xyz):
+        a = np.ascontiguousarray(xyz, np.float64)
+        _abi.check(_abi.lib().lbfs_set_nodes(self._h, _abi.ptr(a)))
+
+    def totals(self):
+        """(n_membranes, 6): V, V0, A, A0, MAD, MAD0."""
+        out = np.zeros((max(1, len(self.membranes)), 6))
+        if self.membranes:
+            _abi.check(_abi.lib().lbfs_get_totals(self._h, _abi.ptr(out)))
+        return out[: len(self.membranes)]
+
+    def residuals(self):
+        out = np.zeros(4)
+        _abi.check(_abi.lib().lbfs_get_residuals(self._h, _abi.ptr(out)))
+        return out
+
+    def keep_residuals(self, on=True):
+        _abi.check(_abi.lib().lbfs_keep_residuals(self._h, 1 if on else 0))
+
+    def field(self, which):
+        m = self.mesh
+        nt = m.n_cells + m.n_bc
+        size = {
+            _abi.LBFS_FIELD_GRADIENTS: 12 * nt, _abi.LBFS_FIELD_FACE_FLUX: 4 * m.n_faces,
+            _abi.LBFS_FIELD_RESIDUAL: 4 * m.n_cells, _abi.LBFS_FIELD_FORCE: 3 * m.n_cells,
+            _abi.LBFS_FIELD_T1: 4 * m.n_cells, _abi.LBFS_FIELD_VISC: m.n_cells, _abi.LBFS_FIELD_GHOST: 4 * m.n_bc,
+            _abi.LBFS_FIELD_SPRING: 9 * self.total_springs,
+        }[which]
+        out = np.zeros(max(size, 1))
+        _abi.check(_abi.lib().lbfs_get_field(self._h, which, _abi.ptr(out)))
+        return out[:size]
+
+    def status(self):
+        f = ctypes.c_uint32()
+        _abi.check(_abi.lib().lbfs_status(self._h, ctypes.byref(f)))
+        return f.value
+
+    def launches_per_step(self):
+        n = ctypes.c_int32()
+        _abi.check(_abi.lib().lbfs_launches_per_step(self._h, ctypes.byref(n)))
+        return n.value
