@@ -1,0 +1,103 @@
+"""Seeded synthetic workloads (the reference ships no input decks or meshes).
+
+poiseuille : 3D square-duct channel driven by a body force along x; no-slip
+             walls in y and z (bc velocity type 1), zero-gradient (type 2) at
+             the x ends, which matches an x-periodic duct once developed.
+shear_rbc  : wall-driven simple shear (bc velocity type 10, u = y * gamma_dot
+             on the y walls) with one red cell: a level-L icosphere of radius R
+             cells as the stress-free shape and its Evans-Fung biconcave map as
+             the initial shape, at the domain centre.
+
+Lengths are in the reference's units: a cell is 2 * dt wide (dt = streaming
+step = 1), so a domain of n cells per axis has X = 2 n.
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from .mesh import build_uniform_mesh
+from .rbc import red_cell, rotation_matrix
+from .solver import StepParams
+
+
+@dataclass
+class Case:
+    name: str
+    mesh: object
+    params: StepParams
+    membranes: list
+    rho: np.ndarray
+    u: np.ndarray
+    v: np.ndarray
+    w: np.ndarray
+    bcs: dict
+    info: dict = field(default_factory=dict)
+
+
+def _initial_state(n_cells, seed, amplitude=1e-4, rho0=1.0, u0=None):
+    rng = np.random.default_rng(seed)
+    rho = np.full(n_cells, rho0)
+    u = rng.uniform(-amplitude, amplitude, n_cells)
+    v = rng.uniform(-amplitude, amplitude, n_cells)
+    w = rng.uniform(-amplitude, amplitude, n_cells)
+    if u0 is not None:
+        u = u + u0
+    return rho, u, v, w
+
+
+def poiseuille(n=32, seed=1234, tau=0.8, u_centre=0.01, delta_t=0.5, precision=_abi.LBFS_FP64, ny=None, nz=None):
+    """Body-force-driven square duct, n x ny x nz cells (default cube)."""
+    ny = ny or n
+    nz = nz or n
+    dt = 1.0
+    visc = (tau - 0.5) / 3.0 * dt
+    mesh = build_uniform_mesh(2.0 * n, 2.0 * ny, 2.0 * nz, dt, visc=visc)
+    bcs = {"left": (2, 2, 1.0, 0.0, 0.0, 0.0), "right": (2, 2, 1.0, 0.0, 0.0, 0.0),
+           "bottom": (2, 1, 1.0, 0.0, 0.0, 0.0), "top": (2, 1, 1.0, 0.0, 0.0, 0.0),
+           "back": (2, 1, 1.0, 0.0, 0.0, 0.0), "front": (2, 1, 1.0, 0.0, 0.0, 0.0)}
+    mesh.set_boundaries(bcs)
+    # square duct of half-width a: u_max = 0.2947 f a^2 / (rho nu)  (series solution)
+    a = 0.5 * 2.0 * min(ny, nz)
+    force = u_centre * visc / (0.2947 * a * a)
+    params = StepParams(visc=visc, delta_t=delta_t, channel_diameter=2.0 * ny, body_force=(force, 0.0, 0.0),
+                        ref_rho=1.0, max_velocity=u_centre, rho0=1.0, visc_factor_initial=1.0, testcase=2,
+                        precision=precision, viscosity_period=0)
+    rho, u, v, w = _initial_state(mesh.n_cells, seed)
+    return Case("poiseuille", mesh, params, [], rho, u, v, w, bcs,
+                {"n": (n, ny, nz), "tau": tau, "force": force, "u_centre": u_centre})
+
+
+def shear_rbc(n=64, level=3, radius_cells=8.0, capillary=0.1, u_wall=0.02, seed=4321, tau=0.8, delta_t=0.5,
+              precision=_abi.LBFS_FP64, ibm_stencil=_abi.LBFS_IBM_PESKIN4, n_cells_y=None, n_cells_z=None,
+              rotate=False):
+    """Simple shear with one red cell of radius `radius_cells` cells at the centre."""
+    ny = n_cells_y or n
+    nz = n_cells_z or n
+    dt = 1.0
+    visc = (tau - 0.5) / 3.0 * dt
+    X, Y, Z = 2.0 * n, 2.0 * ny, 2.0 * nz
+    mesh = build_uniform_mesh(X, Y, Z, dt, visc=visc)
+    gamma = u_wall / Y
+    bcs = {"left": (2, 2, 1.0, 0.0, 0.0, 0.0), "right": (2, 2, 1.0, 0.0, 0.0, 0.0),
+           "bottom": (2, 10, 1.0, gamma, 0.0, 0.0), "top": (2, 10, 1.0, gamma, 0.0, 0.0),
+           "back": (2, 2, 1.0, 0.0, 0.0, 0.0), "front": (2, 2, 1.0, 0.0, 0.0, 0.0)}
+    mesh.set_boundaries(bcs)
+    R = radius_cells * 2.0 * dt
+    shear_modulus = visc * gamma * R / capillary
+    moduli = dict(volume_modulus=500.0 * shear_modulus, local_area_modulus=10.0 * shear_modulus,
+                  global_area_modulus=500.0 * shear_modulus, shear_modulus=shear_modulus,
+                  global_bending_modulus=0.05 * shear_modulus * R * R, local_bending_modulus=0.0,
+                  viscosity=0.0, wlc_ratio=2.2, curvature_ratio=0.0, volume_ratio=1.0,
+                  internal_viscosity_ratio=5.0)
+    rng = np.random.default_rng(seed)
+    rot = rotation_matrix(rng) if rotate else None
+    cell = red_cell(level, R, (0.5 * X, 0.5 * Y, 0.5 * Z), rot, **moduli)
+    params = StepParams(visc=visc, delta_t=delta_t, channel_diameter=Y, ref_rho=1.0, max_velocity=u_wall, rho0=1.0,
+                        visc_factor_initial=1.0, testcase=5, precision=precision, ibm_stencil=ibm_stencil,
+                        viscosity_period=10000)
+    y = mesh.cell_centroid[: mesh.n_cells, 1]
+    rho, u, v, w = _initial_state(mesh.n_cells, seed, u0=gamma * y)
+    return Case("shear_rbc", mesh, params, [cell], rho, u, v, w, bcs,
+                {"n": (n, ny, nz), "level": level, "radius_cells": radius_cells, "capillary": capillary,
+                 "gamma_dot": gamma, "shear_modulus": shear_modulus})
