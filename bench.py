@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark of the LBFS-IBM time step on B200.
+
+Workload (one GPU): wall-driven shear on a 64^3-cell uniform hex mesh stored as
+an unstructured face/cell list (262,144 cells, 798,720 faces), one red cell
+(level-3 icosphere: 642 nodes, 1,280 triangles, 1,920 springs, radius 8 cells,
+capillary number 0.1) with the 4-point Peskin IBM delta, plain FP64 -- the
+single-RBC shear configuration.  A "step" is one time step of the solver.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm: `value` is the device-timed throughput (Mcell-updates/s) with the
+state resident in HBM, L2 flushed between timed steps (the 64^3 working set
+fits in L2), each step timed by the library's CUDA events on its own streams;
+`e2e` is the same metric through the C ABI with host buffers (page-locked H2D
+of the state, the step, D2H of the state, every step); `roofline` is the
+dominant kernel's algorithmic bytes per launch over its event-timed duration
+against the measured HBM copy bandwidth; `cpu_baseline` is the reference's own
+kernels compiled for the host (oracle/_ref) on a bounded sample.
+Reference arm: the reference's own CPU implementation of the step (its kernel
+sources compiled for the host, serial per instance) on every host core, one
+instance per core.  For N > 1 GPUs each rank runs an independent replica of the
+workload (the path has no exchange step between replicas): weak scaling.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lbfs-ibm-ade-sp_b200"))
+
+METRIC = "Mcell-updates/s"
+WORKLOAD = ("shear_rbc: 64^3-cell uniform hex mesh as unstructured faces (262144 cells, 798720 faces), "
+            "wall shear (bc type 10), 1 red cell L3 icosphere (642 nodes, 1280 triangles, 1920 springs), "
+            "radius 8 cells, Ca 0.1, 4-point Peskin IBM, FP64")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=64, help="cells per axis")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(mesh, phase, fp64=True):
+    """Bytes each kernel must move once per launch (every array element it
+    reads or writes counted once), FP64 storage."""
+    nc, nf, ni, nb = mesh.n_cells, mesh.n_faces, mesh.n_interior, mesh.n_bc
+    R = 8 if fp64 else 4
+    if phase == "flux":
+        # per axis face: owner+neighbour ids 8, geometry (area, dt, t1, t2) 4R, flux out 4R;
+        # per bc face: ids 8, geometry 12R, bc types/values 8 + 4R, flux out 4R;
+        # per cell (interior and ghost): state 4R + 12 gradients 12R, visc factor R (interior)
+        return ni * (8 + 8 * R) + nb * (16 + 20 * R) + nc * (17 * R) + nb * (16 * R)
+    if phase == "gradients":
+        # per cell: stencil 24, RHS 18R, LHS^-1 9R, state 4R, gradients out 12R;
+        # per ghost: bc record 9R + types 8 + values 4R, ghost state out 4R, ghost gradients out 12R
+        return nc * (24 + 43 * R) + nb * (8 + 29 * R)
+    if phase == "update":
+        # per cell: face list 24, volume 8, t1 in/out 64, state out 4R; each face flux read once 4R
+        return nc * (96 + 4 * R) + nf * 4 * R
+    return 0
+
+
+def read_traffic(kernel):
+    """DRAM bytes per launch from the committed ncu summary (profiles/dram_traffic.txt)."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if len(f) >= 2 and f[0] == kernel and not line.startswith("#"):
+            try:
+                return float(f[1])
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline_sample(n, budget_s=12.0, max_steps=200):
+    """The reference's own kernels compiled for the host (oracle/_ref), serial,
+    on the same workload (its 2-point IBM; the reference has no 4-point kernel)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import ref_lbfs
+    from lbfs_b200 import _abi, cases
+    c = cases.shear_rbc(n=n, ibm_stencil=_abi.LBFS_IBM_HAT2)
+    if ref_lbfs.available():
+        from make_golden import ref_case
+        solver, kind = ref_case(c), "reference"
+    else:
+        from oracle_lbfs import OracleSolver
+        solver, kind = OracleSolver(c.mesh, c.params, c.membranes), "port"
+        solver.set_state(c.rho, c.u, c.v, c.w)
+    solver.step(1)
+    t0, steps = time.perf_counter(), 0
+    while steps < max_steps and time.perf_counter() - t0 < budget_s:
+        solver.step(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": c.mesh.n_cells * steps / dt / 1e6, "unit": METRIC, "cores": 1, "kind": kind,
+            "sample": f"{steps} steps of the {n}^3 + 1 red cell workload (2-point IBM), serial, {dt:.1f} s"}
+
+
+def _ref_worker(args):
+    n, steps, warmup = args
+    sys.path.insert(0, os.path.join(ROOT, "lbfs-ibm-ade-sp_b200"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from lbfs_b200 import _abi, cases
+    from make_golden import ref_case
+    c = cases.shear_rbc(n=n, ibm_stencil=_abi.LBFS_IBM_HAT2)
+    rc = ref_case(c)
+    rc.step(warmup)
+    t0 = time.perf_counter()
+    rc.step(steps)
+    return c.mesh.n_cells * steps, time.perf_counter() - t0
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_lbfs
+    if not ref_lbfs.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_lbfs.so was not built "
+                          "(the reference sources were absent when build() ran)"}))
+        return 0
+    import multiprocessing as mp
+    try:
+        import psutil
+        mem_procs = int(psutil.virtual_memory().available // (1200 * 2 ** 20))
+    except Exception:
+        mem_procs = os.cpu_count() or 1
+    procs = max(1, min(os.cpu_count() or 1, mem_procs))
+    # each "step" of this arm is one time step of every instance; bound the run to a few minutes
+    steps = max(1, min(args.steps, 60))
+    warmup = max(1, min(args.warmup, 3))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, [(args.n, steps, warmup)] * procs)
+    wall = time.perf_counter() - t0
+    cells = sum(r[0] for r in res)
+    slowest = max(r[1] for r in res)
+    value = cells / slowest / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": world, "steps": steps,
+        "warmup": warmup, "ms_per_step": slowest / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD.replace("4-point Peskin", "2-point hat (the reference has no 4-point kernel)"),
+                   "instances": procs, "parallelism": f"{procs} independent host processes"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "reference",
+                         "sample": f"{steps} steps x {procs} instances of the {args.n}^3 workload, "
+                                   f"reference kernels compiled for the host, one instance per core "
+                                   f"(wall {wall:.1f} s incl. set-up)"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    rank, local_rank, world = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from lbfs_b200 import GpuSolver, _abi, cases
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+    warmup = max(3, args.warmup)
+    K = args.steps
+    c = cases.shear_rbc(n=args.n)
+    mesh = c.mesh
+    s = GpuSolver(mesh, c.params, c.membranes, device=local_rank)
+    s.set_state(c.rho, c.u, c.v, c.w)
+    s.set_profiling(True)
+    flush = torch.empty(512 * 2 ** 20, dtype=torch.uint8, device="cuda")  # 512 MB > 126 MB L2
+    s.step(warmup, graph=True)
+    s.synchronize()
+    launches_per_step = s.launches_per_step()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(local_rank)
+    barrier()
+    sampler.start()
+    phase_sum = np.zeros(6)
+    for k in range(K):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        s.step(1, graph=True)
+        phase_sum += s.phase_times()  # synchronises the solver stream; outside the events
+    barrier()
+    clocks = sampler.stop()
+    t_step_ms = phase_sum[5] / K
+    total_s = phase_sum[5] / 1e3
+    if world > 1:
+        t = torch.tensor([total_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_s = float(t.item())
+    cell_updates = mesh.n_cells * K * world
+    value = cell_updates / total_s / 1e6
+    phases = {name: phase_sum[i] / K for i, name in enumerate(["membrane", "gradients", "flux", "update"])}
+    status = s.status()
+
+    # roofline of the dominant fluid kernel (the membrane kernel overlaps them on a second stream)
+    fluid = {k: v for k, v in phases.items() if k != "membrane"}
+    dom = max(fluid, key=fluid.get)
+    peaks, peak_kind = measured_peaks()
+    alg = algorithmic_bytes(mesh, dom)
+    achieved = alg / (fluid[dom] * 1e-3) / 1e9
+    kname = {"flux": "k_face_flux", "gradients": "k_cell_gradients", "update": "k_cell_update"}[dom]
+    traffic = read_traffic(kname)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": alg, "launch_ms": fluid[dom]}
+
+    # end to end through the C ABI with page-locked host buffers
+    e2e = None
+    if not args.no_e2e:
+        n = mesh.n_cells
+        host = [torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+        rho, u, v, w = s.state()
+        for h, a in zip(host, (rho, u, v, w)):
+            h[:] = a
+        s.set_profiling(False)
+        Ke = min(K, 50)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(Ke):
+            _abi.check(_abi.lib().lbfs_set_state(s._h, *[_abi.ptr(h) for h in host]))
+            s.step(1, graph=True)
+            _abi.check(_abi.lib().lbfs_get_state(s._h, *[_abi.ptr(h) for h in host]))
+        barrier()
+        te = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([te], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": n * Ke * world / te / 1e6, "unit": METRIC, "h2d_bytes_per_step": 4 * 8 * n,
+               "d2h_bytes_per_step": 4 * 8 * n, "steps": Ke, "timing": "host wall clock around set_state, step, "
+               "get_state (page-locked host arrays)"}
+
+    # FP32-bulk form on the same workload: throughput and field error against this FP64 run
+    fp32 = None
+    if rank == 0:
+        c32 = cases.shear_rbc(n=args.n, precision=_abi.LBFS_FP32_BULK)
+        c64 = cases.shear_rbc(n=args.n)
+        a, b = GpuSolver(mesh, c64.params, c64.membranes, device=local_rank), \
+            GpuSolver(c32.mesh, c32.params, c32.membranes, device=local_rank)
+        for x in (a, b):
+            x.set_state(c.rho, c.u, c.v, c.w)
+            x.set_profiling(True)
+        b.step(warmup, graph=True)
+        a.step(warmup, graph=True)
+        tb = 0.0
+        for k in range(K):
+            flush.fill_(k & 0xFF)
+            torch.cuda.synchronize()
+            b.step(1, graph=True)
+            tb += b.phase_times()[5]
+            a.step(1, graph=True)
+        sa, sb = a.state(), b.state()
+        errs = [float(np.max(np.abs(x - y)) / np.max(np.abs(y))) for x, y in zip(sb[1:], sa[1:])]
+        drho = float(np.max(np.abs(sb[0] - sa[0])) / np.max(np.abs(sa[0] - 1.0)))
+        fp32 = {"value": mesh.n_cells * K / (tb * 1e-3) / 1e6, "unit": METRIC, "speedup_vs_fp64": None,
+                "rel_err_velocity_vs_fp64": max(errs), "rel_err_rho_deviation_vs_fp64": drho,
+                "steps_compared": warmup + K}
+        fp32["speedup_vs_fp64"] = fp32["value"] / (mesh.n_cells * K / (phase_sum[5] * 1e-3) / 1e6)
+        a.close()
+        b.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_sample(args.n)
+        except Exception as exc:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": METRIC, "cores": 1, "kind": "reference", "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": warmup,
+            "ms_per_step": t_step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": mesh.n_cells, "faces": mesh.n_faces, "membrane_nodes": 642,
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "flushed between timed steps (512 MB write)", "graph": "CUDA graph per step"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * K,
+            "clocks": clocks,
+            "kernel_ms": phases,
+            "rbc_node_steps_per_s": 642 * K * world / total_s,
+            "fp32_bulk": fp32,
+            "status_flags": status,
+        }
+        print(json.dumps(line))
+    s.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -133,6 +133,9 @@ int lbfs_destroy(lbfs_solver *s);
 int lbfs_set_state(lbfs_solver *s, const double *rho, const double *u, const double *v, const double *w);
 int lbfs_get_state(lbfs_solver *s, double *rho, double *u, double *v, double *w);
 
+/* set_state / get_state copy four planes (rho, u, v, w) with one cudaMemcpyAsync
+ * each, so page-locked host arrays transfer at full DMA bandwidth. */
+
 /* Advance n_steps time steps (one iteration of Solver_gpu.cu:749-1046 each).
  * Enqueued on the solver's stream; returns without waiting. */
 int lbfs_step(lbfs_solver *s, int32_t n_steps);
@@ -182,6 +185,14 @@ int lbfs_keep_residuals(lbfs_solver *s, int32_t on);
 
 /* Accumulated status flags (LBFS_FLAG_*) since creation; reading does not clear. */
 int lbfs_status(lbfs_solver *s, uint32_t *flags);
+/* Per-kernel timing with CUDA events around every launch (also inside the
+ * captured graph).  lbfs_get_phase_times writes the durations in ms of the
+ * last step's kernels: [0] membrane, [1] ghost+gradients, [2] face flux,
+ * [3] cell update, [4] interior viscosity (0 when not launched), and [5] the
+ * whole step (first launch to last, on the solver's stream). */
+int lbfs_set_profiling(lbfs_solver *s, int32_t on);
+int lbfs_get_phase_times(lbfs_solver *s, double *ms);
+
 /* Kernel launches issued per time step by this handle (graph or stream). */
 int lbfs_launches_per_step(lbfs_solver *s, int32_t *launches);
 /* Copy of the last error message (NUL terminated, truncated to len). */

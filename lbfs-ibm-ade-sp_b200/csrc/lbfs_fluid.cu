@@ -433,6 +433,32 @@ __global__ void __launch_bounds__(256) k_cell_update(FluidArgs<R> a) {
     }
 }
 
+// ------------------------------------------------------- state transfer ----
+
+template <typename R>
+__global__ void k_pack_state(FluidArgs<R> a, const double *__restrict__ stage) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nc) return;
+    const size_t n = (size_t)a.nc;
+    const double rho = stage[i], u = stage[n + i], v = stage[2 * n + i], w = stage[3 * n + i];
+    Vec4<R> s;
+    s.u = (R)u; s.v = (R)v; s.w = (R)w; s.rho = (R)(rho - (double)a.rho0);
+    a.state[i] = s;
+    a.t1[i] = make_double4(u, v, w, rho);
+}
+
+template <typename R>
+__global__ void k_unpack_state(FluidArgs<R> a, double *__restrict__ stage) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nc) return;
+    const size_t n = (size_t)a.nc;
+    const Vec4<R> s = a.state[i];
+    stage[i] = (double)s.rho + (double)a.rho0;
+    stage[n + i] = (double)s.u;
+    stage[2 * n + i] = (double)s.v;
+    stage[3 * n + i] = (double)s.w;
+}
+
 // ------------------------------------------------------------ launchers ----
 
 template <typename R> int k3_grid(const FluidArgs<R> &a) {
@@ -449,6 +475,17 @@ template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t
 template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s) {
     k_cell_update<R><<<k3_grid(a), 256, 0, s>>>(a);
 }
+
+template <typename R> void launch_pack_state(const FluidArgs<R> &a, const double *stage, cudaStream_t s) {
+    k_pack_state<R><<<(a.nc + 255) / 256, 256, 0, s>>>(a, stage);
+}
+template <typename R> void launch_unpack_state(const FluidArgs<R> &a, double *stage, cudaStream_t s) {
+    k_unpack_state<R><<<(a.nc + 255) / 256, 256, 0, s>>>(a, stage);
+}
+template void launch_pack_state<double>(const FluidArgs<double> &, const double *, cudaStream_t);
+template void launch_pack_state<float>(const FluidArgs<float> &, const double *, cudaStream_t);
+template void launch_unpack_state<double>(const FluidArgs<double> &, double *, cudaStream_t);
+template void launch_unpack_state<float>(const FluidArgs<float> &, double *, cudaStream_t);
 
 template void launch_fluid_gradients<double>(const FluidArgs<double> &, cudaStream_t);
 template void launch_fluid_flux<double>(const FluidArgs<double> &, cudaStream_t);

@@ -13,6 +13,10 @@ constexpr int kK3MaxBlocks = 148 * 8;
 template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s);
+// stage = 4 planes of n_cells doubles (rho, u, v, w); pack also resets soln_t1
+// to the primitive state (Solver_gpu.cu:746)
+template <typename R> void launch_pack_state(const FluidArgs<R> &a, const double *stage, cudaStream_t s);
+template <typename R> void launch_unpack_state(const FluidArgs<R> &a, double *stage, cudaStream_t s);
 
 // Membrane work modes.
 enum MembraneMode : int {

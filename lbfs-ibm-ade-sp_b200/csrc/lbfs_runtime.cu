@@ -24,6 +24,7 @@
 namespace lbfs {
 
 static thread_local std::string g_last_error;
+constexpr int kPhases = 6;  // 5 kernels + the whole step
 
 int set_error(int code, const std::string &msg) {
     g_last_error = msg;
@@ -63,6 +64,12 @@ struct lbfs_solver {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     int launches_per_step = 0;
+    // per-kernel timing: start/stop events per phase (membrane, gradients, flux, update, viscosity)
+    bool profiling = false;
+    cudaEvent_t ev_phase[kPhases][2] = {};
+    bool phase_recorded[kPhases] = {};
+    // staging buffer for host <-> device state transfers: rho, u, v, w planes
+    double *d_stage = nullptr;
 
     template <typename T> int alloc(T **p, size_t count) {
         void *q = nullptr;
@@ -362,33 +369,53 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     return LBFS_OK;
 }
 
+struct PhaseMark {
+    lbfs_solver *s;
+    int phase;
+    cudaStream_t st;
+    PhaseMark(lbfs_solver *s_, int ph, cudaStream_t st_) : s(s_), phase(ph), st(st_) {
+        if (s->profiling) cudaEventRecord(s->ev_phase[phase][0], st);
+    }
+    ~PhaseMark() {
+        if (s->profiling) {
+            cudaEventRecord(s->ev_phase[phase][1], st);
+            s->phase_recorded[phase] = true;
+        }
+    }
+};
+
 template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *launches) {
     FluidArgs<R> &a = fluid<R>(s);
     int n = 0;
+    if (s->profiling) LBFS_CUDA(cudaEventRecord(s->ev_phase[5][0], s->stream));
     if (s->n_membranes > 0) {
         if (visc_update) {
-            launch_membrane(s->ma, s->stream);
-            launch_interior_viscosity(s->va, s->stream);
-            launch_fluid_gradients<R>(a, s->stream);
-            launch_fluid_flux<R>(a, s->stream);
+            { PhaseMark m(s, 0, s->stream); launch_membrane(s->ma, s->stream); }
+            { PhaseMark m(s, 4, s->stream); launch_interior_viscosity(s->va, s->stream); }
+            { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
+            { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
             n += 4;
         } else {
             LBFS_CUDA(cudaEventRecord(s->ev_fork, s->stream));
             LBFS_CUDA(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
-            launch_membrane(s->ma, s->stream2);
+            { PhaseMark m(s, 0, s->stream2); launch_membrane(s->ma, s->stream2); }
             LBFS_CUDA(cudaEventRecord(s->ev_join, s->stream2));
-            launch_fluid_gradients<R>(a, s->stream);
-            launch_fluid_flux<R>(a, s->stream);
+            { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
+            { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
             LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
             n += 3;
         }
     } else {
-        launch_fluid_gradients<R>(a, s->stream);
-        launch_fluid_flux<R>(a, s->stream);
+        { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
+        { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
         n += 2;
     }
-    launch_fluid_update<R>(a, s->stream);
+    { PhaseMark m(s, 3, s->stream); launch_fluid_update<R>(a, s->stream); }
     n += 1;
+    if (s->profiling) {
+        LBFS_CUDA(cudaEventRecord(s->ev_phase[5][1], s->stream));
+        s->phase_recorded[5] = true;
+    }
     LBFS_CUDA(cudaGetLastError());
     if (launches) *launches = n;
     return LBFS_OK;
@@ -404,6 +431,9 @@ bool visc_due(const lbfs_solver *s, long long t) {
 
 void free_all(lbfs_solver *s) {
     if (s->graph) cudaGraphExecDestroy(s->graph);
+    for (int p = 0; p < kPhases; p++)
+        for (int e = 0; e < 2; e++)
+            if (s->ev_phase[p][e]) cudaEventDestroy(s->ev_phase[p][e]);
     for (void *p : s->allocs) cudaFree(p);
     s->allocs.clear();
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
@@ -473,23 +503,28 @@ extern "C" int lbfs_set_stream(lbfs_solver *s, void *stream) {
     return LBFS_OK;
 }
 
+namespace {
+int ensure_stage(lbfs_solver *s) {
+    if (s->d_stage) return LBFS_OK;
+    return s->alloc(&s->d_stage, 4 * (size_t)s->nc);
+}
+}  // namespace
+
+// Host arrays are copied as four planes into a device staging buffer (one
+// cudaMemcpyAsync each: full DMA bandwidth from pinned memory) and packed into
+// the resident (u, v, w, rho) records by a kernel.
 extern "C" int lbfs_set_state(lbfs_solver *s, const double *rho, const double *u, const double *v, const double *w) {
     if (!s || !rho || !u || !v || !w) return set_error(LBFS_ERR_ARG, "null argument");
     LBFS_CUDA(cudaSetDevice(s->device));
-    const int nc = s->nc;
-    std::vector<double4> t1(nc);
-    for (int i = 0; i < nc; i++) t1[i] = make_double4(u[i], v[i], w[i], rho[i]);
-    if (s->fp32) {
-        std::vector<Vec4<float>> st(nc);
-        for (int i = 0; i < nc; i++) st[i] = {(float)u[i], (float)v[i], (float)w[i], (float)(rho[i] - s->params.rho0)};
-        LBFS_CUDA(cudaMemcpyAsync(s->f32.state, st.data(), nc * sizeof(Vec4<float>), cudaMemcpyHostToDevice, s->stream));
-        LBFS_CUDA(cudaMemcpyAsync(s->f32.t1, t1.data(), nc * sizeof(double4), cudaMemcpyHostToDevice, s->stream));
-    } else {
-        std::vector<Vec4<double>> st(nc);
-        for (int i = 0; i < nc; i++) st[i] = {u[i], v[i], w[i], rho[i]};
-        LBFS_CUDA(cudaMemcpyAsync(s->f64.state, st.data(), nc * sizeof(Vec4<double>), cudaMemcpyHostToDevice, s->stream));
-        LBFS_CUDA(cudaMemcpyAsync(s->f64.t1, t1.data(), nc * sizeof(double4), cudaMemcpyHostToDevice, s->stream));
-    }
+    int rc = ensure_stage(s);
+    if (rc) return rc;
+    const size_t nc = (size_t)s->nc, bytes = nc * sizeof(double);
+    const double *src[4] = {rho, u, v, w};
+    for (int k = 0; k < 4; k++)
+        LBFS_CUDA(cudaMemcpyAsync(s->d_stage + k * nc, src[k], bytes, cudaMemcpyHostToDevice, s->stream));
+    if (s->fp32) launch_pack_state<float>(s->f32, s->d_stage, s->stream);
+    else launch_pack_state<double>(s->f64, s->d_stage, s->stream);
+    LBFS_CUDA(cudaGetLastError());
     LBFS_CUDA(cudaStreamSynchronize(s->stream));
     return LBFS_OK;
 }
@@ -497,19 +532,42 @@ extern "C" int lbfs_set_state(lbfs_solver *s, const double *rho, const double *u
 extern "C" int lbfs_get_state(lbfs_solver *s, double *rho, double *u, double *v, double *w) {
     if (!s || !rho || !u || !v || !w) return set_error(LBFS_ERR_ARG, "null argument");
     LBFS_CUDA(cudaSetDevice(s->device));
-    const int nc = s->nc;
-    if (s->fp32) {
-        std::vector<Vec4<float>> st(nc);
-        LBFS_CUDA(cudaMemcpyAsync(st.data(), s->f32.state, nc * sizeof(Vec4<float>), cudaMemcpyDeviceToHost, s->stream));
-        LBFS_CUDA(cudaStreamSynchronize(s->stream));
-        for (int i = 0; i < nc; i++) {
-            rho[i] = (double)st[i].rho + s->params.rho0; u[i] = st[i].u; v[i] = st[i].v; w[i] = st[i].w;
-        }
-    } else {
-        std::vector<Vec4<double>> st(nc);
-        LBFS_CUDA(cudaMemcpyAsync(st.data(), s->f64.state, nc * sizeof(Vec4<double>), cudaMemcpyDeviceToHost, s->stream));
-        LBFS_CUDA(cudaStreamSynchronize(s->stream));
-        for (int i = 0; i < nc; i++) { rho[i] = st[i].rho; u[i] = st[i].u; v[i] = st[i].v; w[i] = st[i].w; }
+    int rc = ensure_stage(s);
+    if (rc) return rc;
+    const size_t nc = (size_t)s->nc, bytes = nc * sizeof(double);
+    if (s->fp32) launch_unpack_state<float>(s->f32, s->d_stage, s->stream);
+    else launch_unpack_state<double>(s->f64, s->d_stage, s->stream);
+    LBFS_CUDA(cudaGetLastError());
+    double *dst[4] = {rho, u, v, w};
+    for (int k = 0; k < 4; k++)
+        LBFS_CUDA(cudaMemcpyAsync(dst[k], s->d_stage + k * nc, bytes, cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_set_profiling(lbfs_solver *s, int32_t on) {
+    if (!s) return set_error(LBFS_ERR_ARG, "null handle");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    if (on && !s->ev_phase[0][0])
+        for (int p = 0; p < kPhases; p++)
+            for (int e = 0; e < 2; e++) LBFS_CUDA(cudaEventCreate(&s->ev_phase[p][e]));
+    s->profiling = on != 0;
+    for (int p = 0; p < kPhases; p++) s->phase_recorded[p] = false;
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_get_phase_times(lbfs_solver *s, double *ms) {
+    if (!s || !ms) return set_error(LBFS_ERR_ARG, "null argument");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    for (int p = 0; p < kPhases; p++) {
+        ms[p] = 0.0;
+        if (!s->profiling || !s->phase_recorded[p]) continue;
+        float t = 0.f;
+        LBFS_CUDA(cudaEventElapsedTime(&t, s->ev_phase[p][0], s->ev_phase[p][1]));
+        ms[p] = t;
     }
     return LBFS_OK;
 }

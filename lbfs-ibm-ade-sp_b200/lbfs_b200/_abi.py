@@ -114,6 +114,8 @@ def lib():
             "lbfs_keep_residuals": [vp, ctypes.c_int32],
             "lbfs_status": [vp, ctypes.POINTER(ctypes.c_uint32)],
             "lbfs_launches_per_step": [vp, _i32p],
+            "lbfs_set_profiling": [vp, ctypes.c_int32],
+            "lbfs_get_phase_times": [vp, _f64p],
             "lbfs_last_error": [ctypes.c_char_p, ctypes.c_int32],
             "lbfs_mesh_uniform_counts": [ctypes.c_double] * 4 + [_i32p],
             "lbfs_mesh_build_uniform": [ctypes.c_double] * 4 + [_f64p, ctypes.c_double, ctypes.c_double,
@@ -158,5 +160,6 @@ EXPORTED = [
     "lbfs_create", "lbfs_destroy", "lbfs_set_state", "lbfs_get_state", "lbfs_step", "lbfs_step_graph",
     "lbfs_synchronize", "lbfs_set_stream", "lbfs_get_nodes", "lbfs_set_nodes", "lbfs_get_totals",
     "lbfs_get_residuals", "lbfs_get_field", "lbfs_keep_residuals", "lbfs_status", "lbfs_launches_per_step",
+    "lbfs_set_profiling", "lbfs_get_phase_times",
     "lbfs_last_error", "lbfs_mesh_uniform_counts", "lbfs_mesh_build_uniform", "lbfs_rbc_build_springs",
 ]

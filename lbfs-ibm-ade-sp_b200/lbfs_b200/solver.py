@@ -144,6 +144,18 @@ class GpuSolver:
         _abi.check(_abi.lib().lbfs_status(self._h, ctypes.byref(f)))
         return f.value
 
+    def set_profiling(self, on=True):
+        _abi.check(_abi.lib().lbfs_set_profiling(self._h, 1 if on else 0))
+
+    def phase_times(self):
+        """Durations (ms) of the last step: membrane, gradients, flux, update, viscosity kernels, whole step."""
+        out = np.zeros(6)
+        _abi.check(_abi.lib().lbfs_get_phase_times(self._h, _abi.ptr(out)))
+        return out
+
+    def set_stream(self, stream_ptr):
+        _abi.check(_abi.lib().lbfs_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
     def launches_per_step(self):
         n = ctypes.c_int32()
         _abi.check(_abi.lib().lbfs_launches_per_step(self._h, ctypes.byref(n)))

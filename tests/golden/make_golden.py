@@ -1,0 +1,106 @@
+"""Writes the golden fixtures of tests/golden/ by running the REFERENCE itself.
+
+The reference's own sources (unstructured_mesh.cpp, gradients.cpp,
+lagrangian_object.cpp and the kernel bodies of LBFS.cu,
+immersed_boundary_method.cu, spring_network.cu, common_kernels.cu) are
+compiled for the host by oracle/build_ref.sh into oracle/_ref/libref_lbfs.so
+and driven by oracle/ref_driver.cpp in the order of the GPU time loop
+(Solver_gpu.cu:749-1046).  Run here, where the reference sources exist:
+
+    oracle/build_ref.sh && python tests/golden/make_golden.py
+
+Each fixture stores its inputs as well as the reference's outputs, so the
+tests replay them without the reference.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "lbfs-ibm-ade-sp_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import ref_lbfs as R  # noqa: E402
+from lbfs_b200 import _abi, cases, icosphere  # noqa: E402
+
+
+def ref_case(c):
+    m = c.mesh
+    rm = R.RefMesh(m.X, m.Y, m.Z, m.dt, m.origin, c.params.visc)
+    p = R.RefParams()
+    sp = c.params
+    p.visc, p.delta_t, p.gamma_inv, p.channel_diameter = sp.visc, sp.delta_t, sp.gamma_inv, sp.channel_diameter
+    p.force[:] = sp.body_force
+    p.ref_rho, p.max_velocity, p.testcase = sp.ref_rho, sp.max_velocity, sp.testcase
+    p.visc_factor_initial, p.viscosity_period = sp.visc_factor_initial, sp.viscosity_period
+    p.has_rbc = 1 if c.membranes else 0
+    if c.membranes:
+        mb = c.membranes[0]
+        for k in ("volume_modulus", "local_area_modulus", "global_area_modulus", "shear_modulus",
+                  "global_bending_modulus", "local_bending_modulus", "membrane_thickness", "viscosity", "wlc_ratio",
+                  "curvature_ratio", "volume_ratio", "internal_viscosity_ratio", "reference_length"):
+            setattr(p, k, float(getattr(mb, k)))
+        p.pivkin_length, p.sphere_reference = int(mb.pivkin_length), int(mb.sphere_reference)
+    rc = R.RefCase(rm, p, m.bc_rho_type, m.bc_vel_type, m.bc_values)
+    rc.set_state(c.rho, c.u, c.v, c.w)
+    if c.membranes:
+        mb = c.membranes[0]
+        rc.set_rbc(mb.tris, mb.springs, mb.xyz_stress_free, mb.xyz_initial)
+    return rc
+
+
+def mesh_fixture(name, X, Y, Z, hybrid=False):
+    rm = R.RefMesh(X, Y, Z, 1.0, (0.0, 0.0, 0.0), 0.1, hybrid)
+    arrays = rm.arrays()
+    np.savez_compressed(os.path.join(HERE, name), X=X, Y=Y, Z=Z, hybrid=int(hybrid),
+                        counts=np.array([rm.n_cells, rm.n_faces, rm.n_interior, rm.n_bc, rm.n_face_x, rm.n_face_y,
+                                         rm.n_face_z, rm.total_cells]), **arrays)
+
+
+def spring_fixture(name, level):
+    unit, tris = icosphere(level, 1.0)
+    nodes = unit * 8.0
+    spr, tri, xyz = R.ref_springs(nodes, tris, (10.0, 20.0, 30.0))
+    np.savez_compressed(os.path.join(HERE, name), nodes=nodes, tris=tris, ref_springs=spr, ref_tris=tri, ref_xyz=xyz)
+
+
+def step_fixture(name, case, steps):
+    rc = ref_case(case)
+    out = dict(rho0=case.rho, u0=case.u, v0=case.v, w0=case.w)
+    if case.membranes:
+        mb = case.membranes[0]
+        out.update(tris=mb.tris, springs=mb.springs, xyz_stress_free=mb.xyz_stress_free, xyz_initial=mb.xyz_initial,
+                   init_totals=rc.get(R.REF_TOTALS), init_spring=rc.get(R.REF_SPRING))
+    rc.step(1)
+    out.update(s1_grad=rc.get(R.REF_GRAD), s1_flux=rc.get(R.REF_RES_FACE), s1_res=rc.get(R.REF_RES),
+               s1_force=rc.get(R.REF_FORCE), s1_ghost=rc.get(R.REF_GHOST), s1_t1=rc.get(R.REF_T1),
+               s1_state=np.stack(rc.state()), s1_resid=rc.get(R.REF_RESID))
+    if case.membranes:
+        out.update(s1_nodes_x=rc.get(R.REF_NODE_X), s1_nodes_v=rc.get(R.REF_NODE_V), s1_nodes_f=rc.get(R.REF_NODE_F),
+                   s1_totals=rc.get(R.REF_TOTALS), s1_visc=rc.get(R.REF_VISC), s1_spring=rc.get(R.REF_SPRING))
+    rc.step(steps - 1)
+    out.update(sN_state=np.stack(rc.state()), sN_resid=rc.get(R.REF_RESID), steps=steps)
+    if case.membranes:
+        out.update(sN_nodes_x=rc.get(R.REF_NODE_X), sN_nodes_f=rc.get(R.REF_NODE_F), sN_totals=rc.get(R.REF_TOTALS),
+                   sN_visc=rc.get(R.REF_VISC))
+    np.savez_compressed(os.path.join(HERE, name), **out)
+
+
+def main():
+    if not R.available():
+        sys.exit("oracle/_ref/libref_lbfs.so is missing: run oracle/build_ref.sh first")
+    mesh_fixture("mesh_4x3x5.npz", 8.0, 6.0, 10.0)
+    mesh_fixture("mesh_6x6x6_hybrid.npz", 12.0, 12.0, 12.0, hybrid=True)
+    spring_fixture("springs_L1.npz", 1)
+    spring_fixture("springs_L2.npz", 2)
+    spring_fixture("springs_L3.npz", 3)
+    step_fixture("step_poiseuille_6x5x4.npz", cases.poiseuille(n=6, ny=5, nz=4), 20)
+    step_fixture("step_shear_rbc_16.npz",
+                 cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2), 10)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,203 @@
+"""Parity of the CUDA path (called through the C ABI) with the reference and the oracle.
+
+* against the golden fixtures written by the reference itself;
+* against the C restatement oracle on seeded inputs, including the paths the
+  fixtures do not reach (general-normal faces, 4-point Peskin IBM, several
+  membranes);
+* size-independent properties at the full benchmark size (64^3 + one L3 red
+  cell): exactness of uniform states, run-to-run determinism, graph replay
+  identical to eager launches;
+* the FP32-bulk form against the FP64 path within FP32_RTOL.
+"""
+import numpy as np
+import pytest
+
+from helpers import FP32_RTOL, FP64_RTOL, rel_err
+from lbfs_b200 import GpuSolver, _abi, cases, red_cell
+from oracle_lbfs import OracleSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def make(c, cls=GpuSolver):
+    s = cls(c.mesh, c.params, c.membranes)
+    s.set_state(c.rho, c.u, c.v, c.w)
+    return s
+
+
+def fixture_case(golden, name):
+    g = golden(name)
+    if "poiseuille" in name:
+        c = cases.poiseuille(n=6, ny=5, nz=4)
+    else:
+        c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
+        mb = c.membranes[0]
+        mb.xyz_stress_free, mb.xyz_initial = g["xyz_stress_free"], g["xyz_initial"]
+    c.rho, c.u, c.v, c.w = g["rho0"], g["u0"], g["v0"], g["w0"]
+    return c, g
+
+
+@pytest.mark.parametrize("name", ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz"])
+def test_gpu_matches_reference_fixture(golden, name):
+    c, g = fixture_case(golden, name)
+    s = make(c)
+    s.keep_residuals(True)
+    if c.membranes:
+        assert rel_err(s.totals()[0], g["init_totals"]) < FP64_RTOL
+        assert rel_err(s.field(_abi.LBFS_FIELD_SPRING), g["init_spring"]) < FP64_RTOL
+    s.step(1)
+    checks = {
+        "grad": (s.field(_abi.LBFS_FIELD_GRADIENTS), g["s1_grad"]),
+        "flux": (s.field(_abi.LBFS_FIELD_FACE_FLUX), g["s1_flux"]),
+        "res": (s.field(_abi.LBFS_FIELD_RESIDUAL), g["s1_res"]),
+        "force": (s.field(_abi.LBFS_FIELD_FORCE), g["s1_force"]),
+        "ghost": (s.field(_abi.LBFS_FIELD_GHOST), g["s1_ghost"]),
+        "t1": (s.field(_abi.LBFS_FIELD_T1), g["s1_t1"]),
+        "resid": (s.residuals(), g["s1_resid"]),
+    }
+    for k, arr in enumerate(s.state()):
+        checks[f"state{k}"] = (arr, g["s1_state"][k])
+    if c.membranes:
+        checks["nodes_x"] = (s.nodes(_abi.LBFS_NODES_POSITION).ravel(), g["s1_nodes_x"])
+        checks["nodes_v"] = (s.nodes(_abi.LBFS_NODES_VELOCITY).ravel(), g["s1_nodes_v"])
+        checks["nodes_f"] = (s.nodes(_abi.LBFS_NODES_FORCE).ravel(), g["s1_nodes_f"])
+        checks["totals"] = (s.totals()[0], g["s1_totals"])
+        checks["visc"] = (s.field(_abi.LBFS_FIELD_VISC), g["s1_visc"])
+        checks["spring"] = (s.field(_abi.LBFS_FIELD_SPRING), g["s1_spring"])
+    for key, (a, b) in checks.items():
+        assert rel_err(a, b) < FP64_RTOL, (key, rel_err(a, b))
+    s.step(int(g["steps"]) - 1, graph=True)
+    for k, arr in enumerate(s.state()):
+        assert rel_err(arr, g["sN_state"][k]) < FP64_RTOL, (k, rel_err(arr, g["sN_state"][k]))
+    if c.membranes:
+        assert rel_err(s.nodes().ravel(), g["sN_nodes_x"]) < FP64_RTOL
+        assert rel_err(s.nodes(_abi.LBFS_NODES_FORCE).ravel(), g["sN_nodes_f"]) < FP64_RTOL
+        assert rel_err(s.totals()[0], g["sN_totals"]) < FP64_RTOL
+        assert rel_err(s.field(_abi.LBFS_FIELD_VISC), g["sN_visc"]) < FP64_RTOL
+    assert s.status() == 0
+    s.close()
+
+
+def compare_with_oracle(c, steps, fields=True):
+    s, o = make(c), make(c, OracleSolver)
+    s.step(1)
+    o.step(1)
+    if fields:
+        for which in (_abi.LBFS_FIELD_GRADIENTS, _abi.LBFS_FIELD_FACE_FLUX, _abi.LBFS_FIELD_FORCE,
+                      _abi.LBFS_FIELD_VISC, _abi.LBFS_FIELD_GHOST, _abi.LBFS_FIELD_T1):
+            assert rel_err(s.field(which), o.field(which)) < FP64_RTOL, which
+    s.step(steps - 1, graph=True)
+    o.step(steps - 1)
+    for k, (a, b) in enumerate(zip(s.state(), o.state())):
+        assert rel_err(a, b) < FP64_RTOL, (k, rel_err(a, b))
+    assert rel_err(s.residuals(), o.residuals()) < 1e-8
+    if c.membranes:
+        assert rel_err(s.nodes(), o.nodes()) < FP64_RTOL
+        assert rel_err(s.nodes(_abi.LBFS_NODES_FORCE), o.nodes(_abi.LBFS_NODES_FORCE)) < FP64_RTOL
+        assert rel_err(s.totals(), o.totals()) < FP64_RTOL
+    assert s.status() == 0
+    s.close()
+    o.close()
+
+
+def test_axis_faces_vs_oracle_non_cubic():
+    compare_with_oracle(cases.poiseuille(n=12, ny=8, nz=10), 25)
+
+
+def test_general_normal_faces_vs_oracle():
+    # the mesh_type 3 path (calc_face_flux with sign-switch upwinding) on the same mesh
+    c = cases.poiseuille(n=10, ny=8, nz=6)
+    desc = c.mesh.desc
+    c.mesh.desc = lambda: _set_general(desc())
+    compare_with_oracle(c, 15)
+
+
+def _set_general(d):
+    d.axis_aligned = 0
+    return d
+
+
+def test_peskin4_ibm_vs_oracle():
+    compare_with_oracle(cases.shear_rbc(n=20, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_PESKIN4), 8)
+
+
+def test_hat2_ibm_rotated_cell_vs_oracle():
+    compare_with_oracle(cases.shear_rbc(n=20, level=2, radius_cells=3.5, ibm_stencil=_abi.LBFS_IBM_HAT2,
+                                        rotate=True), 8)
+
+
+def test_two_membranes_vs_oracle():
+    c = cases.shear_rbc(n=24, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
+    first = c.membranes[0]
+    moduli = {k: getattr(first, k) for k in ("volume_modulus", "local_area_modulus", "global_area_modulus",
+                                             "shear_modulus", "global_bending_modulus", "wlc_ratio",
+                                             "internal_viscosity_ratio")}
+    X = c.mesh.X
+    c.membranes = [red_cell(2, 6.0, (0.3 * X, 0.5 * X, 0.5 * X), **moduli),
+                   red_cell(1, 5.0, (0.7 * X, 0.45 * X, 0.55 * X), **moduli)]
+    compare_with_oracle(c, 6)
+
+
+def test_uniform_states_stay_exact_at_full_size():
+    c = cases.shear_rbc(n=64)  # the benchmark size
+    c.params.body_force = (0.0, 0.0, 0.0)
+    c.mesh.set_boundaries({p: (2, 2, 1.0, 0.0, 0.0, 0.0) for p in ("left", "right", "bottom", "top", "back", "front")})
+    c.membranes = []
+    n = c.mesh.n_cells
+    for u0 in (0.0, 0.013):
+        c.rho, c.u, c.v, c.w = np.full(n, 1.0), np.full(n, u0), np.zeros(n), np.zeros(n)
+        s = make(c)
+        s.step(5, graph=True)
+        rho, u, v, w = s.state()
+        assert np.all(rho == rho[0]) and np.all(u == u[0]) and np.all(v == 0) and np.all(w == 0)
+        s.close()
+
+
+def test_full_size_deterministic_and_graph_equals_eager():
+    c = cases.shear_rbc(n=64)  # 64^3 cells, one L3 red cell, 4-point Peskin
+    a, b = make(c), make(c)
+    a.step(6)
+    b.step(6, graph=True)
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.nodes(), b.nodes())
+    assert np.array_equal(a.totals(), b.totals())
+    assert all(np.isfinite(x).all() for x in a.state())
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("builder", ["poiseuille", "shear_rbc"])
+def test_fp32_bulk_against_fp64(builder):
+    if builder == "poiseuille":
+        c64 = cases.poiseuille(n=16)
+        c32 = cases.poiseuille(n=16, precision=_abi.LBFS_FP32_BULK)
+    else:
+        c64 = cases.shear_rbc(n=24, level=2, radius_cells=4.0)
+        c32 = cases.shear_rbc(n=24, level=2, radius_cells=4.0, precision=_abi.LBFS_FP32_BULK)
+    a, b = make(c64), make(c32)
+    a.step(40, graph=True)
+    b.step(40, graph=True)
+    sa, sb = a.state(), b.state()
+    assert rel_err(sb[0] - 1.0, sa[0] - 1.0) < 1e-3  # density deviation from rho0
+    for k in (1, 2, 3):
+        assert rel_err(sb[k], sa[k]) < FP32_RTOL, (k, rel_err(sb[k], sa[k]))
+    if c64.membranes:
+        assert rel_err(b.nodes(), a.nodes()) < 1e-9
+    a.close()
+    b.close()
+
+
+def test_nonfinite_state_sets_status_flag():
+    c = cases.poiseuille(n=8)
+    c.u = c.u.copy()
+    c.u[17] = np.nan
+    s = make(c)
+    s.step(1)
+    assert s.status() & _abi.LBFS_FLAG_NONFINITE
+    c2 = cases.poiseuille(n=8)
+    s2 = make(c2)  # the device context stays usable for a new handle
+    s2.step(2)
+    assert s2.status() == 0
+    s.close()
+    s2.close()

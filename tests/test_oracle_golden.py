@@ -1,0 +1,61 @@
+"""The C restatement oracle reproduces the reference's own kernels (golden
+fixtures produced by the reference sources compiled for the host)."""
+import numpy as np
+import pytest
+
+from helpers import FP64_RTOL, rel_err
+from lbfs_b200 import _abi, cases
+from oracle_lbfs import OracleSolver
+
+
+def fixture_case(golden, name):
+    g = golden(name)
+    if "poiseuille" in name:
+        c = cases.poiseuille(n=6, ny=5, nz=4)
+    else:
+        c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
+        mb = c.membranes[0]
+        assert np.array_equal(mb.tris, g["tris"]) and np.array_equal(mb.springs, g["springs"])
+        mb.xyz_stress_free = g["xyz_stress_free"]
+        mb.xyz_initial = g["xyz_initial"]
+    c.rho, c.u, c.v, c.w = g["rho0"], g["u0"], g["v0"], g["w0"]
+    return c, g
+
+
+@pytest.mark.parametrize("name", ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz"])
+def test_oracle_matches_reference(golden, name):
+    c, g = fixture_case(golden, name)
+    o = OracleSolver(c.mesh, c.params, c.membranes)
+    o.set_state(c.rho, c.u, c.v, c.w)
+    if c.membranes:
+        assert rel_err(o.totals()[0], g["init_totals"]) < FP64_RTOL
+        assert rel_err(o.field(_abi.LBFS_FIELD_SPRING), g["init_spring"]) < FP64_RTOL
+    o.step(1)
+    checks = {
+        "grad": (o.field(_abi.LBFS_FIELD_GRADIENTS), g["s1_grad"]),
+        "flux": (o.field(_abi.LBFS_FIELD_FACE_FLUX), g["s1_flux"]),
+        "res": (o.field(_abi.LBFS_FIELD_RESIDUAL), g["s1_res"]),
+        "force": (o.field(_abi.LBFS_FIELD_FORCE), g["s1_force"]),
+        "ghost": (o.field(_abi.LBFS_FIELD_GHOST), g["s1_ghost"]),
+        "t1": (o.field(_abi.LBFS_FIELD_T1), g["s1_t1"]),
+        "resid": (o.residuals(), g["s1_resid"]),
+    }
+    for k, arr in enumerate(o.state()):
+        checks[f"state{k}"] = (arr, g["s1_state"][k])
+    if c.membranes:
+        checks["nodes_x"] = (o.nodes(_abi.LBFS_NODES_POSITION).ravel(), g["s1_nodes_x"])
+        checks["nodes_v"] = (o.nodes(_abi.LBFS_NODES_VELOCITY).ravel(), g["s1_nodes_v"])
+        checks["nodes_f"] = (o.nodes(_abi.LBFS_NODES_FORCE).ravel(), g["s1_nodes_f"])
+        checks["totals"] = (o.totals()[0], g["s1_totals"])
+        checks["visc"] = (o.field(_abi.LBFS_FIELD_VISC), g["s1_visc"])
+        checks["spring"] = (o.field(_abi.LBFS_FIELD_SPRING), g["s1_spring"])
+    for key, (a, b) in checks.items():
+        assert rel_err(a, b) < FP64_RTOL, (key, rel_err(a, b))
+    o.step(int(g["steps"]) - 1)
+    for k, arr in enumerate(o.state()):
+        assert rel_err(arr, g["sN_state"][k]) < FP64_RTOL, (k, rel_err(arr, g["sN_state"][k]))
+    if c.membranes:
+        assert rel_err(o.nodes(_abi.LBFS_NODES_POSITION).ravel(), g["sN_nodes_x"]) < FP64_RTOL
+        assert rel_err(o.nodes(_abi.LBFS_NODES_FORCE).ravel(), g["sN_nodes_f"]) < FP64_RTOL
+        assert rel_err(o.totals()[0], g["sN_totals"]) < FP64_RTOL
+        assert rel_err(o.field(_abi.LBFS_FIELD_VISC), g["sN_visc"]) < FP64_RTOL
