@@ -52,10 +52,13 @@ struct MembraneArgs {
     double *patch_force;         // [n_membranes * kMaxPatchCells * 3]
     unsigned int *flags;
     int sort_capacity;           // power of two >= nodes of the largest membrane
+    int total_nodes, total_springs;
+    const int *spring_mem;       // [total_springs] membrane of each spring
 };
 
 void membrane_prepare(int sort_capacity);
-void launch_membrane(const MembraneArgs &a, cudaStream_t s);
+// Enqueues the membrane kernels of the current mode; returns the launch count.
+int launch_membrane(const MembraneArgs &a, cudaStream_t s);
 
 struct ViscArgs {
     int nc, n_membranes;

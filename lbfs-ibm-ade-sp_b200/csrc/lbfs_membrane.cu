@@ -1,4 +1,10 @@
-// Membrane side of one time step, one CTA (512 threads) per membrane:
+// Membrane side of one time step, five kernels:
+//
+//   M1 k_mem_advect  (one warp per node)      P0
+//   M2 k_mem_totals  (one CTA per membrane)   P1
+//   M3 k_mem_springs (one thread per spring)  P2
+//   M4 k_mem_gather  (one CTA per membrane)   P3, P4, P5
+//   M5 k_mem_spread  (one thread per patch cell of each membrane)  P6
 //
 //   P0  IBM velocity interpolation at the nodes + explicit node advection
 //       (interpolate_velocities_on_nodes, immersed_boundary_method.cu:14-97;
@@ -341,86 +347,101 @@ __device__ void spring_reference(const MembraneArgs &A, const MembraneConst &mc,
     A.area0[2 * s + 1] = norm_2;
 }
 
+// ---- M1: IBM interpolation + advection, one warp per node ----------------
 template <typename R>
-__device__ void interpolate_and_advect(const MembraneArgs &A, const MembraneConst &mc) {
-    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
-        const int n = mc.node0 + ln;
-        const double x = A.x[n], y = A.y[n], z = A.z[n];
-        const Stencil st = node_stencil(A, x, y, z);
-        const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
-        double vx = 0.0, vy = 0.0, vz = 0.0;
-        for (int i = st.i0; i < st.i0 + S; i++)
-            for (int j = st.j0; j < st.j0 + S; j++)
-                for (int k = st.k0; k < st.k0 + S; k++) {
-                    const int idx = i + j * A.grid_nx + k * A.grid_ny * A.grid_nx;
-                    if (idx < A.nc && idx >= 0) {
-                        const double wx = stencil_weight(A.ibm_stencil, i + 0.5 - st.rx);
-                        const double wy = stencil_weight(A.ibm_stencil, j + 0.5 - st.ry);
-                        const double wz = stencil_weight(A.ibm_stencil, k + 0.5 - st.rz);
-                        double u, v, w;
-                        read_velocity<R>(A.state, idx, u, v, w);
-                        vx += u * wx * wy * wz;
-                        vy += v * wx * wy * wz;
-                        vz += w * wx * wy * wz;
-                    }
-                }
-        A.vx[n] = vx;
-        A.vy[n] = vy;
-        A.vz[n] = vz;
-        A.x[n] = x + vx * A.delta_t;
-        A.y[n] = y + vy * A.delta_t;
-        A.z[n] = z + vz * A.delta_t;
+__global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
+    const int lane = threadIdx.x & 31;
+    const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (n >= A.total_nodes) return;
+    const double x = A.x[n], y = A.y[n], z = A.z[n];
+    const Stencil st = node_stencil(A, x, y, z);
+    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+    const int cells = S * S * S;
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int c = lane; c < cells; c += 32) {
+        // cell c of the stencil, z fastest as in the reference's i, j, k loop nest
+        const int i = st.i0 + c / (S * S), j = st.j0 + (c / S) % S, k = st.k0 + c % S;
+        const int idx = i + j * A.grid_nx + k * A.grid_ny * A.grid_nx;
+        if (idx < A.nc && idx >= 0) {
+            const double wx = stencil_weight(A.ibm_stencil, i + 0.5 - st.rx);
+            const double wy = stencil_weight(A.ibm_stencil, j + 0.5 - st.ry);
+            const double wz = stencil_weight(A.ibm_stencil, k + 0.5 - st.rz);
+            double u, vv, w;
+            read_velocity<R>(A.state, idx, u, vv, w);
+            v[0] += u * wx * wy * wz;
+            v[1] += vv * wx * wy * wz;
+            v[2] += w * wx * wy * wz;
+        }
     }
-    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+        for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+    if (lane == 0) {
+        A.vx[n] = v[0];
+        A.vy[n] = v[1];
+        A.vz[n] = v[2];
+        A.x[n] = x + v[0] * A.delta_t;
+        A.y[n] = y + v[1] * A.delta_t;
+        A.z[n] = z + v[2] * A.delta_t;
+    }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(kMembraneThreads) k_membrane(MembraneArgs A) {
-    extern __shared__ unsigned long long skeys[];
+// ---- M2: membrane totals V, A, one CTA per membrane ---------------------------
+__global__ void __launch_bounds__(256) k_mem_totals(MembraneArgs A) {
     __shared__ double sh[33];
-    __shared__ int shi[33];
-    const int m = blockIdx.x;
-    const MembraneConst mc = A.mc[m];
-    MembraneScalars *ms = A.ms + m;
-
-    if (A.mode == kModeReference) {
-        for (int ls = threadIdx.x; ls < mc.n_springs; ls += blockDim.x) spring_reference(A, mc, mc.spring0 + ls);
-        return;
-    }
-    const bool initials = (A.mode == kModeInitial);
-    if (A.mode == kModeStep) {
-        if (A.state_is_float) interpolate_and_advect<float>(A, mc);
-        else interpolate_and_advect<double>(A, mc);
-    }
-    // P1: triangle totals
+    const MembraneConst mc = A.mc[blockIdx.x];
+    MembraneScalars *ms = A.ms + blockIdx.x;
     double pv = 0.0, pa = 0.0;
     for (int lt = threadIdx.x; lt < mc.n_tris; lt += blockDim.x) {
         const int t = mc.tri0 + lt;
         const int na = A.tri[3 * t], nb = A.tri[3 * t + 1], nc = A.tri[3 * t + 2];
         const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]), c = d3(A.x[nc], A.y[nc], A.z[nc]);
         const D3 normal = cross(b - a, c - a);
-        const double area = sqrt(dot(normal, normal)) * 0.5;
-        const D3 centroid = tri_centroid(a, b, c);
-        pv += dot(normal, centroid) / 6;
-        pa += area;
+        pv += dot(normal, tri_centroid(a, b, c)) / 6;
+        pa += sqrt(dot(normal, normal)) * 0.5;
     }
-    const double V = block_sum(pv, sh);
-    const double Ar = block_sum(pa, sh);
-    double V0 = ms->V0, A0 = ms->A0;
-    if (initials) {
-        V0 = V * mc.volume_ratio;
-        A0 = Ar;
+    const double V = block_sum(pv, sh), Ar = block_sum(pa, sh);
+    if (threadIdx.x == 0) {
+        ms->V = V;
+        ms->A = Ar;
+        if (A.mode == kModeInitial) {
+            ms->V0 = V * mc.volume_ratio;
+            ms->A0 = Ar;
+            ms->MAD = 0.0;
+            ms->MAD0 = 0.0;
+        }
     }
-    // P2: springs
+}
+
+// ---- M3: per-spring forces (or the stress-free reference pass), grid over springs
+__global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= A.total_springs) return;
+    const int m = A.spring_mem[s];
+    const MembraneConst mc = A.mc[m];
+    if (A.mode == kModeReference) {
+        spring_reference(A, mc, s);
+        return;
+    }
+    const MembraneScalars ms = A.ms[m];
     const double wr = mc.wlc_ratio;
     const double sfc = (0.25 * wr * wr / ((wr - 1.0) * (wr - 1.0)) - 0.25 + 1.0 / wr);
-    const double vol_coef = -1 * mc.volume_modulus * (V / V0 - 1.0) / 6.0;
-    const double area_coef = -1 * mc.global_area_modulus * (Ar / A0 - 1.0);
-    const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (ms->MAD - ms->MAD0) / A0;
-    for (int ls = threadIdx.x; ls < mc.n_springs; ls += blockDim.x)
-        spring_forces(A, mc, *ms, mc.spring0 + ls, initials, sfc, vol_coef, area_coef, mad_coef);
-    __syncthreads();
-    // P4: MAD over the first n_nodes springs of this membrane
+    const double vol_coef = -1 * mc.volume_modulus * (ms.V / ms.V0 - 1.0) / 6.0;
+    const double area_coef = -1 * mc.global_area_modulus * (ms.A / ms.A0 - 1.0);
+    const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (ms.MAD - ms.MAD0) / ms.A0;
+    spring_forces(A, mc, ms, s, A.mode == kModeInitial, sfc, vol_coef, area_coef, mad_coef);
+}
+
+// ---- M4: node forces, MAD, node bounds, nodes sorted by stencil base cell ----
+__global__ void __launch_bounds__(kMembraneThreads) k_mem_gather(MembraneArgs A) {
+    extern __shared__ unsigned long long skeys[];
+    __shared__ double sh[33];
+    __shared__ int shi[33];
+    const int m = blockIdx.x;
+    const MembraneConst mc = A.mc[m];
+    MembraneScalars *ms = A.ms + m;
+    const double Ar = ms->A;
+    // MAD over the first n_nodes springs of this membrane
     double pm = 0.0;
     const int n_mad = mc.n_nodes < mc.n_springs ? mc.n_nodes : mc.n_springs;
     for (int ls = threadIdx.x; ls < n_mad; ls += blockDim.x) {
@@ -429,12 +450,11 @@ __global__ void __launch_bounds__(kMembraneThreads) k_membrane(MembraneArgs A) {
     }
     const double MAD = block_sum(pm, sh) / Ar;
     if (threadIdx.x == 0) {
-        ms->V = V; ms->A = Ar; ms->MAD = MAD;
-        if (initials) { ms->V0 = V0; ms->A0 = A0; ms->MAD0 = MAD; }
+        ms->MAD = MAD;
+        if (A.mode == kModeInitial) ms->MAD0 = MAD;
     }
     if (A.mode != kModeStep) return;
-
-    // P3: node forces in spring order; node bounds for the interior-viscosity test
+    // node forces in spring order and node bounds
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
         const int n = mc.node0 + ln;
@@ -452,17 +472,15 @@ __global__ void __launch_bounds__(kMembraneThreads) k_membrane(MembraneArgs A) {
         const double l = block_minmax(lo[c], sh, true), h = block_minmax(hi[c], sh, false);
         if (threadIdx.x == 0) { ms->bbox_lo[c] = l; ms->bbox_hi[c] = h; }
     }
-    __syncthreads();  // node forces visible to the whole block
-
-    // P5: sort nodes by the cell at the base of their stencil
+    // stencil base cells: bounds of the patch, then the (bin, node) sort
     const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
     int blo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, bhi_neg[3] = {INT32_MAX, INT32_MAX, INT32_MAX};
     unsigned int range_flag = 0;
+    const int gn[3] = {A.grid_nx, A.grid_ny, A.grid_nz};
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
         const int n = mc.node0 + ln;
         const Stencil st = node_stencil(A, A.x[n], A.y[n], A.z[n]);
         const int b[3] = {st.i0, st.j0, st.k0};
-        const int gn[3] = {A.grid_nx, A.grid_ny, A.grid_nz};
         for (int c = 0; c < 3; c++) {
             blo[c] = min(blo[c], b[c]);
             bhi_neg[c] = min(bhi_neg[c], -b[c]);
@@ -511,43 +529,55 @@ __global__ void __launch_bounds__(kMembraneThreads) k_membrane(MembraneArgs A) {
             __syncthreads();
         }
     }
-    // P6: per patch cell, sum the contributions of the nodes of the bins whose
-    // stencils cover it, bins in (z, y, x) order and nodes in node order.
+    for (int t = threadIdx.x; t < mc.n_nodes; t += blockDim.x) A.keys[mc.node0 + t] = skeys[t];
+}
+
+// ---- M5: spread as a per-cell segmented reduction over the sorted nodes ------
+// Each patch cell sums, bins in (z, y, x) order and nodes in node order, the
+// contributions of the nodes whose stencil covers it.
+__global__ void __launch_bounds__(128) k_mem_spread(MembraneArgs A) {
+    const int m = blockIdx.y;
+    const MembraneScalars ms = A.ms[m];
+    const int pc = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pc >= ms.patch_cells) return;
+    const MembraneConst mc = A.mc[m];
+    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+    const int pdim[3] = {ms.patch_dim[0], ms.patch_dim[1], ms.patch_dim[2]};
+    const int bdim[3] = {pdim[0] - S + 1, pdim[1] - S + 1, pdim[2] - S + 1};
+    const int px = pc % pdim[0], py = (pc / pdim[0]) % pdim[1], pz = pc / (pdim[0] * pdim[1]);
+    const int ci = ms.patch_lo[0] + px, cj = ms.patch_lo[1] + py, ck = ms.patch_lo[2] + pz;
+    const unsigned long long *keys = A.keys + mc.node0;
     const double inv3 = 1 / A.delta_x / A.delta_x / A.delta_x;
-    double *pf = A.patch_force + (size_t)m * kMaxPatchCells * 3;
-    for (int pc = threadIdx.x; pc < (int)pcells; pc += blockDim.x) {
-        const int px = pc % pdim[0], py = (pc / pdim[0]) % pdim[1], pz = pc / (pdim[0] * pdim[1]);
-        const int ci = plo[0] + px, cj = plo[1] + py, ck = plo[2] + pz;
-        double f[3] = {0.0, 0.0, 0.0};
-        const int bx0 = max(px - S + 1, 0), bx1 = min(px, bdim[0] - 1);
-        const int by0 = max(py - S + 1, 0), by1 = min(py, bdim[1] - 1);
-        const int bz0 = max(pz - S + 1, 0), bz1 = min(pz, bdim[2] - 1);
-        for (int bz = bz0; bz <= bz1; bz++)
-            for (int by = by0; by <= by1; by++) {
-                if (bx0 > bx1) continue;
-                const unsigned long long klo = (unsigned long long)(bx0 + bdim[0] * (by + bdim[1] * bz));
-                const unsigned long long khi = (unsigned long long)(bx1 + bdim[0] * (by + bdim[1] * bz));
-                int lo_i = 0, hi_i = mc.n_nodes;  // first sorted entry with bin >= klo
-                while (lo_i < hi_i) {
-                    const int mid = (lo_i + hi_i) >> 1;
-                    if ((skeys[mid] >> 32) < klo) lo_i = mid + 1;
-                    else hi_i = mid;
-                }
-                for (int e = lo_i; e < mc.n_nodes && (skeys[e] >> 32) <= khi; e++) {
-                    const int n = mc.node0 + (int)(skeys[e] & 0xffffffffu);
-                    const Stencil st = node_stencil(A, A.x[n], A.y[n], A.z[n]);
-                    const double wx = stencil_weight(A.ibm_stencil, ci + 0.5 - st.rx);
-                    const double wy = stencil_weight(A.ibm_stencil, cj + 0.5 - st.ry);
-                    const double wz = stencil_weight(A.ibm_stencil, ck + 0.5 - st.rz);
-                    f[0] += A.fx[n] * wx * wy * wz * inv3;
-                    f[1] += A.fy[n] * wx * wy * wz * inv3;
-                    f[2] += A.fz[n] * wx * wy * wz * inv3;
-                }
+    double f[3] = {0.0, 0.0, 0.0};
+    const int bx0 = max(px - S + 1, 0), bx1 = min(px, bdim[0] - 1);
+    const int by0 = max(py - S + 1, 0), by1 = min(py, bdim[1] - 1);
+    const int bz0 = max(pz - S + 1, 0), bz1 = min(pz, bdim[2] - 1);
+    for (int bz = bz0; bz <= bz1; bz++)
+        for (int by = by0; by <= by1; by++) {
+            if (bx0 > bx1) continue;
+            const unsigned long long klo = (unsigned long long)(bx0 + bdim[0] * (by + bdim[1] * bz));
+            const unsigned long long khi = (unsigned long long)(bx1 + bdim[0] * (by + bdim[1] * bz));
+            int lo_i = 0, hi_i = mc.n_nodes;  // first sorted entry with bin >= klo
+            while (lo_i < hi_i) {
+                const int mid = (lo_i + hi_i) >> 1;
+                if ((keys[mid] >> 32) < klo) lo_i = mid + 1;
+                else hi_i = mid;
             }
-        pf[3 * (size_t)pc] = f[0];
-        pf[3 * (size_t)pc + 1] = f[1];
-        pf[3 * (size_t)pc + 2] = f[2];
-    }
+            for (int e = lo_i; e < mc.n_nodes && (keys[e] >> 32) <= khi; e++) {
+                const int n = mc.node0 + (int)(keys[e] & 0xffffffffu);
+                const Stencil st = node_stencil(A, A.x[n], A.y[n], A.z[n]);
+                const double wx = stencil_weight(A.ibm_stencil, ci + 0.5 - st.rx);
+                const double wy = stencil_weight(A.ibm_stencil, cj + 0.5 - st.ry);
+                const double wz = stencil_weight(A.ibm_stencil, ck + 0.5 - st.rz);
+                f[0] += A.fx[n] * wx * wy * wz * inv3;
+                f[1] += A.fy[n] * wx * wy * wz * inv3;
+                f[2] += A.fz[n] * wx * wy * wz * inv3;
+            }
+        }
+    double *pf = A.patch_force + ((size_t)m * kMaxPatchCells + pc) * 3;
+    pf[0] = f[0];
+    pf[1] = f[1];
+    pf[2] = f[2];
 }
 
 // ---- interior viscosity (update_interior_viscosities_plucker, immersed_boundary_method.cu:389-527) ----
@@ -600,18 +630,33 @@ __global__ void k_interior_viscosity(ViscArgs a) {
 
 void membrane_prepare(int sort_capacity) {
     const size_t smem = (size_t)(sort_capacity > 0 ? sort_capacity : 1) * sizeof(unsigned long long);
-    cudaFuncSetAttribute(k_membrane<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_membrane<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_mem_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-void launch_membrane(const MembraneArgs &a, cudaStream_t s) {
-    // dynamic shared memory: one 64-bit sort key per node of the largest
-    // membrane, padded to a power of two
+int launch_membrane(const MembraneArgs &a, cudaStream_t s) {
     const size_t smem = (size_t)(a.sort_capacity > 0 ? a.sort_capacity : 1) * sizeof(unsigned long long);
-    if (a.state_is_float)
-        k_membrane<float><<<a.n_membranes, kMembraneThreads, smem, s>>>(a);
-    else
-        k_membrane<double><<<a.n_membranes, kMembraneThreads, smem, s>>>(a);
+    const int spring_blocks = (a.total_springs + 127) / 128;
+    if (a.mode == kModeReference) {
+        k_mem_springs<<<spring_blocks, 128, 0, s>>>(a);
+        return 1;
+    }
+    int n = 0;
+    if (a.mode == kModeStep) {
+        const int blocks = (a.total_nodes * 32 + 255) / 256;
+        if (a.state_is_float) k_mem_advect<float><<<blocks, 256, 0, s>>>(a);
+        else k_mem_advect<double><<<blocks, 256, 0, s>>>(a);
+        n++;
+    }
+    k_mem_totals<<<a.n_membranes, 256, 0, s>>>(a);
+    k_mem_springs<<<spring_blocks, 128, 0, s>>>(a);
+    k_mem_gather<<<a.n_membranes, kMembraneThreads, smem, s>>>(a);
+    n += 3;
+    if (a.mode == kModeStep) {
+        dim3 grid((kMaxPatchCells + 127) / 128, a.n_membranes);
+        k_mem_spread<<<grid, 128, 0, s>>>(a);
+        n++;
+    }
+    return n;
 }
 
 void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s) {

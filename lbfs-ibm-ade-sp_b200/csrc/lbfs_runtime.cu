@@ -68,6 +68,7 @@ struct lbfs_solver {
     bool profiling = false;
     cudaEvent_t ev_phase[kPhases][2] = {};
     bool phase_recorded[kPhases] = {};
+    bool graph_phase_recorded[kPhases] = {};  // phases recorded by one replay of the graph
     // staging buffer for host <-> device state transfers: rho, u, v, w planes
     double *d_stage = nullptr;
 
@@ -328,7 +329,12 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     std::vector<MembraneScalars> msz(n_rbc);
     std::memset(msz.data(), 0, sizeof(MembraneScalars) * n_rbc);
     int rc = 0;
-    MembraneConst *d_mc; MembraneScalars *d_ms; int *d_tri, *d_spr, *d_inc, *d_incs;
+    std::vector<int> spring_mem(S);
+    for (int r = 0; r < n_rbc; r++)
+        for (int q = 0; q < mc[r].n_springs; q++) spring_mem[mc[r].spring0 + q] = r;
+    ma.total_nodes = N;
+    ma.total_springs = S;
+    MembraneConst *d_mc; MembraneScalars *d_ms; int *d_tri, *d_spr, *d_inc, *d_incs, *d_smem;
     if ((rc = s->upload(&d_mc, mc)) || (rc = s->upload(&d_ms, msz)) || (rc = s->upload(&d_tri, tri)) ||
         (rc = s->upload(&d_spr, spr)) || (rc = s->upload(&d_inc, inc)) || (rc = s->upload(&d_incs, inc_start)) ||
         (rc = s->upload(&ma.x, x)) || (rc = s->upload(&ma.y, y)) || (rc = s->upload(&ma.z, z)) ||
@@ -338,8 +344,10 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         (rc = s->upload(&ma.curv, zeros_s)) || (rc = s->upload(&ma.curv0, zeros_s)) ||
         (rc = s->upload(&ma.angle0, zeros_s)) || (rc = s->upload(&ma.area0, zeros_2s)) ||
         (rc = s->upload(&ma.area, zeros_2s)) || (rc = s->alloc(&ma.contrib, 12 * (size_t)S)) ||
-        (rc = s->alloc(&ma.keys, N)) || (rc = s->alloc(&ma.patch_force, (size_t)n_rbc * kMaxPatchCells * 3)))
+        (rc = s->alloc(&ma.keys, N)) || (rc = s->alloc(&ma.patch_force, (size_t)n_rbc * kMaxPatchCells * 3)) ||
+        (rc = s->upload(&d_smem, spring_mem)))
         return rc;
+    ma.spring_mem = d_smem;
     ma.mc = d_mc; ma.ms = d_ms; ma.tri = d_tri; ma.spring = d_spr; ma.inc = d_inc; ma.inc_start = d_incs;
     ma.flags = s->fp32 ? s->f32.flags : s->f64.flags;
     ma.state = s->fp32 ? (const void *)s->f32.state : (const void *)s->f64.state;
@@ -369,16 +377,25 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     return LBFS_OK;
 }
 
+// Records `ev` on `st`; inside stream capture as an external event node (so the
+// graph replay records it), outside capture as a plain record.
+cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) return cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal);
+    return cudaEventRecord(ev, st);
+}
+
 struct PhaseMark {
     lbfs_solver *s;
     int phase;
     cudaStream_t st;
     PhaseMark(lbfs_solver *s_, int ph, cudaStream_t st_) : s(s_), phase(ph), st(st_) {
-        if (s->profiling) cudaEventRecord(s->ev_phase[phase][0], st);
+        if (s->profiling) record_event(s->ev_phase[phase][0], st);
     }
     ~PhaseMark() {
         if (s->profiling) {
-            cudaEventRecord(s->ev_phase[phase][1], st);
+            record_event(s->ev_phase[phase][1], st);
             s->phase_recorded[phase] = true;
         }
     }
@@ -387,23 +404,24 @@ struct PhaseMark {
 template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *launches) {
     FluidArgs<R> &a = fluid<R>(s);
     int n = 0;
-    if (s->profiling) LBFS_CUDA(cudaEventRecord(s->ev_phase[5][0], s->stream));
+    for (int p = 0; p < kPhases; p++) s->phase_recorded[p] = false;
+    if (s->profiling) LBFS_CUDA(record_event(s->ev_phase[5][0], s->stream));
     if (s->n_membranes > 0) {
         if (visc_update) {
-            { PhaseMark m(s, 0, s->stream); launch_membrane(s->ma, s->stream); }
+            { PhaseMark m(s, 0, s->stream); n += launch_membrane(s->ma, s->stream); }
             { PhaseMark m(s, 4, s->stream); launch_interior_viscosity(s->va, s->stream); }
             { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
             { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
-            n += 4;
+            n += 3;
         } else {
             LBFS_CUDA(cudaEventRecord(s->ev_fork, s->stream));
             LBFS_CUDA(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
-            { PhaseMark m(s, 0, s->stream2); launch_membrane(s->ma, s->stream2); }
+            { PhaseMark m(s, 0, s->stream2); n += launch_membrane(s->ma, s->stream2); }
             LBFS_CUDA(cudaEventRecord(s->ev_join, s->stream2));
             { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
             { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
             LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
-            n += 3;
+            n += 2;
         }
     } else {
         { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
@@ -413,7 +431,7 @@ template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *la
     { PhaseMark m(s, 3, s->stream); launch_fluid_update<R>(a, s->stream); }
     n += 1;
     if (s->profiling) {
-        LBFS_CUDA(cudaEventRecord(s->ev_phase[5][1], s->stream));
+        LBFS_CUDA(record_event(s->ev_phase[5][1], s->stream));
         s->phase_recorded[5] = true;
     }
     LBFS_CUDA(cudaGetLastError());
@@ -479,7 +497,7 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if ((rc = s->upload(&s->d_centroid, centroid))) return fail(rc);
     rc = setup_membranes(s, mesh, rbc, n_rbc);
     if (rc) return fail(rc);
-    s->launches_per_step = n_rbc > 0 ? 4 : 3;
+    s->launches_per_step = n_rbc > 0 ? 3 + 5 : 3;  // fluid kernels + membrane kernels
     *out = s;
     return LBFS_OK;
 }
@@ -599,6 +617,7 @@ extern "C" int lbfs_step_graph(lbfs_solver *s, int32_t n_steps) {
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
         s->graph_steps = 1;
+        for (int p = 0; p < kPhases; p++) s->graph_phase_recorded[p] = s->phase_recorded[p];
     }
     for (int k = 0; k < n_steps; k++) {
         if (visc_due(s, s->t)) {
@@ -606,6 +625,7 @@ extern "C" int lbfs_step_graph(lbfs_solver *s, int32_t n_steps) {
             if (rc) return rc;
         } else {
             LBFS_CUDA(cudaGraphLaunch(s->graph, s->stream));
+            for (int p = 0; p < kPhases; p++) s->phase_recorded[p] = s->graph_phase_recorded[p];
         }
         s->t++;
     }
