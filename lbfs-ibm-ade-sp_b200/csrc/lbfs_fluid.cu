@@ -324,21 +324,27 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
     return interface_flux<R>(fl, a.rho0, tau, a.gamma_inv, geo.area, -1, geo.nx, geo.ny, geo.nz);
 }
 
+// Interior faces of an axis-aligned mesh: faces [0, nfx) x, [nfx, nfx+nfy) y,
+// the rest z; warps never mix axes except at the two range boundaries.
 template <typename R>
-__global__ void __launch_bounds__(128) k_face_flux(FluidArgs<R> a) {
+__global__ void __launch_bounds__(128, 4) k_face_flux(FluidArgs<R> a) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= a.nf) return;
+    if (f >= a.ni) return;
     Vec4<R> out;
-    if (f >= a.ni) {
-        out = general_face_flux<R>(a, f, true);
-    } else if (a.axis_aligned) {
-        if (f < a.nfx) out = axis_face_flux<R, 0>(a, f);
-        else if (f < a.nfx + a.nfy) out = axis_face_flux<R, 1>(a, f);
-        else out = axis_face_flux<R, 2>(a, f);
-    } else {
-        out = general_face_flux<R>(a, f, false);
-    }
+    if (f < a.nfx) out = axis_face_flux<R, 0>(a, f);
+    else if (f < a.nfx + a.nfy) out = axis_face_flux<R, 1>(a, f);
+    else out = axis_face_flux<R, 2>(a, f);
     a.flux[f] = out;
+}
+
+// Boundary faces (always) and the interior faces of meshes that are not axis
+// aligned: the general-normal reconstruction.  `first` is ni (axis-aligned
+// meshes) or 0.
+template <typename R>
+__global__ void __launch_bounds__(128) k_face_flux_general(FluidArgs<R> a, int first) {
+    const int f = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= a.nf) return;
+    a.flux[f] = general_face_flux<R>(a, f, f >= a.ni);
 }
 
 // ------------------------------------------------------------------ K3 ----
@@ -423,13 +429,29 @@ __global__ void __launch_bounds__(256) k_cell_update(FluidArgs<R> a) {
         last_block = (prev == gridDim.x - 1);
     }
     __syncthreads();
-    if (last_block && threadIdx.x < 4) {
+    if (last_block) {
+        // Final sum of the block partials by the whole last block: thread t
+        // adds partials t, t + blockDim, ... (fixed assignment), then the same
+        // warp/block tree as above.  Deterministic for a fixed grid.
         __threadfence();
-        const int m = threadIdx.x;
-        double v = 0;
-        for (int b = 0; b < (int)gridDim.x; b++) v += ((volatile double *)a.partials)[4 * b + m];
-        a.residual_sums[m] = v;
-        if (m == 0) *a.ticket = 0u;
+        double acc[4] = {0, 0, 0, 0};
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+#pragma unroll
+            for (int m = 0; m < 4; m++) acc[m] += __ldcg(a.partials + 4 * b + m);
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            double v = acc[m];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) sh[m][warp] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 4) {
+            double v = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sh[threadIdx.x][w];
+            a.residual_sums[threadIdx.x] = v;
+        }
+        if (threadIdx.x == 0) *a.ticket = 0u;
     }
 }
 
@@ -470,7 +492,9 @@ template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStr
     k_cell_gradients<R><<<(a.nc + 255) / 256, 256, 0, s>>>(a);
 }
 template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s) {
-    k_face_flux<R><<<(a.nf + 127) / 128, 128, 0, s>>>(a);
+    const int first = a.axis_aligned ? a.ni : 0;
+    if (a.axis_aligned && a.ni > 0) k_face_flux<R><<<(a.ni + 127) / 128, 128, 0, s>>>(a);
+    if (a.nf > first) k_face_flux_general<R><<<(a.nf - first + 127) / 128, 128, 0, s>>>(a, first);
 }
 template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s) {
     k_cell_update<R><<<k3_grid(a), 256, 0, s>>>(a);

@@ -25,6 +25,13 @@ enum MembraneMode : int {
     kModeStep = 2,       // one time step: interpolate, advect, forces, spread
 };
 
+// A node as the spread reads it: force, 1D stencil weights per axis, first stencil cell.
+struct SpreadRec {
+    double f[3];
+    double w[12];
+    int b[4];
+};
+
 struct MembraneArgs {
     int n_membranes;
     int mode;
@@ -54,6 +61,10 @@ struct MembraneArgs {
     int sort_capacity;           // power of two >= nodes of the largest membrane
     int total_nodes, total_springs;
     const int *spring_mem;       // [total_springs] membrane of each spring
+    int *node_base;              // [3*total_nodes] first stencil cell per axis (scratch)
+    double *node_w;              // [12*total_nodes] 1D stencil weights per axis (scratch)
+    int *bin_start;              // [n_membranes * (kMaxPatchCells + 1)] first sorted node of each bin (scratch)
+    SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order: force, weights, stencil base (scratch)
 };
 
 void membrane_prepare(int sort_capacity);

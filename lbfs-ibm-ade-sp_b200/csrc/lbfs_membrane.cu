@@ -433,10 +433,14 @@ __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
 }
 
 // ---- M4: node forces, MAD, node bounds, nodes sorted by stencil base cell ----
+// Also writes, for the spread, each node's stencil (first cell and 1D weights)
+// and, for every bin (stencil base cell) of the patch, the range of its nodes
+// in the sorted order.
 __global__ void __launch_bounds__(kMembraneThreads) k_mem_gather(MembraneArgs A) {
     extern __shared__ unsigned long long skeys[];
     __shared__ double sh[33];
-    __shared__ int shi[33];
+    __shared__ double shv[kMembraneThreads / 32][12];
+    __shared__ double red[12];
     const int m = blockIdx.x;
     const MembraneConst mc = A.mc[m];
     MembraneScalars *ms = A.ms + m;
@@ -454,64 +458,94 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_gather(MembraneArgs A)
         if (A.mode == kModeInitial) ms->MAD0 = MAD;
     }
     if (A.mode != kModeStep) return;
-    // node forces in spring order and node bounds
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+    const int gn[3] = {A.grid_nx, A.grid_ny, A.grid_nz};
+    // node forces in spring order, node bounds, stencil bases and weights
+    double v[12];
+    for (int c = 0; c < 3; c++) { v[c] = 1e300; v[3 + c] = 1e300; v[6 + c] = 1e300; v[9 + c] = 1e300; }
+    unsigned int range_flag = 0;
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
         const int n = mc.node0 + ln;
         double f[3] = {0.0, 0.0, 0.0};
-        for (int e = A.inc_start[n]; e < A.inc_start[n + 1]; e++) {
-            const int code = A.inc[e];
-            const double *o = A.contrib + 12 * (size_t)(code >> 2) + 3 * (code & 3);
-            f[0] += o[0]; f[1] += o[1]; f[2] += o[2];
+        // contributions in spring order; the indices of a chunk are loaded
+        // before its data so the loads of a node overlap
+        const int e0 = A.inc_start[n], e1 = A.inc_start[n + 1];
+        for (int c0 = e0; c0 < e1; c0 += 8) {
+            int code[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) code[q] = (c0 + q < e1) ? __ldg(A.inc + c0 + q) : -1;
+            double d[8][3];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (code[q] >= 0) {
+                    const double *o = A.contrib + 12 * (size_t)(code[q] >> 2) + 3 * (code[q] & 3);
+                    d[q][0] = o[0]; d[q][1] = o[1]; d[q][2] = o[2];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (code[q] >= 0) { f[0] += d[q][0]; f[1] += d[q][1]; f[2] += d[q][2]; }
         }
         A.fx[n] = f[0]; A.fy[n] = f[1]; A.fz[n] = f[2];
         const double p[3] = {A.x[n], A.y[n], A.z[n]};
-        for (int c = 0; c < 3; c++) { lo[c] = fmin(lo[c], p[c]); hi[c] = fmax(hi[c], p[c]); }
-    }
-    for (int c = 0; c < 3; c++) {
-        const double l = block_minmax(lo[c], sh, true), h = block_minmax(hi[c], sh, false);
-        if (threadIdx.x == 0) { ms->bbox_lo[c] = l; ms->bbox_hi[c] = h; }
-    }
-    // stencil base cells: bounds of the patch, then the (bin, node) sort
-    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
-    int blo[3] = {INT32_MAX, INT32_MAX, INT32_MAX}, bhi_neg[3] = {INT32_MAX, INT32_MAX, INT32_MAX};
-    unsigned int range_flag = 0;
-    const int gn[3] = {A.grid_nx, A.grid_ny, A.grid_nz};
-    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
-        const int n = mc.node0 + ln;
-        const Stencil st = node_stencil(A, A.x[n], A.y[n], A.z[n]);
+        const Stencil st = node_stencil(A, p[0], p[1], p[2]);
         const int b[3] = {st.i0, st.j0, st.k0};
+        const double r[3] = {st.rx, st.ry, st.rz};
+        double *w = A.node_w + 12 * (size_t)n;
         for (int c = 0; c < 3; c++) {
-            blo[c] = min(blo[c], b[c]);
-            bhi_neg[c] = min(bhi_neg[c], -b[c]);
+            v[c] = fmin(v[c], p[c]);            // lower bound
+            v[3 + c] = fmin(v[3 + c], -p[c]);   // minus upper bound
+            v[6 + c] = fmin(v[6 + c], (double)b[c]);
+            v[9 + c] = fmin(v[9 + c], -(double)b[c]);
             if (b[c] < 0 || b[c] + S > gn[c]) range_flag = LBFS_FLAG_IBM_RANGE;
+            for (int q = 0; q < S; q++) w[4 * c + q] = stencil_weight(A.ibm_stencil, b[c] + q + 0.5 - r[c]);
+            A.node_base[3 * (size_t)n + c] = b[c];
         }
     }
+    // one block reduction of the 12 minima
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 12; q++) {
+        double x = v[q];
+        for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_down_sync(0xffffffffu, x, o));
+        if (lane == 0) shv[warp][q] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        double x = shv[0][threadIdx.x];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) x = fmin(x, shv[w][threadIdx.x]);
+        red[threadIdx.x] = x;
+    }
+    __syncthreads();
     int plo[3], bdim[3], pdim[3];
     for (int c = 0; c < 3; c++) {
-        plo[c] = block_min_int(blo[c], shi);
-        const int phi = -block_min_int(bhi_neg[c], shi);
-        bdim[c] = phi - plo[c] + 1;
+        plo[c] = (int)red[6 + c];
+        bdim[c] = (int)(-red[9 + c]) - plo[c] + 1;
         pdim[c] = bdim[c] + S - 1;
     }
     const long long pcells = (long long)pdim[0] * pdim[1] * pdim[2];
     const bool overflow = pcells > kMaxPatchCells || mc.n_nodes == 0;
     if (range_flag) atomicOr(A.flags, range_flag);
     if (threadIdx.x == 0) {
-        for (int c = 0; c < 3; c++) { ms->patch_lo[c] = plo[c]; ms->patch_dim[c] = pdim[c]; }
+        for (int c = 0; c < 3; c++) {
+            ms->bbox_lo[c] = red[c];
+            ms->bbox_hi[c] = -red[3 + c];
+            ms->patch_lo[c] = plo[c];
+            ms->patch_dim[c] = pdim[c];
+        }
         ms->patch_cells = overflow ? 0 : (int)pcells;
         if (overflow) atomicOr(A.flags, LBFS_FLAG_IBM_RANGE);
     }
     if (overflow) return;
+    // bitonic sort of (bin, node) keys
     int npad = 1;
     while (npad < mc.n_nodes) npad <<= 1;
     for (int t = threadIdx.x; t < npad; t += blockDim.x) {
         unsigned long long key = ~0ull;
         if (t < mc.n_nodes) {
-            const int n = mc.node0 + t;
-            const Stencil st = node_stencil(A, A.x[n], A.y[n], A.z[n]);
+            const int *b = A.node_base + 3 * (size_t)(mc.node0 + t);
             const unsigned long long bin =
-                (unsigned long long)((st.i0 - plo[0]) + bdim[0] * ((st.j0 - plo[1]) + bdim[1] * (st.k0 - plo[2])));
+                (unsigned long long)((b[0] - plo[0]) + bdim[0] * ((b[1] - plo[1]) + bdim[1] * (b[2] - plo[2])));
             key = (bin << 32) | (unsigned long long)t;
         }
         skeys[t] = key;
@@ -529,51 +563,69 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_gather(MembraneArgs A)
             __syncthreads();
         }
     }
-    for (int t = threadIdx.x; t < mc.n_nodes; t += blockDim.x) A.keys[mc.node0 + t] = skeys[t];
+    // sorted node records for the spread, and for every bin b the first
+    // sorted position whose bin is >= b (bins nbins + 1 entries)
+    const int nbins = bdim[0] * bdim[1] * bdim[2];
+    int *bin_start = A.bin_start + (size_t)m * (kMaxPatchCells + 1);
+    for (int b = threadIdx.x; b <= nbins; b += blockDim.x) {
+        int lo = 0, hi = mc.n_nodes;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((skeys[mid] >> 32) < (unsigned long long)b) lo = mid + 1;
+            else hi = mid;
+        }
+        bin_start[b] = lo;
+    }
+    for (int e = threadIdx.x; e < mc.n_nodes; e += blockDim.x) {
+        const int n = mc.node0 + (int)(skeys[e] & 0xffffffffu);
+        SpreadRec r;
+        r.f[0] = A.fx[n]; r.f[1] = A.fy[n]; r.f[2] = A.fz[n];
+        for (int q = 0; q < 12; q++) r.w[q] = A.node_w[12 * (size_t)n + q];
+        for (int c = 0; c < 3; c++) r.b[c] = A.node_base[3 * (size_t)n + c];
+        r.b[3] = 0;
+        A.spread_rec[mc.node0 + e] = r;
+    }
 }
 
 // ---- M5: spread as a per-cell segmented reduction over the sorted nodes ------
-// Each patch cell sums, bins in (z, y, x) order and nodes in node order, the
-// contributions of the nodes whose stencil covers it.
+// Each patch cell sums, stencil rows in (z, y) order and within a row nodes in
+// (bin, node) order, the contributions of the nodes whose stencil covers it.
+// The nodes of one row of bins are contiguous in the sorted order.
+template <int S>
 __global__ void __launch_bounds__(128) k_mem_spread(MembraneArgs A) {
     const int m = blockIdx.y;
-    const MembraneScalars ms = A.ms[m];
     const int pc = blockIdx.x * blockDim.x + threadIdx.x;
+    const MembraneScalars &ms = A.ms[m];
     if (pc >= ms.patch_cells) return;
-    const MembraneConst mc = A.mc[m];
-    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+    const int node0 = A.mc[m].node0;
     const int pdim[3] = {ms.patch_dim[0], ms.patch_dim[1], ms.patch_dim[2]};
     const int bdim[3] = {pdim[0] - S + 1, pdim[1] - S + 1, pdim[2] - S + 1};
     const int px = pc % pdim[0], py = (pc / pdim[0]) % pdim[1], pz = pc / (pdim[0] * pdim[1]);
     const int ci = ms.patch_lo[0] + px, cj = ms.patch_lo[1] + py, ck = ms.patch_lo[2] + pz;
-    const unsigned long long *keys = A.keys + mc.node0;
+    const int *bin_start = A.bin_start + (size_t)m * (kMaxPatchCells + 1);
+    const SpreadRec *rec = A.spread_rec + node0;
     const double inv3 = 1 / A.delta_x / A.delta_x / A.delta_x;
-    double f[3] = {0.0, 0.0, 0.0};
     const int bx0 = max(px - S + 1, 0), bx1 = min(px, bdim[0] - 1);
-    const int by0 = max(py - S + 1, 0), by1 = min(py, bdim[1] - 1);
-    const int bz0 = max(pz - S + 1, 0), bz1 = min(pz, bdim[2] - 1);
-    for (int bz = bz0; bz <= bz1; bz++)
-        for (int by = by0; by <= by1; by++) {
-            if (bx0 > bx1) continue;
-            const unsigned long long klo = (unsigned long long)(bx0 + bdim[0] * (by + bdim[1] * bz));
-            const unsigned long long khi = (unsigned long long)(bx1 + bdim[0] * (by + bdim[1] * bz));
-            int lo_i = 0, hi_i = mc.n_nodes;  // first sorted entry with bin >= klo
-            while (lo_i < hi_i) {
-                const int mid = (lo_i + hi_i) >> 1;
-                if ((keys[mid] >> 32) < klo) lo_i = mid + 1;
-                else hi_i = mid;
-            }
-            for (int e = lo_i; e < mc.n_nodes && (keys[e] >> 32) <= khi; e++) {
-                const int n = mc.node0 + (int)(keys[e] & 0xffffffffu);
-                const Stencil st = node_stencil(A, A.x[n], A.y[n], A.z[n]);
-                const double wx = stencil_weight(A.ibm_stencil, ci + 0.5 - st.rx);
-                const double wy = stencil_weight(A.ibm_stencil, cj + 0.5 - st.ry);
-                const double wz = stencil_weight(A.ibm_stencil, ck + 0.5 - st.rz);
-                f[0] += A.fx[n] * wx * wy * wz * inv3;
-                f[1] += A.fy[n] * wx * wy * wz * inv3;
-                f[2] += A.fz[n] * wx * wy * wz * inv3;
-            }
+    int lo[S * S], hi[S * S];
+#pragma unroll
+    for (int r = 0; r < S * S; r++) {
+        const int by = py - S + 1 + r % S, bz = pz - S + 1 + r / S;
+        const bool ok = by >= 0 && by < bdim[1] && bz >= 0 && bz < bdim[2] && bx0 <= bx1;
+        const int row = bdim[0] * (by + bdim[1] * bz);
+        lo[r] = ok ? __ldg(bin_start + row + bx0) : 0;
+        hi[r] = ok ? __ldg(bin_start + row + bx1 + 1) : 0;
+    }
+    double f[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int r = 0; r < S * S; r++) {
+        for (int e = lo[r]; e < hi[r]; e++) {
+            const SpreadRec &q = rec[e];
+            const double wx = q.w[ci - q.b[0]], wy = q.w[4 + cj - q.b[1]], wz = q.w[8 + ck - q.b[2]];
+            f[0] += q.f[0] * wx * wy * wz * inv3;
+            f[1] += q.f[1] * wx * wy * wz * inv3;
+            f[2] += q.f[2] * wx * wy * wz * inv3;
         }
+    }
     double *pf = A.patch_force + ((size_t)m * kMaxPatchCells + pc) * 3;
     pf[0] = f[0];
     pf[1] = f[1];
@@ -633,27 +685,50 @@ void membrane_prepare(int sort_capacity) {
     cudaFuncSetAttribute(k_mem_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
+namespace {
+// Launch with the device's greatest scheduling priority: the membrane chain is
+// the critical path of a step and runs beside the fluid kernels on a second
+// stream, so its blocks are placed ahead of pending fluid blocks.
+template <typename... Args>
+void launch_hi(void (*kernel)(Args...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const MembraneArgs &a) {
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = hi;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, a);
+}
+}  // namespace
+
 int launch_membrane(const MembraneArgs &a, cudaStream_t s) {
     const size_t smem = (size_t)(a.sort_capacity > 0 ? a.sort_capacity : 1) * sizeof(unsigned long long);
     const int spring_blocks = (a.total_springs + 127) / 128;
     if (a.mode == kModeReference) {
-        k_mem_springs<<<spring_blocks, 128, 0, s>>>(a);
+        launch_hi(k_mem_springs, dim3(spring_blocks), dim3(128), 0, s, a);
         return 1;
     }
     int n = 0;
     if (a.mode == kModeStep) {
         const int blocks = (a.total_nodes * 32 + 255) / 256;
-        if (a.state_is_float) k_mem_advect<float><<<blocks, 256, 0, s>>>(a);
-        else k_mem_advect<double><<<blocks, 256, 0, s>>>(a);
+        if (a.state_is_float) launch_hi(k_mem_advect<float>, dim3(blocks), dim3(256), 0, s, a);
+        else launch_hi(k_mem_advect<double>, dim3(blocks), dim3(256), 0, s, a);
         n++;
     }
-    k_mem_totals<<<a.n_membranes, 256, 0, s>>>(a);
-    k_mem_springs<<<spring_blocks, 128, 0, s>>>(a);
-    k_mem_gather<<<a.n_membranes, kMembraneThreads, smem, s>>>(a);
+    launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(256), 0, s, a);
+    launch_hi(k_mem_springs, dim3(spring_blocks), dim3(128), 0, s, a);
+    launch_hi(k_mem_gather, dim3(a.n_membranes), dim3(kMembraneThreads), smem, s, a);
     n += 3;
     if (a.mode == kModeStep) {
-        dim3 grid((kMaxPatchCells + 127) / 128, a.n_membranes);
-        k_mem_spread<<<grid, 128, 0, s>>>(a);
+        const dim3 grid((kMaxPatchCells + 127) / 128, a.n_membranes);
+        if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(128), 0, s, a);
+        else launch_hi(k_mem_spread<2>, grid, dim3(128), 0, s, a);
         n++;
     }
     return n;

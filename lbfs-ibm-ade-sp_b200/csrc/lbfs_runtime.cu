@@ -345,7 +345,10 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         (rc = s->upload(&ma.angle0, zeros_s)) || (rc = s->upload(&ma.area0, zeros_2s)) ||
         (rc = s->upload(&ma.area, zeros_2s)) || (rc = s->alloc(&ma.contrib, 12 * (size_t)S)) ||
         (rc = s->alloc(&ma.keys, N)) || (rc = s->alloc(&ma.patch_force, (size_t)n_rbc * kMaxPatchCells * 3)) ||
-        (rc = s->upload(&d_smem, spring_mem)))
+        (rc = s->upload(&d_smem, spring_mem)) || (rc = s->alloc(&ma.node_base, 3 * (size_t)N)) ||
+        (rc = s->alloc(&ma.node_w, 12 * (size_t)N)) ||
+        (rc = s->alloc(&ma.bin_start, (size_t)n_rbc * (kMaxPatchCells + 1))) ||
+        (rc = s->alloc(&ma.spread_rec, (size_t)N)))
         return rc;
     ma.spring_mem = d_smem;
     ma.mc = d_mc; ma.ms = d_ms; ma.tri = d_tri; ma.spring = d_spr; ma.inc = d_inc; ma.inc_start = d_incs;
@@ -486,8 +489,10 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     s->n_membranes = n_rbc;
     auto fail = [&](int code) { free_all(s); delete s; return code; };
     if (cudaSetDevice(device) != cudaSuccess) return fail(set_error(LBFS_ERR_CUDA, "cudaSetDevice failed"));
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&s->stream2, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess)
         return fail(set_error(LBFS_ERR_CUDA, "stream/event creation failed"));
@@ -497,7 +502,8 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if ((rc = s->upload(&s->d_centroid, centroid))) return fail(rc);
     rc = setup_membranes(s, mesh, rbc, n_rbc);
     if (rc) return fail(rc);
-    s->launches_per_step = n_rbc > 0 ? 3 + 5 : 3;  // fluid kernels + membrane kernels
+    // gradients, face flux (axis + general), update; membrane kernels
+    s->launches_per_step = 4 + (n_rbc > 0 ? 5 : 0);
     *out = s;
     return LBFS_OK;
 }
