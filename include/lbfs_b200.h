@@ -198,6 +198,28 @@ int lbfs_launches_per_step(lbfs_solver *s, int32_t *launches);
 /* Copy of the last error message (NUL terminated, truncated to len). */
 int lbfs_last_error(char *buf, int32_t len);
 
+/* ---- residual norms without device allocation ---------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc --
+ * host code that drives the step from inside a CUDA-graph capture or a stream
+ * callback (cudaMalloc is illegal during capture and synchronises the device),
+ * or integrations whose device memory is all reserved by their own pool:
+ * the RMS norms of a residual field, as lbfs_get_residuals reports them, with
+ * the reduction's scratch in a fixed __device__ array of the library instead
+ * of allocated memory.  d_res: device [4*n_cells] (res_rho, res_u, res_v,
+ * res_w per cell); d_rms: device [4] (rho, u, v, w norms); stream: a
+ * cudaStream_t (0 = default stream).  Enqueued, not waited for.
+ * Limits: n_cells <= LBFS_NOALLOC_MAX_CELLS (LBFS_ERR_LIMIT beyond); the
+ * scratch array (2 MiB per GPU that loads the library, held until exit) is
+ * shared by every call, so calls that overlap on the GPU race -- serialise
+ * them.  The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress) and must come before any stream capture on that
+ * device. */
+#define LBFS_NOALLOC_MAX_BLOCKS 65536
+#define LBFS_NOALLOC_MAX_CELLS (LBFS_NOALLOC_MAX_BLOCKS * 256)
+int lbfs_residual_rms_noalloc(const double *d_res, int32_t n_cells, double ref_rho, double max_velocity,
+                              double *d_rms, void *stream);
+
 /* ---- host-side set-up helpers ------------------------------------------- */
 
 /* Sizes of the uniform mesh generated for a domain X x Y x Z with streaming

@@ -42,6 +42,9 @@ LBFS_FIELD_VISC = 5
 LBFS_FIELD_GHOST = 6
 LBFS_FIELD_SPRING = 7
 
+LBFS_NOALLOC_MAX_BLOCKS = 65536
+LBFS_NOALLOC_MAX_CELLS = LBFS_NOALLOC_MAX_BLOCKS * 256
+
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _f64p = ctypes.POINTER(ctypes.c_double)
 
@@ -123,6 +126,7 @@ def lib():
                                                                   _f64p, _f64p, _f64p, _i32p, _f64p, _f64p, _i32p,
                                                                   _f64p],
             "lbfs_rbc_build_springs": [ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int32, _i32p, _i32p],
+            "lbfs_residual_rms_noalloc": [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -162,4 +166,5 @@ EXPORTED = [
     "lbfs_get_residuals", "lbfs_get_field", "lbfs_keep_residuals", "lbfs_status", "lbfs_launches_per_step",
     "lbfs_set_profiling", "lbfs_get_phase_times",
     "lbfs_last_error", "lbfs_mesh_uniform_counts", "lbfs_mesh_build_uniform", "lbfs_rbc_build_springs",
+    "lbfs_residual_rms_noalloc",
 ]
