@@ -185,10 +185,11 @@ int lbfs_keep_residuals(lbfs_solver *s, int32_t on);
 
 /* Accumulated status flags (LBFS_FLAG_*) since creation; reading does not clear. */
 int lbfs_status(lbfs_solver *s, uint32_t *flags);
-/* Per-kernel timing with CUDA events around every launch (also inside the
- * captured graph).  lbfs_get_phase_times writes the durations in ms of the
- * last step's kernels: [0] membrane, [1] ghost+gradients, [2] face flux,
- * [3] cell update, [4] interior viscosity (0 when not launched), and [5] the
+/* Timing with CUDA events, also inside the captured graph.  level 1: events
+ * around each whole step; level 2: also around every kernel (or kernel group);
+ * 0: off.  lbfs_get_phase_times writes the durations in ms of the last step:
+ * [0] membrane kernels, [1] ghost+gradients, [2] face flux, [3] cell update,
+ * [4] interior viscosity (0 when not launched or not level 2), and [5] the
  * whole step (first launch to last, on the solver's stream). */
 int lbfs_set_profiling(lbfs_solver *s, int32_t on);
 int lbfs_get_phase_times(lbfs_solver *s, double *ms);

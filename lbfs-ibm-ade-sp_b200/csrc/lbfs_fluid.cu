@@ -45,7 +45,12 @@ __global__ void __launch_bounds__(256) k_cell_gradients(FluidArgs<R> a) {
     R rr[3] = {0, 0, 0}, ru[3] = {0, 0, 0}, rv[3] = {0, 0, 0}, rw[3] = {0, 0, 0};
     int st[6];
 #pragma unroll
-    for (int q = 0; q < 6; q++) st[q] = __ldg(a.stencil + 6 * i + q);
+    for (int q = 0; q < 3; q++) {
+        const int2 p = __ldg(a.stencil + 3 * i + q);
+        st[2 * q] = p.x;
+        st[2 * q + 1] = p.y;
+    }
+    const LsRec<R> ls = a.ls[i];
     bool has_ghost = false;
 #pragma unroll
     for (int q = 0; q < 6; q++) {
@@ -59,17 +64,15 @@ __global__ void __launch_bounds__(256) k_cell_gradients(FluidArgs<R> a) {
         }
         // add_LS_contributions, LBFS.cu:2051-2083
         const R du = s.u - own.u, dv = s.v - own.v, dw = s.w - own.w, dr = s.rho - own.rho;
-        const R *R3 = a.rhs + 18 * i + 3 * q;
-        const R r0 = __ldg(R3), r1 = __ldg(R3 + 1), r2 = __ldg(R3 + 2);
+        const R r0 = ls.rhs[3 * q], r1 = ls.rhs[3 * q + 1], r2 = ls.rhs[3 * q + 2];
         rr[0] = rr[0] + r0 * dr; rr[1] = rr[1] + r1 * dr; rr[2] = rr[2] + r2 * dr;
         ru[0] = ru[0] + r0 * du; ru[1] = ru[1] + r1 * du; ru[2] = ru[2] + r2 * du;
         rv[0] = rv[0] + r0 * dv; rv[1] = rv[1] + r1 * dv; rv[2] = rv[2] + r2 * dv;
         rw[0] = rw[0] + r0 * dw; rw[1] = rw[1] + r1 * dw; rw[2] = rw[2] + r2 * dw;
     }
-    R L[9];
-#pragma unroll
-    for (int q = 0; q < 9; q++) L[q] = __ldg(a.lhs + 9 * i + q);
-    R g[12];
+    const R *L = ls.lhs;
+    GradRec<R> gr;
+    R *g = gr.g;
     const R *rs[4] = {rr, ru, rv, rw};
 #pragma unroll
     for (int m = 0; m < 4; m++) {
@@ -77,9 +80,7 @@ __global__ void __launch_bounds__(256) k_cell_gradients(FluidArgs<R> a) {
         g[3 * m + 1] = L[3] * rs[m][0] + L[4] * rs[m][1] + L[5] * rs[m][2];
         g[3 * m + 2] = L[6] * rs[m][0] + L[7] * rs[m][1] + L[8] * rs[m][2];
     }
-    R *gout = a.grad + (size_t)12 * i;
-#pragma unroll
-    for (int q = 0; q < 12; q++) gout[q] = g[q];
+    reinterpret_cast<GradRec<R> *>(a.grad)[i] = gr;
     if (!has_ghost) return;
     // Ghost states and ghost gradients of this cell's boundary faces
     // (get_bc_gradients, LBFS.cu:1941-2044).
@@ -107,9 +108,10 @@ __global__ void __launch_bounds__(256) k_cell_gradients(FluidArgs<R> a) {
                 gg[3 * m + 2] = g[3 * m + 2] * r.mz;
             }
         }
-        R *go = a.grad + (size_t)12 * j;
+        GradRec<R> gro;
 #pragma unroll
-        for (int t = 0; t < 12; t++) go[t] = gg[t];
+        for (int t = 0; t < 12; t++) gro.g[t] = gg[t];
+        reinterpret_cast<GradRec<R> *>(a.grad)[j] = gro;
     }
 }
 
@@ -181,8 +183,9 @@ __device__ __forceinline__ Vec4<R> interface_flux(const R (&fl)[15], R rho0, R t
 }
 
 template <typename R> __device__ __forceinline__ void load_grad(const R *g, R (&o)[12]) {
+    const GradRec<R> r = *reinterpret_cast<const GradRec<R> *>(g);
 #pragma unroll
-    for (int t = 0; t < 12; t++) o[t] = __ldg(g + t);
+    for (int t = 0; t < 12; t++) o[t] = r.g[t];
 }
 
 // Axis-aligned face: populate_lattice_macros_uniform_{x,y,z} (LBFS.cu:2939-3644).
@@ -358,9 +361,16 @@ __global__ void __launch_bounds__(256) k_cell_update(FluidArgs<R> a) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nc; i += gridDim.x * blockDim.x) {
         const double vol = __ldg(a.cell_volume + i);
         double r[4] = {0, 0, 0, 0};  // rho, u, v, w
+        int cfl[6];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const int2 p = __ldg(reinterpret_cast<const int2 *>(a.cell_faces) + 3 * i + q);
+            cfl[2 * q] = p.x;
+            cfl[2 * q + 1] = p.y;
+        }
 #pragma unroll
         for (int q = 0; q < 6; q++) {
-            const int e = __ldg(a.cell_faces + 6 * i + q);
+            const int e = cfl[q];
             const int f = (e > 0 ? e : -e) - 1;
             const Vec4<R> fx = a.flux[f];
             const double fv[4] = {(double)fx.rho, (double)fx.u, (double)fx.v, (double)fx.w};

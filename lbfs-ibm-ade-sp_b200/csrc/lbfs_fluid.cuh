@@ -47,7 +47,9 @@ __host__ __device__ constexpr int c_ez(int k) {
     return (k == 5 || k == 7 || k == 10 || k == 11 || k == 13) ? 1 : ((k == 6 || k == 8 || k == 9 || k == 12 || k == 14) ? -1 : 0);
 }
 
-template <typename R> struct Vec4 { R u, v, w, rho; };
+// 4-value record with natural vector alignment (32 B in FP64, 16 B in FP32) so
+// loads and stores are emitted as vector instructions.
+template <typename R> struct alignas(4 * sizeof(R)) Vec4 { R u, v, w, rho; };
 
 template <typename R> __host__ __device__ constexpr R lattice_w(int k) {
     return k == 0 ? R(2.0 / 9.0) : (k < 7 ? R(1.0 / 9.0) : R(1.0 / 72.0));
@@ -93,15 +95,28 @@ template <typename R> struct BcRec {
 // Face geometry of an axis-aligned interior face: area, streaming dt,
 // t1 = owner centroid - face centroid and t2 = neighbour centroid - face
 // centroid along the face axis (LBFS.cu:2313-2315, 2950-2951).
-template <typename R> struct AxisFace {
+template <typename R> struct alignas(4 * sizeof(R)) AxisFace {
     R area, dt, t1, t2;
 };
 
 // Face geometry of a general face (boundary faces always; interior faces of
 // meshes that are not axis aligned): area, dt, unit normal, and the full
 // vectors t1 = c_owner - x_face, t2 = c_neighbour - x_face (LBFS.cu:335-337).
-template <typename R> struct GenFace {
+template <typename R> struct alignas(16) GenFace {
     R area, dt, nx, ny, nz, t1x, t1y, t1z, t2x, t2y, t2z, pad;
+};
+
+// Least-squares geometry of one cell: RHS weights of the 6 stencil entries
+// (x, y, z each) then LHS^-1 row major, padded to 28 values (16-B multiple).
+template <typename R> struct alignas(16) LsRec {
+    R rhs[18];
+    R lhs[9];
+    R pad;
+};
+
+// Gradients of one cell: grad rho, grad u, grad v, grad w (x, y, z each).
+template <typename R> struct alignas(16) GradRec {
+    R g[12];
 };
 
 template <typename R> struct FluidArgs {
@@ -115,9 +130,8 @@ template <typename R> struct FluidArgs {
     Vec4<R> *state;              // [nc+nb]
     R *grad;                     // [12*(nc+nb)] rho(x,y,z) u(x,y,z) v(x,y,z) w(x,y,z)
     // K1 geometry
-    const int *stencil;          // [6*nc]
-    const R *rhs;                // [18*nc]
-    const R *lhs;                // [9*nc]
+    const int2 *stencil;         // [3*nc] (6 stencil entries per cell)
+    const LsRec<R> *ls;          // [nc]
     const int *bc_rho_type, *bc_vel_type;
     const Vec4<R> *bc_val;       // [nb] (u, v, w, rho - rho0)
     const BcRec<R> *bc_rec;      // [nb]

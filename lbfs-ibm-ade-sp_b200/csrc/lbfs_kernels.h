@@ -25,12 +25,15 @@ enum MembraneMode : int {
     kModeStep = 2,       // one time step: interpolate, advect, forces, spread
 };
 
-// A node as the spread reads it: force, 1D stencil weights per axis, first stencil cell.
+// A node as the spread reads it, in sorted order: 1D stencil weights per axis,
+// first stencil cell (b[0..2]) and the node index (b[3]).
 struct SpreadRec {
-    double f[3];
     double w[12];
     int b[4];
 };
+
+// Spring blocks of 128 per membrane the MAD partials can hold.
+constexpr int kMaxSpringBlocks = (3 * kMaxMembraneNodes + 127) / 128;
 
 struct MembraneArgs {
     int n_membranes;
@@ -64,12 +67,18 @@ struct MembraneArgs {
     int *node_base;              // [3*total_nodes] first stencil cell per axis (scratch)
     double *node_w;              // [12*total_nodes] 1D stencil weights per axis (scratch)
     int *bin_start;              // [n_membranes * (kMaxPatchCells + 1)] first sorted node of each bin (scratch)
-    SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order: force, weights, stencil base (scratch)
+    SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order (scratch)
+    int max_springs;             // springs of the largest membrane
+    double *mad_partials;        // [n_membranes * kMaxSpringBlocks] (scratch)
+    unsigned int *mad_ticket;    // [n_membranes], zero between launches
 };
 
 void membrane_prepare(int sort_capacity);
-// Enqueues the membrane kernels of the current mode; returns the launch count.
-int launch_membrane(const MembraneArgs &a, cudaStream_t s);
+// Enqueues the membrane kernels of the current mode on `s` (the node sort on
+// `s_side`, joined back before the spread, when the side stream and its two
+// events are given); returns the launch count.
+int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side = nullptr,
+                    cudaEvent_t ev_advected = nullptr, cudaEvent_t ev_sorted = nullptr);
 
 struct ViscArgs {
     int nc, n_membranes;

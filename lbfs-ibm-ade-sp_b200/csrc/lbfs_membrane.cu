@@ -1,10 +1,10 @@
 // Membrane side of one time step, five kernels:
 //
-//   M1 k_mem_advect  (one warp per node)      P0
-//   M2 k_mem_totals  (one CTA per membrane)   P1
-//   M3 k_mem_springs (one thread per spring)  P2
-//   M4 k_mem_gather  (one CTA per membrane)   P3, P4, P5
-//   M5 k_mem_spread  (one thread per patch cell of each membrane)  P6
+//   M1 k_mem_advect    (one warp per node)                           P0
+//   M2 k_mem_springs   (one thread per spring; totals per block)     P1, P2, P4
+//   M3 k_mem_nodeforce (one thread per node)                         P3
+//   M4 k_mem_sort      (one CTA per membrane, on a side stream)      P5
+//   M5 k_mem_spread    (one thread per patch cell of each membrane)  P6
 //
 //   P0  IBM velocity interpolation at the nodes + explicit node advection
 //       (interpolate_velocities_on_nodes, immersed_boundary_method.cu:14-97;
@@ -386,11 +386,28 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
     }
 }
 
-// ---- M2: membrane totals V, A, one CTA per membrane ---------------------------
-__global__ void __launch_bounds__(256) k_mem_totals(MembraneArgs A) {
+// ---- M2: spring forces, one thread per spring, blocks per membrane ----------
+// Every block first forms its membrane's totals V and A over all triangles (the
+// same fixed-order sum in every block, so all blocks agree bit for bit), then
+// its springs' forces; the per-block MAD partials (curvature x area over the
+// first n_nodes springs) are summed by the membrane's last block to finish.
+// Reference mode: the stress-free pass (contour lengths, spring constants,
+// reference curvatures).
+__global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
     __shared__ double sh[33];
-    const MembraneConst mc = A.mc[blockIdx.x];
-    MembraneScalars *ms = A.ms + blockIdx.x;
+    __shared__ bool last_block;
+    const int m = blockIdx.y;
+    const MembraneConst mc = A.mc[m];
+    const int first = blockIdx.x * blockDim.x;
+    if (first >= mc.n_springs) return;  // whole block idle for this membrane
+    const int ls = first + threadIdx.x;
+    const int s = mc.spring0 + ls;
+    if (A.mode == kModeReference) {
+        if (ls < mc.n_springs) spring_reference(A, mc, s);
+        return;
+    }
+    MembraneScalars *ms = A.ms + m;
+    const bool initials = A.mode == kModeInitial;
     double pv = 0.0, pa = 0.0;
     for (int lt = threadIdx.x; lt < mc.n_tris; lt += blockDim.x) {
         const int t = mc.tri0 + lt;
@@ -401,92 +418,90 @@ __global__ void __launch_bounds__(256) k_mem_totals(MembraneArgs A) {
         pa += sqrt(dot(normal, normal)) * 0.5;
     }
     const double V = block_sum(pv, sh), Ar = block_sum(pa, sh);
-    if (threadIdx.x == 0) {
-        ms->V = V;
-        ms->A = Ar;
-        if (A.mode == kModeInitial) {
-            ms->V0 = V * mc.volume_ratio;
-            ms->A0 = Ar;
-            ms->MAD = 0.0;
-            ms->MAD0 = 0.0;
-        }
-    }
-}
-
-// ---- M3: per-spring forces (or the stress-free reference pass), grid over springs
-__global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= A.total_springs) return;
-    const int m = A.spring_mem[s];
-    const MembraneConst mc = A.mc[m];
-    if (A.mode == kModeReference) {
-        spring_reference(A, mc, s);
-        return;
-    }
-    const MembraneScalars ms = A.ms[m];
+    const double V0 = initials ? V * mc.volume_ratio : ms->V0;
+    const double A0 = initials ? Ar : ms->A0;
+    const double MADp = initials ? 0.0 : ms->MAD, MAD0p = initials ? 0.0 : ms->MAD0;
     const double wr = mc.wlc_ratio;
     const double sfc = (0.25 * wr * wr / ((wr - 1.0) * (wr - 1.0)) - 0.25 + 1.0 / wr);
-    const double vol_coef = -1 * mc.volume_modulus * (ms.V / ms.V0 - 1.0) / 6.0;
-    const double area_coef = -1 * mc.global_area_modulus * (ms.A / ms.A0 - 1.0);
-    const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (ms.MAD - ms.MAD0) / ms.A0;
-    spring_forces(A, mc, ms, s, A.mode == kModeInitial, sfc, vol_coef, area_coef, mad_coef);
+    const double vol_coef = -1 * mc.volume_modulus * (V / V0 - 1.0) / 6.0;
+    const double area_coef = -1 * mc.global_area_modulus * (Ar / A0 - 1.0);
+    const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (MADp - MAD0p) / A0;
+    double pm = 0.0;
+    if (ls < mc.n_springs) {
+        MembraneScalars cur = *ms;
+        spring_forces(A, mc, cur, s, initials, sfc, vol_coef, area_coef, mad_coef);
+        if (ls < mc.n_nodes) pm = A.curv[s] * (A.area[2 * s] + A.area[2 * s + 1]) * 1 / 3;
+    }
+    const double part = block_sum(pm, sh);
+    double *partials = A.mad_partials + (size_t)m * kMaxSpringBlocks;
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = part;
+        __threadfence();
+        const int nblk = (mc.n_springs + blockDim.x - 1) / blockDim.x;
+        last_block = atomicAdd(A.mad_ticket + m, 1u) == (unsigned)(nblk - 1);
+    }
+    __syncthreads();
+    if (!last_block) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        const int nblk = (mc.n_springs + blockDim.x - 1) / blockDim.x;
+        double sum = 0.0;
+        for (int b = 0; b < nblk; b++) sum += __ldcg(partials + b);
+        const double MAD = sum / Ar;
+        ms->V = V;
+        ms->A = Ar;
+        ms->MAD = MAD;
+        if (initials) { ms->V0 = V0; ms->A0 = A0; ms->MAD0 = MAD; }
+        A.mad_ticket[m] = 0u;
+    }
 }
 
-// ---- M4: node forces, MAD, node bounds, nodes sorted by stencil base cell ----
-// Also writes, for the spread, each node's stencil (first cell and 1D weights)
-// and, for every bin (stencil base cell) of the patch, the range of its nodes
-// in the sorted order.
-__global__ void __launch_bounds__(kMembraneThreads) k_mem_gather(MembraneArgs A) {
+// ---- M3: node forces, one thread per node, contributions in spring order ----
+__global__ void __launch_bounds__(128) k_mem_nodeforce(MembraneArgs A) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= A.total_nodes) return;
+    double f[3] = {0.0, 0.0, 0.0};
+    const int e0 = A.inc_start[n], e1 = A.inc_start[n + 1];
+    for (int c0 = e0; c0 < e1; c0 += 8) {
+        int code[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) code[q] = (c0 + q < e1) ? __ldg(A.inc + c0 + q) : -1;
+        double d[8][3];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            if (code[q] >= 0) {
+                const double *o = A.contrib + 12 * (size_t)(code[q] >> 2) + 3 * (code[q] & 3);
+                d[q][0] = o[0]; d[q][1] = o[1]; d[q][2] = o[2];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+            if (code[q] >= 0) { f[0] += d[q][0]; f[1] += d[q][1]; f[2] += d[q][2]; }
+    }
+    A.fx[n] = f[0];
+    A.fy[n] = f[1];
+    A.fz[n] = f[2];
+}
+
+// ---- M4: node bounds, stencil tables, nodes sorted by stencil base cell -----
+// One CTA per membrane; needs only the advected positions, so it runs beside
+// M2 and M3.  Writes each node's first stencil cell and 1D weights, the patch,
+// the sorted node list and, for every bin b of the patch, the first sorted
+// position whose bin is >= b.
+__global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     extern __shared__ unsigned long long skeys[];
-    __shared__ double sh[33];
     __shared__ double shv[kMembraneThreads / 32][12];
     __shared__ double red[12];
     const int m = blockIdx.x;
     const MembraneConst mc = A.mc[m];
     MembraneScalars *ms = A.ms + m;
-    const double Ar = ms->A;
-    // MAD over the first n_nodes springs of this membrane
-    double pm = 0.0;
-    const int n_mad = mc.n_nodes < mc.n_springs ? mc.n_nodes : mc.n_springs;
-    for (int ls = threadIdx.x; ls < n_mad; ls += blockDim.x) {
-        const int s = mc.spring0 + ls;
-        pm += A.curv[s] * (A.area[2 * s] + A.area[2 * s + 1]) * 1 / 3;
-    }
-    const double MAD = block_sum(pm, sh) / Ar;
-    if (threadIdx.x == 0) {
-        ms->MAD = MAD;
-        if (A.mode == kModeInitial) ms->MAD0 = MAD;
-    }
-    if (A.mode != kModeStep) return;
     const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
     const int gn[3] = {A.grid_nx, A.grid_ny, A.grid_nz};
-    // node forces in spring order, node bounds, stencil bases and weights
     double v[12];
     for (int c = 0; c < 3; c++) { v[c] = 1e300; v[3 + c] = 1e300; v[6 + c] = 1e300; v[9 + c] = 1e300; }
     unsigned int range_flag = 0;
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
         const int n = mc.node0 + ln;
-        double f[3] = {0.0, 0.0, 0.0};
-        // contributions in spring order; the indices of a chunk are loaded
-        // before its data so the loads of a node overlap
-        const int e0 = A.inc_start[n], e1 = A.inc_start[n + 1];
-        for (int c0 = e0; c0 < e1; c0 += 8) {
-            int code[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) code[q] = (c0 + q < e1) ? __ldg(A.inc + c0 + q) : -1;
-            double d[8][3];
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                if (code[q] >= 0) {
-                    const double *o = A.contrib + 12 * (size_t)(code[q] >> 2) + 3 * (code[q] & 3);
-                    d[q][0] = o[0]; d[q][1] = o[1]; d[q][2] = o[2];
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < 8; q++)
-                if (code[q] >= 0) { f[0] += d[q][0]; f[1] += d[q][1]; f[2] += d[q][2]; }
-        }
-        A.fx[n] = f[0]; A.fy[n] = f[1]; A.fz[n] = f[2];
         const double p[3] = {A.x[n], A.y[n], A.z[n]};
         const Stencil st = node_stencil(A, p[0], p[1], p[2]);
         const int b[3] = {st.i0, st.j0, st.k0};
@@ -502,7 +517,6 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_gather(MembraneArgs A)
             A.node_base[3 * (size_t)n + c] = b[c];
         }
     }
-    // one block reduction of the 12 minima
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < 12; q++) {
@@ -537,7 +551,6 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_gather(MembraneArgs A)
         if (overflow) atomicOr(A.flags, LBFS_FLAG_IBM_RANGE);
     }
     if (overflow) return;
-    // bitonic sort of (bin, node) keys
     int npad = 1;
     while (npad < mc.n_nodes) npad <<= 1;
     for (int t = threadIdx.x; t < npad; t += blockDim.x) {
@@ -563,8 +576,6 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_gather(MembraneArgs A)
             __syncthreads();
         }
     }
-    // sorted node records for the spread, and for every bin b the first
-    // sorted position whose bin is >= b (bins nbins + 1 entries)
     const int nbins = bdim[0] * bdim[1] * bdim[2];
     int *bin_start = A.bin_start + (size_t)m * (kMaxPatchCells + 1);
     for (int b = threadIdx.x; b <= nbins; b += blockDim.x) {
@@ -579,10 +590,9 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_gather(MembraneArgs A)
     for (int e = threadIdx.x; e < mc.n_nodes; e += blockDim.x) {
         const int n = mc.node0 + (int)(skeys[e] & 0xffffffffu);
         SpreadRec r;
-        r.f[0] = A.fx[n]; r.f[1] = A.fy[n]; r.f[2] = A.fz[n];
         for (int q = 0; q < 12; q++) r.w[q] = A.node_w[12 * (size_t)n + q];
         for (int c = 0; c < 3; c++) r.b[c] = A.node_base[3 * (size_t)n + c];
-        r.b[3] = 0;
+        r.b[3] = n;
         A.spread_rec[mc.node0 + e] = r;
     }
 }
@@ -620,10 +630,11 @@ __global__ void __launch_bounds__(128) k_mem_spread(MembraneArgs A) {
     for (int r = 0; r < S * S; r++) {
         for (int e = lo[r]; e < hi[r]; e++) {
             const SpreadRec &q = rec[e];
+            const int n = q.b[3];
             const double wx = q.w[ci - q.b[0]], wy = q.w[4 + cj - q.b[1]], wz = q.w[8 + ck - q.b[2]];
-            f[0] += q.f[0] * wx * wy * wz * inv3;
-            f[1] += q.f[1] * wx * wy * wz * inv3;
-            f[2] += q.f[2] * wx * wy * wz * inv3;
+            f[0] += A.fx[n] * wx * wy * wz * inv3;
+            f[1] += A.fy[n] * wx * wy * wz * inv3;
+            f[2] += A.fz[n] * wx * wy * wz * inv3;
         }
     }
     double *pf = A.patch_force + ((size_t)m * kMaxPatchCells + pc) * 3;
@@ -682,7 +693,7 @@ __global__ void k_interior_viscosity(ViscArgs a) {
 
 void membrane_prepare(int sort_capacity) {
     const size_t smem = (size_t)(sort_capacity > 0 ? sort_capacity : 1) * sizeof(unsigned long long);
-    cudaFuncSetAttribute(k_mem_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_mem_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 namespace {
@@ -707,31 +718,36 @@ void launch_hi(void (*kernel)(Args...), dim3 grid, dim3 block, size_t smem, cuda
 }
 }  // namespace
 
-int launch_membrane(const MembraneArgs &a, cudaStream_t s) {
+int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, cudaEvent_t ev_advected,
+                    cudaEvent_t ev_sorted) {
     const size_t smem = (size_t)(a.sort_capacity > 0 ? a.sort_capacity : 1) * sizeof(unsigned long long);
-    const int spring_blocks = (a.total_springs + 127) / 128;
+    const dim3 spring_grid((a.max_springs + 127) / 128, a.n_membranes);
     if (a.mode == kModeReference) {
-        launch_hi(k_mem_springs, dim3(spring_blocks), dim3(128), 0, s, a);
+        launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
         return 1;
     }
-    int n = 0;
-    if (a.mode == kModeStep) {
-        const int blocks = (a.total_nodes * 32 + 255) / 256;
-        if (a.state_is_float) launch_hi(k_mem_advect<float>, dim3(blocks), dim3(256), 0, s, a);
-        else launch_hi(k_mem_advect<double>, dim3(blocks), dim3(256), 0, s, a);
-        n++;
+    if (a.mode == kModeInitial) {
+        launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
+        return 1;
     }
-    launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(256), 0, s, a);
-    launch_hi(k_mem_springs, dim3(spring_blocks), dim3(128), 0, s, a);
-    launch_hi(k_mem_gather, dim3(a.n_membranes), dim3(kMembraneThreads), smem, s, a);
-    n += 3;
-    if (a.mode == kModeStep) {
-        const dim3 grid((kMaxPatchCells + 127) / 128, a.n_membranes);
-        if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(128), 0, s, a);
-        else launch_hi(k_mem_spread<2>, grid, dim3(128), 0, s, a);
-        n++;
+    const int blocks = (a.total_nodes * 32 + 255) / 256;
+    if (a.state_is_float) launch_hi(k_mem_advect<float>, dim3(blocks), dim3(256), 0, s, a);
+    else launch_hi(k_mem_advect<double>, dim3(blocks), dim3(256), 0, s, a);
+    // the node sort needs only the advected positions: side stream
+    const bool side = s_side != nullptr && ev_advected != nullptr && ev_sorted != nullptr;
+    if (side) {
+        cudaEventRecord(ev_advected, s);
+        cudaStreamWaitEvent(s_side, ev_advected, 0);
     }
-    return n;
+    launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, side ? s_side : s, a);
+    if (side) cudaEventRecord(ev_sorted, s_side);
+    launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
+    launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
+    if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
+    const dim3 grid((kMaxPatchCells + 127) / 128, a.n_membranes);
+    if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(128), 0, s, a);
+    else launch_hi(k_mem_spread<2>, grid, dim3(128), 0, s, a);
+    return 5;
 }
 
 void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s) {

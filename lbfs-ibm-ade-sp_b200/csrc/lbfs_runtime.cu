@@ -45,7 +45,8 @@ using namespace lbfs;
 
 struct lbfs_solver {
     int device = 0;
-    cudaStream_t stream = nullptr, stream2 = nullptr;
+    cudaStream_t stream = nullptr, stream2 = nullptr, stream3 = nullptr;
+    cudaEvent_t ev_advected = nullptr, ev_sorted = nullptr;
     bool own_stream = true;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     lbfs_params params{};
@@ -65,7 +66,8 @@ struct lbfs_solver {
     int graph_steps = 0;
     int launches_per_step = 0;
     // per-kernel timing: start/stop events per phase (membrane, gradients, flux, update, viscosity)
-    bool profiling = false;
+    bool profiling = false;    // step events (level >= 1)
+    bool kernel_events = false; // per-kernel events too (level 2)
     cudaEvent_t ev_phase[kPhases][2] = {};
     bool phase_recorded[kPhases] = {};
     bool graph_phase_recorded[kPhases] = {};  // phases recorded by one replay of the graph
@@ -151,10 +153,14 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     for (int c = 0; c < 3; c++) a.force[c] = p.body_force[c];
     const double *cen = m->cell_centroid, *fc = m->face_centroid, *fn = m->face_normal;
     // K1 geometry
-    std::vector<int> stencil(m->gradient_stencil, m->gradient_stencil + 6 * (size_t)nc);
-    std::vector<R> rhs(18 * (size_t)nc), lhs(9 * (size_t)nc);
-    for (size_t i = 0; i < rhs.size(); i++) rhs[i] = (R)m->rhs[i];
-    for (size_t i = 0; i < lhs.size(); i++) lhs[i] = (R)m->lhs_inverse[i];
+    std::vector<int2> stencil(3 * (size_t)nc);
+    for (size_t q = 0; q < 3 * (size_t)nc; q++) stencil[q] = make_int2(m->gradient_stencil[2 * q], m->gradient_stencil[2 * q + 1]);
+    std::vector<LsRec<R>> ls(nc);
+    for (int i = 0; i < nc; i++) {
+        for (int q = 0; q < 18; q++) ls[i].rhs[q] = (R)m->rhs[18 * (size_t)i + q];
+        for (int q = 0; q < 9; q++) ls[i].lhs[q] = (R)m->lhs_inverse[9 * (size_t)i + q];
+        ls[i].pad = 0;
+    }
     std::vector<int> rt(nb), vt(nb);
     std::vector<Vec4<R>> bcv(nb);
     std::vector<BcRec<R>> bcr(nb);
@@ -214,21 +220,23 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     std::vector<double> vol(m->cell_volume, m->cell_volume + nc);
     std::vector<R> visc(nc, (R)p.visc_factor_initial);
     int rc = 0;
-    int *d_stencil, *d_rt, *d_vt, *d_cf;
-    R *d_rhs, *d_lhs, *d_visc;
+    int *d_rt, *d_vt, *d_cf;
+    int2 *d_stencil;
+    LsRec<R> *d_ls;
+    R *d_visc;
     Vec4<R> *d_bcv;
     BcRec<R> *d_bcr;
     int2 *d_fcells;
     AxisFace<R> *d_axf = nullptr;
     GenFace<R> *d_gen;
     double *d_vol;
-    if ((rc = s->upload(&d_stencil, stencil)) || (rc = s->upload(&d_rhs, rhs)) || (rc = s->upload(&d_lhs, lhs)) ||
+    if ((rc = s->upload(&d_stencil, stencil)) || (rc = s->upload(&d_ls, ls)) ||
         (rc = s->upload(&d_rt, rt)) || (rc = s->upload(&d_vt, vt)) || (rc = s->upload(&d_bcv, bcv)) ||
         (rc = s->upload(&d_bcr, bcr)) || (rc = s->upload(&d_fcells, fcells)) || (rc = s->upload(&d_gen, gen)) ||
         (rc = s->upload(&d_cf, cf)) || (rc = s->upload(&d_vol, vol)) || (rc = s->upload(&d_visc, visc)))
         return rc;
     if (a.axis_aligned && (rc = s->upload(&d_axf, axf))) return rc;
-    a.stencil = d_stencil; a.rhs = d_rhs; a.lhs = d_lhs; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt;
+    a.stencil = d_stencil; a.ls = d_ls; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt;
     a.bc_val = d_bcv; a.bc_rec = d_bcr; a.face_cells = d_fcells; a.axis_face = d_axf; a.gen_face = d_gen;
     a.visc_factor = d_visc; a.cell_faces = d_cf; a.cell_volume = d_vol;
     Vec4<R> *d_state, *d_flux;
@@ -348,8 +356,13 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         (rc = s->upload(&d_smem, spring_mem)) || (rc = s->alloc(&ma.node_base, 3 * (size_t)N)) ||
         (rc = s->alloc(&ma.node_w, 12 * (size_t)N)) ||
         (rc = s->alloc(&ma.bin_start, (size_t)n_rbc * (kMaxPatchCells + 1))) ||
-        (rc = s->alloc(&ma.spread_rec, (size_t)N)))
+        (rc = s->alloc(&ma.spread_rec, (size_t)N)) ||
+        (rc = s->alloc(&ma.mad_partials, (size_t)n_rbc * kMaxSpringBlocks)) ||
+        (rc = s->alloc(&ma.mad_ticket, (size_t)n_rbc)))
         return rc;
+    LBFS_CUDA(cudaMemset(ma.mad_ticket, 0, sizeof(unsigned int) * n_rbc));
+    ma.max_springs = 0;
+    for (int r = 0; r < n_rbc; r++) ma.max_springs = std::max(ma.max_springs, mc[r].n_springs);
     ma.spring_mem = d_smem;
     ma.mc = d_mc; ma.ms = d_ms; ma.tri = d_tri; ma.spring = d_spr; ma.inc = d_inc; ma.inc_start = d_incs;
     ma.flags = s->fp32 ? s->f32.flags : s->f64.flags;
@@ -394,10 +407,10 @@ struct PhaseMark {
     int phase;
     cudaStream_t st;
     PhaseMark(lbfs_solver *s_, int ph, cudaStream_t st_) : s(s_), phase(ph), st(st_) {
-        if (s->profiling) record_event(s->ev_phase[phase][0], st);
+        if (s->kernel_events) record_event(s->ev_phase[phase][0], st);
     }
     ~PhaseMark() {
-        if (s->profiling) {
+        if (s->kernel_events) {
             record_event(s->ev_phase[phase][1], st);
             s->phase_recorded[phase] = true;
         }
@@ -419,7 +432,7 @@ template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *la
         } else {
             LBFS_CUDA(cudaEventRecord(s->ev_fork, s->stream));
             LBFS_CUDA(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
-            { PhaseMark m(s, 0, s->stream2); n += launch_membrane(s->ma, s->stream2); }
+            { PhaseMark m(s, 0, s->stream2); n += launch_membrane(s->ma, s->stream2, s->stream3, s->ev_advected, s->ev_sorted); }
             LBFS_CUDA(cudaEventRecord(s->ev_join, s->stream2));
             { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
             { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
@@ -459,6 +472,9 @@ void free_all(lbfs_solver *s) {
     s->allocs.clear();
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     if (s->ev_join) cudaEventDestroy(s->ev_join);
+    if (s->ev_advected) cudaEventDestroy(s->ev_advected);
+    if (s->ev_sorted) cudaEventDestroy(s->ev_sorted);
+    if (s->stream3) cudaStreamDestroy(s->stream3);
     if (s->stream2) cudaStreamDestroy(s->stream2);
     if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
 }
@@ -493,6 +509,9 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithPriority(&s->stream2, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&s->stream3, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_advected, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_sorted, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess)
         return fail(set_error(LBFS_ERR_CUDA, "stream/event creation failed"));
@@ -577,6 +596,7 @@ extern "C" int lbfs_set_profiling(lbfs_solver *s, int32_t on) {
         for (int p = 0; p < kPhases; p++)
             for (int e = 0; e < 2; e++) LBFS_CUDA(cudaEventCreate(&s->ev_phase[p][e]));
     s->profiling = on != 0;
+    s->kernel_events = on >= 2;
     for (int p = 0; p < kPhases; p++) s->phase_recorded[p] = false;
     if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
     return LBFS_OK;

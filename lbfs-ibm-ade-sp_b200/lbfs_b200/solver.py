@@ -144,8 +144,9 @@ class GpuSolver:
         _abi.check(_abi.lib().lbfs_status(self._h, ctypes.byref(f)))
         return f.value
 
-    def set_profiling(self, on=True):
-        _abi.check(_abi.lib().lbfs_set_profiling(self._h, 1 if on else 0))
+    def set_profiling(self, level=2):
+        """0 off, 1 whole-step events, 2 whole-step and per-kernel events."""
+        _abi.check(_abi.lib().lbfs_set_profiling(self._h, int(level)))
 
     def phase_times(self):
         """Durations (ms) of the last step: membrane, gradients, flux, update, viscosity kernels, whole step."""
