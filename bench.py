@@ -52,10 +52,6 @@ def parse():
     return ap.parse_args()
 
 
-def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
-
-
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -229,6 +225,7 @@ def run_reference(args, rank, world):
 
 
 def main():
+    from lbfs_b200.parallel import dist_env, max_over_ranks
     args = parse()
     rank, local_rank, world = dist_env()
     if args.impl == "reference":
@@ -276,11 +273,7 @@ def main():
     barrier()
     clocks = sampler.stop()
     t_step_ms = step_sum[5] / K
-    total_s = step_sum[5] / 1e3
-    if world > 1:
-        t = torch.tensor([total_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_s = float(t.item())
+    total_s = max_over_ranks(step_sum[5] / 1e3, device="cuda")
     cell_updates = mesh.n_cells * K * world
     value = cell_updates / total_s / 1e6
     # second timed pass with per-kernel events (they cost a few us per step, so
@@ -322,11 +315,7 @@ def main():
             s.step(1, graph=True)
             _abi.check(_abi.lib().lbfs_get_state(s._h, *[_abi.ptr(h) for h in host]))
         barrier()
-        te = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(time.perf_counter() - t0, device="cuda")
         e2e = {"value": n * Ke * world / te / 1e6, "unit": METRIC, "h2d_bytes_per_step": 4 * 8 * n,
                "d2h_bytes_per_step": 4 * 8 * n, "steps": Ke, "timing": "host wall clock around set_state, step, "
                "get_state (page-locked host arrays)"}
