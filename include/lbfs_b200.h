@@ -55,6 +55,14 @@ extern "C" {
 #define LBFS_IBM_HAT2 2         /* 2-point hat stencil (immersed_boundary_method.cu:14-97, 947-1024) */
 #define LBFS_IBM_PESKIN4 4      /* 4-point Peskin cosine-free delta (new; no reference counterpart)  */
 
+/* One instance of a batched ensemble: a contiguous range of interior cells
+ * that forms its own uniform IBM grid (cell index = cell0 + i + nx (j + ny k)). */
+typedef struct lbfs_grid_desc {
+    int32_t cell0, n_cells;
+    double origin[3], length[3];
+    double delta_x, delta_h;
+} lbfs_grid_desc;
+
 /* Mesh arrays, in the reference's layout and order.  Sizes: nc = n_cells,
  * nb = n_bc (boundary faces = ghost cells, ghost of bc face i is cell nc+i),
  * nf = n_faces = n_interior + n_bc (boundary faces last).
@@ -86,6 +94,12 @@ typedef struct lbfs_mesh_desc {
     double length[3];              /* domain.X/Y/Z                               */
     double delta_x;                /* 2 * domain.dt                              */
     double delta_h;                /* unstructured_mesh::get_delta_h()           */
+    /* Batched ensemble (no reference counterpart): n_instances independent
+     * meshes concatenated into this one (interior cells, then ghosts; x, y, z
+     * interior faces, then boundary faces, each category instance by
+     * instance).  0 = one instance described by origin/length/delta_x/delta_h. */
+    int32_t n_instances;
+    const lbfs_grid_desc *instances;
 } lbfs_mesh_desc;
 
 /* Scalars of global_variables / initial_conditions used by the step. */
@@ -116,6 +130,7 @@ typedef struct lbfs_rbc_desc {
     double global_bending_modulus, local_bending_modulus, membrane_thickness, viscosity;
     double wlc_ratio, curvature_ratio, volume_ratio, internal_viscosity_ratio, reference_length;
     int32_t pivkin_length, sphere_reference;
+    int32_t instance;               /* ensemble instance the membrane lives in (0 without an ensemble) */
 } lbfs_rbc_desc;
 
 typedef struct lbfs_solver lbfs_solver;
@@ -198,6 +213,29 @@ int lbfs_get_phase_times(lbfs_solver *s, double *ms);
 int lbfs_launches_per_step(lbfs_solver *s, int32_t *launches);
 /* Copy of the last error message (NUL terminated, truncated to len). */
 int lbfs_last_error(char *buf, int32_t len);
+
+/* ---- launch shapes and the autotuner (no reference counterpart) ----------- *
+ * Block sizes and grid caps of the per-phase kernels.  Results do not depend on
+ * the shape, except the last bits of the residual norms, whose block partials
+ * follow the cell-update grid.  lbfs_autotune times every candidate shape of
+ * each kernel on this handle's own mesh and state (`reps` launches each, CUDA
+ * events), keeps the fastest, and leaves the state as it found it; the next
+ * lbfs_step_graph captures a new graph.  `shape` (may be null) receives the
+ * choice and the mean time of each chosen kernel in microseconds. */
+#define LBFS_MAX_UPDATE_BLOCKS (148 * 16)
+#define LBFS_MAX_SPREAD_BLOCKS (148 * 16)
+typedef struct lbfs_launch_shape {
+    int32_t gradient_threads;       /* 128, 256 or 512 */
+    int32_t flux_threads;           /* interior faces of an axis-aligned mesh: 64, 128 or 256 */
+    int32_t general_flux_threads;   /* boundary / general-normal faces: 64, 128 or 256 */
+    int32_t update_threads;         /* 128, 256 or 512 */
+    int32_t update_blocks;          /* grid cap of the cell update, 1 .. LBFS_MAX_UPDATE_BLOCKS */
+    int32_t spread_blocks;          /* grid of the IBM spread, 1 .. LBFS_MAX_SPREAD_BLOCKS */
+    double time_us[5];              /* autotune: gradients, flux, general flux, update, spread */
+} lbfs_launch_shape;
+int lbfs_get_launch_shape(lbfs_solver *s, lbfs_launch_shape *shape);
+int lbfs_set_launch_shape(lbfs_solver *s, const lbfs_launch_shape *shape);
+int lbfs_autotune(lbfs_solver *s, int32_t reps, lbfs_launch_shape *shape);
 
 /* ---- residual norms without device allocation ---------------------------- */
 

@@ -37,8 +37,8 @@ __device__ __forceinline__ Vec4<R> ghost_state(const FluidArgs<R> &a, int b, con
     return g;
 }
 
-template <typename R>
-__global__ void __launch_bounds__(256) k_cell_gradients(FluidArgs<R> a) {
+template <typename R, int TB>
+__global__ void __launch_bounds__(TB) k_cell_gradients(FluidArgs<R> a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nc) return;
     const Vec4<R> own = a.state[i];
@@ -250,9 +250,9 @@ __device__ __forceinline__ Vec4<R> axis_face_flux(const FluidArgs<R> &a, int f) 
     return interface_flux<R>(fl, a.rho0, tau, R(1), geo.area, axis, 0, 0, 0);
 }
 
-// General face: populate_lattice_macros (LBFS.cu:323-936).  Faces whose
-// neighbour index is greater than n_cells take the boundary branch (the first
-// ghost, index n_cells, takes the interior branch as in the reference).
+// General face: populate_lattice_macros (LBFS.cu:323-936).  Boundary faces
+// take the boundary branch except the face of the first ghost (LBFS.cu tests
+// neighbour > n_cells), which the host marks per instance in bc_branch.
 template <typename R>
 __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int f, bool is_bc) {
     const int2 oc = __ldg(a.face_cells + f);
@@ -264,7 +264,7 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
     const R dt = geo.dt;
     const R S1[4] = {s1.rho, s1.u, s1.v, s1.w}, S2[4] = {s2.rho, s2.u, s2.v, s2.w};
     R pi[4], pn[4], p0[4], g3[12];
-    if (oc.y > a.nc) {
+    if (geo.bc_branch != R(0)) {
         const int b = oc.y - a.nc;
         const Vec4<R> bc = a.bc_val[b];
         const bool rd = a.bc_rho_type[b] == 1, vd = a.bc_vel_type[b] == 1;
@@ -329,8 +329,9 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
 
 // Interior faces of an axis-aligned mesh: faces [0, nfx) x, [nfx, nfx+nfy) y,
 // the rest z; warps never mix axes except at the two range boundaries.
-template <typename R>
-__global__ void __launch_bounds__(128, 4) k_face_flux(FluidArgs<R> a) {
+// TB threads per block, 512 / TB blocks per SM (at most 128 registers a thread).
+template <typename R, int TB>
+__global__ void __launch_bounds__(TB, 512 / TB) k_face_flux(FluidArgs<R> a) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= a.ni) return;
     Vec4<R> out;
@@ -343,8 +344,8 @@ __global__ void __launch_bounds__(128, 4) k_face_flux(FluidArgs<R> a) {
 // Boundary faces (always) and the interior faces of meshes that are not axis
 // aligned: the general-normal reconstruction.  `first` is ni (axis-aligned
 // meshes) or 0.
-template <typename R>
-__global__ void __launch_bounds__(128) k_face_flux_general(FluidArgs<R> a, int first) {
+template <typename R, int TB>
+__global__ void __launch_bounds__(TB) k_face_flux_general(FluidArgs<R> a, int first) {
     const int f = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= a.nf) return;
     a.flux[f] = general_face_flux<R>(a, f, f >= a.ni);
@@ -352,9 +353,9 @@ __global__ void __launch_bounds__(128) k_face_flux_general(FluidArgs<R> a, int f
 
 // ------------------------------------------------------------------ K3 ----
 
-template <typename R>
-__global__ void __launch_bounds__(256) k_cell_update(FluidArgs<R> a) {
-    __shared__ double sh[4][8];
+template <typename R, int TB>
+__global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
+    __shared__ double sh[4][TB / 32];
     __shared__ bool last_block;
     double sq[4] = {0, 0, 0, 0};
     unsigned int flag = 0;
@@ -379,13 +380,16 @@ __global__ void __launch_bounds__(256) k_cell_update(FluidArgs<R> a) {
         }
         double fx = a.force[0], fy = a.force[1], fz = a.force[2];
         if (a.n_membranes > 0) {
-            const int ci = i % a.grid_nx, cj = (i / a.grid_nx) % a.grid_ny, ck = i / (a.grid_nx * a.grid_ny);
+            const int inst = a.cell_instance ? __ldg(a.cell_instance + i) : 0;
+            const InstanceGrid g = reinterpret_cast<const InstanceGrid *>(a.instances)[inst];
+            const int li = i - g.cell0;
+            const int ci = li % g.nx, cj = (li / g.nx) % g.ny, ck = li / (g.nx * g.ny);
             const MembraneScalars *ms = (const MembraneScalars *)a.membrane_scalars;
-            for (int m = 0; m < a.n_membranes; m++) {
+            for (int m = g.mem0; m < g.mem1; m++) {
                 const int px = ci - ms[m].patch_lo[0], py = cj - ms[m].patch_lo[1], pz = ck - ms[m].patch_lo[2];
                 if (ms[m].patch_cells > 0 && px >= 0 && py >= 0 && pz >= 0 && px < ms[m].patch_dim[0] &&
                     py < ms[m].patch_dim[1] && pz < ms[m].patch_dim[2]) {
-                    const double *pf = a.patch_force + ((size_t)m * kMaxPatchCells +
+                    const double *pf = a.patch_force + ((size_t)ms[m].patch_off +
                                                         (px + ms[m].patch_dim[0] * (py + ms[m].patch_dim[1] * pz))) * 3;
                     fx = fx + pf[0];
                     fy = fy + pf[1];
@@ -494,20 +498,40 @@ __global__ void k_unpack_state(FluidArgs<R> a, double *__restrict__ stage) {
 // ------------------------------------------------------------ launchers ----
 
 template <typename R> int k3_grid(const FluidArgs<R> &a) {
-    int g = (a.nc + 255) / 256;
-    return g < kK3MaxBlocks ? g : kK3MaxBlocks;
+    const int g = (a.nc + a.tb_update - 1) / a.tb_update;
+    return g < a.update_blocks ? g : a.update_blocks;
 }
 
 template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStream_t s) {
-    k_cell_gradients<R><<<(a.nc + 255) / 256, 256, 0, s>>>(a);
+    const int tb = a.tb_grad, g = (a.nc + tb - 1) / tb;
+    if (tb == 128) k_cell_gradients<R, 128><<<g, 128, 0, s>>>(a);
+    else if (tb == 512) k_cell_gradients<R, 512><<<g, 512, 0, s>>>(a);
+    else k_cell_gradients<R, 256><<<g, 256, 0, s>>>(a);
+}
+template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s) {
+    if (!a.axis_aligned || a.ni == 0) return;
+    const int tb = a.tb_flux, g = (a.ni + tb - 1) / tb;
+    if (tb == 64) k_face_flux<R, 64><<<g, 64, 0, s>>>(a);
+    else if (tb == 256) k_face_flux<R, 256><<<g, 256, 0, s>>>(a);
+    else k_face_flux<R, 128><<<g, 128, 0, s>>>(a);
+}
+template <typename R> void launch_fluid_flux_general(const FluidArgs<R> &a, cudaStream_t s) {
+    const int first = a.axis_aligned ? a.ni : 0;
+    if (a.nf <= first) return;
+    const int tb = a.tb_gen, g = (a.nf - first + tb - 1) / tb;
+    if (tb == 64) k_face_flux_general<R, 64><<<g, 64, 0, s>>>(a, first);
+    else if (tb == 256) k_face_flux_general<R, 256><<<g, 256, 0, s>>>(a, first);
+    else k_face_flux_general<R, 128><<<g, 128, 0, s>>>(a, first);
 }
 template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s) {
-    const int first = a.axis_aligned ? a.ni : 0;
-    if (a.axis_aligned && a.ni > 0) k_face_flux<R><<<(a.ni + 127) / 128, 128, 0, s>>>(a);
-    if (a.nf > first) k_face_flux_general<R><<<(a.nf - first + 127) / 128, 128, 0, s>>>(a, first);
+    launch_fluid_flux_axis<R>(a, s);
+    launch_fluid_flux_general<R>(a, s);
 }
 template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s) {
-    k_cell_update<R><<<k3_grid(a), 256, 0, s>>>(a);
+    const int tb = a.tb_update, g = k3_grid(a);
+    if (tb == 128) k_cell_update<R, 128><<<g, 128, 0, s>>>(a);
+    else if (tb == 512) k_cell_update<R, 512><<<g, 512, 0, s>>>(a);
+    else k_cell_update<R, 256><<<g, 256, 0, s>>>(a);
 }
 
 template <typename R> void launch_pack_state(const FluidArgs<R> &a, const double *stage, cudaStream_t s) {
@@ -523,6 +547,10 @@ template void launch_unpack_state<float>(const FluidArgs<float> &, double *, cud
 
 template void launch_fluid_gradients<double>(const FluidArgs<double> &, cudaStream_t);
 template void launch_fluid_flux<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_flux_axis<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_flux_general<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_flux_axis<float>(const FluidArgs<float> &, cudaStream_t);
+template void launch_fluid_flux_general<float>(const FluidArgs<float> &, cudaStream_t);
 template void launch_fluid_update<double>(const FluidArgs<double> &, cudaStream_t);
 template void launch_fluid_gradients<float>(const FluidArgs<float> &, cudaStream_t);
 template void launch_fluid_flux<float>(const FluidArgs<float> &, cudaStream_t);

@@ -102,8 +102,12 @@ template <typename R> struct alignas(4 * sizeof(R)) AxisFace {
 // Face geometry of a general face (boundary faces always; interior faces of
 // meshes that are not axis aligned): area, dt, unit normal, and the full
 // vectors t1 = c_owner - x_face, t2 = c_neighbour - x_face (LBFS.cu:335-337).
+// bc_branch is 1 on boundary faces that take the boundary reconstruction: the
+// reference tests neighbour > n_cells, so the face of the first ghost cell
+// (index n_cells) takes the interior branch; in an ensemble, the face of each
+// instance's first ghost does.
 template <typename R> struct alignas(16) GenFace {
-    R area, dt, nx, ny, nz, t1x, t1y, t1z, t2x, t2y, t2z, pad;
+    R area, dt, nx, ny, nz, t1x, t1y, t1z, t2x, t2y, t2z, bc_branch;
 };
 
 // Least-squares geometry of one cell: RHS weights of the 6 stencil entries
@@ -146,15 +150,19 @@ template <typename R> struct FluidArgs {
     const double *cell_volume;   // [nc]
     double4 *t1;                 // [nc] (u, v, w, rho) conservative accumulator, FP64
     double *res_out;             // [4*nc] residuals kept for parity checks (null = not stored)
-    // IBM patches (one per membrane)
-    int n_membranes, grid_nx, grid_ny;
+    // IBM patches (one per membrane), grouped by ensemble instance
+    int n_membranes;
     const void *membrane_scalars;  // MembraneScalars[n_membranes]
+    const void *instances;       // InstanceGrid[n_instances]
+    const int *cell_instance;    // [nc] instance of each cell; null with one instance
     const double *patch_force;   // [n_membranes * kMaxPatchCells * 3]
     // reductions and flags
     double *partials;            // [4 * gridDim of K3]
     unsigned int *ticket;
     double *residual_sums;       // [4] sum of squares of the last step
     unsigned int *flags;
+    // launch shape (read by the host launchers only; lbfs_autotune picks it)
+    int tb_grad, tb_flux, tb_gen, tb_update, update_blocks;
 };
 
 }  // namespace lbfs

@@ -31,7 +31,7 @@ struct MembraneScalars {
     double bbox_lo[3], bbox_hi[3];   // node coordinate bounds (interior viscosity test)
     int patch_lo[3], patch_dim[3];   // IBM patch: first cell and extent per axis
     int patch_cells;                 // product of patch_dim (0 when the patch overflowed)
-    int pad;
+    int patch_off;                   // first cell of this membrane's slice of the patch arrays (set at create)
 };
 
 // Per-membrane constants (moduli) and ranges into the concatenated arrays.
@@ -43,6 +43,17 @@ struct MembraneConst {
     double global_bending_modulus, local_bending_modulus, membrane_thickness, viscosity;
     double wlc_ratio, curvature_ratio, volume_ratio, internal_viscosity_ratio, reference_length;
     int pivkin_length, sphere_reference;
+    // IBM grid of the membrane's instance
+    int cell0, gnx, gny, gnz;
+    double gorigin[3], gdx, gdh;
+    int instance, patch_bound;  // patch cells the spread launch covers
+};
+
+// One ensemble instance as the kernels see it.
+struct InstanceGrid {
+    int cell0, nx, ny, nz;
+    int mem0, mem1;  // membranes [mem0, mem1) live in this instance
+    int pad0, pad1;
 };
 
 }  // namespace lbfs

@@ -8,10 +8,14 @@
 
 namespace lbfs {
 
-constexpr int kK3MaxBlocks = 148 * 8;
+constexpr int kK3MaxBlocks = 148 * 8;      // default grid cap of the cell update (grid-stride)
+constexpr int kSpreadMaxBlocks = 148 * 8;  // default spread grid cap (grid-stride over the tiles)
+constexpr int kK3BlocksLimit = LBFS_MAX_UPDATE_BLOCKS;  // partial-sum slots allocated for the update
 
 template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s);
+template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s);
+template <typename R> void launch_fluid_flux_general(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s);
 // stage = 4 planes of n_cells doubles (rho, u, v, w); pack also resets soln_t1
 // to the primitive state (Solver_gpu.cu:746)
@@ -43,9 +47,7 @@ struct MembraneArgs {
     // fluid state (read) and IBM grid
     const void *state;           // Vec4<R>[nc]
     int state_is_float;
-    int nc, grid_nx, grid_ny, grid_nz;
-    double origin[3];
-    double delta_x;
+    int nc;
     // membranes
     const MembraneConst *mc;     // [n_membranes]
     MembraneScalars *ms;         // [n_membranes]
@@ -59,16 +61,21 @@ struct MembraneArgs {
     double *contour, *kspring, *curv, *curv0, *angle0, *area0, *area; // per spring (area, area0: 2 per spring)
     double *contrib;             // [12*total_springs] per-spring node forces (scratch)
     unsigned long long *keys;    // [total_nodes] bin keys (scratch)
-    double *patch_force;         // [n_membranes * kMaxPatchCells * 3]
+    double *patch_force;         // [sum of patch_bound * 3], membrane m from cell ms[m].patch_off
     unsigned int *flags;
     int sort_capacity;           // power of two >= nodes of the largest membrane
     int total_nodes, total_springs;
     const int *spring_mem;       // [total_springs] membrane of each spring
     int *node_base;              // [3*total_nodes] first stencil cell per axis (scratch)
     double *node_w;              // [12*total_nodes] 1D stencil weights per axis (scratch)
-    int *bin_start;              // [n_membranes * (kMaxPatchCells + 1)] first sorted node of each bin (scratch)
+    int *bin_start;              // [sum of (patch_bound + 1)] first sorted node of each bin, from patch_off + m
+    int *tile_start;             // [n_membranes + 1] first spread tile of each membrane (prefix over patches)
+    unsigned int *sort_ticket;   // membranes whose patch is known in this launch; zero between launches
+    int spread_blocks;           // grid of the spread kernel (grid-stride over the tiles)
     SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order (scratch)
     int max_springs;             // springs of the largest membrane
+    int max_patch_bound;         // largest patch_bound over the membranes (spread grid)
+    const int *node_mem;         // [total_nodes] membrane of each node
     double *mad_partials;        // [n_membranes * kMaxSpringBlocks] (scratch)
     unsigned int *mad_ticket;    // [n_membranes], zero between launches
 };
@@ -85,13 +92,17 @@ struct ViscArgs {
     const double *centroid;      // [3*nc]
     const MembraneConst *mc;
     const MembraneScalars *ms;
+    const InstanceGrid *instances;
+    const int *cell_instance;    // null with one instance
     const int *tri;
     const double *x, *y, *z;
-    double delta_h;
     void *visc_factor;           // R[nc]
     int visc_is_float;
 };
 
 void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s);
+// single phases of the membrane chain (autotuner): node sort + patches, spread
+void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s);
+void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s);
 
 }  // namespace lbfs

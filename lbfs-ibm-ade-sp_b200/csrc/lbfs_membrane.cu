@@ -121,11 +121,12 @@ struct Stencil {
     double rx, ry, rz;
     int i0, j0, k0;
 };
-__device__ __forceinline__ Stencil node_stencil(const MembraneArgs &a, double x, double y, double z) {
+__device__ __forceinline__ Stencil node_stencil(const MembraneArgs &a, const MembraneConst &mc, double x, double y,
+                                                double z) {
     Stencil s;
-    s.rx = (x - a.origin[0]) / a.delta_x;
-    s.ry = fabs((y - a.origin[1]) / a.delta_x);
-    s.rz = fabs((z - a.origin[2]) / a.delta_x);
+    s.rx = (x - mc.gorigin[0]) / mc.gdx;
+    s.ry = fabs((y - mc.gorigin[1]) / mc.gdx);
+    s.rz = fabs((z - mc.gorigin[2]) / mc.gdx);
     if (a.ibm_stencil == LBFS_IBM_PESKIN4) {
         s.i0 = (int)floor(s.rx - 0.5) - 1;
         s.j0 = (int)floor(s.ry - 0.5) - 1;
@@ -353,16 +354,19 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
     const int lane = threadIdx.x & 31;
     const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (n >= A.total_nodes) return;
+    const MembraneConst &mc = A.mc[A.node_mem[n]];
     const double x = A.x[n], y = A.y[n], z = A.z[n];
-    const Stencil st = node_stencil(A, x, y, z);
+    const Stencil st = node_stencil(A, mc, x, y, z);
+    const int n_inst = mc.gnx * mc.gny * mc.gnz;
     const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
     const int cells = S * S * S;
     double v[3] = {0.0, 0.0, 0.0};
     for (int c = lane; c < cells; c += 32) {
         // cell c of the stencil, z fastest as in the reference's i, j, k loop nest
         const int i = st.i0 + c / (S * S), j = st.j0 + (c / S) % S, k = st.k0 + c % S;
-        const int idx = i + j * A.grid_nx + k * A.grid_ny * A.grid_nx;
-        if (idx < A.nc && idx >= 0) {
+        const int lidx = i + j * mc.gnx + k * mc.gny * mc.gnx;
+        if (lidx < n_inst && lidx >= 0) {
+            const int idx = mc.cell0 + lidx;
             const double wx = stencil_weight(A.ibm_stencil, i + 0.5 - st.rx);
             const double wy = stencil_weight(A.ibm_stencil, j + 0.5 - st.ry);
             const double wz = stencil_weight(A.ibm_stencil, k + 0.5 - st.rz);
@@ -496,14 +500,14 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     const MembraneConst mc = A.mc[m];
     MembraneScalars *ms = A.ms + m;
     const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
-    const int gn[3] = {A.grid_nx, A.grid_ny, A.grid_nz};
+    const int gn[3] = {mc.gnx, mc.gny, mc.gnz};
     double v[12];
     for (int c = 0; c < 3; c++) { v[c] = 1e300; v[3 + c] = 1e300; v[6 + c] = 1e300; v[9 + c] = 1e300; }
     unsigned int range_flag = 0;
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
         const int n = mc.node0 + ln;
         const double p[3] = {A.x[n], A.y[n], A.z[n]};
-        const Stencil st = node_stencil(A, p[0], p[1], p[2]);
+        const Stencil st = node_stencil(A, mc, p[0], p[1], p[2]);
         const int b[3] = {st.i0, st.j0, st.k0};
         const double r[3] = {st.rx, st.ry, st.rz};
         double *w = A.node_w + 12 * (size_t)n;
@@ -538,8 +542,9 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         pdim[c] = bdim[c] + S - 1;
     }
     const long long pcells = (long long)pdim[0] * pdim[1] * pdim[2];
-    const bool overflow = pcells > kMaxPatchCells || mc.n_nodes == 0;
+    const bool overflow = pcells > mc.patch_bound || mc.n_nodes == 0;
     if (range_flag) atomicOr(A.flags, range_flag);
+    __shared__ bool last_sorted;
     if (threadIdx.x == 0) {
         for (int c = 0; c < 3; c++) {
             ms->bbox_lo[c] = red[c];
@@ -549,8 +554,37 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         }
         ms->patch_cells = overflow ? 0 : (int)pcells;
         if (overflow) atomicOr(A.flags, LBFS_FLAG_IBM_RANGE);
+        __threadfence();
+        last_sorted = atomicAdd(A.sort_ticket, 1u) == gridDim.x - 1;
     }
-    if (overflow) return;
+    __syncthreads();
+    if (last_sorted) {
+        // every patch is known: spread tiles of 128 cells, prefix over the membranes
+        __threadfence();
+        __shared__ int scan[kMembraneThreads];
+        const int M = gridDim.x;
+        const int per = (M + blockDim.x - 1) / blockDim.x;
+        const int m0 = min(M, (int)threadIdx.x * per), m1 = min(M, m0 + per);
+        int local = 0;
+        for (int q = m0; q < m1; q++) local += (__ldcg(&A.ms[q].patch_cells) + 127) / 128;
+        scan[threadIdx.x] = local;
+        __syncthreads();
+        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+            const int v = threadIdx.x >= (unsigned)o ? scan[threadIdx.x - o] : 0;
+            __syncthreads();
+            scan[threadIdx.x] += v;
+            __syncthreads();
+        }
+        int run = scan[threadIdx.x] - local;
+        for (int q = m0; q < m1; q++) {
+            A.tile_start[q] = run;
+            run += (__ldcg(&A.ms[q].patch_cells) + 127) / 128;
+        }
+        if (threadIdx.x == blockDim.x - 1) {
+            A.tile_start[M] = scan[threadIdx.x];
+            *A.sort_ticket = 0u;
+        }
+    }
     int npad = 1;
     while (npad < mc.n_nodes) npad <<= 1;
     for (int t = threadIdx.x; t < npad; t += blockDim.x) {
@@ -577,7 +611,7 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         }
     }
     const int nbins = bdim[0] * bdim[1] * bdim[2];
-    int *bin_start = A.bin_start + (size_t)m * (kMaxPatchCells + 1);
+    int *bin_start = A.bin_start + (size_t)ms->patch_off + m;
     for (int b = threadIdx.x; b <= nbins; b += blockDim.x) {
         int lo = 0, hi = mc.n_nodes;
         while (lo < hi) {
@@ -602,19 +636,17 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
 // (bin, node) order, the contributions of the nodes whose stencil covers it.
 // The nodes of one row of bins are contiguous in the sorted order.
 template <int S>
-__global__ void __launch_bounds__(128) k_mem_spread(MembraneArgs A) {
-    const int m = blockIdx.y;
-    const int pc = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void spread_cell(const MembraneArgs &A, int m, int pc) {
     const MembraneScalars &ms = A.ms[m];
-    if (pc >= ms.patch_cells) return;
-    const int node0 = A.mc[m].node0;
+    const MembraneConst &mc = A.mc[m];
+    const int node0 = mc.node0;
     const int pdim[3] = {ms.patch_dim[0], ms.patch_dim[1], ms.patch_dim[2]};
     const int bdim[3] = {pdim[0] - S + 1, pdim[1] - S + 1, pdim[2] - S + 1};
     const int px = pc % pdim[0], py = (pc / pdim[0]) % pdim[1], pz = pc / (pdim[0] * pdim[1]);
     const int ci = ms.patch_lo[0] + px, cj = ms.patch_lo[1] + py, ck = ms.patch_lo[2] + pz;
-    const int *bin_start = A.bin_start + (size_t)m * (kMaxPatchCells + 1);
+    const int *bin_start = A.bin_start + (size_t)ms.patch_off + m;
     const SpreadRec *rec = A.spread_rec + node0;
-    const double inv3 = 1 / A.delta_x / A.delta_x / A.delta_x;
+    const double inv3 = 1 / mc.gdx / mc.gdx / mc.gdx;
     const int bx0 = max(px - S + 1, 0), bx1 = min(px, bdim[0] - 1);
     int lo[S * S], hi[S * S];
 #pragma unroll
@@ -637,25 +669,48 @@ __global__ void __launch_bounds__(128) k_mem_spread(MembraneArgs A) {
             f[2] += A.fz[n] * wx * wy * wz * inv3;
         }
     }
-    double *pf = A.patch_force + ((size_t)m * kMaxPatchCells + pc) * 3;
+    double *pf = A.patch_force + ((size_t)ms.patch_off + pc) * 3;
     pf[0] = f[0];
     pf[1] = f[1];
     pf[2] = f[2];
+}
+
+// Grid-stride over the spread tiles of all membranes (128 patch cells each,
+// numbered by the prefix the sort kernel wrote): a fixed grid however many
+// membranes and patch sizes an ensemble has.
+template <int S>
+__global__ void __launch_bounds__(128) k_mem_spread(MembraneArgs A) {
+    const int M = A.n_membranes;
+    const int total = __ldg(A.tile_start + M);
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        int lo = 0, hi = M;  // membrane m with tile_start[m] <= t < tile_start[m + 1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(A.tile_start + mid) <= t) lo = mid;
+            else hi = mid;
+        }
+        const int pc = (t - __ldg(A.tile_start + lo)) * 128 + threadIdx.x;
+        if (pc < A.ms[lo].patch_cells) spread_cell<S>(A, lo, pc);
+    }
 }
 
 // ---- interior viscosity (update_interior_viscosities_plucker, immersed_boundary_method.cu:389-527) ----
 template <typename R>
 __global__ void k_interior_viscosity(ViscArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nc || i == 0) return;  // the reference skips cell 0
+    if (i >= a.nc) return;
+    const int inst = a.cell_instance ? a.cell_instance[i] : 0;
+    const InstanceGrid g = a.instances[inst];
+    if (i == g.cell0) return;  // the reference skips cell 0 (of its mesh)
     const D3 cc = d3(a.centroid[3 * i], a.centroid[3 * i + 1], a.centroid[3 * i + 2]);
     const double pi = acos(-1.0);
-    for (int m = 0; m < a.n_membranes; m++) {
+    for (int m = g.mem0; m < g.mem1; m++) {
         const MembraneScalars ms = a.ms[m];
         const MembraneConst mc = a.mc[m];
-        const double xl = ms.bbox_lo[0] - 2 * a.delta_h, xh = ms.bbox_hi[0] + 2 * a.delta_h;
-        const double yl = ms.bbox_lo[1] - 2 * a.delta_h, yh = ms.bbox_hi[1] + 2 * a.delta_h;
-        const double zl = ms.bbox_lo[2] - 2 * a.delta_h, zh = ms.bbox_hi[2] + 2 * a.delta_h;
+        const double dh = mc.gdh;
+        const double xl = ms.bbox_lo[0] - 2 * dh, xh = ms.bbox_hi[0] + 2 * dh;
+        const double yl = ms.bbox_lo[1] - 2 * dh, yh = ms.bbox_hi[1] + 2 * dh;
+        const double zl = ms.bbox_lo[2] - 2 * dh, zh = ms.bbox_hi[2] + 2 * dh;
         if (!(cc.x >= xl && cc.x <= xh && cc.y >= yl && cc.y <= yh && cc.z >= zl && cc.z <= zh)) continue;
         // ray from the centroid along +x to x = xh; Plucker side tests against each triangle edge
         const double pc0 = cc.x * cc.y - xh * cc.y, pc1 = cc.x * cc.z - xh * cc.z, pc2 = cc.x - xh;
@@ -682,8 +737,7 @@ __global__ void k_interior_viscosity(ViscArgs a) {
         }
         const bool inside = (crossings % 2) != 0;
         const double r = mc.internal_viscosity_ratio;
-        const double factor =
-            2.0 * fmin(0.5, (min_distance * 0.5 / a.delta_h + 1.0 / pi * sin(pi * min_distance / a.delta_h) * 0.5));
+        const double factor = 2.0 * fmin(0.5, (min_distance * 0.5 / dh + 1.0 / pi * sin(pi * min_distance / dh) * 0.5));
         const double visc = inside ? (r + 1.0) + (r - 1.0) * factor : (r + 1.0) + (1.0 - r) * factor;
         ((R *)a.visc_factor)[i] = (R)(visc * 0.5);
     }
@@ -744,10 +798,21 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
     launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
     if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
-    const dim3 grid((kMaxPatchCells + 127) / 128, a.n_membranes);
+    const dim3 grid(a.spread_blocks);
     if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(128), 0, s, a);
     else launch_hi(k_mem_spread<2>, grid, dim3(128), 0, s, a);
     return 5;
+}
+
+void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s) {
+    const size_t smem = (size_t)(a.sort_capacity > 0 ? a.sort_capacity : 1) * sizeof(unsigned long long);
+    launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, s, a);
+}
+
+void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s) {
+    const dim3 grid(a.spread_blocks);
+    if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(128), 0, s, a);
+    else launch_hi(k_mem_spread<2>, grid, dim3(128), 0, s, a);
 }
 
 void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s) {

@@ -12,6 +12,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
+#include <initializer_list>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -73,6 +75,10 @@ struct lbfs_solver {
     bool graph_phase_recorded[kPhases] = {};  // phases recorded by one replay of the graph
     // staging buffer for host <-> device state transfers: rho, u, v, w planes
     double *d_stage = nullptr;
+    // ensemble instances (one when the mesh is a single case)
+    std::vector<lbfs_grid_desc> grids;
+    std::vector<InstanceGrid> inst;
+    long long total_patch = 0;  // cells of all IBM patch slices
 
     template <typename T> int alloc(T **p, size_t count) {
         void *q = nullptr;
@@ -191,6 +197,18 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         }
     }
     const int gf0 = a.axis_aligned ? ni : 0;
+    // first ghost of every instance: its face takes the interior branch
+    std::vector<char> first_ghost(nb, 0);
+    {
+        std::vector<int> starts;
+        for (const lbfs_grid_desc &g : s->grids) starts.push_back(g.cell0);
+        std::vector<char> seen(starts.size(), 0);
+        for (int b = 0; b < nb; b++) {
+            const int o = m->owner[ni + b];
+            const size_t k = std::upper_bound(starts.begin(), starts.end(), o) - starts.begin() - 1;
+            if (!seen[k]) { seen[k] = 1; first_ghost[b] = 1; }
+        }
+    }
     std::vector<GenFace<R>> gen(nf - gf0);
     for (int f = gf0; f < nf; f++) {
         const int o = m->owner[f], n = m->neighbour[f];
@@ -200,7 +218,7 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         g.nx = (R)fn[3 * f]; g.ny = (R)fn[3 * f + 1]; g.nz = (R)fn[3 * f + 2];
         g.t1x = (R)(cen[3 * o] - fc[3 * f]); g.t1y = (R)(cen[3 * o + 1] - fc[3 * f + 1]); g.t1z = (R)(cen[3 * o + 2] - fc[3 * f + 2]);
         g.t2x = (R)(cen[3 * n] - fc[3 * f]); g.t2y = (R)(cen[3 * n + 1] - fc[3 * f + 1]); g.t2z = (R)(cen[3 * n + 2] - fc[3 * f + 2]);
-        g.pad = 0;
+        g.bc_branch = (R)((f >= ni && !first_ghost[f - ni]) ? 1 : 0);
         gen[f - gf0] = g;
     }
     // K3: signed face list per cell, faces in increasing index order
@@ -252,7 +270,7 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     a.state = d_state; a.grad = d_grad; a.flux = d_flux; a.t1 = d_t1;
     double *d_partials, *d_rsum;
     unsigned int *d_ticket, *d_flags;
-    if ((rc = s->alloc(&d_partials, 4 * (size_t)kK3MaxBlocks)) || (rc = s->alloc(&d_rsum, 4)) ||
+    if ((rc = s->alloc(&d_partials, 4 * (size_t)kK3BlocksLimit)) || (rc = s->alloc(&d_rsum, 4)) ||
         (rc = s->alloc(&d_ticket, 1)) || (rc = s->alloc(&d_flags, 1)))
         return rc;
     LBFS_CUDA(cudaMemset(d_ticket, 0, sizeof(unsigned int)));
@@ -260,9 +278,45 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     LBFS_CUDA(cudaMemset(d_rsum, 0, 4 * sizeof(double)));
     a.partials = d_partials; a.residual_sums = d_rsum; a.ticket = d_ticket; a.flags = d_flags;
     a.res_out = nullptr;
-    a.grid_nx = (int)(m->length[0] / m->delta_x);
-    a.grid_ny = (int)(m->length[1] / m->delta_x);
+    a.tb_grad = 256; a.tb_flux = 128; a.tb_gen = 128; a.tb_update = 256; a.update_blocks = kK3MaxBlocks;
     a.n_membranes = 0;
+    a.instances = nullptr;
+    a.cell_instance = nullptr;
+    return LBFS_OK;
+}
+
+// Ensemble instance table: the descriptor's instances, or one instance covering
+// the whole mesh from origin/length/delta_x/delta_h.
+int setup_instances(lbfs_solver *s, const lbfs_mesh_desc *m) {
+    std::vector<lbfs_grid_desc> gd;
+    if (m->n_instances < 0) return set_error(LBFS_ERR_ARG, "negative instance count");
+    if (m->n_instances > 0) {
+        if (!m->instances) return set_error(LBFS_ERR_ARG, "instance table is null");
+        gd.assign(m->instances, m->instances + m->n_instances);
+    } else {
+        lbfs_grid_desc g{};
+        g.cell0 = 0; g.n_cells = m->n_cells;
+        for (int c = 0; c < 3; c++) { g.origin[c] = m->origin[c]; g.length[c] = m->length[c]; }
+        g.delta_x = m->delta_x; g.delta_h = m->delta_h;
+        gd.push_back(g);
+    }
+    int next = 0;
+    s->grids = gd;
+    s->inst.resize(gd.size());
+    for (size_t k = 0; k < gd.size(); k++) {
+        const lbfs_grid_desc &g = gd[k];
+        if (g.cell0 != next || g.n_cells <= 0)
+            return set_error(LBFS_ERR_ARG, "instances must be contiguous, non-empty cell ranges in order");
+        next += g.n_cells;
+        InstanceGrid &q = s->inst[k];
+        q.cell0 = g.cell0;
+        q.nx = g.delta_x > 0 ? (int)(g.length[0] / g.delta_x) : 0;
+        q.ny = g.delta_x > 0 ? (int)(g.length[1] / g.delta_x) : 0;
+        q.nz = g.delta_x > 0 ? (int)(g.length[2] / g.delta_x) : 0;
+        q.mem0 = q.mem1 = 0;
+        q.pad0 = q.pad1 = 0;
+    }
+    if (next != m->n_cells) return set_error(LBFS_ERR_ARG, "instances do not cover the interior cells");
     return LBFS_OK;
 }
 
@@ -273,16 +327,19 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     ma.ibm_stencil = p.ibm_stencil;
     ma.delta_t = p.delta_t;
     ma.nc = m->n_cells;
-    ma.grid_nx = (int)(m->length[0] / m->delta_x);
-    ma.grid_ny = (int)(m->length[1] / m->delta_x);
-    ma.grid_nz = (int)(m->length[2] / m->delta_x);
-    for (int c = 0; c < 3; c++) ma.origin[c] = m->origin[c];
-    ma.delta_x = m->delta_x;
     ma.state_is_float = s->fp32 ? 1 : 0;
     if (n_rbc == 0) return LBFS_OK;
-    if ((long long)ma.grid_nx * ma.grid_ny * ma.grid_nz != m->n_cells)
-        return set_error(LBFS_ERR_ARG, "membranes need the lexicographic uniform grid the IBM stencils index "
-                                       "(length / delta_x cells per axis)");
+    const int n_inst = (int)s->inst.size();
+    for (int r = 0; r < n_rbc; r++) {
+        const int k = rbc[r].instance;
+        if (k < 0 || k >= n_inst) return set_error(LBFS_ERR_ARG, "membrane instance out of range");
+        if (r > 0 && k < rbc[r - 1].instance)
+            return set_error(LBFS_ERR_ARG, "membranes must be grouped by instance, in increasing order");
+        const InstanceGrid &g = s->inst[k];
+        if (!(s->grids[k].delta_x > 0) || (long long)g.nx * g.ny * g.nz != s->grids[k].n_cells)
+            return set_error(LBFS_ERR_ARG, "membranes need the lexicographic uniform grid the IBM stencils index "
+                                           "(length / delta_x cells per axis)");
+    }
     std::vector<MembraneConst> mc(n_rbc);
     std::vector<int> tri, spr;
     std::vector<double> sf, init;
@@ -305,6 +362,20 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         c.curvature_ratio = d.curvature_ratio; c.volume_ratio = d.volume_ratio;
         c.internal_viscosity_ratio = d.internal_viscosity_ratio; c.reference_length = d.reference_length;
         c.pivkin_length = d.pivkin_length; c.sphere_reference = d.sphere_reference;
+        const InstanceGrid &g = s->inst[d.instance];
+        const lbfs_grid_desc &gd = s->grids[d.instance];
+        c.instance = d.instance;
+        c.cell0 = g.cell0; c.gnx = g.nx; c.gny = g.ny; c.gnz = g.nz;
+        for (int q = 0; q < 3; q++) c.gorigin[q] = gd.origin[q];
+        c.gdx = gd.delta_x; c.gdh = gd.delta_h;
+        {
+            // a patch of in-range stencils lies inside the instance's grid
+            const int S = p.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+            const long long cells = (long long)(g.nx + S - 1) * (g.ny + S - 1) * (g.nz + S - 1);
+            c.patch_bound = (int)std::min<long long>(kMaxPatchCells, cells);
+        }
+        if (s->inst[d.instance].mem1 == 0) s->inst[d.instance].mem0 = r;
+        s->inst[d.instance].mem1 = r + 1;
         for (int i = 0; i < 3 * d.n_tris; i++) {
             if (d.tri[i] < 0 || d.tri[i] >= d.n_nodes) return set_error(LBFS_ERR_ARG, "triangle index out of range");
             tri.push_back(d.tri[i] + s->total_nodes);
@@ -336,13 +407,34 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     std::vector<double> zeros_n(N, 0.0), zeros_s(S, 0.0), zeros_2s(2 * (size_t)S, 0.0);
     std::vector<MembraneScalars> msz(n_rbc);
     std::memset(msz.data(), 0, sizeof(MembraneScalars) * n_rbc);
+    long long total_patch = 0, spread_tiles = 0;
+    for (int r = 0; r < n_rbc; r++) {
+        msz[r].patch_off = (int)total_patch;
+        total_patch += mc[r].patch_bound;
+        spread_tiles += (mc[r].patch_bound + 127) / 128;
+    }
+    if (total_patch + n_rbc > INT32_MAX) return set_error(LBFS_ERR_LIMIT, "IBM patches exceed 2^31 cells in total");
+    s->total_patch = total_patch;
+    ma.spread_blocks = (int)std::max<long long>(1, std::min<long long>(spread_tiles, kSpreadMaxBlocks));
     int rc = 0;
-    std::vector<int> spring_mem(S);
-    for (int r = 0; r < n_rbc; r++)
+    std::vector<int> spring_mem(S), node_mem(N);
+    for (int r = 0; r < n_rbc; r++) {
         for (int q = 0; q < mc[r].n_springs; q++) spring_mem[mc[r].spring0 + q] = r;
+        for (int q = 0; q < mc[r].n_nodes; q++) node_mem[mc[r].node0 + q] = r;
+    }
+    std::vector<int> cell_inst;
+    if (n_inst > 1) {
+        cell_inst.resize(m->n_cells);
+        for (int k = 0; k < n_inst; k++)
+            for (int i = 0; i < s->grids[k].n_cells; i++) cell_inst[s->inst[k].cell0 + i] = k;
+    }
     ma.total_nodes = N;
     ma.total_springs = S;
-    MembraneConst *d_mc; MembraneScalars *d_ms; int *d_tri, *d_spr, *d_inc, *d_incs, *d_smem;
+    MembraneConst *d_mc; MembraneScalars *d_ms; int *d_tri, *d_spr, *d_inc, *d_incs, *d_smem, *d_nmem;
+    InstanceGrid *d_inst; int *d_cinst = nullptr;
+    if ((rc = s->upload(&d_inst, s->inst)) || (rc = s->upload(&d_nmem, node_mem)) ||
+        (n_inst > 1 && (rc = s->upload(&d_cinst, cell_inst))))
+        return rc;
     if ((rc = s->upload(&d_mc, mc)) || (rc = s->upload(&d_ms, msz)) || (rc = s->upload(&d_tri, tri)) ||
         (rc = s->upload(&d_spr, spr)) || (rc = s->upload(&d_inc, inc)) || (rc = s->upload(&d_incs, inc_start)) ||
         (rc = s->upload(&ma.x, x)) || (rc = s->upload(&ma.y, y)) || (rc = s->upload(&ma.z, z)) ||
@@ -352,17 +444,26 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         (rc = s->upload(&ma.curv, zeros_s)) || (rc = s->upload(&ma.curv0, zeros_s)) ||
         (rc = s->upload(&ma.angle0, zeros_s)) || (rc = s->upload(&ma.area0, zeros_2s)) ||
         (rc = s->upload(&ma.area, zeros_2s)) || (rc = s->alloc(&ma.contrib, 12 * (size_t)S)) ||
-        (rc = s->alloc(&ma.keys, N)) || (rc = s->alloc(&ma.patch_force, (size_t)n_rbc * kMaxPatchCells * 3)) ||
+        (rc = s->alloc(&ma.keys, N)) || (rc = s->alloc(&ma.patch_force, (size_t)total_patch * 3)) ||
         (rc = s->upload(&d_smem, spring_mem)) || (rc = s->alloc(&ma.node_base, 3 * (size_t)N)) ||
         (rc = s->alloc(&ma.node_w, 12 * (size_t)N)) ||
-        (rc = s->alloc(&ma.bin_start, (size_t)n_rbc * (kMaxPatchCells + 1))) ||
+        (rc = s->alloc(&ma.bin_start, (size_t)total_patch + n_rbc)) ||
+        (rc = s->alloc(&ma.tile_start, (size_t)n_rbc + 1)) || (rc = s->alloc(&ma.sort_ticket, 1)) ||
         (rc = s->alloc(&ma.spread_rec, (size_t)N)) ||
         (rc = s->alloc(&ma.mad_partials, (size_t)n_rbc * kMaxSpringBlocks)) ||
         (rc = s->alloc(&ma.mad_ticket, (size_t)n_rbc)))
         return rc;
     LBFS_CUDA(cudaMemset(ma.mad_ticket, 0, sizeof(unsigned int) * n_rbc));
+    LBFS_CUDA(cudaMemset(ma.sort_ticket, 0, sizeof(unsigned int)));
+    LBFS_CUDA(cudaMemset(ma.tile_start, 0, sizeof(int) * (n_rbc + 1)));
+    LBFS_CUDA(cudaMemset(ma.patch_force, 0, sizeof(double) * 3 * (size_t)total_patch));
     ma.max_springs = 0;
-    for (int r = 0; r < n_rbc; r++) ma.max_springs = std::max(ma.max_springs, mc[r].n_springs);
+    ma.max_patch_bound = 0;
+    for (int r = 0; r < n_rbc; r++) {
+        ma.max_springs = std::max(ma.max_springs, mc[r].n_springs);
+        ma.max_patch_bound = std::max(ma.max_patch_bound, mc[r].patch_bound);
+    }
+    ma.node_mem = d_nmem;
     ma.spring_mem = d_smem;
     ma.mc = d_mc; ma.ms = d_ms; ma.tri = d_tri; ma.spring = d_spr; ma.inc = d_inc; ma.inc_start = d_incs;
     ma.flags = s->fp32 ? s->f32.flags : s->f64.flags;
@@ -384,10 +485,13 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     s->f64.n_membranes = s->f32.n_membranes = n_rbc;
     s->f64.membrane_scalars = s->f32.membrane_scalars = d_ms;
     s->f64.patch_force = s->f32.patch_force = ma.patch_force;
+    s->f64.instances = s->f32.instances = d_inst;
+    s->f64.cell_instance = s->f32.cell_instance = d_cinst;
     // interior viscosity
     ViscArgs &va = s->va;
     va.nc = m->n_cells; va.n_membranes = n_rbc; va.centroid = s->d_centroid; va.mc = d_mc; va.ms = d_ms;
-    va.tri = d_tri; va.x = ma.x; va.y = ma.y; va.z = ma.z; va.delta_h = m->delta_h;
+    va.tri = d_tri; va.x = ma.x; va.y = ma.y; va.z = ma.z;
+    va.instances = d_inst; va.cell_instance = d_cinst;
     va.visc_factor = s->fp32 ? (void *)s->f32.visc_factor : (void *)s->f64.visc_factor;
     va.visc_is_float = s->fp32 ? 1 : 0;
     return LBFS_OK;
@@ -515,6 +619,7 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
         cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess)
         return fail(set_error(LBFS_ERR_CUDA, "stream/event creation failed"));
+    if ((rc = setup_instances(s, mesh))) return fail(rc);
     rc = s->fp32 ? setup_fluid<float>(s, mesh) : setup_fluid<double>(s, mesh);
     if (rc) return fail(rc);
     std::vector<double> centroid(mesh->cell_centroid, mesh->cell_centroid + 3 * (size_t)mesh->n_cells);
@@ -759,17 +864,21 @@ template <typename R> int get_field_t(lbfs_solver *s, int which, double *out) {
         if (s->n_membranes == 0) return LBFS_OK;
         std::vector<MembraneScalars> ms(s->n_membranes);
         LBFS_CUDA(cudaMemcpy(ms.data(), s->ma.ms, ms.size() * sizeof(MembraneScalars), cudaMemcpyDeviceToHost));
-        std::vector<double> pf((size_t)s->n_membranes * kMaxPatchCells * 3);
+        std::vector<double> pf((size_t)s->total_patch * 3);
         LBFS_CUDA(cudaMemcpy(pf.data(), s->ma.patch_force, pf.size() * sizeof(double), cudaMemcpyDeviceToHost));
-        for (int i = 0; i < nc; i++) {
-            const int ci = i % a.grid_nx, cj = (i / a.grid_nx) % a.grid_ny, ck = i / (a.grid_nx * a.grid_ny);
-            for (int m = 0; m < s->n_membranes; m++) {
-                const int px = ci - ms[m].patch_lo[0], py = cj - ms[m].patch_lo[1], pz = ck - ms[m].patch_lo[2];
-                if (ms[m].patch_cells > 0 && px >= 0 && py >= 0 && pz >= 0 && px < ms[m].patch_dim[0] &&
-                    py < ms[m].patch_dim[1] && pz < ms[m].patch_dim[2]) {
-                    const double *p = pf.data() + ((size_t)m * kMaxPatchCells +
-                                                    (px + ms[m].patch_dim[0] * (py + ms[m].patch_dim[1] * pz))) * 3;
-                    out[3 * i] += p[0]; out[3 * i + 1] += p[1]; out[3 * i + 2] += p[2];
+        for (int k = 0; k < (int)s->inst.size(); k++) {
+            const InstanceGrid &g = s->inst[k];
+            for (int i = g.cell0; i < g.cell0 + s->grids[k].n_cells; i++) {
+                const int li = i - g.cell0;
+                const int ci = li % g.nx, cj = (li / g.nx) % g.ny, ck = li / (g.nx * g.ny);
+                for (int m = g.mem0; m < g.mem1; m++) {
+                    const int px = ci - ms[m].patch_lo[0], py = cj - ms[m].patch_lo[1], pz = ck - ms[m].patch_lo[2];
+                    if (ms[m].patch_cells > 0 && px >= 0 && py >= 0 && pz >= 0 && px < ms[m].patch_dim[0] &&
+                        py < ms[m].patch_dim[1] && pz < ms[m].patch_dim[2]) {
+                        const double *p = pf.data() + ((size_t)ms[m].patch_off +
+                                                        (px + ms[m].patch_dim[0] * (py + ms[m].patch_dim[1] * pz))) * 3;
+                        out[3 * i] += p[0]; out[3 * i + 1] += p[1]; out[3 * i + 2] += p[2];
+                    }
                 }
             }
         }
@@ -840,4 +949,184 @@ extern "C" int lbfs_last_error(char *buf, int32_t len) {
     if (!buf || len <= 0) return LBFS_ERR_ARG;
     std::snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
     return LBFS_OK;
+}
+
+// ---- launch shapes and the autotuner ---------------------------------------
+
+namespace {
+
+template <typename R> void shape_to_args(lbfs_solver *s, const lbfs_launch_shape &sh) {
+    FluidArgs<R> &a = fluid<R>(s);
+    a.tb_grad = sh.gradient_threads; a.tb_flux = sh.flux_threads; a.tb_gen = sh.general_flux_threads;
+    a.tb_update = sh.update_threads; a.update_blocks = sh.update_blocks;
+    s->ma.spread_blocks = sh.spread_blocks;
+}
+
+template <typename R> lbfs_launch_shape args_to_shape(lbfs_solver *s) {
+    const FluidArgs<R> &a = fluid<R>(s);
+    lbfs_launch_shape sh{};
+    sh.gradient_threads = a.tb_grad; sh.flux_threads = a.tb_flux; sh.general_flux_threads = a.tb_gen;
+    sh.update_threads = a.tb_update; sh.update_blocks = a.update_blocks;
+    sh.spread_blocks = s->ma.spread_blocks > 0 ? s->ma.spread_blocks : 1;
+    return sh;
+}
+
+bool one_of(int v, std::initializer_list<int> set) {
+    for (int x : set) if (v == x) return true;
+    return false;
+}
+
+int check_shape(const lbfs_launch_shape &sh) {
+    if (!one_of(sh.gradient_threads, {128, 256, 512}) || !one_of(sh.flux_threads, {64, 128, 256}) ||
+        !one_of(sh.general_flux_threads, {64, 128, 256}) || !one_of(sh.update_threads, {128, 256, 512}))
+        return set_error(LBFS_ERR_ARG, "launch shape: block sizes must be 128/256/512 (gradients, update) or "
+                                       "64/128/256 (flux kernels)");
+    if (sh.update_blocks < 1 || sh.update_blocks > LBFS_MAX_UPDATE_BLOCKS || sh.spread_blocks < 1 ||
+        sh.spread_blocks > LBFS_MAX_SPREAD_BLOCKS)
+        return set_error(LBFS_ERR_ARG, "launch shape: grid caps out of range");
+    return LBFS_OK;
+}
+
+void drop_graph(lbfs_solver *s) {
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+}
+
+// Mean device time of `reps` launches of `launch` (after one untimed launch).
+template <typename F> int time_launches(lbfs_solver *s, int reps, cudaEvent_t e0, cudaEvent_t e1, F launch,
+                                        double *us) {
+    launch();
+    LBFS_CUDA(cudaEventRecord(e0, s->stream));
+    for (int r = 0; r < reps; r++) launch();
+    LBFS_CUDA(cudaEventRecord(e1, s->stream));
+    LBFS_CUDA(cudaEventSynchronize(e1));
+    LBFS_CUDA(cudaGetLastError());
+    float ms = 0;
+    LBFS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    *us = 1000.0 * ms / reps;
+    return LBFS_OK;
+}
+
+template <typename R> int autotune(lbfs_solver *s, int reps, lbfs_launch_shape *out) {
+    FluidArgs<R> &a = fluid<R>(s);
+    const size_t nt = (size_t)s->nc + s->nb;
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    // the update advances the state: keep a copy and put it back afterwards
+    void *keep_state = nullptr, *keep_t1 = nullptr, *keep_misc = nullptr;
+    LBFS_CUDA(cudaMalloc(&keep_state, sizeof(Vec4<R>) * nt));
+    LBFS_CUDA(cudaMalloc(&keep_t1, sizeof(double4) * s->nc));
+    LBFS_CUDA(cudaMalloc(&keep_misc, 64));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = LBFS_OK;
+    lbfs_launch_shape best = args_to_shape<R>(s);
+    auto run = [&]() -> int {
+        LBFS_CUDA(cudaEventCreate(&e0));
+        LBFS_CUDA(cudaEventCreate(&e1));
+        LBFS_CUDA(cudaMemcpyAsync(keep_state, a.state, sizeof(Vec4<R>) * nt, cudaMemcpyDeviceToDevice, s->stream));
+        LBFS_CUDA(cudaMemcpyAsync(keep_t1, a.t1, sizeof(double4) * s->nc, cudaMemcpyDeviceToDevice, s->stream));
+        LBFS_CUDA(cudaMemcpyAsync(keep_misc, a.residual_sums, 4 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+        LBFS_CUDA(cudaMemcpyAsync((char *)keep_misc + 32, a.flags, sizeof(unsigned int), cudaMemcpyDeviceToDevice,
+                                  s->stream));
+        double t = 0, tbest;
+        int r;
+        // gradients
+        tbest = 1e300;
+        for (int tb : {128, 256, 512}) {
+            a.tb_grad = tb;
+            if ((r = time_launches(s, reps, e0, e1, [&] { launch_fluid_gradients<R>(a, s->stream); }, &t))) return r;
+            if (t < tbest) { tbest = t; best.gradient_threads = tb; }
+        }
+        best.time_us[0] = tbest;
+        a.tb_grad = best.gradient_threads;
+        // interior (axis-aligned) faces, then the general-normal faces
+        if (a.axis_aligned && a.ni > 0) {
+            tbest = 1e300;
+            for (int tb : {64, 128, 256}) {
+                a.tb_flux = tb;
+                if ((r = time_launches(s, reps, e0, e1, [&] { launch_fluid_flux_axis<R>(a, s->stream); }, &t))) return r;
+                if (t < tbest) { tbest = t; best.flux_threads = tb; }
+            }
+            best.time_us[1] = tbest;
+            a.tb_flux = best.flux_threads;
+        }
+        if (a.nf > (a.axis_aligned ? a.ni : 0)) {
+            tbest = 1e300;
+            for (int tb : {64, 128, 256}) {
+                a.tb_gen = tb;
+                if ((r = time_launches(s, reps, e0, e1, [&] { launch_fluid_flux_general<R>(a, s->stream); }, &t)))
+                    return r;
+                if (t < tbest) { tbest = t; best.general_flux_threads = tb; }
+            }
+            best.time_us[2] = tbest;
+            a.tb_gen = best.general_flux_threads;
+        }
+        // cell update: block size x grid cap
+        tbest = 1e300;
+        for (int tb : {128, 256, 512}) {
+            for (int mult : {2, 4, 8, 16}) {
+                a.tb_update = tb;
+                a.update_blocks = 148 * mult;
+                if ((r = time_launches(s, reps, e0, e1, [&] { launch_fluid_update<R>(a, s->stream); }, &t))) return r;
+                if (t < tbest) { tbest = t; best.update_threads = tb; best.update_blocks = 148 * mult; }
+            }
+        }
+        best.time_us[3] = tbest;
+        a.tb_update = best.update_threads;
+        a.update_blocks = best.update_blocks;
+        // IBM spread over the current node forces and positions
+        if (s->n_membranes > 0) {
+            launch_membrane_sort(s->ma, s->stream);
+            tbest = 1e300;
+            for (int mult : {1, 2, 4, 8, 16}) {
+                s->ma.spread_blocks = 148 * mult;
+                if ((r = time_launches(s, reps, e0, e1, [&] { launch_membrane_spread(s->ma, s->stream); }, &t)))
+                    return r;
+                if (t < tbest) { tbest = t; best.spread_blocks = 148 * mult; }
+            }
+            best.time_us[4] = tbest;
+        }
+        return LBFS_OK;
+    };
+    rc = run();
+    // restore (also after a failure, as far as the device lets us)
+    cudaMemcpyAsync(a.state, keep_state, sizeof(Vec4<R>) * nt, cudaMemcpyDeviceToDevice, s->stream);
+    cudaMemcpyAsync(a.t1, keep_t1, sizeof(double4) * s->nc, cudaMemcpyDeviceToDevice, s->stream);
+    cudaMemcpyAsync(a.residual_sums, keep_misc, 4 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
+    cudaMemcpyAsync(a.flags, (char *)keep_misc + 32, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s->stream);
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    cudaFree(keep_state);
+    cudaFree(keep_t1);
+    cudaFree(keep_misc);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("autotune restore: ") + cudaGetErrorString(e));
+    shape_to_args<R>(s, best);
+    drop_graph(s);
+    if (out) *out = best;
+    return LBFS_OK;
+}
+
+}  // namespace
+
+extern "C" int lbfs_get_launch_shape(lbfs_solver *s, lbfs_launch_shape *shape) {
+    if (!s || !shape) return set_error(LBFS_ERR_ARG, "null argument");
+    *shape = s->fp32 ? args_to_shape<float>(s) : args_to_shape<double>(s);
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_set_launch_shape(lbfs_solver *s, const lbfs_launch_shape *shape) {
+    if (!s || !shape) return set_error(LBFS_ERR_ARG, "null argument");
+    int rc = check_shape(*shape);
+    if (rc) return rc;
+    if (s->fp32) shape_to_args<float>(s, *shape);
+    else shape_to_args<double>(s, *shape);
+    drop_graph(s);
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_autotune(lbfs_solver *s, int32_t reps, lbfs_launch_shape *shape) {
+    if (!s) return set_error(LBFS_ERR_ARG, "null handle");
+    if (reps < 1 || reps > 1000) return set_error(LBFS_ERR_ARG, "reps must be in 1..1000");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    return s->fp32 ? autotune<float>(s, reps, shape) : autotune<double>(s, reps, shape);
 }

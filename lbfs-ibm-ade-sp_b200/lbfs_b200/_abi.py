@@ -49,6 +49,14 @@ _i32p = ctypes.POINTER(ctypes.c_int32)
 _f64p = ctypes.POINTER(ctypes.c_double)
 
 
+class GridDesc(ctypes.Structure):
+    _fields_ = [
+        ("cell0", ctypes.c_int32), ("n_cells", ctypes.c_int32),
+        ("origin", ctypes.c_double * 3), ("length", ctypes.c_double * 3),
+        ("delta_x", ctypes.c_double), ("delta_h", ctypes.c_double),
+    ]
+
+
 class MeshDesc(ctypes.Structure):
     _fields_ = [
         ("n_cells", ctypes.c_int32), ("n_faces", ctypes.c_int32), ("n_interior", ctypes.c_int32),
@@ -60,6 +68,7 @@ class MeshDesc(ctypes.Structure):
         ("bc_rho_type", _i32p), ("bc_vel_type", _i32p), ("bc_values", _f64p),
         ("origin", ctypes.c_double * 3), ("length", ctypes.c_double * 3),
         ("delta_x", ctypes.c_double), ("delta_h", ctypes.c_double),
+        ("n_instances", ctypes.c_int32), ("instances", ctypes.POINTER(GridDesc)),
     ]
 
 
@@ -85,8 +94,21 @@ class RbcDesc(ctypes.Structure):
         ("wlc_ratio", ctypes.c_double), ("curvature_ratio", ctypes.c_double), ("volume_ratio", ctypes.c_double),
         ("internal_viscosity_ratio", ctypes.c_double), ("reference_length", ctypes.c_double),
         ("pivkin_length", ctypes.c_int32), ("sphere_reference", ctypes.c_int32),
+        ("instance", ctypes.c_int32),
     ]
 
+
+class LaunchShape(ctypes.Structure):
+    _fields_ = [
+        ("gradient_threads", ctypes.c_int32), ("flux_threads", ctypes.c_int32),
+        ("general_flux_threads", ctypes.c_int32), ("update_threads", ctypes.c_int32),
+        ("update_blocks", ctypes.c_int32), ("spread_blocks", ctypes.c_int32),
+        ("time_us", ctypes.c_double * 5),
+    ]
+
+
+LBFS_MAX_UPDATE_BLOCKS = 148 * 16
+LBFS_MAX_SPREAD_BLOCKS = 148 * 16
 
 _lib = None
 
@@ -127,6 +149,9 @@ def lib():
                                                                   _f64p],
             "lbfs_rbc_build_springs": [ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int32, _i32p, _i32p],
             "lbfs_residual_rms_noalloc": [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, vp, vp],
+            "lbfs_get_launch_shape": [vp, ctypes.POINTER(LaunchShape)],
+            "lbfs_set_launch_shape": [vp, ctypes.POINTER(LaunchShape)],
+            "lbfs_autotune": [vp, ctypes.c_int32, ctypes.POINTER(LaunchShape)],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -166,5 +191,5 @@ EXPORTED = [
     "lbfs_get_residuals", "lbfs_get_field", "lbfs_keep_residuals", "lbfs_status", "lbfs_launches_per_step",
     "lbfs_set_profiling", "lbfs_get_phase_times",
     "lbfs_last_error", "lbfs_mesh_uniform_counts", "lbfs_mesh_build_uniform", "lbfs_rbc_build_springs",
-    "lbfs_residual_rms_noalloc",
+    "lbfs_residual_rms_noalloc", "lbfs_get_launch_shape", "lbfs_set_launch_shape", "lbfs_autotune",
 ]

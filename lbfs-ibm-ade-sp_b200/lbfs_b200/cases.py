@@ -101,3 +101,79 @@ def shear_rbc(n=64, level=3, radius_cells=8.0, capillary=0.1, u_wall=0.02, seed=
     return Case("shear_rbc", mesh, params, [cell], rho, u, v, w, bcs,
                 {"n": (n, ny, nz), "level": level, "radius_cells": radius_cells, "capillary": capillary,
                  "gamma_dot": gamma, "shear_modulus": shear_modulus})
+
+
+def _rbc_moduli(shear_modulus, R):
+    return dict(volume_modulus=500.0 * shear_modulus, local_area_modulus=10.0 * shear_modulus,
+                global_area_modulus=500.0 * shear_modulus, shear_modulus=shear_modulus,
+                global_bending_modulus=0.05 * shear_modulus * R * R, local_bending_modulus=0.0,
+                viscosity=0.0, wlc_ratio=2.2, curvature_ratio=0.0, volume_ratio=1.0,
+                internal_viscosity_ratio=5.0)
+
+
+def shear_channel(n, n_rbc=1, level=2, radius_cells=3.0, shear_modulus=1e-5, capillary=0.1, seed=99, tau=0.8,
+                  delta_t=0.5, precision=_abi.LBFS_FP64, ibm_stencil=_abi.LBFS_IBM_PESKIN4):
+    """Wall-driven shear in an n^3 channel with up to n_rbc red cells of radius
+    `radius_cells`, randomly oriented at distinct points of a lattice of spacing
+    2 R + 2 cells, at least R + 3 cells from the walls (fewer cells when fewer
+    points fit).  The wall speed follows from the capillary number
+    Ca = mu gamma_dot R / G_s with mu = rho nu, rho = 1."""
+    dt = 1.0
+    visc = (tau - 0.5) / 3.0 * dt
+    L = 2.0 * n
+    mesh = build_uniform_mesh(L, L, L, dt, visc=visc)
+    R = radius_cells * 2.0 * dt
+    gamma = capillary * shear_modulus / (visc * R)
+    bcs = {"left": (2, 2, 1.0, 0.0, 0.0, 0.0), "right": (2, 2, 1.0, 0.0, 0.0, 0.0),
+           "bottom": (2, 10, 1.0, gamma, 0.0, 0.0), "top": (2, 10, 1.0, gamma, 0.0, 0.0),
+           "back": (2, 2, 1.0, 0.0, 0.0, 0.0), "front": (2, 2, 1.0, 0.0, 0.0, 0.0)}
+    mesh.set_boundaries(bcs)
+    rng = np.random.default_rng(seed)
+    margin = R + 3 * 2.0 * dt
+    axis = np.arange(margin, L - margin + 1e-9, 2 * R + 2 * 2.0 * dt)
+    if len(axis) == 0:
+        axis = np.array([0.5 * L])
+    points = np.array([(x, y, z) for z in axis for y in axis for x in axis])
+    chosen = rng.permutation(len(points))[:n_rbc]
+    moduli = _rbc_moduli(shear_modulus, R)
+    cells = [red_cell(level, R, tuple(points[i]), rotation_matrix(rng), **moduli) for i in sorted(chosen)]
+    params = StepParams(visc=visc, delta_t=delta_t, channel_diameter=L, ref_rho=1.0, max_velocity=max(gamma * L, 1e-3),
+                        rho0=1.0, visc_factor_initial=1.0, testcase=5, precision=precision, ibm_stencil=ibm_stencil,
+                        viscosity_period=10000)
+    y = mesh.cell_centroid[: mesh.n_cells, 1]
+    rho, u, v, w = _initial_state(mesh.n_cells, seed, amplitude=1e-5, u0=gamma * y)
+    return Case("shear_channel", mesh, params, cells, rho, u, v, w, bcs,
+                {"n": n, "level": level, "radius_cells": radius_cells, "capillary": capillary,
+                 "shear_modulus": shear_modulus, "gamma_dot": gamma, "n_rbc": len(cells)})
+
+
+def ensemble(n_instances=64, seed=2024, n_range=(16, 48), rbc_range=(1, 8), levels=(2, 3),
+             shear_modulus_range=(2e-6, 2e-5), capillary_range=(0.05, 0.5), precision=_abi.LBFS_FP32_BULK,
+             ibm_stencil=_abi.LBFS_IBM_PESKIN4, tau=0.8, delta_t=0.5, radius_cells=None):
+    """Batched ensemble of independent shear channels: per instance a cube of n
+    cells per axis (n uniform in n_range), 1-8 red cells of a level drawn from
+    `levels`, shear modulus log-uniform and capillary number uniform in their
+    ranges.  Red-cell radius: n / 12 cells, at least 1.5 (unless given).
+    Returns a Case whose mesh is an EnsembleMesh and whose info['members'] holds
+    the stand-alone Case of every instance."""
+    from dataclasses import replace
+    from .ensemble import concatenate
+    rng = np.random.default_rng(seed)
+    members = []
+    for k in range(n_instances):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        n_rbc = int(rng.integers(rbc_range[0], rbc_range[1] + 1))
+        level = int(rng.choice(levels))
+        gs = float(np.exp(rng.uniform(np.log(shear_modulus_range[0]), np.log(shear_modulus_range[1]))))
+        ca = float(rng.uniform(*capillary_range))
+        r = radius_cells if radius_cells is not None else max(1.5, n / 12.0)
+        members.append(shear_channel(n, n_rbc, level, r, gs, ca, seed=seed * 1000 + k, tau=tau, delta_t=delta_t,
+                                     precision=precision, ibm_stencil=ibm_stencil))
+    mesh = concatenate([c.mesh for c in members])
+    membranes = [replace(m, instance=k) for k, c in enumerate(members) for m in c.membranes]
+    p = members[0].params
+    params = replace(p, max_velocity=max(c.params.max_velocity for c in members))
+    cat = lambda name: np.ascontiguousarray(np.concatenate([getattr(c, name) for c in members]))
+    return Case("ensemble", mesh, params, membranes, cat("rho"), cat("u"), cat("v"), cat("w"), None,
+                {"members": members, "n_instances": n_instances, "cells": int(mesh.n_cells),
+                 "membranes": len(membranes), "nodes": int(sum(m.n_nodes for m in membranes))})

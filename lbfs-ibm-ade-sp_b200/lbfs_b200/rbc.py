@@ -113,6 +113,7 @@ class Membrane:
     reference_length: float = 0.0
     pivkin_length: bool = False
     sphere_reference: bool = True
+    instance: int = 0  # ensemble instance the membrane lives in
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -133,6 +134,7 @@ class Membrane:
             setattr(d, name, float(getattr(self, name)))
         d.pivkin_length = int(bool(self.pivkin_length))
         d.sphere_reference = int(bool(self.sphere_reference))
+        d.instance = int(self.instance)
         return d
 
 

@@ -44,6 +44,12 @@ class StepParams:
         return p
 
 
+def _shape_dict(sh):
+    d = {name: getattr(sh, name) for name, _ in _abi.LaunchShape._fields_ if name != "time_us"}
+    d["time_us"] = dict(zip(("gradients", "flux", "general_flux", "update", "spread"), list(sh.time_us)))
+    return d
+
+
 class GpuSolver:
     def __init__(self, mesh, params, membranes=(), device=0):
         self.mesh = mesh
@@ -156,6 +162,29 @@ class GpuSolver:
 
     def set_stream(self, stream_ptr):
         _abi.check(_abi.lib().lbfs_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def launch_shape(self):
+        """Current launch shape as a dict (block sizes, grid caps)."""
+        sh = _abi.LaunchShape()
+        _abi.check(_abi.lib().lbfs_get_launch_shape(self._h, ctypes.byref(sh)))
+        return _shape_dict(sh)
+
+    def set_launch_shape(self, **kw):
+        """Change some fields of the launch shape (the rest stay)."""
+        sh = _abi.LaunchShape()
+        _abi.check(_abi.lib().lbfs_get_launch_shape(self._h, ctypes.byref(sh)))
+        for k, v in kw.items():
+            if k == "time_us" or not hasattr(sh, k):
+                raise KeyError(k)
+            setattr(sh, k, int(v))
+        _abi.check(_abi.lib().lbfs_set_launch_shape(self._h, ctypes.byref(sh)))
+
+    def autotune(self, reps=20):
+        """Time the candidate launch shapes on this handle's mesh and state and
+        keep the fastest; returns the choice with per-kernel mean times (us)."""
+        sh = _abi.LaunchShape()
+        _abi.check(_abi.lib().lbfs_autotune(self._h, int(reps), ctypes.byref(sh)))
+        return _shape_dict(sh)
 
     def launches_per_step(self):
         n = ctypes.c_int32()

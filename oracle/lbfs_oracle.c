@@ -567,6 +567,7 @@ static void interior_viscosity(oracle_case *o) {
 /* ------------------------------------------------------------- API ---- */
 
 oracle_case *oracle_create(const lbfs_mesh_desc *m, const lbfs_params *p, const lbfs_rbc_desc *rbc, int n_rbc) {
+    if (m->n_instances > 1) return NULL; /* one case per oracle object: check ensembles instance by instance */
     oracle_case *o = (oracle_case *)calloc(1, sizeof(oracle_case));
     o->m = *m;
     o->p = *p;

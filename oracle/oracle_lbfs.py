@@ -62,6 +62,8 @@ class OracleSolver:
             self._rdesc = T(*descs)
         self.h = lib().oracle_create(ctypes.addressof(self._mdesc), ctypes.addressof(self._pdesc),
                                      ctypes.addressof(self._rdesc) if self._rdesc is not None else None, len(descs))
+        if not self.h:
+            raise ValueError("the oracle runs one case at a time (no ensemble instance table)")
         self.n_cells = mesh.n_cells
         self.total_nodes = sum(m.n_nodes for m in self.membranes)
         self.total_springs = sum(len(m.springs) for m in self.membranes)

@@ -1,6 +1,7 @@
 """The C-ABI library loads and exports every entry point the header declares."""
 import ctypes
 import os
+import subprocess
 import re
 
 import numpy as np
@@ -32,9 +33,33 @@ def test_library_exports_every_declared_symbol():
 def test_structs_match_header_sizes():
     # sizes of the descriptors as a C compiler lays them out (64-bit)
     from lbfs_b200 import _abi
-    assert ctypes.sizeof(_abi.MeshDesc) == 8 * 4 + 14 * 8 + 8 * 8
+    assert ctypes.sizeof(_abi.MeshDesc) == 8 * 4 + 14 * 8 + 8 * 8 + 8 + 8
+    assert ctypes.sizeof(_abi.GridDesc) == 8 + 8 * 8
     assert ctypes.sizeof(_abi.Params) == 4 * 8 + 3 * 8 + 4 * 8 + 4 * 4
-    assert ctypes.sizeof(_abi.RbcDesc) == 16 + 4 * 8 + 13 * 8 + 8
+    assert ctypes.sizeof(_abi.RbcDesc) == 16 + 4 * 8 + 13 * 8 + 8 + 8
+
+
+def test_struct_layout_matches_c_compiler(tmp_path):
+    # every field offset of the ctypes mirrors equals the C compiler's offsetof
+    from lbfs_b200 import _abi
+    structs = {"lbfs_mesh_desc": _abi.MeshDesc, "lbfs_grid_desc": _abi.GridDesc, "lbfs_params": _abi.Params,
+               "lbfs_rbc_desc": _abi.RbcDesc}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lbfs_b200.h"', 'int main(void) {']
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {(a, b): int(c) for a, b, c in (l.split() for l in out if l)}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f in py._fields_:
+            assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-GPU error path")
