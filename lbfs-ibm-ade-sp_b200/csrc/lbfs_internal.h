@@ -28,6 +28,7 @@ constexpr int kQ = 15;
 // Per-membrane device-side scalars (one record per membrane).
 struct MembraneScalars {
     double V, V0, A, A0, MAD, MAD0;
+    double Vc, Ac;                   // current totals from the totals kernel (when it runs)
     double bbox_lo[3], bbox_hi[3];   // node coordinate bounds (interior viscosity test)
     int patch_lo[3], patch_dim[3];   // IBM patch: first cell and extent per axis
     int patch_cells;                 // product of patch_dim (0 when the patch overflowed)

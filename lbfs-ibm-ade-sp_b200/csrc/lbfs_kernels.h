@@ -31,9 +31,10 @@ enum MembraneMode : int {
 
 // A node as the spread reads it, in sorted order: 1D stencil weights per axis,
 // first stencil cell (b[0..2]) and the node index (b[3]).
-struct SpreadRec {
-    double w[12];
-    int b[4];
+struct alignas(16) SpreadRec {
+    double w[12];  // 1D stencil weights of a node, x then y then z (4 slots per axis)
+    int b0;        // first stencil cell along x
+    int pad[3];
 };
 
 // Spring blocks of 128 per membrane the MAD partials can hold.
@@ -66,12 +67,13 @@ struct MembraneArgs {
     int sort_capacity;           // power of two >= nodes of the largest membrane
     int total_nodes, total_springs;
     const int *spring_mem;       // [total_springs] membrane of each spring
-    int *node_base;              // [3*total_nodes] first stencil cell per axis (scratch)
-    double *node_w;              // [12*total_nodes] 1D stencil weights per axis (scratch)
     int *bin_start;              // [sum of (patch_bound + 1)] first sorted node of each bin, from patch_off + m
-    int *tile_start;             // [n_membranes + 1] first spread tile of each membrane (prefix over patches)
+    int *cell_start;             // [n_membranes + 1] first spread cell of each membrane (prefix over patches)
     unsigned int *sort_ticket;   // membranes whose patch is known in this launch; zero between launches
     int spread_blocks;           // grid of the spread kernel (grid-stride over the tiles)
+    int separate_totals;         // volume/area totals by their own kernel (many membranes)
+    int *sorted_pos;             // [total_nodes] position of each node in its membrane's sorted order
+    double4 *sorted_force;       // [total_nodes] node forces in sorted order (spread input)
     SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order (scratch)
     int max_springs;             // springs of the largest membrane
     int max_patch_bound;         // largest patch_bound over the membranes (spread grid)

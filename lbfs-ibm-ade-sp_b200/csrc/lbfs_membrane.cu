@@ -4,7 +4,7 @@
 //   M2 k_mem_springs   (one thread per spring; totals per block)     P1, P2, P4
 //   M3 k_mem_nodeforce (one thread per node)                         P3
 //   M4 k_mem_sort      (one CTA per membrane, on a side stream)      P5
-//   M5 k_mem_spread    (one thread per patch cell of each membrane)  P6
+//   M5 k_mem_spread    (one warp per patch cell, all membranes)      P6
 //
 //   P0  IBM velocity interpolation at the nodes + explicit node advection
 //       (interpolate_velocities_on_nodes, immersed_boundary_method.cu:14-97;
@@ -66,41 +66,6 @@ __device__ double block_sum(double v, double *sh) {
     }
     __syncthreads();
     const double r = sh[32];
-    __syncthreads();
-    return r;
-}
-__device__ double block_minmax(double v, double *sh, bool is_min) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const double u = __shfl_down_sync(0xffffffffu, v, o);
-        v = is_min ? fmin(v, u) : fmax(v, u);
-    }
-    if (lane == 0) sh[warp] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = sh[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); w++) s = is_min ? fmin(s, sh[w]) : fmax(s, sh[w]);
-        sh[32] = s;
-    }
-    __syncthreads();
-    const double r = sh[32];
-    __syncthreads();
-    return r;
-}
-__device__ int block_min_int(int v, int *sh) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_down_sync(0xffffffffu, v, o));
-    if (lane == 0) sh[warp] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int s = sh[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); w++) s = min(s, sh[w]);
-        sh[32] = s;
-    }
-    __syncthreads();
-    const int r = sh[32];
     __syncthreads();
     return r;
 }
@@ -360,16 +325,27 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
     const int n_inst = mc.gnx * mc.gny * mc.gnz;
     const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
     const int cells = S * S * S;
+    // the 3 S one-dimensional weights, one per lane (lane = axis * S + offset)
+    double w1 = 0.0;
+    if (lane < 3 * S) {
+        const int ax = lane / S, q = lane - ax * S;
+        const int b = ax == 0 ? st.i0 : (ax == 1 ? st.j0 : st.k0);
+        const double r = ax == 0 ? st.rx : (ax == 1 ? st.ry : st.rz);
+        w1 = stencil_weight(A.ibm_stencil, b + q + 0.5 - r);
+    }
     double v[3] = {0.0, 0.0, 0.0};
-    for (int c = lane; c < cells; c += 32) {
+    for (int c0 = 0; c0 < cells; c0 += 32) {
         // cell c of the stencil, z fastest as in the reference's i, j, k loop nest
-        const int i = st.i0 + c / (S * S), j = st.j0 + (c / S) % S, k = st.k0 + c % S;
+        const int c = c0 + lane;
+        const int di = (c / (S * S)) % S, dj = (c / S) % S, dk = c % S;
+        const double wx = __shfl_sync(0xffffffffu, w1, di);
+        const double wy = __shfl_sync(0xffffffffu, w1, S + dj);
+        const double wz = __shfl_sync(0xffffffffu, w1, 2 * S + dk);
+        if (c >= cells) continue;
+        const int i = st.i0 + di, j = st.j0 + dj, k = st.k0 + dk;
         const int lidx = i + j * mc.gnx + k * mc.gny * mc.gnx;
         if (lidx < n_inst && lidx >= 0) {
             const int idx = mc.cell0 + lidx;
-            const double wx = stencil_weight(A.ibm_stencil, i + 0.5 - st.rx);
-            const double wy = stencil_weight(A.ibm_stencil, j + 0.5 - st.ry);
-            const double wz = stencil_weight(A.ibm_stencil, k + 0.5 - st.rz);
             double u, vv, w;
             read_velocity<R>(A.state, idx, u, vv, w);
             v[0] += u * wx * wy * wz;
@@ -397,6 +373,38 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
 // first n_nodes springs) are summed by the membrane's last block to finish.
 // Reference mode: the stress-free pass (contour lengths, spring constants,
 // reference curvatures).
+// Volume and area of membrane mc: per-thread sums over triangles
+// threadIdx.x, threadIdx.x + 128, ..., then block_sum (blocks of 128 threads).
+__device__ __forceinline__ void membrane_totals(const MembraneArgs &A, const MembraneConst &mc, double *sh, double &V,
+                                                double &Ar) {
+    double pv = 0.0, pa = 0.0;
+    for (int lt = threadIdx.x; lt < mc.n_tris; lt += blockDim.x) {
+        const int t = mc.tri0 + lt;
+        const int na = A.tri[3 * t], nb = A.tri[3 * t + 1], nc = A.tri[3 * t + 2];
+        const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]), c = d3(A.x[nc], A.y[nc], A.z[nc]);
+        const D3 normal = cross(b - a, c - a);
+        pv += dot(normal, tri_centroid(a, b, c)) / 6;
+        pa += sqrt(dot(normal, normal)) * 0.5;
+    }
+    V = block_sum(pv, sh);
+    Ar = block_sum(pa, sh);
+}
+
+// Totals once per membrane (one 128-thread block each), for handles with many
+// membranes: the spring blocks then read them instead of forming them again.
+__global__ void __launch_bounds__(128) k_mem_totals(MembraneArgs A) {
+    __shared__ double sh[33];
+    const int m = blockIdx.x;
+    const MembraneConst mc = A.mc[m];
+    double V, Ar;
+    membrane_totals(A, mc, sh, V, Ar);
+    if (threadIdx.x == 0) {
+        A.ms[m].Vc = V;
+        A.ms[m].Ac = Ar;
+    }
+}
+
+template <bool kTotalsHere>
 __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
     __shared__ double sh[33];
     __shared__ bool last_block;
@@ -412,16 +420,13 @@ __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
     }
     MembraneScalars *ms = A.ms + m;
     const bool initials = A.mode == kModeInitial;
-    double pv = 0.0, pa = 0.0;
-    for (int lt = threadIdx.x; lt < mc.n_tris; lt += blockDim.x) {
-        const int t = mc.tri0 + lt;
-        const int na = A.tri[3 * t], nb = A.tri[3 * t + 1], nc = A.tri[3 * t + 2];
-        const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]), c = d3(A.x[nc], A.y[nc], A.z[nc]);
-        const D3 normal = cross(b - a, c - a);
-        pv += dot(normal, tri_centroid(a, b, c)) / 6;
-        pa += sqrt(dot(normal, normal)) * 0.5;
+    double V, Ar;
+    if (kTotalsHere || A.mode != kModeStep) {
+        membrane_totals(A, mc, sh, V, Ar);
+    } else {
+        V = ms->Vc;
+        Ar = ms->Ac;
     }
-    const double V = block_sum(pv, sh), Ar = block_sum(pa, sh);
     const double V0 = initials ? V * mc.volume_ratio : ms->V0;
     const double A0 = initials ? Ar : ms->A0;
     const double MADp = initials ? 0.0 : ms->MAD, MAD0p = initials ? 0.0 : ms->MAD0;
@@ -485,17 +490,33 @@ __global__ void __launch_bounds__(128) k_mem_nodeforce(MembraneArgs A) {
     A.fx[n] = f[0];
     A.fy[n] = f[1];
     A.fz[n] = f[2];
+    A.sorted_force[A.sorted_pos[n]] = make_double4(f[0], f[1], f[2], 0.0);
 }
 
-// ---- M4: node bounds, stencil tables, nodes sorted by stencil base cell -----
+// ---- M4: node bounds, nodes sorted by stencil base cell, spread records -----
 // One CTA per membrane; needs only the advected positions, so it runs beside
-// M2 and M3.  Writes each node's first stencil cell and 1D weights, the patch,
-// the sorted node list and, for every bin b of the patch, the first sorted
-// position whose bin is >= b.
+// M2.  Finds the patch (bounding box of the stencils), sorts (bin, node) keys
+// in shared memory, writes for every bin b of the patch the first sorted
+// position whose bin is >= b, and for every sorted position the node's
+// stencil weights and first x cell (recomputed from its position, so nothing
+// but the keys lives between the phases).  The last CTA of the launch writes
+// the prefix of patch cells over the membranes (the spread kernel's work list).
+__device__ __forceinline__ unsigned long long pack_base(int b0, int b1, int b2) {
+    const unsigned long long o = 1ull << 20;  // bases within +-2^20 cells
+    return ((unsigned long long)(b0 + o) << 42) | ((unsigned long long)(b1 + o) << 21) | (unsigned long long)(b2 + o);
+}
+__device__ __forceinline__ void unpack_base(unsigned long long k, int b[3]) {
+    const long long o = 1ll << 20, mask = (1ll << 21) - 1;
+    b[0] = (int)((long long)(k >> 42) - o);
+    b[1] = (int)((long long)((k >> 21) & mask) - o);
+    b[2] = (int)((long long)(k & mask) - o);
+}
+
 __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     extern __shared__ unsigned long long skeys[];
     __shared__ double shv[kMembraneThreads / 32][12];
     __shared__ double red[12];
+    __shared__ bool last_sorted;
     const int m = blockIdx.x;
     const MembraneConst mc = A.mc[m];
     MembraneScalars *ms = A.ms + m;
@@ -504,22 +525,21 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     double v[12];
     for (int c = 0; c < 3; c++) { v[c] = 1e300; v[3 + c] = 1e300; v[6 + c] = 1e300; v[9 + c] = 1e300; }
     unsigned int range_flag = 0;
+    bool base_range = true;
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
         const int n = mc.node0 + ln;
         const double p[3] = {A.x[n], A.y[n], A.z[n]};
         const Stencil st = node_stencil(A, mc, p[0], p[1], p[2]);
         const int b[3] = {st.i0, st.j0, st.k0};
-        const double r[3] = {st.rx, st.ry, st.rz};
-        double *w = A.node_w + 12 * (size_t)n;
         for (int c = 0; c < 3; c++) {
             v[c] = fmin(v[c], p[c]);            // lower bound
             v[3 + c] = fmin(v[3 + c], -p[c]);   // minus upper bound
             v[6 + c] = fmin(v[6 + c], (double)b[c]);
             v[9 + c] = fmin(v[9 + c], -(double)b[c]);
             if (b[c] < 0 || b[c] + S > gn[c]) range_flag = LBFS_FLAG_IBM_RANGE;
-            for (int q = 0; q < S; q++) w[4 * c + q] = stencil_weight(A.ibm_stencil, b[c] + q + 0.5 - r[c]);
-            A.node_base[3 * (size_t)n + c] = b[c];
+            if (b[c] < -(1 << 19) || b[c] > (1 << 19)) base_range = false;
         }
+        skeys[ln] = pack_base(b[0], b[1], b[2]);
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -542,9 +562,9 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         pdim[c] = bdim[c] + S - 1;
     }
     const long long pcells = (long long)pdim[0] * pdim[1] * pdim[2];
-    const bool overflow = pcells > mc.patch_bound || mc.n_nodes == 0;
+    const bool bases_packed = __syncthreads_and(base_range) != 0;
+    const bool overflow = pcells > mc.patch_bound || mc.n_nodes == 0 || !bases_packed;
     if (range_flag) atomicOr(A.flags, range_flag);
-    __shared__ bool last_sorted;
     if (threadIdx.x == 0) {
         for (int c = 0; c < 3; c++) {
             ms->bbox_lo[c] = red[c];
@@ -559,43 +579,45 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     }
     __syncthreads();
     if (last_sorted) {
-        // every patch is known: spread tiles of 128 cells, prefix over the membranes
+        // every patch is known: prefix of patch cells over the membranes
         __threadfence();
         __shared__ int scan[kMembraneThreads];
         const int M = gridDim.x;
         const int per = (M + blockDim.x - 1) / blockDim.x;
         const int m0 = min(M, (int)threadIdx.x * per), m1 = min(M, m0 + per);
         int local = 0;
-        for (int q = m0; q < m1; q++) local += (__ldcg(&A.ms[q].patch_cells) + 127) / 128;
+        for (int q = m0; q < m1; q++) local += __ldcg(&A.ms[q].patch_cells);
         scan[threadIdx.x] = local;
         __syncthreads();
         for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-            const int v = threadIdx.x >= (unsigned)o ? scan[threadIdx.x - o] : 0;
+            const int x = threadIdx.x >= (unsigned)o ? scan[threadIdx.x - o] : 0;
             __syncthreads();
-            scan[threadIdx.x] += v;
+            scan[threadIdx.x] += x;
             __syncthreads();
         }
         int run = scan[threadIdx.x] - local;
         for (int q = m0; q < m1; q++) {
-            A.tile_start[q] = run;
-            run += (__ldcg(&A.ms[q].patch_cells) + 127) / 128;
+            A.cell_start[q] = run;
+            run += __ldcg(&A.ms[q].patch_cells);
         }
         if (threadIdx.x == blockDim.x - 1) {
-            A.tile_start[M] = scan[threadIdx.x];
+            A.cell_start[M] = scan[threadIdx.x];
             *A.sort_ticket = 0u;
         }
     }
+    if (overflow) return;
     int npad = 1;
     while (npad < mc.n_nodes) npad <<= 1;
     for (int t = threadIdx.x; t < npad; t += blockDim.x) {
         unsigned long long key = ~0ull;
         if (t < mc.n_nodes) {
-            const int *b = A.node_base + 3 * (size_t)(mc.node0 + t);
+            int b[3];
+            unpack_base(skeys[t], b);
             const unsigned long long bin =
                 (unsigned long long)((b[0] - plo[0]) + bdim[0] * ((b[1] - plo[1]) + bdim[1] * (b[2] - plo[2])));
             key = (bin << 32) | (unsigned long long)t;
         }
-        skeys[t] = key;
+        skeys[t] = key;  // each thread rewrites only the keys it packed
     }
     __syncthreads();
     for (int size = 2; size <= npad; size <<= 1) {
@@ -623,74 +645,99 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     }
     for (int e = threadIdx.x; e < mc.n_nodes; e += blockDim.x) {
         const int n = mc.node0 + (int)(skeys[e] & 0xffffffffu);
-        SpreadRec r;
-        for (int q = 0; q < 12; q++) r.w[q] = A.node_w[12 * (size_t)n + q];
-        for (int c = 0; c < 3; c++) r.b[c] = A.node_base[3 * (size_t)n + c];
-        r.b[3] = n;
-        A.spread_rec[mc.node0 + e] = r;
+        const Stencil st = node_stencil(A, mc, A.x[n], A.y[n], A.z[n]);
+        const int b[3] = {st.i0, st.j0, st.k0};
+        const double r[3] = {st.rx, st.ry, st.rz};
+        SpreadRec rec;
+        for (int c = 0; c < 3; c++)
+            for (int q = 0; q < 4; q++)
+                rec.w[4 * c + q] = q < S ? stencil_weight(A.ibm_stencil, b[c] + q + 0.5 - r[c]) : 0.0;
+        rec.b0 = b[0];
+        rec.pad[0] = rec.pad[1] = rec.pad[2] = 0;
+        A.spread_rec[mc.node0 + e] = rec;
+        A.sorted_pos[n] = mc.node0 + e;
     }
 }
 
-// ---- M5: spread as a per-cell segmented reduction over the sorted nodes ------
-// Each patch cell sums, stencil rows in (z, y) order and within a row nodes in
-// (bin, node) order, the contributions of the nodes whose stencil covers it.
-// The nodes of one row of bins are contiguous in the sorted order.
+// ---- M5: spread as a per-cell reduction over the sorted nodes -------------
+// One warp per patch cell.  The cell's contributions are the nodes of S*S rows
+// of bins (rows in (z, y) order, each row a contiguous range of the sorted
+// nodes); lane q of the warp takes contributions q, q + 32, ... of that list,
+// then the warp adds the lanes in a fixed tree.  All nodes of a row share the
+// stencil's y and z offsets, and a node's record carries its first x cell, so
+// the loads of one contribution do not wait on each other.
 template <int S>
-__device__ __forceinline__ void spread_cell(const MembraneArgs &A, int m, int pc) {
-    const MembraneScalars &ms = A.ms[m];
-    const MembraneConst &mc = A.mc[m];
-    const int node0 = mc.node0;
-    const int pdim[3] = {ms.patch_dim[0], ms.patch_dim[1], ms.patch_dim[2]};
-    const int bdim[3] = {pdim[0] - S + 1, pdim[1] - S + 1, pdim[2] - S + 1};
-    const int px = pc % pdim[0], py = (pc / pdim[0]) % pdim[1], pz = pc / (pdim[0] * pdim[1]);
-    const int ci = ms.patch_lo[0] + px, cj = ms.patch_lo[1] + py, ck = ms.patch_lo[2] + pz;
-    const int *bin_start = A.bin_start + (size_t)ms.patch_off + m;
-    const SpreadRec *rec = A.spread_rec + node0;
-    const double inv3 = 1 / mc.gdx / mc.gdx / mc.gdx;
-    const int bx0 = max(px - S + 1, 0), bx1 = min(px, bdim[0] - 1);
-    int lo[S * S], hi[S * S];
-#pragma unroll
-    for (int r = 0; r < S * S; r++) {
-        const int by = py - S + 1 + r % S, bz = pz - S + 1 + r / S;
-        const bool ok = by >= 0 && by < bdim[1] && bz >= 0 && bz < bdim[2] && bx0 <= bx1;
-        const int row = bdim[0] * (by + bdim[1] * bz);
-        lo[r] = ok ? __ldg(bin_start + row + bx0) : 0;
-        hi[r] = ok ? __ldg(bin_start + row + bx1 + 1) : 0;
-    }
-    double f[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int r = 0; r < S * S; r++) {
-        for (int e = lo[r]; e < hi[r]; e++) {
-            const SpreadRec &q = rec[e];
-            const int n = q.b[3];
-            const double wx = q.w[ci - q.b[0]], wy = q.w[4 + cj - q.b[1]], wz = q.w[8 + ck - q.b[2]];
-            f[0] += A.fx[n] * wx * wy * wz * inv3;
-            f[1] += A.fy[n] * wx * wy * wz * inv3;
-            f[2] += A.fz[n] * wx * wy * wz * inv3;
-        }
-    }
-    double *pf = A.patch_force + ((size_t)ms.patch_off + pc) * 3;
-    pf[0] = f[0];
-    pf[1] = f[1];
-    pf[2] = f[2];
-}
-
-// Grid-stride over the spread tiles of all membranes (128 patch cells each,
-// numbered by the prefix the sort kernel wrote): a fixed grid however many
-// membranes and patch sizes an ensemble has.
-template <int S>
-__global__ void __launch_bounds__(128) k_mem_spread(MembraneArgs A) {
+__global__ void __launch_bounds__(256) k_mem_spread(MembraneArgs A) {
+    const int lane = threadIdx.x & 31;
     const int M = A.n_membranes;
-    const int total = __ldg(A.tile_start + M);
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        int lo = 0, hi = M;  // membrane m with tile_start[m] <= t < tile_start[m + 1]
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (__ldg(A.tile_start + mid) <= t) lo = mid;
-            else hi = mid;
+    const int total = __ldg(A.cell_start + M);
+    const int n_warps = (gridDim.x * blockDim.x) >> 5;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < total; t += n_warps) {
+        int lo_m = 0, hi_m = M;  // membrane m with cell_start[m] <= t < cell_start[m + 1]
+        while (hi_m - lo_m > 1) {
+            const int mid = (lo_m + hi_m) >> 1;
+            if (__ldg(A.cell_start + mid) <= t) lo_m = mid;
+            else hi_m = mid;
         }
-        const int pc = (t - __ldg(A.tile_start + lo)) * 128 + threadIdx.x;
-        if (pc < A.ms[lo].patch_cells) spread_cell<S>(A, lo, pc);
+        const int m = lo_m;
+        const MembraneScalars &ms = A.ms[m];
+        const MembraneConst &mc = A.mc[m];
+        const int pc = t - __ldg(A.cell_start + m);
+        const int pdim[3] = {ms.patch_dim[0], ms.patch_dim[1], ms.patch_dim[2]};
+        const int bdim[3] = {pdim[0] - S + 1, pdim[1] - S + 1, pdim[2] - S + 1};
+        const int px = pc % pdim[0], py = (pc / pdim[0]) % pdim[1], pz = pc / (pdim[0] * pdim[1]);
+        const int ci = ms.patch_lo[0] + px;
+        const int *bin_start = A.bin_start + (size_t)ms.patch_off + m;
+        const int bx0 = max(px - S + 1, 0), bx1 = min(px, bdim[0] - 1);
+        // lane r < S*S: sorted range of row r
+        int lo = 0, len = 0;
+        if (lane < S * S) {
+            const int by = py - S + 1 + lane % S, bz = pz - S + 1 + lane / S;
+            if (by >= 0 && by < bdim[1] && bz >= 0 && bz < bdim[2] && bx0 <= bx1) {
+                const int row = bdim[0] * (by + bdim[1] * bz);
+                lo = __ldg(bin_start + row + bx0);
+                len = __ldg(bin_start + row + bx1 + 1) - lo;
+            }
+        }
+        int end = len;  // inclusive prefix of the row lengths
+#pragma unroll
+        for (int o = 1; o < S * S; o <<= 1) {
+            const int x = __shfl_up_sync(0xffffffffu, end, o);
+            if (lane >= o) end += x;
+        }
+        const int count = __shfl_sync(0xffffffffu, end, S * S - 1);
+        const SpreadRec *rec = A.spread_rec + mc.node0;
+        const double4 *frc = A.sorted_force + mc.node0;
+        const double inv3 = 1 / mc.gdx / mc.gdx / mc.gdx;
+        double f[3] = {0.0, 0.0, 0.0};
+        for (int q0 = 0; q0 < count; q0 += 32) {
+            const int q = q0 + lane;
+            int r = 0;  // row of contribution q: rows whose prefix end is <= q come before it
+#pragma unroll
+            for (int k = 0; k < S * S; k++) r += (__shfl_sync(0xffffffffu, end, k) <= q) ? 1 : 0;
+            r = min(r, S * S - 1);
+            const int r_end = __shfl_sync(0xffffffffu, end, r), r_len = __shfl_sync(0xffffffffu, len, r);
+            const int r_lo = __shfl_sync(0xffffffffu, lo, r);
+            if (q < count) {
+                const int e = r_lo + q - (r_end - r_len);
+                const SpreadRec &w = rec[e];
+                const double4 F = frc[e];
+                const double wy = w.w[4 + S - 1 - r % S], wz = w.w[8 + S - 1 - r / S];
+                const double wx = w.w[ci - w.b0];
+                f[0] += F.x * wx * wy * wz * inv3;
+                f[1] += F.y * wx * wy * wz * inv3;
+                f[2] += F.z * wx * wy * wz * inv3;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            for (int o = 16; o > 0; o >>= 1) f[c] += __shfl_down_sync(0xffffffffu, f[c], o);
+        if (lane == 0) {
+            double *pf = A.patch_force + ((size_t)ms.patch_off + pc) * 3;
+            pf[0] = f[0];
+            pf[1] = f[1];
+            pf[2] = f[2];
+        }
     }
 }
 
@@ -776,17 +823,15 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
                     cudaEvent_t ev_sorted) {
     const size_t smem = (size_t)(a.sort_capacity > 0 ? a.sort_capacity : 1) * sizeof(unsigned long long);
     const dim3 spring_grid((a.max_springs + 127) / 128, a.n_membranes);
-    if (a.mode == kModeReference) {
-        launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
+    if (a.mode != kModeStep) {  // stress-free reference pass, initial pass
+        launch_hi(k_mem_springs<true>, spring_grid, dim3(128), 0, s, a);
         return 1;
     }
-    if (a.mode == kModeInitial) {
-        launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
-        return 1;
-    }
+    int n = 0;
     const int blocks = (a.total_nodes * 32 + 255) / 256;
     if (a.state_is_float) launch_hi(k_mem_advect<float>, dim3(blocks), dim3(256), 0, s, a);
     else launch_hi(k_mem_advect<double>, dim3(blocks), dim3(256), 0, s, a);
+    n++;
     // the node sort needs only the advected positions: side stream
     const bool side = s_side != nullptr && ev_advected != nullptr && ev_sorted != nullptr;
     if (side) {
@@ -794,14 +839,23 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
         cudaStreamWaitEvent(s_side, ev_advected, 0);
     }
     launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, side ? s_side : s, a);
+    n++;
     if (side) cudaEventRecord(ev_sorted, s_side);
-    launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
-    launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
+    if (a.separate_totals) {
+        launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(128), 0, s, a);
+        launch_hi(k_mem_springs<false>, spring_grid, dim3(128), 0, s, a);
+        n += 2;
+    } else {
+        launch_hi(k_mem_springs<true>, spring_grid, dim3(128), 0, s, a);
+        n++;
+    }
+    // node forces go to the sorted positions the sort wrote
     if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
+    launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
     const dim3 grid(a.spread_blocks);
-    if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(128), 0, s, a);
-    else launch_hi(k_mem_spread<2>, grid, dim3(128), 0, s, a);
-    return 5;
+    if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
+    else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a);
+    return n + 2;
 }
 
 void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s) {
@@ -811,8 +865,8 @@ void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s) {
 
 void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s) {
     const dim3 grid(a.spread_blocks);
-    if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(128), 0, s, a);
-    else launch_hi(k_mem_spread<2>, grid, dim3(128), 0, s, a);
+    if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
+    else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a);
 }
 
 void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s) {

@@ -407,17 +407,18 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     std::vector<double> zeros_n(N, 0.0), zeros_s(S, 0.0), zeros_2s(2 * (size_t)S, 0.0);
     std::vector<MembraneScalars> msz(n_rbc);
     std::memset(msz.data(), 0, sizeof(MembraneScalars) * n_rbc);
-    long long total_patch = 0, spread_tiles = 0;
+    long long total_patch = 0;
     for (int r = 0; r < n_rbc; r++) {
         msz[r].patch_off = (int)total_patch;
         total_patch += mc[r].patch_bound;
-        spread_tiles += (mc[r].patch_bound + 127) / 128;
     }
     if (total_patch + n_rbc > INT32_MAX) return set_error(LBFS_ERR_LIMIT, "IBM patches exceed 2^31 cells in total");
     s->total_patch = total_patch;
-    ma.spread_blocks = (int)std::max<long long>(1, std::min<long long>(spread_tiles, kSpreadMaxBlocks));
+    // one warp per patch cell, 8 warps a block, grid-stride
+    ma.spread_blocks = (int)std::max<long long>(1, std::min<long long>((total_patch + 7) / 8, kSpreadMaxBlocks));
     int rc = 0;
-    std::vector<int> spring_mem(S), node_mem(N);
+    std::vector<int> spring_mem(S), node_mem(N), identity(N);
+    for (int n = 0; n < N; n++) identity[n] = n;
     for (int r = 0; r < n_rbc; r++) {
         for (int q = 0; q < mc[r].n_springs; q++) spring_mem[mc[r].spring0 + q] = r;
         for (int q = 0; q < mc[r].n_nodes; q++) node_mem[mc[r].node0 + q] = r;
@@ -445,18 +446,19 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         (rc = s->upload(&ma.angle0, zeros_s)) || (rc = s->upload(&ma.area0, zeros_2s)) ||
         (rc = s->upload(&ma.area, zeros_2s)) || (rc = s->alloc(&ma.contrib, 12 * (size_t)S)) ||
         (rc = s->alloc(&ma.keys, N)) || (rc = s->alloc(&ma.patch_force, (size_t)total_patch * 3)) ||
-        (rc = s->upload(&d_smem, spring_mem)) || (rc = s->alloc(&ma.node_base, 3 * (size_t)N)) ||
-        (rc = s->alloc(&ma.node_w, 12 * (size_t)N)) ||
+        (rc = s->upload(&d_smem, spring_mem)) ||
         (rc = s->alloc(&ma.bin_start, (size_t)total_patch + n_rbc)) ||
-        (rc = s->alloc(&ma.tile_start, (size_t)n_rbc + 1)) || (rc = s->alloc(&ma.sort_ticket, 1)) ||
-        (rc = s->alloc(&ma.spread_rec, (size_t)N)) ||
+        (rc = s->alloc(&ma.cell_start, (size_t)n_rbc + 1)) || (rc = s->alloc(&ma.sort_ticket, 1)) ||
+        (rc = s->alloc(&ma.spread_rec, (size_t)N)) || (rc = s->upload(&ma.sorted_pos, identity)) ||
+        (rc = s->alloc(&ma.sorted_force, (size_t)N)) ||
         (rc = s->alloc(&ma.mad_partials, (size_t)n_rbc * kMaxSpringBlocks)) ||
         (rc = s->alloc(&ma.mad_ticket, (size_t)n_rbc)))
         return rc;
     LBFS_CUDA(cudaMemset(ma.mad_ticket, 0, sizeof(unsigned int) * n_rbc));
     LBFS_CUDA(cudaMemset(ma.sort_ticket, 0, sizeof(unsigned int)));
-    LBFS_CUDA(cudaMemset(ma.tile_start, 0, sizeof(int) * (n_rbc + 1)));
+    LBFS_CUDA(cudaMemset(ma.cell_start, 0, sizeof(int) * (n_rbc + 1)));
     LBFS_CUDA(cudaMemset(ma.patch_force, 0, sizeof(double) * 3 * (size_t)total_patch));
+    LBFS_CUDA(cudaMemset(ma.sorted_force, 0, sizeof(double4) * (size_t)N));
     ma.max_springs = 0;
     ma.max_patch_bound = 0;
     for (int r = 0; r < n_rbc; r++) {
@@ -464,6 +466,12 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         ma.max_patch_bound = std::max(ma.max_patch_bound, mc[r].patch_bound);
     }
     ma.node_mem = d_nmem;
+    {
+        // totals in their own kernel once the spring blocks fill the GPU
+        long long spring_blocks = 0;
+        for (int r = 0; r < n_rbc; r++) spring_blocks += (mc[r].n_springs + 127) / 128;
+        ma.separate_totals = spring_blocks > 2 * 148 ? 1 : 0;
+    }
     ma.spring_mem = d_smem;
     ma.mc = d_mc; ma.ms = d_ms; ma.tri = d_tri; ma.spring = d_spr; ma.inc = d_inc; ma.inc_start = d_incs;
     ma.flags = s->fp32 ? s->f32.flags : s->f64.flags;
@@ -627,7 +635,7 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     rc = setup_membranes(s, mesh, rbc, n_rbc);
     if (rc) return fail(rc);
     // gradients, face flux (axis + general), update; membrane kernels
-    s->launches_per_step = 4 + (n_rbc > 0 ? 5 : 0);
+    s->launches_per_step = 4 + (n_rbc > 0 ? 5 + s->ma.separate_totals : 0);
     *out = s;
     return LBFS_OK;
 }
@@ -941,7 +949,7 @@ extern "C" int lbfs_status(lbfs_solver *s, uint32_t *flags) {
 
 extern "C" int lbfs_launches_per_step(lbfs_solver *s, int32_t *launches) {
     if (!s || !launches) return set_error(LBFS_ERR_ARG, "null argument");
-    *launches = s->launches_per_step;
+    *launches = 4 + (s->n_membranes > 0 ? 5 + s->ma.separate_totals : 0);
     return LBFS_OK;
 }
 
@@ -960,6 +968,7 @@ template <typename R> void shape_to_args(lbfs_solver *s, const lbfs_launch_shape
     a.tb_grad = sh.gradient_threads; a.tb_flux = sh.flux_threads; a.tb_gen = sh.general_flux_threads;
     a.tb_update = sh.update_threads; a.update_blocks = sh.update_blocks;
     s->ma.spread_blocks = sh.spread_blocks;
+    s->ma.separate_totals = sh.membrane_totals;
 }
 
 template <typename R> lbfs_launch_shape args_to_shape(lbfs_solver *s) {
@@ -968,6 +977,7 @@ template <typename R> lbfs_launch_shape args_to_shape(lbfs_solver *s) {
     sh.gradient_threads = a.tb_grad; sh.flux_threads = a.tb_flux; sh.general_flux_threads = a.tb_gen;
     sh.update_threads = a.tb_update; sh.update_blocks = a.update_blocks;
     sh.spread_blocks = s->ma.spread_blocks > 0 ? s->ma.spread_blocks : 1;
+    sh.membrane_totals = s->ma.separate_totals;
     return sh;
 }
 
@@ -984,6 +994,8 @@ int check_shape(const lbfs_launch_shape &sh) {
     if (sh.update_blocks < 1 || sh.update_blocks > LBFS_MAX_UPDATE_BLOCKS || sh.spread_blocks < 1 ||
         sh.spread_blocks > LBFS_MAX_SPREAD_BLOCKS)
         return set_error(LBFS_ERR_ARG, "launch shape: grid caps out of range");
+    if (sh.membrane_totals != 0 && sh.membrane_totals != 1)
+        return set_error(LBFS_ERR_ARG, "launch shape: membrane_totals must be 0 or 1");
     return LBFS_OK;
 }
 

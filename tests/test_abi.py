@@ -43,7 +43,7 @@ def test_struct_layout_matches_c_compiler(tmp_path):
     # every field offset of the ctypes mirrors equals the C compiler's offsetof
     from lbfs_b200 import _abi
     structs = {"lbfs_mesh_desc": _abi.MeshDesc, "lbfs_grid_desc": _abi.GridDesc, "lbfs_params": _abi.Params,
-               "lbfs_rbc_desc": _abi.RbcDesc}
+               "lbfs_rbc_desc": _abi.RbcDesc, "lbfs_launch_shape": _abi.LaunchShape}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "lbfs_b200.h"', 'int main(void) {']
     for cname, py in structs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
