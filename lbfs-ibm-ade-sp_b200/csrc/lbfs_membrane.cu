@@ -673,11 +673,17 @@ __global__ void __launch_bounds__(256) k_mem_spread(MembraneArgs A) {
     const int total = __ldg(A.cell_start + M);
     const int n_warps = (gridDim.x * blockDim.x) >> 5;
     for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < total; t += n_warps) {
-        int lo_m = 0, hi_m = M;  // membrane m with cell_start[m] <= t < cell_start[m + 1]
+        // membrane m with cell_start[m] <= t < cell_start[m + 1]: the warp probes
+        // 32 evenly spaced entries of [lo_m, hi_m) per round (one load per lane)
+        int lo_m = 0, hi_m = M;
         while (hi_m - lo_m > 1) {
-            const int mid = (lo_m + hi_m) >> 1;
-            if (__ldg(A.cell_start + mid) <= t) lo_m = mid;
-            else hi_m = mid;
+            const int step = (hi_m - lo_m + 31) / 32;
+            const int probe = lo_m + lane * step;
+            const bool le = probe < hi_m && __ldg(A.cell_start + probe) <= t;
+            const unsigned ballot = __ballot_sync(0xffffffffu, le);
+            const int last = 31 - __clz(ballot);  // lane 0 always qualifies: cell_start[lo_m] <= t
+            lo_m = lo_m + last * step;
+            hi_m = min(hi_m, lo_m + step);
         }
         const int m = lo_m;
         const MembraneScalars &ms = A.ms[m];
