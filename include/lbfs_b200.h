@@ -239,6 +239,29 @@ int lbfs_get_launch_shape(lbfs_solver *s, lbfs_launch_shape *shape);
 int lbfs_set_launch_shape(lbfs_solver *s, const lbfs_launch_shape *shape);
 int lbfs_autotune(lbfs_solver *s, int32_t reps, lbfs_launch_shape *shape);
 
+/* ---- discrete adjoint (no reference counterpart) --------------------------- *
+ * lbfs_adjoint runs n_steps forward from the handle's state, keeping soln_t1
+ * (and, with membranes, node positions and MAD) every `checkpoint_every`
+ * steps, evaluates the objective on the final state, then sweeps backwards
+ * segment by segment: each segment is recomputed from its checkpoint and the
+ * discrete adjoint of every step is applied in reverse.  FP64 handles without
+ * preconditioning.  On return the handle holds the final forward state and
+ * the step counter has advanced by n_steps.
+ *   J        objective value
+ *   grad[0]  dJ / d(shear modulus of every membrane)
+ *   grad[1]  dJ / d(global bending modulus of every membrane)
+ *   grad[2]  dJ / d sigma, every boundary velocity value scaled by sigma at 1
+ *   times_ms (may be null): forward sweep and reverse sweep, device time. */
+#define LBFS_OBJ_VELOCITY 0   /* J = sum over cells of w_c . (u, v, w)_c at the final step */
+#define LBFS_OBJ_TAYLOR 1     /* J = Taylor deformation (L - B) / (L + B) of one membrane in the x-y plane */
+typedef struct lbfs_objective {
+    int32_t kind;
+    int32_t membrane;             /* LBFS_OBJ_TAYLOR */
+    const double *cell_weights;   /* LBFS_OBJ_VELOCITY: 3 per interior cell */
+} lbfs_objective;
+int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_every, const lbfs_objective *obj, double *J,
+                 double *grad, double *times_ms);
+
 /* ---- residual norms without device allocation ---------------------------- */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc --

@@ -18,6 +18,7 @@
 #include <string>
 #include <vector>
 
+#include "lbfs_adjoint.h"
 #include "lbfs_b200.h"
 #include "lbfs_fluid.cuh"
 #include "lbfs_internal.h"
@@ -79,6 +80,9 @@ struct lbfs_solver {
     std::vector<lbfs_grid_desc> grids;
     std::vector<InstanceGrid> inst;
     long long total_patch = 0;  // cells of all IBM patch slices
+    // discrete adjoint: persistent buffers (allocated on first use)
+    AdjointArgs adj{};
+    bool adj_ready = false;
 
     template <typename T> int alloc(T **p, size_t count) {
         void *q = nullptr;
@@ -1141,4 +1145,171 @@ extern "C" int lbfs_autotune(lbfs_solver *s, int32_t reps, lbfs_launch_shape *sh
     if (reps < 1 || reps > 1000) return set_error(LBFS_ERR_ARG, "reps must be in 1..1000");
     LBFS_CUDA(cudaSetDevice(s->device));
     return s->fp32 ? autotune<float>(s, reps, shape) : autotune<double>(s, reps, shape);
+}
+
+
+// ---- discrete adjoint -------------------------------------------------------
+
+namespace {
+
+int adj_prepare(lbfs_solver *s) {
+    if (s->adj_ready) return LBFS_OK;
+    AdjointArgs &j = s->adj;
+    const int nc = s->nc, nf = s->nf, nb = s->nb;
+    int rc;
+    if ((rc = s->alloc(&j.lam_t1, nc)) || (rc = s->alloc(&j.lam_face, 32 * (size_t)nf)) ||
+        (rc = s->alloc(&j.lam_bcv, 4 * (size_t)(nb > 0 ? nb : 1))) || (rc = s->alloc(&j.lam_rs, 12 * (size_t)nc)) ||
+        (rc = s->alloc(&j.lam_state, 4 * (size_t)nc)) || (rc = s->alloc(&j.sigma_acc, nc)))
+        return rc;
+    LBFS_CUDA(cudaMemset(j.lam_bcv, 0, sizeof(double) * 4 * (size_t)(nb > 0 ? nb : 1)));
+    // transposed gradient stencil: for each interior cell, the (cell, slot) pairs that read it
+    std::vector<int2> st(3 * (size_t)nc);
+    LBFS_CUDA(cudaMemcpy(st.data(), s->f64.stencil, sizeof(int2) * st.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> start(nc + 1, 0);
+    auto entry = [&](int i, int q) { return q & 1 ? st[3 * (size_t)i + q / 2].y : st[3 * (size_t)i + q / 2].x; };
+    for (int i = 0; i < nc; i++)
+        for (int q = 0; q < 6; q++) {
+            const int c = entry(i, q);
+            if (c < nc) start[c + 1]++;
+        }
+    for (int c = 0; c < nc; c++) start[c + 1] += start[c];
+    std::vector<int> fill(start.begin(), start.end() - 1), tst(start[nc] > 0 ? start[nc] : 1);
+    for (int i = 0; i < nc; i++)
+        for (int q = 0; q < 6; q++) {
+            const int c = entry(i, q);
+            if (c < nc) tst[fill[c]++] = 8 * i + q;
+        }
+    int *d_start, *d_tst;
+    if ((rc = s->upload(&d_start, start)) || (rc = s->upload(&d_tst, tst))) return rc;
+    j.tst_start = d_start;
+    j.tst = d_tst;
+    j.dt = s->params.delta_t;
+    j.lam_u_ibm = nullptr;
+    s->adj_ready = true;
+    return LBFS_OK;
+}
+
+// Device buffer freed when it leaves scope (temporary adjoint storage).
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+
+int run_one_step(lbfs_solver *s) {
+    if (visc_due(s, s->t)) {
+        int rc = enqueue(s, true, nullptr);
+        if (rc) return rc;
+    } else {
+        int rc = lbfs_step_graph(s, 1);
+        if (rc) return rc;
+        s->t--;  // lbfs_step_graph advanced it
+    }
+    s->t++;
+    return LBFS_OK;
+}
+
+}  // namespace
+
+extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_every, const lbfs_objective *obj,
+                            double *J, double *grad, double *times_ms) {
+    if (!s || !obj || !J || !grad || n_steps < 1 || checkpoint_every < 1)
+        return set_error(LBFS_ERR_ARG, "lbfs_adjoint: bad arguments");
+    if (s->fp32) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: FP64 handles only");
+    if (s->params.gamma_inv != 1.0) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: no preconditioning");
+    if (s->n_membranes > 0) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: membranes not supported yet");
+    if (obj->kind != LBFS_OBJ_VELOCITY || !obj->cell_weights)
+        return set_error(LBFS_ERR_ARG, "lbfs_adjoint: objective kind/weights");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    int rc = adj_prepare(s);
+    if (rc) return rc;
+    FluidArgs<double> &a = s->f64;
+    AdjointArgs &j = s->adj;
+    const int nc = s->nc, nt = s->nc + s->nb;
+    const int K = checkpoint_every, n_ck = (n_steps + K - 1) / K;
+    cudaStream_t st = s->stream;
+    DevBuf ck, seg, st0, fin_t1, fin_state, wts;
+    LBFS_CUDA(cudaMalloc(&ck.p, sizeof(double4) * (size_t)nc * n_ck));
+    LBFS_CUDA(cudaMalloc(&seg.p, sizeof(double4) * (size_t)nc * K));
+    LBFS_CUDA(cudaMalloc(&st0.p, sizeof(Vec4<double>) * (size_t)nt));
+    LBFS_CUDA(cudaMalloc(&fin_t1.p, sizeof(double4) * (size_t)nc));
+    LBFS_CUDA(cudaMalloc(&fin_state.p, sizeof(Vec4<double>) * (size_t)nt));
+    LBFS_CUDA(cudaMalloc(&wts.p, sizeof(double) * 3 * (size_t)nc));
+    LBFS_CUDA(cudaMemcpyAsync(wts.p, obj->cell_weights, sizeof(double) * 3 * (size_t)nc, cudaMemcpyHostToDevice, st));
+    double4 *ck_t1 = (double4 *)ck.p, *seg_t1 = (double4 *)seg.p;
+    const long long t_start = s->t;
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
+    // ---- forward sweep with checkpoints
+    LBFS_CUDA(cudaMemcpyAsync(st0.p, a.state, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
+    cudaEventRecord(e0, st);
+    for (int n = 0; n < n_steps; n++) {
+        if (n % K == 0)
+            LBFS_CUDA(cudaMemcpyAsync(ck_t1 + (size_t)(n / K) * nc, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
+        if ((rc = run_one_step(s))) return rc;
+    }
+    cudaEventRecord(e1, st);
+    LBFS_CUDA(cudaMemcpyAsync(fin_t1.p, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
+    LBFS_CUDA(cudaMemcpyAsync(fin_state.p, a.state, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
+    // ---- objective at the final state (host, fixed order)
+    {
+        std::vector<double4> t1h(nc);
+        LBFS_CUDA(cudaMemcpyAsync(t1h.data(), a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToHost, st));
+        LBFS_CUDA(cudaStreamSynchronize(st));
+        double acc = 0.0;
+        for (int c = 0; c < nc; c++) {
+            const double *w = obj->cell_weights + 3 * (size_t)c;
+            acc += w[0] * (t1h[c].x / t1h[c].w) + w[1] * (t1h[c].y / t1h[c].w) + w[2] * (t1h[c].z / t1h[c].w);
+        }
+        *J = acc;
+    }
+    // ---- reverse sweep
+    LBFS_CUDA(cudaMemsetAsync(j.lam_t1, 0, sizeof(double4) * nc, st));
+    LBFS_CUDA(cudaMemsetAsync(j.sigma_acc, 0, sizeof(double) * nc, st));
+    launch_adj_velocity_seed(a, j, (const double *)wts.p, st);
+    for (int sg = n_ck - 1; sg >= 0; sg--) {
+        const int n0 = sg * K, n1 = std::min(n_steps, n0 + K);
+        // re-run the segment from its checkpoint, keeping t1 before every step
+        LBFS_CUDA(cudaMemcpyAsync(a.t1, ck_t1 + (size_t)sg * nc, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
+        if (n0 == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
+        else launch_adj_prim(a, st);
+        for (int n = n0; n < n1; n++) {
+            LBFS_CUDA(cudaMemcpyAsync(seg_t1 + (size_t)(n - n0) * nc, a.t1, sizeof(double4) * nc,
+                                      cudaMemcpyDeviceToDevice, st));
+            if (n + 1 < n1) {
+                s->t = t_start + n;
+                if ((rc = run_one_step(s))) return rc;
+            }
+        }
+        for (int n = n1 - 1; n >= n0; n--) {
+            LBFS_CUDA(cudaMemcpyAsync(a.t1, seg_t1 + (size_t)(n - n0) * nc, sizeof(double4) * nc,
+                                      cudaMemcpyDeviceToDevice, st));
+            if (n == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
+            else launch_adj_prim(a, st);
+            launch_fluid_gradients<double>(a, st);
+            launch_adj_fluid(a, j, st);
+            LBFS_CUDA(cudaGetLastError());
+        }
+    }
+    cudaEventRecord(e2, st);
+    // ---- final forward state back, sensitivities
+    LBFS_CUDA(cudaMemcpyAsync(a.t1, fin_t1.p, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
+    LBFS_CUDA(cudaMemcpyAsync(a.state, fin_state.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
+    s->t = t_start + n_steps;
+    std::vector<double> sig(nc);
+    LBFS_CUDA(cudaMemcpyAsync(sig.data(), j.sigma_acc, sizeof(double) * nc, cudaMemcpyDeviceToHost, st));
+    LBFS_CUDA(cudaStreamSynchronize(st));
+    double sigma = 0.0;
+    for (int c = 0; c < nc; c++) sigma += sig[c];
+    grad[0] = 0.0;
+    grad[1] = 0.0;
+    grad[2] = sigma;
+    if (times_ms) {
+        float f = 0, r = 0;
+        cudaEventElapsedTime(&f, e0, e1);
+        cudaEventElapsedTime(&r, e1, e2);
+        times_ms[0] = f;
+        times_ms[1] = r;
+    }
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+    return LBFS_OK;
 }

@@ -107,6 +107,13 @@ class LaunchShape(ctypes.Structure):
     ]
 
 
+class Objective(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("membrane", ctypes.c_int32), ("cell_weights", _f64p)]
+
+
+LBFS_OBJ_VELOCITY = 0
+LBFS_OBJ_TAYLOR = 1
+
 LBFS_MAX_UPDATE_BLOCKS = 148 * 16
 LBFS_MAX_SPREAD_BLOCKS = 148 * 16
 
@@ -152,6 +159,7 @@ def lib():
             "lbfs_get_launch_shape": [vp, ctypes.POINTER(LaunchShape)],
             "lbfs_set_launch_shape": [vp, ctypes.POINTER(LaunchShape)],
             "lbfs_autotune": [vp, ctypes.c_int32, ctypes.POINTER(LaunchShape)],
+            "lbfs_adjoint": [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(Objective), _f64p, _f64p, _f64p],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -192,4 +200,5 @@ EXPORTED = [
     "lbfs_set_profiling", "lbfs_get_phase_times",
     "lbfs_last_error", "lbfs_mesh_uniform_counts", "lbfs_mesh_build_uniform", "lbfs_rbc_build_springs",
     "lbfs_residual_rms_noalloc", "lbfs_get_launch_shape", "lbfs_set_launch_shape", "lbfs_autotune",
+    "lbfs_adjoint",
 ]

@@ -186,6 +186,28 @@ class GpuSolver:
         _abi.check(_abi.lib().lbfs_autotune(self._h, int(reps), ctypes.byref(sh)))
         return _shape_dict(sh)
 
+    def adjoint(self, n_steps, checkpoint_every=25, weights=None, membrane=None):
+        """Discrete adjoint over n_steps from the current state.  Objective: the
+        Taylor deformation of `membrane` (x-y plane) when given, else
+        sum_c weights[c] . (u, v, w)_c at the final step.  Returns
+        (J, {"shear_modulus", "bending_modulus", "velocity_scale"}, times_ms);
+        the handle ends on the final forward state."""
+        obj = _abi.Objective()
+        keep = None
+        if membrane is not None:
+            obj.kind, obj.membrane = _abi.LBFS_OBJ_TAYLOR, int(membrane)
+        else:
+            keep = np.ascontiguousarray(weights, np.float64).reshape(-1)
+            if keep.size != 3 * self.n_cells:
+                raise ValueError("weights: 3 per interior cell")
+            obj.kind, obj.cell_weights = _abi.LBFS_OBJ_VELOCITY, _abi.ptr(keep)
+        J = ctypes.c_double()
+        g = np.zeros(3)
+        t = np.zeros(2)
+        _abi.check(_abi.lib().lbfs_adjoint(self._h, int(n_steps), int(checkpoint_every), ctypes.byref(obj),
+                                           ctypes.byref(J), _abi.ptr(g), _abi.ptr(t)))
+        return J.value, dict(zip(("shear_modulus", "bending_modulus", "velocity_scale"), g.tolist())), t.tolist()
+
     def launches_per_step(self):
         n = ctypes.c_int32()
         _abi.check(_abi.lib().lbfs_launches_per_step(self._h, ctypes.byref(n)))
