@@ -21,6 +21,30 @@ struct AdjointArgs {
     const double *lam_u_ibm;     // [3 nc] adjoint of the cell velocities through the IBM interpolation (or null)
 };
 
+// Membrane part of the adjoint (lbfs_adjoint_mem.cu).
+struct MemAdjArgs {
+    double dt;
+    const double4 *lam_t1;       // fluid adjoint of t1_{n+1}: the IBM force adjoint is dt * its momentum part
+    double *lam_x;               // [3 N] node-position adjoint, carried between steps (in: x_{n+1}, out: x_n)
+    double *lam_xp;              // [3 N] adjoint of x' = x_{n+1} within the step
+    double *lam_F;               // [3 N] node-force adjoint
+    double *adjm;                // [17 S] spring adjoint per input direction
+    double *lam_mad;             // [M] MAD adjoint, carried (in: MAD_{n+1}, out: MAD_n)
+    double *red;                 // [5 M] per-membrane sums of the step
+    double *gs_acc, *kb_acc;     // [M] d J / d G_s, d J / d k_b, summed over the steps
+    const double *mad_n;         // [M] MAD at the start of the step
+    const int *tri_start;        // [N + 1] node -> triangle incidence
+    const int *tri_inc;          // codes 4 t + vertex
+    const double *xn, *yn, *zn;  // node positions at the start of the step
+    double *lam_u_ibm;           // [3 nc] cell velocity adjoint through the IBM interpolation
+    MembraneArgs mb;             // sort / spread buffers of the interpolation transpose (positions xn)
+};
+
+void launch_adjm_get_mad(const MembraneArgs &A, double *out, cudaStream_t s);
+void launch_adjm_set_mad(const MembraneArgs &A, const double *in, cudaStream_t s);
+int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, const int *cell_instance,
+                        const InstanceGrid *instances, cudaStream_t s);
+
 void launch_adj_prim(const FluidArgs<double> &a, cudaStream_t s);
 void launch_adj_velocity_seed(const FluidArgs<double> &a, const AdjointArgs &j, const double *weights, cudaStream_t s);
 int launch_adj_fluid(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);

@@ -83,6 +83,8 @@ struct lbfs_solver {
     // discrete adjoint: persistent buffers (allocated on first use)
     AdjointArgs adj{};
     bool adj_ready = false;
+    MemAdjArgs madj{};
+    bool madj_ready = false;
 
     template <typename T> int alloc(T **p, size_t count) {
         void *q = nullptr;
@@ -1208,6 +1210,83 @@ int run_one_step(lbfs_solver *s) {
     return LBFS_OK;
 }
 
+// Membrane adjoint buffers: the adjoints, the node -> triangle incidence, and
+// a second set of sort / spread buffers (the interpolation transpose).
+int adjm_prepare(lbfs_solver *s) {
+    if (s->madj_ready) return LBFS_OK;
+    MemAdjArgs &J = s->madj;
+    const MembraneArgs &ma = s->ma;
+    const int N = s->total_nodes, S = s->total_springs, M = s->n_membranes, T = s->total_tris;
+    int rc;
+    if ((rc = s->alloc(&J.lam_x, 3 * (size_t)N)) || (rc = s->alloc(&J.lam_xp, 3 * (size_t)N)) ||
+        (rc = s->alloc(&J.lam_F, 3 * (size_t)N)) || (rc = s->alloc(&J.adjm, 17 * (size_t)S)) ||
+        (rc = s->alloc(&J.lam_mad, M)) || (rc = s->alloc(&J.red, 5 * (size_t)M)) || (rc = s->alloc(&J.gs_acc, M)) ||
+        (rc = s->alloc(&J.kb_acc, M)) || (rc = s->alloc(&J.lam_u_ibm, 3 * (size_t)s->nc)))
+        return rc;
+    std::vector<int> tri(3 * (size_t)T);
+    LBFS_CUDA(cudaMemcpy(tri.data(), ma.tri, sizeof(int) * tri.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> start(N + 1, 0);
+    for (int q = 0; q < 3 * T; q++) start[tri[q] + 1]++;
+    for (int n = 0; n < N; n++) start[n + 1] += start[n];
+    std::vector<int> fill(start.begin(), start.end() - 1), inc(3 * (size_t)T);
+    for (int t = 0; t < T; t++)
+        for (int v = 0; v < 3; v++) inc[fill[tri[3 * t + v]]++] = 4 * t + v;
+    int *d_start, *d_inc;
+    if ((rc = s->upload(&d_start, start)) || (rc = s->upload(&d_inc, inc))) return rc;
+    J.tri_start = d_start;
+    J.tri_inc = d_inc;
+    // second sort / spread set
+    MembraneArgs mb = ma;
+    std::vector<int> identity(N);
+    for (int n = 0; n < N; n++) identity[n] = n;
+    MembraneScalars *ms2;
+    if ((rc = s->alloc(&ms2, M)) || (rc = s->alloc(&mb.spread_rec, N)) ||
+        (rc = s->alloc(&mb.bin_start, (size_t)s->total_patch + M)) || (rc = s->alloc(&mb.cell_start, (size_t)M + 1)) ||
+        (rc = s->alloc(&mb.sort_ticket, 1)) || (rc = s->upload(&mb.sorted_pos, identity)) ||
+        (rc = s->alloc(&mb.sorted_force, N)) || (rc = s->alloc(&mb.patch_force, 3 * (size_t)s->total_patch)))
+        return rc;
+    LBFS_CUDA(cudaMemcpy(ms2, ma.ms, sizeof(MembraneScalars) * M, cudaMemcpyDeviceToDevice));
+    LBFS_CUDA(cudaMemset(mb.sort_ticket, 0, sizeof(unsigned int)));
+    LBFS_CUDA(cudaMemset(mb.cell_start, 0, sizeof(int) * (M + 1)));
+    LBFS_CUDA(cudaMemset(mb.sorted_force, 0, sizeof(double4) * N));
+    mb.ms = ms2;
+    J.mb = mb;
+    J.dt = s->params.delta_t;
+    s->madj_ready = true;
+    return LBFS_OK;
+}
+
+// Taylor deformation (L - B) / (L + B) of one membrane in the x-y plane, L and
+// B the square roots of the eigenvalues of its nodes' 2-D second-moment
+// tensor about their centroid; and dD / d(node positions).
+double taylor_deformation(const double *x, const double *y, int n, double *gx, double *gy) {
+    double cx = 0, cy = 0;
+    for (int i = 0; i < n; i++) { cx += x[i]; cy += y[i]; }
+    cx /= n;
+    cy /= n;
+    double Ixx = 0, Iyy = 0, Ixy = 0;
+    for (int i = 0; i < n; i++) {
+        const double dx = x[i] - cx, dy = y[i] - cy;
+        Ixx += dx * dx; Iyy += dy * dy; Ixy += dx * dy;
+    }
+    const double T = 0.5 * (Ixx + Iyy), D = 0.5 * (Ixx - Iyy), R = std::sqrt(D * D + Ixy * Ixy);
+    const double lp = T + R, lm = T - R;
+    const double L = std::sqrt(lp), B = std::sqrt(lm);
+    const double J = (L - B) / (L + B);
+    const double dJdL = 2 * B / ((L + B) * (L + B)), dJdB = -2 * L / ((L + B) * (L + B));
+    const double dJdlp = dJdL / (2 * L), dJdlm = dJdB / (2 * B);
+    // d lambda+- / d(Ixx, Iyy, Ixy)
+    const double dxx = dJdlp * (0.5 + 0.5 * D / R) + dJdlm * (0.5 - 0.5 * D / R);
+    const double dyy = dJdlp * (0.5 - 0.5 * D / R) + dJdlm * (0.5 + 0.5 * D / R);
+    const double dxy = dJdlp * (Ixy / R) - dJdlm * (Ixy / R);
+    for (int i = 0; i < n; i++) {
+        const double dx = x[i] - cx, dy = y[i] - cy;
+        gx[i] = dxx * 2 * dx + dxy * dy;
+        gy[i] = dyy * 2 * dy + dxy * dx;
+    }
+    return J;
+}
+
 }  // namespace
 
 extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_every, const lbfs_objective *obj,
@@ -1216,42 +1295,111 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
         return set_error(LBFS_ERR_ARG, "lbfs_adjoint: bad arguments");
     if (s->fp32) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: FP64 handles only");
     if (s->params.gamma_inv != 1.0) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: no preconditioning");
-    if (s->n_membranes > 0) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: membranes not supported yet");
-    if (obj->kind != LBFS_OBJ_VELOCITY || !obj->cell_weights)
-        return set_error(LBFS_ERR_ARG, "lbfs_adjoint: objective kind/weights");
+    if (obj->kind == LBFS_OBJ_VELOCITY) {
+        if (!obj->cell_weights) return set_error(LBFS_ERR_ARG, "lbfs_adjoint: velocity objective needs weights");
+    } else if (obj->kind == LBFS_OBJ_TAYLOR) {
+        if (obj->membrane < 0 || obj->membrane >= s->n_membranes)
+            return set_error(LBFS_ERR_ARG, "lbfs_adjoint: objective membrane out of range");
+    } else {
+        return set_error(LBFS_ERR_ARG, "lbfs_adjoint: unknown objective");
+    }
     LBFS_CUDA(cudaSetDevice(s->device));
+    const int M = s->n_membranes, N = s->total_nodes;
+    std::vector<MembraneConst> mch(M);
+    if (M > 0) {
+        LBFS_CUDA(cudaMemcpy(mch.data(), s->ma.mc, sizeof(MembraneConst) * M, cudaMemcpyDeviceToHost));
+        bool visc_in_window = false;
+        for (long long t = s->t; t < s->t + n_steps; t++) visc_in_window = visc_in_window || visc_due(s, t);
+        for (const MembraneConst &c : mch) {
+            if (c.viscosity != 0.0) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: membrane viscosity must be 0");
+            if (!(c.shear_modulus > 0.0)) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: shear modulus must be > 0");
+            if (visc_in_window && c.internal_viscosity_ratio != 1.0)
+                return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: an interior-viscosity update falls in the window "
+                                                       "(its position dependence is not differentiated) unless the "
+                                                       "interior viscosity ratio is 1");
+        }
+    }
     int rc = adj_prepare(s);
     if (rc) return rc;
+    if (M > 0 && (rc = adjm_prepare(s))) return rc;
     FluidArgs<double> &a = s->f64;
+    MembraneArgs &ma = s->ma;
     AdjointArgs &j = s->adj;
+    MemAdjArgs &mj = s->madj;
     const int nc = s->nc, nt = s->nc + s->nb;
     const int K = checkpoint_every, n_ck = (n_steps + K - 1) / K;
+    const size_t xs = 3 * (size_t)N;  // positions of one step: x, y, z planes
     cudaStream_t st = s->stream;
-    DevBuf ck, seg, st0, fin_t1, fin_state, wts;
+    DevBuf ck, seg, st0, fin_t1, fin_state, wts, ckx, segx, ckm, segm, finx, finm;
     LBFS_CUDA(cudaMalloc(&ck.p, sizeof(double4) * (size_t)nc * n_ck));
     LBFS_CUDA(cudaMalloc(&seg.p, sizeof(double4) * (size_t)nc * K));
     LBFS_CUDA(cudaMalloc(&st0.p, sizeof(Vec4<double>) * (size_t)nt));
     LBFS_CUDA(cudaMalloc(&fin_t1.p, sizeof(double4) * (size_t)nc));
     LBFS_CUDA(cudaMalloc(&fin_state.p, sizeof(Vec4<double>) * (size_t)nt));
-    LBFS_CUDA(cudaMalloc(&wts.p, sizeof(double) * 3 * (size_t)nc));
-    LBFS_CUDA(cudaMemcpyAsync(wts.p, obj->cell_weights, sizeof(double) * 3 * (size_t)nc, cudaMemcpyHostToDevice, st));
+    if (obj->kind == LBFS_OBJ_VELOCITY) {
+        LBFS_CUDA(cudaMalloc(&wts.p, sizeof(double) * 3 * (size_t)nc));
+        LBFS_CUDA(cudaMemcpyAsync(wts.p, obj->cell_weights, sizeof(double) * 3 * (size_t)nc, cudaMemcpyHostToDevice, st));
+    }
+    if (M > 0) {
+        LBFS_CUDA(cudaMalloc(&ckx.p, sizeof(double) * xs * n_ck));
+        LBFS_CUDA(cudaMalloc(&segx.p, sizeof(double) * xs * K));
+        LBFS_CUDA(cudaMalloc(&ckm.p, sizeof(double) * M * n_ck));
+        LBFS_CUDA(cudaMalloc(&segm.p, sizeof(double) * M * K));
+        LBFS_CUDA(cudaMalloc(&finx.p, sizeof(double) * xs));
+        LBFS_CUDA(cudaMalloc(&finm.p, sizeof(double) * M));
+    }
     double4 *ck_t1 = (double4 *)ck.p, *seg_t1 = (double4 *)seg.p;
+    double *ck_x = (double *)ckx.p, *seg_x = (double *)segx.p, *ck_m = (double *)ckm.p, *seg_m = (double *)segm.p;
+    auto save_x = [&](double *dst) -> int {
+        LBFS_CUDA(cudaMemcpyAsync(dst, ma.x, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+        LBFS_CUDA(cudaMemcpyAsync(dst + N, ma.y, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+        LBFS_CUDA(cudaMemcpyAsync(dst + 2 * (size_t)N, ma.z, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+        return LBFS_OK;
+    };
+    auto load_x = [&](const double *src) -> int {
+        LBFS_CUDA(cudaMemcpyAsync(ma.x, src, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+        LBFS_CUDA(cudaMemcpyAsync(ma.y, src + N, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+        LBFS_CUDA(cudaMemcpyAsync(ma.z, src + 2 * (size_t)N, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+        return LBFS_OK;
+    };
     const long long t_start = s->t;
     cudaEvent_t e0, e1, e2;
     cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
     // ---- forward sweep with checkpoints
     LBFS_CUDA(cudaMemcpyAsync(st0.p, a.state, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
+    LBFS_CUDA(cudaMemsetAsync(a.flags, 0, sizeof(unsigned int), st));
     cudaEventRecord(e0, st);
     for (int n = 0; n < n_steps; n++) {
-        if (n % K == 0)
+        if (n % K == 0) {
             LBFS_CUDA(cudaMemcpyAsync(ck_t1 + (size_t)(n / K) * nc, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
+            if (M > 0) {
+                if ((rc = save_x(ck_x + (size_t)(n / K) * xs))) return rc;
+                launch_adjm_get_mad(ma, ck_m + (size_t)(n / K) * M, st);
+            }
+        }
         if ((rc = run_one_step(s))) return rc;
     }
     cudaEventRecord(e1, st);
     LBFS_CUDA(cudaMemcpyAsync(fin_t1.p, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
     LBFS_CUDA(cudaMemcpyAsync(fin_state.p, a.state, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
-    // ---- objective at the final state (host, fixed order)
-    {
+    if (M > 0) {
+        if ((rc = save_x((double *)finx.p))) return rc;
+        launch_adjm_get_mad(ma, (double *)finm.p, st);
+    }
+    unsigned int flags = 0;
+    LBFS_CUDA(cudaMemcpyAsync(&flags, a.flags, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    LBFS_CUDA(cudaStreamSynchronize(st));
+    if (flags) return set_error(LBFS_ERR_STATE, "lbfs_adjoint: the forward run raised status flags " + std::to_string(flags));
+    // ---- objective and its seed
+    LBFS_CUDA(cudaMemsetAsync(j.lam_t1, 0, sizeof(double4) * nc, st));
+    LBFS_CUDA(cudaMemsetAsync(j.sigma_acc, 0, sizeof(double) * nc, st));
+    if (M > 0) {
+        LBFS_CUDA(cudaMemsetAsync(mj.lam_x, 0, sizeof(double) * xs, st));
+        LBFS_CUDA(cudaMemsetAsync(mj.lam_mad, 0, sizeof(double) * M, st));
+        LBFS_CUDA(cudaMemsetAsync(mj.gs_acc, 0, sizeof(double) * M, st));
+        LBFS_CUDA(cudaMemsetAsync(mj.kb_acc, 0, sizeof(double) * M, st));
+    }
+    if (obj->kind == LBFS_OBJ_VELOCITY) {
         std::vector<double4> t1h(nc);
         LBFS_CUDA(cudaMemcpyAsync(t1h.data(), a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToHost, st));
         LBFS_CUDA(cudaStreamSynchronize(st));
@@ -1261,20 +1409,43 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
             acc += w[0] * (t1h[c].x / t1h[c].w) + w[1] * (t1h[c].y / t1h[c].w) + w[2] * (t1h[c].z / t1h[c].w);
         }
         *J = acc;
+        launch_adj_velocity_seed(a, j, (const double *)wts.p, st);
+    } else {
+        const MembraneConst &c = mch[obj->membrane];
+        std::vector<double> xh(xs), g(xs, 0.0);
+        LBFS_CUDA(cudaMemcpyAsync(xh.data(), finx.p, sizeof(double) * xs, cudaMemcpyDeviceToHost, st));
+        LBFS_CUDA(cudaStreamSynchronize(st));
+        *J = taylor_deformation(xh.data() + c.node0, xh.data() + N + c.node0, c.n_nodes, g.data() + 0,
+                                g.data() + c.n_nodes);
+        // lam_x is node-major (x, y, z per node)
+        std::vector<double> lam(xs, 0.0);
+        for (int i = 0; i < c.n_nodes; i++) {
+            lam[3 * (size_t)(c.node0 + i)] = g[i];
+            lam[3 * (size_t)(c.node0 + i) + 1] = g[c.n_nodes + i];
+        }
+        LBFS_CUDA(cudaMemcpyAsync(mj.lam_x, lam.data(), sizeof(double) * xs, cudaMemcpyHostToDevice, st));
+        LBFS_CUDA(cudaStreamSynchronize(st));
     }
     // ---- reverse sweep
-    LBFS_CUDA(cudaMemsetAsync(j.lam_t1, 0, sizeof(double4) * nc, st));
-    LBFS_CUDA(cudaMemsetAsync(j.sigma_acc, 0, sizeof(double) * nc, st));
-    launch_adj_velocity_seed(a, j, (const double *)wts.p, st);
+    j.lam_u_ibm = M > 0 ? mj.lam_u_ibm : nullptr;
+    mj.lam_t1 = j.lam_t1;
     for (int sg = n_ck - 1; sg >= 0; sg--) {
         const int n0 = sg * K, n1 = std::min(n_steps, n0 + K);
-        // re-run the segment from its checkpoint, keeping t1 before every step
+        // re-run the segment from its checkpoint, keeping the inputs of every step
         LBFS_CUDA(cudaMemcpyAsync(a.t1, ck_t1 + (size_t)sg * nc, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
         if (n0 == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
         else launch_adj_prim(a, st);
+        if (M > 0) {
+            if ((rc = load_x(ck_x + (size_t)sg * xs))) return rc;
+            launch_adjm_set_mad(ma, ck_m + (size_t)sg * M, st);
+        }
         for (int n = n0; n < n1; n++) {
             LBFS_CUDA(cudaMemcpyAsync(seg_t1 + (size_t)(n - n0) * nc, a.t1, sizeof(double4) * nc,
                                       cudaMemcpyDeviceToDevice, st));
+            if (M > 0) {
+                if ((rc = save_x(seg_x + (size_t)(n - n0) * xs))) return rc;
+                launch_adjm_get_mad(ma, seg_m + (size_t)(n - n0) * M, st);
+            }
             if (n + 1 < n1) {
                 s->t = t_start + n;
                 if ((rc = run_one_step(s))) return rc;
@@ -1286,6 +1457,22 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
             if (n == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
             else launch_adj_prim(a, st);
             launch_fluid_gradients<double>(a, st);
+            if (M > 0) {
+                const double *xn = seg_x + (size_t)(n - n0) * xs;
+                const double *mn = seg_m + (size_t)(n - n0) * M;
+                if ((rc = load_x(xn))) return rc;
+                launch_adjm_set_mad(ma, mn, st);
+                launch_membrane(ma, st);  // x -> x', forces, totals, MAD_{n+1}
+                mj.mad_n = mn;
+                mj.xn = xn;
+                mj.yn = xn + N;
+                mj.zn = xn + 2 * (size_t)N;
+                // the interpolation transpose sorts the nodes at x_n (read only)
+                mj.mb.x = const_cast<double *>(mj.xn);
+                mj.mb.y = const_cast<double *>(mj.yn);
+                mj.mb.z = const_cast<double *>(mj.zn);
+                launch_adj_membrane(ma, mj, nc, a.cell_instance, (const InstanceGrid *)a.instances, st);
+            }
             launch_adj_fluid(a, j, st);
             LBFS_CUDA(cudaGetLastError());
         }
@@ -1294,14 +1481,23 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     // ---- final forward state back, sensitivities
     LBFS_CUDA(cudaMemcpyAsync(a.t1, fin_t1.p, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
     LBFS_CUDA(cudaMemcpyAsync(a.state, fin_state.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
+    if (M > 0) {
+        if ((rc = load_x((const double *)finx.p))) return rc;
+        launch_adjm_set_mad(ma, (const double *)finm.p, st);
+    }
     s->t = t_start + n_steps;
-    std::vector<double> sig(nc);
+    std::vector<double> sig(nc), gs(M > 0 ? M : 1, 0.0), kb(M > 0 ? M : 1, 0.0);
     LBFS_CUDA(cudaMemcpyAsync(sig.data(), j.sigma_acc, sizeof(double) * nc, cudaMemcpyDeviceToHost, st));
+    if (M > 0) {
+        LBFS_CUDA(cudaMemcpyAsync(gs.data(), mj.gs_acc, sizeof(double) * M, cudaMemcpyDeviceToHost, st));
+        LBFS_CUDA(cudaMemcpyAsync(kb.data(), mj.kb_acc, sizeof(double) * M, cudaMemcpyDeviceToHost, st));
+    }
     LBFS_CUDA(cudaStreamSynchronize(st));
-    double sigma = 0.0;
+    double sigma = 0.0, gsum = 0.0, ksum = 0.0;
     for (int c = 0; c < nc; c++) sigma += sig[c];
-    grad[0] = 0.0;
-    grad[1] = 0.0;
+    for (int m = 0; m < M; m++) { gsum += gs[m]; ksum += kb[m]; }
+    grad[0] = gsum;
+    grad[1] = ksum;
     grad[2] = sigma;
     if (times_ms) {
         float f = 0, r = 0;
