@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble section")
     ap.add_argument("--instances", type=int, default=64, help="instances of the batched ensemble")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint section")
+    ap.add_argument("--adjoint-steps", type=int, default=500)
     return ap.parse_args()
 
 
@@ -297,6 +299,75 @@ def run_batched(args, K, warmup, flush, device, plain_fp64_value):
                         "4-point Peskin IBM; seed 2024"}
 
 
+def run_adjoint(args, device):
+    """Discrete adjoint on the adjoint configuration: 48^3 shear channel, one
+    level-4 red cell (2562 nodes, 5120 triangles, radius 8 cells), FP64,
+    objective = Taylor deformation after N steps, checkpoints every 25 steps;
+    gradient in the shear modulus, the bending modulus and the wall velocity,
+    against central differences."""
+    import dataclasses
+
+    import numpy as np
+
+    from lbfs_b200 import GpuSolver, cases
+    c = cases.shear_rbc(n=48, level=4, radius_cells=8.0, rotate=True)
+    c.membranes = [dataclasses.replace(m, internal_viscosity_ratio=1.0) for m in c.membranes]
+    N, K = args.adjoint_steps, 25
+    # plain forward step of the same case (graph, device events)
+    with GpuSolver(c.mesh, c.params, c.membranes, device=device) as s:
+        s.set_state(c.rho, c.u, c.v, c.w)
+        s.set_profiling(1)
+        s.step(5, graph=True)
+        acc = 0.0
+        for _ in range(50):
+            s.step(1, graph=True)
+            acc += s.phase_times()[5]
+        fwd_ms = acc / 50
+    with GpuSolver(c.mesh, c.params, c.membranes, device=device) as s:
+        s.set_state(c.rho, c.u, c.v, c.w)
+        J, g, t = s.adjoint(N, K, membrane=0)
+
+    def taylor(gs=1.0, kb=1.0, su=1.0):
+        mems = [dataclasses.replace(m, shear_modulus=m.shear_modulus * gs,
+                                    global_bending_modulus=m.global_bending_modulus * kb) for m in c.membranes]
+        bcv = c.mesh.bc_values
+        keep = bcv.copy()
+        bcv[:, :3] *= su
+        try:
+            with GpuSolver(c.mesh, c.params, mems, device=device) as s:
+                s.set_state(c.rho, c.u, c.v, c.w)
+                s.step(N, graph=True)
+                xyz = s.nodes().reshape(-1, 3)
+        finally:
+            bcv[:] = keep
+        dx, dy = xyz[:, 0] - xyz[:, 0].mean(), xyz[:, 1] - xyz[:, 1].mean()
+        Ixx, Iyy, Ixy = np.sum(dx * dx), np.sum(dy * dy), np.sum(dx * dy)
+        T, D = 0.5 * (Ixx + Iyy), 0.5 * (Ixx - Iyy)
+        R = np.sqrt(D * D + Ixy * Ixy)
+        L, B = np.sqrt(T + R), np.sqrt(T - R)
+        return (L - B) / (L + B)
+
+    m = c.membranes[0]
+    scale = {"shear_modulus": m.shear_modulus, "bending_modulus": m.global_bending_modulus,
+             "velocity_scale": 1.0}
+    fd = {}
+    for h in (1e-6, 1e-4):
+        fd[h] = {"shear_modulus": (taylor(gs=1 + h) - taylor(gs=1 - h)) / (2 * h * scale["shear_modulus"]),
+                 "bending_modulus": (taylor(kb=1 + h) - taylor(kb=1 - h)) / (2 * h * scale["bending_modulus"]),
+                 "velocity_scale": (taylor(su=1 + h) - taylor(su=1 - h)) / (2 * h)}
+    rel = {h: {k: abs(g[k] - v) / abs(v) if v != 0 else None for k, v in d.items()} for h, d in fd.items()}
+    return {"workload": "48^3 shear channel (110592 cells), 1 red cell L4 icosphere (2562 nodes, 5120 triangles), "
+                        f"radius 8 cells, Ca 0.1, 4-point Peskin IBM, FP64, {N} steps, checkpoint every {K}",
+            "objective": "Taylor deformation (L - B)/(L + B) of the red cell in the x-y plane at the final step",
+            "J": J, "gradient": g,
+            "gradient_note": "d/d shear modulus, d/d bending modulus, d/d sigma with every wall velocity value x sigma",
+            "forward_ms_per_step": fwd_ms, "adjoint_forward_sweep_ms": t[0], "adjoint_reverse_sweep_ms": t[1],
+            "reverse_over_forward": t[1] / (N * fwd_ms),
+            "reverse_over_forward_note": "reverse sweep (segment recomputation + backward kernels) per step over "
+                                         "one plain forward step (graph, device events)",
+            "fd_h1e-6": fd[1e-6], "rel_err_h1e-6": rel[1e-6], "fd_h1e-4": fd[1e-4], "rel_err_h1e-4": rel[1e-4]}
+
+
 def main():
     from lbfs_b200.parallel import dist_env, max_over_ranks
     args = parse()
@@ -429,6 +500,13 @@ def main():
         except Exception as exc:
             batched = {"value": None, "error": f"{type(exc).__name__}: {exc}"}
 
+    adjoint = None
+    if rank == 0 and not args.no_adjoint:
+        try:
+            adjoint = run_adjoint(args, local_rank)
+        except Exception as exc:
+            adjoint = {"error": f"{type(exc).__name__}: {exc}"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -453,6 +531,7 @@ def main():
             "rbc_node_steps_per_s": 642 * K * world / total_s,
             "fp32_bulk": fp32,
             "batched": batched,
+            "adjoint": adjoint,
             "status_flags": status,
         }
         print(json.dumps(line))

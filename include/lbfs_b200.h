@@ -231,8 +231,6 @@ typedef struct lbfs_launch_shape {
     int32_t update_threads;         /* 128, 256 or 512 */
     int32_t update_blocks;          /* grid cap of the cell update, 1 .. LBFS_MAX_UPDATE_BLOCKS */
     int32_t spread_blocks;          /* grid of the IBM spread, 1 .. LBFS_MAX_SPREAD_BLOCKS */
-    int32_t membrane_totals;        /* membrane volume/area: 0 in every spring block, 1 own kernel
-                                       (chosen at create: 1 when the spring blocks exceed 2 per SM) */
     double time_us[5];              /* autotune: gradients, flux, general flux, update, spread */
 } lbfs_launch_shape;
 int lbfs_get_launch_shape(lbfs_solver *s, lbfs_launch_shape *shape);

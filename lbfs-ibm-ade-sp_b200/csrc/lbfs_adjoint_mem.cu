@@ -312,7 +312,8 @@ __global__ void __launch_bounds__(128) k_adjm_springs(MembraneArgs A, MemAdjArgs
     J.adjm[kDirs * (size_t)s + k] = acc;
 }
 
-__device__ double block_sum128(double v, double *sh) {
+// Block sum in a fixed order (warp trees, then the warps in order).
+__device__ double block_sum_fixed(double v, double *sh) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0) sh[warp] = v;
@@ -324,7 +325,7 @@ __device__ double block_sum128(double v, double *sh) {
 }
 
 // ---- B3: per-membrane sums ----------------------------------------------------
-__global__ void __launch_bounds__(128) k_adjm_reduce(MembraneArgs A, MemAdjArgs J) {
+__global__ void __launch_bounds__(512) k_adjm_reduce(MembraneArgs A, MemAdjArgs J) {
     __shared__ double sh[32];
     const int m = blockIdx.x;
     const MembraneConst &mc = A.mc[m];
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(128) k_adjm_reduce(MembraneArgs A, MemAdjArgs 
         for (int q = 0; q < 5; q++) v[q] += r[q];
     }
     double t[5];
-    for (int q = 0; q < 5; q++) t[q] = block_sum128(v[q], sh);
+    for (int q = 0; q < 5; q++) t[q] = block_sum_fixed(v[q], sh);
     if (threadIdx.x == 0) {
         const MembraneScalars &ms = A.ms[m];
         const double lam_mad_next = J.lam_mad[m];
@@ -476,7 +477,7 @@ int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, cons
     const int node_blocks = (A.total_nodes * 32 + 255) / 256;
     k_adjm_spread<<<node_blocks, 256, 0, s>>>(A, J);
     k_adjm_springs<<<dim3((A.total_springs + 127) / 128, kDirs), 128, 0, s>>>(A, J);
-    k_adjm_reduce<<<A.n_membranes, 128, 0, s>>>(A, J);
+    k_adjm_reduce<<<A.n_membranes, 512, 0, s>>>(A, J);
     k_adjm_nodes<<<(A.total_nodes + 127) / 128, 128, 0, s>>>(A, J);
     launch_membrane_sort(J.mb, s);
     if (A.state_is_float) k_adjm_advect<float><<<node_blocks, 256, 0, s>>>(A, J);

@@ -17,7 +17,7 @@ int set_error(int code, const std::string &msg);
 constexpr int kMaxPatchCells = 48 * 48 * 48;
 // Threads of the one-CTA-per-membrane kernel (512 leaves 128 registers per
 // thread for the spring-force derivatives).
-constexpr int kMembraneThreads = 512;
+constexpr int kMembraneThreads = 1024;
 // Largest membrane handled by one CTA (nodes; springs = 3 (nodes - 2)).
 constexpr int kMaxMembraneNodes = 16384;
 

@@ -71,7 +71,6 @@ struct MembraneArgs {
     int *cell_start;             // [n_membranes + 1] first spread cell of each membrane (prefix over patches)
     unsigned int *sort_ticket;   // membranes whose patch is known in this launch; zero between launches
     int spread_blocks;           // grid of the spread kernel (grid-stride over the tiles)
-    int separate_totals;         // volume/area totals by their own kernel (many membranes)
     int *sorted_pos;             // [total_nodes] position of each node in its membrane's sorted order
     double4 *sorted_force;       // [total_nodes] node forces in sorted order (spread input)
     SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order (scratch)
@@ -103,6 +102,8 @@ struct ViscArgs {
 };
 
 void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s);
+// advection, totals, spring and node forces only (adjoint recomputation)
+void launch_membrane_forces(const MembraneArgs &a, cudaStream_t s);
 // single phases of the membrane chain (autotuner): node sort + patches, spread
 void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s);
 void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s);

@@ -4,6 +4,7 @@
 //   M2 k_mem_springs   (one thread per spring; totals per block)     P1, P2, P4
 //   M3 k_mem_nodeforce (one thread per node)                         P3
 //   M4 k_mem_sort      (one CTA per membrane, on a side stream)      P5
+//   k_mem_totals       (one CTA per membrane: V, A)                  P1
 //   M5 k_mem_spread    (one warp per patch cell, all membranes)      P6
 //
 //   P0  IBM velocity interpolation at the nodes + explicit node advection
@@ -373,10 +374,15 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
 // first n_nodes springs) are summed by the membrane's last block to finish.
 // Reference mode: the stress-free pass (contour lengths, spring constants,
 // reference curvatures).
-// Volume and area of membrane mc: per-thread sums over triangles
-// threadIdx.x, threadIdx.x + 128, ..., then block_sum (blocks of 128 threads).
-__device__ __forceinline__ void membrane_totals(const MembraneArgs &A, const MembraneConst &mc, double *sh, double &V,
-                                                double &Ar) {
+// ---- M2: membrane totals, one CTA per membrane ------------------------------
+// Volume and area: per-thread sums over triangles t, t + blockDim, ..., then
+// the block tree (fixed order).  Written to ms.Vc / ms.Ac for the spring
+// kernel, which every spring block reads instead of forming them again.
+constexpr int kTotalsThreads = 512;
+__global__ void __launch_bounds__(kTotalsThreads) k_mem_totals(MembraneArgs A) {
+    __shared__ double sh[33];
+    const int m = blockIdx.x;
+    const MembraneConst mc = A.mc[m];
     double pv = 0.0, pa = 0.0;
     for (int lt = threadIdx.x; lt < mc.n_tris; lt += blockDim.x) {
         const int t = mc.tri0 + lt;
@@ -386,25 +392,13 @@ __device__ __forceinline__ void membrane_totals(const MembraneArgs &A, const Mem
         pv += dot(normal, tri_centroid(a, b, c)) / 6;
         pa += sqrt(dot(normal, normal)) * 0.5;
     }
-    V = block_sum(pv, sh);
-    Ar = block_sum(pa, sh);
-}
-
-// Totals once per membrane (one 128-thread block each), for handles with many
-// membranes: the spring blocks then read them instead of forming them again.
-__global__ void __launch_bounds__(128) k_mem_totals(MembraneArgs A) {
-    __shared__ double sh[33];
-    const int m = blockIdx.x;
-    const MembraneConst mc = A.mc[m];
-    double V, Ar;
-    membrane_totals(A, mc, sh, V, Ar);
+    const double V = block_sum(pv, sh), Ar = block_sum(pa, sh);
     if (threadIdx.x == 0) {
         A.ms[m].Vc = V;
         A.ms[m].Ac = Ar;
     }
 }
 
-template <bool kTotalsHere>
 __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
     __shared__ double sh[33];
     __shared__ bool last_block;
@@ -420,13 +414,7 @@ __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
     }
     MembraneScalars *ms = A.ms + m;
     const bool initials = A.mode == kModeInitial;
-    double V, Ar;
-    if (kTotalsHere || A.mode != kModeStep) {
-        membrane_totals(A, mc, sh, V, Ar);
-    } else {
-        V = ms->Vc;
-        Ar = ms->Ac;
-    }
+    const double V = ms->Vc, Ar = ms->Ac;  // k_mem_totals of this launch sequence
     const double V0 = initials ? V * mc.volume_ratio : ms->V0;
     const double A0 = initials ? Ar : ms->A0;
     const double MADp = initials ? 0.0 : ms->MAD, MAD0p = initials ? 0.0 : ms->MAD0;
@@ -829,15 +817,18 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
                     cudaEvent_t ev_sorted) {
     const size_t smem = (size_t)(a.sort_capacity > 0 ? a.sort_capacity : 1) * sizeof(unsigned long long);
     const dim3 spring_grid((a.max_springs + 127) / 128, a.n_membranes);
-    if (a.mode != kModeStep) {  // stress-free reference pass, initial pass
-        launch_hi(k_mem_springs<true>, spring_grid, dim3(128), 0, s, a);
+    if (a.mode == kModeReference) {  // stress-free reference pass
+        launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
         return 1;
     }
-    int n = 0;
+    if (a.mode == kModeInitial) {  // initial pass: V0, A0, MAD0, areas, angles
+        launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a);
+        launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
+        return 2;
+    }
     const int blocks = (a.total_nodes * 32 + 255) / 256;
     if (a.state_is_float) launch_hi(k_mem_advect<float>, dim3(blocks), dim3(256), 0, s, a);
     else launch_hi(k_mem_advect<double>, dim3(blocks), dim3(256), 0, s, a);
-    n++;
     // the node sort needs only the advected positions: side stream
     const bool side = s_side != nullptr && ev_advected != nullptr && ev_sorted != nullptr;
     if (side) {
@@ -845,23 +836,28 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
         cudaStreamWaitEvent(s_side, ev_advected, 0);
     }
     launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, side ? s_side : s, a);
-    n++;
     if (side) cudaEventRecord(ev_sorted, s_side);
-    if (a.separate_totals) {
-        launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(128), 0, s, a);
-        launch_hi(k_mem_springs<false>, spring_grid, dim3(128), 0, s, a);
-        n += 2;
-    } else {
-        launch_hi(k_mem_springs<true>, spring_grid, dim3(128), 0, s, a);
-        n++;
-    }
+    launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a);
+    launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
     // node forces go to the sorted positions the sort wrote
     if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
     launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
     const dim3 grid(a.spread_blocks);
     if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
     else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a);
-    return n + 2;
+    return 6;
+}
+
+// Advection, totals, spring forces and node forces of a step (no sort, no
+// spread): what the adjoint's recomputation of a step needs.
+void launch_membrane_forces(const MembraneArgs &a, cudaStream_t s) {
+    const dim3 spring_grid((a.max_springs + 127) / 128, a.n_membranes);
+    const int blocks = (a.total_nodes * 32 + 255) / 256;
+    if (a.state_is_float) launch_hi(k_mem_advect<float>, dim3(blocks), dim3(256), 0, s, a);
+    else launch_hi(k_mem_advect<double>, dim3(blocks), dim3(256), 0, s, a);
+    launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a);
+    launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
+    launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
 }
 
 void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s) {

@@ -472,12 +472,7 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         ma.max_patch_bound = std::max(ma.max_patch_bound, mc[r].patch_bound);
     }
     ma.node_mem = d_nmem;
-    {
-        // totals in their own kernel once the spring blocks fill the GPU
-        long long spring_blocks = 0;
-        for (int r = 0; r < n_rbc; r++) spring_blocks += (mc[r].n_springs + 127) / 128;
-        ma.separate_totals = spring_blocks > 2 * 148 ? 1 : 0;
-    }
+
     ma.spring_mem = d_smem;
     ma.mc = d_mc; ma.ms = d_ms; ma.tri = d_tri; ma.spring = d_spr; ma.inc = d_inc; ma.inc_start = d_incs;
     ma.flags = s->fp32 ? s->f32.flags : s->f64.flags;
@@ -641,7 +636,7 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     rc = setup_membranes(s, mesh, rbc, n_rbc);
     if (rc) return fail(rc);
     // gradients, face flux (axis + general), update; membrane kernels
-    s->launches_per_step = 4 + (n_rbc > 0 ? 5 + s->ma.separate_totals : 0);
+    s->launches_per_step = 4 + (n_rbc > 0 ? 6 : 0);
     *out = s;
     return LBFS_OK;
 }
@@ -955,7 +950,7 @@ extern "C" int lbfs_status(lbfs_solver *s, uint32_t *flags) {
 
 extern "C" int lbfs_launches_per_step(lbfs_solver *s, int32_t *launches) {
     if (!s || !launches) return set_error(LBFS_ERR_ARG, "null argument");
-    *launches = 4 + (s->n_membranes > 0 ? 5 + s->ma.separate_totals : 0);
+    *launches = s->launches_per_step;
     return LBFS_OK;
 }
 
@@ -974,7 +969,6 @@ template <typename R> void shape_to_args(lbfs_solver *s, const lbfs_launch_shape
     a.tb_grad = sh.gradient_threads; a.tb_flux = sh.flux_threads; a.tb_gen = sh.general_flux_threads;
     a.tb_update = sh.update_threads; a.update_blocks = sh.update_blocks;
     s->ma.spread_blocks = sh.spread_blocks;
-    s->ma.separate_totals = sh.membrane_totals;
 }
 
 template <typename R> lbfs_launch_shape args_to_shape(lbfs_solver *s) {
@@ -983,7 +977,6 @@ template <typename R> lbfs_launch_shape args_to_shape(lbfs_solver *s) {
     sh.gradient_threads = a.tb_grad; sh.flux_threads = a.tb_flux; sh.general_flux_threads = a.tb_gen;
     sh.update_threads = a.tb_update; sh.update_blocks = a.update_blocks;
     sh.spread_blocks = s->ma.spread_blocks > 0 ? s->ma.spread_blocks : 1;
-    sh.membrane_totals = s->ma.separate_totals;
     return sh;
 }
 
@@ -1000,8 +993,6 @@ int check_shape(const lbfs_launch_shape &sh) {
     if (sh.update_blocks < 1 || sh.update_blocks > LBFS_MAX_UPDATE_BLOCKS || sh.spread_blocks < 1 ||
         sh.spread_blocks > LBFS_MAX_SPREAD_BLOCKS)
         return set_error(LBFS_ERR_ARG, "launch shape: grid caps out of range");
-    if (sh.membrane_totals != 0 && sh.membrane_totals != 1)
-        return set_error(LBFS_ERR_ARG, "launch shape: membrane_totals must be 0 or 1");
     return LBFS_OK;
 }
 
@@ -1462,7 +1453,7 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
                 const double *mn = seg_m + (size_t)(n - n0) * M;
                 if ((rc = load_x(xn))) return rc;
                 launch_adjm_set_mad(ma, mn, st);
-                launch_membrane(ma, st);  // x -> x', forces, totals, MAD_{n+1}
+                launch_membrane_forces(ma, st);  // x -> x', totals, forces, MAD_{n+1}
                 mj.mad_n = mn;
                 mj.xn = xn;
                 mj.yn = xn + N;

@@ -139,3 +139,15 @@ def test_coupled_adjoint_velocity_objective():
         return _objective(cc, 1.0, steps, weights)
     fd_gs = (with_gs(1 + h) - with_gs(1 - h)) / (2 * h * m.shear_modulus)
     assert abs(g["shear_modulus"] - fd_gs) <= FD_RTOL * abs(fd_gs), (g, fd_gs)
+
+
+@pytest.mark.gpu
+def test_torch_gradcheck_through_the_adjoint():
+    """torch.autograd.gradcheck of the Taylor deformation in the multipliers of
+    (shear modulus, bending modulus, boundary velocity), central differences."""
+    import torch
+    from lbfs_b200.autograd import deformation
+    c = _rbc_case()
+    theta = torch.ones(3, dtype=torch.float64, requires_grad=True)
+    f = lambda t: deformation(t, c, 16, 5)
+    assert torch.autograd.gradcheck(f, (theta,), eps=FD_H_MODULI, atol=1e-9, rtol=FD_RTOL, fast_mode=False)

@@ -86,9 +86,9 @@ def test_launch_shapes_do_not_change_fields():
     from lbfs_b200 import GpuSolver, cases
     c = cases.shear_rbc(n=16, level=2, radius_cells=3.0)
     shapes = [dict(), dict(gradient_threads=128, flux_threads=64, general_flux_threads=256, update_threads=512,
-                           update_blocks=296, spread_blocks=148, membrane_totals=1),
+                           update_blocks=296, spread_blocks=148),
               dict(gradient_threads=512, flux_threads=256, general_flux_threads=64, update_threads=128,
-                   update_blocks=2368, spread_blocks=2368, membrane_totals=0)]
+                   update_blocks=2368, spread_blocks=2368)]
     out = []
     for sh in shapes:
         with GpuSolver(c.mesh, c.params, c.membranes) as s:
