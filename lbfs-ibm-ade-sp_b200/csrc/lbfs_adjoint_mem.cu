@@ -479,6 +479,7 @@ int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, cons
     k_adjm_springs<<<dim3((A.total_springs + 127) / 128, kDirs), 128, 0, s>>>(A, J);
     k_adjm_reduce<<<A.n_membranes, 512, 0, s>>>(A, J);
     k_adjm_nodes<<<(A.total_nodes + 127) / 128, 128, 0, s>>>(A, J);
+    launch_membrane_tables(J.mb, s);
     launch_membrane_sort(J.mb, s);
     if (A.state_is_float) k_adjm_advect<float><<<node_blocks, 256, 0, s>>>(A, J);
     else k_adjm_advect<double><<<node_blocks, 256, 0, s>>>(A, J);

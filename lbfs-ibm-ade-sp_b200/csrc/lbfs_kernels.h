@@ -68,9 +68,12 @@ struct MembraneArgs {
     int total_nodes, total_springs;
     const int *spring_mem;       // [total_springs] membrane of each spring
     int *bin_start;              // [sum of (patch_bound + 1)] first sorted node of each bin, from patch_off + m
+    int *bin_cursor;             // [sum of (patch_bound + 1)] placement cursors of the node sort (scratch)
     int *cell_start;             // [n_membranes + 1] first spread cell of each membrane (prefix over patches)
     unsigned int *sort_ticket;   // membranes whose patch is known in this launch; zero between launches
     int spread_blocks;           // grid of the spread kernel (grid-stride over the tiles)
+    int *node_base;              // [3 total_nodes] first IBM stencil cell per axis at the current positions
+    double *node_w;              // [12 total_nodes] 1D stencil weights per axis (4 slots) at the current positions
     int *sorted_pos;             // [total_nodes] position of each node in its membrane's sorted order
     double4 *sorted_force;       // [total_nodes] node forces in sorted order (spread input)
     SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order (scratch)
@@ -102,6 +105,8 @@ struct ViscArgs {
 };
 
 void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s);
+// stencil tables at the current positions (k_mem_advect writes them at x')
+void launch_membrane_tables(const MembraneArgs &a, cudaStream_t s);
 // advection, totals, spring and node forces only (adjoint recomputation)
 void launch_membrane_forces(const MembraneArgs &a, cudaStream_t s);
 // single phases of the membrane chain (autotuner): node sort + patches, spread

@@ -314,6 +314,31 @@ __device__ void spring_reference(const MembraneArgs &A, const MembraneConst &mc,
     A.area0[2 * s + 1] = norm_2;
 }
 
+// Stencil tables of node n at position p, by the lanes of one warp: lane l < 12
+// writes weight slot l (axis l / 4, offset l % 4; 0 beyond the stencil) and
+// lanes 0..2 the first stencil cell per axis.  The sort and the spread read
+// them instead of evaluating the delta kernel again.
+__device__ __forceinline__ void write_stencil_tables(const MembraneArgs &A, const MembraneConst &mc, int n,
+                                                     double x, double y, double z, int lane) {
+    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+    const Stencil st = node_stencil(A, mc, x, y, z);
+    if (lane < 12) {
+        const int ax = lane >> 2, q = lane & 3;
+        const int b = ax == 0 ? st.i0 : (ax == 1 ? st.j0 : st.k0);
+        const double r = ax == 0 ? st.rx : (ax == 1 ? st.ry : st.rz);
+        A.node_w[12 * (size_t)n + lane] = q < S ? stencil_weight(A.ibm_stencil, b + q + 0.5 - r) : 0.0;
+    }
+    if (lane < 3) A.node_base[3 * (size_t)n + lane] = lane == 0 ? st.i0 : (lane == 1 ? st.j0 : st.k0);
+}
+
+// Tables at the current positions (the adjoint's interpolation transpose).
+__global__ void __launch_bounds__(256) k_mem_tables(MembraneArgs A) {
+    const int lane = threadIdx.x & 31;
+    const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (n >= A.total_nodes) return;
+    write_stencil_tables(A, A.mc[A.node_mem[n]], n, A.x[n], A.y[n], A.z[n], lane);
+}
+
 // ---- M1: IBM interpolation + advection, one warp per node ----------------
 template <typename R>
 __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
@@ -357,14 +382,18 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
 #pragma unroll
     for (int c = 0; c < 3; c++)
         for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+    const double xp = x + v[0] * A.delta_t, yp = y + v[1] * A.delta_t, zp = z + v[2] * A.delta_t;
     if (lane == 0) {
         A.vx[n] = v[0];
         A.vy[n] = v[1];
         A.vz[n] = v[2];
-        A.x[n] = x + v[0] * A.delta_t;
-        A.y[n] = y + v[1] * A.delta_t;
-        A.z[n] = z + v[2] * A.delta_t;
+        A.x[n] = xp;
+        A.y[n] = yp;
+        A.z[n] = zp;
     }
+    // stencil tables at the advected position (lane 0 holds the sums)
+    write_stencil_tables(A, mc, n, __shfl_sync(0xffffffffu, xp, 0), __shfl_sync(0xffffffffu, yp, 0),
+                         __shfl_sync(0xffffffffu, zp, 0), lane);
 }
 
 // ---- M2: spring forces, one thread per spring, blocks per membrane ----------
@@ -489,19 +518,8 @@ __global__ void __launch_bounds__(128) k_mem_nodeforce(MembraneArgs A) {
 // stencil weights and first x cell (recomputed from its position, so nothing
 // but the keys lives between the phases).  The last CTA of the launch writes
 // the prefix of patch cells over the membranes (the spread kernel's work list).
-__device__ __forceinline__ unsigned long long pack_base(int b0, int b1, int b2) {
-    const unsigned long long o = 1ull << 20;  // bases within +-2^20 cells
-    return ((unsigned long long)(b0 + o) << 42) | ((unsigned long long)(b1 + o) << 21) | (unsigned long long)(b2 + o);
-}
-__device__ __forceinline__ void unpack_base(unsigned long long k, int b[3]) {
-    const long long o = 1ll << 20, mask = (1ll << 21) - 1;
-    b[0] = (int)((long long)(k >> 42) - o);
-    b[1] = (int)((long long)((k >> 21) & mask) - o);
-    b[2] = (int)((long long)(k & mask) - o);
-}
-
 __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
-    extern __shared__ unsigned long long skeys[];
+    extern __shared__ unsigned long long skeys[];  // 2 int arrays of sort_capacity: bins, sorted list
     __shared__ double shv[kMembraneThreads / 32][12];
     __shared__ double red[12];
     __shared__ bool last_sorted;
@@ -517,8 +535,7 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
         const int n = mc.node0 + ln;
         const double p[3] = {A.x[n], A.y[n], A.z[n]};
-        const Stencil st = node_stencil(A, mc, p[0], p[1], p[2]);
-        const int b[3] = {st.i0, st.j0, st.k0};
+        const int b[3] = {A.node_base[3 * (size_t)n], A.node_base[3 * (size_t)n + 1], A.node_base[3 * (size_t)n + 2]};
         for (int c = 0; c < 3; c++) {
             v[c] = fmin(v[c], p[c]);            // lower bound
             v[3 + c] = fmin(v[3 + c], -p[c]);   // minus upper bound
@@ -527,7 +544,6 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
             if (b[c] < 0 || b[c] + S > gn[c]) range_flag = LBFS_FLAG_IBM_RANGE;
             if (b[c] < -(1 << 19) || b[c] > (1 << 19)) base_range = false;
         }
-        skeys[ln] = pack_base(b[0], b[1], b[2]);
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -550,8 +566,8 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         pdim[c] = bdim[c] + S - 1;
     }
     const long long pcells = (long long)pdim[0] * pdim[1] * pdim[2];
-    const bool bases_packed = __syncthreads_and(base_range) != 0;
-    const bool overflow = pcells > mc.patch_bound || mc.n_nodes == 0 || !bases_packed;
+    const bool bases_sane = __syncthreads_and(base_range) != 0;
+    const bool overflow = pcells > mc.patch_bound || mc.n_nodes == 0 || !bases_sane;
     if (range_flag) atomicOr(A.flags, range_flag);
     if (threadIdx.x == 0) {
         for (int c = 0; c < 3; c++) {
@@ -594,53 +610,67 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         }
     }
     if (overflow) return;
-    int npad = 1;
-    while (npad < mc.n_nodes) npad <<= 1;
-    for (int t = threadIdx.x; t < npad; t += blockDim.x) {
-        unsigned long long key = ~0ull;
-        if (t < mc.n_nodes) {
-            int b[3];
-            unpack_base(skeys[t], b);
-            const unsigned long long bin =
-                (unsigned long long)((b[0] - plo[0]) + bdim[0] * ((b[1] - plo[1]) + bdim[1] * (b[2] - plo[2])));
-            key = (bin << 32) | (unsigned long long)t;
-        }
-        skeys[t] = key;  // each thread rewrites only the keys it packed
-    }
-    __syncthreads();
-    for (int size = 2; size <= npad; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int t = threadIdx.x; t < (npad >> 1); t += blockDim.x) {
-                const int i = 2 * stride * (t / stride) + (t % stride);
-                const int j = i + stride;
-                const bool up = ((i & size) == 0);
-                const unsigned long long ki = skeys[i], kj = skeys[j];
-                if ((ki > kj) == up) { skeys[i] = kj; skeys[j] = ki; }
-            }
-            __syncthreads();
-        }
-    }
+    // counting sort of the nodes by stencil bin: counts, exclusive prefix
+    // (bin_start), placement, then each bin's few nodes in index order, so the
+    // result is the (bin, node) order whatever order the atomics took
     const int nbins = bdim[0] * bdim[1] * bdim[2];
     int *bin_start = A.bin_start + (size_t)ms->patch_off + m;
-    for (int b = threadIdx.x; b <= nbins; b += blockDim.x) {
-        int lo = 0, hi = mc.n_nodes;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if ((skeys[mid] >> 32) < (unsigned long long)b) lo = mid + 1;
-            else hi = mid;
-        }
-        bin_start[b] = lo;
+    int *cursor = A.bin_cursor + (size_t)ms->patch_off + m;
+    int *bins = reinterpret_cast<int *>(skeys);
+    int *list = bins + A.sort_capacity;
+    for (int b = threadIdx.x; b <= nbins; b += blockDim.x) bin_start[b] = 0;
+    __syncthreads();
+    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
+        const int *bb = A.node_base + 3 * (size_t)(mc.node0 + ln);
+        const int bin = (bb[0] - plo[0]) + bdim[0] * ((bb[1] - plo[1]) + bdim[1] * (bb[2] - plo[2]));
+        bins[ln] = bin;
+        atomicAdd(bin_start + bin, 1);
     }
+    __syncthreads();
+    {
+        __shared__ int bscan[kMembraneThreads];
+        const int count = nbins + 1;
+        const int per = (count + blockDim.x - 1) / blockDim.x;
+        const int b0 = min(count, (int)threadIdx.x * per), b1 = min(count, b0 + per);
+        int local = 0;
+        for (int b = b0; b < b1; b++) local += bin_start[b];
+        bscan[threadIdx.x] = local;
+        __syncthreads();
+        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+            const int x = threadIdx.x >= (unsigned)o ? bscan[threadIdx.x - o] : 0;
+            __syncthreads();
+            bscan[threadIdx.x] += x;
+            __syncthreads();
+        }
+        int run = bscan[threadIdx.x] - local;
+        for (int b = b0; b < b1; b++) {
+            const int c = bin_start[b];
+            bin_start[b] = run;
+            cursor[b] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) list[atomicAdd(cursor + bins[ln], 1)] = ln;
+    __syncthreads();
+    for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
+        const int lo = bin_start[b], hi = bin_start[b + 1];
+        for (int i = lo + 1; i < hi; i++) {
+            const int v = list[i];
+            int j = i - 1;
+            while (j >= lo && list[j] > v) {
+                list[j + 1] = list[j];
+                j--;
+            }
+            list[j + 1] = v;
+        }
+    }
+    __syncthreads();
     for (int e = threadIdx.x; e < mc.n_nodes; e += blockDim.x) {
-        const int n = mc.node0 + (int)(skeys[e] & 0xffffffffu);
-        const Stencil st = node_stencil(A, mc, A.x[n], A.y[n], A.z[n]);
-        const int b[3] = {st.i0, st.j0, st.k0};
-        const double r[3] = {st.rx, st.ry, st.rz};
+        const int n = mc.node0 + list[e];
         SpreadRec rec;
-        for (int c = 0; c < 3; c++)
-            for (int q = 0; q < 4; q++)
-                rec.w[4 * c + q] = q < S ? stencil_weight(A.ibm_stencil, b[c] + q + 0.5 - r[c]) : 0.0;
-        rec.b0 = b[0];
+        for (int q = 0; q < 12; q++) rec.w[q] = A.node_w[12 * (size_t)n + q];
+        rec.b0 = A.node_base[3 * (size_t)n];
         rec.pad[0] = rec.pad[1] = rec.pad[2] = 0;
         A.spread_rec[mc.node0 + e] = rec;
         A.sorted_pos[n] = mc.node0 + e;
@@ -846,6 +876,10 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
     else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a);
     return 6;
+}
+
+void launch_membrane_tables(const MembraneArgs &a, cudaStream_t s) {
+    launch_hi(k_mem_tables, dim3((a.total_nodes * 32 + 255) / 256), dim3(256), 0, s, a);
 }
 
 // Advection, totals, spring forces and node forces of a step (no sort, no

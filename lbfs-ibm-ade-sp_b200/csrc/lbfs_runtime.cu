@@ -454,9 +454,11 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         (rc = s->alloc(&ma.keys, N)) || (rc = s->alloc(&ma.patch_force, (size_t)total_patch * 3)) ||
         (rc = s->upload(&d_smem, spring_mem)) ||
         (rc = s->alloc(&ma.bin_start, (size_t)total_patch + n_rbc)) ||
+        (rc = s->alloc(&ma.bin_cursor, (size_t)total_patch + n_rbc)) ||
         (rc = s->alloc(&ma.cell_start, (size_t)n_rbc + 1)) || (rc = s->alloc(&ma.sort_ticket, 1)) ||
         (rc = s->alloc(&ma.spread_rec, (size_t)N)) || (rc = s->upload(&ma.sorted_pos, identity)) ||
-        (rc = s->alloc(&ma.sorted_force, (size_t)N)) ||
+        (rc = s->alloc(&ma.sorted_force, (size_t)N)) || (rc = s->alloc(&ma.node_base, 3 * (size_t)N)) ||
+        (rc = s->alloc(&ma.node_w, 12 * (size_t)N)) ||
         (rc = s->alloc(&ma.mad_partials, (size_t)n_rbc * kMaxSpringBlocks)) ||
         (rc = s->alloc(&ma.mad_ticket, (size_t)n_rbc)))
         return rc;
@@ -487,6 +489,7 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     LBFS_CUDA(cudaMemcpyAsync(ma.z, z.data(), N * sizeof(double), cudaMemcpyHostToDevice, s->stream));
     ma.mode = kModeInitial;
     launch_membrane(ma, s->stream);
+    launch_membrane_tables(ma, s->stream);  // stencil tables at the initial positions
     LBFS_CUDA(cudaGetLastError());
     LBFS_CUDA(cudaStreamSynchronize(s->stream));
     ma.mode = kModeStep;
@@ -1083,6 +1086,7 @@ template <typename R> int autotune(lbfs_solver *s, int reps, lbfs_launch_shape *
         a.update_blocks = best.update_blocks;
         // IBM spread over the current node forces and positions
         if (s->n_membranes > 0) {
+            launch_membrane_tables(s->ma, s->stream);
             launch_membrane_sort(s->ma, s->stream);
             tbest = 1e300;
             for (int mult : {1, 2, 4, 8, 16}) {
@@ -1233,8 +1237,10 @@ int adjm_prepare(lbfs_solver *s) {
     MembraneScalars *ms2;
     if ((rc = s->alloc(&ms2, M)) || (rc = s->alloc(&mb.spread_rec, N)) ||
         (rc = s->alloc(&mb.bin_start, (size_t)s->total_patch + M)) || (rc = s->alloc(&mb.cell_start, (size_t)M + 1)) ||
+        (rc = s->alloc(&mb.bin_cursor, (size_t)s->total_patch + M)) ||
         (rc = s->alloc(&mb.sort_ticket, 1)) || (rc = s->upload(&mb.sorted_pos, identity)) ||
-        (rc = s->alloc(&mb.sorted_force, N)) || (rc = s->alloc(&mb.patch_force, 3 * (size_t)s->total_patch)))
+        (rc = s->alloc(&mb.sorted_force, N)) || (rc = s->alloc(&mb.patch_force, 3 * (size_t)s->total_patch)) ||
+        (rc = s->alloc(&mb.node_base, 3 * (size_t)N)) || (rc = s->alloc(&mb.node_w, 12 * (size_t)N)))
         return rc;
     LBFS_CUDA(cudaMemcpy(ms2, ma.ms, sizeof(MembraneScalars) * M, cudaMemcpyDeviceToDevice));
     LBFS_CUDA(cudaMemset(mb.sort_ticket, 0, sizeof(unsigned int)));
@@ -1321,9 +1327,13 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     const int K = checkpoint_every, n_ck = (n_steps + K - 1) / K;
     const size_t xs = 3 * (size_t)N;  // positions of one step: x, y, z planes
     cudaStream_t st = s->stream;
-    DevBuf ck, seg, st0, fin_t1, fin_state, wts, ckx, segx, ckm, segm, finx, finm;
+    DevBuf ck, seg, st0, fin_t1, fin_state, wts, ckx, segx, ckm, segm, finx, finm, segg, segh, segf, segs;
     LBFS_CUDA(cudaMalloc(&ck.p, sizeof(double4) * (size_t)nc * n_ck));
     LBFS_CUDA(cudaMalloc(&seg.p, sizeof(double4) * (size_t)nc * K));
+    // per step of a segment: the gradients and ghost states of its K1
+    const size_t gsz = 12 * (size_t)nt;
+    LBFS_CUDA(cudaMalloc(&segg.p, sizeof(double) * gsz * K));
+    LBFS_CUDA(cudaMalloc(&segh.p, sizeof(Vec4<double>) * (size_t)(s->nb > 0 ? s->nb : 1) * K));
     LBFS_CUDA(cudaMalloc(&st0.p, sizeof(Vec4<double>) * (size_t)nt));
     LBFS_CUDA(cudaMalloc(&fin_t1.p, sizeof(double4) * (size_t)nc));
     LBFS_CUDA(cudaMalloc(&fin_state.p, sizeof(Vec4<double>) * (size_t)nt));
@@ -1333,7 +1343,9 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     }
     if (M > 0) {
         LBFS_CUDA(cudaMalloc(&ckx.p, sizeof(double) * xs * n_ck));
-        LBFS_CUDA(cudaMalloc(&segx.p, sizeof(double) * xs * K));
+        LBFS_CUDA(cudaMalloc(&segx.p, sizeof(double) * xs * (K + 1)));
+        LBFS_CUDA(cudaMalloc(&segf.p, sizeof(double) * xs * K));
+        LBFS_CUDA(cudaMalloc(&segs.p, sizeof(MembraneScalars) * M * K));
         LBFS_CUDA(cudaMalloc(&ckm.p, sizeof(double) * M * n_ck));
         LBFS_CUDA(cudaMalloc(&segm.p, sizeof(double) * M * K));
         LBFS_CUDA(cudaMalloc(&finx.p, sizeof(double) * xs));
@@ -1341,6 +1353,9 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     }
     double4 *ck_t1 = (double4 *)ck.p, *seg_t1 = (double4 *)seg.p;
     double *ck_x = (double *)ckx.p, *seg_x = (double *)segx.p, *ck_m = (double *)ckm.p, *seg_m = (double *)segm.p;
+    double *seg_g = (double *)segg.p, *seg_f = (double *)segf.p;
+    Vec4<double> *seg_h = (Vec4<double> *)segh.p;
+    MembraneScalars *seg_s = (MembraneScalars *)segs.p;
     auto save_x = [&](double *dst) -> int {
         LBFS_CUDA(cudaMemcpyAsync(dst, ma.x, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
         LBFS_CUDA(cudaMemcpyAsync(dst + N, ma.y, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
@@ -1430,31 +1445,50 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
             if ((rc = load_x(ck_x + (size_t)sg * xs))) return rc;
             launch_adjm_set_mad(ma, ck_m + (size_t)sg * M, st);
         }
+        // keeping each step's inputs (t1, x, MAD) and what its backward reads
+        // (gradients, ghost states, x', node forces, membrane scalars)
         for (int n = n0; n < n1; n++) {
-            LBFS_CUDA(cudaMemcpyAsync(seg_t1 + (size_t)(n - n0) * nc, a.t1, sizeof(double4) * nc,
-                                      cudaMemcpyDeviceToDevice, st));
+            const size_t i = n - n0;
+            LBFS_CUDA(cudaMemcpyAsync(seg_t1 + i * nc, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
             if (M > 0) {
-                if ((rc = save_x(seg_x + (size_t)(n - n0) * xs))) return rc;
-                launch_adjm_get_mad(ma, seg_m + (size_t)(n - n0) * M, st);
+                if ((rc = save_x(seg_x + i * xs))) return rc;
+                launch_adjm_get_mad(ma, seg_m + i * M, st);
             }
-            if (n + 1 < n1) {
-                s->t = t_start + n;
-                if ((rc = run_one_step(s))) return rc;
+            s->t = t_start + n;
+            if ((rc = run_one_step(s))) return rc;
+            LBFS_CUDA(cudaMemcpyAsync(seg_g + i * gsz, a.grad, sizeof(double) * gsz, cudaMemcpyDeviceToDevice, st));
+            if (s->nb > 0)
+                LBFS_CUDA(cudaMemcpyAsync(seg_h + i * s->nb, a.state + nc, sizeof(Vec4<double>) * s->nb,
+                                          cudaMemcpyDeviceToDevice, st));
+            if (M > 0) {
+                if ((rc = save_x(seg_x + (i + 1) * xs))) return rc;
+                LBFS_CUDA(cudaMemcpyAsync(seg_f + i * xs, ma.fx, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+                LBFS_CUDA(cudaMemcpyAsync(seg_f + i * xs + N, ma.fy, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+                LBFS_CUDA(cudaMemcpyAsync(seg_f + i * xs + 2 * (size_t)N, ma.fz, sizeof(double) * N,
+                                          cudaMemcpyDeviceToDevice, st));
+                LBFS_CUDA(cudaMemcpyAsync(seg_s + i * M, ma.ms, sizeof(MembraneScalars) * M, cudaMemcpyDeviceToDevice, st));
             }
         }
         for (int n = n1 - 1; n >= n0; n--) {
-            LBFS_CUDA(cudaMemcpyAsync(a.t1, seg_t1 + (size_t)(n - n0) * nc, sizeof(double4) * nc,
-                                      cudaMemcpyDeviceToDevice, st));
-            if (n == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
+            const size_t i = n - n0;
+            // the state of step n: t1, primitive interior, its ghosts and gradients
+            LBFS_CUDA(cudaMemcpyAsync(a.t1, seg_t1 + i * nc, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
+            if (n == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nc, cudaMemcpyDeviceToDevice, st));
             else launch_adj_prim(a, st);
-            launch_fluid_gradients<double>(a, st);
+            if (s->nb > 0)
+                LBFS_CUDA(cudaMemcpyAsync(a.state + nc, seg_h + i * s->nb, sizeof(Vec4<double>) * s->nb,
+                                          cudaMemcpyDeviceToDevice, st));
+            LBFS_CUDA(cudaMemcpyAsync(a.grad, seg_g + i * gsz, sizeof(double) * gsz, cudaMemcpyDeviceToDevice, st));
             if (M > 0) {
-                const double *xn = seg_x + (size_t)(n - n0) * xs;
-                const double *mn = seg_m + (size_t)(n - n0) * M;
-                if ((rc = load_x(xn))) return rc;
-                launch_adjm_set_mad(ma, mn, st);
-                launch_membrane_forces(ma, st);  // x -> x', totals, forces, MAD_{n+1}
-                mj.mad_n = mn;
+                // after the step's membrane chain: x', forces, totals, MAD_{n+1}
+                const double *xn = seg_x + i * xs;
+                if ((rc = load_x(seg_x + (i + 1) * xs))) return rc;
+                LBFS_CUDA(cudaMemcpyAsync(ma.fx, seg_f + i * xs, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+                LBFS_CUDA(cudaMemcpyAsync(ma.fy, seg_f + i * xs + N, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+                LBFS_CUDA(cudaMemcpyAsync(ma.fz, seg_f + i * xs + 2 * (size_t)N, sizeof(double) * N,
+                                          cudaMemcpyDeviceToDevice, st));
+                LBFS_CUDA(cudaMemcpyAsync(ma.ms, seg_s + i * M, sizeof(MembraneScalars) * M, cudaMemcpyDeviceToDevice, st));
+                mj.mad_n = seg_m + i * M;
                 mj.xn = xn;
                 mj.yn = xn + N;
                 mj.zn = xn + 2 * (size_t)N;
