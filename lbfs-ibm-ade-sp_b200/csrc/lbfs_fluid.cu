@@ -126,7 +126,19 @@ __device__ __forceinline__ Dir dir_of(int k) { return {c_ex(k), c_ey(k), c_ez(k)
 // the flux through the face: calculate_flux_at_interface (LBFS.cu:1462-1648)
 // and its axis-aligned forms (LBFS.cu:3648-4092).  `axis` < 0 selects the
 // general three-component form with the face normal; otherwise only the
-// directions crossing the face are formed.
+// face-normal component is formed.
+//
+// The relaxed populations are f_k - tau (f_k - fl_k), f_k the interface
+// equilibrium, so the flux tensor is (1 - tau) F_eq + tau F_fl, F_fl the
+// first and second moments of the reconstructed fl_k over the directions
+// crossing the face and F_eq those of the equilibrium.  The D3Q15 weights
+// make the equilibrium moments exact closed forms (sum w e = 0,
+// sum w e e = I / 3, sum w e e e e = (dd + dd + dd) / 9):
+//   sum_k e_c f_k = rho u_c,  sum_k e_c e_m f_k = rho (q u_c u_m + d_cm / 3)
+// (q the preconditioning factor); in the deviation form (f' = f - w rho0)
+// the second moment's d_cm term is rho' / 3.  The reference sums the 15
+// equilibria explicitly; the closed form is the same quantity with fewer
+// roundings.
 template <typename R>
 __device__ __forceinline__ Vec4<R> interface_flux(const R (&fl)[15], R rho0, R tau, R qscale, R area, int axis,
                                                   R nx, R ny, R nz) {
@@ -143,8 +155,9 @@ __device__ __forceinline__ Vec4<R> interface_flux(const R (&fl)[15], R rho0, R t
     }
     const R rho_i = rho_dev + rho0;
     const R inv = R(1) / rho_i;
-    const R ux = inv * mx, uy = inv * my, uz = inv * mz;
-    // flux tensors: F[c][m], c = face axis component (x,y,z), m = (mass, mom x, mom y, mom z)
+    const R u[3] = {inv * mx, inv * my, inv * mz};
+    // moments of the reconstructed populations: F_fl[c][m], c = face axis
+    // component, m = (mass, mom x, mom y, mom z)
     R F[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
 #pragma unroll
     for (int k = 1; k < 15; k++) {
@@ -152,8 +165,7 @@ __device__ __forceinline__ Vec4<R> interface_flux(const R (&fl)[15], R rho0, R t
         if (axis == 0 && !e.ex) continue;
         if (axis == 1 && !e.ey) continue;
         if (axis == 2 && !e.ez) continue;
-        R f = feq_dev<R>(k, rho_dev, ux, uy, uz, rho0, qscale);
-        f = f - tau * (f - fl[k]);
+        const R f = fl[k];
         const int ee[3] = {e.ex, e.ey, e.ez};
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -165,6 +177,18 @@ __device__ __forceinline__ Vec4<R> interface_flux(const R (&fl)[15], R rho0, R t
                 if (!ee[m]) continue;
                 F[c][1 + m] = (ee[c] * ee[m] > 0) ? F[c][1 + m] + f : F[c][1 + m] - f;
             }
+        }
+    }
+    const R keep = R(1) - tau;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if (axis >= 0 && c != axis) continue;
+        F[c][0] = keep * (rho_i * u[c]) + tau * F[c][0];
+#pragma unroll
+        for (int m = 0; m < 3; m++) {
+            R eq = rho_i * (qscale * u[c] * u[m]);
+            if (m == c) eq = eq + rho_dev * R(1.0 / 3.0);
+            F[c][1 + m] = keep * eq + tau * F[c][1 + m];
         }
     }
     Vec4<R> out;
@@ -360,7 +384,7 @@ __global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
     double sq[4] = {0, 0, 0, 0};
     unsigned int flag = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nc; i += gridDim.x * blockDim.x) {
-        const double vol = __ldg(a.cell_volume + i);
+        const double iv = __ldg(a.cell_inv_volume + i);  // 1 / volume: products instead of 24 divisions
         double r[4] = {0, 0, 0, 0};  // rho, u, v, w
         int cfl[6];
 #pragma unroll
@@ -376,7 +400,7 @@ __global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
             const Vec4<R> fx = a.flux[f];
             const double fv[4] = {(double)fx.rho, (double)fx.u, (double)fx.v, (double)fx.w};
 #pragma unroll
-            for (int m = 0; m < 4; m++) r[m] = (e > 0) ? r[m] + (-fv[m] / vol) : r[m] + fv[m] / vol;
+            for (int m = 0; m < 4; m++) r[m] = (e > 0) ? r[m] + (-fv[m] * iv) : r[m] + fv[m] * iv;
         }
         double fx = a.force[0], fy = a.force[1], fz = a.force[2];
         if (a.n_membranes > 0) {

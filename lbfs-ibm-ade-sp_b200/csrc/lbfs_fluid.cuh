@@ -148,6 +148,7 @@ template <typename R> struct FluidArgs {
     // K3
     const int *cell_faces;       // [6*nc] +(f+1) owner, -(f+1) neighbour
     const double *cell_volume;   // [nc]
+    const double *cell_inv_volume;  // [nc] 1 / cell_volume
     double4 *t1;                 // [nc] (u, v, w, rho) conservative accumulator, FP64
     double *res_out;             // [4*nc] residuals kept for parity checks (null = not stored)
     // IBM patches (one per membrane), grouped by ensemble instance

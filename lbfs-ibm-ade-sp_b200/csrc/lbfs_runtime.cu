@@ -241,7 +241,8 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     }
     for (int i = 0; i < nc; i++)
         if (cnt[i] != 6) return set_error(LBFS_ERR_UNSUPPORTED, "cell without 6 faces (hexahedra only)");
-    std::vector<double> vol(m->cell_volume, m->cell_volume + nc);
+    std::vector<double> vol(m->cell_volume, m->cell_volume + nc), inv_vol(nc);
+    for (int i = 0; i < nc; i++) inv_vol[i] = 1.0 / vol[i];
     std::vector<R> visc(nc, (R)p.visc_factor_initial);
     int rc = 0;
     int *d_rt, *d_vt, *d_cf;
@@ -253,16 +254,17 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     int2 *d_fcells;
     AxisFace<R> *d_axf = nullptr;
     GenFace<R> *d_gen;
-    double *d_vol;
+    double *d_vol, *d_ivol;
     if ((rc = s->upload(&d_stencil, stencil)) || (rc = s->upload(&d_ls, ls)) ||
         (rc = s->upload(&d_rt, rt)) || (rc = s->upload(&d_vt, vt)) || (rc = s->upload(&d_bcv, bcv)) ||
         (rc = s->upload(&d_bcr, bcr)) || (rc = s->upload(&d_fcells, fcells)) || (rc = s->upload(&d_gen, gen)) ||
-        (rc = s->upload(&d_cf, cf)) || (rc = s->upload(&d_vol, vol)) || (rc = s->upload(&d_visc, visc)))
+        (rc = s->upload(&d_cf, cf)) || (rc = s->upload(&d_vol, vol)) || (rc = s->upload(&d_ivol, inv_vol)) ||
+        (rc = s->upload(&d_visc, visc)))
         return rc;
     if (a.axis_aligned && (rc = s->upload(&d_axf, axf))) return rc;
     a.stencil = d_stencil; a.ls = d_ls; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt;
     a.bc_val = d_bcv; a.bc_rec = d_bcr; a.face_cells = d_fcells; a.axis_face = d_axf; a.gen_face = d_gen;
-    a.visc_factor = d_visc; a.cell_faces = d_cf; a.cell_volume = d_vol;
+    a.visc_factor = d_visc; a.cell_faces = d_cf; a.cell_volume = d_vol; a.cell_inv_volume = d_ivol;
     Vec4<R> *d_state, *d_flux;
     R *d_grad;
     double4 *d_t1;
