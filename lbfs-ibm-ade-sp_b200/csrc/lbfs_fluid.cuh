@@ -56,28 +56,21 @@ template <typename R> __host__ __device__ constexpr R lattice_w(int k) {
 }
 
 // Equilibrium deviation  f'_k = w_k (rho' (1 + X) + rho0 X),
-// X = 3 e.u + 4.5 (e.u)^2 - 1.5 |u|^2, with the term grouping of
-// populate_feq_lattice_explicit (LBFS.cu:1041-1354).  With rho0 = 0 it is the
-// reference's equilibrium w_k rho (1 + X) evaluated as w_k (rho (1 + X)).
+// X = 3 e.u + q (4.5 (e.u)^2 - 1.5 |u|^2)  (q the preconditioning factor),
+// formed as w_k (rho' + (rho' + rho0) X).  With rho0 = 0 it is the reference's
+// equilibrium w_k rho (1 + X) (populate_feq_lattice_explicit, LBFS.cu:1041-1354,
+// which expands (e.u)^2 into its component products; the same polynomial with
+// fewer operations).
 template <typename R>
 __device__ __forceinline__ R feq_dev(int k, R rho, R u, R v, R w, R rho0, R qscale) {
-    const R uu2 = u * u * qscale, vv2 = v * v * qscale, ww2 = w * w * qscale;
-    const R u2v2w2 = (uu2 + vv2 + ww2) * R(1.5);
     const int ex = c_ex(k), ey = c_ey(k), ez = c_ez(k);
-    R X;
-    if (k == 0) {
-        X = -u2v2w2;
-    } else if (k < 7) {
-        const R comp = ex ? u : (ey ? v : w);
-        const R comp2 = ex ? uu2 : (ey ? vv2 : ww2);
-        const R s = R(ex + ey + ez);
-        X = s * R(3.0) * comp + R(4.5) * comp2 - u2v2w2;
-    } else {
-        const R uv = u * v * R(9.0) * qscale, uw = u * w * R(9.0) * qscale, vw = v * w * R(9.0) * qscale;
-        X = R(ex) * R(3.0) * u + R(ey) * R(3.0) * v + R(ez) * R(3.0) * w + R(ex * ey) * uv + R(ex * ez) * uw +
-            R(ey * ez) * vw + R(4.5) * uu2 + R(4.5) * vv2 + R(4.5) * ww2 - u2v2w2;
-    }
-    return lattice_w<R>(k) * (rho * (R(1.0) + X) + rho0 * X);
+    R eu = R(0);
+    if (ex) eu = ex > 0 ? eu + u : eu - u;
+    if (ey) eu = ey > 0 ? eu + v : eu - v;
+    if (ez) eu = ez > 0 ? eu + w : eu - w;
+    const R usq = u * u + v * v + w * w;
+    const R X = R(3.0) * eu + qscale * (R(4.5) * eu * eu - R(1.5) * usq);
+    return lattice_w<R>(k) * (rho + (rho + rho0) * X);
 }
 
 }  // namespace lbfs
