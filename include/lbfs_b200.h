@@ -237,6 +237,17 @@ int lbfs_get_launch_shape(lbfs_solver *s, lbfs_launch_shape *shape);
 int lbfs_set_launch_shape(lbfs_solver *s, const lbfs_launch_shape *shape);
 int lbfs_autotune(lbfs_solver *s, int32_t reps, lbfs_launch_shape *shape);
 
+/* ---- lossless checkpoint / restart ------------------------------------------ *
+ * Replaces the reference's restart from its 6-digit text output
+ * (Solution::output, Solution.cpp:221-251; Solver_gpu.cu:1953-1980): a
+ * caller-owned binary blob with soln_t1, the state with its ghosts, the
+ * viscosity field, the step counter and every membrane array, so a run resumed
+ * from it continues bit for bit.  Load checks sizes and precision against the
+ * handle (LBFS_ERR_ARG otherwise). */
+int lbfs_checkpoint_size(lbfs_solver *s, uint64_t *bytes);
+int lbfs_checkpoint_save(lbfs_solver *s, void *buf, uint64_t bytes);
+int lbfs_checkpoint_load(lbfs_solver *s, const void *buf, uint64_t bytes);
+
 /* ---- discrete adjoint (no reference counterpart) --------------------------- *
  * lbfs_adjoint runs n_steps forward from the handle's state, keeping soln_t1
  * (and, with membranes, node positions and MAD) every `checkpoint_every`

@@ -1536,3 +1536,106 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
     return LBFS_OK;
 }
+
+// ---- lossless checkpoint / restart -----------------------------------------
+//
+// Everything a step reads that a step or the set-up wrote: soln_t1, the
+// primitive state with its ghosts, the viscosity field, the residual sums, the
+// status word, the step counter; per membrane the node positions, velocities
+// and forces, the scalars (V0, A0, MAD0, MAD, V, A, bounds) and every
+// per-spring array.  Gradients and fluxes are not saved: each step forms them
+// before reading them.  The blob starts with a header that a load checks
+// against the handle (sizes, precision).
+
+namespace {
+
+struct CkHeader {
+    char magic[8];
+    int32_t version, precision, nc, nb, nf, n_membranes, total_nodes, total_springs;
+    int64_t t;
+    uint32_t flags, pad;
+};
+
+struct CkPart {
+    void *dev;
+    size_t bytes;
+};
+
+std::vector<CkPart> ck_parts(lbfs_solver *s) {
+    const size_t nc = s->nc, nt = (size_t)s->nc + s->nb, N = s->total_nodes, S = s->total_springs;
+    const size_t r = s->fp32 ? sizeof(float) : sizeof(double);
+    void *state = s->fp32 ? (void *)s->f32.state : (void *)s->f64.state;
+    void *visc = s->fp32 ? (void *)s->f32.visc_factor : (void *)s->f64.visc_factor;
+    void *t1 = s->fp32 ? (void *)s->f32.t1 : (void *)s->f64.t1;
+    void *rsum = s->fp32 ? (void *)s->f32.residual_sums : (void *)s->f64.residual_sums;
+    std::vector<CkPart> p = {{t1, sizeof(double4) * nc}, {state, 4 * r * nt}, {visc, r * nc}, {rsum, 4 * sizeof(double)}};
+    if (s->n_membranes > 0) {
+        const MembraneArgs &m = s->ma;
+        for (double *a : {m.x, m.y, m.z, m.vx, m.vy, m.vz, m.fx, m.fy, m.fz}) p.push_back({a, sizeof(double) * N});
+        p.push_back({m.ms, sizeof(MembraneScalars) * s->n_membranes});
+        for (double *a : {m.contour, m.kspring, m.curv, m.curv0, m.angle0}) p.push_back({a, sizeof(double) * S});
+        for (double *a : {m.area0, m.area}) p.push_back({a, sizeof(double) * 2 * S});
+    }
+    return p;
+}
+
+}  // namespace
+
+extern "C" int lbfs_checkpoint_size(lbfs_solver *s, uint64_t *bytes) {
+    if (!s || !bytes) return set_error(LBFS_ERR_ARG, "null argument");
+    size_t b = sizeof(CkHeader);
+    for (const CkPart &p : ck_parts(s)) b += p.bytes;
+    *bytes = b;
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_checkpoint_save(lbfs_solver *s, void *buf, uint64_t bytes) {
+    uint64_t need = 0;
+    int rc = lbfs_checkpoint_size(s, &need);
+    if (rc) return rc;
+    if (!buf || bytes < need) return set_error(LBFS_ERR_ARG, "checkpoint buffer too small (lbfs_checkpoint_size)");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    const unsigned int *flags = s->fp32 ? s->f32.flags : s->f64.flags;
+    CkHeader h{};
+    std::memcpy(h.magic, "LBFSCK01", 8);
+    h.version = 1;
+    h.precision = s->params.precision;
+    h.nc = s->nc; h.nb = s->nb; h.nf = s->nf;
+    h.n_membranes = s->n_membranes; h.total_nodes = s->total_nodes; h.total_springs = s->total_springs;
+    h.t = s->t;
+    LBFS_CUDA(cudaMemcpy(&h.flags, flags, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+    char *o = (char *)buf;
+    std::memcpy(o, &h, sizeof(h));
+    o += sizeof(h);
+    for (const CkPart &p : ck_parts(s)) {
+        LBFS_CUDA(cudaMemcpy(o, p.dev, p.bytes, cudaMemcpyDeviceToHost));
+        o += p.bytes;
+    }
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_checkpoint_load(lbfs_solver *s, const void *buf, uint64_t bytes) {
+    uint64_t need = 0;
+    int rc = lbfs_checkpoint_size(s, &need);
+    if (rc) return rc;
+    if (!buf || bytes < need) return set_error(LBFS_ERR_ARG, "checkpoint shorter than this handle's state");
+    CkHeader h;
+    std::memcpy(&h, buf, sizeof(h));
+    if (std::memcmp(h.magic, "LBFSCK01", 8) != 0 || h.version != 1)
+        return set_error(LBFS_ERR_ARG, "not an lbfs_b200 checkpoint");
+    if (h.precision != s->params.precision || h.nc != s->nc || h.nb != s->nb || h.nf != s->nf ||
+        h.n_membranes != s->n_membranes || h.total_nodes != s->total_nodes || h.total_springs != s->total_springs)
+        return set_error(LBFS_ERR_ARG, "checkpoint of a different mesh, membrane set or precision");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    const char *o = (const char *)buf + sizeof(h);
+    for (const CkPart &p : ck_parts(s)) {
+        LBFS_CUDA(cudaMemcpy(p.dev, o, p.bytes, cudaMemcpyHostToDevice));
+        o += p.bytes;
+    }
+    unsigned int *flags = s->fp32 ? s->f32.flags : s->f64.flags;
+    LBFS_CUDA(cudaMemcpy(flags, &h.flags, sizeof(unsigned int), cudaMemcpyHostToDevice));
+    s->t = h.t;
+    return LBFS_OK;
+}

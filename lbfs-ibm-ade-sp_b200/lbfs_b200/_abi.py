@@ -160,6 +160,9 @@ def lib():
             "lbfs_set_launch_shape": [vp, ctypes.POINTER(LaunchShape)],
             "lbfs_autotune": [vp, ctypes.c_int32, ctypes.POINTER(LaunchShape)],
             "lbfs_adjoint": [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(Objective), _f64p, _f64p, _f64p],
+            "lbfs_checkpoint_size": [vp, ctypes.POINTER(ctypes.c_uint64)],
+            "lbfs_checkpoint_save": [vp, vp, ctypes.c_uint64],
+            "lbfs_checkpoint_load": [vp, vp, ctypes.c_uint64],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -200,5 +203,5 @@ EXPORTED = [
     "lbfs_set_profiling", "lbfs_get_phase_times",
     "lbfs_last_error", "lbfs_mesh_uniform_counts", "lbfs_mesh_build_uniform", "lbfs_rbc_build_springs",
     "lbfs_residual_rms_noalloc", "lbfs_get_launch_shape", "lbfs_set_launch_shape", "lbfs_autotune",
-    "lbfs_adjoint",
+    "lbfs_adjoint", "lbfs_checkpoint_size", "lbfs_checkpoint_save", "lbfs_checkpoint_load",
 ]

@@ -208,6 +208,19 @@ class GpuSolver:
                                            ctypes.byref(J), _abi.ptr(g), _abi.ptr(t)))
         return J.value, dict(zip(("shear_modulus", "bending_modulus", "velocity_scale"), g.tolist())), t.tolist()
 
+    def checkpoint(self):
+        """Lossless snapshot of the handle's state (bytes)."""
+        n = ctypes.c_uint64()
+        _abi.check(_abi.lib().lbfs_checkpoint_size(self._h, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _abi.check(_abi.lib().lbfs_checkpoint_save(self._h, buf, n.value))
+        return buf.raw
+
+    def restore(self, blob):
+        """Resume from a snapshot taken by checkpoint() on a handle of the same case."""
+        buf = ctypes.create_string_buffer(blob, len(blob))
+        _abi.check(_abi.lib().lbfs_checkpoint_load(self._h, buf, len(blob)))
+
     def launches_per_step(self):
         n = ctypes.c_int32()
         _abi.check(_abi.lib().lbfs_launches_per_step(self._h, ctypes.byref(n)))

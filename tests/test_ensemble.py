@@ -130,3 +130,38 @@ def test_launch_shape_struct_roundtrip():
     sh = _abi.LaunchShape()
     sh.update_blocks = _abi.LBFS_MAX_UPDATE_BLOCKS
     assert sh.update_blocks == 148 * 16
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+def test_checkpoint_restart_is_lossless(precision):
+    """Snapshot, run on, restore (into the same and into a fresh handle), run
+    the same steps again: bit-identical states, nodes and residuals."""
+    from lbfs_b200 import GpuSolver, cases
+    c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, precision=precision)
+    with GpuSolver(c.mesh, c.params, c.membranes) as s:
+        s.set_state(c.rho, c.u, c.v, c.w)
+        s.step(3, graph=True)
+        blob = s.checkpoint()
+        s.step(5, graph=True)
+        ref = (s.state(), s.nodes(), s.residuals())
+        s.restore(blob)
+        s.step(5, graph=True)
+        again = (s.state(), s.nodes(), s.residuals())
+    with GpuSolver(c.mesh, c.params, c.membranes) as t:
+        t.restore(blob)
+        t.step(5)
+        fresh = (t.state(), t.nodes(), t.residuals())
+    for other in (again, fresh):
+        for a, b in zip(other[0], ref[0]):
+            assert np.array_equal(a, b)
+        assert np.array_equal(other[1], ref[1])
+        assert np.array_equal(other[2], ref[2])
+
+
+def test_checkpoint_rejects_foreign_blob():
+    from lbfs_b200 import _abi
+    import ctypes
+    buf = ctypes.create_string_buffer(b"not a checkpoint" * 8)
+    # argument checks run before any device work: a null handle is an argument error
+    assert _abi.lib().lbfs_checkpoint_load(None, buf, len(buf)) == _abi.LBFS_ERR_ARG
