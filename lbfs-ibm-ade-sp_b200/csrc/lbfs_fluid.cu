@@ -139,69 +139,93 @@ __device__ __forceinline__ Dir dir_of(int k) { return {c_ex(k), c_ey(k), c_ez(k)
 // the second moment's d_cm term is rho' / 3.  The reference sums the 15
 // equilibria explicitly; the closed form is the same quantity with fewer
 // roundings.
-template <typename R>
-__device__ __forceinline__ Vec4<R> interface_flux(const R (&fl)[15], R rho0, R tau, R qscale, R area, int axis,
-                                                  R nx, R ny, R nz) {
-    R rho_dev = fl[0];
+// Moments of the reconstructed populations, accumulated direction by
+// direction in the order k = 0..14 (the same sums and order as over a stored
+// fl[15], with 8-16 accumulators live instead of 15 populations).
+template <typename R> struct Moments {
+    R rho, m[3], F[3][4];  // F[c][.] over the directions crossing the face (c = axis, or all c)
+};
+template <typename R> __device__ __forceinline__ void moments_init(Moments<R> &M) {
+    M.rho = R(0);
 #pragma unroll
-    for (int k = 1; k < 15; k++) rho_dev = rho_dev + fl[k];
-    R mx = 0, my = 0, mz = 0;
+    for (int c = 0; c < 3; c++) {
+        M.m[c] = R(0);
 #pragma unroll
-    for (int k = 1; k < 15; k++) {
-        const Dir e = dir_of(k);
-        if (e.ex) mx = (e.ex > 0) ? mx + fl[k] : mx - fl[k];
-        if (e.ey) my = (e.ey > 0) ? my + fl[k] : my - fl[k];
-        if (e.ez) mz = (e.ez > 0) ? mz + fl[k] : mz - fl[k];
+        for (int j = 0; j < 4; j++) M.F[c][j] = R(0);
     }
-    const R rho_i = rho_dev + rho0;
-    const R inv = R(1) / rho_i;
-    const R u[3] = {inv * mx, inv * my, inv * mz};
-    // moments of the reconstructed populations: F_fl[c][m], c = face axis
-    // component, m = (mass, mom x, mom y, mom z)
-    R F[3][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}};
+}
+template <typename R>
+__device__ __forceinline__ void moments_add(Moments<R> &M, int k, R f, int axis) {
+    M.rho = (k == 0) ? f : M.rho + f;
+    if (k == 0) return;
+    const Dir e = dir_of(k);
+    if (e.ex) M.m[0] = (e.ex > 0) ? M.m[0] + f : M.m[0] - f;
+    if (e.ey) M.m[1] = (e.ey > 0) ? M.m[1] + f : M.m[1] - f;
+    if (e.ez) M.m[2] = (e.ez > 0) ? M.m[2] + f : M.m[2] - f;
+    if (axis == 0 && !e.ex) return;
+    if (axis == 1 && !e.ey) return;
+    if (axis == 2 && !e.ez) return;
+    const int ee[3] = {e.ex, e.ey, e.ez};
 #pragma unroll
-    for (int k = 1; k < 15; k++) {
-        const Dir e = dir_of(k);
-        if (axis == 0 && !e.ex) continue;
-        if (axis == 1 && !e.ey) continue;
-        if (axis == 2 && !e.ez) continue;
-        const R f = fl[k];
-        const int ee[3] = {e.ex, e.ey, e.ez};
+    for (int c = 0; c < 3; c++) {
+        if (axis >= 0 && c != axis) continue;
+        if (!ee[c]) continue;
+        M.F[c][0] = (ee[c] > 0) ? M.F[c][0] + f : M.F[c][0] - f;
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            if (axis >= 0 && c != axis) continue;
-            if (!ee[c]) continue;
-            F[c][0] = (ee[c] > 0) ? F[c][0] + f : F[c][0] - f;
-#pragma unroll
-            for (int m = 0; m < 3; m++) {
-                if (!ee[m]) continue;
-                F[c][1 + m] = (ee[c] * ee[m] > 0) ? F[c][1 + m] + f : F[c][1 + m] - f;
-            }
+        for (int q = 0; q < 3; q++) {
+            if (!ee[q]) continue;
+            M.F[c][1 + q] = (ee[c] * ee[q] > 0) ? M.F[c][1 + q] + f : M.F[c][1 + q] - f;
         }
     }
+}
+
+// Interface equilibrium, BGK relaxation towards the lattice equilibria and
+// the flux through the face: calculate_flux_at_interface (LBFS.cu:1462-1648)
+// and its axis-aligned forms (LBFS.cu:3648-4092).  `axis` < 0 selects the
+// general three-component form with the face normal; otherwise only the
+// face-normal component is formed.
+//
+// The relaxed populations are f_k - tau (f_k - fl_k), f_k the interface
+// equilibrium, so the flux tensor is (1 - tau) F_eq + tau F_fl, F_fl the
+// first and second moments of the reconstructed fl_k over the directions
+// crossing the face and F_eq those of the equilibrium.  The D3Q15 weights
+// make the equilibrium moments exact closed forms (sum w e = 0,
+// sum w e e = I / 3, sum w e e e e = (dd + dd + dd) / 9):
+//   sum_k e_c f_k = rho u_c,  sum_k e_c e_m f_k = rho (q u_c u_m + d_cm / 3)
+// (q the preconditioning factor); in the deviation form (f' = f - w rho0)
+// the second moment's d_cm term is rho' / 3.  The reference sums the 15
+// equilibria explicitly; the closed form is the same quantity with fewer
+// roundings.
+template <typename R>
+__device__ __forceinline__ Vec4<R> interface_flux(Moments<R> &M, R rho0, R tau, R qscale, R area, int axis, R nx,
+                                                  R ny, R nz) {
+    const R rho_dev = M.rho;
+    const R rho_i = rho_dev + rho0;
+    const R inv = R(1) / rho_i;
+    const R u[3] = {inv * M.m[0], inv * M.m[1], inv * M.m[2]};
     const R keep = R(1) - tau;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         if (axis >= 0 && c != axis) continue;
-        F[c][0] = keep * (rho_i * u[c]) + tau * F[c][0];
+        M.F[c][0] = keep * (rho_i * u[c]) + tau * M.F[c][0];
 #pragma unroll
         for (int m = 0; m < 3; m++) {
             R eq = rho_i * (qscale * u[c] * u[m]);
             if (m == c) eq = eq + rho_dev * R(1.0 / 3.0);
-            F[c][1 + m] = keep * eq + tau * F[c][1 + m];
+            M.F[c][1 + m] = keep * eq + tau * M.F[c][1 + m];
         }
     }
     Vec4<R> out;
     if (axis >= 0) {
-        out.rho = F[axis][0] * area;
-        out.u = F[axis][1] * area;
-        out.v = F[axis][2] * area;
-        out.w = F[axis][3] * area;
+        out.rho = M.F[axis][0] * area;
+        out.u = M.F[axis][1] * area;
+        out.v = M.F[axis][2] * area;
+        out.w = M.F[axis][3] * area;
     } else {
-        out.rho = (F[0][0] * nx + F[1][0] * ny + F[2][0] * nz) * area;
-        out.u = (F[0][1] * nx + F[1][1] * ny + F[2][1] * nz) * area;
-        out.v = (F[0][2] * nx + F[1][2] * ny + F[2][2] * nz) * area;
-        out.w = (F[0][3] * nx + F[1][3] * ny + F[2][3] * nz) * area;
+        out.rho = (M.F[0][0] * nx + M.F[1][0] * ny + M.F[2][0] * nz) * area;
+        out.u = (M.F[0][1] * nx + M.F[1][1] * ny + M.F[2][1] * nz) * area;
+        out.v = (M.F[0][2] * nx + M.F[1][2] * ny + M.F[2][2] * nz) * area;
+        out.w = (M.F[0][3] * nx + M.F[1][3] * ny + M.F[2][3] * nz) * area;
     }
     return out;
 }
@@ -237,7 +261,8 @@ __device__ __forceinline__ Vec4<R> axis_face_flux(const FluidArgs<R> &a, int f) 
     }
     constexpr int ob = axis == 0 ? 1 : 0;  // other axes in increasing order
     constexpr int oc2 = axis == 2 ? 1 : 2;
-    R fl[15];
+    Moments<R> M;
+    moments_init(M);
 #pragma unroll
     for (int k = 0; k < 15; k++) {
         const Dir e = dir_of(k);
@@ -267,11 +292,11 @@ __device__ __forceinline__ Vec4<R> axis_face_flux(const FluidArgs<R> &a, int f) 
             }
             L[m] = val;
         }
-        fl[k] = feq_dev<R>(k, L[0], L[1], L[2], L[3], a.rho0, R(1));
+        moments_add(M, k, feq_dev<R>(k, L[0], L[1], L[2], L[3], a.rho0, R(1)), axis);
     }
     const R vf = a.visc_factor[oc.x];
     const R tau = (a.testcase == 8) ? R(0) : (a.visc * vf * R(3) / dt * a.gamma_inv);
-    return interface_flux<R>(fl, a.rho0, tau, R(1), geo.area, axis, 0, 0, 0);
+    return interface_flux<R>(M, a.rho0, tau, R(1), geo.area, axis, 0, 0, 0);
 }
 
 // General face: populate_lattice_macros (LBFS.cu:323-936).  Boundary faces
@@ -316,8 +341,9 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
     // Upwind selection by the sign of n.e_k with the threshold 0.001 dt
     // (LBFS.cu:351-352 override the sin(pi/14) arguments).
     const R thr = R(0.001) * dt;
-    R fl[15];
-    fl[0] = feq_dev<R>(0, p0[0], p0[1], p0[2], p0[3], a.rho0, R(1));
+    Moments<R> M;
+    moments_init(M);
+    moments_add(M, 0, feq_dev<R>(0, p0[0], p0[1], p0[2], p0[3], a.rho0, R(1)), -1);
 #pragma unroll
     for (int k = 1; k < 15; k += 2) {
         const Dir e = dir_of(k);
@@ -343,19 +369,19 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
                 }
                 L[m] = val;
             }
-            fl[kk] = feq_dev<R>(kk, L[0], L[1], L[2], L[3], a.rho0, R(1));
+            moments_add(M, kk, feq_dev<R>(kk, L[0], L[1], L[2], L[3], a.rho0, R(1)), -1);
         }
     }
     const R vf = is_bc ? R(1) : a.visc_factor[oc.x];
     const R tau = (a.testcase == 8) ? R(0) : (a.visc * vf * R(3) / dt * a.gamma_inv);
-    return interface_flux<R>(fl, a.rho0, tau, a.gamma_inv, geo.area, -1, geo.nx, geo.ny, geo.nz);
+    return interface_flux<R>(M, a.rho0, tau, a.gamma_inv, geo.area, -1, geo.nx, geo.ny, geo.nz);
 }
 
 // Interior faces of an axis-aligned mesh: faces [0, nfx) x, [nfx, nfx+nfy) y,
 // the rest z; warps never mix axes except at the two range boundaries.
-// TB threads per block, 512 / TB blocks per SM (at most 128 registers a thread).
+// TB threads per block, 640 / TB blocks per SM (at most 102 registers a thread).
 template <typename R, int TB>
-__global__ void __launch_bounds__(TB, 512 / TB) k_face_flux(FluidArgs<R> a) {
+__global__ void __launch_bounds__(TB, 640 / TB) k_face_flux(FluidArgs<R> a) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= a.ni) return;
     Vec4<R> out;
