@@ -217,11 +217,12 @@ int lbfs_last_error(char *buf, int32_t len);
 /* ---- launch shapes and the autotuner (no reference counterpart) ----------- *
  * Block sizes and grid caps of the per-phase kernels.  Results do not depend on
  * the shape, except the last bits of the residual norms, whose block partials
- * follow the cell-update grid.  lbfs_autotune times every candidate shape of
- * each kernel on this handle's own mesh and state (`reps` launches each, CUDA
- * events), keeps the fastest, and leaves the state as it found it; the next
- * lbfs_step_graph captures a new graph.  `shape` (may be null) receives the
- * choice and the mean time of each chosen kernel in microseconds. */
+ * follow the cell-update grid.  lbfs_autotune searches the shape coordinate by
+ * coordinate, timing each candidate as `reps` whole steps (CUDA-graph replays,
+ * CUDA events) from the handle's current state, which it saves and puts back;
+ * it keeps a candidate only for a gain above 1 %.  The next lbfs_step_graph
+ * captures a new graph.  `shape` (may be null) receives the choice;
+ * time_us[0] is its mean step time in microseconds. */
 #define LBFS_MAX_UPDATE_BLOCKS (148 * 16)
 #define LBFS_MAX_SPREAD_BLOCKS (148 * 16)
 typedef struct lbfs_launch_shape {
@@ -231,7 +232,7 @@ typedef struct lbfs_launch_shape {
     int32_t update_threads;         /* 128, 256 or 512 */
     int32_t update_blocks;          /* grid cap of the cell update, 1 .. LBFS_MAX_UPDATE_BLOCKS */
     int32_t spread_blocks;          /* grid of the IBM spread, 1 .. LBFS_MAX_SPREAD_BLOCKS */
-    double time_us[5];              /* autotune: gradients, flux, general flux, update, spread */
+    double time_us[5];              /* autotune: [0] mean step time of the chosen shape (us) */
 } lbfs_launch_shape;
 int lbfs_get_launch_shape(lbfs_solver *s, lbfs_launch_shape *shape);
 int lbfs_set_launch_shape(lbfs_solver *s, const lbfs_launch_shape *shape);

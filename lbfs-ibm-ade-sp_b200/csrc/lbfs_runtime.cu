@@ -1005,121 +1005,7 @@ void drop_graph(lbfs_solver *s) {
     if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
 }
 
-// Mean device time of `reps` launches of `launch` (after one untimed launch).
-template <typename F> int time_launches(lbfs_solver *s, int reps, cudaEvent_t e0, cudaEvent_t e1, F launch,
-                                        double *us) {
-    launch();
-    LBFS_CUDA(cudaEventRecord(e0, s->stream));
-    for (int r = 0; r < reps; r++) launch();
-    LBFS_CUDA(cudaEventRecord(e1, s->stream));
-    LBFS_CUDA(cudaEventSynchronize(e1));
-    LBFS_CUDA(cudaGetLastError());
-    float ms = 0;
-    LBFS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    *us = 1000.0 * ms / reps;
-    return LBFS_OK;
-}
-
-template <typename R> int autotune(lbfs_solver *s, int reps, lbfs_launch_shape *out) {
-    FluidArgs<R> &a = fluid<R>(s);
-    const size_t nt = (size_t)s->nc + s->nb;
-    LBFS_CUDA(cudaStreamSynchronize(s->stream));
-    // the update advances the state: keep a copy and put it back afterwards
-    void *keep_state = nullptr, *keep_t1 = nullptr, *keep_misc = nullptr;
-    LBFS_CUDA(cudaMalloc(&keep_state, sizeof(Vec4<R>) * nt));
-    LBFS_CUDA(cudaMalloc(&keep_t1, sizeof(double4) * s->nc));
-    LBFS_CUDA(cudaMalloc(&keep_misc, 64));
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    int rc = LBFS_OK;
-    lbfs_launch_shape best = args_to_shape<R>(s);
-    auto run = [&]() -> int {
-        LBFS_CUDA(cudaEventCreate(&e0));
-        LBFS_CUDA(cudaEventCreate(&e1));
-        LBFS_CUDA(cudaMemcpyAsync(keep_state, a.state, sizeof(Vec4<R>) * nt, cudaMemcpyDeviceToDevice, s->stream));
-        LBFS_CUDA(cudaMemcpyAsync(keep_t1, a.t1, sizeof(double4) * s->nc, cudaMemcpyDeviceToDevice, s->stream));
-        LBFS_CUDA(cudaMemcpyAsync(keep_misc, a.residual_sums, 4 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-        LBFS_CUDA(cudaMemcpyAsync((char *)keep_misc + 32, a.flags, sizeof(unsigned int), cudaMemcpyDeviceToDevice,
-                                  s->stream));
-        double t = 0, tbest;
-        int r;
-        // gradients
-        tbest = 1e300;
-        for (int tb : {128, 256, 512}) {
-            a.tb_grad = tb;
-            if ((r = time_launches(s, reps, e0, e1, [&] { launch_fluid_gradients<R>(a, s->stream); }, &t))) return r;
-            if (t < tbest) { tbest = t; best.gradient_threads = tb; }
-        }
-        best.time_us[0] = tbest;
-        a.tb_grad = best.gradient_threads;
-        // interior (axis-aligned) faces, then the general-normal faces
-        if (a.axis_aligned && a.ni > 0) {
-            tbest = 1e300;
-            for (int tb : {64, 128, 256}) {
-                a.tb_flux = tb;
-                if ((r = time_launches(s, reps, e0, e1, [&] { launch_fluid_flux_axis<R>(a, s->stream); }, &t))) return r;
-                if (t < tbest) { tbest = t; best.flux_threads = tb; }
-            }
-            best.time_us[1] = tbest;
-            a.tb_flux = best.flux_threads;
-        }
-        if (a.nf > (a.axis_aligned ? a.ni : 0)) {
-            tbest = 1e300;
-            for (int tb : {64, 128, 256}) {
-                a.tb_gen = tb;
-                if ((r = time_launches(s, reps, e0, e1, [&] { launch_fluid_flux_general<R>(a, s->stream); }, &t)))
-                    return r;
-                if (t < tbest) { tbest = t; best.general_flux_threads = tb; }
-            }
-            best.time_us[2] = tbest;
-            a.tb_gen = best.general_flux_threads;
-        }
-        // cell update: block size x grid cap
-        tbest = 1e300;
-        for (int tb : {128, 256, 512}) {
-            for (int mult : {2, 4, 8, 16}) {
-                a.tb_update = tb;
-                a.update_blocks = 148 * mult;
-                if ((r = time_launches(s, reps, e0, e1, [&] { launch_fluid_update<R>(a, s->stream); }, &t))) return r;
-                if (t < tbest) { tbest = t; best.update_threads = tb; best.update_blocks = 148 * mult; }
-            }
-        }
-        best.time_us[3] = tbest;
-        a.tb_update = best.update_threads;
-        a.update_blocks = best.update_blocks;
-        // IBM spread over the current node forces and positions
-        if (s->n_membranes > 0) {
-            launch_membrane_tables(s->ma, s->stream);
-            launch_membrane_sort(s->ma, s->stream);
-            tbest = 1e300;
-            for (int mult : {1, 2, 4, 8, 16}) {
-                s->ma.spread_blocks = 148 * mult;
-                if ((r = time_launches(s, reps, e0, e1, [&] { launch_membrane_spread(s->ma, s->stream); }, &t)))
-                    return r;
-                if (t < tbest) { tbest = t; best.spread_blocks = 148 * mult; }
-            }
-            best.time_us[4] = tbest;
-        }
-        return LBFS_OK;
-    };
-    rc = run();
-    // restore (also after a failure, as far as the device lets us)
-    cudaMemcpyAsync(a.state, keep_state, sizeof(Vec4<R>) * nt, cudaMemcpyDeviceToDevice, s->stream);
-    cudaMemcpyAsync(a.t1, keep_t1, sizeof(double4) * s->nc, cudaMemcpyDeviceToDevice, s->stream);
-    cudaMemcpyAsync(a.residual_sums, keep_misc, 4 * sizeof(double), cudaMemcpyDeviceToDevice, s->stream);
-    cudaMemcpyAsync(a.flags, (char *)keep_misc + 32, sizeof(unsigned int), cudaMemcpyDeviceToDevice, s->stream);
-    cudaError_t e = cudaStreamSynchronize(s->stream);
-    cudaFree(keep_state);
-    cudaFree(keep_t1);
-    cudaFree(keep_misc);
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
-    if (rc) return rc;
-    if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("autotune restore: ") + cudaGetErrorString(e));
-    shape_to_args<R>(s, best);
-    drop_graph(s);
-    if (out) *out = best;
-    return LBFS_OK;
-}
+int autotune_steps(lbfs_solver *s, int reps, lbfs_launch_shape *out, bool fp32);
 
 }  // namespace
 
@@ -1143,7 +1029,7 @@ extern "C" int lbfs_autotune(lbfs_solver *s, int32_t reps, lbfs_launch_shape *sh
     if (!s) return set_error(LBFS_ERR_ARG, "null handle");
     if (reps < 1 || reps > 1000) return set_error(LBFS_ERR_ARG, "reps must be in 1..1000");
     LBFS_CUDA(cudaSetDevice(s->device));
-    return s->fp32 ? autotune<float>(s, reps, shape) : autotune<double>(s, reps, shape);
+    return autotune_steps(s, reps, shape, s->fp32);
 }
 
 
@@ -1639,3 +1525,110 @@ extern "C" int lbfs_checkpoint_load(lbfs_solver *s, const void *buf, uint64_t by
     s->t = h.t;
     return LBFS_OK;
 }
+
+// ---- step-level autotuner ---------------------------------------------------
+
+namespace {
+
+// Coordinate descent over the launch shape, each candidate timed as whole
+// steps (graph replays, CUDA events on the handle's stream) from the same
+// saved state: the kernels run with the contention of a real step (the
+// membrane chain beside the fluid kernels), which isolated kernel timings
+// miss.  The state (the checkpoint parts, the counter and the status word)
+// is put back afterwards.
+int autotune_steps(lbfs_solver *s, int reps, lbfs_launch_shape *out, bool fp32) {
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    const std::vector<CkPart> parts = ck_parts(s);
+    size_t total = 0;
+    for (const CkPart &p : parts) total += p.bytes;
+    DevBuf snap;
+    LBFS_CUDA(cudaMalloc(&snap.p, total + sizeof(unsigned int)));
+    unsigned int *flags = fp32 ? s->f32.flags : s->f64.flags;
+    auto copy_all = [&](bool save) -> int {
+        char *o = (char *)snap.p;
+        for (const CkPart &p : parts) {
+            LBFS_CUDA(cudaMemcpyAsync(save ? (void *)o : p.dev, save ? p.dev : (void *)o, p.bytes,
+                                      cudaMemcpyDeviceToDevice, s->stream));
+            o += p.bytes;
+        }
+        LBFS_CUDA(cudaMemcpyAsync(save ? (void *)o : (void *)flags, save ? (void *)flags : (void *)o,
+                                  sizeof(unsigned int), cudaMemcpyDeviceToDevice, s->stream));
+        return LBFS_OK;
+    };
+    int rc = copy_all(true);
+    if (rc) return rc;
+    const long long t0 = s->t;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    LBFS_CUDA(cudaEventCreate(&e0));
+    LBFS_CUDA(cudaEventCreate(&e1));
+    auto measure = [&](double *us) -> int {
+        int r = copy_all(false);
+        if (r) return r;
+        s->t = t0;
+        drop_graph(s);
+        if ((r = lbfs_step_graph(s, 2))) return r;  // capture + warm
+        LBFS_CUDA(cudaEventRecord(e0, s->stream));
+        if ((r = lbfs_step_graph(s, reps))) return r;
+        LBFS_CUDA(cudaEventRecord(e1, s->stream));
+        LBFS_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        LBFS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        *us = 1000.0 * ms / reps;
+        return LBFS_OK;
+    };
+    auto apply = [&](const lbfs_launch_shape &sh) {
+        if (fp32) shape_to_args<float>(s, sh);
+        else shape_to_args<double>(s, sh);
+    };
+    struct Knob {
+        int32_t lbfs_launch_shape::*field;
+        std::vector<int> values;
+    };
+    const bool membranes = s->n_membranes > 0;
+    const std::vector<Knob> knobs = {
+        {&lbfs_launch_shape::gradient_threads, {128, 256, 512}},
+        {&lbfs_launch_shape::flux_threads, {64, 128, 256}},
+        {&lbfs_launch_shape::general_flux_threads, {64, 128, 256}},
+        {&lbfs_launch_shape::update_threads, {128, 256, 512}},
+        {&lbfs_launch_shape::update_blocks, {148 * 2, 148 * 4, 148 * 8, 148 * 16}},
+        {&lbfs_launch_shape::spread_blocks,
+         membranes ? std::vector<int>{148, 296, 592, 1184, 2368} : std::vector<int>{}},
+    };
+    lbfs_launch_shape cur = fp32 ? args_to_shape<float>(s) : args_to_shape<double>(s);
+    double best = 0;
+    rc = measure(&best);
+    for (size_t q = 0; !rc && q < knobs.size(); q++) {
+        const Knob &k = knobs[q];
+        for (size_t v = 0; !rc && v < k.values.size(); v++) {
+            if (cur.*(k.field) == k.values[v]) continue;
+            lbfs_launch_shape trial = cur;
+            trial.*(k.field) = k.values[v];
+            apply(trial);
+            double t = 0;
+            rc = measure(&t);
+            if (!rc && t < 0.99 * best) {  // keep only a clear gain
+                best = t;
+                cur = trial;
+            }
+        }
+        apply(cur);
+    }
+    apply(cur);
+    const int r2 = copy_all(false);
+    if (!rc) rc = r2;
+    s->t = t0;
+    drop_graph(s);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+    if (out) {
+        *out = cur;
+        for (int q = 0; q < 5; q++) out->time_us[q] = 0.0;
+        out->time_us[0] = best;
+    }
+    return LBFS_OK;
+}
+
+}  // namespace

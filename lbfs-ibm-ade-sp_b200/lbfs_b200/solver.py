@@ -46,7 +46,7 @@ class StepParams:
 
 def _shape_dict(sh):
     d = {name: getattr(sh, name) for name, _ in _abi.LaunchShape._fields_ if name != "time_us"}
-    d["time_us"] = dict(zip(("gradients", "flux", "general_flux", "update", "spread"), list(sh.time_us)))
+    d["step_us"] = float(sh.time_us[0])
     return d
 
 
@@ -174,14 +174,14 @@ class GpuSolver:
         sh = _abi.LaunchShape()
         _abi.check(_abi.lib().lbfs_get_launch_shape(self._h, ctypes.byref(sh)))
         for k, v in kw.items():
-            if k == "time_us" or not hasattr(sh, k):
+            if k in ("time_us", "step_us") or not hasattr(sh, k):
                 raise KeyError(k)
             setattr(sh, k, int(v))
         _abi.check(_abi.lib().lbfs_set_launch_shape(self._h, ctypes.byref(sh)))
 
     def autotune(self, reps=20):
-        """Time the candidate launch shapes on this handle's mesh and state and
-        keep the fastest; returns the choice with per-kernel mean times (us)."""
+        """Search the launch shape by timing whole steps from this handle's state
+        (which it puts back); returns the choice and its step time (us)."""
         sh = _abi.LaunchShape()
         _abi.check(_abi.lib().lbfs_autotune(self._h, int(reps), ctypes.byref(sh)))
         return _shape_dict(sh)

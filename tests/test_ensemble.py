@@ -113,7 +113,7 @@ def test_autotune_keeps_state_and_results():
             h.step(2, graph=True)
         before = s.state()
         chosen = s.autotune(reps=3)
-        assert all(v > 0 for k, v in chosen["time_us"].items())
+        assert chosen["step_us"] > 0
         for a, b in zip(s.state(), before):
             assert np.array_equal(a, b)
         assert s.launch_shape()["update_blocks"] == chosen["update_blocks"]
