@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble section")
     ap.add_argument("--instances", type=int, default=64, help="instances of the batched ensemble")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint section")
+    ap.add_argument("--no-precision", action="store_true", help="skip the jittered 128^3 FP32/FP64 precision study")
+    ap.add_argument("--precision-steps", type=int, default=1000)
     ap.add_argument("--adjoint-steps", type=int, default=500)
     return ap.parse_args()
 
@@ -299,6 +301,45 @@ def run_batched(args, K, warmup, flush, device, plain_fp64_value):
                         "4-point Peskin IBM; seed 2024"}
 
 
+def run_precision(args, device):
+    """FP32-bulk vs FP64 precision study: 128^3 jittered hex mesh (interior
+    vertices moved by up to 10 % of the spacing, general-normal fluxes on every
+    face), body-force duct flow with 16 L3 red cells, N steps in each precision;
+    field and red-cell shape errors of the FP32 run against the FP64 run."""
+    import numpy as np
+
+    from lbfs_b200 import GpuSolver, _abi, cases
+    N = args.precision_steps
+    out = {}
+    runs = {}
+    for name, prec in (("fp64", _abi.LBFS_FP64), ("fp32", _abi.LBFS_FP32_BULK)):
+        c = cases.jittered_channel(precision=prec)
+        with GpuSolver(c.mesh, c.params, c.membranes, device=device) as s:
+            s.set_state(c.rho, c.u, c.v, c.w)
+            s.step(3, graph=True)
+            s.autotune(reps=5)
+            s.set_profiling(1)
+            t = 0.0
+            for _ in range(N - 3):
+                s.step(1, graph=True)
+                t += s.phase_times()[5]
+            runs[name] = (s.state(), s.nodes().reshape(-1, 3), s.status())
+            out[name] = {"value": c.mesh.n_cells * (N - 3) / (t * 1e-3) / 1e6, "ms_per_step": t / (N - 3)}
+        info = c.info
+    (r64, x64, f64), (r32, x32, f32) = runs["fp64"], runs["fp32"]
+    rel_inf = {k: float(np.max(np.abs(a - b)) / np.max(np.abs(b))) for k, a, b in zip("uvw", r32[1:], r64[1:])}
+    rel_l2 = {k: float(np.linalg.norm(a - b) / np.linalg.norm(b)) for k, a, b in zip("uvw", r32[1:], r64[1:])}
+    R = info["radius_cells"] * 2.0
+    return {"workload": f"128^3 jittered hex mesh (jitter 0.1 of the spacing, seed 1313; 2097152 cells, general-normal "
+                        f"fluxes), body-force duct, {info['n_rbc']} L3 red cells radius 6 cells, 4-point Peskin IBM, "
+                        f"{N} steps per precision",
+            "fp64": out["fp64"], "fp32_bulk": out["fp32"], "speedup": out["fp32"]["value"] / out["fp64"]["value"],
+            "rel_err_velocity_inf": rel_inf, "rel_err_velocity_l2": rel_l2,
+            "rel_err_rho_deviation_inf": float(np.max(np.abs(r32[0] - r64[0])) / np.max(np.abs(r64[0] - 1.0))),
+            "rbc_shape_err_over_radius": float(np.max(np.abs(x32 - x64)) / R),
+            "status_flags": [f64, f32], "unit": METRIC}
+
+
 def run_adjoint(args, device):
     """Discrete adjoint on the adjoint configuration: 48^3 shear channel, one
     level-4 red cell (2562 nodes, 5120 triangles, radius 8 cells), FP64,
@@ -504,6 +545,13 @@ def main():
         except Exception as exc:
             batched = {"value": None, "error": f"{type(exc).__name__}: {exc}"}
 
+    precision = None
+    if rank == 0 and not args.no_precision:
+        try:
+            precision = run_precision(args, local_rank)
+        except Exception as exc:
+            precision = {"error": f"{type(exc).__name__}: {exc}"}
+
     adjoint = None
     if rank == 0 and not args.no_adjoint:
         try:
@@ -537,6 +585,7 @@ def main():
             "fp32_bulk": fp32,
             "batched": batched,
             "adjoint": adjoint,
+            "precision_study": precision,
             "status_flags": status,
         }
         print(json.dumps(line))

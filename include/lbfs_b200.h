@@ -314,6 +314,23 @@ int lbfs_mesh_build_uniform(double X, double Y, double Z, double dt, const doubl
                             double *cell_volume, double *cell_centroid, int32_t *gradient_stencil,
                             double *lhs_inverse, double *rhs, int32_t *bc_patch, double *delta_h);
 
+/* The same mesh with every interior vertex moved by a seeded uniform
+ * perturbation of up to `jitter` (< 0.25) times the cell spacing per axis
+ * (boundary vertices stay, so the box and its patches stay).  Faces are then
+ * non-planar quadrilaterals and normals general: a stand-in for the imported
+ * (mesh_type 3) meshes the reference reads through its OpenFOAM importer
+ * (unstructured_mesh.cpp:705-869), with the same geometry and gradient
+ * formulas except one: a face's area is the length of the sum of its two
+ * triangles' vector areas (the reference sums their lengths, which on a
+ * warped face makes the vector areas of a cell's faces fail to close, so a
+ * fluid at rest starts to move).  Step it with axis_aligned = 0. */
+int lbfs_mesh_build_jittered(double X, double Y, double Z, double dt, const double *origin, double visc,
+                             double fneq_min, int32_t gradient_hybrid, double jitter, uint64_t seed, int32_t *owner,
+                             int32_t *neighbour, double *face_area, double *face_normal, double *face_centroid,
+                             double *streaming_dt, double *cell_volume, double *cell_centroid,
+                             int32_t *gradient_stencil, double *lhs_inverse, double *rhs, int32_t *bc_patch,
+                             double *delta_h);
+
 /* Spring connectivity of a closed triangulated membrane, in the order the
  * reference's Osay reader produces it (lagrangian_object.cpp:238-481).
  * spring_out must hold 4 * capacity ints; *n_springs receives the count. */

@@ -64,12 +64,57 @@ extern "C" int lbfs_mesh_uniform_counts(double X, double Y, double Z, double dt,
     return LBFS_OK;
 }
 
+namespace {
+
+// Seeded uniform variate in [-1, 1) for (seed, vertex, axis): splitmix64 of
+// the combined key, top 53 bits.
+double jitter_unit(uint64_t seed, uint64_t vertex, int axis) {
+    uint64_t z = seed * 0x9E3779B97F4A7C15ull + vertex * 3 + (uint64_t)axis + 0x632BE59BD9B4E019ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z = z ^ (z >> 31);
+    return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+int build_mesh(double X, double Y, double Z, double dt, const double *origin, double visc, double fneq_min,
+               int32_t gradient_hybrid, double jitter, uint64_t seed, int32_t *owner, int32_t *neighbour,
+               double *face_area, double *face_normal, double *face_centroid, double *streaming_dt,
+               double *cell_volume, double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse,
+               double *rhs, int32_t *bc_patch, double *delta_h);
+
+}  // namespace
+
 extern "C" int lbfs_mesh_build_uniform(double X, double Y, double Z, double dt, const double *origin, double visc,
                                        double fneq_min, int32_t gradient_hybrid, int32_t *owner, int32_t *neighbour,
                                        double *face_area, double *face_normal, double *face_centroid,
                                        double *streaming_dt, double *cell_volume, double *cell_centroid,
                                        int32_t *gradient_stencil, double *lhs_inverse, double *rhs, int32_t *bc_patch,
                                        double *delta_h) {
+    return build_mesh(X, Y, Z, dt, origin, visc, fneq_min, gradient_hybrid, 0.0, 0, owner, neighbour, face_area,
+                      face_normal, face_centroid, streaming_dt, cell_volume, cell_centroid, gradient_stencil,
+                      lhs_inverse, rhs, bc_patch, delta_h);
+}
+
+extern "C" int lbfs_mesh_build_jittered(double X, double Y, double Z, double dt, const double *origin, double visc,
+                                        double fneq_min, int32_t gradient_hybrid, double jitter, uint64_t seed,
+                                        int32_t *owner, int32_t *neighbour, double *face_area, double *face_normal,
+                                        double *face_centroid, double *streaming_dt, double *cell_volume,
+                                        double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse,
+                                        double *rhs, int32_t *bc_patch, double *delta_h) {
+    if (!(jitter >= 0.0 && jitter < 0.25))
+        return lbfs::set_error(LBFS_ERR_ARG, "jitter must be in [0, 0.25) of the cell spacing");
+    return build_mesh(X, Y, Z, dt, origin, visc, fneq_min, gradient_hybrid, jitter, seed, owner, neighbour,
+                      face_area, face_normal, face_centroid, streaming_dt, cell_volume, cell_centroid,
+                      gradient_stencil, lhs_inverse, rhs, bc_patch, delta_h);
+}
+
+namespace {
+
+int build_mesh(double X, double Y, double Z, double dt, const double *origin, double visc, double fneq_min,
+               int32_t gradient_hybrid, double jitter, uint64_t seed, int32_t *owner, int32_t *neighbour,
+               double *face_area, double *face_normal, double *face_centroid, double *streaming_dt,
+               double *cell_volume, double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse,
+               double *rhs, int32_t *bc_patch, double *delta_h) {
     int32_t cnt[8];
     int rc = lbfs_mesh_uniform_counts(X, Y, Z, dt, cnt);
     if (rc) return rc;
@@ -87,9 +132,16 @@ extern "C" int lbfs_mesh_build_uniform(double X, double Y, double Z, double dt, 
         for (int k = 0; k < nvz; k++)
             for (int j = 0; j < nvy; j++)
                 for (int i = 0; i < nvx; i++, t++) {
-                    vx[t] = (float)(origin[0] + i * d.dx);
-                    vy[t] = (float)(origin[1] + j * d.dy);
-                    vz[t] = (float)(origin[2] + k * d.dz);
+                    double px = origin[0] + i * d.dx, py = origin[1] + j * d.dy, pz = origin[2] + k * d.dz;
+                    // interior vertices move by up to jitter * spacing per axis (the box stays a box)
+                    if (jitter > 0 && i > 0 && j > 0 && k > 0 && i < nvx - 1 && j < nvy - 1 && k < nvz - 1) {
+                        px += jitter * d.dx * jitter_unit(seed, t, 0);
+                        py += jitter * d.dy * jitter_unit(seed, t, 1);
+                        pz += jitter * d.dz * jitter_unit(seed, t, 2);
+                    }
+                    vx[t] = (float)px;
+                    vy[t] = (float)py;
+                    vz[t] = (float)pz;
                 }
     }
     // Face loop order and vertex winding: unstructured_mesh.cpp:415-664.
@@ -191,7 +243,13 @@ extern "C" int lbfs_mesh_build_uniform(double X, double Y, double Z, double dt, 
             fcen = add(fcen, cen);
             fnorm = add(fnorm, n);
         }
-        face_area[f] = area_f;
+        // Warped faces: the face's vector area is the sum of its triangles'
+        // vector areas, |N1 + N2| / 2 along (N1 + N2).  The reference's scalar
+        // sum |N1| / 2 + |N2| / 2 (kept for the area-weighted centroids) is
+        // longer whenever N1 and N2 are not parallel, so the vector areas of a
+        // cell's faces would not close and a fluid at rest would be pushed by
+        // its own pressure.
+        face_area[f] = jitter > 0 ? 0.5 * mag(fnorm) : area_f;
         csum_area[owner[f]] = csum_area[owner[f]] + area_f;
         cx[owner[f]] = cx[owner[f]] + fcen.x;
         cy[owner[f]] = cy[owner[f]] + fcen.y;
@@ -310,6 +368,8 @@ extern "C" int lbfs_mesh_build_uniform(double X, double Y, double Z, double dt, 
     }
     return LBFS_OK;
 }
+
+}  // namespace
 
 // Spring connectivity: the neighbour-ring construction, duplicate removal and
 // spring hashing of lagrangian_object::osay_mesh_read (lagrangian_object.cpp:

@@ -154,6 +154,10 @@ def lib():
                                                                   ctypes.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p,
                                                                   _f64p, _f64p, _f64p, _i32p, _f64p, _f64p, _i32p,
                                                                   _f64p],
+            "lbfs_mesh_build_jittered": [ctypes.c_double] * 4 + [_f64p, ctypes.c_double, ctypes.c_double,
+                                                                   ctypes.c_int32, ctypes.c_double, ctypes.c_uint64,
+                                                                   _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p,
+                                                                   _f64p, _i32p, _f64p, _f64p, _i32p, _f64p],
             "lbfs_rbc_build_springs": [ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int32, _i32p, _i32p],
             "lbfs_residual_rms_noalloc": [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, vp, vp],
             "lbfs_get_launch_shape": [vp, ctypes.POINTER(LaunchShape)],
@@ -204,4 +208,5 @@ EXPORTED = [
     "lbfs_last_error", "lbfs_mesh_uniform_counts", "lbfs_mesh_build_uniform", "lbfs_rbc_build_springs",
     "lbfs_residual_rms_noalloc", "lbfs_get_launch_shape", "lbfs_set_launch_shape", "lbfs_autotune",
     "lbfs_adjoint", "lbfs_checkpoint_size", "lbfs_checkpoint_save", "lbfs_checkpoint_load",
+    "lbfs_mesh_build_jittered",
 ]

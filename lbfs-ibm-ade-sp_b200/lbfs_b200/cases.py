@@ -177,3 +177,41 @@ def ensemble(n_instances=64, seed=2024, n_range=(16, 48), rbc_range=(1, 8), leve
     return Case("ensemble", mesh, params, membranes, cat("rho"), cat("u"), cat("v"), cat("w"), None,
                 {"members": members, "n_instances": n_instances, "cells": int(mesh.n_cells),
                  "membranes": len(membranes), "nodes": int(sum(m.n_nodes for m in membranes))})
+
+
+def jittered_channel(n=128, n_rbc=16, jitter=0.1, level=3, radius_cells=6.0, capillary=0.1, u_centre=0.01,
+                     seed=1313, tau=0.8, delta_t=0.5, precision=_abi.LBFS_FP64, ibm_stencil=_abi.LBFS_IBM_PESKIN4):
+    """Body-force-driven square duct on a jittered n^3 hex mesh (every interior
+    vertex moved by a seeded offset of up to `jitter` x spacing per axis;
+    general-normal fluxes) with up to n_rbc red cells of radius `radius_cells`,
+    randomly oriented at distinct points of a lattice of spacing 2 R + 2 cells,
+    at least R + 3 cells from the walls.  The shear modulus follows from
+    Ca = mu gamma R / G_s with gamma = 4 u_centre / (duct width), the wall shear
+    rate of the duct."""
+    dt = 1.0
+    visc = (tau - 0.5) / 3.0 * dt
+    L = 2.0 * n
+    mesh = build_uniform_mesh(L, L, L, dt, visc=visc, jitter=jitter, seed=seed)
+    bcs = {"left": (2, 2, 1.0, 0.0, 0.0, 0.0), "right": (2, 2, 1.0, 0.0, 0.0, 0.0),
+           "bottom": (2, 1, 1.0, 0.0, 0.0, 0.0), "top": (2, 1, 1.0, 0.0, 0.0, 0.0),
+           "back": (2, 1, 1.0, 0.0, 0.0, 0.0), "front": (2, 1, 1.0, 0.0, 0.0, 0.0)}
+    mesh.set_boundaries(bcs)
+    a = 0.5 * L
+    force = u_centre * visc / (0.2947 * a * a)
+    R = radius_cells * 2.0 * dt
+    gamma = 4.0 * u_centre / L
+    shear_modulus = visc * gamma * R / capillary
+    rng = np.random.default_rng(seed)
+    margin = R + 3 * 2.0 * dt
+    axis = np.arange(margin, L - margin + 1e-9, 2 * R + 2 * 2.0 * dt)
+    points = np.array([(x, y, z) for z in axis for y in axis for x in axis])
+    chosen = rng.permutation(len(points))[:n_rbc]
+    moduli = _rbc_moduli(shear_modulus, R)
+    cells = [red_cell(level, R, tuple(points[i]), rotation_matrix(rng), **moduli) for i in sorted(chosen)]
+    params = StepParams(visc=visc, delta_t=delta_t, channel_diameter=L, body_force=(force, 0.0, 0.0), ref_rho=1.0,
+                        max_velocity=u_centre, rho0=1.0, visc_factor_initial=1.0, testcase=5, precision=precision,
+                        ibm_stencil=ibm_stencil, viscosity_period=10000)
+    rho, u, v, w = _initial_state(mesh.n_cells, seed)
+    return Case("jittered_channel", mesh, params, cells, rho, u, v, w, bcs,
+                {"n": n, "jitter": jitter, "level": level, "radius_cells": radius_cells, "n_rbc": len(cells),
+                 "shear_modulus": shear_modulus, "force": force})

@@ -47,6 +47,7 @@ class UniformMesh:
     bc_rho_type: np.ndarray = field(default=None)
     bc_vel_type: np.ndarray = field(default=None)
     bc_values: np.ndarray = field(default=None)
+    axis_aligned: bool = True  # False for jittered meshes: every face takes the general-normal flux
 
     @property
     def shape(self):
@@ -81,7 +82,7 @@ class UniformMesh:
         d = _abi.MeshDesc()
         d.n_cells, d.n_faces, d.n_interior, d.n_bc = self.n_cells, self.n_faces, self.n_interior, self.n_bc
         d.n_face_x, d.n_face_y, d.n_face_z = self.n_face_x, self.n_face_y, self.n_face_z
-        d.axis_aligned = 1
+        d.axis_aligned = 1 if self.axis_aligned else 0
         d.owner, d.neighbour = _abi.iptr(self.owner), _abi.iptr(self.neighbour)
         d.face_area, d.face_normal = _abi.ptr(self.face_area), _abi.ptr(self.face_normal)
         d.face_centroid, d.streaming_dt = _abi.ptr(self.face_centroid), _abi.ptr(self.streaming_dt)
@@ -103,8 +104,11 @@ def uniform_counts(X, Y, Z, dt):
     return list(out)
 
 
-def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_min=0.0, gradient="LS"):
-    """Uniform mesh of ceil(X/(2 dt)) x ceil(Y/(2 dt)) x ceil(Z/(2 dt)) cells (mesh_type 6)."""
+def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_min=0.0, gradient="LS", jitter=0.0,
+                       seed=0):
+    """Uniform mesh of ceil(X/(2 dt)) x ceil(Y/(2 dt)) x ceil(Z/(2 dt)) cells (mesh_type 6); with
+    jitter > 0 every interior vertex moves by a seeded uniform offset of up to jitter x spacing per
+    axis and the mesh is stepped through the general-normal flux (mesh_type 3)."""
     nc, nf, ni, nb, nfx, nfy, nfz, nt = uniform_counts(X, Y, Z, dt)
     owner = np.zeros(nf, np.int32)
     neighbour = np.zeros(nf, np.int32)
@@ -120,9 +124,14 @@ def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_m
     patch = np.zeros(nb, np.int32)
     dh = ctypes.c_double()
     org = np.asarray(origin, np.float64)
-    _abi.check(_abi.lib().lbfs_mesh_build_uniform(
-        X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, 1 if gradient == "hybrid" else 0, _abi.iptr(owner),
-        _abi.iptr(neighbour), _abi.ptr(area), _abi.ptr(normal), _abi.ptr(fcen), _abi.ptr(sdt), _abi.ptr(vol),
-        _abi.ptr(ccen), _abi.iptr(stencil), _abi.ptr(lhs), _abi.ptr(rhs), _abi.iptr(patch), ctypes.byref(dh)))
+    outs = (_abi.iptr(owner), _abi.iptr(neighbour), _abi.ptr(area), _abi.ptr(normal), _abi.ptr(fcen), _abi.ptr(sdt),
+            _abi.ptr(vol), _abi.ptr(ccen), _abi.iptr(stencil), _abi.ptr(lhs), _abi.ptr(rhs), _abi.iptr(patch),
+            ctypes.byref(dh))
+    hybrid = 1 if gradient == "hybrid" else 0
+    if jitter > 0:
+        _abi.check(_abi.lib().lbfs_mesh_build_jittered(X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, hybrid,
+                                                       float(jitter), int(seed), *outs))
+    else:
+        _abi.check(_abi.lib().lbfs_mesh_build_uniform(X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, hybrid, *outs))
     return UniformMesh(X, Y, Z, dt, tuple(origin), nc, nf, ni, nb, nfx, nfy, nfz, owner, neighbour, area, normal,
-                       fcen, sdt, vol, ccen, stencil, lhs, rhs, patch, dh.value)
+                       fcen, sdt, vol, ccen, stencil, lhs, rhs, patch, dh.value, axis_aligned=not jitter > 0)
