@@ -338,12 +338,23 @@ __device__ __forceinline__ void general_face_bwd(const FluidArgs<double> &a, int
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             const double lL = lfl[kk] * d[m];
-            double *lp = side == 0 ? lpi : (side == 1 ? lpn : lp0);
-            double *lg = side == 0 ? lg1 : (side == 1 ? lg2 : lg3);
-            lp[m] += lL;
+            // branches instead of a selected pointer keep the arrays in registers
+            if (side == 0) {
+                lpi[m] += lL;
 #pragma unroll
-            for (int q = 0; q < 3; q++)
-                if (ee[q]) lg[3 * m + q] -= ee[q] * lL * dt;
+                for (int q = 0; q < 3; q++)
+                    if (ee[q]) lg1[3 * m + q] -= ee[q] * lL * dt;
+            } else if (side == 1) {
+                lpn[m] += lL;
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+                    if (ee[q]) lg2[3 * m + q] -= ee[q] * lL * dt;
+            } else {
+                lp0[m] += lL;
+#pragma unroll
+                for (int q = 0; q < 3; q++)
+                    if (ee[q]) lg3[3 * m + q] -= ee[q] * lL * dt;
+            }
         }
     }
 #pragma unroll
@@ -634,12 +645,28 @@ void launch_adj_velocity_seed(const FluidArgs<double> &a, const AdjointArgs &j, 
     k_adj_velocity_seed<<<(a.nc + 255) / 256, 256, 0, s>>>(a, j, weights);
 }
 
-int launch_adj_fluid(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
+void launch_adj_flux_axis(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
     if (a.axis_aligned && a.ni > 0) k_adj_flux_axis<<<(a.ni + 127) / 128, 128, 0, s>>>(a, j);
+}
+
+void launch_adj_flux_general(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
     const int first = a.axis_aligned ? a.ni : 0;
     if (a.nf > first) k_adj_flux_general<<<(a.nf - first + 127) / 128, 128, 0, s>>>(a, j, first);
+}
+
+void launch_adj_cells(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
     k_adj_cell<<<(a.nc + 127) / 128, 128, 0, s>>>(a, j);
+}
+
+void launch_adj_gather(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
     k_adj_gather<<<(a.nc + 127) / 128, 128, 0, s>>>(a, j);
+}
+
+int launch_adj_fluid(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
+    launch_adj_flux_axis(a, j, s);
+    launch_adj_flux_general(a, j, s);
+    launch_adj_cells(a, j, s);
+    launch_adj_gather(a, j, s);
     return 4;
 }
 

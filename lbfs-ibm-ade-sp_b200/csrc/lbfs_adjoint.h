@@ -48,5 +48,11 @@ int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, cons
 void launch_adj_prim(const FluidArgs<double> &a, cudaStream_t s);
 void launch_adj_velocity_seed(const FluidArgs<double> &a, const AdjointArgs &j, const double *weights, cudaStream_t s);
 int launch_adj_fluid(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
+// the phases of launch_adj_fluid: A1 on axis and on general faces (independent,
+// disjoint face records), A2 after both, A3 after A2 and the membrane part
+void launch_adj_flux_axis(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
+void launch_adj_flux_general(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
+void launch_adj_cells(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
+void launch_adj_gather(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
 
 }  // namespace lbfs

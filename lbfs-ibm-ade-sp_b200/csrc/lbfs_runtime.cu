@@ -1215,14 +1215,31 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     const int K = checkpoint_every, n_ck = (n_steps + K - 1) / K;
     const size_t xs = 3 * (size_t)N;  // positions of one step: x, y, z planes
     cudaStream_t st = s->stream;
-    DevBuf ck, seg, st0, fin_t1, fin_state, wts, ckx, segx, ckm, segm, finx, finm, segg, segh, segf, segs;
+    DevBuf ck, st0, fin_t1, fin_state, wts, ckx, ckm, finx, finm, bst;
+    // segment storage, two sets: the re-run of one segment fills one set while
+    // the backward sweep of the next later segment reads the other
+    struct SegStore {
+        DevBuf t1, g, h, x, f, s, m;
+    } segbuf[2];
+    const int n_sets = n_ck > 1 ? 2 : 1;
     LBFS_CUDA(cudaMalloc(&ck.p, sizeof(double4) * (size_t)nc * n_ck));
-    LBFS_CUDA(cudaMalloc(&seg.p, sizeof(double4) * (size_t)nc * K));
-    // per step of a segment: the gradients and ghost states of its K1
+    // per step of a segment: t1, the gradients and ghost states of its K1
     const size_t gsz = 12 * (size_t)nt;
-    LBFS_CUDA(cudaMalloc(&segg.p, sizeof(double) * gsz * K));
-    LBFS_CUDA(cudaMalloc(&segh.p, sizeof(Vec4<double>) * (size_t)(s->nb > 0 ? s->nb : 1) * K));
+    const size_t nbx = s->nb > 0 ? s->nb : 1;
+    for (int b = 0; b < n_sets; b++) {
+        SegStore &q = segbuf[b];
+        LBFS_CUDA(cudaMalloc(&q.t1.p, sizeof(double4) * (size_t)nc * K));
+        LBFS_CUDA(cudaMalloc(&q.g.p, sizeof(double) * gsz * K));
+        LBFS_CUDA(cudaMalloc(&q.h.p, sizeof(Vec4<double>) * nbx * K));
+        if (M > 0) {
+            LBFS_CUDA(cudaMalloc(&q.x.p, sizeof(double) * xs * (K + 1)));
+            LBFS_CUDA(cudaMalloc(&q.f.p, sizeof(double) * xs * K));
+            LBFS_CUDA(cudaMalloc(&q.s.p, sizeof(MembraneScalars) * M * K));
+            LBFS_CUDA(cudaMalloc(&q.m.p, sizeof(double) * M * K));
+        }
+    }
     LBFS_CUDA(cudaMalloc(&st0.p, sizeof(Vec4<double>) * (size_t)nt));
+    LBFS_CUDA(cudaMalloc(&bst.p, sizeof(Vec4<double>) * (size_t)nt));
     LBFS_CUDA(cudaMalloc(&fin_t1.p, sizeof(double4) * (size_t)nc));
     LBFS_CUDA(cudaMalloc(&fin_state.p, sizeof(Vec4<double>) * (size_t)nt));
     if (obj->kind == LBFS_OBJ_VELOCITY) {
@@ -1231,19 +1248,13 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     }
     if (M > 0) {
         LBFS_CUDA(cudaMalloc(&ckx.p, sizeof(double) * xs * n_ck));
-        LBFS_CUDA(cudaMalloc(&segx.p, sizeof(double) * xs * (K + 1)));
-        LBFS_CUDA(cudaMalloc(&segf.p, sizeof(double) * xs * K));
-        LBFS_CUDA(cudaMalloc(&segs.p, sizeof(MembraneScalars) * M * K));
         LBFS_CUDA(cudaMalloc(&ckm.p, sizeof(double) * M * n_ck));
-        LBFS_CUDA(cudaMalloc(&segm.p, sizeof(double) * M * K));
         LBFS_CUDA(cudaMalloc(&finx.p, sizeof(double) * xs));
         LBFS_CUDA(cudaMalloc(&finm.p, sizeof(double) * M));
     }
-    double4 *ck_t1 = (double4 *)ck.p, *seg_t1 = (double4 *)seg.p;
-    double *ck_x = (double *)ckx.p, *seg_x = (double *)segx.p, *ck_m = (double *)ckm.p, *seg_m = (double *)segm.p;
-    double *seg_g = (double *)segg.p, *seg_f = (double *)segf.p;
-    Vec4<double> *seg_h = (Vec4<double> *)segh.p;
-    MembraneScalars *seg_s = (MembraneScalars *)segs.p;
+    double4 *ck_t1 = (double4 *)ck.p;
+    double *ck_x = (double *)ckx.p, *ck_m = (double *)ckm.p;
+    Vec4<double> *bstate = (Vec4<double> *)bst.p;
     auto save_x = [&](double *dst) -> int {
         LBFS_CUDA(cudaMemcpyAsync(dst, ma.x, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
         LBFS_CUDA(cudaMemcpyAsync(dst + N, ma.y, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
@@ -1256,6 +1267,28 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
         LBFS_CUDA(cudaMemcpyAsync(ma.z, src + 2 * (size_t)N, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
         return LBFS_OK;
     };
+    // streams of the reverse sweep: fluid backward (sf), general faces (sg_),
+    // membrane backward (sm); the re-runs stay on the handle's stream
+    struct Streams {
+        cudaStream_t f = nullptr, g = nullptr, m = nullptr;
+        cudaEvent_t ev[8] = {};
+        ~Streams() {
+            for (cudaEvent_t e : ev)
+                if (e) cudaEventDestroy(e);
+            for (cudaStream_t x : {f, g, m})
+                if (x) cudaStreamDestroy(x);
+        }
+    } rs;
+    {
+        int prio_lo = 0, prio_hi = 0;
+        cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+        LBFS_CUDA(cudaStreamCreateWithPriority(&rs.f, cudaStreamNonBlocking, prio_hi));
+        LBFS_CUDA(cudaStreamCreateWithPriority(&rs.g, cudaStreamNonBlocking, prio_hi));
+        LBFS_CUDA(cudaStreamCreateWithPriority(&rs.m, cudaStreamNonBlocking, prio_hi));
+        for (cudaEvent_t &e : rs.ev) LBFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaEvent_t &ev_setup = rs.ev[0], &ev_gen = rs.ev[1], &ev_mem = rs.ev[2], &ev_start = rs.ev[3];
+    cudaEvent_t *ev_rerun = rs.ev + 4, *ev_back = rs.ev + 6;  // per segment set
     const long long t_start = s->t;
     cudaEvent_t e0, e1, e2;
     cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
@@ -1323,9 +1356,17 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     // ---- reverse sweep
     j.lam_u_ibm = M > 0 ? mj.lam_u_ibm : nullptr;
     mj.lam_t1 = j.lam_t1;
-    for (int sg = n_ck - 1; sg >= 0; sg--) {
+    // re-run segment sg from its checkpoint into segment set b, keeping each
+    // step's inputs (t1, x, MAD) and what its backward reads (gradients, ghost
+    // states, x', node forces, membrane scalars); on the handle's stream
+    auto rerun = [&](int sg, int b) -> int {
+        SegStore &q = segbuf[b];
+        double4 *seg_t1 = (double4 *)q.t1.p;
+        double *seg_g = (double *)q.g.p, *seg_x = (double *)q.x.p, *seg_f = (double *)q.f.p, *seg_m = (double *)q.m.p;
+        Vec4<double> *seg_h = (Vec4<double> *)q.h.p;
+        MembraneScalars *seg_s = (MembraneScalars *)q.s.p;
         const int n0 = sg * K, n1 = std::min(n_steps, n0 + K);
-        // re-run the segment from its checkpoint, keeping the inputs of every step
+        int rc;
         LBFS_CUDA(cudaMemcpyAsync(a.t1, ck_t1 + (size_t)sg * nc, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
         if (n0 == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
         else launch_adj_prim(a, st);
@@ -1333,8 +1374,6 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
             if ((rc = load_x(ck_x + (size_t)sg * xs))) return rc;
             launch_adjm_set_mad(ma, ck_m + (size_t)sg * M, st);
         }
-        // keeping each step's inputs (t1, x, MAD) and what its backward reads
-        // (gradients, ghost states, x', node forces, membrane scalars)
         for (int n = n0; n < n1; n++) {
             const size_t i = n - n0;
             LBFS_CUDA(cudaMemcpyAsync(seg_t1 + i * nc, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
@@ -1357,25 +1396,43 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
                 LBFS_CUDA(cudaMemcpyAsync(seg_s + i * M, ma.ms, sizeof(MembraneScalars) * M, cudaMemcpyDeviceToDevice, st));
             }
         }
+        return LBFS_OK;
+    };
+    // backward sweep of segment sg from segment set b.  The kernels read the
+    // stored intermediates in place (their own FluidArgs / MembraneArgs), so
+    // nothing of the handle's live buffers is touched and the next re-run
+    // overlaps it.  Per step: setup (state of step n) on sf; the membrane
+    // backward on sm and the general faces on sg_, beside the axis faces and
+    // A2 on sf; A3 (which updates lam_t1) after all of them.
+    auto backward = [&](int sg, int b) -> int {
+        SegStore &q = segbuf[b];
+        double4 *seg_t1 = (double4 *)q.t1.p;
+        double *seg_g = (double *)q.g.p, *seg_x = (double *)q.x.p, *seg_f = (double *)q.f.p, *seg_m = (double *)q.m.p;
+        Vec4<double> *seg_h = (Vec4<double> *)q.h.p;
+        MembraneScalars *seg_s = (MembraneScalars *)q.s.p;
+        const int n0 = sg * K, n1 = std::min(n_steps, n0 + K);
         for (int n = n1 - 1; n >= n0; n--) {
             const size_t i = n - n0;
-            // the state of step n: t1, primitive interior, its ghosts and gradients
-            LBFS_CUDA(cudaMemcpyAsync(a.t1, seg_t1 + i * nc, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
-            if (n == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nc, cudaMemcpyDeviceToDevice, st));
-            else launch_adj_prim(a, st);
+            FluidArgs<double> ab = a;
+            ab.t1 = seg_t1 + i * nc;
+            ab.grad = seg_g + i * gsz;
+            ab.state = bstate;
+            // the state of step n: primitive interior from t1 (the user's state at n = 0) and its ghosts
+            if (n == 0) LBFS_CUDA(cudaMemcpyAsync(bstate, st0.p, sizeof(Vec4<double>) * nc, cudaMemcpyDeviceToDevice, rs.f));
+            else launch_adj_prim(ab, rs.f);
             if (s->nb > 0)
-                LBFS_CUDA(cudaMemcpyAsync(a.state + nc, seg_h + i * s->nb, sizeof(Vec4<double>) * s->nb,
-                                          cudaMemcpyDeviceToDevice, st));
-            LBFS_CUDA(cudaMemcpyAsync(a.grad, seg_g + i * gsz, sizeof(double) * gsz, cudaMemcpyDeviceToDevice, st));
+                LBFS_CUDA(cudaMemcpyAsync(bstate + nc, seg_h + i * s->nb, sizeof(Vec4<double>) * s->nb,
+                                          cudaMemcpyDeviceToDevice, rs.f));
+            LBFS_CUDA(cudaEventRecord(ev_setup, rs.f));
             if (M > 0) {
-                // after the step's membrane chain: x', forces, totals, MAD_{n+1}
+                // after the step's membrane chain: x', forces, totals, MAD_{n+1}; x_n and MAD_n before it
+                MembraneArgs mbk = ma;
+                double *xp = seg_x + (i + 1) * xs, *fp = seg_f + i * xs;
+                mbk.x = xp; mbk.y = xp + N; mbk.z = xp + 2 * (size_t)N;
+                mbk.fx = fp; mbk.fy = fp + N; mbk.fz = fp + 2 * (size_t)N;
+                mbk.ms = seg_s + i * M;
+                mbk.state = bstate;
                 const double *xn = seg_x + i * xs;
-                if ((rc = load_x(seg_x + (i + 1) * xs))) return rc;
-                LBFS_CUDA(cudaMemcpyAsync(ma.fx, seg_f + i * xs, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
-                LBFS_CUDA(cudaMemcpyAsync(ma.fy, seg_f + i * xs + N, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
-                LBFS_CUDA(cudaMemcpyAsync(ma.fz, seg_f + i * xs + 2 * (size_t)N, sizeof(double) * N,
-                                          cudaMemcpyDeviceToDevice, st));
-                LBFS_CUDA(cudaMemcpyAsync(ma.ms, seg_s + i * M, sizeof(MembraneScalars) * M, cudaMemcpyDeviceToDevice, st));
                 mj.mad_n = seg_m + i * M;
                 mj.xn = xn;
                 mj.yn = xn + N;
@@ -1384,12 +1441,40 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
                 mj.mb.x = const_cast<double *>(mj.xn);
                 mj.mb.y = const_cast<double *>(mj.yn);
                 mj.mb.z = const_cast<double *>(mj.zn);
-                launch_adj_membrane(ma, mj, nc, a.cell_instance, (const InstanceGrid *)a.instances, st);
+                LBFS_CUDA(cudaStreamWaitEvent(rs.m, ev_setup, 0));
+                launch_adj_membrane(mbk, mj, nc, a.cell_instance, (const InstanceGrid *)a.instances, rs.m);
+                LBFS_CUDA(cudaEventRecord(ev_mem, rs.m));
             }
-            launch_adj_fluid(a, j, st);
+            LBFS_CUDA(cudaStreamWaitEvent(rs.g, ev_setup, 0));
+            launch_adj_flux_general(ab, j, rs.g);
+            LBFS_CUDA(cudaEventRecord(ev_gen, rs.g));
+            launch_adj_flux_axis(ab, j, rs.f);
+            LBFS_CUDA(cudaStreamWaitEvent(rs.f, ev_gen, 0));
+            launch_adj_cells(ab, j, rs.f);
+            if (M > 0) LBFS_CUDA(cudaStreamWaitEvent(rs.f, ev_mem, 0));
+            launch_adj_gather(ab, j, rs.f);
             LBFS_CUDA(cudaGetLastError());
         }
+        return LBFS_OK;
+    };
+    LBFS_CUDA(cudaEventRecord(ev_start, st));
+    LBFS_CUDA(cudaStreamWaitEvent(rs.f, ev_start, 0));
+    if ((rc = rerun(n_ck - 1, (n_ck - 1) % n_sets))) return rc;
+    LBFS_CUDA(cudaEventRecord(ev_rerun[(n_ck - 1) % n_sets], st));
+    for (int sg = n_ck - 1; sg >= 0; sg--) {
+        if (sg > 0) {
+            const int b = (sg - 1) % n_sets;
+            // set b was last read by the backward sweep of segment sg + 1
+            if (sg + 1 < n_ck) LBFS_CUDA(cudaStreamWaitEvent(st, ev_back[b], 0));
+            if ((rc = rerun(sg - 1, b))) return rc;
+            LBFS_CUDA(cudaEventRecord(ev_rerun[b], st));
+        }
+        const int b = sg % n_sets;
+        LBFS_CUDA(cudaStreamWaitEvent(rs.f, ev_rerun[b], 0));
+        if ((rc = backward(sg, b))) return rc;
+        LBFS_CUDA(cudaEventRecord(ev_back[b], rs.f));
     }
+    LBFS_CUDA(cudaStreamWaitEvent(st, ev_back[0], 0));
     cudaEventRecord(e2, st);
     // ---- final forward state back, sensitivities
     LBFS_CUDA(cudaMemcpyAsync(a.t1, fin_t1.p, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
