@@ -110,24 +110,51 @@ __device__ __forceinline__ void interface_flux_bwd(const double (&fl)[15], doubl
     }
 }
 
+// 12 consecutive doubles (16-B aligned) as six vector loads through the
+// read-only path (the array is not written while the kernel runs).
+__device__ __forceinline__ void load12(const double *p, double (&g)[12]) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+#pragma unroll
+    for (int t = 0; t < 6; t++) {
+        const double2 v = __ldg(q + t);
+        g[2 * t] = v.x;
+        g[2 * t + 1] = v.y;
+    }
+}
+__device__ __forceinline__ void load4(const double *p, double (&g)[4]) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    const double2 v0 = __ldg(q), v1 = __ldg(q + 1);
+    g[0] = v0.x; g[1] = v0.y; g[2] = v1.x; g[3] = v1.y;
+}
+
 // Face adjoint record: lambda of owner state (rho, u, v, w), neighbour state,
 // owner gradient (12), neighbour gradient (12).
 struct FaceAdj {
     double s1[4], s2[4], g1[12], g2[12];
 };
 
-// Axis-aligned interior face (axis_face_flux of the forward kernel).
+// One side of a face record: lambda of the side's state (4) and gradient (12).
+__device__ __forceinline__ void store_face_side(const AdjointArgs &j, int f, int side, const double (&ls)[4],
+                                                const double (&lg)[12]) {
+    double2 *o = reinterpret_cast<double2 *>(j.lam_face + 32 * (size_t)f);
+    double2 *os = o + (side == 0 ? 0 : 2), *og = o + (side == 0 ? 4 : 10);
+    os[0] = make_double2(ls[0], ls[1]);
+    os[1] = make_double2(ls[2], ls[3]);
+#pragma unroll
+    for (int t = 0; t < 6; t++) og[t] = make_double2(lg[2 * t], lg[2 * t + 1]);
+}
+
+// Axis-aligned interior face (axis_face_flux of the forward kernel): writes
+// the face's adjoint record.
 template <int axis>
-__device__ __forceinline__ void axis_face_bwd(const FluidArgs<double> &a, int f, const double (&lo)[4], FaceAdj &out) {
+__device__ __forceinline__ void axis_face_bwd(const FluidArgs<double> &a, const AdjointArgs &j, int f,
+                                              const double (&lo)[4]) {
     const int2 oc = __ldg(a.face_cells + f);
     const AxisFace<double> geo = a.axis_face[f];
     const Vec4<double> s1 = a.state[oc.x], s2 = a.state[oc.y];
     double g1[12], g2[12];
-#pragma unroll
-    for (int t = 0; t < 12; t++) {
-        g1[t] = a.grad[12 * (size_t)oc.x + t];
-        g2[t] = a.grad[12 * (size_t)oc.y + t];
-    }
+    load12(a.grad + 12 * (size_t)oc.x, g1);
+    load12(a.grad + 12 * (size_t)oc.y, g2);
     const double dt = geo.dt, t1 = geo.t1, t2 = geo.t2;
     const double c = t2 - t1;
     const double wa = fabs(t2 / c), wb = fabs(t1 / c);
@@ -183,50 +210,75 @@ __device__ __forceinline__ void axis_face_bwd(const FluidArgs<double> &a, int f,
 #pragma unroll
     for (int k = 0; k < 15; k++) lfl[k] = 0.0;
     interface_flux_bwd(fl, tau, geo.area, axis, 0, 0, 0, lo, lfl);
-    double lpi[4] = {0, 0, 0, 0}, lpn[4] = {0, 0, 0, 0}, lp0[4] = {0, 0, 0, 0};
+    // Reconstruction backward, one side at a time so that only one side's
+    // outputs are live: the centre directions (e_axis = 0, lattice value from
+    // p0 and the distance-weighted gradients) first, then the owner's
+    // directions (stored), then the neighbour's (stored).  The lattice values
+    // are recomputed here rather than kept from the forward pass (60 values):
+    // the empty asm statements hide that the inputs are unchanged.
 #pragma unroll
-    for (int t = 0; t < 12; t++) { out.g1[t] = 0.0; out.g2[t] = 0.0; }
-#pragma unroll
-    for (int k = 0; k < 15; k++) {
-        double L[4], d[4];
-        recon(k, L);
-        feq_grad(k, L[0], L[1], L[2], L[3], d);
-        const Dir3 e = dir3(k);
-        const int ee[3] = {e.ex, e.ey, e.ez};
-#pragma unroll
-        for (int m = 0; m < 4; m++) {
-            const double lL = lfl[k] * d[m];
-            if (ee[axis] > 0) {
-                lpi[m] += lL;
-                out.g1[3 * m + axis] -= lL * dt;
-                if (ee[ob]) out.g1[3 * m + ob] -= ee[ob] * lL * dt;
-                if (ee[oc2]) out.g1[3 * m + oc2] -= ee[oc2] * lL * dt;
-            } else if (ee[axis] < 0) {
-                lpn[m] += lL;
-                out.g2[3 * m + axis] += lL * dt;
-                if (ee[ob]) out.g2[3 * m + ob] -= ee[ob] * lL * dt;
-                if (ee[oc2]) out.g2[3 * m + oc2] -= ee[oc2] * lL * dt;
-            } else {
-                lp0[m] += lL;
-                if (ee[ob]) {
-                    out.g1[3 * m + ob] -= ee[ob] * lL * wa * dt;
-                    out.g2[3 * m + ob] -= ee[ob] * lL * wb * dt;
-                }
-                if (ee[oc2]) {
-                    out.g1[3 * m + oc2] -= ee[oc2] * lL * wa * dt;
-                    out.g2[3 * m + oc2] -= ee[oc2] * lL * wb * dt;
-                }
-            }
-        }
+    for (int t = 0; t < 12; t++) {
+        asm volatile("" : "+d"(g1[t]));
+        asm volatile("" : "+d"(g2[t]));
     }
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-        lpi[m] += 0.5 * lp0[m];
-        lpn[m] += 0.5 * lp0[m];
-        out.s1[m] = lpi[m];
-        out.g1[3 * m + axis] -= t1 * lpi[m];
-        out.s2[m] = lpn[m];
-        out.g2[3 * m + axis] -= t2 * lpn[m];
+        asm volatile("" : "+d"(pi[m]));
+        asm volatile("" : "+d"(pn[m]));
+        asm volatile("" : "+d"(p0[m]));
+    }
+    double lp0[4] = {0, 0, 0, 0}, lgc[12];  // lgc[3 m + c] = sum_k e_c lL_k[m] over the centre directions
+#pragma unroll
+    for (int t = 0; t < 12; t++) lgc[t] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 15; k++) {
+        const Dir3 e = dir3(k);
+        const int ee[3] = {e.ex, e.ey, e.ez};
+        if (ee[axis] != 0) continue;
+        double L[4], d[4];
+        recon(k, L);
+        feq_grad(k, L[0], L[1], L[2], L[3], d);
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const double lL = lfl[k] * d[m];
+            lp0[m] += lL;
+            if (ee[ob]) lgc[3 * m + ob] += ee[ob] * lL;
+            if (ee[oc2]) lgc[3 * m + oc2] += ee[oc2] * lL;
+        }
+    }
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+        const int sgn = side == 0 ? 1 : -1;  // the side's upwind directions have e_axis = sgn
+        const double wside = side == 0 ? wa : wb, tside = side == 0 ? t1 : t2;
+        double lp[4] = {0, 0, 0, 0}, lg[12];
+#pragma unroll
+        for (int t = 0; t < 12; t++) lg[t] = 0.0;
+#pragma unroll
+        for (int k = 1; k < 15; k++) {
+            const Dir3 e = dir3(k);
+            const int ee[3] = {e.ex, e.ey, e.ez};
+            if (ee[axis] != sgn) continue;
+            double L[4], d[4];
+            recon(k, L);
+            feq_grad(k, L[0], L[1], L[2], L[3], d);
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                const double lL = lfl[k] * d[m];
+                lp[m] += lL;
+                if (sgn > 0) lg[3 * m + axis] -= lL * dt;
+                else lg[3 * m + axis] += lL * dt;
+                if (ee[ob]) lg[3 * m + ob] -= ee[ob] * lL * dt;
+                if (ee[oc2]) lg[3 * m + oc2] -= ee[oc2] * lL * dt;
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            lp[m] += 0.5 * lp0[m];
+            lg[3 * m + ob] -= lgc[3 * m + ob] * wside * dt;
+            lg[3 * m + oc2] -= lgc[3 * m + oc2] * wside * dt;
+            lg[3 * m + axis] -= tside * lp[m];
+        }
+        store_face_side(j, f, side, lp, lg);
     }
 }
 
@@ -239,11 +291,8 @@ __device__ __forceinline__ void general_face_bwd(const FluidArgs<double> &a, int
     const GenFace<double> geo = a.gen_face[a.axis_aligned ? f - a.ni : f];
     const Vec4<double> s1 = a.state[oc.x], s2 = a.state[oc.y];
     double g1[12], g2[12];
-#pragma unroll
-    for (int t = 0; t < 12; t++) {
-        g1[t] = a.grad[12 * (size_t)oc.x + t];
-        g2[t] = a.grad[12 * (size_t)oc.y + t];
-    }
+    load12(a.grad + 12 * (size_t)oc.x, g1);
+    load12(a.grad + 12 * (size_t)oc.y, g2);
     const double dt = geo.dt;
     const double S1[4] = {s1.rho, s1.u, s1.v, s1.w}, S2[4] = {s2.rho, s2.u, s2.v, s2.w};
     const double t1v[3] = {geo.t1x, geo.t1y, geo.t1z}, t2v[3] = {geo.t2x, geo.t2y, geo.t2z};
@@ -416,23 +465,27 @@ __device__ __forceinline__ void face_flux_adjoint(const FluidArgs<double> &a, co
 }
 
 __device__ __forceinline__ void store_face(const AdjointArgs &j, int f, const FaceAdj &r) {
-    double *o = j.lam_face + 32 * (size_t)f;
+    double2 *o = reinterpret_cast<double2 *>(j.lam_face + 32 * (size_t)f);
 #pragma unroll
-    for (int m = 0; m < 4; m++) { o[m] = r.s1[m]; o[4 + m] = r.s2[m]; }
+    for (int m = 0; m < 2; m++) {
+        o[m] = make_double2(r.s1[2 * m], r.s1[2 * m + 1]);
+        o[2 + m] = make_double2(r.s2[2 * m], r.s2[2 * m + 1]);
+    }
 #pragma unroll
-    for (int t = 0; t < 12; t++) { o[8 + t] = r.g1[t]; o[20 + t] = r.g2[t]; }
+    for (int t = 0; t < 6; t++) {
+        o[4 + t] = make_double2(r.g1[2 * t], r.g1[2 * t + 1]);
+        o[10 + t] = make_double2(r.g2[2 * t], r.g2[2 * t + 1]);
+    }
 }
 
-__global__ void __launch_bounds__(128) k_adj_flux_axis(FluidArgs<double> a, AdjointArgs j) {
+__global__ void __launch_bounds__(128, 3) k_adj_flux_axis(FluidArgs<double> a, AdjointArgs j) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= a.ni) return;
     double lo[4];
     face_flux_adjoint(a, j, f, lo);
-    FaceAdj r;
-    if (f < a.nfx) axis_face_bwd<0>(a, f, lo, r);
-    else if (f < a.nfx + a.nfy) axis_face_bwd<1>(a, f, lo, r);
-    else axis_face_bwd<2>(a, f, lo, r);
-    store_face(j, f, r);
+    if (f < a.nfx) axis_face_bwd<0>(a, j, f, lo);
+    else if (f < a.nfx + a.nfy) axis_face_bwd<1>(a, j, f, lo);
+    else axis_face_bwd<2>(a, j, f, lo);
 }
 
 __global__ void __launch_bounds__(128) k_adj_flux_general(FluidArgs<double> a, AdjointArgs j, int first) {
@@ -456,7 +509,7 @@ __global__ void __launch_bounds__(128) k_adj_flux_general(FluidArgs<double> a, A
 // stencil differences and the ghost stencil entries.  The sensitivity to the
 // boundary-velocity scale sigma (every boundary velocity value times sigma)
 // is added to sigma_acc[cell].
-__global__ void __launch_bounds__(128) k_adj_cell(FluidArgs<double> a, AdjointArgs j) {
+__global__ void __launch_bounds__(128, 4) k_adj_cell(FluidArgs<double> a, AdjointArgs j) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nc) return;
     double ls[4] = {0, 0, 0, 0}, lg[12];
@@ -467,8 +520,9 @@ __global__ void __launch_bounds__(128) k_adj_cell(FluidArgs<double> a, AdjointAr
         const int e = a.cell_faces[6 * i + q];
         const int f = (e > 0 ? e : -e) - 1;
         const double *r = j.lam_face + 32 * (size_t)f;
-        const double *rs = e > 0 ? r : r + 4;
-        const double *rg = e > 0 ? r + 8 : r + 20;
+        double rs[4], rg[12];
+        load4(e > 0 ? r : r + 4, rs);
+        load12(e > 0 ? r + 8 : r + 20, rg);
 #pragma unroll
         for (int m = 0; m < 4; m++) ls[m] += rs[m];
 #pragma unroll
@@ -585,7 +639,8 @@ __global__ void __launch_bounds__(128) k_adj_gather(FluidArgs<double> a, Adjoint
         const int code = j.tst[e];
         const int i = code >> 3, q = code & 7;
         const double *r = a.ls[i].rhs + 3 * q;
-        const double *lr = j.lam_rs + 12 * (size_t)i;
+        double lr[12];
+        load12(j.lam_rs + 12 * (size_t)i, lr);
 #pragma unroll
         for (int m = 0; m < 4; m++) ls[m] += r[0] * lr[3 * m] + r[1] * lr[3 * m + 1] + r[2] * lr[3 * m + 2];
     }

@@ -42,6 +42,7 @@ struct MemAdjArgs {
 
 void launch_adjm_get_mad(const MembraneArgs &A, double *out, cudaStream_t s);
 void launch_adjm_set_mad(const MembraneArgs &A, const double *in, cudaStream_t s);
+void launch_adj_membrane_sort(const MemAdjArgs &J, cudaStream_t s);
 int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, const int *cell_instance,
                         const InstanceGrid *instances, cudaStream_t s);
 

@@ -470,8 +470,16 @@ void launch_adjm_set_mad(const MembraneArgs &A, const double *in, cudaStream_t s
     k_adjm_set_mad<<<(A.n_membranes + 127) / 128, 128, 0, s>>>(A, in);
 }
 
-// Membrane part of one backward step; the forward chain of the step has just
-// been recomputed (x = x', forces, totals and MAD_{n+1} in place).
+// The interpolation transpose's stencil tables and node sort at x_n
+// (J.mb.x): independent of the adjoints, so they may run ahead of the step's
+// other membrane kernels (which must follow them on the same stream).
+void launch_adj_membrane_sort(const MemAdjArgs &J, cudaStream_t s) {
+    launch_membrane_tables(J.mb, s);
+    launch_membrane_sort(J.mb, s);
+}
+
+// Membrane part of one backward step, after launch_adj_membrane_sort: A holds
+// the step's x', node forces, totals and MAD_{n+1}.
 int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, const int *cell_instance,
                         const InstanceGrid *instances, cudaStream_t s) {
     const int node_blocks = (A.total_nodes * 32 + 255) / 256;
@@ -479,13 +487,11 @@ int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, cons
     k_adjm_springs<<<dim3((A.total_springs + 127) / 128, kDirs), 128, 0, s>>>(A, J);
     k_adjm_reduce<<<A.n_membranes, 512, 0, s>>>(A, J);
     k_adjm_nodes<<<(A.total_nodes + 127) / 128, 128, 0, s>>>(A, J);
-    launch_membrane_tables(J.mb, s);
-    launch_membrane_sort(J.mb, s);
     if (A.state_is_float) k_adjm_advect<float><<<node_blocks, 256, 0, s>>>(A, J);
     else k_adjm_advect<double><<<node_blocks, 256, 0, s>>>(A, J);
     launch_membrane_spread(J.mb, s);
     k_adjm_cells<<<(nc + 255) / 256, 256, 0, s>>>(J, nc, cell_instance, instances);
-    return 9;
+    return 7;
 }
 
 }  // namespace lbfs

@@ -1411,6 +1411,7 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
         Vec4<double> *seg_h = (Vec4<double> *)q.h.p;
         MembraneScalars *seg_s = (MembraneScalars *)q.s.p;
         const int n0 = sg * K, n1 = std::min(n_steps, n0 + K);
+        if (M > 0) LBFS_CUDA(cudaStreamWaitEvent(rs.m, ev_rerun[b], 0));
         for (int n = n1 - 1; n >= n0; n--) {
             const size_t i = n - n0;
             FluidArgs<double> ab = a;
@@ -1437,10 +1438,12 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
                 mj.xn = xn;
                 mj.yn = xn + N;
                 mj.zn = xn + 2 * (size_t)N;
-                // the interpolation transpose sorts the nodes at x_n (read only)
+                // the interpolation transpose sorts the nodes at x_n (read
+                // only), ahead of the step's adjoints
                 mj.mb.x = const_cast<double *>(mj.xn);
                 mj.mb.y = const_cast<double *>(mj.yn);
                 mj.mb.z = const_cast<double *>(mj.zn);
+                launch_adj_membrane_sort(mj, rs.m);
                 LBFS_CUDA(cudaStreamWaitEvent(rs.m, ev_setup, 0));
                 launch_adj_membrane(mbk, mj, nc, a.cell_instance, (const InstanceGrid *)a.instances, rs.m);
                 LBFS_CUDA(cudaEventRecord(ev_mem, rs.m));
