@@ -117,7 +117,22 @@ typedef struct lbfs_params {
     int32_t precision;          /* LBFS_FP64 or LBFS_FP32_BULK                               */
     int32_t ibm_stencil;        /* LBFS_IBM_HAT2 or LBFS_IBM_PESKIN4                         */
     int32_t viscosity_period;   /* interior viscosity update when t % period == 1 (10000); 0 = never */
+    /* Time stepping (globals.gpu_time_stepping, global_variables.h:59).  0 or
+     * LBFS_DT_CONSTANT: delta_t is the step.  Otherwise every step starts with
+     * get_cfl_device (LBFS.cu:2868-2932): a per-cell step
+     * delta_t * volume / (CFL eigenvalue) and its minimum over the cells
+     * (min<128> + min_block, Solver_gpu.cu:767-787); LBFS_DT_LOCAL advances each
+     * cell with its own step, LBFS_DT_MIN and LBFS_DT_TALTS with the minimum
+     * (time_integration, LBFS.cu:2089-2172); node advection always uses the
+     * minimum. */
+    int32_t time_stepping;
+    double pre_conditioned_gamma; /* globals.pre_conditioned_gamma (get_cfl_device); 0 = 1 / gamma_inv */
 } lbfs_params;
+
+#define LBFS_DT_LOCAL 1
+#define LBFS_DT_CONSTANT 2
+#define LBFS_DT_MIN 3
+#define LBFS_DT_TALTS 4         /* as LBFS_DT_MIN: the GPU path advances talts with the minimum step */
 
 /* One spring-network membrane (lagrangian_object with type == 2). */
 typedef struct lbfs_rbc_desc {
@@ -173,6 +188,10 @@ int lbfs_set_nodes(lbfs_solver *s, const double *xyz);
 int lbfs_get_totals(lbfs_solver *s, double *out);
 /* RMS residuals of the last step, host [4]: rho, u, v, w (residuals::l2_norm_rms_moukallad). */
 int lbfs_get_residuals(lbfs_solver *s, double *out);
+/* The time step of the last step (the solver loop's delta_t): params.delta_t
+ * with constant time stepping, else the minimum of the per-cell steps
+ * (Solver_gpu.cu:776). */
+int lbfs_get_time_step(lbfs_solver *s, double *delta_t);
 
 /* Internal arrays for parity checking, copied to host.  Layouts:
  *  LBFS_FIELD_GRADIENTS  [12*(nc+nb)]  per cell: grad rho, grad u, grad v, grad w (x,y,z each)
@@ -183,7 +202,9 @@ int lbfs_get_residuals(lbfs_solver *s, double *out);
  *  LBFS_FIELD_VISC       [nc]          per cell: visc_factor
  *  LBFS_FIELD_GHOST      [4*nb]        per ghost: (u, v, w, rho)
  *  LBFS_FIELD_SPRING     [9*total_springs] contour length, spring constant, curvature,
- *                        curvature_0, angle_0, area_0[2], area[2]                     */
+ *                        curvature_0, angle_0, area_0[2], area[2]
+ *  LBFS_FIELD_DT_LOCAL   [nc]          per cell: delta_t_local of the last step (the constant step, the
+ *                        cell's own CFL step with local or talts, the minimum with min)     */
 int lbfs_get_field(lbfs_solver *s, int32_t which, double *out);
 #define LBFS_FIELD_GRADIENTS 0
 #define LBFS_FIELD_FACE_FLUX 1
@@ -193,6 +214,7 @@ int lbfs_get_field(lbfs_solver *s, int32_t which, double *out);
 #define LBFS_FIELD_VISC 5
 #define LBFS_FIELD_GHOST 6
 #define LBFS_FIELD_SPRING 7
+#define LBFS_FIELD_DT_LOCAL 8
 
 /* Keep the per-cell residuals of every step for lbfs_get_field(LBFS_FIELD_RESIDUAL).
  * Off by default: it adds 32 bytes of writes per cell per step. */

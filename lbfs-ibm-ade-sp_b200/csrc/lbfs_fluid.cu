@@ -2,6 +2,8 @@
 // the reference kernels they replace.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "lbfs_fluid.cuh"
 #include "lbfs_internal.h"
 #include "lbfs_kernels.h"
@@ -401,6 +403,53 @@ __global__ void __launch_bounds__(TB) k_face_flux_general(FluidArgs<R> a, int fi
     a.flux[f] = general_face_flux<R>(a, f, f >= a.ni);
 }
 
+// ----------------------------------------------------------------- CFL ----
+// get_cfl_device (LBFS.cu:2868-2932) per cell, then the minimum over the cells
+// (min<128> + min_block, common_kernels.hpp:147-170, Solver_gpu.cu:57-66):
+// block minima, the last block takes the minimum of the block minima.  A
+// minimum is exact, so the result does not depend on the grid.  The effective
+// speed of sound (a constant of the step) is formed on the host.  Products and
+// sums use explicitly rounded intrinsics so no multiply-add is contracted,
+// as in the reference's evaluation.
+template <typename R>
+__global__ void __launch_bounds__(256) k_cfl(FluidArgs<R> a) {
+    __shared__ double sh[8];
+    __shared__ bool last_block;
+    double mn = 100000000.0;  // min<128> pads its blocks with 1e8
+    const double ce = __dadd_rn(a.cfl_max_velocity, a.cfl_esos);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nc; i += gridDim.x * blockDim.x) {
+        const double4 c = a.cfl[i];  // area x, y, z, volume
+        const double rho = (double)a.state[i].rho + (double)a.rho0;
+        double eig = __dadd_rn(__dadd_rn(__dmul_rn(ce, c.x), __dmul_rn(ce, c.y)), __dmul_rn(ce, c.z));
+        eig = eig / a.cfl_gamma;
+        double ve = 2.0 * a.cfl_visc / a.cfl_gamma / rho / c.w;
+        ve = __dmul_rn(ve, __dadd_rn(__dadd_rn(__dmul_rn(c.x, c.x), __dmul_rn(c.y, c.y)), __dmul_rn(c.z, c.z)));
+        eig = __dadd_rn(eig, __dmul_rn(4.0, ve));
+        const double dt = __dmul_rn(a.cfl_factor, c.w) / eig;
+        a.dt_local[i] = dt;
+        mn = fmin(mn, dt);
+    }
+    for (int o = 16; o > 0; o >>= 1) mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sh[warp] = mn;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = sh[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) b = fmin(b, sh[w]);
+        a.dt_partials[blockIdx.x] = b;
+        __threadfence();
+        last_block = atomicAdd(a.dt_ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last_block && threadIdx.x == 0) {
+        __threadfence();
+        double b = 100000000.0;
+        for (int k = 0; k < (int)gridDim.x; k++) b = fmin(b, __ldcg(a.dt_partials + k));
+        *a.dt_min = b;
+        *a.dt_ticket = 0u;
+    }
+}
+
 // ------------------------------------------------------------------ K3 ----
 
 template <typename R, int TB>
@@ -409,6 +458,10 @@ __global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
     __shared__ bool last_block;
     double sq[4] = {0, 0, 0, 0};
     unsigned int flag = 0;
+    // the step: constant, or the minimum per-cell step, or each cell's own (LBFS_DT_LOCAL)
+    const bool local_dt = a.time_stepping == LBFS_DT_LOCAL;
+    const double dt_all = (a.time_stepping == LBFS_DT_MIN || a.time_stepping == LBFS_DT_TALTS) ? __ldcg(a.dt_min)
+                                                                                                 : a.delta_t;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nc; i += gridDim.x * blockDim.x) {
         const double iv = __ldg(a.cell_inv_volume + i);  // 1 / volume: products instead of 24 divisions
         double r[4] = {0, 0, 0, 0};  // rho, u, v, w
@@ -451,10 +504,11 @@ __global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
         r[2] = r[2] + fy;
         r[3] = r[3] + fz;
         double4 t = a.t1[i];
-        t.w = t.w + a.delta_t * r[0];
-        t.x = t.x + a.delta_t * r[1];
-        t.y = t.y + a.delta_t * r[2];
-        t.z = t.z + a.delta_t * r[3];
+        const double dt = local_dt ? a.dt_local[i] : dt_all;
+        t.w = t.w + dt * r[0];
+        t.x = t.x + dt * r[1];
+        t.y = t.y + dt * r[2];
+        t.z = t.z + dt * r[3];
         a.t1[i] = t;
         Vec4<R> s;
         s.rho = (R)(t.w - (double)a.rho0);
@@ -584,6 +638,11 @@ template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream
     else k_cell_update<R, 256><<<g, 256, 0, s>>>(a);
 }
 
+template <typename R> void launch_fluid_cfl(const FluidArgs<R> &a, cudaStream_t s) {
+    const int g = std::min(kCflBlocks, (a.nc + 255) / 256);
+    k_cfl<R><<<g, 256, 0, s>>>(a);
+}
+
 template <typename R> void launch_pack_state(const FluidArgs<R> &a, const double *stage, cudaStream_t s) {
     k_pack_state<R><<<(a.nc + 255) / 256, 256, 0, s>>>(a, stage);
 }
@@ -605,5 +664,7 @@ template void launch_fluid_update<double>(const FluidArgs<double> &, cudaStream_
 template void launch_fluid_gradients<float>(const FluidArgs<float> &, cudaStream_t);
 template void launch_fluid_flux<float>(const FluidArgs<float> &, cudaStream_t);
 template void launch_fluid_update<float>(const FluidArgs<float> &, cudaStream_t);
+template void launch_fluid_cfl<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_cfl<float>(const FluidArgs<float> &, cudaStream_t);
 
 }  // namespace lbfs

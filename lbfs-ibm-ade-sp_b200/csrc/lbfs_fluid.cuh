@@ -157,6 +157,16 @@ template <typename R> struct FluidArgs {
     unsigned int *flags;
     // launch shape (read by the host launchers only; lbfs_autotune picks it)
     int tb_grad, tb_flux, tb_gen, tb_update, update_blocks;
+    // time stepping other than constant (get_cfl_device, LBFS.cu:2868-2932)
+    int time_stepping;           // LBFS_DT_*; 0 or LBFS_DT_CONSTANT: delta_t
+    const double4 *cfl;          // [nc] (cfl area x, y, z, cell volume)
+    double *dt_local;            // [nc] per-cell step of the current step
+    double *dt_min;              // [1] minimum over the cells (the step's delta_t)
+    double *dt_partials;         // [kCflBlocks] block minima
+    unsigned int *dt_ticket;
+    double cfl_factor, cfl_esos, cfl_gamma, cfl_visc, cfl_max_velocity;
 };
+
+constexpr int kCflBlocks = 148 * 4;  // grid of the CFL kernel (grid-stride over the cells)
 
 }  // namespace lbfs

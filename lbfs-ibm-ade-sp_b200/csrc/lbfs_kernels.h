@@ -17,6 +17,8 @@ template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t
 template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_flux_general(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s);
+// per-cell step and its minimum (time stepping other than constant)
+template <typename R> void launch_fluid_cfl(const FluidArgs<R> &a, cudaStream_t s);
 // stage = 4 planes of n_cells doubles (rho, u, v, w); pack also resets soln_t1
 // to the primitive state (Solver_gpu.cu:746)
 template <typename R> void launch_pack_state(const FluidArgs<R> &a, const double *stage, cudaStream_t s);
@@ -45,6 +47,7 @@ struct MembraneArgs {
     int mode;
     int ibm_stencil;             // 2 or 4
     double delta_t;
+    const double *dt_dev;        // [1] the step's delta_t on the device (time stepping not constant), else null
     // fluid state (read) and IBM grid
     const void *state;           // Vec4<R>[nc]
     int state_is_float;

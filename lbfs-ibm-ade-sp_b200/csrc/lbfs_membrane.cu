@@ -382,7 +382,8 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
 #pragma unroll
     for (int c = 0; c < 3; c++)
         for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
-    const double xp = x + v[0] * A.delta_t, yp = y + v[1] * A.delta_t, zp = z + v[2] * A.delta_t;
+    const double dt = A.dt_dev ? __ldcg(A.dt_dev) : A.delta_t;
+    const double xp = x + v[0] * dt, yp = y + v[1] * dt, zp = z + v[2] * dt;
     if (lane == 0) {
         A.vx[n] = v[0];
         A.vy[n] = v[1];

@@ -109,6 +109,9 @@ struct lbfs_solver {
 
 namespace {
 
+// time stepping other than constant (lbfs_params.time_stepping 1, 3, 4)
+bool dynamic_dt(const lbfs_params &p) { return p.time_stepping != 0 && p.time_stepping != LBFS_DT_CONSTANT; }
+
 template <typename R> FluidArgs<R> &fluid(lbfs_solver *s);
 template <> FluidArgs<double> &fluid<double>(lbfs_solver *s) { return s->f64; }
 template <> FluidArgs<float> &fluid<float>(lbfs_solver *s) { return s->f32; }
@@ -290,6 +293,60 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     a.n_membranes = 0;
     a.instances = nullptr;
     a.cell_instance = nullptr;
+    return LBFS_OK;
+}
+
+// Time stepping other than constant: the per-cell CFL areas (populate_cfl_areas,
+// Solver_gpu.cu:1657-1687: half the sums of |n_c| * area over the cell's faces,
+// in the order of gradient_faces, i.e. the face loop of
+// unstructured_mesh.cpp:1645-1665) with the cell volume, the per-cell steps,
+// their minimum, and the constants of get_cfl_device.
+template <typename R> int setup_time_stepping(lbfs_solver *s, const lbfs_mesh_desc *m) {
+    FluidArgs<R> &a = fluid<R>(s);
+    const lbfs_params &p = s->params;
+    a.time_stepping = p.time_stepping;
+    a.cfl = nullptr; a.dt_local = nullptr; a.dt_min = nullptr; a.dt_partials = nullptr; a.dt_ticket = nullptr;
+    s->ma.dt_dev = nullptr;
+    if (!dynamic_dt(p)) return LBFS_OK;
+    const int nc = m->n_cells;
+    std::vector<double4> cfl(nc, make_double4(0, 0, 0, 0));
+    for (int f = 0; f < m->n_faces; f++) {
+        const double *n = m->face_normal + 3 * (size_t)f;
+        const double ar = m->face_area[f];
+        const int cells[2] = {m->owner[f], f < m->n_interior ? m->neighbour[f] : -1};
+        for (int c : cells) {
+            if (c < 0 || c >= nc) continue;
+            cfl[c].x = cfl[c].x + std::fabs(n[0] * ar);
+            cfl[c].y = cfl[c].y + std::fabs(n[1] * ar);
+            cfl[c].z = cfl[c].z + std::fabs(n[2] * ar);
+        }
+    }
+    for (int i = 0; i < nc; i++) {
+        cfl[i].x = cfl[i].x / 2;
+        cfl[i].y = cfl[i].y / 2;
+        cfl[i].z = cfl[i].z / 2;
+        cfl[i].w = m->cell_volume[i];
+    }
+    double4 *d_cfl;
+    double *d_dtl, *d_min, *d_part;
+    unsigned int *d_ticket;
+    int rc;
+    if ((rc = s->upload(&d_cfl, cfl)) || (rc = s->alloc(&d_dtl, nc)) || (rc = s->alloc(&d_min, 1)) ||
+        (rc = s->alloc(&d_part, kCflBlocks)) || (rc = s->alloc(&d_ticket, 1)))
+        return rc;
+    LBFS_CUDA(cudaMemset(d_ticket, 0, sizeof(unsigned int)));
+    LBFS_CUDA(cudaMemcpy(d_min, &p.delta_t, sizeof(double), cudaMemcpyHostToDevice));
+    LBFS_CUDA(cudaMemset(d_dtl, 0, sizeof(double) * nc));
+    a.cfl = d_cfl; a.dt_local = d_dtl; a.dt_min = d_min; a.dt_partials = d_part; a.dt_ticket = d_ticket;
+    const double g = p.pre_conditioned_gamma > 0 ? p.pre_conditioned_gamma : 1.0 / p.gamma_inv;
+    const double mv = p.max_velocity;
+    // effective speed of sound of get_cfl_device (LBFS.cu:2888-2889), a constant of the run
+    a.cfl_esos = mv * std::sqrt(1 - g + std::pow(g / std::sqrt(3.0) / mv, 2));
+    a.cfl_gamma = g;
+    a.cfl_visc = p.visc;
+    a.cfl_max_velocity = mv;
+    a.cfl_factor = p.delta_t;  // globals.time_marching_step
+    s->ma.dt_dev = d_min;      // node advection moves by the minimum step (Solver_gpu.cu:827)
     return LBFS_OK;
 }
 
@@ -540,6 +597,11 @@ template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *la
     int n = 0;
     for (int p = 0; p < kPhases; p++) s->phase_recorded[p] = false;
     if (s->profiling) LBFS_CUDA(record_event(s->ev_phase[5][0], s->stream));
+    if (a.time_stepping != 0 && a.time_stepping != LBFS_DT_CONSTANT) {
+        // the step's time step from the state at its start (Solver_gpu.cu:767-787)
+        launch_fluid_cfl<R>(a, s->stream);
+        n += 1;
+    }
     if (s->n_membranes > 0) {
         if (visc_update) {
             { PhaseMark m(s, 0, s->stream); n += launch_membrane(s->ma, s->stream); }
@@ -611,6 +673,16 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if (params->ibm_stencil != LBFS_IBM_HAT2 && params->ibm_stencil != LBFS_IBM_PESKIN4)
         return set_error(LBFS_ERR_ARG, "ibm_stencil must be 2 or 4");
     if (!(params->delta_t > 0)) return set_error(LBFS_ERR_ARG, "delta_t must be positive");
+    if (params->time_stepping < 0 || params->time_stepping > LBFS_DT_TALTS)
+        return set_error(LBFS_ERR_ARG, "time_stepping must be 0 or LBFS_DT_LOCAL/CONSTANT/MIN/TALTS");
+    if (dynamic_dt(*params)) {
+        if (mesh->n_instances > 1)
+            return set_error(LBFS_ERR_UNSUPPORTED, "time stepping other than constant couples the instances of an "
+                                                   "ensemble through the minimum step; use constant time stepping");
+        const double g = params->pre_conditioned_gamma > 0 ? params->pre_conditioned_gamma : 1.0 / params->gamma_inv;
+        if (!(g > 0) || !(params->max_velocity > 0))
+            return set_error(LBFS_ERR_ARG, "time stepping other than constant needs gamma > 0 and max_velocity > 0");
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return set_error(LBFS_ERR_CUDA, "no CUDA device: this library has no CPU path");
@@ -640,8 +712,10 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if ((rc = s->upload(&s->d_centroid, centroid))) return fail(rc);
     rc = setup_membranes(s, mesh, rbc, n_rbc);
     if (rc) return fail(rc);
-    // gradients, face flux (axis + general), update; membrane kernels
-    s->launches_per_step = 4 + (n_rbc > 0 ? 6 : 0);
+    rc = s->fp32 ? setup_time_stepping<float>(s, mesh) : setup_time_stepping<double>(s, mesh);
+    if (rc) return fail(rc);
+    // gradients, face flux (axis + general), update; membrane kernels; CFL
+    s->launches_per_step = 4 + (n_rbc > 0 ? 6 : 0) + (dynamic_dt(s->params) ? 1 : 0);
     *out = s;
     return LBFS_OK;
 }
@@ -863,6 +937,17 @@ template <typename R> int get_field_t(lbfs_solver *s, int which, double *out) {
         return copy_real<double>(s, s->d_res_out, 4 * (size_t)s->nc, out);
     case LBFS_FIELD_T1: return copy_real<double>(s, (const double *)a.t1, 4 * (size_t)s->nc, out);
     case LBFS_FIELD_VISC: return copy_real<R>(s, a.visc_factor, (size_t)s->nc, out);
+    case LBFS_FIELD_DT_LOCAL: {
+        // delta_t_local as the reference leaves it: the constant step
+        // (fill_double), each cell's own step (local, talts), or the minimum
+        // (min; Solver_gpu.cu:781-787)
+        if (a.time_stepping == LBFS_DT_LOCAL || a.time_stepping == LBFS_DT_TALTS)
+            return copy_real<double>(s, a.dt_local, (size_t)s->nc, out);
+        double dt = s->params.delta_t;
+        if (a.dt_min) LBFS_CUDA(cudaMemcpy(&dt, a.dt_min, sizeof(double), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < s->nc; i++) out[i] = dt;
+        return LBFS_OK;
+    }
     case LBFS_FIELD_GHOST: {
         std::vector<double> tmp(4 * nt);
         int rc = copy_real<R>(s, (const R *)a.state, 4 * nt, tmp.data());
@@ -926,6 +1011,17 @@ extern "C" int lbfs_get_field(lbfs_solver *s, int32_t which, double *out) {
     LBFS_CUDA(cudaSetDevice(s->device));
     LBFS_CUDA(cudaStreamSynchronize(s->stream));
     return s->fp32 ? get_field_t<float>(s, which, out) : get_field_t<double>(s, which, out);
+}
+
+extern "C" int lbfs_get_time_step(lbfs_solver *s, double *delta_t) {
+    if (!s || !delta_t) return set_error(LBFS_ERR_ARG, "null argument");
+    const double *d = s->fp32 ? s->f32.dt_min : s->f64.dt_min;
+    *delta_t = s->params.delta_t;
+    if (!d) return LBFS_OK;
+    LBFS_CUDA(cudaSetDevice(s->device));
+    LBFS_CUDA(cudaMemcpyAsync(delta_t, d, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    return LBFS_OK;
 }
 
 extern "C" int lbfs_keep_residuals(lbfs_solver *s, int32_t on) {
@@ -1180,6 +1276,8 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
         return set_error(LBFS_ERR_ARG, "lbfs_adjoint: bad arguments");
     if (s->fp32) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: FP64 handles only");
     if (s->params.gamma_inv != 1.0) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: no preconditioning");
+    if (dynamic_dt(s->params))
+        return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: constant time stepping only");
     if (obj->kind == LBFS_OBJ_VELOCITY) {
         if (!obj->cell_weights) return set_error(LBFS_ERR_ARG, "lbfs_adjoint: velocity objective needs weights");
     } else if (obj->kind == LBFS_OBJ_TAYLOR) {

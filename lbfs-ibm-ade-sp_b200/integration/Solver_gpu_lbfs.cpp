@@ -41,8 +41,8 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
                                              domain_geometry &domain, initial_conditions &init_conds,
                                              unstructured_bcs &quad_bcs_orig, int mg, Solution &residual, int fmg,
                                              post_processing &pp, std::vector<lagrangian_object> &object_vec) {
-    if (globals.gpu_time_stepping != 2 || globals.preconditioning_active) {
-        std::fprintf(stderr, "lbfs_b200: time_stepping must be \"constant\" and preconditioning off\n");
+    if (globals.preconditioning_active) {
+        std::fprintf(stderr, "lbfs_b200: preconditioning must be off\n");
         std::exit(-1);
     }
     const int nc = Mesh.get_n_cells(), nf = Mesh.get_n_faces(), ni = Mesh.get_n_neighbours();
@@ -113,6 +113,9 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
     p.precision = LBFS_FP64;
     p.ibm_stencil = LBFS_IBM_HAT2;
     p.viscosity_period = 10000;
+    // local = 1, constant = 2, min = 3, talts = 4 (global_variables.h:59)
+    p.time_stepping = globals.gpu_time_stepping;
+    p.pre_conditioned_gamma = globals.pre_conditioned_gamma;
 
     // membranes (Solver_gpu.cu:659-735): sprIdx / sorted_triIdx / stress-free
     // coordinates, then the initial mesh read over the node arrays

@@ -41,6 +41,12 @@ LBFS_FIELD_T1 = 4
 LBFS_FIELD_VISC = 5
 LBFS_FIELD_GHOST = 6
 LBFS_FIELD_SPRING = 7
+LBFS_FIELD_DT_LOCAL = 8
+
+LBFS_DT_LOCAL = 1
+LBFS_DT_CONSTANT = 2
+LBFS_DT_MIN = 3
+LBFS_DT_TALTS = 4
 
 LBFS_NOALLOC_MAX_BLOCKS = 65536
 LBFS_NOALLOC_MAX_CELLS = LBFS_NOALLOC_MAX_BLOCKS * 256
@@ -80,6 +86,7 @@ class Params(ctypes.Structure):
         ("visc_factor_initial", ctypes.c_double),
         ("testcase", ctypes.c_int32), ("precision", ctypes.c_int32), ("ibm_stencil", ctypes.c_int32),
         ("viscosity_period", ctypes.c_int32),
+        ("time_stepping", ctypes.c_int32), ("pre_conditioned_gamma", ctypes.c_double),
     ]
 
 
@@ -142,6 +149,7 @@ def lib():
             "lbfs_set_nodes": [vp, _f64p],
             "lbfs_get_totals": [vp, _f64p],
             "lbfs_get_residuals": [vp, _f64p],
+            "lbfs_get_time_step": [vp, ctypes.POINTER(ctypes.c_double)],
             "lbfs_get_field": [vp, ctypes.c_int32, _f64p],
             "lbfs_keep_residuals": [vp, ctypes.c_int32],
             "lbfs_status": [vp, ctypes.POINTER(ctypes.c_uint32)],
@@ -203,7 +211,7 @@ def iptr(a):
 EXPORTED = [
     "lbfs_create", "lbfs_destroy", "lbfs_set_state", "lbfs_get_state", "lbfs_step", "lbfs_step_graph",
     "lbfs_synchronize", "lbfs_set_stream", "lbfs_get_nodes", "lbfs_set_nodes", "lbfs_get_totals",
-    "lbfs_get_residuals", "lbfs_get_field", "lbfs_keep_residuals", "lbfs_status", "lbfs_launches_per_step",
+    "lbfs_get_residuals", "lbfs_get_time_step", "lbfs_get_field", "lbfs_keep_residuals", "lbfs_status", "lbfs_launches_per_step",
     "lbfs_set_profiling", "lbfs_get_phase_times",
     "lbfs_last_error", "lbfs_mesh_uniform_counts", "lbfs_mesh_build_uniform", "lbfs_rbc_build_springs",
     "lbfs_residual_rms_noalloc", "lbfs_get_launch_shape", "lbfs_set_launch_shape", "lbfs_autotune",

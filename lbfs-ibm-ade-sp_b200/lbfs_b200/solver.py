@@ -31,6 +31,8 @@ class StepParams:
     precision: int = _abi.LBFS_FP64
     ibm_stencil: int = _abi.LBFS_IBM_HAT2
     viscosity_period: int = 10000
+    time_stepping: int = _abi.LBFS_DT_CONSTANT
+    pre_conditioned_gamma: float = 0.0  # 0: 1 / gamma_inv
 
     def to_c(self):
         p = _abi.Params()
@@ -41,6 +43,7 @@ class StepParams:
         p.visc_factor_initial = self.visc_factor_initial
         p.testcase, p.precision, p.ibm_stencil = self.testcase, self.precision, self.ibm_stencil
         p.viscosity_period = self.viscosity_period
+        p.time_stepping, p.pre_conditioned_gamma = self.time_stepping, self.pre_conditioned_gamma
         return p
 
 
@@ -139,11 +142,17 @@ class GpuSolver:
             _abi.LBFS_FIELD_GRADIENTS: 12 * nt, _abi.LBFS_FIELD_FACE_FLUX: 4 * m.n_faces,
             _abi.LBFS_FIELD_RESIDUAL: 4 * m.n_cells, _abi.LBFS_FIELD_FORCE: 3 * m.n_cells,
             _abi.LBFS_FIELD_T1: 4 * m.n_cells, _abi.LBFS_FIELD_VISC: m.n_cells, _abi.LBFS_FIELD_GHOST: 4 * m.n_bc,
-            _abi.LBFS_FIELD_SPRING: 9 * self.total_springs,
+            _abi.LBFS_FIELD_SPRING: 9 * self.total_springs, _abi.LBFS_FIELD_DT_LOCAL: m.n_cells,
         }[which]
         out = np.zeros(max(size, 1))
         _abi.check(_abi.lib().lbfs_get_field(self._h, which, _abi.ptr(out)))
         return out[:size]
+
+    def time_step(self):
+        """The delta_t of the last step (the minimum per-cell step unless constant)."""
+        dt = ctypes.c_double()
+        _abi.check(_abi.lib().lbfs_get_time_step(self._h, ctypes.byref(dt)))
+        return dt.value
 
     def status(self):
         f = ctypes.c_uint32()

@@ -44,6 +44,8 @@ typedef struct oracle_case {
     double *area, *normal, *fcen, *sdt, *vol, *cen, *lhs, *rhs, *bcv;
     /* state: (u, v, w, rho) per cell incl. ghosts, soln_t1 per cell */
     double *soln, *t1, *grad, *flux, *res, *force, *visc;
+    double *cfl, *dtl; /* cfl areas (x, y, z per cell), per-cell step */
+    double dt;         /* the step's delta_t */
     double resid[4];
     long long t;
     /* membranes */
@@ -314,9 +316,9 @@ static void interpolate_and_move(oracle_case *o) {
                     }
                 }
         o->vx[n] = v[0]; o->vy[n] = v[1]; o->vz[n] = v[2];
-        o->x[n] += v[0] * o->p.delta_t;
-        o->y[n] += v[1] * o->p.delta_t;
-        o->z[n] += v[2] * o->p.delta_t;
+        o->x[n] += v[0] * o->dt;
+        o->y[n] += v[1] * o->dt;
+        o->z[n] += v[2] * o->dt;
     }
 }
 
@@ -564,6 +566,49 @@ static void interior_viscosity(oracle_case *o) {
     }
 }
 
+/* -------------------------------------------------------- time step ---- */
+
+static int dynamic_dt(const oracle_case *o) { return o->p.time_stepping != 0 && o->p.time_stepping != LBFS_DT_CONSTANT; }
+
+/* populate_cfl_areas (Solver_gpu.cu:1657-1687): per cell, half the sums of
+ * |n_c * area| over its faces in gradient_faces order (the face loop,
+ * unstructured_mesh.cpp:1645-1665). */
+static void cfl_areas(oracle_case *o) {
+    for (int f = 0; f < o->nf; f++) {
+        const int cells[2] = {o->owner[f], f < o->ni ? o->neighbour[f] : -1};
+        for (int k = 0; k < 2; k++) {
+            const int c = cells[k];
+            if (c < 0 || c >= o->nc) continue;
+            for (int d = 0; d < 3; d++) o->cfl[3 * c + d] = o->cfl[3 * c + d] + fabs(o->normal[3 * f + d] * o->area[f]);
+        }
+    }
+    for (int i = 0; i < 3 * o->nc; i++) o->cfl[i] = o->cfl[i] / 2;
+}
+
+/* get_cfl_device (LBFS.cu:2868-2932) per cell, then min<128> + min_block
+ * (common_kernels.hpp:147-170, Solver_gpu.cu:57-66, 767-787): the minimum of
+ * the per-cell steps and of min<128>'s padding value 1e8. */
+static void time_step(oracle_case *o) {
+    if (!dynamic_dt(o)) { o->dt = o->p.delta_t; return; }
+    const double g = o->p.pre_conditioned_gamma > 0 ? o->p.pre_conditioned_gamma : 1.0 / o->p.gamma_inv;
+    const double mv = o->p.max_velocity, factor = o->p.delta_t;
+    const double esos = mv * sqrt(1 - g + pow(g / sqrt(3.0) / mv, 2));
+    double mn = 100000000.0;
+    for (int i = 0; i < o->nc; i++) {
+        const double *a = o->cfl + 3 * i;
+        double eig = (mv + esos) * a[0] + (mv + esos) * a[1] + (mv + esos) * a[2];
+        eig = eig / g;
+        double ve = 2 * o->p.visc / g / o->soln[4 * i + 3] / o->vol[i];
+        ve = ve * (a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        eig = eig + 4 * ve;
+        o->dtl[i] = factor * o->vol[i] / eig;
+        mn = fmin(o->dtl[i], mn);
+    }
+    o->dt = mn;
+    if (o->p.time_stepping == LBFS_DT_MIN)
+        for (int i = 0; i < o->nc; i++) o->dtl[i] = mn; /* fill_double (Solver_gpu.cu:781-783) */
+}
+
 /* ------------------------------------------------------------- API ---- */
 
 oracle_case *oracle_create(const lbfs_mesh_desc *m, const lbfs_params *p, const lbfs_rbc_desc *rbc, int n_rbc) {
@@ -595,6 +640,11 @@ oracle_case *oracle_create(const lbfs_mesh_desc *m, const lbfs_params *p, const 
     o->force = dup(NULL, 3 * nc * sizeof(double));
     o->visc = (double *)malloc(nc * sizeof(double));
     for (size_t i = 0; i < nc; i++) o->visc[i] = p->visc_factor_initial;
+    o->cfl = dup(NULL, 3 * nc * sizeof(double));
+    o->dtl = (double *)malloc(nc * sizeof(double));
+    for (size_t i = 0; i < nc; i++) o->dtl[i] = p->delta_t;
+    o->dt = p->delta_t;
+    cfl_areas(o);
     o->n_mem = n_rbc;
     o->mem = (omem *)calloc(n_rbc > 0 ? n_rbc : 1, sizeof(omem));
     for (int r = 0; r < n_rbc; r++) {
@@ -644,7 +694,7 @@ void oracle_free(oracle_case *o) {
     void *ptrs[] = {o->owner, o->neighbour, o->stencil, o->rt, o->vt, o->area, o->normal, o->fcen, o->sdt, o->vol,
                     o->cen, o->lhs, o->rhs, o->bcv, o->soln, o->t1, o->grad, o->flux, o->res, o->force, o->visc, o->mem,
                     o->tri, o->spr, o->x, o->y, o->z, o->vx, o->vy, o->vz, o->fx, o->fy, o->fz, o->contour, o->kspr,
-                    o->curv, o->curv0, o->ang0, o->area0, o->sarea};
+                    o->curv, o->curv0, o->ang0, o->area0, o->sarea, o->cfl, o->dtl};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(o);
 }
@@ -664,10 +714,11 @@ void oracle_get_state(const oracle_case *o, double *rho, double *u, double *v, d
     }
 }
 
-/* One iteration of the time loop, Solver_gpu.cu:749-1046 (time_stepping constant, one RK stage). */
+/* One iteration of the time loop, Solver_gpu.cu:749-1046 (one RK stage). */
 void oracle_step(oracle_case *o, int n_steps) {
-    const double dtm = o->p.delta_t;
     for (int st = 0; st < n_steps; st++, o->t++) {
+        time_step(o);
+        const int local = o->p.time_stepping == LBFS_DT_LOCAL;
         if (o->n_mem > 0) interpolate_and_move(o);
         for (int i = 0; i < o->nc; i++)
             for (int c = 0; c < 3; c++) o->force[3 * i + c] = o->p.body_force[c];
@@ -709,6 +760,7 @@ void oracle_step(oracle_case *o, int n_steps) {
             double *r = o->res + 4 * i, *t1 = o->t1 + 4 * i, *s = o->soln + 4 * i;
             for (int c = 0; c < 3; c++) r[1 + c] = r[1 + c] + o->force[3 * i + c];
             /* time_integration, last (only) stage (LBFS.cu:2089-2172) */
+            const double dtm = local ? o->dtl[i] : o->dt;
             t1[3] = t1[3] + dtm * 1.0 * r[0];
             t1[0] = t1[0] + dtm * 1.0 * r[1];
             t1[1] = t1[1] + dtm * 1.0 * r[2];
@@ -733,6 +785,7 @@ int oracle_get_field(const oracle_case *o, int which, double *out) {
     case LBFS_FIELD_FORCE: memcpy(out, o->force, 3 * (size_t)o->nc * sizeof(double)); return 0;
     case LBFS_FIELD_T1: memcpy(out, o->t1, 4 * (size_t)o->nc * sizeof(double)); return 0;
     case LBFS_FIELD_VISC: memcpy(out, o->visc, (size_t)o->nc * sizeof(double)); return 0;
+    case LBFS_FIELD_DT_LOCAL: memcpy(out, o->dtl, (size_t)o->nc * sizeof(double)); return 0;
     case LBFS_FIELD_GHOST: memcpy(out, o->soln + 4 * (size_t)o->nc, 4 * (size_t)o->nb * sizeof(double)); return 0;
     case LBFS_FIELD_SPRING:
         for (int s = 0; s < o->S; s++) {
@@ -763,3 +816,5 @@ void oracle_get_totals(const oracle_case *o, double *out) {
 }
 
 void oracle_get_residuals(const oracle_case *o, double *out) { memcpy(out, o->resid, 4 * sizeof(double)); }
+
+double oracle_time_step(const oracle_case *o) { return o->dt; }

@@ -24,8 +24,8 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        src = os.path.join(HERE, "lbfs_oracle.c")
-        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        srcs = [os.path.join(HERE, "lbfs_oracle.c"), os.path.join(HERE, "..", "include", "lbfs_b200.h")]
+        if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < max(os.path.getmtime(f) for f in srcs):
             build()
         L = ctypes.CDLL(LIB_PATH)
         vp = ctypes.c_void_p
@@ -39,6 +39,8 @@ def lib():
         L.oracle_get_nodes.argtypes = [vp, ctypes.c_int, vp]
         L.oracle_get_totals.argtypes = [vp, vp]
         L.oracle_get_residuals.argtypes = [vp, vp]
+        L.oracle_time_step.argtypes = [vp]
+        L.oracle_time_step.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -115,7 +117,10 @@ class OracleSolver:
         m = self.mesh
         nt = m.n_cells + m.n_bc
         size = {0: 12 * nt, 1: 4 * m.n_faces, 2: 4 * m.n_cells, 3: 3 * m.n_cells, 4: 4 * m.n_cells, 5: m.n_cells,
-                6: 4 * m.n_bc, 7: 9 * self.total_springs}[which]
+                6: 4 * m.n_bc, 7: 9 * self.total_springs, 8: m.n_cells}[which]
         out = np.zeros(max(size, 1))
         lib().oracle_get_field(self.h, which, _p(out))
         return out[:size]
+
+    def time_step(self):
+        return lib().oracle_time_step(self.h)

@@ -223,6 +223,8 @@ struct ref_params {
     double wlc_ratio, curvature_ratio, volume_ratio, internal_viscosity_ratio, reference_length;
     int pivkin_length, sphere_reference;
     int viscosity_period;  // update_viscosities when t % period == 1
+    int time_stepping;     // globals.gpu_time_stepping: 1 local, 2 constant, 3 min, 4 talts (0 = 2)
+    double pre_conditioned_gamma;  // get_cfl_device's gamma (0 = 1 / gamma_inv)
 };
 
 namespace {
@@ -234,6 +236,8 @@ struct RefCase {
     std::vector<int> owner, neighbour, stencil, rho_type, vel_type;
     std::vector<double3> ccen, fnorm, fcen, rhs, g_rho, g_u, g_v, g_w;
     std::vector<double> vol, area, sdt, L[9], res_rho, res_u, res_v, res_w, fx, fy, fz, visc_factor, local_fneq, dtl;
+    std::vector<double3> cfl_areas;
+    double delta_t = 0;  // the step's delta_t (the loop's variable)
     double residual_rms[4];
     // RBC
     int n_nodes = 0, n_tets = 0, n_springs = 0;
@@ -313,6 +317,20 @@ extern "C" void *ref_case_create(void *mesh, const ref_params *p, const int *rho
     c->visc_factor.assign(nc, p->visc_factor_initial);
     c->local_fneq.assign(nt, 0.0);
     c->dtl.assign(nc, p->delta_t);
+    c->delta_t = p->delta_t;
+    // gpu_solver::populate_cfl_areas (Solver_gpu.cu:1657-1687), restated: the
+    // method is a member of the GPU solver class, which is not built here
+    c->cfl_areas.assign(nc, make_double3(0, 0, 0));
+    for (int i = 0; i < nc; i++) {
+        double ax = 0, ay = 0, az = 0;
+        for (int f = 0; f < (int)M.gradient_faces[i].size(); f++) {
+            const int face = M.gradient_faces[i][f];
+            ax = ax + fabs(M.get_face_i(face) * M.get_face_area(face));
+            ay = ay + fabs(M.get_face_j(face) * M.get_face_area(face));
+            az = az + fabs(M.get_face_k(face) * M.get_face_area(face));
+        }
+        c->cfl_areas[i] = make_double3(ax / 2, ay / 2, az / 2);
+    }
     // D3Q15 weights, gpu_solver::populate_e_alpha (Solver_gpu.cu:1407-1445)
     for (int k = 0; k < 15; k++) lattice_weight[k] = (k > 0 && k < 7) ? 1.0 / 9.0 : (k > 6 ? 1.0 / 72.0 : 2.0 / 9.0);
     return c;
@@ -371,7 +389,18 @@ extern "C" void ref_case_step(void *h, int n_steps) {
     for (int s = 0; s < n_steps; s++, c->t++) {
         int t = c->t;
         clone_a_to_b(nc, c->t1.data(), c->t0.data());
-        double delta_t = p.delta_t;  // time_stepping = constant (gpu_time_stepping 2)
+        // local time stepping calculation (Solver_gpu.cu:767-787)
+        const int mode = p.time_stepping == 0 ? 2 : p.time_stepping;
+        double delta_t = p.delta_t;
+        if (mode != 2) {
+            const double gamma = p.pre_conditioned_gamma > 0 ? p.pre_conditioned_gamma : 1 / p.gamma_inv;
+            get_cfl_device(nc, c->soln.data(), c->vol.data(), c->dtl.data(), c->cfl_areas.data(), p.delta_t,
+                           p.max_velocity, gamma, p.visc, mode);
+            delta_t = block_min_max(c->dtl.data(), nc, (nc + 127) / 128, true);
+        }
+        if (mode == 3) fill_double(nc, c->dtl.data(), delta_t);
+        else if (mode == 2) fill_double(nc, c->dtl.data(), p.delta_t);
+        c->delta_t = delta_t;
         if (p.has_rbc) {
             interpolate_velocities_on_nodes(c->n_nodes, c->vx.data(), c->vy.data(), c->vz.data(), c->x.data(), c->y.data(),
                                             c->z.data(), origin, lengths, delta_x, c->soln.data(), nc);
@@ -443,7 +472,7 @@ extern "C" void ref_case_step(void *h, int n_steps) {
         add(nc, c->res_v.data(), c->fy.data());
         add(nc, c->res_w.data(), c->fz.data());
         time_integration(nc, 0, 1, c->dtl.data(), c->t0.data(), c->t1.data(), c->soln.data(), c->res_rho.data(),
-                         c->res_u.data(), c->res_v.data(), c->res_w.data(), delta_t, 2);
+                         c->res_u.data(), c->res_v.data(), c->res_w.data(), delta_t, mode);
         // residual RMS (Solver_gpu.cu:1033-1046, residuals.cpp:114-133)
         int nblk = (nc + 127) / 128;
         std::vector<double> sq(nc);
@@ -473,6 +502,8 @@ enum {
     REF_SPRING = 14,                              // per spring: contour, k, curvature, curvature0, angle0, area0[2], area[2]
     REF_RESID = 15,                               // 4 residual rms
     REF_GHOST = 16,                               // 4*n_bc ghost (u,v,w,rho)
+    REF_DT_LOCAL = 17,                            // n_cells delta_t_local
+    REF_DELTA_T = 18,                             // 1: the last step's delta_t
 };
 
 extern "C" void ref_case_get(void *h, int which, double *out) {
@@ -538,6 +569,12 @@ extern "C" void ref_case_get(void *h, int which, double *out) {
             double4 g = c->soln[nc + i];
             out[4 * i] = g.x; out[4 * i + 1] = g.y; out[4 * i + 2] = g.z; out[4 * i + 3] = g.w;
         }
+        break;
+    case REF_DT_LOCAL:
+        for (int i = 0; i < nc; i++) out[i] = c->dtl[i];
+        break;
+    case REF_DELTA_T:
+        out[0] = c->delta_t;
         break;
     }
 }

@@ -14,6 +14,7 @@ tests replay them without the reference.
 """
 import os
 import sys
+from dataclasses import replace
 
 import numpy as np
 
@@ -35,6 +36,7 @@ def ref_case(c):
     p.force[:] = sp.body_force
     p.ref_rho, p.max_velocity, p.testcase = sp.ref_rho, sp.max_velocity, sp.testcase
     p.visc_factor_initial, p.viscosity_period = sp.visc_factor_initial, sp.viscosity_period
+    p.time_stepping, p.pre_conditioned_gamma = sp.time_stepping, sp.pre_conditioned_gamma
     p.has_rbc = 1 if c.membranes else 0
     if c.membranes:
         mb = c.membranes[0]
@@ -76,12 +78,14 @@ def step_fixture(name, case, steps):
     rc.step(1)
     out.update(s1_grad=rc.get(R.REF_GRAD), s1_flux=rc.get(R.REF_RES_FACE), s1_res=rc.get(R.REF_RES),
                s1_force=rc.get(R.REF_FORCE), s1_ghost=rc.get(R.REF_GHOST), s1_t1=rc.get(R.REF_T1),
-               s1_state=np.stack(rc.state()), s1_resid=rc.get(R.REF_RESID))
+               s1_state=np.stack(rc.state()), s1_resid=rc.get(R.REF_RESID), time_stepping=case.params.time_stepping,
+               s1_dtl=rc.get(R.REF_DT_LOCAL), s1_dt=rc.get(R.REF_DELTA_T)[0])
     if case.membranes:
         out.update(s1_nodes_x=rc.get(R.REF_NODE_X), s1_nodes_v=rc.get(R.REF_NODE_V), s1_nodes_f=rc.get(R.REF_NODE_F),
                    s1_totals=rc.get(R.REF_TOTALS), s1_visc=rc.get(R.REF_VISC), s1_spring=rc.get(R.REF_SPRING))
     rc.step(steps - 1)
-    out.update(sN_state=np.stack(rc.state()), sN_resid=rc.get(R.REF_RESID), steps=steps)
+    out.update(sN_state=np.stack(rc.state()), sN_resid=rc.get(R.REF_RESID), steps=steps,
+               sN_dtl=rc.get(R.REF_DT_LOCAL), sN_dt=rc.get(R.REF_DELTA_T)[0])
     if case.membranes:
         out.update(sN_nodes_x=rc.get(R.REF_NODE_X), sN_nodes_f=rc.get(R.REF_NODE_F), sN_totals=rc.get(R.REF_TOTALS),
                    sN_visc=rc.get(R.REF_VISC))
@@ -99,6 +103,14 @@ def main():
     step_fixture("step_poiseuille_6x5x4.npz", cases.poiseuille(n=6, ny=5, nz=4), 20)
     step_fixture("step_shear_rbc_16.npz",
                  cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2), 10)
+    # time stepping other than constant (get_cfl_device + min, Solver_gpu.cu:767-787)
+    for name, mode in (("local", _abi.LBFS_DT_LOCAL), ("talts", _abi.LBFS_DT_TALTS)):
+        c = cases.poiseuille(n=6, ny=5, nz=4)
+        c.params = replace(c.params, time_stepping=mode)
+        step_fixture(f"step_poiseuille_6x5x4_{name}.npz", c, 20)
+    c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
+    c.params = replace(c.params, time_stepping=_abi.LBFS_DT_MIN)
+    step_fixture("step_shear_rbc_16_min.npz", c, 10)
     print("golden fixtures written to", HERE)
 
 

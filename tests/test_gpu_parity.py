@@ -9,6 +9,8 @@
   identical to eager launches;
 * the FP32-bulk form against the FP64 path within FP32_RTOL.
 """
+from dataclasses import replace
+
 import numpy as np
 import pytest
 
@@ -34,10 +36,16 @@ def fixture_case(golden, name):
         mb = c.membranes[0]
         mb.xyz_stress_free, mb.xyz_initial = g["xyz_stress_free"], g["xyz_initial"]
     c.rho, c.u, c.v, c.w = g["rho0"], g["u0"], g["v0"], g["w0"]
+    if "time_stepping" in g.files:
+        c.params = replace(c.params, time_stepping=int(g["time_stepping"]))
     return c, g
 
 
-@pytest.mark.parametrize("name", ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz"])
+FIXTURES = ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz", "step_poiseuille_6x5x4_local.npz",
+            "step_poiseuille_6x5x4_talts.npz", "step_shear_rbc_16_min.npz"]
+
+
+@pytest.mark.parametrize("name", FIXTURES)
 def test_gpu_matches_reference_fixture(golden, name):
     c, g = fixture_case(golden, name)
     s = make(c)
@@ -54,6 +62,8 @@ def test_gpu_matches_reference_fixture(golden, name):
         "ghost": (s.field(_abi.LBFS_FIELD_GHOST), g["s1_ghost"]),
         "t1": (s.field(_abi.LBFS_FIELD_T1), g["s1_t1"]),
         "resid": (s.residuals(), g["s1_resid"]),
+        "dt_local": (s.field(_abi.LBFS_FIELD_DT_LOCAL), g["s1_dtl"]),
+        "dt": (np.array([s.time_step()]), np.array([g["s1_dt"]])),
     }
     for k, arr in enumerate(s.state()):
         checks[f"state{k}"] = (arr, g["s1_state"][k])
@@ -69,6 +79,8 @@ def test_gpu_matches_reference_fixture(golden, name):
     s.step(int(g["steps"]) - 1, graph=True)
     for k, arr in enumerate(s.state()):
         assert rel_err(arr, g["sN_state"][k]) < FP64_RTOL, (k, rel_err(arr, g["sN_state"][k]))
+    assert rel_err(s.field(_abi.LBFS_FIELD_DT_LOCAL), g["sN_dtl"]) < FP64_RTOL
+    assert rel_err(s.time_step(), g["sN_dt"]) < FP64_RTOL
     if c.membranes:
         assert rel_err(s.nodes().ravel(), g["sN_nodes_x"]) < FP64_RTOL
         assert rel_err(s.nodes(_abi.LBFS_NODES_FORCE).ravel(), g["sN_nodes_f"]) < FP64_RTOL

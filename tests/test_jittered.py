@@ -90,3 +90,33 @@ def test_jittered_box_at_rest_stays_at_rest():
     rho, u, v, w = o.state()
     assert np.max(np.abs(rho - 1.0)) < 1e-12
     assert max(np.max(np.abs(u)), np.max(np.abs(v)), np.max(np.abs(w))) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["local", "min"])
+def test_jittered_time_stepping_matches_oracle(mode):
+    """Per-cell CFL steps vary across a jittered mesh (volumes and face areas
+    differ per cell): local and minimum time stepping against the oracle, with
+    a red cell moving by the minimum step."""
+    from dataclasses import replace
+    from lbfs_b200 import GpuSolver, _abi, cases
+    from oracle_lbfs import OracleSolver
+    ts = {"local": _abi.LBFS_DT_LOCAL, "min": _abi.LBFS_DT_MIN}[mode]
+    c = cases.jittered_channel(n=16, n_rbc=1, level=2, radius_cells=2.0)
+    c.params = replace(c.params, time_stepping=ts)
+    steps = 8
+    with GpuSolver(c.mesh, c.params, c.membranes) as s:
+        s.set_state(c.rho, c.u, c.v, c.w)
+        s.step(steps, graph=True)
+        got, nodes, dtl, dt = s.state(), s.nodes(), s.field(_abi.LBFS_FIELD_DT_LOCAL), s.time_step()
+        assert s.status() == 0
+    o = OracleSolver(c.mesh, c.params, c.membranes)
+    o.set_state(c.rho, c.u, c.v, c.w)
+    o.step(steps)
+    for a, b in zip(got, o.state()):
+        assert rel_err(a, b) <= FP64_RTOL
+    assert rel_err(nodes, o.nodes()) <= FP64_RTOL
+    want = o.field(_abi.LBFS_FIELD_DT_LOCAL)
+    assert rel_err(dtl, want) <= FP64_RTOL and rel_err(dt, o.time_step()) <= FP64_RTOL
+    if mode == "local":
+        assert np.ptp(want) > 1e-3 * np.mean(want)  # the steps do vary from cell to cell

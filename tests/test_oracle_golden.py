@@ -1,5 +1,7 @@
 """The C restatement oracle reproduces the reference's own kernels (golden
 fixtures produced by the reference sources compiled for the host)."""
+from dataclasses import replace
+
 import numpy as np
 import pytest
 
@@ -19,10 +21,16 @@ def fixture_case(golden, name):
         mb.xyz_stress_free = g["xyz_stress_free"]
         mb.xyz_initial = g["xyz_initial"]
     c.rho, c.u, c.v, c.w = g["rho0"], g["u0"], g["v0"], g["w0"]
+    if "time_stepping" in g.files:
+        c.params = replace(c.params, time_stepping=int(g["time_stepping"]))
     return c, g
 
 
-@pytest.mark.parametrize("name", ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz"])
+FIXTURES = ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz", "step_poiseuille_6x5x4_local.npz",
+            "step_poiseuille_6x5x4_talts.npz", "step_shear_rbc_16_min.npz"]
+
+
+@pytest.mark.parametrize("name", FIXTURES)
 def test_oracle_matches_reference(golden, name):
     c, g = fixture_case(golden, name)
     o = OracleSolver(c.mesh, c.params, c.membranes)
@@ -39,6 +47,8 @@ def test_oracle_matches_reference(golden, name):
         "ghost": (o.field(_abi.LBFS_FIELD_GHOST), g["s1_ghost"]),
         "t1": (o.field(_abi.LBFS_FIELD_T1), g["s1_t1"]),
         "resid": (o.residuals(), g["s1_resid"]),
+        "dt_local": (o.field(_abi.LBFS_FIELD_DT_LOCAL), g["s1_dtl"]),
+        "dt": (np.array([o.time_step()]), np.array([g["s1_dt"]])),
     }
     for k, arr in enumerate(o.state()):
         checks[f"state{k}"] = (arr, g["s1_state"][k])
@@ -54,6 +64,8 @@ def test_oracle_matches_reference(golden, name):
     o.step(int(g["steps"]) - 1)
     for k, arr in enumerate(o.state()):
         assert rel_err(arr, g["sN_state"][k]) < FP64_RTOL, (k, rel_err(arr, g["sN_state"][k]))
+    assert rel_err(o.field(_abi.LBFS_FIELD_DT_LOCAL), g["sN_dtl"]) < FP64_RTOL
+    assert rel_err(o.time_step(), g["sN_dt"]) < FP64_RTOL
     if c.membranes:
         assert rel_err(o.nodes(_abi.LBFS_NODES_POSITION).ravel(), g["sN_nodes_x"]) < FP64_RTOL
         assert rel_err(o.nodes(_abi.LBFS_NODES_FORCE).ravel(), g["sN_nodes_f"]) < FP64_RTOL
