@@ -54,6 +54,9 @@ extern "C" {
 /* ---- IBM kernels ---------------------------------------------------------- */
 #define LBFS_IBM_HAT2 2         /* 2-point hat stencil (immersed_boundary_method.cu:14-97, 947-1024) */
 #define LBFS_IBM_PESKIN4 4      /* 4-point Peskin cosine-free delta (new; no reference counterpart)  */
+#define LBFS_IBM_VANDERMONDE4 5 /* 4x4x4 Lagrange (Vandermonde first column) weights on a rectilinear
+                                   mesh, the mesh_type 4 kernels (immersed_boundary_method.cu:588-872,
+                                   919-941); needs lbfs_mesh_desc.grid_x/y/z                       */
 
 /* One instance of a batched ensemble: a contiguous range of interior cells
  * that forms its own uniform IBM grid (cell index = cell0 + i + nx (j + ny k)). */
@@ -100,6 +103,10 @@ typedef struct lbfs_mesh_desc {
      * instance).  0 = one instance described by origin/length/delta_x/delta_h. */
     int32_t n_instances;
     const lbfs_grid_desc *instances;
+    /* Vertex coordinates per axis of a rectilinear mesh, [nx+1], [ny+1], [nz+1]
+     * (plateau_x, plateau_y, plateau_z, Solver_gpu.cu:637-639): read only by
+     * LBFS_IBM_VANDERMONDE4; null otherwise. */
+    const double *grid_x, *grid_y, *grid_z;
 } lbfs_mesh_desc;
 
 /* Scalars of global_variables / initial_conditions used by the step. */
@@ -335,6 +342,21 @@ int lbfs_mesh_build_uniform(double X, double Y, double Z, double dt, const doubl
                             double *face_area, double *face_normal, double *face_centroid, double *streaming_dt,
                             double *cell_volume, double *cell_centroid, int32_t *gradient_stencil,
                             double *lhs_inverse, double *rhs, int32_t *bc_patch, double *delta_h);
+
+/* Rectilinear meshes of the reference generator (create_uniform_openfoam_mesh,
+ * unstructured_mesh.cpp:238-380): mesh_type 6 uniform, 7 cosine-clustered in
+ * x and y, 5 in x, y and z, 4 the plateau mesh (domain.plateau_width,
+ * plateau_slope).  Outputs as lbfs_mesh_build_uniform, plus grid_xyz
+ * [(nx+1) + (ny+1) + (nz+1)]: the vertex coordinates per axis (for mesh_type 4
+ * the plateau arrays the 4x4x4 IBM stencil searches).  Faces stay axis
+ * aligned (axis_aligned = 1). */
+int lbfs_mesh_build_rectilinear(double X, double Y, double Z, double dt, const double *origin, double visc,
+                                double fneq_min, int32_t gradient_hybrid, int32_t mesh_type, double plateau_width,
+                                double plateau_slope, int32_t *owner, int32_t *neighbour, double *face_area,
+                                double *face_normal, double *face_centroid, double *streaming_dt,
+                                double *cell_volume, double *cell_centroid, int32_t *gradient_stencil,
+                                double *lhs_inverse, double *rhs, int32_t *bc_patch, double *delta_h,
+                                double *grid_xyz);
 
 /* The same mesh with every interior vertex moved by a seeded uniform
  * perturbation of up to `jitter` (< 0.25) times the cell spacing per axis

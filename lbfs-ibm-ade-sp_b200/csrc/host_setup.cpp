@@ -76,11 +76,21 @@ double jitter_unit(uint64_t seed, uint64_t vertex, int axis) {
     return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
 }
 
+// How the generator places the vertices: the reference's mesh types
+// (unstructured_mesh.cpp:354-378) and the seeded jitter of interior vertices.
+struct VertexSpec {
+    int mesh_type = 6;           // 6 uniform, 7 cosine in x and y, 5 cosine in x, y, z, 4 plateau
+    double plateau_width = 0.0;  // domain.plateau_width (mesh_type 4)
+    double plateau_slope = 0.0;  // domain.plateau_slope (mesh_type 4)
+    double jitter = 0.0;
+    uint64_t seed = 0;
+};
+
 int build_mesh(double X, double Y, double Z, double dt, const double *origin, double visc, double fneq_min,
-               int32_t gradient_hybrid, double jitter, uint64_t seed, int32_t *owner, int32_t *neighbour,
+               int32_t gradient_hybrid, const VertexSpec &vs, int32_t *owner, int32_t *neighbour,
                double *face_area, double *face_normal, double *face_centroid, double *streaming_dt,
                double *cell_volume, double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse,
-               double *rhs, int32_t *bc_patch, double *delta_h);
+               double *rhs, int32_t *bc_patch, double *delta_h, double *grid_xyz);
 
 }  // namespace
 
@@ -90,9 +100,28 @@ extern "C" int lbfs_mesh_build_uniform(double X, double Y, double Z, double dt, 
                                        double *streaming_dt, double *cell_volume, double *cell_centroid,
                                        int32_t *gradient_stencil, double *lhs_inverse, double *rhs, int32_t *bc_patch,
                                        double *delta_h) {
-    return build_mesh(X, Y, Z, dt, origin, visc, fneq_min, gradient_hybrid, 0.0, 0, owner, neighbour, face_area,
+    return build_mesh(X, Y, Z, dt, origin, visc, fneq_min, gradient_hybrid, VertexSpec(), owner, neighbour, face_area,
                       face_normal, face_centroid, streaming_dt, cell_volume, cell_centroid, gradient_stencil,
-                      lhs_inverse, rhs, bc_patch, delta_h);
+                      lhs_inverse, rhs, bc_patch, delta_h, nullptr);
+}
+
+extern "C" int lbfs_mesh_build_rectilinear(double X, double Y, double Z, double dt, const double *origin, double visc,
+                                           double fneq_min, int32_t gradient_hybrid, int32_t mesh_type,
+                                           double plateau_width, double plateau_slope, int32_t *owner,
+                                           int32_t *neighbour, double *face_area, double *face_normal,
+                                           double *face_centroid, double *streaming_dt, double *cell_volume,
+                                           double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse,
+                                           double *rhs, int32_t *bc_patch, double *delta_h, double *grid_xyz) {
+    if (mesh_type != 4 && mesh_type != 5 && mesh_type != 6 && mesh_type != 7)
+        return lbfs::set_error(LBFS_ERR_ARG, "mesh_type must be 4 (plateau), 5, 6 (uniform) or 7 (cosine)");
+    if (!grid_xyz) return lbfs::set_error(LBFS_ERR_ARG, "null output buffer");
+    VertexSpec vs;
+    vs.mesh_type = mesh_type;
+    vs.plateau_width = plateau_width;
+    vs.plateau_slope = plateau_slope;
+    return build_mesh(X, Y, Z, dt, origin, visc, fneq_min, gradient_hybrid, vs, owner, neighbour, face_area,
+                      face_normal, face_centroid, streaming_dt, cell_volume, cell_centroid, gradient_stencil,
+                      lhs_inverse, rhs, bc_patch, delta_h, grid_xyz);
 }
 
 extern "C" int lbfs_mesh_build_jittered(double X, double Y, double Z, double dt, const double *origin, double visc,
@@ -103,18 +132,45 @@ extern "C" int lbfs_mesh_build_jittered(double X, double Y, double Z, double dt,
                                         double *rhs, int32_t *bc_patch, double *delta_h) {
     if (!(jitter >= 0.0 && jitter < 0.25))
         return lbfs::set_error(LBFS_ERR_ARG, "jitter must be in [0, 0.25) of the cell spacing");
-    return build_mesh(X, Y, Z, dt, origin, visc, fneq_min, gradient_hybrid, jitter, seed, owner, neighbour,
+    VertexSpec vs;
+    vs.jitter = jitter;
+    vs.seed = seed;
+    return build_mesh(X, Y, Z, dt, origin, visc, fneq_min, gradient_hybrid, vs, owner, neighbour,
                       face_area, face_normal, face_centroid, streaming_dt, cell_volume, cell_centroid,
-                      gradient_stencil, lhs_inverse, rhs, bc_patch, delta_h);
+                      gradient_stencil, lhs_inverse, rhs, bc_patch, delta_h, nullptr);
 }
 
 namespace {
 
+// Vertex coordinates along one axis of n cells (unstructured_mesh.cpp:290-378):
+// uniform, cosine-clustered, or the plateau function normalised to the length.
+std::vector<double> axis_vertices(int mesh_type, bool clustered, int n, double origin, double length, double step,
+                                  double ap, double bp) {
+    std::vector<double> v(n + 1);
+    const double PI = std::acos(-1.0);  // globals.PI
+    if (mesh_type == 4) {
+        double sum = 0.0;
+        for (int i = 1; i < n + 1; i++) {
+            const double fx = i - n / 2.0 - 0.5;
+            v[i] = (std::exp(bp * (fx - ap)) + 1) * (std::exp(bp * (-fx - ap)) + 1);
+            sum = sum + v[i];
+        }
+        for (int i = 0; i < n + 1; i++) v[i] = i == 0 ? origin : v[i - 1] + v[i] * length / sum;
+    } else if (clustered) {
+        for (int i = 0; i < n + 1; i++) v[i] = origin + 0.5 * (1 - std::cos(i / (double)(n)*PI)) * length;
+    } else {
+        for (int i = 0; i < n + 1; i++) v[i] = origin + i * step;
+    }
+    return v;
+}
+
 int build_mesh(double X, double Y, double Z, double dt, const double *origin, double visc, double fneq_min,
-               int32_t gradient_hybrid, double jitter, uint64_t seed, int32_t *owner, int32_t *neighbour,
+               int32_t gradient_hybrid, const VertexSpec &vs, int32_t *owner, int32_t *neighbour,
                double *face_area, double *face_normal, double *face_centroid, double *streaming_dt,
                double *cell_volume, double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse,
-               double *rhs, int32_t *bc_patch, double *delta_h) {
+               double *rhs, int32_t *bc_patch, double *delta_h, double *grid_xyz) {
+    const double jitter = vs.jitter;
+    const uint64_t seed = vs.seed;
     int32_t cnt[8];
     int rc = lbfs_mesh_uniform_counts(X, Y, Z, dt, cnt);
     if (rc) return rc;
@@ -126,13 +182,25 @@ int build_mesh(double X, double Y, double Z, double dt, const double *origin, do
     const int nc = d.n_cells, nf = d.n_faces, ni = d.n_interior, nt = nc + d.n_bc;
 
     // Vertices are stored as float in the reference (unstructured_mesh.h:59).
+    const int mt = vs.mesh_type;
+    const std::vector<double> ax = axis_vertices(mt, mt == 5 || mt == 7, d.nx, origin[0], X, d.dx, vs.plateau_width,
+                                                 vs.plateau_slope),
+                              ay = axis_vertices(mt, mt == 5 || mt == 7, d.ny, origin[1], Y, d.dy, vs.plateau_width,
+                                                 vs.plateau_slope),
+                              az = axis_vertices(mt, mt == 5, d.nz, origin[2], Z, d.dz, vs.plateau_width,
+                                                 vs.plateau_slope);
+    if (grid_xyz) {
+        std::copy(ax.begin(), ax.end(), grid_xyz);
+        std::copy(ay.begin(), ay.end(), grid_xyz + nvx);
+        std::copy(az.begin(), az.end(), grid_xyz + nvx + nvy);
+    }
     std::vector<float> vx((size_t)nvx * nvy * nvz), vy(vx.size()), vz(vx.size());
     {
         size_t t = 0;
         for (int k = 0; k < nvz; k++)
             for (int j = 0; j < nvy; j++)
                 for (int i = 0; i < nvx; i++, t++) {
-                    double px = origin[0] + i * d.dx, py = origin[1] + j * d.dy, pz = origin[2] + k * d.dz;
+                    double px = ax[i], py = ay[j], pz = az[k];
                     // interior vertices move by up to jitter * spacing per axis (the box stays a box)
                     if (jitter > 0 && i > 0 && j > 0 && k > 0 && i < nvx - 1 && j < nvy - 1 && k < nvz - 1) {
                         px += jitter * d.dx * jitter_unit(seed, t, 0);

@@ -80,12 +80,21 @@ struct MembraneArgs {
     int *sorted_pos;             // [total_nodes] position of each node in its membrane's sorted order
     double4 *sorted_force;       // [total_nodes] node forces in sorted order (spread input)
     SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order (scratch)
+    // LBFS_IBM_VANDERMONDE4 (rectilinear meshes, one instance): per axis the
+    // vertex coordinates [n + 1] and the centroid coordinate of each cell row [n]
+    // (centroid[i].x, centroid[j nx].y, centroid[k nx ny].z), and the cell volumes
+    const double *grid_v[3];
+    const double *grid_c[3];
+    const double *cell_volume;
     int max_springs;             // springs of the largest membrane
     int max_patch_bound;         // largest patch_bound over the membranes (spread grid)
     const int *node_mem;         // [total_nodes] membrane of each node
     double *mad_partials;        // [n_membranes * kMaxSpringBlocks] (scratch)
     unsigned int *mad_ticket;    // [n_membranes], zero between launches
 };
+
+// points per axis of an IBM stencil
+__host__ __device__ constexpr int stencil_width(int ibm_stencil) { return ibm_stencil == 2 ? 2 : 4; }
 
 void membrane_prepare(int sort_capacity);
 // Enqueues the membrane kernels of the current mode on `s` (the node sort on

@@ -87,9 +87,60 @@ struct Stencil {
     double rx, ry, rz;
     int i0, j0, k0;
 };
+
+// Index of the vertex closest to t in the increasing array v[0..n), ties to
+// the upper vertex; t outside the array gives its end (find_index_closest,
+// immersed_boundary_method.cu:588-630).
+__device__ __forceinline__ int closest_vertex(const double *v, int n, double t) {
+    if (t <= v[0]) return 0;
+    if (t >= v[n - 1]) return n - 1;
+    int lo = 0, hi = n - 1;  // v[lo] < t < v[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (v[mid] == t) return mid;
+        if (v[mid] < t) lo = mid;
+        else hi = mid;
+    }
+    return (t - v[lo] >= v[hi] - t) ? hi : lo;
+}
+
+// Weights at 0 of the Lagrange polynomials through x1..x4: the first column
+// of the inverse Vandermonde matrix as vandemonde_inverse forms it
+// (immersed_boundary_method.cu:919-941).
+__device__ __forceinline__ double lagrange4_at0(const double (&x)[4], int q) {
+    const double sxy = 1 / (x[0] - x[1]), sxz = 1 / (x[0] - x[2]), sxw = 1 / (x[0] - x[3]);
+    const double syz = 1 / (x[1] - x[2]), syw = 1 / (x[1] - x[3]), szw = 1 / (x[2] - x[3]);
+    if (q == 0) return -1 * x[1] * x[2] * x[3] * sxy * sxz * sxw;
+    if (q == 1) return x[0] * x[2] * x[3] * sxy * syz * syw;
+    if (q == 2) return -1 * x[0] * x[1] * x[3] * sxz * syz * szw;
+    return x[0] * x[1] * x[2] * sxw * syw * szw;
+}
+
+// One-dimensional weight q of the 4x4x4 stencil on a rectilinear mesh along
+// axis ax: cells b .. b + 3 of the row, offsets of their centroids from p.  A
+// stencil that leaves the mesh gets zero weights (the node sort raises
+// LBFS_FLAG_IBM_RANGE; the reference reads outside its arrays there).
+__device__ __forceinline__ double vandermonde_weight(const MembraneArgs &a, const MembraneConst &mc, int ax, int b,
+                                                     double p, int q) {
+    const int n = ax == 0 ? mc.gnx : (ax == 1 ? mc.gny : mc.gnz);
+    if (b < 0 || b + 3 >= n) return 0.0;
+    const double *c = a.grid_c[ax] + b;
+    const double x[4] = {c[0] - p, c[1] - p, c[2] - p, c[3] - p};
+    return lagrange4_at0(x, q);
+}
+
 __device__ __forceinline__ Stencil node_stencil(const MembraneArgs &a, const MembraneConst &mc, double x, double y,
                                                 double z) {
     Stencil s;
+    if (a.ibm_stencil == LBFS_IBM_VANDERMONDE4) {
+        // the closest vertex, minus 2: the first of the 4 cells per axis
+        // (interpolate_velocities_on_nodes_non_uniform_grid, immersed_boundary_method.cu:685-711)
+        s.rx = x; s.ry = y; s.rz = z;
+        s.i0 = closest_vertex(a.grid_v[0], mc.gnx + 1, x) - 2;
+        s.j0 = closest_vertex(a.grid_v[1], mc.gny + 1, y) - 2;
+        s.k0 = closest_vertex(a.grid_v[2], mc.gnz + 1, z) - 2;
+        return s;
+    }
     s.rx = (x - mc.gorigin[0]) / mc.gdx;
     s.ry = fabs((y - mc.gorigin[1]) / mc.gdx);
     s.rz = fabs((z - mc.gorigin[2]) / mc.gdx);
@@ -320,13 +371,16 @@ __device__ void spring_reference(const MembraneArgs &A, const MembraneConst &mc,
 // them instead of evaluating the delta kernel again.
 __device__ __forceinline__ void write_stencil_tables(const MembraneArgs &A, const MembraneConst &mc, int n,
                                                      double x, double y, double z, int lane) {
-    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+    const int S = stencil_width(A.ibm_stencil);
     const Stencil st = node_stencil(A, mc, x, y, z);
     if (lane < 12) {
         const int ax = lane >> 2, q = lane & 3;
         const int b = ax == 0 ? st.i0 : (ax == 1 ? st.j0 : st.k0);
         const double r = ax == 0 ? st.rx : (ax == 1 ? st.ry : st.rz);
-        A.node_w[12 * (size_t)n + lane] = q < S ? stencil_weight(A.ibm_stencil, b + q + 0.5 - r) : 0.0;
+        A.node_w[12 * (size_t)n + lane] =
+            q >= S ? 0.0
+                   : (A.ibm_stencil == LBFS_IBM_VANDERMONDE4 ? vandermonde_weight(A, mc, ax, b, r, q)
+                                                              : stencil_weight(A.ibm_stencil, b + q + 0.5 - r));
     }
     if (lane < 3) A.node_base[3 * (size_t)n + lane] = lane == 0 ? st.i0 : (lane == 1 ? st.j0 : st.k0);
 }
@@ -349,7 +403,7 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
     const double x = A.x[n], y = A.y[n], z = A.z[n];
     const Stencil st = node_stencil(A, mc, x, y, z);
     const int n_inst = mc.gnx * mc.gny * mc.gnz;
-    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+    const int S = stencil_width(A.ibm_stencil);
     const int cells = S * S * S;
     // the 3 S one-dimensional weights, one per lane (lane = axis * S + offset)
     double w1 = 0.0;
@@ -357,7 +411,8 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
         const int ax = lane / S, q = lane - ax * S;
         const int b = ax == 0 ? st.i0 : (ax == 1 ? st.j0 : st.k0);
         const double r = ax == 0 ? st.rx : (ax == 1 ? st.ry : st.rz);
-        w1 = stencil_weight(A.ibm_stencil, b + q + 0.5 - r);
+        w1 = A.ibm_stencil == LBFS_IBM_VANDERMONDE4 ? vandermonde_weight(A, mc, ax, b, r, q)
+                                                    : stencil_weight(A.ibm_stencil, b + q + 0.5 - r);
     }
     double v[3] = {0.0, 0.0, 0.0};
     for (int c0 = 0; c0 < cells; c0 += 32) {
@@ -527,7 +582,7 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     const int m = blockIdx.x;
     const MembraneConst mc = A.mc[m];
     MembraneScalars *ms = A.ms + m;
-    const int S = A.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+    const int S = stencil_width(A.ibm_stencil);
     const int gn[3] = {mc.gnx, mc.gny, mc.gnz};
     double v[12];
     for (int c = 0; c < 3; c++) { v[c] = 1e300; v[3 + c] = 1e300; v[6 + c] = 1e300; v[9 + c] = 1e300; }
@@ -733,7 +788,15 @@ __global__ void __launch_bounds__(256) k_mem_spread(MembraneArgs A) {
         const int count = __shfl_sync(0xffffffffu, end, S * S - 1);
         const SpreadRec *rec = A.spread_rec + mc.node0;
         const double4 *frc = A.sorted_force + mc.node0;
-        const double inv3 = 1 / mc.gdx / mc.gdx / mc.gdx;
+        double inv3 = 1 / mc.gdx / mc.gdx / mc.gdx;
+        if (A.ibm_stencil == LBFS_IBM_VANDERMONDE4) {
+            // divided by the cell's volume (spread_forces_on_non_uniform_grid, immersed_boundary_method.cu:851)
+            const int cj = ms.patch_lo[1] + py, ck = ms.patch_lo[2] + pz;
+            const int lidx = ci + mc.gnx * (cj + mc.gny * ck);
+            inv3 = (ci >= 0 && ci < mc.gnx && cj >= 0 && cj < mc.gny && ck >= 0 && ck < mc.gnz)
+                       ? 1.0 / __ldg(A.cell_volume + mc.cell0 + lidx)
+                       : 0.0;
+        }
         double f[3] = {0.0, 0.0, 0.0};
         for (int q0 = 0; q0 < count; q0 += 32) {
             const int q = q0 + lane;
@@ -874,7 +937,7 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
     launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
     const dim3 grid(a.spread_blocks);
-    if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
+    if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
     else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a);
     return 6;
 }
@@ -902,7 +965,7 @@ void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s) {
 
 void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s) {
     const dim3 grid(a.spread_blocks);
-    if (a.ibm_stencil == LBFS_IBM_PESKIN4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
+    if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
     else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a);
 }
 

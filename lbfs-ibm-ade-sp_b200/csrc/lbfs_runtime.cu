@@ -350,6 +350,33 @@ template <typename R> int setup_time_stepping(lbfs_solver *s, const lbfs_mesh_de
     return LBFS_OK;
 }
 
+// LBFS_IBM_VANDERMONDE4: the vertex coordinates per axis (plateau_x/y/z), the
+// centroid coordinate of each cell row (the cells the reference indexes,
+// centroid[i].x, centroid[j nx].y, centroid[k nx ny].z,
+// immersed_boundary_method.cu:718-740) and the cell volumes.
+int setup_rectilinear_ibm(lbfs_solver *s, const lbfs_mesh_desc *m) {
+    MembraneArgs &ma = s->ma;
+    for (int q = 0; q < 3; q++) { ma.grid_v[q] = nullptr; ma.grid_c[q] = nullptr; }
+    ma.cell_volume = s->fp32 ? s->f32.cell_volume : s->f64.cell_volume;
+    if (s->params.ibm_stencil != LBFS_IBM_VANDERMONDE4 || s->n_membranes == 0) return LBFS_OK;
+    const InstanceGrid &g = s->inst[0];
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const double *gv[3] = {m->grid_x, m->grid_y, m->grid_z};
+    const long long stride[3] = {1, (long long)g.nx, (long long)g.nx * g.ny};
+    int rc;
+    for (int q = 0; q < 3; q++) {
+        std::vector<double> v(gv[q], gv[q] + n[q] + 1), c(n[q]);
+        for (int i = 1; i < n[q] + 1; i++)
+            if (!(v[i] > v[i - 1])) return set_error(LBFS_ERR_ARG, "grid vertex coordinates must increase");
+        for (int i = 0; i < n[q]; i++) c[i] = m->cell_centroid[3 * (g.cell0 + i * stride[q]) + q];
+        double *dv, *dc;
+        if ((rc = s->upload(&dv, v)) || (rc = s->upload(&dc, c))) return rc;
+        ma.grid_v[q] = dv;
+        ma.grid_c[q] = dc;
+    }
+    return LBFS_OK;
+}
+
 // Ensemble instance table: the descriptor's instances, or one instance covering
 // the whole mesh from origin/length/delta_x/delta_h.
 int setup_instances(lbfs_solver *s, const lbfs_mesh_desc *m) {
@@ -435,7 +462,7 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         c.gdx = gd.delta_x; c.gdh = gd.delta_h;
         {
             // a patch of in-range stencils lies inside the instance's grid
-            const int S = p.ibm_stencil == LBFS_IBM_PESKIN4 ? 4 : 2;
+            const int S = stencil_width(p.ibm_stencil);
             const long long cells = (long long)(g.nx + S - 1) * (g.ny + S - 1) * (g.nz + S - 1);
             c.patch_bound = (int)std::min<long long>(kMaxPatchCells, cells);
         }
@@ -670,8 +697,15 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if (n_rbc < 0 || (n_rbc > 0 && !rbc)) return set_error(LBFS_ERR_ARG, "bad membrane count");
     if (params->precision != LBFS_FP64 && params->precision != LBFS_FP32_BULK)
         return set_error(LBFS_ERR_ARG, "precision must be LBFS_FP64 or LBFS_FP32_BULK");
-    if (params->ibm_stencil != LBFS_IBM_HAT2 && params->ibm_stencil != LBFS_IBM_PESKIN4)
-        return set_error(LBFS_ERR_ARG, "ibm_stencil must be 2 or 4");
+    if (params->ibm_stencil != LBFS_IBM_HAT2 && params->ibm_stencil != LBFS_IBM_PESKIN4 &&
+        params->ibm_stencil != LBFS_IBM_VANDERMONDE4)
+        return set_error(LBFS_ERR_ARG, "ibm_stencil must be LBFS_IBM_HAT2, LBFS_IBM_PESKIN4 or LBFS_IBM_VANDERMONDE4");
+    if (params->ibm_stencil == LBFS_IBM_VANDERMONDE4 && n_rbc > 0) {
+        if (!mesh->grid_x || !mesh->grid_y || !mesh->grid_z)
+            return set_error(LBFS_ERR_ARG, "LBFS_IBM_VANDERMONDE4 needs the mesh's vertex coordinates (grid_x/y/z)");
+        if (mesh->n_instances > 1 || !mesh->axis_aligned)
+            return set_error(LBFS_ERR_UNSUPPORTED, "LBFS_IBM_VANDERMONDE4 runs on one rectilinear mesh");
+    }
     if (!(params->delta_t > 0)) return set_error(LBFS_ERR_ARG, "delta_t must be positive");
     if (params->time_stepping < 0 || params->time_stepping > LBFS_DT_TALTS)
         return set_error(LBFS_ERR_ARG, "time_stepping must be 0 or LBFS_DT_LOCAL/CONSTANT/MIN/TALTS");
@@ -710,6 +744,7 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if (rc) return fail(rc);
     std::vector<double> centroid(mesh->cell_centroid, mesh->cell_centroid + 3 * (size_t)mesh->n_cells);
     if ((rc = s->upload(&s->d_centroid, centroid))) return fail(rc);
+    if ((rc = setup_rectilinear_ibm(s, mesh))) return fail(rc);  // read by the stencil tables of the set-up
     rc = setup_membranes(s, mesh, rbc, n_rbc);
     if (rc) return fail(rc);
     rc = s->fp32 ? setup_time_stepping<float>(s, mesh) : setup_time_stepping<double>(s, mesh);
@@ -1278,6 +1313,8 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     if (s->params.gamma_inv != 1.0) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: no preconditioning");
     if (dynamic_dt(s->params))
         return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: constant time stepping only");
+    if (s->params.ibm_stencil == LBFS_IBM_VANDERMONDE4 && s->n_membranes > 0)
+        return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: LBFS_IBM_HAT2 or LBFS_IBM_PESKIN4 only");
     if (obj->kind == LBFS_OBJ_VELOCITY) {
         if (!obj->cell_weights) return set_error(LBFS_ERR_ARG, "lbfs_adjoint: velocity objective needs weights");
     } else if (obj->kind == LBFS_OBJ_TAYLOR) {

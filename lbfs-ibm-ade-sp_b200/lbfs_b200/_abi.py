@@ -28,6 +28,7 @@ LBFS_FP64 = 0
 LBFS_FP32_BULK = 1
 LBFS_IBM_HAT2 = 2
 LBFS_IBM_PESKIN4 = 4
+LBFS_IBM_VANDERMONDE4 = 5
 
 LBFS_NODES_POSITION = 0
 LBFS_NODES_VELOCITY = 1
@@ -75,6 +76,7 @@ class MeshDesc(ctypes.Structure):
         ("origin", ctypes.c_double * 3), ("length", ctypes.c_double * 3),
         ("delta_x", ctypes.c_double), ("delta_h", ctypes.c_double),
         ("n_instances", ctypes.c_int32), ("instances", ctypes.POINTER(GridDesc)),
+        ("grid_x", _f64p), ("grid_y", _f64p), ("grid_z", _f64p),
     ]
 
 
@@ -166,6 +168,11 @@ def lib():
                                                                    ctypes.c_int32, ctypes.c_double, ctypes.c_uint64,
                                                                    _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p,
                                                                    _f64p, _i32p, _f64p, _f64p, _i32p, _f64p],
+            "lbfs_mesh_build_rectilinear": [ctypes.c_double] * 4 + [_f64p, ctypes.c_double, ctypes.c_double,
+                                                                      ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                                                      ctypes.c_double, _i32p, _i32p, _f64p, _f64p,
+                                                                      _f64p, _f64p, _f64p, _f64p, _i32p, _f64p,
+                                                                      _f64p, _i32p, _f64p, _f64p],
             "lbfs_rbc_build_springs": [ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int32, _i32p, _i32p],
             "lbfs_residual_rms_noalloc": [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, vp, vp],
             "lbfs_get_launch_shape": [vp, ctypes.POINTER(LaunchShape)],
@@ -216,5 +223,5 @@ EXPORTED = [
     "lbfs_last_error", "lbfs_mesh_uniform_counts", "lbfs_mesh_build_uniform", "lbfs_rbc_build_springs",
     "lbfs_residual_rms_noalloc", "lbfs_get_launch_shape", "lbfs_set_launch_shape", "lbfs_autotune",
     "lbfs_adjoint", "lbfs_checkpoint_size", "lbfs_checkpoint_save", "lbfs_checkpoint_load",
-    "lbfs_mesh_build_jittered",
+    "lbfs_mesh_build_jittered", "lbfs_mesh_build_rectilinear",
 ]

@@ -70,14 +70,17 @@ def poiseuille(n=32, seed=1234, tau=0.8, u_centre=0.01, delta_t=0.5, precision=_
 
 def shear_rbc(n=64, level=3, radius_cells=8.0, capillary=0.1, u_wall=0.02, seed=4321, tau=0.8, delta_t=0.5,
               precision=_abi.LBFS_FP64, ibm_stencil=_abi.LBFS_IBM_PESKIN4, n_cells_y=None, n_cells_z=None,
-              rotate=False):
-    """Simple shear with one red cell of radius `radius_cells` cells at the centre."""
+              rotate=False, mesh_type=6, plateau=(0.0, 0.0)):
+    """Simple shear with one red cell of radius `radius_cells` cells at the centre.  mesh_type 4 with
+    plateau = (width, slope) is the reference's plateau mesh (uniform cells in the middle, coarser
+    towards the walls), whose IBM is LBFS_IBM_VANDERMONDE4."""
     ny = n_cells_y or n
     nz = n_cells_z or n
     dt = 1.0
     visc = (tau - 0.5) / 3.0 * dt
     X, Y, Z = 2.0 * n, 2.0 * ny, 2.0 * nz
-    mesh = build_uniform_mesh(X, Y, Z, dt, visc=visc)
+    mesh = build_uniform_mesh(X, Y, Z, dt, visc=visc, mesh_type=mesh_type, plateau_width=plateau[0],
+                              plateau_slope=plateau[1])
     gamma = u_wall / Y
     bcs = {"left": (2, 2, 1.0, 0.0, 0.0, 0.0), "right": (2, 2, 1.0, 0.0, 0.0, 0.0),
            "bottom": (2, 10, 1.0, gamma, 0.0, 0.0), "top": (2, 10, 1.0, gamma, 0.0, 0.0),

@@ -48,6 +48,9 @@ class UniformMesh:
     bc_vel_type: np.ndarray = field(default=None)
     bc_values: np.ndarray = field(default=None)
     axis_aligned: bool = True  # False for jittered meshes: every face takes the general-normal flux
+    mesh_type: int = 6         # 6 uniform, 7 / 5 cosine-clustered, 4 plateau (rectilinear), 3 jittered
+    grid: tuple = None         # vertex coordinates per axis (rectilinear meshes)
+    plateau: tuple = (0.0, 0.0)  # plateau width and slope (mesh_type 4)
 
     @property
     def shape(self):
@@ -95,6 +98,8 @@ class UniformMesh:
         d.length[:] = (self.X, self.Y, self.Z)
         d.delta_x = self.delta_x
         d.delta_h = self.delta_h
+        if self.grid is not None:
+            d.grid_x, d.grid_y, d.grid_z = (_abi.ptr(g) for g in self.grid)
         return d
 
 
@@ -105,10 +110,12 @@ def uniform_counts(X, Y, Z, dt):
 
 
 def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_min=0.0, gradient="LS", jitter=0.0,
-                       seed=0):
-    """Uniform mesh of ceil(X/(2 dt)) x ceil(Y/(2 dt)) x ceil(Z/(2 dt)) cells (mesh_type 6); with
-    jitter > 0 every interior vertex moves by a seeded uniform offset of up to jitter x spacing per
-    axis and the mesh is stepped through the general-normal flux (mesh_type 3)."""
+                       seed=0, mesh_type=6, plateau_width=0.0, plateau_slope=0.0):
+    """Mesh of ceil(X/(2 dt)) x ceil(Y/(2 dt)) x ceil(Z/(2 dt)) cells.  mesh_type 6 (uniform),
+    7 / 5 (cosine-clustered in x, y / in x, y, z) and 4 (the plateau mesh of plateau_width,
+    plateau_slope) are the reference generator's rectilinear meshes; with jitter > 0 every
+    interior vertex of the uniform mesh moves by a seeded uniform offset of up to jitter x spacing
+    per axis and the mesh is stepped through the general-normal flux (mesh_type 3)."""
     nc, nf, ni, nb, nfx, nfy, nfz, nt = uniform_counts(X, Y, Z, dt)
     owner = np.zeros(nf, np.int32)
     neighbour = np.zeros(nf, np.int32)
@@ -128,10 +135,22 @@ def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_m
             _abi.ptr(vol), _abi.ptr(ccen), _abi.iptr(stencil), _abi.ptr(lhs), _abi.ptr(rhs), _abi.iptr(patch),
             ctypes.byref(dh))
     hybrid = 1 if gradient == "hybrid" else 0
-    if jitter > 0:
+    grid = None
+    if mesh_type != 6:
+        if jitter > 0:
+            raise ValueError("jitter applies to the uniform mesh only")
+        nx, ny, nz = (int(np.ceil(L / dt * 0.5)) for L in (X, Y, Z))
+        g = np.zeros(nx + ny + nz + 3)
+        _abi.check(_abi.lib().lbfs_mesh_build_rectilinear(X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, hybrid,
+                                                          int(mesh_type), float(plateau_width),
+                                                          float(plateau_slope), *outs, _abi.ptr(g)))
+        grid = (g[:nx + 1].copy(), g[nx + 1:nx + ny + 2].copy(), g[nx + ny + 2:].copy())
+    elif jitter > 0:
         _abi.check(_abi.lib().lbfs_mesh_build_jittered(X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, hybrid,
                                                        float(jitter), int(seed), *outs))
     else:
         _abi.check(_abi.lib().lbfs_mesh_build_uniform(X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, hybrid, *outs))
     return UniformMesh(X, Y, Z, dt, tuple(origin), nc, nf, ni, nb, nfx, nfy, nfz, owner, neighbour, area, normal,
-                       fcen, sdt, vol, ccen, stencil, lhs, rhs, patch, dh.value, axis_aligned=not jitter > 0)
+                       fcen, sdt, vol, ccen, stencil, lhs, rhs, patch, dh.value, axis_aligned=not jitter > 0,
+                       mesh_type=3 if jitter > 0 else int(mesh_type), grid=grid,
+                       plateau=(float(plateau_width), float(plateau_slope)))

@@ -45,6 +45,9 @@ typedef struct oracle_case {
     /* state: (u, v, w, rho) per cell incl. ghosts, soln_t1 per cell */
     double *soln, *t1, *grad, *flux, *res, *force, *visc;
     double *cfl, *dtl; /* cfl areas (x, y, z per cell), per-cell step */
+    /* LBFS_IBM_VANDERMONDE4: vertex coordinates and cell-row centroids per axis */
+    double *gv[3], *gc[3];
+    int gn[3];
     double dt;         /* the step's delta_t */
     double resid[4];
     long long t;
@@ -297,10 +300,82 @@ static double ibm_weight(const oracle_case *o, double d) {
     return o->p.ibm_stencil == LBFS_IBM_PESKIN4 ? peskin4(d) : 1 - fabs(d);
 }
 
+/* find_index_closest (immersed_boundary_method.cu:588-630), as written there. */
+static int find_index_closest(const double *arr, int n, double target) {
+    if (target <= arr[0]) return 0;
+    if (target >= arr[n - 1]) return n - 1;
+    int i = 0, j = n, mid = 0;
+    while (i < j) {
+        mid = (i + j) / 2;
+        if (arr[mid] == target) return mid;
+        if (target < arr[mid]) {
+            if (mid > 0 && target > arr[mid - 1]) return (target - arr[mid - 1] >= arr[mid] - target) ? mid : mid - 1;
+            j = mid;
+        } else {
+            if (mid < n - 1 && target < arr[mid + 1]) return (target - arr[mid] >= arr[mid + 1] - target) ? mid + 1 : mid;
+            i = mid + 1;
+        }
+    }
+    return mid;
+}
+
+/* vandemonde_inverse, 4 points (immersed_boundary_method.cu:919-941). */
+static void vandermonde_inverse4(double x, double y, double z, double w, double out[4]) {
+    const double sub_xy = 1 / (x - y), sub_xz = 1 / (x - z), sub_xw = 1 / (x - w);
+    const double sub_yz = 1 / (y - z), sub_yw = 1 / (y - w), sub_zw = 1 / (z - w);
+    out[0] = -1 * y * z * w * sub_xy * sub_xz * sub_xw;
+    out[1] = x * z * w * sub_xy * sub_yz * sub_yw;
+    out[2] = -1 * x * y * w * sub_xz * sub_yz * sub_zw;
+    out[3] = x * y * z * sub_xw * sub_yw * sub_zw;
+}
+
+/* The 4x4x4 stencil of the mesh_type 4 kernels (immersed_boundary_method.cu:
+ * 685-740, 790-840): first cell per axis (closest vertex - 2) and the 1D
+ * weights from the cell-row centroid offsets.  A stencil leaving the mesh
+ * (the reference reads outside its arrays) gets zero weights. */
+static void vandermonde_stencil(const oracle_case *o, const double p[3], int i0[3], double w[3][4]) {
+    for (int a = 0; a < 3; a++) {
+        i0[a] = find_index_closest(o->gv[a], o->gn[a] + 1, p[a]) - 2;
+        if (i0[a] < 0 || i0[a] + 3 >= o->gn[a]) {
+            for (int q = 0; q < 4; q++) w[a][q] = 0.0;
+            continue;
+        }
+        const double *c = o->gc[a] + i0[a];
+        vandermonde_inverse4(c[0] - p[a], c[1] - p[a], c[2] - p[a], c[3] - p[a], w[a]);
+    }
+}
+
+/* interpolate_velocities_on_nodes_non_uniform_grid (immersed_boundary_method.cu:633-758), one node */
+static void interpolate_vandermonde(const oracle_case *o, int n, double v[3]) {
+    const int nx = o->gn[0], ny = o->gn[1];
+    const double p[3] = {o->x[n], o->y[n], o->z[n]};
+    int i0[3];
+    double w[3][4];
+    vandermonde_stencil(o, p, i0, w);
+    for (int i = i0[0]; i <= i0[0] + 3; i++)
+        for (int j = i0[1]; j <= i0[1] + 3; j++)
+            for (int k = i0[2]; k <= i0[2] + 3; k++) {
+                const int idx = i + j * nx + k * ny * nx;
+                if (idx < o->nc && idx >= 0) {
+                    const double weight = w[0][i - i0[0]] * w[1][j - i0[1]] * w[2][k - i0[2]];
+                    for (int c = 0; c < 3; c++) v[c] += o->soln[4 * idx + c] * weight;
+                }
+            }
+}
+
 /* interpolate_velocities_on_nodes + update_node_positions (immersed_boundary_method.cu:14-97, 234-264) */
 static void interpolate_and_move(oracle_case *o) {
     const int nx = (int)(o->m.length[0] / o->m.delta_x), ny = (int)(o->m.length[1] / o->m.delta_x);
     for (int n = 0; n < o->N; n++) {
+        if (o->p.ibm_stencil == LBFS_IBM_VANDERMONDE4) {
+            double v[3] = {0.0, 0.0, 0.0};
+            interpolate_vandermonde(o, n, v);
+            o->vx[n] = v[0]; o->vy[n] = v[1]; o->vz[n] = v[2];
+            o->x[n] += v[0] * o->dt;
+            o->y[n] += v[1] * o->dt;
+            o->z[n] += v[2] * o->dt;
+            continue;
+        }
         double r[3];
         int i0[3], S;
         node_stencil(o, o->x[n], o->y[n], o->z[n], r, i0, &S);
@@ -327,6 +402,25 @@ static void spread(oracle_case *o) {
     const int nx = (int)(o->m.length[0] / o->m.delta_x), ny = (int)(o->m.length[1] / o->m.delta_x);
     const double inv3 = 1 / o->m.delta_x / o->m.delta_x / o->m.delta_x;
     for (int n = 0; n < o->N; n++) {
+        if (o->p.ibm_stencil == LBFS_IBM_VANDERMONDE4) {
+            /* spread_forces_on_non_uniform_grid (immersed_boundary_method.cu:761-872) */
+            const double p[3] = {o->x[n], o->y[n], o->z[n]};
+            int i0[3];
+            double w[3][4];
+            vandermonde_stencil(o, p, i0, w);
+            for (int i = i0[0]; i <= i0[0] + 3; i++)
+                for (int j = i0[1]; j <= i0[1] + 3; j++)
+                    for (int k = i0[2]; k <= i0[2] + 3; k++) {
+                        const int idx = i + j * o->gn[0] + k * o->gn[1] * o->gn[0];
+                        if (idx < o->nc && idx >= 0) {
+                            const double weight = w[0][i - i0[0]] * w[1][j - i0[1]] * w[2][k - i0[2]] / o->vol[idx];
+                            o->force[3 * idx] += o->fx[n] * weight;
+                            o->force[3 * idx + 1] += o->fy[n] * weight;
+                            o->force[3 * idx + 2] += o->fz[n] * weight;
+                        }
+                    }
+            continue;
+        }
         double r[3];
         int i0[3], S;
         node_stencil(o, o->x[n], o->y[n], o->z[n], r, i0, &S);
@@ -645,6 +739,16 @@ oracle_case *oracle_create(const lbfs_mesh_desc *m, const lbfs_params *p, const 
     for (size_t i = 0; i < nc; i++) o->dtl[i] = p->delta_t;
     o->dt = p->delta_t;
     cfl_areas(o);
+    {
+        const double *g[3] = {m->grid_x, m->grid_y, m->grid_z};
+        for (int a = 0; a < 3; a++) {
+            o->gn[a] = (int)(m->length[a] / m->delta_x);
+            const long long stride = a == 0 ? 1 : (a == 1 ? o->gn[0] : (long long)o->gn[0] * o->gn[1]);
+            o->gv[a] = dup(g[a], g[a] ? (o->gn[a] + 1) * sizeof(double) : 0);
+            o->gc[a] = (double *)malloc((o->gn[a] + 1) * sizeof(double));
+            for (int i = 0; i < o->gn[a] && i * stride < o->nc; i++) o->gc[a][i] = m->cell_centroid[3 * (i * stride) + a];
+        }
+    }
     o->n_mem = n_rbc;
     o->mem = (omem *)calloc(n_rbc > 0 ? n_rbc : 1, sizeof(omem));
     for (int r = 0; r < n_rbc; r++) {
@@ -694,7 +798,8 @@ void oracle_free(oracle_case *o) {
     void *ptrs[] = {o->owner, o->neighbour, o->stencil, o->rt, o->vt, o->area, o->normal, o->fcen, o->sdt, o->vol,
                     o->cen, o->lhs, o->rhs, o->bcv, o->soln, o->t1, o->grad, o->flux, o->res, o->force, o->visc, o->mem,
                     o->tri, o->spr, o->x, o->y, o->z, o->vx, o->vy, o->vz, o->fx, o->fy, o->fz, o->contour, o->kspr,
-                    o->curv, o->curv0, o->ang0, o->area0, o->sarea, o->cfl, o->dtl};
+                    o->curv, o->curv0, o->ang0, o->area0, o->sarea, o->cfl, o->dtl, o->gv[0], o->gv[1],
+                    o->gv[2], o->gc[0], o->gc[1], o->gc[2]};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     free(o);
 }

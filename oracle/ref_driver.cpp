@@ -107,15 +107,16 @@ double block_min_max(const double *v, int n, int n_blocks, bool is_min) {
 
 // ---------------------------------------------------------------- mesh ----
 extern "C" void *ref_mesh_create(double X, double Y, double Z, double dt, double ox, double oy, double oz,
-                                 double visc, int gradient_hybrid, const char *outdir) {
+                                 double visc, int gradient_hybrid, const char *outdir, int mesh_type,
+                                 double plateau_width, double plateau_slope) {
     Quiet q;
     RefMesh *m = new RefMesh();
     m->domain.X = X; m->domain.Y = Y; m->domain.Z = Z; m->domain.dt = dt;
     m->domain.dx = 2 * dt; m->domain.dy = 2 * dt; m->domain.dz = 2 * dt;
     m->domain.origin_x = ox; m->domain.origin_y = oy; m->domain.origin_z = oz;
-    m->domain.ref_length = Y; m->domain.plateau_width = 0; m->domain.plateau_slope = 0;
+    m->domain.ref_length = Y; m->domain.plateau_width = plateau_width; m->domain.plateau_slope = plateau_slope;
     m->domain.IBM_face = "none";
-    m->globals.mesh_type = 6;
+    m->globals.mesh_type = mesh_type;
     m->globals.import_format = "openfoam";
     m->globals.import_file = std::string(outdir) + "/no_such_case/";
     m->globals.output_file = outdir;
@@ -178,6 +179,14 @@ extern "C" void ref_mesh_dump(void *h, int *owner, int *neighbour, double *area,
     *delta_h = M.get_delta_h();
 }
 
+// The generator's plateau arrays (Solver_gpu.cu:637-639, mesh_to_array): [nx+1], [ny+1], [nz+1].
+extern "C" void ref_mesh_plateau(void *h, int nx, int ny, int nz, double *out) {
+    unstructured_mesh &M = *((RefMesh *)h)->mesh;
+    for (int i = 0; i < nx + 1; i++) out[i] = M.get_plateau_x(i);
+    for (int i = 0; i < ny + 1; i++) out[nx + 1 + i] = M.get_plateau_y(i);
+    for (int i = 0; i < nz + 1; i++) out[nx + ny + 2 + i] = M.get_plateau_z(i);
+}
+
 extern "C" void ref_mesh_free(void *h) { delete (RefMesh *)h; }
 
 // ----------------------------------------------------------------- RBC ----
@@ -238,6 +247,7 @@ struct RefCase {
     std::vector<double> vol, area, sdt, L[9], res_rho, res_u, res_v, res_w, fx, fy, fz, visc_factor, local_fneq, dtl;
     std::vector<double3> cfl_areas;
     double delta_t = 0;  // the step's delta_t (the loop's variable)
+    std::vector<double> plateau[3];  // mesh_type 4: vertex coordinates per axis (Solver_gpu.cu:637-639)
     double residual_rms[4];
     // RBC
     int n_nodes = 0, n_tets = 0, n_springs = 0;
@@ -318,6 +328,15 @@ extern "C" void *ref_case_create(void *mesh, const ref_params *p, const int *rho
     c->local_fneq.assign(nt, 0.0);
     c->dtl.assign(nc, p->delta_t);
     c->delta_t = p->delta_t;
+    {
+        domain_geometry &D = c->m->domain;
+        const int n[3] = {(int)ceil(D.X / D.dt * 0.5), (int)ceil(D.Y / D.dt * 0.5), (int)ceil(D.Z / D.dt * 0.5)};
+        for (int a = 0; a < 3; a++) {
+            c->plateau[a].resize(n[a] + 1);
+            for (int i = 0; i < n[a] + 1; i++)
+                c->plateau[a][i] = a == 0 ? M.get_plateau_x(i) : (a == 1 ? M.get_plateau_y(i) : M.get_plateau_z(i));
+        }
+    }
     // gpu_solver::populate_cfl_areas (Solver_gpu.cu:1657-1687), restated: the
     // method is a member of the GPU solver class, which is not built here
     c->cfl_areas.assign(nc, make_double3(0, 0, 0));
@@ -401,7 +420,14 @@ extern "C" void ref_case_step(void *h, int n_steps) {
         if (mode == 3) fill_double(nc, c->dtl.data(), delta_t);
         else if (mode == 2) fill_double(nc, c->dtl.data(), p.delta_t);
         c->delta_t = delta_t;
+        const bool plateau_ibm = c->m->globals.mesh_type == 4;  // Solver_gpu.cu:810-820, 899-912
         if (p.has_rbc) {
+            if (plateau_ibm)
+                interpolate_velocities_on_nodes_non_uniform_grid(
+                    c->n_nodes, c->vx.data(), c->vy.data(), c->vz.data(), c->x.data(), c->y.data(), c->z.data(), origin,
+                    lengths, delta_x, c->soln.data(), nc, acos(-1.0), c->ccen.data(), c->vol.data(),
+                    c->plateau[0].data(), c->plateau[1].data(), c->plateau[2].data());
+            else
             interpolate_velocities_on_nodes(c->n_nodes, c->vx.data(), c->vy.data(), c->vz.data(), c->x.data(), c->y.data(),
                                             c->z.data(), origin, lengths, delta_x, c->soln.data(), nc);
             update_node_positions(c->n_nodes, c->vx.data(), c->vy.data(), c->vz.data(), c->x.data(), c->y.data(), c->z.data(),
@@ -429,6 +455,13 @@ extern "C" void ref_case_step(void *h, int n_steps) {
                                                     mxy, mnz, mxz, c->n_nodes, c->visc_factor.data(), M.get_delta_h(),
                                                     acos(-1.0), p.internal_viscosity_ratio, c->n_tets, c->tri.data());
             }
+            if (plateau_ibm)
+                spread_forces_on_non_uniform_grid(c->n_nodes, c->nfx_.data(), c->nfy_.data(), c->nfz_.data(),
+                                                  c->x.data(), c->y.data(), c->z.data(), origin, lengths, delta_x,
+                                                  c->fx.data(), c->fy.data(), c->fz.data(), nc, acos(-1.0),
+                                                  c->ccen.data(), c->vol.data(), c->plateau[0].data(),
+                                                  c->plateau[1].data(), c->plateau[2].data());
+            else
             spread_forces_on_structured_grid(c->n_nodes, c->nfx_.data(), c->nfy_.data(), c->nfz_.data(), c->x.data(),
                                              c->y.data(), c->z.data(), origin, lengths, delta_x, c->fx.data(),
                                              c->fy.data(), c->fz.data(), nc);

@@ -50,7 +50,9 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         vp = ctypes.c_void_p
         L.ref_mesh_create.restype = vp
-        L.ref_mesh_create.argtypes = [ctypes.c_double] * 8 + [ctypes.c_int, ctypes.c_char_p]
+        L.ref_mesh_create.argtypes = [ctypes.c_double] * 8 + [ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                                               ctypes.c_double, ctypes.c_double]
+        L.ref_mesh_plateau.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         L.ref_mesh_counts.argtypes = [vp, ctypes.c_void_p]
         L.ref_mesh_dump.argtypes = [vp] + [ctypes.c_void_p] * 12
         L.ref_mesh_free.argtypes = [vp]
@@ -75,12 +77,15 @@ def _p(a):
 
 
 class RefMesh:
-    """unstructured_mesh (mesh_type 6) + gradients built by the reference code."""
+    """unstructured_mesh (generated: mesh_type 6, 7, 5 or 4) + gradients built by the reference code."""
 
-    def __init__(self, X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, hybrid=False):
+    def __init__(self, X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, hybrid=False, mesh_type=6,
+                 plateau_width=0.0, plateau_slope=0.0):
         self._dir = tempfile.mkdtemp(prefix="refmesh")
+        self.dims = tuple(int(np.ceil(L / dt * 0.5)) for L in (X, Y, Z))
         self.h = lib().ref_mesh_create(X, Y, Z, dt, origin[0], origin[1], origin[2], visc, int(hybrid),
-                                       self._dir.encode())
+                                       self._dir.encode(), int(mesh_type), float(plateau_width),
+                                       float(plateau_slope))
         c = (ctypes.c_int * 8)()
         lib().ref_mesh_counts(self.h, c)
         (self.n_cells, self.n_faces, self.n_interior, self.n_bc, self.n_face_x, self.n_face_y, self.n_face_z,
@@ -96,6 +101,10 @@ class RefMesh:
         dh = ctypes.c_double()
         lib().ref_mesh_dump(self.h, *[_p(a) for a in A.values()], ctypes.byref(dh))
         A["delta_h"] = dh.value
+        nx, ny, nz = self.dims
+        g = np.zeros(nx + ny + nz + 3)
+        lib().ref_mesh_plateau(self.h, nx, ny, nz, _p(g))
+        A["plateau"] = g
         return A
 
 

@@ -13,6 +13,7 @@ Each fixture stores its inputs as well as the reference's outputs, so the
 tests replay them without the reference.
 """
 import os
+import subprocess
 import sys
 from dataclasses import replace
 
@@ -29,7 +30,8 @@ from lbfs_b200 import _abi, cases, icosphere  # noqa: E402
 
 def ref_case(c):
     m = c.mesh
-    rm = R.RefMesh(m.X, m.Y, m.Z, m.dt, m.origin, c.params.visc)
+    rm = R.RefMesh(m.X, m.Y, m.Z, m.dt, m.origin, c.params.visc, mesh_type=m.mesh_type, plateau_width=m.plateau[0],
+                   plateau_slope=m.plateau[1])
     p = R.RefParams()
     sp = c.params
     p.visc, p.delta_t, p.gamma_inv, p.channel_diameter = sp.visc, sp.delta_t, sp.gamma_inv, sp.channel_diameter
@@ -53,10 +55,13 @@ def ref_case(c):
     return rc
 
 
-def mesh_fixture(name, X, Y, Z, hybrid=False):
-    rm = R.RefMesh(X, Y, Z, 1.0, (0.0, 0.0, 0.0), 0.1, hybrid)
+def mesh_fixture(name, X, Y, Z, hybrid=False, mesh_type=6, plateau=(0.0, 0.0)):
+    rm = R.RefMesh(X, Y, Z, 1.0, (0.0, 0.0, 0.0), 0.1, hybrid, mesh_type, *plateau)
     arrays = rm.arrays()
-    np.savez_compressed(os.path.join(HERE, name), X=X, Y=Y, Z=Z, hybrid=int(hybrid),
+    if mesh_type != 4:
+        arrays.pop("plateau")
+    np.savez_compressed(os.path.join(HERE, name), X=X, Y=Y, Z=Z, hybrid=int(hybrid), mesh_type=mesh_type,
+                        plateau_params=np.array(plateau),
                         counts=np.array([rm.n_cells, rm.n_faces, rm.n_interior, rm.n_bc, rm.n_face_x, rm.n_face_y,
                                          rm.n_face_z, rm.total_cells]), **arrays)
 
@@ -66,6 +71,11 @@ def spring_fixture(name, level):
     nodes = unit * 8.0
     spr, tri, xyz = R.ref_springs(nodes, tris, (10.0, 20.0, 30.0))
     np.savez_compressed(os.path.join(HERE, name), nodes=nodes, tris=tris, ref_springs=spr, ref_tris=tri, ref_xyz=xyz)
+
+
+def plateau_case():
+    return cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_VANDERMONDE4, mesh_type=4,
+                           plateau=(5.0, 0.3))
 
 
 def step_fixture(name, case, steps):
@@ -97,6 +107,10 @@ def main():
         sys.exit("oracle/_ref/libref_lbfs.so is missing: run oracle/build_ref.sh first")
     mesh_fixture("mesh_4x3x5.npz", 8.0, 6.0, 10.0)
     mesh_fixture("mesh_6x6x6_hybrid.npz", 12.0, 12.0, 12.0, hybrid=True)
+    # the generator's other rectilinear meshes: cosine in x, y, z (5), cosine in x, y (7); the plateau
+    # mesh (4) in a process of its own, below
+    mesh_fixture("mesh_cosine5_8x6x5.npz", 16.0, 12.0, 10.0, mesh_type=5)
+    mesh_fixture("mesh_cosine7_8x6x5.npz", 16.0, 12.0, 10.0, mesh_type=7)
     spring_fixture("springs_L1.npz", 1)
     spring_fixture("springs_L2.npz", 2)
     spring_fixture("springs_L3.npz", 3)
@@ -111,8 +125,33 @@ def main():
     c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
     c.params = replace(c.params, time_stepping=_abi.LBFS_DT_MIN)
     step_fixture("step_shear_rbc_16_min.npz", c, 10)
+    subprocess.run([sys.executable, os.path.abspath(__file__), "--plateau"], check=True)
     print("golden fixtures written to", HERE)
 
 
+def plateau_fixtures():
+    """The plateau mesh (mesh_type 4) and a step on it with the 4x4x4 Vandermonde IBM.
+
+    create_uniform_openfoam_mesh initialises plateau_sum_x but not plateau_sum_y
+    and plateau_sum_z (unstructured_mesh.cpp:296-317), so the reference's y and z
+    plateau arrays depend on what those reads return.  This runs in a fresh
+    process (where they read 0, the value plateau_sum_x starts from) and checks
+    that every plateau array ends at the domain length before writing."""
+    rm = R.RefMesh(20.0, 16.0, 12.0, 1.0, (0.0, 0.0, 0.0), 0.1, False, 4, 2.0, 0.6)
+    pl = rm.arrays()["plateau"]
+    ends = np.cumsum([11, 9, 7]) - 1
+    if not np.allclose(pl[ends], (20.0, 16.0, 12.0), rtol=0, atol=1e-9):
+        sys.exit("the reference's plateau sums were not zero-initialised in this process; not writing fixtures")
+    mesh_fixture("mesh_plateau_10x8x6.npz", 20.0, 16.0, 12.0, mesh_type=4, plateau=(2.0, 0.6))
+    c = plateau_case()
+    g = R.RefMesh(c.mesh.X, c.mesh.Y, c.mesh.Z, 1.0, (0.0, 0.0, 0.0), c.params.visc, False, 4, *c.mesh.plateau)
+    if not np.array_equal(g.arrays()["plateau"], np.concatenate(c.mesh.grid)):
+        sys.exit("plateau arrays of the step case differ from the builder's; not writing fixtures")
+    step_fixture("step_plateau_rbc_16.npz", c, 10)
+
+
 if __name__ == "__main__":
-    main()
+    if "--plateau" in sys.argv:
+        plateau_fixtures()
+    else:
+        main()

@@ -31,6 +31,11 @@ def fixture_case(golden, name):
     g = golden(name)
     if "poiseuille" in name:
         c = cases.poiseuille(n=6, ny=5, nz=4)
+    elif "plateau" in name:
+        c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_VANDERMONDE4, mesh_type=4,
+                            plateau=(5.0, 0.3))
+        mb = c.membranes[0]
+        mb.xyz_stress_free, mb.xyz_initial = g["xyz_stress_free"], g["xyz_initial"]
     else:
         c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
         mb = c.membranes[0]
@@ -42,7 +47,7 @@ def fixture_case(golden, name):
 
 
 FIXTURES = ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz", "step_poiseuille_6x5x4_local.npz",
-            "step_poiseuille_6x5x4_talts.npz", "step_shear_rbc_16_min.npz"]
+            "step_poiseuille_6x5x4_talts.npz", "step_shear_rbc_16_min.npz", "step_plateau_rbc_16.npz"]
 
 
 @pytest.mark.parametrize("name", FIXTURES)

@@ -6,12 +6,18 @@ import pytest
 from lbfs_b200 import build_springs, build_uniform_mesh, icosphere, uniform_counts
 
 
-@pytest.mark.parametrize("name", ["mesh_4x3x5.npz", "mesh_6x6x6_hybrid.npz"])
+@pytest.mark.parametrize("name", ["mesh_4x3x5.npz", "mesh_6x6x6_hybrid.npz", "mesh_plateau_10x8x6.npz",
+                                  "mesh_cosine5_8x6x5.npz", "mesh_cosine7_8x6x5.npz"])
 def test_uniform_mesh_bit_exact(golden, name):
     g = golden(name)
     X, Y, Z, hybrid = float(g["X"]), float(g["Y"]), float(g["Z"]), int(g["hybrid"])
+    mesh_type, plateau = int(g["mesh_type"]), tuple(float(x) for x in g["plateau_params"])
     assert uniform_counts(X, Y, Z, 1.0) == list(g["counts"])
-    m = build_uniform_mesh(X, Y, Z, 1.0, visc=0.1, gradient="hybrid" if hybrid else "LS")
+    m = build_uniform_mesh(X, Y, Z, 1.0, visc=0.1, gradient="hybrid" if hybrid else "LS", mesh_type=mesh_type,
+                           plateau_width=plateau[0], plateau_slope=plateau[1])
+    if mesh_type == 4:
+        # the plateau arrays the 4x4x4 IBM stencil searches (plateau_x, _y, _z)
+        assert np.array_equal(np.concatenate(m.grid), g["plateau"])
     mine = dict(owner=m.owner, neighbour=m.neighbour, face_area=m.face_area, face_normal=m.face_normal,
                 face_centroid=m.face_centroid, streaming_dt=m.streaming_dt, cell_volume=m.cell_volume,
                 cell_centroid=m.cell_centroid, gradient_stencil=m.gradient_stencil, lhs_inverse=m.lhs_inverse,
