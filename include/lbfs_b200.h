@@ -134,6 +134,11 @@ typedef struct lbfs_params {
      * minimum. */
     int32_t time_stepping;
     double pre_conditioned_gamma; /* globals.pre_conditioned_gamma (get_cfl_device); 0 = 1 / gamma_inv */
+    /* globals.preconditioning_active: the lattice equilibria of the general-normal
+     * and boundary faces take the 1/gamma factor (populate_feq, LBFS.cu:940-1036,
+     * chosen at LBFS.cu:2637-2647); the interface equilibria and relaxation take
+     * gamma_inv in any case. */
+    int32_t preconditioning;
 } lbfs_params;
 
 #define LBFS_DT_LOCAL 1

@@ -345,7 +345,7 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
     const R thr = R(0.001) * dt;
     Moments<R> M;
     moments_init(M);
-    moments_add(M, 0, feq_dev<R>(0, p0[0], p0[1], p0[2], p0[3], a.rho0, R(1)), -1);
+    moments_add(M, 0, feq_dev<R>(0, p0[0], p0[1], p0[2], p0[3], a.rho0, a.recon_q), -1);
 #pragma unroll
     for (int k = 1; k < 15; k += 2) {
         const Dir e = dir_of(k);
@@ -371,7 +371,7 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
                 }
                 L[m] = val;
             }
-            moments_add(M, kk, feq_dev<R>(kk, L[0], L[1], L[2], L[3], a.rho0, R(1)), -1);
+            moments_add(M, kk, feq_dev<R>(kk, L[0], L[1], L[2], L[3], a.rho0, a.recon_q), -1);
         }
     }
     const R vf = is_bc ? R(1) : a.visc_factor[oc.x];

@@ -121,6 +121,7 @@ template <typename R> struct FluidArgs {
     int testcase;
     R rho0;          // density offset of the stored state (0 in FP64)
     R gamma_inv, visc;
+    R recon_q;       // quadratic factor of the general-face lattice equilibria: gamma_inv when preconditioning, else 1
     double delta_t, H2, H4;
     double force[3];
     // state and gradients

@@ -161,6 +161,7 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     a.testcase = p.testcase;
     a.rho0 = (R)rho0;
     a.gamma_inv = (R)p.gamma_inv;
+    a.recon_q = p.preconditioning ? (R)p.gamma_inv : R(1);
     a.visc = (R)p.visc;
     a.delta_t = p.delta_t;
     a.H2 = p.channel_diameter * 0.5;
@@ -1310,7 +1311,8 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     if (!s || !obj || !J || !grad || n_steps < 1 || checkpoint_every < 1)
         return set_error(LBFS_ERR_ARG, "lbfs_adjoint: bad arguments");
     if (s->fp32) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: FP64 handles only");
-    if (s->params.gamma_inv != 1.0) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: no preconditioning");
+    if (s->params.gamma_inv != 1.0 || s->params.preconditioning)
+        return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: no preconditioning");
     if (dynamic_dt(s->params))
         return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: constant time stepping only");
     if (s->params.ibm_stencil == LBFS_IBM_VANDERMONDE4 && s->n_membranes > 0)

@@ -41,10 +41,6 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
                                              domain_geometry &domain, initial_conditions &init_conds,
                                              unstructured_bcs &quad_bcs_orig, int mg, Solution &residual, int fmg,
                                              post_processing &pp, std::vector<lagrangian_object> &object_vec) {
-    if (globals.preconditioning_active) {
-        std::fprintf(stderr, "lbfs_b200: preconditioning must be off\n");
-        std::exit(-1);
-    }
     const int nc = Mesh.get_n_cells(), nf = Mesh.get_n_faces(), ni = Mesh.get_n_neighbours();
     const int nb = Mesh.get_num_bc(), nt = Mesh.get_total_cells();
 
@@ -96,6 +92,18 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
     md.length[0] = domain.X; md.length[1] = domain.Y; md.length[2] = domain.Z;
     md.delta_x = domain.dt * 2;
     md.delta_h = Mesh.get_delta_h();
+    // plateau meshes: the vertex coordinates the 4x4x4 IBM searches (Solver_gpu.cu:497-499, 637-639)
+    std::vector<double> plateau[3];
+    if (globals.mesh_type == 4) {
+        const double len[3] = {domain.X, domain.Y, domain.Z};
+        for (int a = 0; a < 3; a++) {
+            const int n = (int)std::ceil(len[a] / domain.dt * 0.5) + 1;
+            plateau[a].resize(n);
+            for (int i = 0; i < n; i++)
+                plateau[a][i] = a == 0 ? Mesh.get_plateau_x(i) : (a == 1 ? Mesh.get_plateau_y(i) : Mesh.get_plateau_z(i));
+        }
+        md.grid_x = plateau[0].data(); md.grid_y = plateau[1].data(); md.grid_z = plateau[2].data();
+    }
 
     lbfs_params p = {};
     p.visc = globals.visc;
@@ -111,11 +119,13 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
     p.visc_factor_initial = globals.testcase == 2 ? 1.0 : 0.0;
     p.testcase = globals.testcase;
     p.precision = LBFS_FP64;
-    p.ibm_stencil = LBFS_IBM_HAT2;
+    // interpolate_velocities_on_nodes(_non_uniform_grid), Solver_gpu.cu:810-820
+    p.ibm_stencil = globals.mesh_type == 4 ? LBFS_IBM_VANDERMONDE4 : LBFS_IBM_HAT2;
     p.viscosity_period = 10000;
     // local = 1, constant = 2, min = 3, talts = 4 (global_variables.h:59)
     p.time_stepping = globals.gpu_time_stepping;
     p.pre_conditioned_gamma = globals.pre_conditioned_gamma;
+    p.preconditioning = globals.preconditioning_active ? 1 : 0;
 
     // membranes (Solver_gpu.cu:659-735): sprIdx / sorted_triIdx / stress-free
     // coordinates, then the initial mesh read over the node arrays

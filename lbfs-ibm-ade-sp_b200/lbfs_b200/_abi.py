@@ -89,6 +89,7 @@ class Params(ctypes.Structure):
         ("testcase", ctypes.c_int32), ("precision", ctypes.c_int32), ("ibm_stencil", ctypes.c_int32),
         ("viscosity_period", ctypes.c_int32),
         ("time_stepping", ctypes.c_int32), ("pre_conditioned_gamma", ctypes.c_double),
+        ("preconditioning", ctypes.c_int32),
     ]
 
 

@@ -33,6 +33,7 @@ class StepParams:
     viscosity_period: int = 10000
     time_stepping: int = _abi.LBFS_DT_CONSTANT
     pre_conditioned_gamma: float = 0.0  # 0: 1 / gamma_inv
+    preconditioning: int = 0             # globals.preconditioning_active
 
     def to_c(self):
         p = _abi.Params()
@@ -44,6 +45,7 @@ class StepParams:
         p.testcase, p.precision, p.ibm_stencil = self.testcase, self.precision, self.ibm_stencil
         p.viscosity_period = self.viscosity_period
         p.time_stepping, p.pre_conditioned_gamma = self.time_stepping, self.pre_conditioned_gamma
+        p.preconditioning = self.preconditioning
         return p
 
 

@@ -267,7 +267,9 @@ static void general_face(oracle_case *o, int f, int is_bc) {
         }
     }
     double fl[15];
-    for (int k = 0; k < 15; k++) fl[k] = feq(k, L[k][0], L[k][1], L[k][2], L[k][3], 1.0);
+    /* populate_feq with 1/gamma when preconditioning, else the explicit form (LBFS.cu:2637-2647) */
+    const double q = o->p.preconditioning ? o->p.gamma_inv : 1.0;
+    for (int k = 0; k < 15; k++) fl[k] = feq(k, L[k][0], L[k][1], L[k][2], L[k][3], q);
     const double vf = is_bc ? 1.0 : o->visc[i];
     const double tau = (o->p.testcase == 8) ? 0.0 : (o->p.visc * vf * 3 / dt * o->p.gamma_inv);
     flux_from_lattice(fl, tau, o->p.gamma_inv, o->area[f], -1, n, o->flux + 4 * f);

@@ -234,6 +234,7 @@ struct ref_params {
     int viscosity_period;  // update_viscosities when t % period == 1
     int time_stepping;     // globals.gpu_time_stepping: 1 local, 2 constant, 3 min, 4 talts (0 = 2)
     double pre_conditioned_gamma;  // get_cfl_device's gamma (0 = 1 / gamma_inv)
+    int preconditioning;           // globals.preconditioning_active
 };
 
 namespace {
@@ -498,7 +499,7 @@ extern "C" void ref_case_step(void *h, int n_steps) {
                           c->ccen.data(), c->fcen.data(), c->fnorm.data(), c->sdt.data(), c->g_rho.data(), c->g_u.data(),
                           c->g_v.data(), c->g_w.data(), nc, p.gamma_inv, c->local_fneq.data(), p.visc, c->res_rho.data(),
                           c->res_u.data(), c->res_v.data(), c->res_w.data(), c->res_face.data(), c->rho_type.data(),
-                          c->vel_type.data(), c->bcs_arr.data(), acos(-1.0), c->nn, p.testcase, false);
+                          c->vel_type.data(), c->bcs_arr.data(), acos(-1.0), c->nn, p.testcase, p.preconditioning != 0);
         add_face_flux_to_cell(c->nf, c->res_face.data(), c->vol.data(), c->owner.data(), c->neighbour.data(),
                               c->res_rho.data(), c->res_u.data(), c->res_v.data(), c->res_w.data());
         add(nc, c->res_u.data(), c->fx.data());

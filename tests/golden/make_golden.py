@@ -39,6 +39,7 @@ def ref_case(c):
     p.ref_rho, p.max_velocity, p.testcase = sp.ref_rho, sp.max_velocity, sp.testcase
     p.visc_factor_initial, p.viscosity_period = sp.visc_factor_initial, sp.viscosity_period
     p.time_stepping, p.pre_conditioned_gamma = sp.time_stepping, sp.pre_conditioned_gamma
+    p.preconditioning = sp.preconditioning
     p.has_rbc = 1 if c.membranes else 0
     if c.membranes:
         mb = c.membranes[0]
@@ -89,7 +90,8 @@ def step_fixture(name, case, steps):
     out.update(s1_grad=rc.get(R.REF_GRAD), s1_flux=rc.get(R.REF_RES_FACE), s1_res=rc.get(R.REF_RES),
                s1_force=rc.get(R.REF_FORCE), s1_ghost=rc.get(R.REF_GHOST), s1_t1=rc.get(R.REF_T1),
                s1_state=np.stack(rc.state()), s1_resid=rc.get(R.REF_RESID), time_stepping=case.params.time_stepping,
-               s1_dtl=rc.get(R.REF_DT_LOCAL), s1_dt=rc.get(R.REF_DELTA_T)[0])
+               s1_dtl=rc.get(R.REF_DT_LOCAL), s1_dt=rc.get(R.REF_DELTA_T)[0], gamma_inv=case.params.gamma_inv,
+               preconditioning=case.params.preconditioning)
     if case.membranes:
         out.update(s1_nodes_x=rc.get(R.REF_NODE_X), s1_nodes_v=rc.get(R.REF_NODE_V), s1_nodes_f=rc.get(R.REF_NODE_F),
                    s1_totals=rc.get(R.REF_TOTALS), s1_visc=rc.get(R.REF_VISC), s1_spring=rc.get(R.REF_SPRING))
@@ -125,6 +127,11 @@ def main():
     c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
     c.params = replace(c.params, time_stepping=_abi.LBFS_DT_MIN)
     step_fixture("step_shear_rbc_16_min.npz", c, 10)
+    # preconditioning: gamma = 2 in the relaxation, the interface and the
+    # boundary faces' lattice equilibria, with local time stepping
+    c = cases.poiseuille(n=6, ny=5, nz=4)
+    c.params = replace(c.params, gamma_inv=0.5, preconditioning=1, time_stepping=_abi.LBFS_DT_LOCAL)
+    step_fixture("step_poiseuille_6x5x4_precond.npz", c, 20)
     subprocess.run([sys.executable, os.path.abspath(__file__), "--plateau"], check=True)
     print("golden fixtures written to", HERE)
 

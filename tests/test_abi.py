@@ -35,7 +35,7 @@ def test_structs_match_header_sizes():
     from lbfs_b200 import _abi
     assert ctypes.sizeof(_abi.MeshDesc) == 8 * 4 + 14 * 8 + 8 * 8 + 8 + 8 + 3 * 8
     assert ctypes.sizeof(_abi.GridDesc) == 8 + 8 * 8
-    assert ctypes.sizeof(_abi.Params) == 4 * 8 + 3 * 8 + 4 * 8 + 4 * 4 + 8 + 8  # time_stepping (+ padding), gamma
+    assert ctypes.sizeof(_abi.Params) == 4 * 8 + 3 * 8 + 4 * 8 + 4 * 4 + 8 + 8 + 8  # time stepping, gamma, precond.
     assert ctypes.sizeof(_abi.RbcDesc) == 16 + 4 * 8 + 13 * 8 + 8 + 8
 
 

@@ -42,12 +42,14 @@ def fixture_case(golden, name):
         mb.xyz_stress_free, mb.xyz_initial = g["xyz_stress_free"], g["xyz_initial"]
     c.rho, c.u, c.v, c.w = g["rho0"], g["u0"], g["v0"], g["w0"]
     if "time_stepping" in g.files:
-        c.params = replace(c.params, time_stepping=int(g["time_stepping"]))
+        c.params = replace(c.params, time_stepping=int(g["time_stepping"]), gamma_inv=float(g["gamma_inv"]),
+                           preconditioning=int(g["preconditioning"]))
     return c, g
 
 
 FIXTURES = ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz", "step_poiseuille_6x5x4_local.npz",
-            "step_poiseuille_6x5x4_talts.npz", "step_shear_rbc_16_min.npz", "step_plateau_rbc_16.npz"]
+            "step_poiseuille_6x5x4_talts.npz", "step_shear_rbc_16_min.npz", "step_plateau_rbc_16.npz",
+            "step_poiseuille_6x5x4_precond.npz"]
 
 
 @pytest.mark.parametrize("name", FIXTURES)

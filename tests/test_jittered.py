@@ -120,3 +120,25 @@ def test_jittered_time_stepping_matches_oracle(mode):
     assert rel_err(dtl, want) <= FP64_RTOL and rel_err(dt, o.time_step()) <= FP64_RTOL
     if mode == "local":
         assert np.ptp(want) > 1e-3 * np.mean(want)  # the steps do vary from cell to cell
+
+
+@pytest.mark.gpu
+def test_jittered_preconditioning_matches_oracle():
+    """Preconditioning (gamma = 2) where every face takes the general-normal
+    flux: the lattice equilibria of all faces carry 1/gamma."""
+    from dataclasses import replace
+    from lbfs_b200 import GpuSolver, cases
+    from oracle_lbfs import OracleSolver
+    c = cases.poiseuille(n=8, ny=6, nz=5)
+    c.params = replace(c.params, gamma_inv=0.5, preconditioning=1)
+    m = _mesh(0.1)
+    m.set_boundaries(c.bcs)
+    with GpuSolver(m, c.params) as s:
+        s.set_state(c.rho, c.u, c.v, c.w)
+        s.step(10)
+        got = s.state()
+    o = OracleSolver(m, c.params, [])
+    o.set_state(c.rho, c.u, c.v, c.w)
+    o.step(10)
+    for a, b in zip(got, o.state()):
+        assert rel_err(a, b) <= FP64_RTOL
