@@ -366,19 +366,46 @@ int lbfs_mesh_build_rectilinear(double X, double Y, double Z, double dt, const d
 /* The same mesh with every interior vertex moved by a seeded uniform
  * perturbation of up to `jitter` (< 0.25) times the cell spacing per axis
  * (boundary vertices stay, so the box and its patches stay).  Faces are then
- * non-planar quadrilaterals and normals general: a stand-in for the imported
- * (mesh_type 3) meshes the reference reads through its OpenFOAM importer
- * (unstructured_mesh.cpp:705-869), with the same geometry and gradient
- * formulas except one: a face's area is the length of the sum of its two
- * triangles' vector areas (the reference sums their lengths, which on a
- * warped face makes the vector areas of a cell's faces fail to close, so a
- * fluid at rest starts to move).  Step it with axis_aligned = 0. */
+ * non-planar quadrilaterals and normals general, as in the imported
+ * (mesh_type 3) meshes; step it with axis_aligned = 0.  closed_faces = 0
+ * gives exactly the geometry the reference's importer forms from this mesh
+ * written as a polyMesh (lbfs_mesh_write_openfoam): a face's area is the sum
+ * of its two triangles' areas, which on a warped face makes the vector areas
+ * of a cell's faces fail to close, so a fluid at rest starts to move.
+ * closed_faces = 1 uses the length of the face's vector area instead (the
+ * faces of every cell close; the one deviation from the reference's
+ * formulas). */
 int lbfs_mesh_build_jittered(double X, double Y, double Z, double dt, const double *origin, double visc,
-                             double fneq_min, int32_t gradient_hybrid, double jitter, uint64_t seed, int32_t *owner,
-                             int32_t *neighbour, double *face_area, double *face_normal, double *face_centroid,
-                             double *streaming_dt, double *cell_volume, double *cell_centroid,
-                             int32_t *gradient_stencil, double *lhs_inverse, double *rhs, int32_t *bc_patch,
-                             double *delta_h);
+                             double fneq_min, int32_t gradient_hybrid, double jitter, uint64_t seed,
+                             int32_t closed_faces, int32_t *owner, int32_t *neighbour, double *face_area,
+                             double *face_normal, double *face_centroid, double *streaming_dt, double *cell_volume,
+                             double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse, double *rhs,
+                             int32_t *bc_patch, double *delta_h);
+
+/* OpenFOAM polyMesh.  lbfs_mesh_write_openfoam writes the generator's mesh
+ * (mesh_type 4-7, or 6 with jitter) as <dir>/points, faces, owner, neighbour
+ * and boundary (ASCII; patches left, right, bottom, top, back, front; the
+ * owner file's 13th line carries the note the reference's importer reads).
+ * lbfs_mesh_openfoam_counts reads the sizes: counts[6] = n_points, n_cells,
+ * n_faces, n_internal_faces, n_boundary_faces, n_patches.
+ * lbfs_mesh_import_openfoam reads a polyMesh as unstructured_mesh::
+ * import_openfoam_mesh and import_openfoam_BC_tags do (unstructured_mesh.cpp:
+ * 670-941, 2533-2608: the header note, lists between a line starting with "("
+ * and one starting with ")", points read as float, faces "4(a b c d)") and
+ * forms the geometry and least-squares matrices with the same code as the
+ * generated meshes (generate_internal_mesh); hexahedral cells only.  bc_patch
+ * is each boundary face's patch index in the boundary file, names the patch
+ * names separated by newlines.  The imported mesh steps with axis_aligned = 0
+ * (mesh_type 3). */
+int lbfs_mesh_write_openfoam(const char *dir, double X, double Y, double Z, double dt, const double *origin,
+                             int32_t mesh_type, double plateau_width, double plateau_slope, double jitter,
+                             uint64_t seed);
+int lbfs_mesh_openfoam_counts(const char *dir, int32_t *counts);
+int lbfs_mesh_import_openfoam(const char *dir, double visc, double fneq_min, int32_t gradient_hybrid,
+                              int32_t closed_faces, int32_t *owner, int32_t *neighbour, double *face_area,
+                              double *face_normal, double *face_centroid, double *streaming_dt, double *cell_volume,
+                              double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse, double *rhs,
+                              int32_t *bc_patch, char *names, int32_t names_len);
 
 /* Spring connectivity of a closed triangulated membrane, in the order the
  * reference's Osay reader produces it (lagrangian_object.cpp:238-481).

@@ -9,7 +9,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
 #include <limits>
 #include <unordered_set>
 #include <vector>
@@ -84,13 +88,15 @@ struct VertexSpec {
     double plateau_slope = 0.0;  // domain.plateau_slope (mesh_type 4)
     double jitter = 0.0;
     uint64_t seed = 0;
+    bool closed_faces = true;    // jittered faces: vector areas (true) or the reference's triangle sums
 };
 
 int build_mesh(double X, double Y, double Z, double dt, const double *origin, double visc, double fneq_min,
                int32_t gradient_hybrid, const VertexSpec &vs, int32_t *owner, int32_t *neighbour,
                double *face_area, double *face_normal, double *face_centroid, double *streaming_dt,
                double *cell_volume, double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse,
-               double *rhs, int32_t *bc_patch, double *delta_h, double *grid_xyz);
+               double *rhs, int32_t *bc_patch, double *delta_h, double *grid_xyz,
+               std::vector<float> *verts_out = nullptr, std::vector<int> *faces_out = nullptr);
 
 }  // namespace
 
@@ -126,15 +132,16 @@ extern "C" int lbfs_mesh_build_rectilinear(double X, double Y, double Z, double 
 
 extern "C" int lbfs_mesh_build_jittered(double X, double Y, double Z, double dt, const double *origin, double visc,
                                         double fneq_min, int32_t gradient_hybrid, double jitter, uint64_t seed,
-                                        int32_t *owner, int32_t *neighbour, double *face_area, double *face_normal,
-                                        double *face_centroid, double *streaming_dt, double *cell_volume,
-                                        double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse,
-                                        double *rhs, int32_t *bc_patch, double *delta_h) {
+                                        int32_t closed_faces, int32_t *owner, int32_t *neighbour, double *face_area,
+                                        double *face_normal, double *face_centroid, double *streaming_dt,
+                                        double *cell_volume, double *cell_centroid, int32_t *gradient_stencil,
+                                        double *lhs_inverse, double *rhs, int32_t *bc_patch, double *delta_h) {
     if (!(jitter >= 0.0 && jitter < 0.25))
         return lbfs::set_error(LBFS_ERR_ARG, "jitter must be in [0, 0.25) of the cell spacing");
     VertexSpec vs;
     vs.jitter = jitter;
     vs.seed = seed;
+    vs.closed_faces = closed_faces != 0;
     return build_mesh(X, Y, Z, dt, origin, visc, fneq_min, gradient_hybrid, vs, owner, neighbour,
                       face_area, face_normal, face_centroid, streaming_dt, cell_volume, cell_centroid,
                       gradient_stencil, lhs_inverse, rhs, bc_patch, delta_h, nullptr);
@@ -164,11 +171,181 @@ std::vector<double> axis_vertices(int mesh_type, bool clustered, int n, double o
     return v;
 }
 
+// Geometry and least-squares matrices of a hex mesh given as float vertices,
+// quadrilateral faces (4 vertex ids each, winding giving the owner -> neighbour
+// normal), owner and neighbour (boundary faces: any neighbour, replaced by
+// the ghost cell n_cells + f - n_interior): unstructured_mesh::
+// generate_internal_mesh (unstructured_mesh.cpp:1592-1692), tet_volume
+// (:1015-1040), cell_tet_area (:1170-1204), calc_face_delta_t (:1349-1446),
+// populate_ghost_cell_from_foam_face (:1963-1996) and gradients::
+// pre_fill_LHS_and_RHS_matrix (gradients.cpp:214-315).  closed_faces: a
+// face's area is the length of its vector area (see lbfs_mesh_build_jittered)
+// instead of the reference's sum of its triangles' areas.
+int mesh_geometry(int nc, int nf, int ni, const float *vx, const float *vy, const float *vz, const int *fv,
+                  int32_t *owner, int32_t *neighbour, double visc, double fneq_min, int32_t gradient_hybrid,
+                  bool closed_faces, double *face_area, double *face_normal, double *face_centroid,
+                  double *streaming_dt, double *cell_volume, double *cell_centroid, int32_t *gradient_stencil,
+                  double *lhs_inverse, double *rhs) {
+    const int nt = nc + (nf - ni);
+    // Geometry: unstructured_mesh::generate_internal_mesh (unstructured_mesh.cpp:1592-1692),
+    // tet_volume (:1015-1040), cell_tet_area (:1170-1204), calc_face_delta_t (:1349-1446).
+    std::vector<double> cvol(nt, 0.0), csum_area(nt, 0.0), cx(nt, 0.0), cy(nt, 0.0), cz(nt, 0.0);
+    std::vector<std::vector<int>> gcells(nt), gfaces(nt);
+    const double reference_dt = visc * 3 / 1.0 / fneq_min;  // pre_conditioned_gamma = 1
+    for (int f = 0; f < nf; f++) {
+        V3 nd[4];
+        for (int q = 0; q < 4; q++) {
+            int t = fv[4 * f + q];
+            nd[q] = {(double)vx[t], (double)vy[t], (double)vz[t]};
+        }
+        for (int t = 0; t < 2; t++) {
+            V3 a = nd[0], b = sub(nd[t + 1], a), c = sub(nd[t + 2], a);
+            double vol = dot(a, cross(b, c)) / 6;
+            cvol[owner[f]] = cvol[owner[f]] + vol;
+            if (f < ni) cvol[neighbour[f]] = cvol[neighbour[f]] - vol;
+        }
+        double area_f = 0.0;
+        V3 fcen = {0, 0, 0}, fnorm = {0, 0, 0};
+        for (int t = 0; t < 2; t++) {
+            V3 a = nd[0], b = nd[t + 1], c = nd[t + 2];
+            V3 cen = {(a.x + b.x + c.x) / 3, (a.y + b.y + c.y) / 3, (a.z + b.z + c.z) / 3};
+            V3 n = cross(sub(b, a), sub(c, a));
+            double ar = 0.5 * mag(n);
+            area_f = area_f + ar;
+            double inv = 1 / ar;  // vector_var::factor divides by its argument
+            cen = {cen.x / inv, cen.y / inv, cen.z / inv};
+            fcen = add(fcen, cen);
+            fnorm = add(fnorm, n);
+        }
+        // Warped faces: the face's vector area is the sum of its triangles'
+        // vector areas, |N1 + N2| / 2 along (N1 + N2).  The reference's scalar
+        // sum |N1| / 2 + |N2| / 2 (kept for the area-weighted centroids) is
+        // longer whenever N1 and N2 are not parallel, so the vector areas of a
+        // cell's faces would not close and a fluid at rest would be pushed by
+        // its own pressure.
+        face_area[f] = closed_faces ? 0.5 * mag(fnorm) : area_f;
+        csum_area[owner[f]] = csum_area[owner[f]] + area_f;
+        cx[owner[f]] = cx[owner[f]] + fcen.x;
+        cy[owner[f]] = cy[owner[f]] + fcen.y;
+        cz[owner[f]] = cz[owner[f]] + fcen.z;
+        face_centroid[3 * f] = fcen.x / area_f;
+        face_centroid[3 * f + 1] = fcen.y / area_f;
+        face_centroid[3 * f + 2] = fcen.z / area_f;
+        double nm = mag(fnorm);
+        face_normal[3 * f] = fnorm.x / nm;
+        face_normal[3 * f + 1] = fnorm.y / nm;
+        face_normal[3 * f + 2] = fnorm.z / nm;
+        double face_dt = 0.5 * std::sqrt(area_f);
+        streaming_dt[f] = std::min(face_dt, reference_dt);
+        if (f > ni - 1) {
+            int g = f - ni + nc;
+            gcells[owner[f]].push_back(g);
+            gfaces[owner[f]].push_back(f);
+        } else {
+            int nb = neighbour[f];
+            csum_area[nb] = csum_area[nb] + area_f;
+            cx[nb] = cx[nb] + fcen.x;
+            cy[nb] = cy[nb] + fcen.y;
+            cz[nb] = cz[nb] + fcen.z;
+            gcells[owner[f]].push_back(nb);
+            gcells[nb].push_back(owner[f]);
+            gfaces[owner[f]].push_back(f);
+            gfaces[nb].push_back(f);
+        }
+    }
+    for (int i = 0; i < nc; i++) {
+        cx[i] = cx[i] / csum_area[i];
+        cy[i] = cy[i] / csum_area[i];
+        cz[i] = cz[i] / csum_area[i];
+    }
+    // ghost centroids: populate_ghost_cell_from_foam_face, unstructured_mesh.cpp:1963-1996
+    for (int f = ni; f < nf; f++) {
+        int g = nc + f - ni, o = owner[f];
+        double ex = (face_centroid[3 * f] - cx[o]) / 0.5;
+        double ey = (face_centroid[3 * f + 1] - cy[o]) / 0.5;
+        double ez = (face_centroid[3 * f + 2] - cz[o]) / 0.5;
+        cx[g] = cx[o] + ex;
+        cy[g] = cy[o] + ey;
+        cz[g] = cz[o] + ez;
+        neighbour[f] = g;
+    }
+    for (int i = 0; i < nt; i++) {
+        cell_volume[i] = cvol[i];
+        cell_centroid[3 * i] = cx[i];
+        cell_centroid[3 * i + 1] = cy[i];
+        cell_centroid[3 * i + 2] = cz[i];
+    }
+    // Least-squares / hybrid gradient geometry: gradients::pre_fill_LHS_and_RHS_matrix
+    // (gradients.cpp:214-315) and add_non_macrovariable_contributions (:149-211).
+    for (int i = 0; i < nc; i++) {
+        if (gcells[i].size() != 6) return lbfs::set_error(LBFS_ERR_ARG, "hex cell without 6 stencil entries");
+        double L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        double max_area = 0.0, max_disp = 0.0;
+        for (int q = 0; q < 6; q++) {
+            int i1 = gcells[i][q], f = gfaces[i][q];
+            max_area = std::max(max_area, face_area[f]);
+            double ddx = cx[i1] - cx[i], ddy = cy[i1] - cy[i], ddz = cz[i1] - cz[i];
+            max_disp = std::max(std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz), max_disp);
+        }
+        double aspect = 2 * std::fabs(max_disp) * max_area / cvol[i];
+        double beta = gradient_hybrid ? std::min(1.0, (2 / aspect)) : 1.0;
+        L[0] = L[0] + 2 * (1 - beta) * cvol[i];
+        L[4] = L[4] + 2 * (1 - beta) * cvol[i];
+        L[8] = L[8] + 2 * (1 - beta) * cvol[i];
+        for (int q = 0; q < 6; q++) {
+            int i1 = gcells[i][q], f = gfaces[i][q];
+            double fi = face_normal[3 * f], fj = face_normal[3 * f + 1], fk = face_normal[3 * f + 2];
+            double ddx = face_centroid[3 * f] - cx[i], ddy = face_centroid[3 * f + 1] - cy[i],
+                   ddz = face_centroid[3 * f + 2] - cz[i];
+            double l_norm = ddx * fi + ddy * fj + ddz * fk;
+            ddx = cx[i1] - cx[i]; ddy = cy[i1] - cy[i]; ddz = cz[i1] - cz[i];
+            double Ld = std::sqrt(std::pow(ddx, 2.0) + std::pow(ddy, 2.0) + std::pow(ddz, 2.0));
+            double s = face_area[f];
+            double L_norm = ddx * fi + ddy * fj + ddz * fk;
+            double alpha_w = std::pow(2 * l_norm / L_norm, 2.0);
+            double w = alpha_w * s / Ld;
+            L[0] = L[0] + w * ddx * ddx * beta; L[1] = L[1] + w * ddx * ddy * beta; L[2] = L[2] + w * ddx * ddz * beta;
+            L[3] = L[3] + w * ddy * ddx * beta; L[4] = L[4] + w * ddy * ddy * beta; L[5] = L[5] + w * ddy * ddz * beta;
+            L[6] = L[6] + w * ddz * ddx * beta; L[7] = L[7] + w * ddz * ddy * beta; L[8] = L[8] + w * ddz * ddz * beta;
+            double sgn = (owner[f] == i) ? 1.0 : -1.0;
+            double *R = rhs + 18 * i + 3 * q;
+            if (sgn > 0) {
+                R[0] = (beta * w * ddx + 2 * (1 - beta) * 0.5 * fi * s);
+                R[1] = (beta * w * ddy + 2 * (1 - beta) * 0.5 * fj * s);
+                R[2] = (beta * w * ddz + 2 * (1 - beta) * 0.5 * fk * s);
+            } else {
+                R[0] = (beta * w * ddx + 2 * (1 - beta) * 0.5 * fi * -1 * s);
+                R[1] = (beta * w * ddy + 2 * (1 - beta) * 0.5 * fj * -1 * s);
+                R[2] = (beta * w * ddz + 2 * (1 - beta) * 0.5 * fk * -1 * s);
+            }
+            gradient_stencil[6 * i + q] = i1;
+        }
+        // Determinant exactly as the reference forms it (gradients.cpp:282-284;
+        // its second cofactor is not the true one, which only matters on
+        // non-orthogonal meshes), then the adjugate / det.
+        double det = L[0] * (L[4] * L[8] - L[5] * L[7]) + L[1] * (L[3] * L[8] - L[5] - L[6]) +
+                     L[2] * (L[3] * L[7] - L[4] * L[6]);
+        double a = L[0], b = L[1], c = L[2], dd = L[3], e = L[4], f = L[5], g = L[6], h = L[7], k = L[8];
+        double *I = lhs_inverse + 9 * i;
+        I[0] = 1 / det * (e * k - f * h);
+        I[1] = 1 / det * (c * h - b * k);
+        I[2] = 1 / det * (b * f - c * e);
+        I[3] = 1 / det * (f * g - dd * k);
+        I[4] = 1 / det * (a * k - c * g);
+        I[5] = 1 / det * (c * dd - a * f);
+        I[6] = 1 / det * (dd * h - e * g);
+        I[7] = 1 / det * (b * g - a * h);
+        I[8] = 1 / det * (a * e - b * dd);
+    }
+    return LBFS_OK;
+}
+
 int build_mesh(double X, double Y, double Z, double dt, const double *origin, double visc, double fneq_min,
                int32_t gradient_hybrid, const VertexSpec &vs, int32_t *owner, int32_t *neighbour,
                double *face_area, double *face_normal, double *face_centroid, double *streaming_dt,
                double *cell_volume, double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse,
-               double *rhs, int32_t *bc_patch, double *delta_h, double *grid_xyz) {
+               double *rhs, int32_t *bc_patch, double *delta_h, double *grid_xyz, std::vector<float> *verts_out,
+               std::vector<int> *faces_out) {
     const double jitter = vs.jitter;
     const uint64_t seed = vs.seed;
     int32_t cnt[8];
@@ -281,163 +458,272 @@ int build_mesh(double X, double Y, double Z, double dt, const double *origin, do
             put(a, b, c, c - 1, i + j * d.nx + (k - 1) * d.nx * d.ny, 0);
         }
 
-    // Geometry: unstructured_mesh::generate_internal_mesh (unstructured_mesh.cpp:1592-1692),
-    // tet_volume (:1015-1040), cell_tet_area (:1170-1204), calc_face_delta_t (:1349-1446).
-    std::vector<double> cvol(nt, 0.0), csum_area(nt, 0.0), cx(nt, 0.0), cy(nt, 0.0), cz(nt, 0.0);
-    std::vector<std::vector<int>> gcells(nt), gfaces(nt);
-    const double reference_dt = visc * 3 / 1.0 / fneq_min;  // pre_conditioned_gamma = 1
-    for (int f = 0; f < nf; f++) {
-        V3 nd[4];
-        for (int q = 0; q < 4; q++) {
-            int t = fv[4 * f + q];
-            nd[q] = {(double)vx[t], (double)vy[t], (double)vz[t]};
-        }
-        for (int t = 0; t < 2; t++) {
-            V3 a = nd[0], b = sub(nd[t + 1], a), c = sub(nd[t + 2], a);
-            double vol = dot(a, cross(b, c)) / 6;
-            cvol[owner[f]] = cvol[owner[f]] + vol;
-            if (f < ni) cvol[neighbour[f]] = cvol[neighbour[f]] - vol;
-        }
-        double area_f = 0.0;
-        V3 fcen = {0, 0, 0}, fnorm = {0, 0, 0};
-        for (int t = 0; t < 2; t++) {
-            V3 a = nd[0], b = nd[t + 1], c = nd[t + 2];
-            V3 cen = {(a.x + b.x + c.x) / 3, (a.y + b.y + c.y) / 3, (a.z + b.z + c.z) / 3};
-            V3 n = cross(sub(b, a), sub(c, a));
-            double ar = 0.5 * mag(n);
-            area_f = area_f + ar;
-            double inv = 1 / ar;  // vector_var::factor divides by its argument
-            cen = {cen.x / inv, cen.y / inv, cen.z / inv};
-            fcen = add(fcen, cen);
-            fnorm = add(fnorm, n);
-        }
-        // Warped faces: the face's vector area is the sum of its triangles'
-        // vector areas, |N1 + N2| / 2 along (N1 + N2).  The reference's scalar
-        // sum |N1| / 2 + |N2| / 2 (kept for the area-weighted centroids) is
-        // longer whenever N1 and N2 are not parallel, so the vector areas of a
-        // cell's faces would not close and a fluid at rest would be pushed by
-        // its own pressure.
-        face_area[f] = jitter > 0 ? 0.5 * mag(fnorm) : area_f;
-        csum_area[owner[f]] = csum_area[owner[f]] + area_f;
-        cx[owner[f]] = cx[owner[f]] + fcen.x;
-        cy[owner[f]] = cy[owner[f]] + fcen.y;
-        cz[owner[f]] = cz[owner[f]] + fcen.z;
-        face_centroid[3 * f] = fcen.x / area_f;
-        face_centroid[3 * f + 1] = fcen.y / area_f;
-        face_centroid[3 * f + 2] = fcen.z / area_f;
-        double nm = mag(fnorm);
-        face_normal[3 * f] = fnorm.x / nm;
-        face_normal[3 * f + 1] = fnorm.y / nm;
-        face_normal[3 * f + 2] = fnorm.z / nm;
-        double face_dt = 0.5 * std::sqrt(area_f);
-        streaming_dt[f] = std::min(face_dt, reference_dt);
-        if (f > ni - 1) {
-            int g = f - ni + nc;
-            gcells[owner[f]].push_back(g);
-            gfaces[owner[f]].push_back(f);
-        } else {
-            int nb = neighbour[f];
-            csum_area[nb] = csum_area[nb] + area_f;
-            cx[nb] = cx[nb] + fcen.x;
-            cy[nb] = cy[nb] + fcen.y;
-            cz[nb] = cz[nb] + fcen.z;
-            gcells[owner[f]].push_back(nb);
-            gcells[nb].push_back(owner[f]);
-            gfaces[owner[f]].push_back(f);
-            gfaces[nb].push_back(f);
-        }
-    }
-    for (int i = 0; i < nc; i++) {
-        cx[i] = cx[i] / csum_area[i];
-        cy[i] = cy[i] / csum_area[i];
-        cz[i] = cz[i] / csum_area[i];
-    }
-    // ghost centroids: populate_ghost_cell_from_foam_face, unstructured_mesh.cpp:1963-1996
-    for (int f = ni; f < nf; f++) {
-        int g = nc + f - ni, o = owner[f];
-        double ex = (face_centroid[3 * f] - cx[o]) / 0.5;
-        double ey = (face_centroid[3 * f + 1] - cy[o]) / 0.5;
-        double ez = (face_centroid[3 * f + 2] - cz[o]) / 0.5;
-        cx[g] = cx[o] + ex;
-        cy[g] = cy[o] + ey;
-        cz[g] = cz[o] + ez;
-        neighbour[f] = g;
-    }
-    for (int i = 0; i < nt; i++) {
-        cell_volume[i] = cvol[i];
-        cell_centroid[3 * i] = cx[i];
-        cell_centroid[3 * i + 1] = cy[i];
-        cell_centroid[3 * i + 2] = cz[i];
-    }
     double dh = std::min(d.dx, std::min(d.dy, d.dz)) * 0.5;
     *delta_h = std::min(dh, 0.1);
+    if (verts_out) {
+        verts_out->resize(3 * vx.size());
+        for (size_t t = 0; t < vx.size(); t++) {
+            (*verts_out)[3 * t] = vx[t];
+            (*verts_out)[3 * t + 1] = vy[t];
+            (*verts_out)[3 * t + 2] = vz[t];
+        }
+    }
+    if (faces_out) *faces_out = fv;
 
-    // Least-squares / hybrid gradient geometry: gradients::pre_fill_LHS_and_RHS_matrix
-    // (gradients.cpp:214-315) and add_non_macrovariable_contributions (:149-211).
-    for (int i = 0; i < nc; i++) {
-        if (gcells[i].size() != 6) return lbfs::set_error(LBFS_ERR_ARG, "hex cell without 6 stencil entries");
-        double L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        double max_area = 0.0, max_disp = 0.0;
-        for (int q = 0; q < 6; q++) {
-            int i1 = gcells[i][q], f = gfaces[i][q];
-            max_area = std::max(max_area, face_area[f]);
-            double ddx = cx[i1] - cx[i], ddy = cy[i1] - cy[i], ddz = cz[i1] - cz[i];
-            max_disp = std::max(std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz), max_disp);
-        }
-        double aspect = 2 * std::fabs(max_disp) * max_area / cvol[i];
-        double beta = gradient_hybrid ? std::min(1.0, (2 / aspect)) : 1.0;
-        L[0] = L[0] + 2 * (1 - beta) * cvol[i];
-        L[4] = L[4] + 2 * (1 - beta) * cvol[i];
-        L[8] = L[8] + 2 * (1 - beta) * cvol[i];
-        for (int q = 0; q < 6; q++) {
-            int i1 = gcells[i][q], f = gfaces[i][q];
-            double fi = face_normal[3 * f], fj = face_normal[3 * f + 1], fk = face_normal[3 * f + 2];
-            double ddx = face_centroid[3 * f] - cx[i], ddy = face_centroid[3 * f + 1] - cy[i],
-                   ddz = face_centroid[3 * f + 2] - cz[i];
-            double l_norm = ddx * fi + ddy * fj + ddz * fk;
-            ddx = cx[i1] - cx[i]; ddy = cy[i1] - cy[i]; ddz = cz[i1] - cz[i];
-            double Ld = std::sqrt(std::pow(ddx, 2.0) + std::pow(ddy, 2.0) + std::pow(ddz, 2.0));
-            double s = face_area[f];
-            double L_norm = ddx * fi + ddy * fj + ddz * fk;
-            double alpha_w = std::pow(2 * l_norm / L_norm, 2.0);
-            double w = alpha_w * s / Ld;
-            L[0] = L[0] + w * ddx * ddx * beta; L[1] = L[1] + w * ddx * ddy * beta; L[2] = L[2] + w * ddx * ddz * beta;
-            L[3] = L[3] + w * ddy * ddx * beta; L[4] = L[4] + w * ddy * ddy * beta; L[5] = L[5] + w * ddy * ddz * beta;
-            L[6] = L[6] + w * ddz * ddx * beta; L[7] = L[7] + w * ddz * ddy * beta; L[8] = L[8] + w * ddz * ddz * beta;
-            double sgn = (owner[f] == i) ? 1.0 : -1.0;
-            double *R = rhs + 18 * i + 3 * q;
-            if (sgn > 0) {
-                R[0] = (beta * w * ddx + 2 * (1 - beta) * 0.5 * fi * s);
-                R[1] = (beta * w * ddy + 2 * (1 - beta) * 0.5 * fj * s);
-                R[2] = (beta * w * ddz + 2 * (1 - beta) * 0.5 * fk * s);
-            } else {
-                R[0] = (beta * w * ddx + 2 * (1 - beta) * 0.5 * fi * -1 * s);
-                R[1] = (beta * w * ddy + 2 * (1 - beta) * 0.5 * fj * -1 * s);
-                R[2] = (beta * w * ddz + 2 * (1 - beta) * 0.5 * fk * -1 * s);
+    return mesh_geometry(nc, nf, ni, vx.data(), vy.data(), vz.data(), fv.data(), owner, neighbour, visc, fneq_min,
+                         gradient_hybrid, jitter > 0 && vs.closed_faces, face_area, face_normal, face_centroid,
+                         streaming_dt, cell_volume, cell_centroid, gradient_stencil, lhs_inverse, rhs);
+}
+
+}  // namespace
+
+// ---- OpenFOAM polyMesh ------------------------------------------------------
+
+namespace {
+
+const char *const kPatchNames[6] = {"left", "right", "bottom", "top", "back", "front"};
+
+void foam_header(std::FILE *f, const char *cls, const char *object, const std::string &note) {
+    std::fprintf(f,
+                 "/*--------------------------------*- C++ -*----------------------------------*\\\n"
+                 "  =========                 |\n"
+                 "  \\\\      /  F ield         | polyMesh written by lbfs_mesh_write_openfoam\n"
+                 "   \\\\    /   O peration     |\n"
+                 "    \\\\  /    A nd           |\n"
+                 "     \\\\/     M anipulation  |\n"
+                 "\\*---------------------------------------------------------------------------*/\n"
+                 "FoamFile\n{\n    version     2.0;\n    format      ascii;\n    class       %s;\n", cls);
+    if (!note.empty()) std::fprintf(f, "    note        \"%s\";\n", note.c_str());
+    std::fprintf(f, "    location    \"constant/polyMesh\";\n    object      %s;\n}\n"
+                    "// * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * * //\n\n\n", object);
+}
+
+// Lines of a file; false if it cannot be opened.
+bool read_lines(const std::string &path, std::vector<std::string> &lines) {
+    std::ifstream in(path);
+    if (!in) return false;
+    std::string line;
+    while (std::getline(in, line)) lines.push_back(line);
+    return true;
+}
+
+// The entries of the list of a polyMesh file: the lines after the first line
+// that starts with '(' up to the next line that starts with ')', as the
+// reference's reader delimits them (unstructured_mesh.cpp:749-770).
+std::vector<std::string> list_entries(const std::vector<std::string> &lines) {
+    std::vector<std::string> out;
+    bool start = false;
+    for (const std::string &l : lines) {
+        const char c = l.empty() ? 0 : l[0];
+        if (c == ')') start = false;
+        if (start && !l.empty()) out.push_back(l);
+        if (c == '(') start = true;
+    }
+    return out;
+}
+
+struct FoamMesh {
+    int n_points = 0, n_cells = 0, n_faces = 0, n_internal = 0;
+    std::vector<float> x, y, z;
+    std::vector<int> fv, owner, neighbour;
+    std::vector<std::string> patch_names;
+    std::vector<int> patch_faces;
+};
+
+// The owner file's note on its 13th line (nPoints, nCells, nFaces,
+// nInternalFaces), the lists of points, faces, owner and neighbour, and the
+// patch names and face counts of the boundary file (import_openfoam_mesh,
+// unstructured_mesh.cpp:670-941; import_openfoam_BC_tags, :2533-2608).
+int read_foam(const std::string &dir0, FoamMesh &m, bool header_only) {
+    const std::string dir = dir0.empty() || dir0.back() == '/' ? dir0 : dir0 + "/";
+    std::vector<std::string> own;
+    if (!read_lines(dir + "owner", own)) return lbfs::set_error(LBFS_ERR_ARG, "cannot open " + dir + "owner");
+    if (own.size() < 13) return lbfs::set_error(LBFS_ERR_ARG, "owner: no header note on line 13");
+    const std::string &note = own[12];
+    auto field = [&](const char *key, int &v) {
+        const size_t p = note.find(key);
+        if (p == std::string::npos) return false;
+        std::istringstream is(note.substr(p + std::strlen(key)));
+        return (bool)(is >> v);
+    };
+    if (!field("nPoints:", m.n_points) || !field("nCells:", m.n_cells) || !field("nFaces:", m.n_faces) ||
+        !field("nInternalFaces:", m.n_internal))
+        return lbfs::set_error(LBFS_ERR_ARG, "owner: line 13 must carry nPoints:, nCells:, nFaces:, nInternalFaces:");
+    if (m.n_points <= 0 || m.n_cells <= 0 || m.n_internal < 0 || m.n_faces <= m.n_internal)
+        return lbfs::set_error(LBFS_ERR_ARG, "owner: inconsistent sizes in the header note");
+    std::vector<std::string> bnd;
+    if (!read_lines(dir + "boundary", bnd)) return lbfs::set_error(LBFS_ERR_ARG, "cannot open " + dir + "boundary");
+    {
+        std::string last_name;
+        for (const std::string &l : list_entries(bnd)) {
+            std::istringstream is(l);
+            std::string t1, t2;
+            is >> t1 >> t2;
+            if (t1 == "{" || t1 == "}" || t1.empty()) continue;
+            if (t2.empty()) { last_name = t1; continue; }
+            if (t1 == "nFaces") {
+                if (!t2.empty() && t2.back() == ';') t2.pop_back();
+                m.patch_names.push_back(last_name);
+                m.patch_faces.push_back(std::stoi(t2));
             }
-            gradient_stencil[6 * i + q] = i1;
         }
-        // Determinant exactly as the reference forms it (gradients.cpp:282-284;
-        // its second cofactor is not the true one, which only matters on
-        // non-orthogonal meshes), then the adjugate / det.
-        double det = L[0] * (L[4] * L[8] - L[5] * L[7]) + L[1] * (L[3] * L[8] - L[5] - L[6]) +
-                     L[2] * (L[3] * L[7] - L[4] * L[6]);
-        double a = L[0], b = L[1], c = L[2], dd = L[3], e = L[4], f = L[5], g = L[6], h = L[7], k = L[8];
-        double *I = lhs_inverse + 9 * i;
-        I[0] = 1 / det * (e * k - f * h);
-        I[1] = 1 / det * (c * h - b * k);
-        I[2] = 1 / det * (b * f - c * e);
-        I[3] = 1 / det * (f * g - dd * k);
-        I[4] = 1 / det * (a * k - c * g);
-        I[5] = 1 / det * (c * dd - a * f);
-        I[6] = 1 / det * (dd * h - e * g);
-        I[7] = 1 / det * (b * g - a * h);
-        I[8] = 1 / det * (a * e - b * dd);
+    }
+    int nbf = 0;
+    for (int n : m.patch_faces) nbf += n;
+    if (nbf != m.n_faces - m.n_internal)
+        return lbfs::set_error(LBFS_ERR_ARG, "boundary: patch face counts do not add up to the boundary faces");
+    if (header_only) return LBFS_OK;
+    std::vector<std::string> pts, fcs, nbr;
+    if (!read_lines(dir + "points", pts) || !read_lines(dir + "faces", fcs) || !read_lines(dir + "neighbour", nbr))
+        return lbfs::set_error(LBFS_ERR_ARG, "cannot open points, faces or neighbour in " + dir);
+    const std::vector<std::string> P = list_entries(pts), F = list_entries(fcs), O = list_entries(own),
+                                   N = list_entries(nbr);
+    if ((int)P.size() != m.n_points || (int)F.size() != m.n_faces || (int)O.size() != m.n_faces ||
+        (int)N.size() != m.n_internal)
+        return lbfs::set_error(LBFS_ERR_ARG, "polyMesh lists do not match the owner file's header note");
+    m.x.resize(m.n_points); m.y.resize(m.n_points); m.z.resize(m.n_points);
+    for (int i = 0; i < m.n_points; i++) {
+        std::istringstream is(P[i]);
+        is.ignore(1);  // '('; the coordinates are read as float (unstructured_mesh.h:59)
+        if (!(is >> m.x[i] >> m.y[i] >> m.z[i])) return lbfs::set_error(LBFS_ERR_ARG, "points: bad entry");
+    }
+    m.fv.resize(4 * (size_t)m.n_faces);
+    for (int f = 0; f < m.n_faces; f++) {
+        std::istringstream is(F[f]);
+        int n = 0;
+        is >> n;
+        if (n != 4) return lbfs::set_error(LBFS_ERR_UNSUPPORTED, "faces: quadrilaterals only (hexahedral cells)");
+        is.ignore(1);
+        for (int q = 0; q < 4; q++) {
+            if (!(is >> m.fv[4 * f + q]) || m.fv[4 * f + q] < 0 || m.fv[4 * f + q] >= m.n_points)
+                return lbfs::set_error(LBFS_ERR_ARG, "faces: bad vertex index");
+        }
+    }
+    m.owner.resize(m.n_faces);
+    m.neighbour.assign(m.n_faces, 0);
+    for (int f = 0; f < m.n_faces; f++) {
+        std::istringstream is(O[f]);
+        if (!(is >> m.owner[f]) || m.owner[f] < 0 || m.owner[f] >= m.n_cells)
+            return lbfs::set_error(LBFS_ERR_ARG, "owner: bad cell index");
+    }
+    for (int f = 0; f < m.n_internal; f++) {
+        std::istringstream is(N[f]);
+        if (!(is >> m.neighbour[f]) || m.neighbour[f] < 0 || m.neighbour[f] >= m.n_cells)
+            return lbfs::set_error(LBFS_ERR_ARG, "neighbour: bad cell index");
     }
     return LBFS_OK;
 }
 
 }  // namespace
+
+extern "C" int lbfs_mesh_write_openfoam(const char *dir, double X, double Y, double Z, double dt, const double *origin,
+                                        int32_t mesh_type, double plateau_width, double plateau_slope, double jitter,
+                                        uint64_t seed) {
+    if (!dir || !origin) return lbfs::set_error(LBFS_ERR_ARG, "null argument");
+    if (mesh_type != 4 && mesh_type != 5 && mesh_type != 6 && mesh_type != 7)
+        return lbfs::set_error(LBFS_ERR_ARG, "mesh_type must be 4, 5, 6 or 7");
+    if (!(jitter >= 0.0 && jitter < 0.25) || (jitter > 0 && mesh_type != 6))
+        return lbfs::set_error(LBFS_ERR_ARG, "jitter must be in [0, 0.25), on the uniform mesh only");
+    int32_t cnt[8];
+    int rc = lbfs_mesh_uniform_counts(X, Y, Z, dt, cnt);
+    if (rc) return rc;
+    const int nc = cnt[0], nf = cnt[1], ni = cnt[2], nb = cnt[3], nt = cnt[7];
+    VertexSpec vs;
+    vs.mesh_type = mesh_type; vs.plateau_width = plateau_width; vs.plateau_slope = plateau_slope;
+    vs.jitter = jitter; vs.seed = seed;
+    std::vector<int32_t> owner(nf), neighbour(nf), stencil(6 * (size_t)nc), patch(nb);
+    std::vector<double> area(nf), normal(3 * (size_t)nf), fcen(3 * (size_t)nf), sdt(nf), vol(nt),
+        cen(3 * (size_t)nt), lhs(9 * (size_t)nc), rhs(18 * (size_t)nc);
+    double dh = 0;
+    std::vector<float> verts;
+    std::vector<int> fv;
+    if ((rc = build_mesh(X, Y, Z, dt, origin, 0.1, 0.0, 0, vs, owner.data(), neighbour.data(), area.data(),
+                         normal.data(), fcen.data(), sdt.data(), vol.data(), cen.data(), stencil.data(), lhs.data(),
+                         rhs.data(), patch.data(), &dh, nullptr, &verts, &fv)))
+        return rc;
+    const std::string d = std::string(dir) + (std::string(dir).back() == '/' ? "" : "/");
+    const int np = (int)(verts.size() / 3);
+    char note[256];
+    std::snprintf(note, sizeof note, "nPoints:%d  nCells:%d  nFaces:%d  nInternalFaces:%d", np, nc, nf, ni);
+    auto open = [&](const char *name) { return std::fopen((d + name).c_str(), "w"); };
+    std::FILE *f = open("points");
+    if (!f) return lbfs::set_error(LBFS_ERR_ARG, "cannot write " + d + "points");
+    foam_header(f, "vectorField", "points", "");
+    std::fprintf(f, "%d\n(\n", np);
+    for (int t = 0; t < np; t++)  // %.9g reproduces a float exactly
+        std::fprintf(f, "(%.9g %.9g %.9g)\n", verts[3 * t], verts[3 * t + 1], verts[3 * t + 2]);
+    std::fprintf(f, ")\n");
+    std::fclose(f);
+    if (!(f = open("faces"))) return lbfs::set_error(LBFS_ERR_ARG, "cannot write " + d + "faces");
+    foam_header(f, "faceList", "faces", "");
+    std::fprintf(f, "%d\n(\n", nf);
+    for (int q = 0; q < nf; q++) std::fprintf(f, "4(%d %d %d %d)\n", fv[4 * q], fv[4 * q + 1], fv[4 * q + 2], fv[4 * q + 3]);
+    std::fprintf(f, ")\n");
+    std::fclose(f);
+    if (!(f = open("owner"))) return lbfs::set_error(LBFS_ERR_ARG, "cannot write " + d + "owner");
+    foam_header(f, "labelList", "owner", note);
+    std::fprintf(f, "%d\n(\n", nf);
+    for (int q = 0; q < nf; q++) std::fprintf(f, "%d\n", owner[q]);
+    std::fprintf(f, ")\n");
+    std::fclose(f);
+    if (!(f = open("neighbour"))) return lbfs::set_error(LBFS_ERR_ARG, "cannot write " + d + "neighbour");
+    foam_header(f, "labelList", "neighbour", note);
+    std::fprintf(f, "%d\n(\n", ni);
+    for (int q = 0; q < ni; q++) std::fprintf(f, "%d\n", neighbour[q]);
+    std::fprintf(f, ")\n");
+    std::fclose(f);
+    if (!(f = open("boundary"))) return lbfs::set_error(LBFS_ERR_ARG, "cannot write " + d + "boundary");
+    foam_header(f, "polyBoundaryMesh", "boundary", "");
+    std::fprintf(f, "6\n(\n");
+    int start = ni;
+    for (int p = 0; p < 6; p++) {
+        int n = 0;
+        for (int b = 0; b < nb; b++) n += patch[b] == p ? 1 : 0;
+        std::fprintf(f, "    %s\n    {\n        type            patch;\n        nFaces          %d;\n"
+                        "        startFace       %d;\n    }\n", kPatchNames[p], n, start);
+        start += n;
+    }
+    std::fprintf(f, ")\n");
+    std::fclose(f);
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_mesh_openfoam_counts(const char *dir, int32_t *counts) {
+    if (!dir || !counts) return lbfs::set_error(LBFS_ERR_ARG, "null argument");
+    FoamMesh m;
+    int rc = read_foam(dir, m, true);
+    if (rc) return rc;
+    counts[0] = m.n_points; counts[1] = m.n_cells; counts[2] = m.n_faces; counts[3] = m.n_internal;
+    counts[4] = m.n_faces - m.n_internal; counts[5] = (int32_t)m.patch_names.size();
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_mesh_import_openfoam(const char *dir, double visc, double fneq_min, int32_t gradient_hybrid,
+                                         int32_t closed_faces, int32_t *owner, int32_t *neighbour, double *face_area,
+                                         double *face_normal, double *face_centroid, double *streaming_dt,
+                                         double *cell_volume, double *cell_centroid, int32_t *gradient_stencil,
+                                         double *lhs_inverse, double *rhs, int32_t *bc_patch, char *names,
+                                         int32_t names_len) {
+    if (!dir || !owner || !neighbour || !face_area || !face_normal || !face_centroid || !streaming_dt ||
+        !cell_volume || !cell_centroid || !gradient_stencil || !lhs_inverse || !rhs || !bc_patch)
+        return lbfs::set_error(LBFS_ERR_ARG, "null argument");
+    FoamMesh m;
+    int rc = read_foam(dir, m, false);
+    if (rc) return rc;
+    std::copy(m.owner.begin(), m.owner.end(), owner);
+    std::copy(m.neighbour.begin(), m.neighbour.end(), neighbour);
+    int b = 0;
+    for (size_t p = 0; p < m.patch_faces.size(); p++)
+        for (int q = 0; q < m.patch_faces[p]; q++) bc_patch[b++] = (int32_t)p;
+    if (names && names_len > 0) {
+        std::string all;
+        for (const std::string &n : m.patch_names) all += n + "\n";
+        std::snprintf(names, (size_t)names_len, "%s", all.c_str());
+    }
+    return mesh_geometry(m.n_cells, m.n_faces, m.n_internal, m.x.data(), m.y.data(), m.z.data(), m.fv.data(), owner,
+                         neighbour, visc, fneq_min, gradient_hybrid, closed_faces != 0, face_area, face_normal,
+                         face_centroid, streaming_dt, cell_volume, cell_centroid, gradient_stencil, lhs_inverse, rhs);
+}
 
 // Spring connectivity: the neighbour-ring construction, duplicate removal and
 // spring hashing of lagrangian_object::osay_mesh_read (lagrangian_object.cpp:

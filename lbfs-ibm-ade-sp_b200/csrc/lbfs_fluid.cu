@@ -481,6 +481,10 @@ __global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
 #pragma unroll
             for (int m = 0; m < 4; m++) r[m] = (e > 0) ? r[m] + (-fv[m] * iv) : r[m] + fv[m] * iv;
         }
+        if (a.closure) {
+#pragma unroll
+            for (int m = 0; m < 3; m++) r[1 + m] = r[1 + m] + __ldg(a.closure + 3 * (size_t)i + m);
+        }
         double fx = a.force[0], fy = a.force[1], fz = a.force[2];
         if (a.n_membranes > 0) {
             const int inst = a.cell_instance ? __ldg(a.cell_instance + i) : 0;

@@ -143,6 +143,11 @@ template <typename R> struct FluidArgs {
     const int *cell_faces;       // [6*nc] +(f+1) owner, -(f+1) neighbour
     const double *cell_volume;   // [nc]
     const double *cell_inv_volume;  // [nc] 1 / cell_volume
+    // FP32 bulk on meshes whose cell faces do not close: per cell the momentum
+    // residual of the constant flux rho0/3 n area that the deviation form
+    // leaves out, sum over the faces of -+ rho0/3 n area / volume (null when
+    // every cell closes, where it vanishes)
+    const double *closure;       // [3 nc]
     double4 *t1;                 // [nc] (u, v, w, rho) conservative accumulator, FP64
     double *res_out;             // [4*nc] residuals kept for parity checks (null = not stored)
     // IBM patches (one per membrane), grouped by ensemble instance

@@ -247,6 +247,28 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         if (cnt[i] != 6) return set_error(LBFS_ERR_UNSUPPORTED, "cell without 6 faces (hexahedra only)");
     std::vector<double> vol(m->cell_volume, m->cell_volume + nc), inv_vol(nc);
     for (int i = 0; i < nc; i++) inv_vol[i] = 1.0 / vol[i];
+    // FP32 bulk: the per-cell residual of the constant flux rho0/3 n area the
+    // deviation form leaves out; zero on cells whose faces close
+    std::vector<double> closure;
+    if (s->fp32) {
+        closure.assign(3 * (size_t)nc, 0.0);
+        double amax = 0.0, cmax = 0.0;
+        for (int f = 0; f < nf; f++) {
+            const double c = rho0 / 3.0 * m->face_area[f];
+            amax = std::max(amax, std::fabs(c));
+            for (int q = 0; q < 3; q++) {
+                const double v = c * fn[3 * f + q];
+                closure[3 * (size_t)m->owner[f] + q] -= v;
+                if (f < ni) closure[3 * (size_t)m->neighbour[f] + q] += v;
+            }
+        }
+        for (int i = 0; i < nc; i++)
+            for (int q = 0; q < 3; q++) cmax = std::max(cmax, std::fabs(closure[3 * (size_t)i + q]));
+        if (cmax <= 1e-12 * amax) closure.clear();  // every cell closes
+        else
+            for (int i = 0; i < nc; i++)
+                for (int q = 0; q < 3; q++) closure[3 * (size_t)i + q] *= inv_vol[i];
+    }
     std::vector<R> visc(nc, (R)p.visc_factor_initial);
     int rc = 0;
     int *d_rt, *d_vt, *d_cf;
@@ -266,6 +288,12 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         (rc = s->upload(&d_visc, visc)))
         return rc;
     if (a.axis_aligned && (rc = s->upload(&d_axf, axf))) return rc;
+    a.closure = nullptr;
+    if (!closure.empty()) {
+        double *d_cl;
+        if ((rc = s->upload(&d_cl, closure))) return rc;
+        a.closure = d_cl;
+    }
     a.stencil = d_stencil; a.ls = d_ls; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt;
     a.bc_val = d_bcv; a.bc_rec = d_bcr; a.face_cells = d_fcells; a.axis_face = d_axf; a.gen_face = d_gen;
     a.visc_factor = d_visc; a.cell_faces = d_cf; a.cell_volume = d_vol; a.cell_inv_volume = d_ivol;

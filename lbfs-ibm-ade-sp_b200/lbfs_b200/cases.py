@@ -16,7 +16,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from .mesh import build_uniform_mesh
+from .mesh import build_uniform_mesh, import_openfoam, write_openfoam
 from .rbc import red_cell, rotation_matrix
 from .solver import StepParams
 
@@ -183,7 +183,8 @@ def ensemble(n_instances=64, seed=2024, n_range=(16, 48), rbc_range=(1, 8), leve
 
 
 def jittered_channel(n=128, n_rbc=16, jitter=0.1, level=3, radius_cells=6.0, capillary=0.1, u_centre=0.01,
-                     seed=1313, tau=0.8, delta_t=0.5, precision=_abi.LBFS_FP64, ibm_stencil=_abi.LBFS_IBM_PESKIN4):
+                     seed=1313, tau=0.8, delta_t=0.5, precision=_abi.LBFS_FP64, ibm_stencil=_abi.LBFS_IBM_PESKIN4,
+                     closed_faces=True):
     """Body-force-driven square duct on a jittered n^3 hex mesh (every interior
     vertex moved by a seeded offset of up to `jitter` x spacing per axis;
     general-normal fluxes) with up to n_rbc red cells of radius `radius_cells`,
@@ -194,7 +195,8 @@ def jittered_channel(n=128, n_rbc=16, jitter=0.1, level=3, radius_cells=6.0, cap
     dt = 1.0
     visc = (tau - 0.5) / 3.0 * dt
     L = 2.0 * n
-    mesh = build_uniform_mesh(L, L, L, dt, visc=visc, jitter=jitter, seed=seed)
+    # closed_faces=False: the geometry the reference's importer forms from this mesh as a polyMesh
+    mesh = build_uniform_mesh(L, L, L, dt, visc=visc, jitter=jitter, seed=seed, closed_faces=closed_faces)
     bcs = {"left": (2, 2, 1.0, 0.0, 0.0, 0.0), "right": (2, 2, 1.0, 0.0, 0.0, 0.0),
            "bottom": (2, 1, 1.0, 0.0, 0.0, 0.0), "top": (2, 1, 1.0, 0.0, 0.0, 0.0),
            "back": (2, 1, 1.0, 0.0, 0.0, 0.0), "front": (2, 1, 1.0, 0.0, 0.0, 0.0)}
@@ -218,3 +220,16 @@ def jittered_channel(n=128, n_rbc=16, jitter=0.1, level=3, radius_cells=6.0, cap
     return Case("jittered_channel", mesh, params, cells, rho, u, v, w, bcs,
                 {"n": n, "jitter": jitter, "level": level, "radius_cells": radius_cells, "n_rbc": len(cells),
                  "shear_modulus": shear_modulus, "force": force})
+
+
+def imported(case, directory, jitter=0.1, seed=5):
+    """The case on its box meshed as a jittered hex mesh written as an OpenFOAM polyMesh in
+    `directory` and read back through the importer (mesh_type 3: the reference importer's
+    geometry, general-normal fluxes on every face)."""
+    from dataclasses import replace
+    m = case.mesh
+    write_openfoam(directory, m.X, m.Y, m.Z, m.dt, m.origin, jitter=jitter, seed=seed)
+    mesh = import_openfoam(directory, dt=m.dt, visc=case.params.visc)
+    mesh.source = str(directory)
+    mesh.set_boundaries(case.bcs)
+    return replace(case, mesh=mesh, info=dict(case.info, jitter=jitter, seed=seed, polymesh=str(directory)))

@@ -51,6 +51,8 @@ class UniformMesh:
     mesh_type: int = 6         # 6 uniform, 7 / 5 cosine-clustered, 4 plateau (rectilinear), 3 jittered
     grid: tuple = None         # vertex coordinates per axis (rectilinear meshes)
     plateau: tuple = (0.0, 0.0)  # plateau width and slope (mesh_type 4)
+    patch_names: tuple = PATCHES  # boundary patches in bc_patch order
+    source: str = None            # polyMesh directory of an imported mesh
 
     @property
     def shape(self):
@@ -69,7 +71,7 @@ class UniformMesh:
         rt = np.zeros(self.n_bc, np.int32)
         vt = np.zeros(self.n_bc, np.int32)
         vals = np.zeros((self.n_bc, 4), np.float64)
-        for p, name in enumerate(PATCHES):
+        for p, name in enumerate(self.patch_names):
             rho_type, vel_type, rho, u, v, w = spec[name]
             sel = self.bc_patch == p
             rt[sel] = rho_type
@@ -110,12 +112,13 @@ def uniform_counts(X, Y, Z, dt):
 
 
 def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_min=0.0, gradient="LS", jitter=0.0,
-                       seed=0, mesh_type=6, plateau_width=0.0, plateau_slope=0.0):
+                       seed=0, mesh_type=6, plateau_width=0.0, plateau_slope=0.0, closed_faces=True):
     """Mesh of ceil(X/(2 dt)) x ceil(Y/(2 dt)) x ceil(Z/(2 dt)) cells.  mesh_type 6 (uniform),
     7 / 5 (cosine-clustered in x, y / in x, y, z) and 4 (the plateau mesh of plateau_width,
     plateau_slope) are the reference generator's rectilinear meshes; with jitter > 0 every
     interior vertex of the uniform mesh moves by a seeded uniform offset of up to jitter x spacing
-    per axis and the mesh is stepped through the general-normal flux (mesh_type 3)."""
+    per axis and the mesh is stepped through the general-normal flux (mesh_type 3); closed_faces=False
+    gives the reference importer's geometry of that mesh (lbfs_mesh_build_jittered)."""
     nc, nf, ni, nb, nfx, nfy, nfz, nt = uniform_counts(X, Y, Z, dt)
     owner = np.zeros(nf, np.int32)
     neighbour = np.zeros(nf, np.int32)
@@ -147,10 +150,58 @@ def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_m
         grid = (g[:nx + 1].copy(), g[nx + 1:nx + ny + 2].copy(), g[nx + ny + 2:].copy())
     elif jitter > 0:
         _abi.check(_abi.lib().lbfs_mesh_build_jittered(X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, hybrid,
-                                                       float(jitter), int(seed), *outs))
+                                                       float(jitter), int(seed), 1 if closed_faces else 0, *outs))
     else:
         _abi.check(_abi.lib().lbfs_mesh_build_uniform(X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, hybrid, *outs))
     return UniformMesh(X, Y, Z, dt, tuple(origin), nc, nf, ni, nb, nfx, nfy, nfz, owner, neighbour, area, normal,
                        fcen, sdt, vol, ccen, stencil, lhs, rhs, patch, dh.value, axis_aligned=not jitter > 0,
                        mesh_type=3 if jitter > 0 else int(mesh_type), grid=grid,
                        plateau=(float(plateau_width), float(plateau_slope)))
+
+
+def write_openfoam(directory, X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), mesh_type=6, plateau_width=0.0,
+                   plateau_slope=0.0, jitter=0.0, seed=0):
+    """Write the generator's mesh as an ASCII OpenFOAM polyMesh in `directory` (points, faces,
+    owner, neighbour, boundary; patches left, right, bottom, top, back, front)."""
+    org = np.asarray(origin, np.float64)
+    _abi.check(_abi.lib().lbfs_mesh_write_openfoam(str(directory).encode(), X, Y, Z, dt, _abi.ptr(org),
+                                                   int(mesh_type), float(plateau_width), float(plateau_slope),
+                                                   float(jitter), int(seed)))
+
+
+def import_openfoam(directory, dt=1.0, visc=0.1, fneq_min=0.0, gradient="LS", closed_faces=False, delta_h=None):
+    """Read an OpenFOAM polyMesh of hexahedra as the reference's importer does (mesh_type 3: every face
+    takes the general-normal flux).  The IBM grid is the mesh's bounding box with cells of 2 dt
+    (cell order must be lexicographic for the IBM, as in the reference); delta_h defaults to
+    min(0.1, dt)."""
+    d = str(directory).encode()
+    c = (ctypes.c_int32 * 6)()
+    _abi.check(_abi.lib().lbfs_mesh_openfoam_counts(d, c))
+    n_points, nc, nf, ni, nb, n_patches = list(c)
+    nt = nc + nb
+    owner = np.zeros(nf, np.int32)
+    neighbour = np.zeros(nf, np.int32)
+    area = np.zeros(nf)
+    normal = np.zeros((nf, 3))
+    fcen = np.zeros((nf, 3))
+    sdt = np.zeros(nf)
+    vol = np.zeros(nt)
+    ccen = np.zeros((nt, 3))
+    stencil = np.zeros((nc, 6), np.int32)
+    lhs = np.zeros((nc, 9))
+    rhs = np.zeros((nc, 6, 3))
+    patch = np.zeros(nb, np.int32)
+    names = ctypes.create_string_buffer(64 * (n_patches + 1) + 64)
+    _abi.check(_abi.lib().lbfs_mesh_import_openfoam(
+        d, visc, fneq_min, 1 if gradient == "hybrid" else 0, 1 if closed_faces else 0, _abi.iptr(owner),
+        _abi.iptr(neighbour), _abi.ptr(area), _abi.ptr(normal), _abi.ptr(fcen), _abi.ptr(sdt), _abi.ptr(vol),
+        _abi.ptr(ccen), _abi.iptr(stencil), _abi.ptr(lhs), _abi.ptr(rhs), _abi.iptr(patch), names, len(names)))
+    patch_names = tuple(names.value.decode().split())
+    # bounding box of the boundary face centroids: the box the IBM grid covers
+    bf = fcen[ni:]
+    lo, hi = bf.min(axis=0), bf.max(axis=0)
+    m = UniformMesh(float(hi[0] - lo[0]), float(hi[1] - lo[1]), float(hi[2] - lo[2]), dt, tuple(lo), nc, nf, ni, nb,
+                    0, 0, 0, owner, neighbour, area, normal, fcen, sdt, vol, ccen, stencil, lhs, rhs, patch,
+                    float(min(0.1, dt)) if delta_h is None else float(delta_h), axis_aligned=False, mesh_type=3)
+    m.patch_names = patch_names
+    return m

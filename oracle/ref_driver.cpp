@@ -108,7 +108,7 @@ double block_min_max(const double *v, int n, int n_blocks, bool is_min) {
 // ---------------------------------------------------------------- mesh ----
 extern "C" void *ref_mesh_create(double X, double Y, double Z, double dt, double ox, double oy, double oz,
                                  double visc, int gradient_hybrid, const char *outdir, int mesh_type,
-                                 double plateau_width, double plateau_slope) {
+                                 double plateau_width, double plateau_slope, const char *import_dir) {
     Quiet q;
     RefMesh *m = new RefMesh();
     m->domain.X = X; m->domain.Y = Y; m->domain.Z = Z; m->domain.dt = dt;
@@ -118,7 +118,9 @@ extern "C" void *ref_mesh_create(double X, double Y, double Z, double dt, double
     m->domain.IBM_face = "none";
     m->globals.mesh_type = mesh_type;
     m->globals.import_format = "openfoam";
-    m->globals.import_file = std::string(outdir) + "/no_such_case/";
+    // mesh_type 3 reads the polyMesh in import_dir (import_openfoam_mesh); the
+    // generated types find no boundary file here
+    m->globals.import_file = import_dir ? std::string(import_dir) + "/" : std::string(outdir) + "/no_such_case/";
     m->globals.output_file = outdir;
     m->globals.testcase = 1;
     m->globals.visc = visc;
@@ -329,7 +331,7 @@ extern "C" void *ref_case_create(void *mesh, const ref_params *p, const int *rho
     c->local_fneq.assign(nt, 0.0);
     c->dtl.assign(nc, p->delta_t);
     c->delta_t = p->delta_t;
-    {
+    if (c->m->globals.mesh_type != 3) {  // generated meshes only: the importer allocates no plateau arrays
         domain_geometry &D = c->m->domain;
         const int n[3] = {(int)ceil(D.X / D.dt * 0.5), (int)ceil(D.Y / D.dt * 0.5), (int)ceil(D.Z / D.dt * 0.5)};
         for (int a = 0; a < 3; a++) {
@@ -479,6 +481,14 @@ extern "C" void ref_case_step(void *h, int n_steps) {
         get_bc_gradients(c->nb, c->nn, nc, c->owner.data(), c->rho_type.data(), c->vel_type.data(), c->soln.data(),
                          c->fnorm.data(), c->ccen.data(), c->bcs_arr.data(), c->g_rho.data(), c->g_u.data(), c->g_v.data(),
                          c->g_w.data());
+        if (c->m->globals.mesh_type == 3) {  // imported meshes: general-normal interior faces (Solver_gpu.cu:970-976)
+            calc_face_flux(c->nn, c->soln.data(), c->vol.data(), c->area.data(), c->owner.data(), c->neighbour.data(),
+                           c->ccen.data(), c->fcen.data(), c->fnorm.data(), c->sdt.data(), c->g_rho.data(),
+                           c->g_u.data(), c->g_v.data(), c->g_w.data(), nc, p.gamma_inv, c->local_fneq.data(), p.visc,
+                           c->res_rho.data(), c->res_u.data(), c->res_v.data(), c->res_w.data(), c->res_face.data(),
+                           c->rho_type.data(), c->vel_type.data(), c->bcs_arr.data(), acos(-1.0), p.testcase,
+                           c->visc_factor.data(), p.preconditioning != 0);
+        } else {
         calc_face_flux_x(c->nfx, c->soln.data(), c->vol.data(), c->area.data(), c->owner.data(), c->neighbour.data(),
                          c->ccen.data(), c->fcen.data(), c->fnorm.data(), c->sdt.data(), c->g_rho.data(), c->g_u.data(),
                          c->g_v.data(), c->g_w.data(), nc, p.gamma_inv, c->local_fneq.data(), p.visc, c->res_rho.data(),
@@ -495,6 +505,7 @@ extern "C" void ref_case_step(void *h, int n_steps) {
                          c->res_u.data(), c->res_v.data(), c->res_w.data(), c->res_face.data(), c->rho_type.data(),
                          c->vel_type.data(), c->bcs_arr.data(), acos(-1.0), c->nfx + c->nfy, c->visc_factor.data(),
                          p.testcase);
+        }
         calc_face_flux_bc(c->nb, c->soln.data(), c->vol.data(), c->area.data(), c->owner.data(), c->neighbour.data(),
                           c->ccen.data(), c->fcen.data(), c->fnorm.data(), c->sdt.data(), c->g_rho.data(), c->g_u.data(),
                           c->g_v.data(), c->g_w.data(), nc, p.gamma_inv, c->local_fneq.data(), p.visc, c->res_rho.data(),

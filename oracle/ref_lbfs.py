@@ -52,7 +52,7 @@ def lib():
         vp = ctypes.c_void_p
         L.ref_mesh_create.restype = vp
         L.ref_mesh_create.argtypes = [ctypes.c_double] * 8 + [ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
-                                                               ctypes.c_double, ctypes.c_double]
+                                                               ctypes.c_double, ctypes.c_double, ctypes.c_char_p]
         L.ref_mesh_plateau.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         L.ref_mesh_counts.argtypes = [vp, ctypes.c_void_p]
         L.ref_mesh_dump.argtypes = [vp] + [ctypes.c_void_p] * 12
@@ -81,12 +81,13 @@ class RefMesh:
     """unstructured_mesh (generated: mesh_type 6, 7, 5 or 4) + gradients built by the reference code."""
 
     def __init__(self, X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, hybrid=False, mesh_type=6,
-                 plateau_width=0.0, plateau_slope=0.0):
+                 plateau_width=0.0, plateau_slope=0.0, import_dir=None):
         self._dir = tempfile.mkdtemp(prefix="refmesh")
         self.dims = tuple(int(np.ceil(L / dt * 0.5)) for L in (X, Y, Z))
+        self.mesh_type = mesh_type
         self.h = lib().ref_mesh_create(X, Y, Z, dt, origin[0], origin[1], origin[2], visc, int(hybrid),
                                        self._dir.encode(), int(mesh_type), float(plateau_width),
-                                       float(plateau_slope))
+                                       float(plateau_slope), None if import_dir is None else str(import_dir).encode())
         c = (ctypes.c_int * 8)()
         lib().ref_mesh_counts(self.h, c)
         (self.n_cells, self.n_faces, self.n_interior, self.n_bc, self.n_face_x, self.n_face_y, self.n_face_z,
@@ -102,10 +103,11 @@ class RefMesh:
         dh = ctypes.c_double()
         lib().ref_mesh_dump(self.h, *[_p(a) for a in A.values()], ctypes.byref(dh))
         A["delta_h"] = dh.value
-        nx, ny, nz = self.dims
-        g = np.zeros(nx + ny + nz + 3)
-        lib().ref_mesh_plateau(self.h, nx, ny, nz, _p(g))
-        A["plateau"] = g
+        if self.mesh_type != 3:  # the importer allocates no plateau arrays
+            nx, ny, nz = self.dims
+            g = np.zeros(nx + ny + nz + 3)
+            lib().ref_mesh_plateau(self.h, nx, ny, nz, _p(g))
+            A["plateau"] = g
         return A
 
 

@@ -15,6 +15,7 @@ tests replay them without the reference.
 import os
 import subprocess
 import sys
+import tempfile
 from dataclasses import replace
 
 import numpy as np
@@ -25,13 +26,13 @@ sys.path.insert(0, os.path.join(ROOT, "lbfs-ibm-ade-sp_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 import ref_lbfs as R  # noqa: E402
-from lbfs_b200 import _abi, cases, icosphere  # noqa: E402
+from lbfs_b200 import _abi, cases, icosphere, write_openfoam  # noqa: E402
 
 
 def ref_case(c):
     m = c.mesh
     rm = R.RefMesh(m.X, m.Y, m.Z, m.dt, m.origin, c.params.visc, mesh_type=m.mesh_type, plateau_width=m.plateau[0],
-                   plateau_slope=m.plateau[1])
+                   plateau_slope=m.plateau[1], import_dir=m.source)
     p = R.RefParams()
     sp = c.params
     p.visc, p.delta_t, p.gamma_inv, p.channel_diameter = sp.visc, sp.delta_t, sp.gamma_inv, sp.channel_diameter
@@ -132,6 +133,24 @@ def main():
     c = cases.poiseuille(n=6, ny=5, nz=4)
     c.params = replace(c.params, gamma_inv=0.5, preconditioning=1, time_stepping=_abi.LBFS_DT_LOCAL)
     step_fixture("step_poiseuille_6x5x4_precond.npz", c, 20)
+    # OpenFOAM polyMesh: a jittered mesh written by lbfs_mesh_write_openfoam (kept as a fixture) and
+    # read by the reference's importer; steps on imported meshes take the general-normal flux
+    foam = os.path.join(HERE, "polymesh_jitter_8x6x5")
+    os.makedirs(foam, exist_ok=True)
+    write_openfoam(foam, 16.0, 12.0, 10.0, 1.0, jitter=0.1, seed=5)
+    for hybrid in (False, True):
+        rm = R.RefMesh(16.0, 12.0, 10.0, 1.0, (0.0, 0.0, 0.0), 0.1, hybrid, 3, 0.0, 0.0, foam)
+        np.savez_compressed(os.path.join(HERE, f"mesh_foam_jitter_8x6x5{'_hybrid' if hybrid else ''}.npz"),
+                            hybrid=int(hybrid), counts=np.array([rm.n_cells, rm.n_faces, rm.n_interior, rm.n_bc]),
+                            **rm.arrays())
+    with tempfile.TemporaryDirectory() as d:
+        step_fixture("step_foam_duct_8x6x5.npz", cases.imported(cases.poiseuille(n=8, ny=6, nz=5), d), 20)
+    with tempfile.TemporaryDirectory() as d:
+        # no interior-viscosity update: on imported meshes the reference reads an
+        # uninitialised delta_h there (unstructured_mesh.h:61 is set only by the generator)
+        c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
+        c.params = replace(c.params, viscosity_period=0)
+        step_fixture("step_foam_shear_rbc_16.npz", cases.imported(c, d), 10)
     subprocess.run([sys.executable, os.path.abspath(__file__), "--plateau"], check=True)
     print("golden fixtures written to", HERE)
 

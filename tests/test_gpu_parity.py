@@ -9,6 +9,7 @@
   identical to eager launches;
 * the FP32-bulk form against the FP64 path within FP32_RTOL.
 """
+import tempfile
 from dataclasses import replace
 
 import numpy as np
@@ -29,7 +30,15 @@ def make(c, cls=GpuSolver):
 
 def fixture_case(golden, name):
     g = golden(name)
-    if "poiseuille" in name:
+    if "foam_duct" in name:  # the imported jittered mesh (general-normal fluxes everywhere)
+        c = cases.imported(cases.poiseuille(n=8, ny=6, nz=5), tempfile.mkdtemp(prefix="polymesh"))
+    elif "foam_shear" in name:
+        c = cases.imported(cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2),
+                           tempfile.mkdtemp(prefix="polymesh"))
+        c.params = replace(c.params, viscosity_period=0)  # as the fixture (the reference's delta_h is unset)
+        mb = c.membranes[0]
+        mb.xyz_stress_free, mb.xyz_initial = g["xyz_stress_free"], g["xyz_initial"]
+    elif "poiseuille" in name:
         c = cases.poiseuille(n=6, ny=5, nz=4)
     elif "plateau" in name:
         c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_VANDERMONDE4, mesh_type=4,
@@ -49,7 +58,7 @@ def fixture_case(golden, name):
 
 FIXTURES = ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz", "step_poiseuille_6x5x4_local.npz",
             "step_poiseuille_6x5x4_talts.npz", "step_shear_rbc_16_min.npz", "step_plateau_rbc_16.npz",
-            "step_poiseuille_6x5x4_precond.npz"]
+            "step_poiseuille_6x5x4_precond.npz", "step_foam_duct_8x6x5.npz", "step_foam_shear_rbc_16.npz"]
 
 
 @pytest.mark.parametrize("name", FIXTURES)
@@ -197,11 +206,17 @@ def test_full_size_deterministic_and_graph_equals_eager():
     b.close()
 
 
-@pytest.mark.parametrize("builder", ["poiseuille", "shear_rbc"])
+@pytest.mark.parametrize("builder", ["poiseuille", "shear_rbc", "imported_channel"])
 def test_fp32_bulk_against_fp64(builder):
     if builder == "poiseuille":
         c64 = cases.poiseuille(n=16)
         c32 = cases.poiseuille(n=16, precision=_abi.LBFS_FP32_BULK)
+    elif builder == "imported_channel":
+        # the reference importer's geometry of a jittered mesh: cell faces do not close, so the
+        # FP32 form needs its per-cell closure term to stay with the FP64 path
+        c64 = cases.jittered_channel(n=16, n_rbc=1, level=2, radius_cells=2.0, closed_faces=False)
+        c32 = cases.jittered_channel(n=16, n_rbc=1, level=2, radius_cells=2.0, closed_faces=False,
+                                     precision=_abi.LBFS_FP32_BULK)
     else:
         c64 = cases.shear_rbc(n=24, level=2, radius_cells=4.0)
         c32 = cases.shear_rbc(n=24, level=2, radius_cells=4.0, precision=_abi.LBFS_FP32_BULK)

@@ -1,5 +1,6 @@
 """The C restatement oracle reproduces the reference's own kernels (golden
 fixtures produced by the reference sources compiled for the host)."""
+import tempfile
 from dataclasses import replace
 
 import numpy as np
@@ -12,7 +13,15 @@ from oracle_lbfs import OracleSolver
 
 def fixture_case(golden, name):
     g = golden(name)
-    if "poiseuille" in name:
+    if "foam_duct" in name:  # the imported jittered mesh (general-normal fluxes everywhere)
+        c = cases.imported(cases.poiseuille(n=8, ny=6, nz=5), tempfile.mkdtemp(prefix="polymesh"))
+    elif "foam_shear" in name:
+        c = cases.imported(cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2),
+                           tempfile.mkdtemp(prefix="polymesh"))
+        c.params = replace(c.params, viscosity_period=0)  # as the fixture (the reference's delta_h is unset)
+        mb = c.membranes[0]
+        mb.xyz_stress_free, mb.xyz_initial = g["xyz_stress_free"], g["xyz_initial"]
+    elif "poiseuille" in name:
         c = cases.poiseuille(n=6, ny=5, nz=4)
     elif "plateau" in name:
         c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_VANDERMONDE4, mesh_type=4,
@@ -34,7 +43,7 @@ def fixture_case(golden, name):
 
 FIXTURES = ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz", "step_poiseuille_6x5x4_local.npz",
             "step_poiseuille_6x5x4_talts.npz", "step_shear_rbc_16_min.npz", "step_plateau_rbc_16.npz",
-            "step_poiseuille_6x5x4_precond.npz"]
+            "step_poiseuille_6x5x4_precond.npz", "step_foam_duct_8x6x5.npz", "step_foam_shear_rbc_16.npz"]
 
 
 @pytest.mark.parametrize("name", FIXTURES)

@@ -51,3 +51,53 @@ def test_springs_cover_every_edge_once():
     edges = {tuple(sorted((int(a), int(c)))) for a, _, c, _ in spr}
     tri_edges = {tuple(sorted((int(t[i]), int(t[(i + 1) % 3])))) for t in tris for i in range(3)}
     assert edges == tri_edges
+
+
+FOAM = "polymesh_jitter_8x6x5"
+
+
+@pytest.mark.parametrize("hybrid", [False, True], ids=["LS", "hybrid"])
+def test_openfoam_import_bit_exact(golden, hybrid):
+    """The importer reads the committed polyMesh exactly as the reference's importer did
+    (import_openfoam_mesh + generate_internal_mesh + pre_fill_LHS_and_RHS_matrix)."""
+    import os
+    from conftest import ROOT
+    from lbfs_b200 import import_openfoam
+    g = golden(f"mesh_foam_jitter_8x6x5{'_hybrid' if hybrid else ''}.npz")
+    m = import_openfoam(os.path.join(ROOT, "tests", "golden", FOAM), gradient="hybrid" if hybrid else "LS")
+    assert [m.n_cells, m.n_faces, m.n_interior, m.n_bc] == list(g["counts"])
+    for key in ("owner", "neighbour", "face_area", "face_normal", "face_centroid", "streaming_dt", "cell_volume",
+                "cell_centroid", "gradient_stencil", "lhs_inverse", "rhs"):
+        assert np.array_equal(getattr(m, key), g[key]), key
+    assert m.patch_names == ("left", "right", "bottom", "top", "back", "front") and not m.axis_aligned
+
+
+def test_openfoam_writer_and_round_trip(tmp_path):
+    """The writer reproduces the committed polyMesh byte for byte, and reading it back gives the
+    generator's mesh with the reference's face areas (lbfs_mesh_build_jittered, closed_faces=0)."""
+    import os
+    from conftest import ROOT
+    from lbfs_b200 import import_openfoam, write_openfoam
+    write_openfoam(tmp_path, 16.0, 12.0, 10.0, 1.0, jitter=0.1, seed=5)
+    for name in ("points", "faces", "owner", "neighbour", "boundary"):
+        with open(os.path.join(ROOT, "tests", "golden", FOAM, name)) as a, open(tmp_path / name) as b:
+            assert a.read() == b.read(), name
+    m = import_openfoam(tmp_path)
+    g = build_uniform_mesh(16.0, 12.0, 10.0, 1.0, visc=0.1, jitter=0.1, seed=5, closed_faces=False)
+    for key in ("owner", "neighbour", "face_area", "face_normal", "face_centroid", "streaming_dt", "cell_volume",
+                "cell_centroid", "gradient_stencil", "lhs_inverse", "rhs", "bc_patch"):
+        assert np.array_equal(getattr(m, key), getattr(g, key)), key
+    # the closed-face variant changes only the areas of warped faces (and what depends on them)
+    c = build_uniform_mesh(16.0, 12.0, 10.0, 1.0, visc=0.1, jitter=0.1, seed=5)
+    assert np.array_equal(c.face_normal, g.face_normal) and not np.array_equal(c.face_area, g.face_area)
+    assert np.allclose(c.face_area, g.face_area, rtol=5e-2)  # warped faces: up to about 2 % apart
+
+
+def test_openfoam_import_rejects_bad_headers(tmp_path):
+    from lbfs_b200 import LbfsError, import_openfoam, write_openfoam
+    write_openfoam(tmp_path, 8.0, 6.0, 10.0, 1.0)
+    lines = (tmp_path / "owner").read_text().split("\n")
+    lines[12] = "    note        \"no counts here\";"
+    (tmp_path / "owner").write_text("\n".join(lines))
+    with pytest.raises(LbfsError):
+        import_openfoam(tmp_path)
