@@ -304,8 +304,11 @@ def run_batched(args, K, warmup, flush, device, plain_fp64_value):
 def run_precision(args, device):
     """FP32-bulk vs FP64 precision study: 128^3 jittered hex mesh (interior
     vertices moved by up to 10 % of the spacing, general-normal fluxes on every
-    face), body-force duct flow with 16 L3 red cells, N steps in each precision;
-    field and red-cell shape errors of the FP32 run against the FP64 run."""
+    face, faces' vector areas so that every cell closes), body-force duct flow
+    with 16 L3 red cells, N steps in each precision; field and red-cell shape
+    errors of the FP32 run against the FP64 run.  (With the reference
+    importer's face areas the cells of this mesh do not close and the duct
+    diverges in both precisions before 1000 steps.)"""
     import numpy as np
 
     from lbfs_b200 import GpuSolver, _abi, cases
