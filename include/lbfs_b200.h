@@ -198,6 +198,12 @@ int lbfs_set_nodes(lbfs_solver *s, const double *xyz);
 /* Membrane totals, host [6*n_rbc]: V, V0, A, A0, MAD, MAD0 per membrane
  * (lagrangian_object::total_volume ... total_MAD_0). */
 int lbfs_get_totals(lbfs_solver *s, double *out);
+/* Membrane energies, host [7*n_rbc]: volume, global area, local area, local
+ * bending, ADE, spring (WLC) and total energy per membrane, the columns of the
+ * reference's energy_log.txt (Solver_gpu.cu:1073-1136; the per-spring sums
+ * of get_area_energy, get_bending_energy and get_spring_energy,
+ * spring_network.cu:1687-1768, formed on the device in FP64). */
+int lbfs_get_energies(lbfs_solver *s, double *out);
 /* RMS residuals of the last step, host [4]: rho, u, v, w (residuals::l2_norm_rms_moukallad). */
 int lbfs_get_residuals(lbfs_solver *s, double *out);
 /* The time step of the last step (the solver loop's delta_t): params.delta_t

@@ -103,8 +103,21 @@ void membrane_prepare(int sort_capacity);
 int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side = nullptr,
                     cudaEvent_t ev_advected = nullptr, cudaEvent_t ev_sorted = nullptr);
 
+// Per membrane, the y-z binning of its triangles for the interior test: bins
+// of size >= every triangle's y-z extent and >= 4 delta_h over the membrane's
+// box (+- 2 delta_h), at most kViscBins of them.
+constexpr int kViscBins = 64 * 64;
+struct ViscBins {
+    double y0, z0, inv_b;
+    int ny, nz;
+};
+
 struct ViscArgs {
     int nc, n_membranes;
+    ViscBins *bins;              // [n_membranes]
+    int *bin_start;              // [n_membranes * (kViscBins + 1)] first list entry of each bin
+    int *bin_list;               // [4 total_tris] triangles (global ids) per bin, membrane m from 4 tri0
+    int total_tris;
     const double *centroid;      // [3*nc]
     const MembraneConst *mc;
     const MembraneScalars *ms;
@@ -124,5 +137,7 @@ void launch_membrane_forces(const MembraneArgs &a, cudaStream_t s);
 // single phases of the membrane chain (autotuner): node sort + patches, spread
 void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s);
 void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s);
+// per membrane the local area, local bending and spring energy sums, out[3 n_membranes]
+void launch_membrane_energies(const MembraneArgs &a, double *out, cudaStream_t s);
 
 }  // namespace lbfs

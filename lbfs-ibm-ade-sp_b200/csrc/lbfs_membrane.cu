@@ -829,7 +829,135 @@ __global__ void __launch_bounds__(256) k_mem_spread(MembraneArgs A) {
     }
 }
 
+// ---- energy diagnostics (Solver_gpu.cu:1073-1136) ------------------------
+// One CTA per membrane: the sums over its springs of get_area_energy,
+// get_bending_energy and get_spring_energy (spring_network.cu:1687-1768),
+// each a fixed-order block sum.  out[3 m + 0..2]: local area, local bending,
+// spring (WLC) energy.  As the reference launches them: the area energy uses
+// the global area modulus, the bending energy divides by spring_area[i] (the
+// i-th entry of the two-per-spring array), the WLC constants take
+// 1 / wlc_ratio.
+__global__ void __launch_bounds__(kTotalsThreads) k_mem_energies(MembraneArgs A, double *out) {
+    __shared__ double sh[33];
+    const int m = blockIdx.x;
+    const MembraneConst &mc = A.mc[m];
+    const double r = 1 / mc.wlc_ratio;
+    const double c1 = (0.25 / (1 - r) / (1 - r) - 0.25 + r);
+    const double c2 = r * r * (3.0 - 2.0 * r) / (1.0 - r) - 4 * c1 * r;
+    double ea = 0.0, eb = 0.0, es = 0.0;
+    for (int ls = threadIdx.x; ls < mc.n_springs; ls += blockDim.x) {
+        const int i = mc.spring0 + ls;
+        const double a0 = A.area[2 * i] - A.area0[2 * i], a1 = A.area[2 * i + 1] - A.area0[2 * i + 1];
+        ea += mc.global_area_modulus * 0.5 * (a0 * a0 / A.area0[2 * i] + a1 * a1 / A.area0[2 * i + 1]);
+        const double dc = A.curv[i] - A.curv0[i];
+        eb += 0.5 * mc.local_bending_modulus * dc * dc / A.area[i];
+        const int na = A.spring[4 * i], nc = A.spring[4 * i + 2];
+        const D3 d = d3(A.x[nc], A.y[nc], A.z[nc]) - d3(A.x[na], A.y[na], A.z[na]);
+        const double len = sqrt(dot(d, d)), L0 = A.contour[i], sr = len / L0;
+        es += 0.5 * A.kspring[i] * fabs(0.25 * L0 * (sr * sr * (3.0 - 2.0 * sr) / (1.0 - sr) - 4 * sr * c1 - c2));
+    }
+    const double ta = block_sum(ea, sh), tb = block_sum(eb, sh), ts = block_sum(es, sh);
+    if (threadIdx.x == 0) {
+        out[3 * m] = ta;
+        out[3 * m + 1] = tb;
+        out[3 * m + 2] = ts;
+    }
+}
+
 // ---- interior viscosity (update_interior_viscosities_plucker, immersed_boundary_method.cu:389-527) ----
+//
+// The reference tests every cell of the membrane's box (+- 2 delta_h) against
+// every triangle: the parity of the crossings of the +x ray from the cell's
+// centroid (Plucker side tests, triangles entirely ahead of the cell) and
+// the smallest distance to a vertex of those triangles, which enters the
+// smoothed step (d / dh + sin(pi d / dh) / pi) / 2 capped at 1/2.  Here the
+// triangles are first binned by their y-z boxes (V1, one CTA per membrane),
+// so a cell tests only the triangles of the bin holding its (y, z) for
+// crossings (a crossed triangle's y-z box holds the point) and those of the
+// bins within 2 delta_h for the distance (the smoothed step is exactly 1 at
+// distances >= delta_h, so a distance needs to be exact only below that).
+// Counts and minima do not depend on the order of the candidates: the result
+// is the same as testing every triangle.
+
+__device__ __forceinline__ int visc_bin(double v, double v0, double inv_b, int n) {
+    const int b = (int)floor((v - v0) * inv_b);
+    return b < 0 ? 0 : (b >= n ? n - 1 : b);
+}
+
+// V1: bins of one membrane's triangles (counting sort in shared memory).
+__global__ void __launch_bounds__(512) k_visc_bins(ViscArgs a) {
+    __shared__ int cnt[kViscBins];
+    __shared__ double shd[33];
+    __shared__ ViscBins g;
+    const int m = blockIdx.x;
+    const MembraneConst mc = a.mc[m];
+    const MembraneScalars ms = a.ms[m];
+    const double dh = mc.gdh;
+    double ext = 4.0 * dh;
+    for (int lt = threadIdx.x; lt < mc.n_tris; lt += blockDim.x) {
+        const int t = mc.tri0 + lt;
+        const int n0 = a.tri[3 * t], n1 = a.tri[3 * t + 1], n2 = a.tri[3 * t + 2];
+        const double ey = fmax(a.y[n0], fmax(a.y[n1], a.y[n2])) - fmin(a.y[n0], fmin(a.y[n1], a.y[n2]));
+        const double ez = fmax(a.z[n0], fmax(a.z[n1], a.z[n2])) - fmin(a.z[n0], fmin(a.z[n1], a.z[n2]));
+        ext = fmax(ext, fmax(ey, ez));
+    }
+    // block maximum
+    for (int o = 16; o > 0; o >>= 1) ext = fmax(ext, __shfl_down_sync(0xffffffffu, ext, o));
+    if ((threadIdx.x & 31) == 0) shd[threadIdx.x >> 5] = ext;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = shd[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) b = fmax(b, shd[w]);
+        const double y0 = ms.bbox_lo[1] - 2 * dh, y1 = ms.bbox_hi[1] + 2 * dh;
+        const double z0 = ms.bbox_lo[2] - 2 * dh, z1 = ms.bbox_hi[2] + 2 * dh;
+        int ny = (int)((y1 - y0) / b) + 1, nz = (int)((z1 - z0) / b) + 1;
+        while (ny * nz > kViscBins) {
+            b *= 1.5;
+            ny = (int)((y1 - y0) / b) + 1;
+            nz = (int)((z1 - z0) / b) + 1;
+        }
+        g = {y0, z0, 1.0 / b, ny, nz};
+        a.bins[m] = g;
+    }
+    __syncthreads();
+    const int nb = g.ny * g.nz;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) cnt[q] = 0;
+    __syncthreads();
+    // each triangle goes to every bin its y-z box overlaps (at most 2 x 2)
+    for (int pass = 0; pass < 2; pass++) {
+        for (int lt = threadIdx.x; lt < mc.n_tris; lt += blockDim.x) {
+            const int t = mc.tri0 + lt;
+            const int n0 = a.tri[3 * t], n1 = a.tri[3 * t + 1], n2 = a.tri[3 * t + 2];
+            const int y_lo = visc_bin(fmin(a.y[n0], fmin(a.y[n1], a.y[n2])), g.y0, g.inv_b, g.ny);
+            const int y_hi = visc_bin(fmax(a.y[n0], fmax(a.y[n1], a.y[n2])), g.y0, g.inv_b, g.ny);
+            const int z_lo = visc_bin(fmin(a.z[n0], fmin(a.z[n1], a.z[n2])), g.z0, g.inv_b, g.nz);
+            const int z_hi = visc_bin(fmax(a.z[n0], fmax(a.z[n1], a.z[n2])), g.z0, g.inv_b, g.nz);
+            for (int iz = z_lo; iz <= z_hi; iz++)
+                for (int iy = y_lo; iy <= y_hi; iy++) {
+                    const int bin = iy + g.ny * iz;
+                    if (pass == 0) atomicAdd(&cnt[bin], 1);
+                    else a.bin_list[4 * (size_t)mc.tri0 + atomicAdd(&cnt[bin], 1)] = t;
+                }
+        }
+        __syncthreads();
+        if (pass == 0) {
+            // exclusive prefix of the counts (one thread: at most 4096 bins, once per 10^4 steps)
+            if (threadIdx.x == 0) {
+                int run = 0;
+                int *start = a.bin_start + (size_t)m * (kViscBins + 1);
+                for (int q = 0; q < nb; q++) {
+                    const int c = cnt[q];
+                    start[q] = run;
+                    cnt[q] = run;  // placement cursor
+                    run += c;
+                }
+                start[nb] = run;
+            }
+            __syncthreads();
+        }
+    }
+}
+
 template <typename R>
 __global__ void k_interior_viscosity(ViscArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -849,27 +977,40 @@ __global__ void k_interior_viscosity(ViscArgs a) {
         if (!(cc.x >= xl && cc.x <= xh && cc.y >= yl && cc.y <= yh && cc.z >= zl && cc.z <= zh)) continue;
         // ray from the centroid along +x to x = xh; Plucker side tests against each triangle edge
         const double pc0 = cc.x * cc.y - xh * cc.y, pc1 = cc.x * cc.z - xh * cc.z, pc2 = cc.x - xh;
+        const ViscBins bg = a.bins[m];
+        const int *start = a.bin_start + (size_t)m * (kViscBins + 1);
+        const int *list = a.bin_list + 4 * (size_t)mc.tri0;
+        const int by = visc_bin(cc.y, bg.y0, bg.inv_b, bg.ny), bz = visc_bin(cc.z, bg.z0, bg.inv_b, bg.nz);
+        const int dy0 = visc_bin(cc.y - 2 * dh, bg.y0, bg.inv_b, bg.ny), dy1 = visc_bin(cc.y + 2 * dh, bg.y0, bg.inv_b, bg.ny);
+        const int dz0 = visc_bin(cc.z - 2 * dh, bg.z0, bg.inv_b, bg.nz), dz1 = visc_bin(cc.z + 2 * dh, bg.z0, bg.inv_b, bg.nz);
         int crossings = 0;
         double min_distance = 1000000000;
-        for (int lt = 0; lt < mc.n_tris; lt++) {
-            const int t = mc.tri0 + lt;
-            const int na = a.tri[3 * t], nb = a.tri[3 * t + 1], nc = a.tri[3 * t + 2];
-            const D3 A = d3(a.x[na], a.y[na], a.z[na]), B = d3(a.x[nb], a.y[nb], a.z[nb]), C = d3(a.x[nc], a.y[nc], a.z[nc]);
-            if (A.x > cc.x && B.x > cc.x && C.x > cc.x) {
-                const D3 P[3] = {A, B, C};
-                double side[3];
-                for (int e = 0; e < 3; e++) {
-                    const D3 p = P[e], q = P[(e + 1) % 3];
-                    const double e0 = p.y * q.z - q.y * p.z, e1 = p.z - q.z, e2 = q.y - p.y;
-                    side[e] = pc0 * e1 + pc1 * e2 + pc2 * e0;
+        for (int iz = dz0; iz <= dz1; iz++)
+            for (int iy = dy0; iy <= dy1; iy++) {
+                const int bin = iy + bg.ny * iz;
+                const bool own_bin = iy == by && iz == bz;  // crossings from this bin only (each triangle once)
+                for (int e0 = start[bin]; e0 < start[bin + 1]; e0++) {
+                    const int t = list[e0];
+                    const int na = a.tri[3 * t], nb = a.tri[3 * t + 1], nc = a.tri[3 * t + 2];
+                    const D3 A = d3(a.x[na], a.y[na], a.z[na]), B = d3(a.x[nb], a.y[nb], a.z[nb]),
+                             C = d3(a.x[nc], a.y[nc], a.z[nc]);
+                    if (!(A.x > cc.x && B.x > cc.x && C.x > cc.x)) continue;
+                    if (own_bin) {
+                        const D3 P[3] = {A, B, C};
+                        double side[3];
+                        for (int e = 0; e < 3; e++) {
+                            const D3 p = P[e], q = P[(e + 1) % 3];
+                            const double e0v = p.y * q.z - q.y * p.z, e1 = p.z - q.z, e2 = q.y - p.y;
+                            side[e] = pc0 * e1 + pc1 * e2 + pc2 * e0v;
+                        }
+                        if ((side[0] < 0 && side[1] < 0 && side[2] < 0) || (side[0] > 0 && side[1] > 0 && side[2] > 0))
+                            crossings++;
+                    }
+                    min_distance = fmin(sqrt(dot(cc - A, cc - A)), min_distance);
+                    min_distance = fmin(sqrt(dot(cc - B, cc - B)), min_distance);
+                    min_distance = fmin(sqrt(dot(cc - C, cc - C)), min_distance);
                 }
-                if ((side[0] < 0 && side[1] < 0 && side[2] < 0) || (side[0] > 0 && side[1] > 0 && side[2] > 0))
-                    crossings++;
-                min_distance = fmin(sqrt(dot(cc - A, cc - A)), min_distance);
-                min_distance = fmin(sqrt(dot(cc - B, cc - B)), min_distance);
-                min_distance = fmin(sqrt(dot(cc - C, cc - C)), min_distance);
             }
-        }
         const bool inside = (crossings % 2) != 0;
         const double r = mc.internal_viscosity_ratio;
         const double factor = 2.0 * fmin(0.5, (min_distance * 0.5 / dh + 1.0 / pi * sin(pi * min_distance / dh) * 0.5));
@@ -963,6 +1104,10 @@ void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s) {
     launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, s, a);
 }
 
+void launch_membrane_energies(const MembraneArgs &a, double *out, cudaStream_t s) {
+    if (a.n_membranes > 0) k_mem_energies<<<a.n_membranes, kTotalsThreads, 0, s>>>(a, out);
+}
+
 void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s) {
     const dim3 grid(a.spread_blocks);
     if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
@@ -970,6 +1115,7 @@ void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s) {
 }
 
 void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s) {
+    if (a.n_membranes > 0) k_visc_bins<<<a.n_membranes, 512, 0, s>>>(a);
     const int blocks = (a.nc + 255) / 256;
     if (a.visc_is_float) k_interior_viscosity<float><<<blocks, 256, 0, s>>>(a);
     else k_interior_viscosity<double><<<blocks, 256, 0, s>>>(a);

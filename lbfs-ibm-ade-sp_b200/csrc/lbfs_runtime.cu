@@ -112,6 +112,12 @@ namespace {
 // time stepping other than constant (lbfs_params.time_stepping 1, 3, 4)
 bool dynamic_dt(const lbfs_params &p) { return p.time_stepping != 0 && p.time_stepping != LBFS_DT_CONSTANT; }
 
+// Device buffer freed when it leaves scope (temporary storage).
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+
 template <typename R> FluidArgs<R> &fluid(lbfs_solver *s);
 template <> FluidArgs<double> &fluid<double>(lbfs_solver *s) { return s->f64; }
 template <> FluidArgs<float> &fluid<float>(lbfs_solver *s) { return s->f32; }
@@ -621,6 +627,10 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     va.instances = d_inst; va.cell_instance = d_cinst;
     va.visc_factor = s->fp32 ? (void *)s->f32.visc_factor : (void *)s->f64.visc_factor;
     va.visc_is_float = s->fp32 ? 1 : 0;
+    va.total_tris = s->total_tris;
+    if ((rc = s->alloc(&va.bins, n_rbc)) || (rc = s->alloc(&va.bin_start, (size_t)n_rbc * (kViscBins + 1))) ||
+        (rc = s->alloc(&va.bin_list, 4 * (size_t)s->total_tris)))
+        return rc;
     return LBFS_OK;
 }
 
@@ -970,6 +980,35 @@ extern "C" int lbfs_get_totals(lbfs_solver *s, double *out) {
     return LBFS_OK;
 }
 
+extern "C" int lbfs_get_energies(lbfs_solver *s, double *out) {
+    if (!s || !out) return set_error(LBFS_ERR_ARG, "null argument");
+    const int M = s->n_membranes;
+    if (M == 0) return LBFS_OK;
+    LBFS_CUDA(cudaSetDevice(s->device));
+    DevBuf sums;
+    LBFS_CUDA(cudaMalloc(&sums.p, sizeof(double) * 3 * (size_t)M));
+    launch_membrane_energies(s->ma, (double *)sums.p, s->stream);
+    LBFS_CUDA(cudaGetLastError());
+    std::vector<double> e(3 * (size_t)M);
+    std::vector<MembraneScalars> h(M);
+    std::vector<MembraneConst> c(M);
+    LBFS_CUDA(cudaMemcpyAsync(e.data(), sums.p, e.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaMemcpyAsync(h.data(), s->ma.ms, h.size() * sizeof(MembraneScalars), cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaMemcpyAsync(c.data(), s->ma.mc, c.size() * sizeof(MembraneConst), cudaMemcpyDeviceToHost, s->stream));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    for (int m = 0; m < M; m++) {
+        // Solver_gpu.cu:1073-1136
+        const MembraneScalars &q = h[m];
+        const double ade = 0.5 * c[m].global_bending_modulus * (q.MAD - q.MAD0) * (q.MAD - q.MAD0) / q.A0;
+        const double vol = 0.5 * c[m].volume_modulus * (q.V - q.V0) * (q.V - q.V0) / q.V0;
+        const double gar = 0.5 * c[m].global_area_modulus * (q.A - q.A0) * (q.A - q.A0) / q.A0;
+        double *o = out + 7 * (size_t)m;
+        o[0] = vol; o[1] = gar; o[2] = e[3 * m]; o[3] = e[3 * m + 1]; o[4] = ade; o[5] = e[3 * m + 2];
+        o[6] = vol + gar + o[2] + o[3] + ade + o[5];
+    }
+    return LBFS_OK;
+}
+
 extern "C" int lbfs_get_residuals(lbfs_solver *s, double *out) {
     if (!s || !out) return set_error(LBFS_ERR_ARG, "null argument");
     LBFS_CUDA(cudaSetDevice(s->device));
@@ -1234,11 +1273,6 @@ int adj_prepare(lbfs_solver *s) {
     return LBFS_OK;
 }
 
-// Device buffer freed when it leaves scope (temporary adjoint storage).
-struct DevBuf {
-    void *p = nullptr;
-    ~DevBuf() { if (p) cudaFree(p); }
-};
 
 int run_one_step(lbfs_solver *s) {
     if (visc_due(s, s->t)) {

@@ -152,6 +152,7 @@ def lib():
             "lbfs_set_nodes": [vp, _f64p],
             "lbfs_get_totals": [vp, _f64p],
             "lbfs_get_residuals": [vp, _f64p],
+            "lbfs_get_energies": [vp, _f64p],
             "lbfs_get_time_step": [vp, ctypes.POINTER(ctypes.c_double)],
             "lbfs_get_field": [vp, ctypes.c_int32, _f64p],
             "lbfs_keep_residuals": [vp, ctypes.c_int32],
@@ -227,7 +228,7 @@ def iptr(a):
 EXPORTED = [
     "lbfs_create", "lbfs_destroy", "lbfs_set_state", "lbfs_get_state", "lbfs_step", "lbfs_step_graph",
     "lbfs_synchronize", "lbfs_set_stream", "lbfs_get_nodes", "lbfs_set_nodes", "lbfs_get_totals",
-    "lbfs_get_residuals", "lbfs_get_time_step", "lbfs_get_field", "lbfs_keep_residuals", "lbfs_status", "lbfs_launches_per_step",
+    "lbfs_get_residuals", "lbfs_get_time_step", "lbfs_get_energies", "lbfs_get_field", "lbfs_keep_residuals", "lbfs_status", "lbfs_launches_per_step",
     "lbfs_set_profiling", "lbfs_get_phase_times",
     "lbfs_last_error", "lbfs_mesh_uniform_counts", "lbfs_mesh_build_uniform", "lbfs_rbc_build_springs",
     "lbfs_residual_rms_noalloc", "lbfs_get_launch_shape", "lbfs_set_launch_shape", "lbfs_autotune",

@@ -129,6 +129,13 @@ class GpuSolver:
             _abi.check(_abi.lib().lbfs_get_totals(self._h, _abi.ptr(out)))
         return out[: len(self.membranes)]
 
+    def energies(self):
+        """Per membrane: volume, global area, local area, local bending, ADE, spring, total energy."""
+        out = np.zeros((max(1, len(self.membranes)), 7))
+        if self.membranes:
+            _abi.check(_abi.lib().lbfs_get_energies(self._h, _abi.ptr(out)))
+        return out[: len(self.membranes)]
+
     def residuals(self):
         out = np.zeros(4)
         _abi.check(_abi.lib().lbfs_get_residuals(self._h, _abi.ptr(out)))

@@ -925,3 +925,36 @@ void oracle_get_totals(const oracle_case *o, double *out) {
 void oracle_get_residuals(const oracle_case *o, double *out) { memcpy(out, o->resid, 4 * sizeof(double)); }
 
 double oracle_time_step(const oracle_case *o) { return o->dt; }
+
+/* The energy log of Solver_gpu.cu:1060-1136 per membrane: volume, global area,
+ * local area, local bending, ADE, spring (WLC) and total energy; the per-spring
+ * terms of get_area_energy, get_bending_energy and get_spring_energy
+ * (spring_network.cu:1687-1768) summed in spring order. */
+void oracle_get_energies(const oracle_case *o, double *out) {
+    for (int r = 0; r < o->n_mem; r++) {
+        const omem *M = o->mem + r;
+        const lbfs_rbc_desc *d = &M->d;
+        const double w = 1 / d->wlc_ratio;
+        const double c1 = (0.25 / (1 - w) / (1 - w) - 0.25 + w);
+        const double c2 = w * w * (3.0 - 2.0 * w) / (1.0 - w) - 4 * c1 * w;
+        double la = 0, lb = 0, sp = 0;
+        for (int q = 0; q < M->n_springs; q++) {
+            const int i = M->spring0 + q;
+            const double *a = o->sarea + 2 * (size_t)i, *a0 = o->area0 + 2 * (size_t)i;
+            la += d->global_area_modulus * 0.5 *
+                  ((a[0] - a0[0]) * (a[0] - a0[0]) / a0[0] + (a[1] - a0[1]) * (a[1] - a0[1]) / a0[1]);
+            lb += 0.5 * d->local_bending_modulus * (o->curv[i] - o->curv0[i]) * (o->curv[i] - o->curv0[i]) /
+                  o->sarea[i]; /* the reference passes spring_area as the nodal area, indexed by spring */
+            const int na = o->spr[4 * i], nc = o->spr[4 * i + 2];
+            const double dx = o->x[nc] - o->x[na], dy = o->y[nc] - o->y[na], dz = o->z[nc] - o->z[na];
+            const double len = sqrt(dx * dx + dy * dy + dz * dz), sr = len / o->contour[i];
+            sp += 0.5 * o->kspr[i] * fabs(0.25 * o->contour[i] * (sr * sr * (3.0 - 2.0 * sr) / (1.0 - sr) - 4 * sr * c1 - c2));
+        }
+        const double ade = 0.5 * d->global_bending_modulus * (M->MAD - M->MAD0) * (M->MAD - M->MAD0) / M->A0;
+        const double vol = 0.5 * d->volume_modulus * (M->V - M->V0) * (M->V - M->V0) / M->V0;
+        const double gar = 0.5 * d->global_area_modulus * (M->A - M->A0) * (M->A - M->A0) / M->A0;
+        double *e = out + 7 * (size_t)r;
+        e[0] = vol; e[1] = gar; e[2] = la; e[3] = lb; e[4] = ade; e[5] = sp;
+        e[6] = vol + gar + la + lb + ade + sp;
+    }
+}

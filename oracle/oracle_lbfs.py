@@ -39,6 +39,7 @@ def lib():
         L.oracle_get_nodes.argtypes = [vp, ctypes.c_int, vp]
         L.oracle_get_totals.argtypes = [vp, vp]
         L.oracle_get_residuals.argtypes = [vp, vp]
+        L.oracle_get_energies.argtypes = [vp, vp]
         L.oracle_time_step.argtypes = [vp]
         L.oracle_time_step.restype = ctypes.c_double
         _lib = L
@@ -124,3 +125,9 @@ class OracleSolver:
 
     def time_step(self):
         return lib().oracle_time_step(self.h)
+
+    def energies(self):
+        out = np.zeros((max(1, len(self.membranes)), 7))
+        if self.membranes:
+            lib().oracle_get_energies(self.h, _p(out))
+        return out[: len(self.membranes)]

@@ -549,6 +549,7 @@ enum {
     REF_GHOST = 16,                               // 4*n_bc ghost (u,v,w,rho)
     REF_DT_LOCAL = 17,                            // n_cells delta_t_local
     REF_DELTA_T = 18,                             // 1: the last step's delta_t
+    REF_ENERGY = 19,                              // 7: volume, global area, local area, local bending, ADE, spring, total
 };
 
 extern "C" void ref_case_get(void *h, int which, double *out) {
@@ -621,6 +622,26 @@ extern "C" void ref_case_get(void *h, int which, double *out) {
     case REF_DELTA_T:
         out[0] = c->delta_t;
         break;
+    case REF_ENERGY: {
+        // the energy log of Solver_gpu.cu:1060-1136: host formulas for the
+        // global terms, the reference's kernels summed as total<128> block
+        // partials, of which the host adds the first n_tet_Blocks
+        const ref_params &p = c->p;
+        const int S = c->n_springs, nblk = (c->n_tets + 127) / 128;
+        std::vector<double> ea(S), eb(S), es(S);
+        get_area_energy(S, c->sarea.data(), c->sarea0.data(), ea.data(), p.global_area_modulus);
+        get_bending_energy(S, c->curv.data(), c->curv0.data(), eb.data(), c->sarea.data(), p.local_bending_modulus);
+        get_spring_energy(S, c->spr.data(), c->spr.data(), c->x.data(), c->y.data(), c->z.data(), 0,
+                          c->contour.data(), 1 / p.wlc_ratio, es.data(), c->kspring.data());
+        const double ade = 0.5 * p.global_bending_modulus * (c->MAD - c->MAD0) * (c->MAD - c->MAD0) / c->A0;
+        const double vol = 0.5 * p.volume_modulus * (c->V - c->V0) * (c->V - c->V0) / c->V0;
+        const double gar = 0.5 * p.global_area_modulus * (c->A - c->A0) * (c->A - c->A0) / c->A0;
+        const double la = block_tree_total(ea.data(), S, nblk), lb = block_tree_total(eb.data(), S, nblk),
+                     sp = block_tree_total(es.data(), S, nblk);
+        out[0] = vol; out[1] = gar; out[2] = la; out[3] = lb; out[4] = ade; out[5] = sp;
+        out[6] = vol + gar + la + lb + ade + sp;
+        break;
+    }
     }
 }
 

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "_ref", "libref_lbfs.so")
 REF_RHO, REF_U, REF_V, REF_W = 0, 1, 2, 3
 REF_T1, REF_GRAD, REF_RES_FACE, REF_RES, REF_FORCE = 4, 5, 6, 7, 8
 REF_NODE_X, REF_NODE_V, REF_NODE_F, REF_TOTALS, REF_VISC, REF_SPRING, REF_RESID, REF_GHOST = range(9, 17)
-REF_DT_LOCAL, REF_DELTA_T = 17, 18
+REF_DT_LOCAL, REF_DELTA_T, REF_ENERGY = 17, 18, 19
 
 
 class RefParams(ctypes.Structure):
@@ -164,7 +164,7 @@ class RefCase:
                 REF_GRAD: 12 * m.total_cells, REF_RES_FACE: 4 * m.n_faces, REF_RES: 4 * m.n_cells,
                 REF_FORCE: 3 * m.n_cells, REF_NODE_X: 3 * self.n_nodes, REF_NODE_V: 3 * self.n_nodes,
                 REF_NODE_F: 3 * self.n_nodes, REF_TOTALS: 6, REF_VISC: m.n_cells, REF_SPRING: 9 * self.n_springs,
-                REF_RESID: 4, REF_GHOST: 4 * m.n_bc, REF_DT_LOCAL: m.n_cells, REF_DELTA_T: 1}[which]
+                REF_RESID: 4, REF_GHOST: 4 * m.n_bc, REF_DT_LOCAL: m.n_cells, REF_DELTA_T: 1, REF_ENERGY: 7}[which]
         out = np.zeros(max(size, 1))
         lib().ref_case_get(self.h, which, _p(out))
         return out[:size]

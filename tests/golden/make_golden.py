@@ -95,13 +95,14 @@ def step_fixture(name, case, steps):
                preconditioning=case.params.preconditioning)
     if case.membranes:
         out.update(s1_nodes_x=rc.get(R.REF_NODE_X), s1_nodes_v=rc.get(R.REF_NODE_V), s1_nodes_f=rc.get(R.REF_NODE_F),
-                   s1_totals=rc.get(R.REF_TOTALS), s1_visc=rc.get(R.REF_VISC), s1_spring=rc.get(R.REF_SPRING))
+                   s1_totals=rc.get(R.REF_TOTALS), s1_visc=rc.get(R.REF_VISC), s1_spring=rc.get(R.REF_SPRING),
+                   s1_energy=rc.get(R.REF_ENERGY))
     rc.step(steps - 1)
     out.update(sN_state=np.stack(rc.state()), sN_resid=rc.get(R.REF_RESID), steps=steps,
                sN_dtl=rc.get(R.REF_DT_LOCAL), sN_dt=rc.get(R.REF_DELTA_T)[0])
     if case.membranes:
         out.update(sN_nodes_x=rc.get(R.REF_NODE_X), sN_nodes_f=rc.get(R.REF_NODE_F), sN_totals=rc.get(R.REF_TOTALS),
-                   sN_visc=rc.get(R.REF_VISC))
+                   sN_visc=rc.get(R.REF_VISC), sN_energy=rc.get(R.REF_ENERGY))
     np.savez_compressed(os.path.join(HERE, name), **out)
 
 

@@ -90,6 +90,7 @@ def test_gpu_matches_reference_fixture(golden, name):
         checks["totals"] = (s.totals()[0], g["s1_totals"])
         checks["visc"] = (s.field(_abi.LBFS_FIELD_VISC), g["s1_visc"])
         checks["spring"] = (s.field(_abi.LBFS_FIELD_SPRING), g["s1_spring"])
+        checks["energy"] = (s.energies()[0], g["s1_energy"])
     for key, (a, b) in checks.items():
         assert rel_err(a, b) < FP64_RTOL, (key, rel_err(a, b))
     s.step(int(g["steps"]) - 1, graph=True)
@@ -102,6 +103,7 @@ def test_gpu_matches_reference_fixture(golden, name):
         assert rel_err(s.nodes(_abi.LBFS_NODES_FORCE).ravel(), g["sN_nodes_f"]) < FP64_RTOL
         assert rel_err(s.totals()[0], g["sN_totals"]) < FP64_RTOL
         assert rel_err(s.field(_abi.LBFS_FIELD_VISC), g["sN_visc"]) < FP64_RTOL
+        assert rel_err(s.energies()[0], g["sN_energy"]) < FP64_RTOL
     assert s.status() == 0
     s.close()
 

@@ -75,6 +75,7 @@ def test_oracle_matches_reference(golden, name):
         checks["totals"] = (o.totals()[0], g["s1_totals"])
         checks["visc"] = (o.field(_abi.LBFS_FIELD_VISC), g["s1_visc"])
         checks["spring"] = (o.field(_abi.LBFS_FIELD_SPRING), g["s1_spring"])
+        checks["energy"] = (o.energies()[0], g["s1_energy"])
     for key, (a, b) in checks.items():
         assert rel_err(a, b) < FP64_RTOL, (key, rel_err(a, b))
     o.step(int(g["steps"]) - 1)
@@ -87,3 +88,4 @@ def test_oracle_matches_reference(golden, name):
         assert rel_err(o.nodes(_abi.LBFS_NODES_FORCE).ravel(), g["sN_nodes_f"]) < FP64_RTOL
         assert rel_err(o.totals()[0], g["sN_totals"]) < FP64_RTOL
         assert rel_err(o.field(_abi.LBFS_FIELD_VISC), g["sN_visc"]) < FP64_RTOL
+        assert rel_err(o.energies()[0], g["sN_energy"]) < FP64_RTOL
