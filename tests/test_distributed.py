@@ -56,6 +56,10 @@ def _worker(rank, world, port, q):
 
 
 def test_two_rank_gloo_replicas_match_single_process():
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_lbfs
+    oracle_lbfs.lib()  # build the oracle here, not in both ranks at once
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
