@@ -272,6 +272,9 @@ typedef struct lbfs_launch_shape {
     int32_t update_threads;         /* 128, 256 or 512 */
     int32_t update_blocks;          /* grid cap of the cell update, 1 .. LBFS_MAX_UPDATE_BLOCKS */
     int32_t spread_blocks;          /* grid of the IBM spread, 1 .. LBFS_MAX_SPREAD_BLOCKS */
+    int32_t flux_chunks;            /* 1, 2, 4 or 8: gradients and interior-face fluxes of an axis-aligned
+                                       mesh pipelined in that many chunks of cells on two streams
+                                       (0 = 1; meshes that do not allow it use 1) */
     double time_us[5];              /* autotune: [0] mean step time of the chosen shape (us) */
 } lbfs_launch_shape;
 int lbfs_get_launch_shape(lbfs_solver *s, lbfs_launch_shape *shape);

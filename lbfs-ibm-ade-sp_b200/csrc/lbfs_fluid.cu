@@ -40,9 +40,9 @@ __device__ __forceinline__ Vec4<R> ghost_state(const FluidArgs<R> &a, int b, con
 }
 
 template <typename R, int TB>
-__global__ void __launch_bounds__(TB) k_cell_gradients(FluidArgs<R> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nc) return;
+__global__ void __launch_bounds__(TB) k_cell_gradients(FluidArgs<R> a, int begin, int end) {
+    const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= end) return;
     const Vec4<R> own = a.state[i];
     R rr[3] = {0, 0, 0}, ru[3] = {0, 0, 0}, rv[3] = {0, 0, 0}, rw[3] = {0, 0, 0};
     int st[6];
@@ -383,9 +383,12 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
 // the rest z; warps never mix axes except at the two range boundaries.
 // TB threads per block, 640 / TB blocks per SM (at most 102 registers a thread).
 template <typename R, int TB>
-__global__ void __launch_bounds__(TB, 640 / TB) k_face_flux(FluidArgs<R> a) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= a.ni) return;
+__global__ void __launch_bounds__(TB, 640 / TB) k_face_flux(FluidArgs<R> a, FaceRanges r) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x, f;
+    if (t < r.count[0]) f = r.start[0] + t;
+    else if ((t -= r.count[0]) < r.count[1]) f = r.start[1] + t;
+    else if ((t -= r.count[1]) < r.count[2]) f = r.start[2] + t;
+    else return;
     Vec4<R> out;
     if (f < a.nfx) out = axis_face_flux<R, 0>(a, f);
     else if (f < a.nfx + a.nfy) out = axis_face_flux<R, 1>(a, f);
@@ -610,18 +613,27 @@ template <typename R> int k3_grid(const FluidArgs<R> &a) {
     return g < a.update_blocks ? g : a.update_blocks;
 }
 
+template <typename R> void launch_fluid_gradients_range(const FluidArgs<R> &a, int begin, int end, cudaStream_t s) {
+    if (end <= begin) return;
+    const int tb = a.tb_grad, g = (end - begin + tb - 1) / tb;
+    if (tb == 128) k_cell_gradients<R, 128><<<g, 128, 0, s>>>(a, begin, end);
+    else if (tb == 512) k_cell_gradients<R, 512><<<g, 512, 0, s>>>(a, begin, end);
+    else k_cell_gradients<R, 256><<<g, 256, 0, s>>>(a, begin, end);
+}
 template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStream_t s) {
-    const int tb = a.tb_grad, g = (a.nc + tb - 1) / tb;
-    if (tb == 128) k_cell_gradients<R, 128><<<g, 128, 0, s>>>(a);
-    else if (tb == 512) k_cell_gradients<R, 512><<<g, 512, 0, s>>>(a);
-    else k_cell_gradients<R, 256><<<g, 256, 0, s>>>(a);
+    launch_fluid_gradients_range<R>(a, 0, a.nc, s);
+}
+template <typename R> void launch_fluid_flux_axis_ranges(const FluidArgs<R> &a, const FaceRanges &r, cudaStream_t s) {
+    const int n = r.count[0] + r.count[1] + r.count[2];
+    if (!a.axis_aligned || n == 0) return;
+    const int tb = a.tb_flux, g = (n + tb - 1) / tb;
+    if (tb == 64) k_face_flux<R, 64><<<g, 64, 0, s>>>(a, r);
+    else if (tb == 256) k_face_flux<R, 256><<<g, 256, 0, s>>>(a, r);
+    else k_face_flux<R, 128><<<g, 128, 0, s>>>(a, r);
 }
 template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s) {
-    if (!a.axis_aligned || a.ni == 0) return;
-    const int tb = a.tb_flux, g = (a.ni + tb - 1) / tb;
-    if (tb == 64) k_face_flux<R, 64><<<g, 64, 0, s>>>(a);
-    else if (tb == 256) k_face_flux<R, 256><<<g, 256, 0, s>>>(a);
-    else k_face_flux<R, 128><<<g, 128, 0, s>>>(a);
+    const FaceRanges r = {{0, a.nfx, a.nfx + a.nfy}, {a.nfx, a.nfy, a.ni - a.nfx - a.nfy}};
+    launch_fluid_flux_axis_ranges<R>(a, r, s);
 }
 template <typename R> void launch_fluid_flux_general(const FluidArgs<R> &a, cudaStream_t s) {
     const int first = a.axis_aligned ? a.ni : 0;
@@ -669,6 +681,10 @@ template void launch_fluid_gradients<float>(const FluidArgs<float> &, cudaStream
 template void launch_fluid_flux<float>(const FluidArgs<float> &, cudaStream_t);
 template void launch_fluid_update<float>(const FluidArgs<float> &, cudaStream_t);
 template void launch_fluid_cfl<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_gradients_range<double>(const FluidArgs<double> &, int, int, cudaStream_t);
+template void launch_fluid_gradients_range<float>(const FluidArgs<float> &, int, int, cudaStream_t);
+template void launch_fluid_flux_axis_ranges<double>(const FluidArgs<double> &, const FaceRanges &, cudaStream_t);
+template void launch_fluid_flux_axis_ranges<float>(const FluidArgs<float> &, const FaceRanges &, cudaStream_t);
 template void launch_fluid_cfl<float>(const FluidArgs<float> &, cudaStream_t);
 
 }  // namespace lbfs

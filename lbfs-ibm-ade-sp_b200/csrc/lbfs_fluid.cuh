@@ -175,4 +175,11 @@ template <typename R> struct FluidArgs {
 
 constexpr int kCflBlocks = 148 * 4;  // grid of the CFL kernel (grid-stride over the cells)
 
+// Up to three ranges of axis-aligned interior faces (x, y, z) for one launch
+// of the face flux: a chunk of the pipelined K1 -> K2.
+struct FaceRanges {
+    int start[3], count[3];
+};
+constexpr int kMaxFluxChunks = 8;
+
 }  // namespace lbfs

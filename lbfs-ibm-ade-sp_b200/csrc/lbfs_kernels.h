@@ -13,6 +13,9 @@ constexpr int kSpreadMaxBlocks = 148 * 8;  // default spread grid cap (grid-stri
 constexpr int kK3BlocksLimit = LBFS_MAX_UPDATE_BLOCKS;  // partial-sum slots allocated for the update
 
 template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStream_t s);
+// K1 over cells [begin, end) and K2 over up to three axis face ranges (the pipelined form)
+template <typename R> void launch_fluid_gradients_range(const FluidArgs<R> &a, int begin, int end, cudaStream_t s);
+template <typename R> void launch_fluid_flux_axis_ranges(const FluidArgs<R> &a, const FaceRanges &r, cudaStream_t s);
 template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_flux_general(const FluidArgs<R> &a, cudaStream_t s);

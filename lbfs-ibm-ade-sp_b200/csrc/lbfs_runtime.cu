@@ -48,7 +48,16 @@ using namespace lbfs;
 
 struct lbfs_solver {
     int device = 0;
-    cudaStream_t stream = nullptr, stream2 = nullptr, stream3 = nullptr;
+    cudaStream_t stream = nullptr, stream2 = nullptr, stream3 = nullptr, stream4 = nullptr;
+    // pipelined K1 -> K2 (axis-aligned meshes): chunk c covers cells [chunk_cell[c], chunk_cell[c + 1])
+    // and the interior faces chunk_faces[c] (every face whose cells lie in chunks <= c)
+    int flux_chunks = 1;
+    bool chunkable = false;
+    std::vector<int> chunk_nb;   // neighbours of the interior faces (for the plan)
+    int chunk_start[3] = {0, 0, 0}, chunk_count[3] = {0, 0, 0};
+    std::vector<int> chunk_cell;
+    std::vector<FaceRanges> chunk_faces;
+    cudaEvent_t ev_chunk[kMaxFluxChunks] = {}, ev_flux = nullptr;
     cudaEvent_t ev_advected = nullptr, ev_sorted = nullptr;
     bool own_stream = true;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -643,6 +652,48 @@ cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
     return cudaEventRecord(ev, st);
 }
 
+// The chunk plan of the pipelined K1 -> K2.  It needs an axis-aligned mesh
+// whose interior faces have owner < neighbour and, within each axis range,
+// non-decreasing neighbours (the generator's order; ensembles keep it): then
+// the faces whose neighbour lies below a split form a prefix of each range,
+// and the faces of chunk c need the gradients of chunks <= c only.
+void plan_chunks(lbfs_solver *s, const int *owner, const int *neighbour, int nfx, int nfy, int nfz) {
+    s->chunkable = false;
+    const int ni = s->ni, nc = s->nc;
+    if (ni == 0 || nc < 2 * kMaxFluxChunks * 256 || !owner) return;
+    const int start[3] = {0, nfx, nfx + nfy}, count[3] = {nfx, nfy, nfz};
+    for (int ax = 0; ax < 3; ax++)
+        for (int f = start[ax]; f < start[ax] + count[ax]; f++)
+            if (!(owner[f] < neighbour[f]) || (f > start[ax] && neighbour[f] < neighbour[f - 1])) return;
+    s->chunkable = true;
+    s->chunk_nb.assign(neighbour, neighbour + ni);
+    for (int ax = 0; ax < 3; ax++) { s->chunk_start[ax] = start[ax]; s->chunk_count[ax] = count[ax]; }
+}
+
+// Cell splits and face ranges for K chunks (chunk_cell has K + 1 entries).
+void set_chunks(lbfs_solver *s, int K) {
+    if (!s->chunkable || K < 2) K = 1;
+    s->flux_chunks = K;
+    // gradients and interior fluxes (K each), boundary fluxes, update; membrane kernels; CFL
+    s->launches_per_step = 2 * K + 2 + (s->n_membranes > 0 ? 6 : 0) + (dynamic_dt(s->params) ? 1 : 0);
+    s->chunk_cell.assign(K + 1, 0);
+    s->chunk_faces.assign(K, FaceRanges{});
+    for (int c = 0; c <= K; c++) s->chunk_cell[c] = (int)((long long)s->nc * c / K);
+    if (K == 1) return;
+    int prev[3] = {0, 0, 0};
+    for (int c = 0; c < K; c++) {
+        FaceRanges &r = s->chunk_faces[c];
+        for (int ax = 0; ax < 3; ax++) {
+            const int *b = s->chunk_nb.data() + s->chunk_start[ax], n = s->chunk_count[ax];
+            // faces of this axis whose neighbour lies below the chunk's upper split
+            const int end = c == K - 1 ? n : (int)(std::lower_bound(b, b + n, s->chunk_cell[c + 1]) - b);
+            r.start[ax] = s->chunk_start[ax] + prev[ax];
+            r.count[ax] = end - prev[ax];
+            prev[ax] = end;
+        }
+    }
+}
+
 struct PhaseMark {
     lbfs_solver *s;
     int phase;
@@ -657,6 +708,43 @@ struct PhaseMark {
         }
     }
 };
+
+// K1 and K2 of a step: in sequence on the handle's stream, or pipelined in
+// chunks of cells: the gradients of each chunk on the handle's stream, the
+// interior-face fluxes of that chunk on a second stream as soon as they (and
+// the chunks before) are done, so the FP64-heavy fluxes of one chunk run beside
+// the load-latency-bound gradients of the next; the boundary faces (which read
+// ghost gradients) follow every K1, and the handle's stream joins the second.
+template <typename R> int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n) {
+    const int K = a.axis_aligned ? s->flux_chunks : 1;
+    if (K <= 1) {
+        { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
+        { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
+        *n += 2;
+        return LBFS_OK;
+    }
+    {
+        PhaseMark m(s, 1, s->stream);
+        for (int c = 0; c < K; c++) {
+            launch_fluid_gradients_range<R>(a, s->chunk_cell[c], s->chunk_cell[c + 1], s->stream);
+            LBFS_CUDA(cudaEventRecord(s->ev_chunk[c], s->stream));
+        }
+    }
+    for (int c = 0; c < K; c++) {
+        LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_chunk[c], 0));
+        if (c == 0 && s->kernel_events) LBFS_CUDA(record_event(s->ev_phase[2][0], s->stream4));
+        launch_fluid_flux_axis_ranges<R>(a, s->chunk_faces[c], s->stream4);
+    }
+    if (s->kernel_events) {
+        LBFS_CUDA(record_event(s->ev_phase[2][1], s->stream4));
+        s->phase_recorded[2] = true;
+    }
+    LBFS_CUDA(cudaEventRecord(s->ev_flux, s->stream4));
+    launch_fluid_flux_general<R>(a, s->stream);
+    LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_flux, 0));
+    *n += 2 * K + 1;
+    return LBFS_OK;
+}
 
 template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *launches) {
     FluidArgs<R> &a = fluid<R>(s);
@@ -680,15 +768,13 @@ template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *la
             LBFS_CUDA(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
             { PhaseMark m(s, 0, s->stream2); n += launch_membrane(s->ma, s->stream2, s->stream3, s->ev_advected, s->ev_sorted); }
             LBFS_CUDA(cudaEventRecord(s->ev_join, s->stream2));
-            { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
-            { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
+            int rc = enqueue_k1_k2<R>(s, a, &n);
+            if (rc) return rc;
             LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
-            n += 2;
         }
     } else {
-        { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
-        { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
-        n += 2;
+        int rc = enqueue_k1_k2<R>(s, a, &n);
+        if (rc) return rc;
     }
     { PhaseMark m(s, 3, s->stream); launch_fluid_update<R>(a, s->stream); }
     n += 1;
@@ -721,6 +807,10 @@ void free_all(lbfs_solver *s) {
     if (s->ev_advected) cudaEventDestroy(s->ev_advected);
     if (s->ev_sorted) cudaEventDestroy(s->ev_sorted);
     if (s->stream3) cudaStreamDestroy(s->stream3);
+    if (s->stream4) cudaStreamDestroy(s->stream4);
+    if (s->ev_flux) cudaEventDestroy(s->ev_flux);
+    for (cudaEvent_t e : s->ev_chunk)
+        if (e) cudaEventDestroy(e);
     if (s->stream2) cudaStreamDestroy(s->stream2);
     if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
 }
@@ -773,11 +863,16 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithPriority(&s->stream2, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithPriority(&s->stream3, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->stream4, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_flux, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_advected, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_sorted, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess)
         return fail(set_error(LBFS_ERR_CUDA, "stream/event creation failed"));
+    for (cudaEvent_t &e : s->ev_chunk)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return fail(set_error(LBFS_ERR_CUDA, "event creation failed"));
     if ((rc = setup_instances(s, mesh))) return fail(rc);
     rc = s->fp32 ? setup_fluid<float>(s, mesh) : setup_fluid<double>(s, mesh);
     if (rc) return fail(rc);
@@ -788,8 +883,9 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if (rc) return fail(rc);
     rc = s->fp32 ? setup_time_stepping<float>(s, mesh) : setup_time_stepping<double>(s, mesh);
     if (rc) return fail(rc);
-    // gradients, face flux (axis + general), update; membrane kernels; CFL
-    s->launches_per_step = 4 + (n_rbc > 0 ? 6 : 0) + (dynamic_dt(s->params) ? 1 : 0);
+    if (mesh->axis_aligned)
+        plan_chunks(s, mesh->owner, mesh->neighbour, mesh->n_face_x, mesh->n_face_y, mesh->n_face_z);
+    set_chunks(s, 1);
     *out = s;
     return LBFS_OK;
 }
@@ -1173,6 +1269,7 @@ template <typename R> void shape_to_args(lbfs_solver *s, const lbfs_launch_shape
     a.tb_grad = sh.gradient_threads; a.tb_flux = sh.flux_threads; a.tb_gen = sh.general_flux_threads;
     a.tb_update = sh.update_threads; a.update_blocks = sh.update_blocks;
     s->ma.spread_blocks = sh.spread_blocks;
+    set_chunks(s, sh.flux_chunks);
 }
 
 template <typename R> lbfs_launch_shape args_to_shape(lbfs_solver *s) {
@@ -1181,6 +1278,7 @@ template <typename R> lbfs_launch_shape args_to_shape(lbfs_solver *s) {
     sh.gradient_threads = a.tb_grad; sh.flux_threads = a.tb_flux; sh.general_flux_threads = a.tb_gen;
     sh.update_threads = a.tb_update; sh.update_blocks = a.update_blocks;
     sh.spread_blocks = s->ma.spread_blocks > 0 ? s->ma.spread_blocks : 1;
+    sh.flux_chunks = s->flux_chunks;
     return sh;
 }
 
@@ -1197,6 +1295,8 @@ int check_shape(const lbfs_launch_shape &sh) {
     if (sh.update_blocks < 1 || sh.update_blocks > LBFS_MAX_UPDATE_BLOCKS || sh.spread_blocks < 1 ||
         sh.spread_blocks > LBFS_MAX_SPREAD_BLOCKS)
         return set_error(LBFS_ERR_ARG, "launch shape: grid caps out of range");
+    if (!one_of(sh.flux_chunks, {0, 1, 2, 4, 8}))
+        return set_error(LBFS_ERR_ARG, "launch shape: flux_chunks must be 1, 2, 4 or 8");
     return LBFS_OK;
 }
 
@@ -1880,6 +1980,7 @@ int autotune_steps(lbfs_solver *s, int reps, lbfs_launch_shape *out, bool fp32) 
         {&lbfs_launch_shape::update_blocks, {148 * 2, 148 * 4, 148 * 8, 148 * 16}},
         {&lbfs_launch_shape::spread_blocks,
          membranes ? std::vector<int>{148, 296, 592, 1184, 2368} : std::vector<int>{}},
+        {&lbfs_launch_shape::flux_chunks, s->chunkable ? std::vector<int>{1, 2, 4, 8} : std::vector<int>{}},
     };
     lbfs_launch_shape cur = fp32 ? args_to_shape<float>(s) : args_to_shape<double>(s);
     double best = 0;

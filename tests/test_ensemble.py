@@ -88,7 +88,8 @@ def test_launch_shapes_do_not_change_fields():
     shapes = [dict(), dict(gradient_threads=128, flux_threads=64, general_flux_threads=256, update_threads=512,
                            update_blocks=296, spread_blocks=148),
               dict(gradient_threads=512, flux_threads=256, general_flux_threads=64, update_threads=128,
-                   update_blocks=2368, spread_blocks=2368)]
+                   update_blocks=2368, spread_blocks=2368),
+              dict(flux_chunks=2), dict(flux_chunks=8, gradient_threads=128)]
     out = []
     for sh in shapes:
         with GpuSolver(c.mesh, c.params, c.membranes) as s:
