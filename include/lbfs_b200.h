@@ -275,6 +275,9 @@ typedef struct lbfs_launch_shape {
     int32_t flux_chunks;            /* 1, 2, 4 or 8: gradients and interior-face fluxes of an axis-aligned
                                        mesh pipelined in that many chunks of cells on two streams
                                        (0 = 1; meshes that do not allow it use 1) */
+    int32_t membrane_cluster;       /* 8 or 16: a membrane's totals, spring and node forces as one
+                                       thread-block cluster of that many CTAs; 0: three kernels.  It
+                                       changes the summation order of V, A and MAD (rounding only) */
     double time_us[5];              /* autotune: [0] mean step time of the chosen shape (us) */
 } lbfs_launch_shape;
 int lbfs_get_launch_shape(lbfs_solver *s, lbfs_launch_shape *shape);

@@ -421,7 +421,9 @@ __global__ void __launch_bounds__(256) k_adjm_advect(MembraneArgs A, MemAdjArgs 
         // dt lambda_x' as the "force" the spread kernel distributes over the cells
         // (x dx^3, which its 1 / dx^3 removes)
         const double sc = J.dt * mc.gdx * mc.gdx * mc.gdx;
-        J.mb.sorted_force[J.mb.sorted_pos[n]] = make_double4(sc * lxp[0], sc * lxp[1], sc * lxp[2], 0.0);
+        J.mb.fx[n] = sc * lxp[0];
+        J.mb.fy[n] = sc * lxp[1];
+        J.mb.fz[n] = sc * lxp[2];
     }
 }
 

@@ -39,8 +39,11 @@ enum MembraneMode : int {
 struct alignas(16) SpreadRec {
     double w[12];  // 1D stencil weights of a node, x then y then z (4 slots per axis)
     int b0;        // first stencil cell along x
-    int pad[3];
+    int node;      // the node (global index): the spread reads its force in node order
+    int pad[2];
 };
+
+
 
 // Spring blocks of 128 per membrane the MAD partials can hold.
 constexpr int kMaxSpringBlocks = (3 * kMaxMembraneNodes + 127) / 128;
@@ -78,10 +81,11 @@ struct MembraneArgs {
     int *cell_start;             // [n_membranes + 1] first spread cell of each membrane (prefix over patches)
     unsigned int *sort_ticket;   // membranes whose patch is known in this launch; zero between launches
     int spread_blocks;           // grid of the spread kernel (grid-stride over the tiles)
+    int force_cluster;           // 8 or 16: totals, spring and node forces as one cluster of that many
+                                 // CTAs per membrane (k_mem_forces); 0: three kernels
     int *node_base;              // [3 total_nodes] first IBM stencil cell per axis at the current positions
     double *node_w;              // [12 total_nodes] 1D stencil weights per axis (4 slots) at the current positions
     int *sorted_pos;             // [total_nodes] position of each node in its membrane's sorted order
-    double4 *sorted_force;       // [total_nodes] node forces in sorted order (spread input)
     SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order (scratch)
     // LBFS_IBM_VANDERMONDE4 (rectilinear meshes, one instance): per axis the
     // vertex coordinates [n + 1] and the centroid coordinate of each cell row [n]

@@ -26,6 +26,7 @@
 //   P6  force spreading as a per-cell segmented reduction over the sorted
 //       nodes into a dense patch around the membrane (replaces
 //       spread_forces_on_structured_grid, :947-1024, and its CAS atomics).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -563,7 +564,88 @@ __global__ void __launch_bounds__(128) k_mem_nodeforce(MembraneArgs A) {
     A.fx[n] = f[0];
     A.fy[n] = f[1];
     A.fz[n] = f[2];
-    A.sorted_force[A.sorted_pos[n]] = make_double4(f[0], f[1], f[2], 0.0);
+}
+
+// ---- M2+M3 fused: totals, spring forces, MAD and node forces of a step -------
+// One thread-block cluster of kForceCluster CTAs (8, or 16 where the device
+// allows non-portable cluster sizes) per membrane.  The CTAs
+// split the triangles, then the springs, then the nodes; the membrane-wide
+// sums (volume, area, then MAD) are the CTAs' block sums added in rank order
+// through distributed shared memory, so every CTA holds the same values.  The
+// cluster barriers (release / acquire at cluster scope) also publish the
+// per-spring contributions that the node gather of another CTA reads.  Node
+// forces are written in node order; the spread reads them through the node
+// index of its sorted record, so this kernel does not wait for the sort.
+template <int kForceCluster>
+__global__ void __launch_bounds__(128) k_mem_forces(MembraneArgs A) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    __shared__ double sh[33];
+    __shared__ double part_va[2], part_mad[1];
+    const int m = blockIdx.y;
+    const int rank = (int)cluster.block_rank();
+    const int nth = kForceCluster * blockDim.x, tid = rank * blockDim.x + threadIdx.x;
+    const MembraneConst mc = A.mc[m];
+    MembraneScalars *ms = A.ms + m;
+    // volume and area (update_spring_network_tet_parameters + total<128>)
+    double pv = 0.0, pa = 0.0;
+    for (int lt = tid; lt < mc.n_tris; lt += nth) {
+        const int t = mc.tri0 + lt;
+        const int na = A.tri[3 * t], nb = A.tri[3 * t + 1], nc = A.tri[3 * t + 2];
+        const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]), c = d3(A.x[nc], A.y[nc], A.z[nc]);
+        const D3 normal = cross(b - a, c - a);
+        pv += dot(normal, tri_centroid(a, b, c)) / 6;
+        pa += sqrt(dot(normal, normal)) * 0.5;
+    }
+    const double bv = block_sum(pv, sh), ba = block_sum(pa, sh);
+    if (threadIdx.x == 0) { part_va[0] = bv; part_va[1] = ba; }
+    const double V0 = ms->V0, A0 = ms->A0, MADp = ms->MAD, MAD0p = ms->MAD0;
+    cluster.sync();
+    double V = 0.0, Ar = 0.0;
+    for (int r = 0; r < kForceCluster; r++) {
+        const double *p = cluster.map_shared_rank(part_va, r);
+        V += p[0];
+        Ar += p[1];
+    }
+    // spring forces (get_spring_forces_atomics) and the MAD terms of the first n_nodes springs
+    const double wr = mc.wlc_ratio;
+    const double sfc = (0.25 * wr * wr / ((wr - 1.0) * (wr - 1.0)) - 0.25 + 1.0 / wr);
+    const double vol_coef = -1 * mc.volume_modulus * (V / V0 - 1.0) / 6.0;
+    const double area_coef = -1 * mc.global_area_modulus * (Ar / A0 - 1.0);
+    const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (MADp - MAD0p) / A0;
+    const MembraneScalars cur = *ms;
+    double pm = 0.0;
+    for (int ls = tid; ls < mc.n_springs; ls += nth) {
+        const int sp = mc.spring0 + ls;
+        spring_forces(A, mc, cur, sp, false, sfc, vol_coef, area_coef, mad_coef);
+        if (ls < mc.n_nodes) pm += A.curv[sp] * (A.area[2 * sp] + A.area[2 * sp + 1]) * 1 / 3;
+    }
+    const double bm = block_sum(pm, sh);
+    if (threadIdx.x == 0) part_mad[0] = bm;
+    cluster.sync();
+    double mad = 0.0;
+    for (int r = 0; r < kForceCluster; r++) mad += *cluster.map_shared_rank(part_mad, r);
+    // node forces: each node's contributions in spring order
+    for (int ln = tid; ln < mc.n_nodes; ln += nth) {
+        const int n = mc.node0 + ln;
+        double f[3] = {0.0, 0.0, 0.0};
+        for (int e = A.inc_start[n]; e < A.inc_start[n + 1]; e++) {
+            const int code = __ldg(A.inc + e);
+            const double *o = A.contrib + 12 * (size_t)(code >> 2) + 3 * (code & 3);
+            f[0] += o[0]; f[1] += o[1]; f[2] += o[2];
+        }
+        A.fx[n] = f[0];
+        A.fy[n] = f[1];
+        A.fz[n] = f[2];
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+        ms->Vc = V;
+        ms->Ac = Ar;
+        ms->V = V;
+        ms->A = Ar;
+        ms->MAD = mad / Ar;
+    }
+    cluster.sync();  // no CTA leaves while another may still read its shared memory
 }
 
 // ---- M4: node bounds, nodes sorted by stencil base cell, spread records -----
@@ -727,7 +809,8 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         SpreadRec rec;
         for (int q = 0; q < 12; q++) rec.w[q] = A.node_w[12 * (size_t)n + q];
         rec.b0 = A.node_base[3 * (size_t)n];
-        rec.pad[0] = rec.pad[1] = rec.pad[2] = 0;
+        rec.node = n;
+        rec.pad[0] = rec.pad[1] = 0;
         A.spread_rec[mc.node0 + e] = rec;
         A.sorted_pos[n] = mc.node0 + e;
     }
@@ -787,7 +870,7 @@ __global__ void __launch_bounds__(256) k_mem_spread(MembraneArgs A) {
         }
         const int count = __shfl_sync(0xffffffffu, end, S * S - 1);
         const SpreadRec *rec = A.spread_rec + mc.node0;
-        const double4 *frc = A.sorted_force + mc.node0;
+
         double inv3 = 1 / mc.gdx / mc.gdx / mc.gdx;
         if (A.ibm_stencil == LBFS_IBM_VANDERMONDE4) {
             // divided by the cell's volume (spread_forces_on_non_uniform_grid, immersed_boundary_method.cu:851)
@@ -809,7 +892,7 @@ __global__ void __launch_bounds__(256) k_mem_spread(MembraneArgs A) {
             if (q < count) {
                 const int e = r_lo + q - (r_end - r_len);
                 const SpreadRec &w = rec[e];
-                const double4 F = frc[e];
+                const double3 F = make_double3(__ldg(A.fx + w.node), __ldg(A.fy + w.node), __ldg(A.fz + w.node));
                 const double wy = w.w[4 + S - 1 - r % S], wz = w.w[8 + S - 1 - r / S];
                 const double wx = w.w[ci - w.b0];
                 f[0] += F.x * wx * wy * wz * inv3;
@@ -1024,6 +1107,7 @@ __global__ void k_interior_viscosity(ViscArgs a) {
 void membrane_prepare(int sort_capacity) {
     const size_t smem = (size_t)(sort_capacity > 0 ? sort_capacity : 1) * sizeof(unsigned long long);
     cudaFuncSetAttribute(k_mem_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_mem_forces<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 
 namespace {
@@ -1031,19 +1115,28 @@ namespace {
 // the critical path of a step and runs beside the fluid kernels on a second
 // stream, so its blocks are placed ahead of pending fluid blocks.
 template <typename... Args>
-void launch_hi(void (*kernel)(Args...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const MembraneArgs &a) {
+void launch_hi(void (*kernel)(Args...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const MembraneArgs &a,
+               int cluster_x = 0) {
     int lo = 0, hi = 0;
     cudaDeviceGetStreamPriorityRange(&lo, &hi);
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributePriority;
     attr[0].val.priority = hi;
+    int n_attr = 1;
+    if (cluster_x > 0) {  // thread-block clusters of cluster_x CTAs along x
+        attr[1].id = cudaLaunchAttributeClusterDimension;
+        attr[1].val.clusterDim.x = cluster_x;
+        attr[1].val.clusterDim.y = 1;
+        attr[1].val.clusterDim.z = 1;
+        n_attr = 2;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = n_attr;
     cudaLaunchKernelEx(&cfg, kernel, a);
 }
 }  // namespace
@@ -1072,15 +1165,23 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     }
     launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, side ? s_side : s, a);
     if (side) cudaEventRecord(ev_sorted, s_side);
-    launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a);
-    launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
-    // node forces go to the sorted positions the sort wrote
+    int n = 4;
+    if (a.force_cluster == 16) {
+        launch_hi(k_mem_forces<16>, dim3(16, a.n_membranes), dim3(128), 0, s, a, 16);
+    } else if (a.force_cluster == 8) {
+        launch_hi(k_mem_forces<8>, dim3(8, a.n_membranes), dim3(128), 0, s, a, 8);
+    } else {  // separate kernels: more CTAs for the springs, two more launches
+        launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a);
+        launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
+        launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
+        n = 6;
+    }
+    // the spread reads the sorted records and the node forces
     if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
-    launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
     const dim3 grid(a.spread_blocks);
     if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
     else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a);
-    return 6;
+    return n;
 }
 
 void launch_membrane_tables(const MembraneArgs &a, cudaStream_t s) {

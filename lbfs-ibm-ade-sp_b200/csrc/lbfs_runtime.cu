@@ -462,6 +462,7 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     ma.n_membranes = n_rbc;
     ma.ibm_stencil = p.ibm_stencil;
     ma.delta_t = p.delta_t;
+    ma.force_cluster = 0;  // separate kernels; lbfs_autotune may choose a cluster of 8 or 16
     ma.nc = m->n_cells;
     ma.state_is_float = s->fp32 ? 1 : 0;
     if (n_rbc == 0) return LBFS_OK;
@@ -587,7 +588,7 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         (rc = s->alloc(&ma.bin_cursor, (size_t)total_patch + n_rbc)) ||
         (rc = s->alloc(&ma.cell_start, (size_t)n_rbc + 1)) || (rc = s->alloc(&ma.sort_ticket, 1)) ||
         (rc = s->alloc(&ma.spread_rec, (size_t)N)) || (rc = s->upload(&ma.sorted_pos, identity)) ||
-        (rc = s->alloc(&ma.sorted_force, (size_t)N)) || (rc = s->alloc(&ma.node_base, 3 * (size_t)N)) ||
+        (rc = s->alloc(&ma.node_base, 3 * (size_t)N)) ||
         (rc = s->alloc(&ma.node_w, 12 * (size_t)N)) ||
         (rc = s->alloc(&ma.mad_partials, (size_t)n_rbc * kMaxSpringBlocks)) ||
         (rc = s->alloc(&ma.mad_ticket, (size_t)n_rbc)))
@@ -596,7 +597,6 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     LBFS_CUDA(cudaMemset(ma.sort_ticket, 0, sizeof(unsigned int)));
     LBFS_CUDA(cudaMemset(ma.cell_start, 0, sizeof(int) * (n_rbc + 1)));
     LBFS_CUDA(cudaMemset(ma.patch_force, 0, sizeof(double) * 3 * (size_t)total_patch));
-    LBFS_CUDA(cudaMemset(ma.sorted_force, 0, sizeof(double4) * (size_t)N));
     ma.max_springs = 0;
     ma.max_patch_bound = 0;
     for (int r = 0; r < n_rbc; r++) {
@@ -675,7 +675,7 @@ void set_chunks(lbfs_solver *s, int K) {
     if (!s->chunkable || K < 2) K = 1;
     s->flux_chunks = K;
     // gradients and interior fluxes (K each), boundary fluxes, update; membrane kernels; CFL
-    s->launches_per_step = 2 * K + 2 + (s->n_membranes > 0 ? 6 : 0) + (dynamic_dt(s->params) ? 1 : 0);
+    s->launches_per_step = 2 * K + 2 + (s->n_membranes > 0 ? (s->ma.force_cluster > 0 ? 4 : 6) : 0) + (dynamic_dt(s->params) ? 1 : 0);
     s->chunk_cell.assign(K + 1, 0);
     s->chunk_faces.assign(K, FaceRanges{});
     for (int c = 0; c <= K; c++) s->chunk_cell[c] = (int)((long long)s->nc * c / K);
@@ -1269,6 +1269,7 @@ template <typename R> void shape_to_args(lbfs_solver *s, const lbfs_launch_shape
     a.tb_grad = sh.gradient_threads; a.tb_flux = sh.flux_threads; a.tb_gen = sh.general_flux_threads;
     a.tb_update = sh.update_threads; a.update_blocks = sh.update_blocks;
     s->ma.spread_blocks = sh.spread_blocks;
+    s->ma.force_cluster = sh.membrane_cluster;
     set_chunks(s, sh.flux_chunks);
 }
 
@@ -1279,6 +1280,7 @@ template <typename R> lbfs_launch_shape args_to_shape(lbfs_solver *s) {
     sh.update_threads = a.tb_update; sh.update_blocks = a.update_blocks;
     sh.spread_blocks = s->ma.spread_blocks > 0 ? s->ma.spread_blocks : 1;
     sh.flux_chunks = s->flux_chunks;
+    sh.membrane_cluster = s->ma.force_cluster;
     return sh;
 }
 
@@ -1297,6 +1299,8 @@ int check_shape(const lbfs_launch_shape &sh) {
         return set_error(LBFS_ERR_ARG, "launch shape: grid caps out of range");
     if (!one_of(sh.flux_chunks, {0, 1, 2, 4, 8}))
         return set_error(LBFS_ERR_ARG, "launch shape: flux_chunks must be 1, 2, 4 or 8");
+    if (!one_of(sh.membrane_cluster, {0, 8, 16}))
+        return set_error(LBFS_ERR_ARG, "launch shape: membrane_cluster must be 0, 8 or 16");
     return LBFS_OK;
 }
 
@@ -1421,13 +1425,17 @@ int adjm_prepare(lbfs_solver *s) {
         (rc = s->alloc(&mb.bin_start, (size_t)s->total_patch + M)) || (rc = s->alloc(&mb.cell_start, (size_t)M + 1)) ||
         (rc = s->alloc(&mb.bin_cursor, (size_t)s->total_patch + M)) ||
         (rc = s->alloc(&mb.sort_ticket, 1)) || (rc = s->upload(&mb.sorted_pos, identity)) ||
-        (rc = s->alloc(&mb.sorted_force, N)) || (rc = s->alloc(&mb.patch_force, 3 * (size_t)s->total_patch)) ||
+        (rc = s->alloc(&mb.fx, N)) || (rc = s->alloc(&mb.fy, N)) || (rc = s->alloc(&mb.fz, N)) ||
+        (rc = s->alloc(&mb.patch_force, 3 * (size_t)s->total_patch)) ||
         (rc = s->alloc(&mb.node_base, 3 * (size_t)N)) || (rc = s->alloc(&mb.node_w, 12 * (size_t)N)))
         return rc;
     LBFS_CUDA(cudaMemcpy(ms2, ma.ms, sizeof(MembraneScalars) * M, cudaMemcpyDeviceToDevice));
     LBFS_CUDA(cudaMemset(mb.sort_ticket, 0, sizeof(unsigned int)));
     LBFS_CUDA(cudaMemset(mb.cell_start, 0, sizeof(int) * (M + 1)));
-    LBFS_CUDA(cudaMemset(mb.sorted_force, 0, sizeof(double4) * N));
+    // the interpolation transpose's "forces" (dt lambda_x'), which its spread reads in node order
+    LBFS_CUDA(cudaMemset(mb.fx, 0, sizeof(double) * N));
+    LBFS_CUDA(cudaMemset(mb.fy, 0, sizeof(double) * N));
+    LBFS_CUDA(cudaMemset(mb.fz, 0, sizeof(double) * N));
     mb.ms = ms2;
     J.mb = mb;
     J.dt = s->params.delta_t;
@@ -1981,6 +1989,7 @@ int autotune_steps(lbfs_solver *s, int reps, lbfs_launch_shape *out, bool fp32) 
         {&lbfs_launch_shape::spread_blocks,
          membranes ? std::vector<int>{148, 296, 592, 1184, 2368} : std::vector<int>{}},
         {&lbfs_launch_shape::flux_chunks, s->chunkable ? std::vector<int>{1, 2, 4, 8} : std::vector<int>{}},
+        {&lbfs_launch_shape::membrane_cluster, membranes ? std::vector<int>{0, 8, 16} : std::vector<int>{}},
     };
     lbfs_launch_shape cur = fp32 ? args_to_shape<float>(s) : args_to_shape<double>(s);
     double best = 0;

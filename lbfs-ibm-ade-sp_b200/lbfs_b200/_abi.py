@@ -112,7 +112,7 @@ class LaunchShape(ctypes.Structure):
     _fields_ = [
         ("gradient_threads", ctypes.c_int32), ("flux_threads", ctypes.c_int32),
         ("general_flux_threads", ctypes.c_int32), ("update_threads", ctypes.c_int32),
-        ("update_blocks", ctypes.c_int32), ("spread_blocks", ctypes.c_int32), ("flux_chunks", ctypes.c_int32),
+        ("update_blocks", ctypes.c_int32), ("spread_blocks", ctypes.c_int32), ("flux_chunks", ctypes.c_int32), ("membrane_cluster", ctypes.c_int32),
         ("time_us", ctypes.c_double * 5),
     ]
 

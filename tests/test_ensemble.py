@@ -89,19 +89,25 @@ def test_launch_shapes_do_not_change_fields():
                            update_blocks=296, spread_blocks=148),
               dict(gradient_threads=512, flux_threads=256, general_flux_threads=64, update_threads=128,
                    update_blocks=2368, spread_blocks=2368),
-              dict(flux_chunks=2), dict(flux_chunks=8, gradient_threads=128)]
+              dict(flux_chunks=2), dict(flux_chunks=8, gradient_threads=128),
+              dict(membrane_cluster=0), dict(membrane_cluster=16, flux_chunks=4)]
     out = []
     for sh in shapes:
         with GpuSolver(c.mesh, c.params, c.membranes) as s:
             s.set_launch_shape(**sh)
             s.set_state(c.rho, c.u, c.v, c.w)
             s.step(6, graph=True)
-            out.append((s.state(), s.nodes(), s.residuals()))
-    for st, nd, res in out[1:]:
-        for a, b in zip(st, out[0][0]):
-            assert np.array_equal(a, b)
-        assert np.array_equal(nd, out[0][1])
-        assert rel_err(res, out[0][2]) < 1e-12  # block partials follow the update grid
+            out.append((s.state(), s.nodes(), s.residuals(), s.launch_shape()["membrane_cluster"]))
+    for st, nd, res, mcl in out[1:]:
+        if mcl == out[0][3]:
+            for a, b in zip(st, out[0][0]):
+                assert np.array_equal(a, b)
+            assert np.array_equal(nd, out[0][1])
+        else:  # the membrane's V, A and MAD are summed in another order: rounding-level differences
+            for a, b in zip(st, out[0][0]):
+                assert rel_err(a, b) < 1e-12
+            assert rel_err(nd, out[0][1]) < 1e-12
+        assert rel_err(res, out[0][2]) < 1e-9  # block partials follow the update grid
 
 
 @pytest.mark.gpu
@@ -118,6 +124,8 @@ def test_autotune_keeps_state_and_results():
         for a, b in zip(s.state(), before):
             assert np.array_equal(a, b)
         assert s.launch_shape()["update_blocks"] == chosen["update_blocks"]
+        # the reference handle takes the chosen shape too (membrane_cluster changes rounding)
+        ref.set_launch_shape(**{k: v for k, v in s.launch_shape().items() if k != "step_us"})
         s.step(4, graph=True)
         ref.step(4, graph=True)
         for a, b in zip(s.state(), ref.state()):
