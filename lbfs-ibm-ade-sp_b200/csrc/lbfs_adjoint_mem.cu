@@ -78,12 +78,19 @@ __device__ __forceinline__ V3 centroid3(V3 a, V3 b, V3 c) {
     return {(a.x + b.x + c.x) / 3.0, (a.y + b.y + c.y) / 3.0, (a.z + b.z + c.z) / 3.0};
 }
 
+// What the spring's force depends on linearly through its scalar inputs,
+// filled by the value pass of spring_eval: the volume, local-area, curvature
+// and length-gradient terms and the WLC polynomial.
+struct ScalarTerms {
+    double dvol[12], dnb[3], dnd[3], dcurve[12], dL[3], poly, curv_minus_c0;
+};
+
 // The spring force of the forward kernel (spring_forces), in dual numbers,
 // step mode, membrane viscosity zero.  Outputs the 12 node-force
 // contributions and the spring's MAD term curvature (A1 + A2) / 3.
 __device__ void spring_eval(const MembraneArgs &A, const MembraneConst &mc, int s, V3 a, V3 b, V3 c, V3 d,
                             Dual vol_coef, Dual area_coef, Dual mad_coef, Dual kspring, Dual kb, double sfc,
-                            Dual (&out)[12], Dual &mad_term) {
+                            Dual (&out)[12], Dual &mad_term, ScalarTerms *st = nullptr) {
     const V3 l = c - a;
     Dual length = dsqrt(dot(l, l));
     const V3 normal_a = cross(b - a, c - a), normal_b = cross(c - a, d - a);
@@ -191,6 +198,13 @@ __device__ void spring_eval(const MembraneArgs &A, const MembraneConst &mc, int 
     out[6] = fc.x; out[7] = fc.y; out[8] = fc.z;
     out[9] = fd.x; out[10] = fd.y; out[11] = fd.z;
     mad_term = curvature * (norm_1 + norm_2) * 1.0 / 3.0;
+    if (st) {
+        for (int j = 0; j < 12; j++) { st->dvol[j] = val(d_volume[j]); st->dcurve[j] = val(d_curve[j]); }
+        for (int j = 0; j < 3; j++) { st->dnb[j] = val(dn1[3 + j]); st->dnd[j] = val(dn2[3 + j]); }
+        st->dL[0] = val(dL_ds.x); st->dL[1] = val(dL_ds.y); st->dL[2] = val(dL_ds.z);
+        st->poly = val((0.25 / ((1.0 - sr) * (1.0 - sr))) - 0.25 + sr - sfc);
+        st->curv_minus_c0 = val(curvature) - c0;
+    }
 }
 
 // ---- IBM stencil weights and their derivatives ------------------------------
@@ -276,7 +290,8 @@ __global__ void __launch_bounds__(256) k_adjm_spread(MembraneArgs A, MemAdjArgs 
 }
 
 // ---- B2: spring adjoint by dual numbers ---------------------------------------
-constexpr int kDirs = 17;  // 12 coordinates, V, A, MAD_n, G_s, k_b
+constexpr int kDirs = 17;   // 12 coordinates, V, A, MAD_n, G_s, k_b
+constexpr int kPasses = 13; // the 12 coordinate directions in dual numbers, then one value pass for the 5 scalars
 
 __global__ void __launch_bounds__(128) k_adjm_springs(MembraneArgs A, MemAdjArgs J) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -293,23 +308,44 @@ __global__ void __launch_bounds__(128) k_adjm_springs(MembraneArgs A, MemAdjArgs
         p[q] = {mk(A.x[n], k == 3 * q ? 1.0 : 0.0), mk(A.y[n], k == 3 * q + 1 ? 1.0 : 0.0),
                 mk(A.z[n], k == 3 * q + 2 ? 1.0 : 0.0)};
     }
-    const Dual V = mk(ms.V, k == 12 ? 1.0 : 0.0), Ar = mk(ms.A, k == 13 ? 1.0 : 0.0);
-    const Dual MADp = mk(J.mad_n[m], k == 14 ? 1.0 : 0.0);
     const double ks = A.kspring[s];
-    const Dual kspring = mk(ks, k == 15 ? ks / mc.shear_modulus : 0.0);
-    const Dual kb = mk(mc.global_bending_modulus, k == 16 ? 1.0 : 0.0);
     const double wr = mc.wlc_ratio;
     const double sfc = (0.25 * wr * wr / ((wr - 1.0) * (wr - 1.0)) - 0.25 + 1.0 / wr);
-    const Dual vol_coef = -1.0 * mc.volume_modulus * (V / ms.V0 - 1.0) / 6.0;
-    const Dual area_coef = -1.0 * mc.global_area_modulus * (Ar / ms.A0 - 1.0);
-    const Dual mad_coef = -1.0 * 2.0 * kb * (MADp - ms.MAD0) / ms.A0;
+    const Dual vol_coef = mk(-1.0 * mc.volume_modulus * (ms.V / ms.V0 - 1.0) / 6.0);
+    const Dual area_coef = mk(-1.0 * mc.global_area_modulus * (ms.A / ms.A0 - 1.0));
+    const Dual mad_coef = mk(-1.0 * 2.0 * mc.global_bending_modulus * (J.mad_n[m] - ms.MAD0) / ms.A0);
     Dual out[12], term;
-    spring_eval(A, mc, s, p[0], p[1], p[2], p[3], vol_coef, area_coef, mad_coef, kspring, kb, sfc, out, term);
-    double acc = 0.0;
+    if (k < 12) {  // node coordinate 3 q + c: J^T lambda by one forward-mode pass
+        spring_eval(A, mc, s, p[0], p[1], p[2], p[3], vol_coef, area_coef, mad_coef, mk(ks),
+                    mk(mc.global_bending_modulus), sfc, out, term);
+        double acc = 0.0;
+        for (int q = 0; q < 4; q++)
+            for (int c = 0; c < 3; c++) acc += J.lam_F[3 * (size_t)node[q] + c] * out[3 * q + c].d;
+        if (s - mc.spring0 < mc.n_nodes) acc += J.lam_mad[m] / ms.A * term.d;
+        J.adjm[kDirs * (size_t)s + k] = acc;
+        return;
+    }
+    // V, A, MAD_n, G_s and k_b enter the force linearly, through vol_coef,
+    // area_coef (the local-area terms of nodes b and d), mad_coef and k_b (the
+    // curvature term) and the spring constant (the WLC term of a and c); the
+    // spring's MAD term does not depend on them.  One value pass gives them all.
+    ScalarTerms st;
+    spring_eval(A, mc, s, p[0], p[1], p[2], p[3], vol_coef, area_coef, mad_coef, mk(ks),
+                mk(mc.global_bending_modulus), sfc, out, term, &st);
+    double lf[12];
     for (int q = 0; q < 4; q++)
-        for (int c = 0; c < 3; c++) acc += J.lam_F[3 * (size_t)node[q] + c] * out[3 * q + c].d;
-    if (s - mc.spring0 < mc.n_nodes) acc += J.lam_mad[m] / ms.A * term.d;
-    J.adjm[kDirs * (size_t)s + k] = acc;
+        for (int c = 0; c < 3; c++) lf[3 * q + c] = J.lam_F[3 * (size_t)node[q] + c];
+    double dv = 0.0, dc = 0.0;
+    for (int j = 0; j < 12; j++) { dv += lf[j] * st.dvol[j]; dc += lf[j] * st.dcurve[j]; }
+    const double da = lf[3] * st.dnb[0] + lf[4] * st.dnb[1] + lf[5] * st.dnb[2] + lf[9] * st.dnd[0] +
+                      lf[10] * st.dnd[1] + lf[11] * st.dnd[2];
+    const double dl = (lf[6] - lf[0]) * st.dL[0] + (lf[7] - lf[1]) * st.dL[1] + (lf[8] - lf[2]) * st.dL[2];
+    double *o = J.adjm + kDirs * (size_t)s + 12;
+    o[0] = -mc.volume_modulus / (6.0 * ms.V0) * dv;                              // V
+    o[1] = -mc.global_area_modulus / ms.A0 * da;                                 // A
+    o[2] = -2.0 * mc.global_bending_modulus / ms.A0 * dc;                        // MAD_n
+    o[3] = -(ks / mc.shear_modulus) * st.poly * dl;                              // G_s (k_spring proportional to G_s)
+    o[4] = (-st.curv_minus_c0 - 2.0 * (J.mad_n[m] - ms.MAD0) / ms.A0) * dc;     // k_b
 }
 
 // Block sum in a fixed order (warp trees, then the warps in order).
@@ -486,7 +522,7 @@ int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, cons
                         const InstanceGrid *instances, cudaStream_t s) {
     const int node_blocks = (A.total_nodes * 32 + 255) / 256;
     k_adjm_spread<<<node_blocks, 256, 0, s>>>(A, J);
-    k_adjm_springs<<<dim3((A.total_springs + 127) / 128, kDirs), 128, 0, s>>>(A, J);
+    k_adjm_springs<<<dim3((A.total_springs + 127) / 128, kPasses), 128, 0, s>>>(A, J);
     k_adjm_reduce<<<A.n_membranes, 512, 0, s>>>(A, J);
     k_adjm_nodes<<<(A.total_nodes + 127) / 128, 128, 0, s>>>(A, J);
     if (A.state_is_float) k_adjm_advect<float><<<node_blocks, 256, 0, s>>>(A, J);
