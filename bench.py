@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--no-precision", action="store_true", help="skip the jittered 128^3 FP32/FP64 precision study")
     ap.add_argument("--precision-steps", type=int, default=1000)
     ap.add_argument("--adjoint-steps", type=int, default=500)
+    ap.add_argument("--launch-shape", default=None,
+                    help="JSON object of launch-shape fields to use instead of autotuning the headline workload "
+                         "(e.g. the launch_shape a plain run printed, so a profiler run launches the same kernels)")
     return ap.parse_args()
 
 
@@ -436,7 +439,12 @@ def main():
     s.set_state(c.rho, c.u, c.v, c.w)
     flush = torch.empty(512 * 2 ** 20, dtype=torch.uint8, device="cuda")  # 512 MB > 126 MB L2
     s.step(warmup, graph=True)
-    shape = s.autotune(reps=10)  # launch shape by whole-step timing (the library's autotuner)
+    if args.launch_shape:
+        fixed = {k: v for k, v in json.loads(args.launch_shape).items() if k not in ("time_us", "step_us")}
+        s.set_launch_shape(**fixed)
+        shape = dict(s.launch_shape(), source="--launch-shape")
+    else:
+        shape = s.autotune(reps=10)  # launch shape by whole-step timing (the library's autotuner)
     s.set_profiling(1)  # events around each whole step only
     s.step(2, graph=True)
     s.synchronize()

@@ -348,21 +348,9 @@ __global__ void __launch_bounds__(128) k_adjm_springs(MembraneArgs A, MemAdjArgs
     o[4] = (-st.curv_minus_c0 - 2.0 * (J.mad_n[m] - ms.MAD0) / ms.A0) * dc;     // k_b
 }
 
-// Block sum in a fixed order (warp trees, then the warps in order).
-__device__ double block_sum_fixed(double v, double *sh) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) sh[warp] = v;
-    __syncthreads();
-    double r = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) r += sh[w];
-    __syncthreads();
-    return r;
-}
-
 // ---- B3: per-membrane sums ----------------------------------------------------
-__global__ void __launch_bounds__(512) k_adjm_reduce(MembraneArgs A, MemAdjArgs J) {
-    __shared__ double sh[32];
+__global__ void __launch_bounds__(1024) k_adjm_reduce(MembraneArgs A, MemAdjArgs J) {
+    __shared__ double sh[32][5];
     const int m = blockIdx.x;
     const MembraneConst &mc = A.mc[m];
     double v[5] = {0, 0, 0, 0, 0};
@@ -370,8 +358,17 @@ __global__ void __launch_bounds__(512) k_adjm_reduce(MembraneArgs A, MemAdjArgs 
         const double *r = J.adjm + kDirs * (size_t)(mc.spring0 + ls) + 12;
         for (int q = 0; q < 5; q++) v[q] += r[q];
     }
-    double t[5];
-    for (int q = 0; q < 5; q++) t[q] = block_sum_fixed(v[q], sh);
+    // the five sums in one pass: warp trees, then the warps in order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int q = 0; q < 5; q++) {
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+        if (lane == 0) sh[warp][q] = v[q];
+    }
+    __syncthreads();
+    double t[5] = {0, 0, 0, 0, 0};
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+            for (int q = 0; q < 5; q++) t[q] += sh[w][q];
     if (threadIdx.x == 0) {
         const MembraneScalars &ms = A.ms[m];
         const double lam_mad_next = J.lam_mad[m];
@@ -523,7 +520,7 @@ int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, cons
     const int node_blocks = (A.total_nodes * 32 + 255) / 256;
     k_adjm_spread<<<node_blocks, 256, 0, s>>>(A, J);
     k_adjm_springs<<<dim3((A.total_springs + 127) / 128, kPasses), 128, 0, s>>>(A, J);
-    k_adjm_reduce<<<A.n_membranes, 512, 0, s>>>(A, J);
+    k_adjm_reduce<<<A.n_membranes, 1024, 0, s>>>(A, J);
     k_adjm_nodes<<<(A.total_nodes + 127) / 128, 128, 0, s>>>(A, J);
     if (A.state_is_float) k_adjm_advect<float><<<node_blocks, 256, 0, s>>>(A, J);
     else k_adjm_advect<double><<<node_blocks, 256, 0, s>>>(A, J);
