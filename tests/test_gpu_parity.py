@@ -130,6 +130,24 @@ def compare_with_oracle(c, steps, fields=True):
     o.close()
 
 
+def test_interior_viscosity_l4_vs_oracle():
+    # the binned interior-viscosity test (triangles binned by their y-z boxes) against the oracle's
+    # test of every triangle: a rotated L4 cell (5120 triangles over many bins), 805 cells inside;
+    # the update runs in the second step (t % period == 1)
+    c = cases.shear_rbc(n=32, level=4, radius_cells=8.0, rotate=True)
+    s, o = make(c), make(c, OracleSolver)
+    s.step(2)
+    o.step(2)
+    a, b = s.field(_abi.LBFS_FIELD_VISC), o.field(_abi.LBFS_FIELD_VISC)
+    assert np.count_nonzero(b != 1.0) > 500
+    assert rel_err(a, b) < FP64_RTOL
+    for x, y in zip(s.state(), o.state()):
+        assert rel_err(x, y) < FP64_RTOL
+    assert s.status() == 0
+    s.close()
+    o.close()
+
+
 def test_axis_faces_vs_oracle_non_cubic():
     compare_with_oracle(cases.poiseuille(n=12, ny=8, nz=10), 25)
 
