@@ -16,7 +16,8 @@
  * descriptors below carry exactly the arrays the reference copies (same
  * ordering, same meaning), lbfs_create replaces the set-up block, lbfs_step
  * replaces one iteration of the time loop, and lbfs_get_state replaces the
- * write-back into Solution.  INTEGRATION.md shows the C++ shim.
+ * write-back into Solution.  lbfs-ibm-ade-sp_b200/integration/Solver_gpu_lbfs.cpp
+ * is that method written over this ABI.
  *
  * Conventions: every entry point returns an int status (LBFS_OK = 0); no C++
  * exception crosses the boundary; all pointers in descriptors are HOST
@@ -89,8 +90,8 @@ typedef struct lbfs_mesh_desc {
     const int32_t *gradient_stencil; /* [6*nc]          gradient_cells          */
     const double *lhs_inverse;     /* [9*nc]  row major LHS_xx,LHS_xy,...,LHS_zz */
     const double *rhs;             /* [18*nc] RHS_arr (6 neighbours x 3)        */
-    const int32_t *bc_rho_type;    /* [nb]    1 Dirichlet, 2 Neumann            */
-    const int32_t *bc_vel_type;    /* [nb]    1 Dirichlet, 2 Neumann, 9 duct, 10 shear */
+    const int32_t *bc_rho_type;    /* [nb]    1 Dirichlet, 2 Neumann, 3 periodic */
+    const int32_t *bc_vel_type;    /* [nb]    1 Dirichlet, 2 Neumann, 3 periodic, 9 duct, 10 shear */
     const double *bc_values;       /* [4*nb]  (u, v, w, rho) = bcs_arr          */
     /* Uniform Eulerian grid seen by the IBM stencils (Solver_gpu.cu:448, 538-544). */
     double origin[3];              /* domain.origin_x/y/z                        */
@@ -107,6 +108,15 @@ typedef struct lbfs_mesh_desc {
      * (plateau_x, plateau_y, plateau_z, Solver_gpu.cu:637-639): read only by
      * LBFS_IBM_VANDERMONDE4; null otherwise. */
     const double *grid_x, *grid_y, *grid_z;
+    /* Periodic boundaries (type 3; Boundary_Conditions::periodic_node,
+     * Boundary_Conditions.cpp:417-432): per ghost the interior cell whose
+     * state (Solution::update_unstructured_bcs, Solution.cpp:777-803) and
+     * gradients (gradients::Get_LS_Gradients, gradients.cpp:428-440) a type-3
+     * ghost takes, e.g. from lbfs_mesh_find_periodic_nodes.  Required when a
+     * boundary has type 3, ignored for other ghosts; null otherwise.  The
+     * reference's GPU kernels implement no periodic type (LBFS.cu:1872-1918):
+     * this is its CPU solver's definition on the GPU path. */
+    const int32_t *periodic_node;
 } lbfs_mesh_desc;
 
 /* Scalars of global_variables / initial_conditions used by the step. */
@@ -158,6 +168,12 @@ typedef struct lbfs_rbc_desc {
     double wlc_ratio, curvature_ratio, volume_ratio, internal_viscosity_ratio, reference_length;
     int32_t pivkin_length, sphere_reference;
     int32_t instance;               /* ensemble instance the membrane lives in (0 without an ensemble) */
+    /* lagrangian_object::periodic (its XML key): at t % 5000 == 1, after the
+     * step's fluid update, a membrane whose mean node z exceeds
+     * origin_z + 0.75 Z moves by -0.5 Z in z (gpu_solver::check_periodic_object,
+     * Solver_gpu.cu:1027-1029, 1277-1304; the reference tests the mean of all
+     * objects' nodes together, here each membrane's own). */
+    int32_t periodic;
 } lbfs_rbc_desc;
 
 typedef struct lbfs_solver lbfs_solver;
@@ -409,6 +425,18 @@ int lbfs_mesh_build_jittered(double X, double Y, double Z, double dt, const doub
  * is each boundary face's patch index in the boundary file, names the patch
  * names separated by newlines.  The imported mesh steps with axis_aligned = 0
  * (mesh_type 3). */
+/* Periodic partners (Boundary_Conditions::assign_boundary_conditions,
+ * Boundary_Conditions.cpp:417-432): for every ghost b whose rho or velocity
+ * type is 3, out[b] = the interior cell whose centroid is nearest to the
+ * ghost's centroid moved by +translation or by -translation (the smaller
+ * distance; ties to the lower cell index); 0 for other ghosts, as the
+ * reference leaves them.  The reference searches all cells per ghost from an
+ * uninitialised cell index (`nb`, line 420); here the point is the ghost's
+ * own centroid, and the search bins the cells (O(cells + ghosts) instead of
+ * O(cells x ghosts)) with the same result as the all-cell search.  Needs the
+ * descriptor's sizes, owner/neighbour, cell_centroid and bc types. */
+int lbfs_mesh_find_periodic_nodes(const lbfs_mesh_desc *mesh, const double *translation, int32_t *out);
+
 int lbfs_mesh_write_openfoam(const char *dir, double X, double Y, double Z, double dt, const double *origin,
                              int32_t mesh_type, double plateau_width, double plateau_slope, double jitter,
                              uint64_t seed);

@@ -725,6 +725,116 @@ extern "C" int lbfs_mesh_import_openfoam(const char *dir, double visc, double fn
                          face_centroid, streaming_dt, cell_volume, cell_centroid, gradient_stencil, lhs_inverse, rhs);
 }
 
+// Periodic partners (Boundary_Conditions::assign_boundary_conditions,
+// Boundary_Conditions.cpp:417-432): the interior cell nearest to a point,
+// distance |c_i - p| formed as vector_var::Magnitude does, the lowest index
+// among equal distances (the reference's strict < over ascending i).  The
+// cells are binned on a uniform grid over their centroids' box and the search
+// walks shells of bins outwards: a cell in a bin r shells away from the
+// point's (clamped) bin is at least (r - 1) times the smallest bin width away,
+// so the walk stops once the best distance is below r times that width; the
+// result is the all-cell search's.
+namespace {
+struct CellBins {
+    int n[3];
+    double lo[3], w[3], wmin;
+    std::vector<int> start, list;
+};
+
+CellBins bin_cells(const double *cen, int nc) {
+    CellBins b;
+    double hi[3];
+    for (int a = 0; a < 3; a++) b.lo[a] = hi[a] = cen[a];
+    for (int i = 1; i < nc; i++)
+        for (int a = 0; a < 3; a++) {
+            b.lo[a] = std::min(b.lo[a], cen[3 * (size_t)i + a]);
+            hi[a] = std::max(hi[a], cen[3 * (size_t)i + a]);
+        }
+    const double ext_max = std::max(hi[0] - b.lo[0], std::max(hi[1] - b.lo[1], hi[2] - b.lo[2]));
+    const double h = ext_max > 0 ? ext_max / std::cbrt((double)nc) : 1.0;
+    b.wmin = std::numeric_limits<double>::infinity();
+    for (int a = 0; a < 3; a++) {
+        const double ext = hi[a] - b.lo[a];
+        b.n[a] = ext > 0 ? std::max(1, std::min(1 << 10, (int)std::ceil(ext / h))) : 1;
+        b.w[a] = ext > 0 ? ext / b.n[a] : h;
+        b.wmin = std::min(b.wmin, b.w[a]);
+    }
+    const size_t nbins = (size_t)b.n[0] * b.n[1] * b.n[2];
+    b.start.assign(nbins + 1, 0);
+    std::vector<int> key(nc);
+    for (int i = 0; i < nc; i++) {
+        int k[3];
+        for (int a = 0; a < 3; a++) {
+            const int q = (int)std::floor((cen[3 * (size_t)i + a] - b.lo[a]) / b.w[a]);
+            k[a] = std::max(0, std::min(b.n[a] - 1, q));
+        }
+        key[i] = k[0] + b.n[0] * (k[1] + b.n[1] * k[2]);
+        b.start[key[i] + 1]++;
+    }
+    for (size_t q = 0; q < nbins; q++) b.start[q + 1] += b.start[q];
+    b.list.resize(nc);
+    std::vector<int> fill(b.start.begin(), b.start.end() - 1);
+    for (int i = 0; i < nc; i++) b.list[fill[key[i]]++] = i;  // ascending cell index within a bin
+    return b;
+}
+
+void nearest_cell(const CellBins &b, const double *cen, V3 p, double &best, int &best_i) {
+    int c[3];
+    const double pp[3] = {p.x, p.y, p.z};
+    for (int a = 0; a < 3; a++) {
+        const double q = std::floor((pp[a] - b.lo[a]) / b.w[a]);
+        c[a] = (int)std::max(0.0, std::min((double)(b.n[a] - 1), q));
+    }
+    const int rmax = std::max(b.n[0], std::max(b.n[1], b.n[2]));
+    for (int r = 0; r <= rmax; r++) {
+        for (int k = c[2] - r; k <= c[2] + r; k++) {
+            if (k < 0 || k >= b.n[2]) continue;
+            for (int j = c[1] - r; j <= c[1] + r; j++) {
+                if (j < 0 || j >= b.n[1]) continue;
+                for (int i = c[0] - r; i <= c[0] + r; i++) {
+                    if (i < 0 || i >= b.n[0]) continue;
+                    const int cheb = std::max(std::abs(i - c[0]), std::max(std::abs(j - c[1]), std::abs(k - c[2])));
+                    if (cheb != r) continue;
+                    const int bin = i + b.n[0] * (j + b.n[1] * k);
+                    for (int q = b.start[bin]; q < b.start[bin + 1]; q++) {
+                        const int cell = b.list[q];
+                        const V3 ci = {cen[3 * (size_t)cell], cen[3 * (size_t)cell + 1], cen[3 * (size_t)cell + 2]};
+                        const double d = mag(sub(ci, p));
+                        if (d < best || (d == best && cell < best_i)) {
+                            best = d;
+                            best_i = cell;
+                        }
+                    }
+                }
+            }
+        }
+        if (best < r * b.wmin) break;
+    }
+}
+}  // namespace
+
+extern "C" int lbfs_mesh_find_periodic_nodes(const lbfs_mesh_desc *m, const double *translation, int32_t *out) {
+    if (!m || !translation || !out || !m->cell_centroid || m->n_cells <= 0 || m->n_bc < 0 ||
+        (m->n_bc > 0 && (!m->bc_rho_type || !m->bc_vel_type)))
+        return lbfs::set_error(LBFS_ERR_ARG, "lbfs_mesh_find_periodic_nodes: bad arguments");
+    const int nc = m->n_cells;
+    const double *cen = m->cell_centroid;
+    const CellBins bins = bin_cells(cen, nc);
+    const V3 T = {translation[0], translation[1], translation[2]};
+    for (int b = 0; b < m->n_bc; b++) {
+        out[b] = 0;
+        if (m->bc_rho_type[b] != 3 && m->bc_vel_type[b] != 3) continue;
+        const size_t g = (size_t)nc + b;
+        const V3 c = {cen[3 * g], cen[3 * g + 1], cen[3 * g + 2]};
+        double best = std::numeric_limits<double>::infinity();
+        int best_i = -1;
+        nearest_cell(bins, cen, add(c, T), best, best_i);
+        nearest_cell(bins, cen, sub(c, T), best, best_i);
+        out[b] = best_i;
+    }
+    return LBFS_OK;
+}
+
 // Spring connectivity: the neighbour-ring construction, duplicate removal and
 // spring hashing of lagrangian_object::osay_mesh_read (lagrangian_object.cpp:
 // 299-481).  The ring is assembled by the same sequence of pair swaps, so the

@@ -13,16 +13,22 @@ namespace lbfs {
 // ------------------------------------------------------------------ K1 ----
 
 // Ghost-cell macros from the owner state (update_unstructured_bcs,
-// LBFS.cu:1868-1918).  Types outside {1,2} / {1,2,9,10} are rejected at
+// LBFS.cu:1868-1918).  Type 3 (periodic) takes the partner cell's state, as
+// the reference's CPU solver does (Solution::update_unstructured_bcs,
+// Solution.cpp:777-803).  Types outside {1,2,3} / {1,2,3,9,10} are rejected at
 // creation, so every branch here assigns.
 template <typename R>
 __device__ __forceinline__ Vec4<R> ghost_state(const FluidArgs<R> &a, int b, const Vec4<R> &own) {
     const Vec4<R> bc = a.bc_val[b];
     Vec4<R> g;
-    if (a.bc_rho_type[b] == 1) g.rho = bc.rho - (own.rho - bc.rho);
-    else g.rho = own.rho;
-    const int vt = a.bc_vel_type[b];
-    if (vt == 2) {
+    const int rt = a.bc_rho_type[b], vt = a.bc_vel_type[b];
+    const Vec4<R> p = (rt == 3 || vt == 3) ? a.state[a.bc_periodic[b]] : own;
+    if (rt == 1) g.rho = bc.rho - (own.rho - bc.rho);
+    else if (rt == 2) g.rho = own.rho;
+    else g.rho = p.rho;
+    if (vt == 3) {
+        g.u = p.u; g.v = p.v; g.w = p.w;
+    } else if (vt == 2) {
         g.u = own.u; g.v = own.v; g.w = own.w;
     } else {
         R ut = bc.u;
@@ -85,7 +91,10 @@ __global__ void __launch_bounds__(TB) k_cell_gradients(FluidArgs<R> a, int begin
     reinterpret_cast<GradRec<R> *>(a.grad)[i] = gr;
     if (!has_ghost) return;
     // Ghost states and ghost gradients of this cell's boundary faces
-    // (get_bc_gradients, LBFS.cu:1941-2044).
+    // (get_bc_gradients, LBFS.cu:1941-2044).  A periodic component's ghost
+    // gradient is its partner's, which this launch may not have formed yet:
+    // the boundary-face flux kernel reads it from the partner and stores it
+    // here.
     for (int q = 0; q < 6; q++) {
         const int j = st[q];
         if (j < a.nc) continue;
@@ -96,7 +105,7 @@ __global__ void __launch_bounds__(TB) k_cell_gradients(FluidArgs<R> a, int begin
         R gg[12];
         const R d[4] = {gs.rho - own.rho, gs.u - own.u, gs.v - own.v, gs.w - own.w};
         const bool dir_rho = a.bc_rho_type[b] == 1;
-        const bool dir_vel = a.bc_vel_type[b] != 2;
+        const bool dir_vel = a.bc_vel_type[b] != 2 && a.bc_vel_type[b] != 3;
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             const bool dirichlet = (m == 0) ? dir_rho : dir_vel;
@@ -124,23 +133,6 @@ struct Dir {
 };
 __device__ __forceinline__ Dir dir_of(int k) { return {c_ex(k), c_ey(k), c_ez(k)}; }
 
-// Interface equilibrium, BGK relaxation towards the lattice equilibria and
-// the flux through the face: calculate_flux_at_interface (LBFS.cu:1462-1648)
-// and its axis-aligned forms (LBFS.cu:3648-4092).  `axis` < 0 selects the
-// general three-component form with the face normal; otherwise only the
-// face-normal component is formed.
-//
-// The relaxed populations are f_k - tau (f_k - fl_k), f_k the interface
-// equilibrium, so the flux tensor is (1 - tau) F_eq + tau F_fl, F_fl the
-// first and second moments of the reconstructed fl_k over the directions
-// crossing the face and F_eq those of the equilibrium.  The D3Q15 weights
-// make the equilibrium moments exact closed forms (sum w e = 0,
-// sum w e e = I / 3, sum w e e e e = (dd + dd + dd) / 9):
-//   sum_k e_c f_k = rho u_c,  sum_k e_c e_m f_k = rho (q u_c u_m + d_cm / 3)
-// (q the preconditioning factor); in the deviation form (f' = f - w rho0)
-// the second moment's d_cm term is rho' / 3.  The reference sums the 15
-// equilibria explicitly; the closed form is the same quantity with fewer
-// roundings.
 // Moments of the reconstructed populations, accumulated direction by
 // direction in the order k = 0..14 (the same sums and order as over a stored
 // fl[15], with 8-16 accumulators live instead of 15 populations).
@@ -315,6 +307,24 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
     const R dt = geo.dt;
     const R S1[4] = {s1.rho, s1.u, s1.v, s1.w}, S2[4] = {s2.rho, s2.u, s2.v, s2.w};
     R pi[4], pn[4], p0[4], g3[12];
+    if (is_bc) {
+        // Periodic ghost (type 3): the partner's gradients (gradients::
+        // Get_LS_Gradients, gradients.cpp:428-440), complete now that every
+        // cell's gradients are formed; stored in the ghost's record too.
+        const int b = oc.y - a.nc;
+        const int rt = a.bc_rho_type[b], vt = a.bc_vel_type[b];
+        if (rt == 3 || vt == 3) {
+            R gp[12];
+            load_grad(a.grad + (size_t)12 * a.bc_periodic[b], gp);
+#pragma unroll
+            for (int t = 0; t < 12; t++)
+                if ((t < 3) ? rt == 3 : vt == 3) g2[t] = gp[t];
+            GradRec<R> gr;
+#pragma unroll
+            for (int t = 0; t < 12; t++) gr.g[t] = g2[t];
+            reinterpret_cast<GradRec<R> *>(a.grad)[oc.y] = gr;
+        }
+    }
     if (geo.bc_branch != R(0)) {
         const int b = oc.y - a.nc;
         const Vec4<R> bc = a.bc_val[b];

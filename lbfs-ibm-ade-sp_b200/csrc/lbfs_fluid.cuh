@@ -131,6 +131,7 @@ template <typename R> struct FluidArgs {
     const int2 *stencil;         // [3*nc] (6 stencil entries per cell)
     const LsRec<R> *ls;          // [nc]
     const int *bc_rho_type, *bc_vel_type;
+    const int *bc_periodic;      // [nb] partner cell of a type-3 ghost (Boundary_Conditions::periodic_node)
     const Vec4<R> *bc_val;       // [nb] (u, v, w, rho - rho0)
     const BcRec<R> *bc_rec;      // [nb]
     // K2 geometry

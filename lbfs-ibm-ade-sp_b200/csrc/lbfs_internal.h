@@ -39,7 +39,7 @@ struct MembraneScalars {
 struct MembraneConst {
     int node0, n_nodes, tri0, n_tris, spring0, n_springs;
     int inc0;  // start of this membrane's node->(spring,slot) incidence list
-    int pad;
+    int periodic;  // lagrangian_object::periodic (check_periodic_object)
     double volume_modulus, local_area_modulus, global_area_modulus, shear_modulus;
     double global_bending_modulus, local_bending_modulus, membrane_thickness, viscosity;
     double wlc_ratio, curvature_ratio, volume_ratio, internal_viscosity_ratio, reference_length;
@@ -48,6 +48,7 @@ struct MembraneConst {
     int cell0, gnx, gny, gnz;
     double gorigin[3], gdx, gdh;
     int instance, patch_bound;  // patch cells the spread launch covers
+    double domain_z0, domain_Z;  // origin_z and Z of the instance's domain (check_periodic_object)
 };
 
 // One ensemble instance as the kernels see it.

@@ -146,5 +146,7 @@ void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s);
 void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s);
 // per membrane the local area, local bending and spring energy sums, out[3 n_membranes]
 void launch_membrane_energies(const MembraneArgs &a, double *out, cudaStream_t s);
+// check_periodic_object for the membranes flagged periodic (after a step's fluid update)
+void launch_membrane_wrap(const MembraneArgs &a, cudaStream_t s);
 
 }  // namespace lbfs

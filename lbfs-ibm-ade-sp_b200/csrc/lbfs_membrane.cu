@@ -947,6 +947,39 @@ __global__ void __launch_bounds__(kTotalsThreads) k_mem_energies(MembraneArgs A,
     }
 }
 
+// ---- periodic object (gpu_solver::check_periodic_object, Solver_gpu.cu:1277-1304) ----
+// One CTA of 128 threads per membrane flagged periodic.  The mean z of its
+// nodes is summed as total<128> does (common_kernels.hpp:71-94: every 256
+// consecutive nodes tree-summed, stride 128 down to 1) with the chunk sums
+// added in order from 0, as the host adds the block partials; a mean above
+// origin_z + 0.75 Z moves every node by -0.5 Z (add_double).
+__global__ void __launch_bounds__(128) k_mem_wrap(MembraneArgs A) {
+    __shared__ double part[256];
+    __shared__ bool shift;
+    const int m = blockIdx.x;
+    const MembraneConst &mc = A.mc[m];
+    if (!mc.periodic) return;
+    const int t = threadIdx.x;
+    const double *z = A.z + mc.node0;
+    double sum = 0.0;
+    for (int s0 = 0; s0 < mc.n_nodes; s0 += 256) {
+        part[t] = s0 + t < mc.n_nodes ? z[s0 + t] : 0.0;
+        part[128 + t] = s0 + 128 + t < mc.n_nodes ? z[s0 + 128 + t] : 0.0;
+        for (int stride = 128; stride >= 1; stride >>= 1) {
+            __syncthreads();
+            if (t < stride) part[t] += part[t + stride];
+        }
+        __syncthreads();
+        if (t == 0) sum = sum + part[0];
+        __syncthreads();
+    }
+    if (t == 0) shift = sum / mc.n_nodes > mc.domain_z0 + 0.75 * mc.domain_Z;
+    __syncthreads();
+    if (!shift) return;
+    const double dz = -0.5 * mc.domain_Z;
+    for (int n = t; n < mc.n_nodes; n += blockDim.x) A.z[mc.node0 + n] = A.z[mc.node0 + n] + dz;
+}
+
 // ---- interior viscosity (update_interior_viscosities_plucker, immersed_boundary_method.cu:389-527) ----
 //
 // The reference tests every cell of the membrane's box (+- 2 delta_h) against
@@ -1207,6 +1240,10 @@ void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s) {
 
 void launch_membrane_energies(const MembraneArgs &a, double *out, cudaStream_t s) {
     if (a.n_membranes > 0) k_mem_energies<<<a.n_membranes, kTotalsThreads, 0, s>>>(a, out);
+}
+
+void launch_membrane_wrap(const MembraneArgs &a, cudaStream_t s) {
+    if (a.n_membranes > 0) k_mem_wrap<<<a.n_membranes, 128, 0, s>>>(a);
 }
 
 void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s) {

@@ -63,6 +63,8 @@ struct lbfs_solver {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     lbfs_params params{};
     bool fp32 = false;
+    bool periodic = false;  // some boundary has type 3
+    bool wrap_membranes = false;  // some membrane is periodic (check_periodic_object)
     int nc = 0, nf = 0, ni = 0, nb = 0;
     int n_membranes = 0, total_nodes = 0, total_springs = 0, total_tris = 0;
     std::vector<void *> allocs;
@@ -155,10 +157,15 @@ int check_mesh(const lbfs_mesh_desc *m) {
             return set_error(LBFS_ERR_ARG, "gradient stencil index out of range");
     for (int b = 0; b < m->n_bc; b++) {
         const int rt = m->bc_rho_type[b], vt = m->bc_vel_type[b];
-        if (!(rt == 1 || rt == 2) || !(vt == 1 || vt == 2 || vt == 9 || vt == 10))
+        if (!(rt == 1 || rt == 2 || rt == 3) || !(vt == 1 || vt == 2 || vt == 3 || vt == 9 || vt == 10))
             return set_error(LBFS_ERR_UNSUPPORTED,
-                             "boundary types: rho must be 1 or 2, velocity 1, 2, 9 or 10 (the reference GPU kernels "
-                             "implement no others, LBFS.cu:1872-1918)");
+                             "boundary types: rho must be 1, 2 or 3, velocity 1, 2, 3, 9 or 10 (the reference GPU "
+                             "kernels implement 1, 2, 9 and 10, LBFS.cu:1872-1918; 3 is its CPU solver's periodic)");
+        if (rt == 3 || vt == 3) {
+            if (!m->periodic_node) return set_error(LBFS_ERR_ARG, "periodic boundary without periodic_node");
+            if (m->periodic_node[b] < 0 || m->periodic_node[b] >= m->n_cells)
+                return set_error(LBFS_ERR_ARG, "periodic_node must be an interior cell");
+        }
     }
     for (int i = 0; i < m->n_cells; i++)
         if (!(m->cell_volume[i] > 0)) return set_error(LBFS_ERR_ARG, "cell volume must be positive");
@@ -192,12 +199,16 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         for (int q = 0; q < 9; q++) ls[i].lhs[q] = (R)m->lhs_inverse[9 * (size_t)i + q];
         ls[i].pad = 0;
     }
-    std::vector<int> rt(nb), vt(nb);
+    std::vector<int> rt(nb), vt(nb), per(nb, 0);
     std::vector<Vec4<R>> bcv(nb);
     std::vector<BcRec<R>> bcr(nb);
     for (int b = 0; b < nb; b++) {
         rt[b] = m->bc_rho_type[b];
         vt[b] = m->bc_vel_type[b];
+        if (rt[b] == 3 || vt[b] == 3) {
+            per[b] = m->periodic_node[b];
+            s->periodic = true;
+        }
         const double *v = m->bc_values + 4 * b;
         bcv[b] = {(R)v[0], (R)v[1], (R)v[2], (R)(v[3] - rho0)};
         const int f = ni + b, g = nc + b, o = m->owner[f];
@@ -286,7 +297,7 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     }
     std::vector<R> visc(nc, (R)p.visc_factor_initial);
     int rc = 0;
-    int *d_rt, *d_vt, *d_cf;
+    int *d_rt, *d_vt, *d_per, *d_cf;
     int2 *d_stencil;
     LsRec<R> *d_ls;
     R *d_visc;
@@ -297,7 +308,8 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     GenFace<R> *d_gen;
     double *d_vol, *d_ivol;
     if ((rc = s->upload(&d_stencil, stencil)) || (rc = s->upload(&d_ls, ls)) ||
-        (rc = s->upload(&d_rt, rt)) || (rc = s->upload(&d_vt, vt)) || (rc = s->upload(&d_bcv, bcv)) ||
+        (rc = s->upload(&d_rt, rt)) || (rc = s->upload(&d_vt, vt)) || (rc = s->upload(&d_per, per)) ||
+        (rc = s->upload(&d_bcv, bcv)) ||
         (rc = s->upload(&d_bcr, bcr)) || (rc = s->upload(&d_fcells, fcells)) || (rc = s->upload(&d_gen, gen)) ||
         (rc = s->upload(&d_cf, cf)) || (rc = s->upload(&d_vol, vol)) || (rc = s->upload(&d_ivol, inv_vol)) ||
         (rc = s->upload(&d_visc, visc)))
@@ -309,7 +321,7 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         if ((rc = s->upload(&d_cl, closure))) return rc;
         a.closure = d_cl;
     }
-    a.stencil = d_stencil; a.ls = d_ls; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt;
+    a.stencil = d_stencil; a.ls = d_ls; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt; a.bc_periodic = d_per;
     a.bc_val = d_bcv; a.bc_rec = d_bcr; a.face_cells = d_fcells; a.axis_face = d_axf; a.gen_face = d_gen;
     a.visc_factor = d_visc; a.cell_faces = d_cf; a.cell_volume = d_vol; a.cell_inv_volume = d_ivol;
     Vec4<R> *d_state, *d_flux;
@@ -505,6 +517,10 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         c.cell0 = g.cell0; c.gnx = g.nx; c.gny = g.ny; c.gnz = g.nz;
         for (int q = 0; q < 3; q++) c.gorigin[q] = gd.origin[q];
         c.gdx = gd.delta_x; c.gdh = gd.delta_h;
+        c.periodic = d.periodic ? 1 : 0;
+        c.domain_z0 = gd.origin[2];
+        c.domain_Z = gd.length[2];
+        if (d.periodic) s->wrap_membranes = true;
         {
             // a patch of in-range stencils lies inside the instance's grid
             const int S = stencil_width(p.ibm_stencil);
@@ -795,6 +811,17 @@ bool visc_due(const lbfs_solver *s, long long t) {
     return s->n_membranes > 0 && s->params.viscosity_period > 0 && t % s->params.viscosity_period == 1;
 }
 
+// gpu_solver::check_periodic_object at t % 5000 == 1 (Solver_gpu.cu:1027-1029),
+// after the step's fluid update: enqueued behind the step on the solver stream.
+constexpr int kWrapPeriod = 5000;
+bool wrap_due(const lbfs_solver *s, long long t) { return s->wrap_membranes && t % kWrapPeriod == 1; }
+int after_step(lbfs_solver *s) {
+    if (!wrap_due(s, s->t)) return LBFS_OK;
+    launch_membrane_wrap(s->ma, s->stream);
+    LBFS_CUDA(cudaGetLastError());
+    return LBFS_OK;
+}
+
 void free_all(lbfs_solver *s) {
     if (s->graph) cudaGraphExecDestroy(s->graph);
     for (int p = 0; p < kPhases; p++)
@@ -985,7 +1012,7 @@ extern "C" int lbfs_step(lbfs_solver *s, int32_t n_steps) {
     for (int k = 0; k < n_steps; k++) {
         int n = 0;
         int rc = enqueue(s, visc_due(s, s->t), &n);
-        if (rc) return rc;
+        if (rc || (rc = after_step(s))) return rc;
         s->t++;
     }
     return LBFS_OK;
@@ -1016,6 +1043,7 @@ extern "C" int lbfs_step_graph(lbfs_solver *s, int32_t n_steps) {
             LBFS_CUDA(cudaGraphLaunch(s->graph, s->stream));
             for (int p = 0; p < kPhases; p++) s->phase_recorded[p] = s->graph_phase_recorded[p];
         }
+        if (int rc = after_step(s)) return rc;
         s->t++;
     }
     return LBFS_OK;
@@ -1381,7 +1409,7 @@ int adj_prepare(lbfs_solver *s) {
 int run_one_step(lbfs_solver *s) {
     if (visc_due(s, s->t)) {
         int rc = enqueue(s, true, nullptr);
-        if (rc) return rc;
+        if (rc || (rc = after_step(s))) return rc;
     } else {
         int rc = lbfs_step_graph(s, 1);
         if (rc) return rc;
@@ -1485,6 +1513,7 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
         return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: no preconditioning");
     if (dynamic_dt(s->params))
         return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: constant time stepping only");
+    if (s->periodic) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: no periodic boundaries");
     if (s->params.ibm_stencil == LBFS_IBM_VANDERMONDE4 && s->n_membranes > 0)
         return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: LBFS_IBM_HAT2 or LBFS_IBM_PESKIN4 only");
     if (obj->kind == LBFS_OBJ_VELOCITY) {
@@ -1500,8 +1529,13 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     std::vector<MembraneConst> mch(M);
     if (M > 0) {
         LBFS_CUDA(cudaMemcpy(mch.data(), s->ma.mc, sizeof(MembraneConst) * M, cudaMemcpyDeviceToHost));
-        bool visc_in_window = false;
-        for (long long t = s->t; t < s->t + n_steps; t++) visc_in_window = visc_in_window || visc_due(s, t);
+        bool visc_in_window = false, wrap_in_window = false;
+        for (long long t = s->t; t < s->t + n_steps; t++) {
+            visc_in_window = visc_in_window || visc_due(s, t);
+            wrap_in_window = wrap_in_window || wrap_due(s, t);
+        }
+        if (wrap_in_window)
+            return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: a periodic membrane's z wrap falls in the window");
         for (const MembraneConst &c : mch) {
             if (c.viscosity != 0.0) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: membrane viscosity must be 0");
             if (!(c.shear_modulus > 0.0)) return set_error(LBFS_ERR_UNSUPPORTED, "lbfs_adjoint: shear modulus must be > 0");

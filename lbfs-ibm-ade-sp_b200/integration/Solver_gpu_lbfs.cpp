@@ -92,6 +92,17 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
     md.length[0] = domain.X; md.length[1] = domain.Y; md.length[2] = domain.Z;
     md.delta_x = domain.dt * 2;
     md.delta_h = Mesh.get_delta_h();
+    // periodic boundaries (type 3; the CPU solver's, Solution.cpp:777-803): each ghost's partner cell by
+    // the deck's periodic_translation (preprocessor.cpp:532-534, Boundary_Conditions.cpp:417-432)
+    std::vector<int32_t> partner(nb, 0);
+    bool any_periodic = false;
+    for (int i = 0; i < nb; i++) any_periodic = any_periodic || rho_type[i] == 3 || vel_type[i] == 3;
+    if (any_periodic) {
+        const double T[3] = {quad_bcs_orig.per_translate_x, quad_bcs_orig.per_translate_y,
+                             quad_bcs_orig.per_translate_z};
+        lbfs_check(lbfs_mesh_find_periodic_nodes(&md, T, partner.data()), "lbfs_mesh_find_periodic_nodes");
+        md.periodic_node = partner.data();
+    }
     // plateau meshes: the vertex coordinates the 4x4x4 IBM searches (Solver_gpu.cu:497-499, 637-639)
     std::vector<double> plateau[3];
     if (globals.mesh_type == 4) {
@@ -152,6 +163,7 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
             d.curvature_ratio = o.curvature_ratio; d.volume_ratio = o.volume_ratio;
             d.internal_viscosity_ratio = o.internal_viscosity_ratio; d.reference_length = o.reference_length;
             d.pivkin_length = o.pivkin_length; d.sphere_reference = o.sphere_reference;
+            d.periodic = object_vec[0].periodic;  // the reference's gate of check_periodic_object (Solver_gpu.cu:1027)
             rbc.push_back(d);
         }
         for (size_t k = 0; k < rbc.size(); k++) {

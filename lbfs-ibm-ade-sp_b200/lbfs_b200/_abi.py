@@ -77,6 +77,7 @@ class MeshDesc(ctypes.Structure):
         ("delta_x", ctypes.c_double), ("delta_h", ctypes.c_double),
         ("n_instances", ctypes.c_int32), ("instances", ctypes.POINTER(GridDesc)),
         ("grid_x", _f64p), ("grid_y", _f64p), ("grid_z", _f64p),
+        ("periodic_node", _i32p),
     ]
 
 
@@ -104,7 +105,7 @@ class RbcDesc(ctypes.Structure):
         ("wlc_ratio", ctypes.c_double), ("curvature_ratio", ctypes.c_double), ("volume_ratio", ctypes.c_double),
         ("internal_viscosity_ratio", ctypes.c_double), ("reference_length", ctypes.c_double),
         ("pivkin_length", ctypes.c_int32), ("sphere_reference", ctypes.c_int32),
-        ("instance", ctypes.c_int32),
+        ("instance", ctypes.c_int32), ("periodic", ctypes.c_int32),
     ]
 
 
@@ -175,6 +176,7 @@ def lib():
                                                                                        ctypes.c_double, ctypes.c_double,
                                                                                        ctypes.c_double, ctypes.c_uint64],
             "lbfs_mesh_openfoam_counts": [ctypes.c_char_p, _i32p],
+            "lbfs_mesh_find_periodic_nodes": [ctypes.POINTER(MeshDesc), _f64p, _i32p],
             "lbfs_mesh_import_openfoam": [ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                           ctypes.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
                                           _i32p, _f64p, _f64p, _i32p, ctypes.c_char_p, ctypes.c_int32],
@@ -234,5 +236,5 @@ EXPORTED = [
     "lbfs_residual_rms_noalloc", "lbfs_get_launch_shape", "lbfs_set_launch_shape", "lbfs_autotune",
     "lbfs_adjoint", "lbfs_checkpoint_size", "lbfs_checkpoint_save", "lbfs_checkpoint_load",
     "lbfs_mesh_build_jittered", "lbfs_mesh_build_rectilinear", "lbfs_mesh_write_openfoam", "lbfs_mesh_openfoam_counts",
-    "lbfs_mesh_import_openfoam",
+    "lbfs_mesh_import_openfoam", "lbfs_mesh_find_periodic_nodes",
 ]

@@ -46,17 +46,21 @@ def _initial_state(n_cells, seed, amplitude=1e-4, rho0=1.0, u0=None):
     return rho, u, v, w
 
 
-def poiseuille(n=32, seed=1234, tau=0.8, u_centre=0.01, delta_t=0.5, precision=_abi.LBFS_FP64, ny=None, nz=None):
-    """Body-force-driven square duct, n x ny x nz cells (default cube)."""
+def poiseuille(n=32, seed=1234, tau=0.8, u_centre=0.01, delta_t=0.5, precision=_abi.LBFS_FP64, ny=None, nz=None,
+               periodic_x=False, jitter=0.0, mesh_seed=1):
+    """Body-force-driven square duct, n x ny x nz cells (default cube).  The x ends are
+    Neumann (type 2), or periodic (type 3, translation X along x) with periodic_x; jitter > 0
+    moves the interior vertices (general-normal fluxes, closed faces)."""
     ny = ny or n
     nz = nz or n
     dt = 1.0
     visc = (tau - 0.5) / 3.0 * dt
-    mesh = build_uniform_mesh(2.0 * n, 2.0 * ny, 2.0 * nz, dt, visc=visc)
-    bcs = {"left": (2, 2, 1.0, 0.0, 0.0, 0.0), "right": (2, 2, 1.0, 0.0, 0.0, 0.0),
+    mesh = build_uniform_mesh(2.0 * n, 2.0 * ny, 2.0 * nz, dt, visc=visc, jitter=jitter, seed=mesh_seed)
+    end = (3, 3, 1.0, 0.0, 0.0, 0.0) if periodic_x else (2, 2, 1.0, 0.0, 0.0, 0.0)
+    bcs = {"left": end, "right": end,
            "bottom": (2, 1, 1.0, 0.0, 0.0, 0.0), "top": (2, 1, 1.0, 0.0, 0.0, 0.0),
            "back": (2, 1, 1.0, 0.0, 0.0, 0.0), "front": (2, 1, 1.0, 0.0, 0.0, 0.0)}
-    mesh.set_boundaries(bcs)
+    mesh.set_boundaries(bcs, periodic_translation=(2.0 * n, 0.0, 0.0) if periodic_x else None)
     # square duct of half-width a: u_max = 0.2947 f a^2 / (rho nu)  (series solution)
     a = 0.5 * 2.0 * min(ny, nz)
     force = u_centre * visc / (0.2947 * a * a)
@@ -70,10 +74,11 @@ def poiseuille(n=32, seed=1234, tau=0.8, u_centre=0.01, delta_t=0.5, precision=_
 
 def shear_rbc(n=64, level=3, radius_cells=8.0, capillary=0.1, u_wall=0.02, seed=4321, tau=0.8, delta_t=0.5,
               precision=_abi.LBFS_FP64, ibm_stencil=_abi.LBFS_IBM_PESKIN4, n_cells_y=None, n_cells_z=None,
-              rotate=False, mesh_type=6, plateau=(0.0, 0.0)):
-    """Simple shear with one red cell of radius `radius_cells` cells at the centre.  mesh_type 4 with
-    plateau = (width, slope) is the reference's plateau mesh (uniform cells in the middle, coarser
-    towards the walls), whose IBM is LBFS_IBM_VANDERMONDE4."""
+              rotate=False, mesh_type=6, plateau=(0.0, 0.0), centre=None, periodic_object=False):
+    """Simple shear with one red cell of radius `radius_cells` cells at the centre (or at `centre`,
+    as fractions of the box).  mesh_type 4 with plateau = (width, slope) is the reference's plateau
+    mesh (uniform cells in the middle, coarser towards the walls), whose IBM is
+    LBFS_IBM_VANDERMONDE4.  periodic_object sets the membrane's periodic flag (its z wrap)."""
     ny = n_cells_y or n
     nz = n_cells_z or n
     dt = 1.0
@@ -95,7 +100,9 @@ def shear_rbc(n=64, level=3, radius_cells=8.0, capillary=0.1, u_wall=0.02, seed=
                   internal_viscosity_ratio=5.0)
     rng = np.random.default_rng(seed)
     rot = rotation_matrix(rng) if rotate else None
-    cell = red_cell(level, R, (0.5 * X, 0.5 * Y, 0.5 * Z), rot, **moduli)
+    fx, fy, fz = centre or (0.5, 0.5, 0.5)
+    cell = red_cell(level, R, (fx * X, fy * Y, fz * Z), rot, **moduli)
+    cell.periodic = periodic_object
     params = StepParams(visc=visc, delta_t=delta_t, channel_diameter=Y, ref_rho=1.0, max_velocity=u_wall, rho0=1.0,
                         visc_factor_initial=1.0, testcase=5, precision=precision, ibm_stencil=ibm_stencil,
                         viscosity_period=10000)

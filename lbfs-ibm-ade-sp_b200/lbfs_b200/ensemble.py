@@ -53,6 +53,7 @@ class EnsembleMesh:
     cells: np.ndarray            # interior cells of each instance
     members: list = field(default_factory=list, repr=False)
     _grids: object = field(default=None, repr=False)
+    periodic_node: np.ndarray = field(default=None)  # partner cells of type-3 ghosts (whole-mesh indices)
 
     @property
     def n_instances(self):
@@ -75,6 +76,8 @@ class EnsembleMesh:
         d.lhs_inverse, d.rhs = _abi.ptr(self.lhs_inverse), _abi.ptr(self.rhs)
         d.bc_rho_type, d.bc_vel_type = _abi.iptr(self.bc_rho_type), _abi.iptr(self.bc_vel_type)
         d.bc_values = _abi.ptr(self.bc_values)
+        if self.periodic_node is not None:
+            d.periodic_node = _abi.iptr(self.periodic_node)
         grids = (_abi.GridDesc * self.n_instances)()
         for k, m in enumerate(self.members):
             g = grids[k]
@@ -143,4 +146,7 @@ def concatenate(meshes):
         bc_rho_type=cat([m.bc_rho_type for m in meshes], np.int32),
         bc_vel_type=cat([m.bc_vel_type for m in meshes], np.int32),
         bc_values=cat([m.bc_values for m in meshes], np.float64),
-        cell0=C.astype(np.int64), cells=nc.astype(np.int64), members=meshes)
+        cell0=C.astype(np.int64), cells=nc.astype(np.int64), members=meshes,
+        periodic_node=(cat([C[k] + (m.periodic_node if m.periodic_node is not None else np.zeros(m.n_bc, np.int64))
+                            for k, m in enumerate(meshes)], np.int32)
+                       if any(m.periodic_node is not None for m in meshes) else None))

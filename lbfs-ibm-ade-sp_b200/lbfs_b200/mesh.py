@@ -53,6 +53,7 @@ class UniformMesh:
     plateau: tuple = (0.0, 0.0)  # plateau width and slope (mesh_type 4)
     patch_names: tuple = PATCHES  # boundary patches in bc_patch order
     source: str = None            # polyMesh directory of an imported mesh
+    periodic_node: np.ndarray = field(default=None)  # partner cell of each type-3 ghost
 
     @property
     def shape(self):
@@ -64,10 +65,13 @@ class UniformMesh:
     def delta_x(self):
         return 2 * self.dt
 
-    def set_boundaries(self, spec):
+    def set_boundaries(self, spec, periodic_translation=None):
         """spec: {patch: (rho_type, vel_type, rho, u, v, w)} for the six patches,
         values already scaled as after preprocessor::mach_number_factor
-        (Boundary_Conditions::assign_boundary_conditions, Boundary_Conditions.cpp:377-441)."""
+        (Boundary_Conditions::assign_boundary_conditions, Boundary_Conditions.cpp:377-441).
+        Type 3 is periodic: each such ghost takes the state and gradients of the interior
+        cell nearest to its centroid moved by +-periodic_translation (the XML's
+        periodic_translation, one vector for every periodic patch)."""
         rt = np.zeros(self.n_bc, np.int32)
         vt = np.zeros(self.n_bc, np.int32)
         vals = np.zeros((self.n_bc, 4), np.float64)
@@ -78,6 +82,11 @@ class UniformMesh:
             vt[sel] = vel_type
             vals[sel] = (u, v, w, rho)
         self.bc_rho_type, self.bc_vel_type, self.bc_values = rt, vt, np.ascontiguousarray(vals)
+        self.periodic_node = None
+        if np.any(rt == 3) or np.any(vt == 3):
+            if periodic_translation is None:
+                raise ValueError("periodic boundaries (type 3) need periodic_translation")
+            self.periodic_node = find_periodic_nodes(self, periodic_translation)
         return self
 
     def desc(self):
@@ -102,7 +111,24 @@ class UniformMesh:
         d.delta_h = self.delta_h
         if self.grid is not None:
             d.grid_x, d.grid_y, d.grid_z = (_abi.ptr(g) for g in self.grid)
+        if self.periodic_node is not None:
+            d.periodic_node = _abi.iptr(self.periodic_node)
         return d
+
+
+def find_periodic_nodes(mesh, translation):
+    """Partner cell of every type-3 ghost: the interior cell nearest to the ghost's centroid
+    moved by +translation or -translation (lbfs_mesh_find_periodic_nodes); 0 elsewhere."""
+    out = np.zeros(mesh.n_bc, np.int32)
+    keep = mesh.periodic_node
+    mesh.periodic_node = None  # the search reads sizes, centroids and types only
+    try:
+        d = mesh.desc()
+    finally:
+        mesh.periodic_node = keep
+    t = np.ascontiguousarray(translation, dtype=np.float64)
+    _abi.check(_abi.lib().lbfs_mesh_find_periodic_nodes(ctypes.byref(d), _abi.ptr(t), _abi.iptr(out)))
+    return out
 
 
 def uniform_counts(X, Y, Z, dt):

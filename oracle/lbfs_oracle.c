@@ -40,7 +40,7 @@ typedef struct oracle_case {
     lbfs_params p;
     int nc, nf, ni, nb, nt;
     /* copies of the mesh arrays (the descriptor's pointers are the caller's) */
-    int *owner, *neighbour, *stencil, *rt, *vt;
+    int *owner, *neighbour, *stencil, *rt, *vt, *per;
     double *area, *normal, *fcen, *sdt, *vol, *cen, *lhs, *rhs, *bcv;
     /* state: (u, v, w, rho) per cell incl. ghosts, soln_t1 per cell */
     double *soln, *t1, *grad, *flux, *res, *force, *visc;
@@ -68,7 +68,9 @@ static void *dup(const void *src, size_t bytes) {
 
 /* ------------------------------------------------------------ fluid ---- */
 
-/* update_unstructured_bcs, LBFS.cu:1843-1928 */
+/* update_unstructured_bcs, LBFS.cu:1843-1928; type 3 (periodic) as the CPU
+ * solver's Solution::update_unstructured_bcs (Solution.cpp:777-803): the
+ * partner cell's values. */
 static void ghost_update(oracle_case *o) {
     const double H2 = o->p.channel_diameter * 0.5;
     const double H4 = o->p.channel_diameter * o->p.channel_diameter * o->p.channel_diameter * o->p.channel_diameter;
@@ -77,9 +79,13 @@ static void ghost_update(oracle_case *o) {
         const double *s = o->soln + 4 * nb, *bc = o->bcv + 4 * i;
         double *g = o->soln + 4 * j;
         /* soln layout: 0 u, 1 v, 2 w, 3 rho; bcv layout: u, v, w, rho */
+        const double *ps = o->soln + 4 * o->per[i];
         if (o->rt[i] == 1) g[3] = bc[3] - (s[3] - bc[3]);
+        else if (o->rt[i] == 3) g[3] = ps[3];
         else g[3] = s[3];
-        if (o->vt[i] == 1) {
+        if (o->vt[i] == 3) {
+            for (int c = 0; c < 3; c++) g[c] = ps[c];
+        } else if (o->vt[i] == 1) {
             for (int c = 0; c < 3; c++) g[c] = bc[c] - (s[c] - bc[c]);
         } else if (o->vt[i] == 2) {
             for (int c = 0; c < 3; c++) g[c] = s[c];
@@ -116,7 +122,9 @@ static void interior_gradients(oracle_case *o) {
     }
 }
 
-/* get_bc_gradients, LBFS.cu:1933-2048 */
+/* get_bc_gradients, LBFS.cu:1933-2048; a periodic (type 3) component takes
+ * the partner cell's gradient (gradients::Get_LS_Gradients,
+ * gradients.cpp:428-440), formed before the ghosts' as there. */
 static void bc_gradients(oracle_case *o) {
     static const int var[4] = {3, 0, 1, 2};
     for (int i = 0; i < o->nb; i++) {
@@ -130,9 +138,12 @@ static void bc_gradients(oracle_case *o) {
         const double *go = o->grad + 12 * nbi;
         for (int m = 0; m < 4; m++) {
             const int dirichlet = (m == 0) ? (o->rt[i] == 1) : (o->vt[i] == 1 || o->vt[i] == 9 || o->vt[i] == 10);
+            const int periodic = (m == 0) ? (o->rt[i] == 3) : (o->vt[i] == 3);
             const double d = o->soln[4 * j + var[m]] - o->soln[4 * nbi + var[m]];
+            const double *gp = o->grad + 12 * o->per[i];
             for (int c = 0; c < 3; c++)
-                g[3 * m + c] = dirichlet ? d / dmag * un[c] : go[3 * m + c] * (1 - fabs(n[c]));
+                g[3 * m + c] = periodic ? gp[3 * m + c]
+                                        : (dirichlet ? d / dmag * un[c] : go[3 * m + c] * (1 - fabs(n[c])));
         }
     }
 }
@@ -719,6 +730,7 @@ oracle_case *oracle_create(const lbfs_mesh_desc *m, const lbfs_params *p, const 
     o->stencil = dup(m->gradient_stencil, 6 * nc * sizeof(int));
     o->rt = dup(m->bc_rho_type, nb * sizeof(int));
     o->vt = dup(m->bc_vel_type, nb * sizeof(int));
+    o->per = dup(m->periodic_node, nb * sizeof(int)); /* zeros when absent */
     o->area = dup(m->face_area, nf * sizeof(double));
     o->normal = dup(m->face_normal, 3 * nf * sizeof(double));
     o->fcen = dup(m->face_centroid, 3 * nf * sizeof(double));
@@ -797,7 +809,7 @@ oracle_case *oracle_create(const lbfs_mesh_desc *m, const lbfs_params *p, const 
 
 void oracle_free(oracle_case *o) {
     if (!o) return;
-    void *ptrs[] = {o->owner, o->neighbour, o->stencil, o->rt, o->vt, o->area, o->normal, o->fcen, o->sdt, o->vol,
+    void *ptrs[] = {o->owner, o->neighbour, o->stencil, o->rt, o->vt, o->per, o->area, o->normal, o->fcen, o->sdt, o->vol,
                     o->cen, o->lhs, o->rhs, o->bcv, o->soln, o->t1, o->grad, o->flux, o->res, o->force, o->visc, o->mem,
                     o->tri, o->spr, o->x, o->y, o->z, o->vx, o->vy, o->vz, o->fx, o->fy, o->fz, o->contour, o->kspr,
                     o->curv, o->curv0, o->ang0, o->area0, o->sarea, o->cfl, o->dtl, o->gv[0], o->gv[1],
@@ -818,6 +830,28 @@ void oracle_get_state(const oracle_case *o, double *rho, double *u, double *v, d
     for (int i = 0; i < o->nc; i++) {
         const double *s = o->soln + 4 * i;
         u[i] = s[0]; v[i] = s[1]; w[i] = s[2]; rho[i] = s[3];
+    }
+}
+
+/* gpu_solver::check_periodic_object (Solver_gpu.cu:1027-1029, 1277-1304), per
+ * periodic membrane: the mean node z as total<128> sums it (256 nodes per
+ * block tree-summed, stride 128 down to 1; the block sums added in order
+ * from 0), and a move by -0.5 Z when it exceeds origin_z + 0.75 Z. */
+static void periodic_wrap(oracle_case *o) {
+    const double z0 = o->m.origin[2], Z = o->m.length[2];
+    for (int r = 0; r < o->n_mem; r++) {
+        const omem *M = o->mem + r;
+        if (!M->d.periodic) continue;
+        double *z = o->z + M->node0, sum = 0.0;
+        for (int s0 = 0; s0 < M->n_nodes; s0 += 256) {
+            double part[256];
+            for (int t = 0; t < 256; t++) part[t] = s0 + t < M->n_nodes ? z[s0 + t] : 0.0;
+            for (int stride = 128; stride >= 1; stride >>= 1)
+                for (int t = 0; t < stride; t++) part[t] += part[t + stride];
+            sum = sum + part[0];
+        }
+        if (sum / M->n_nodes > z0 + 0.75 * Z)
+            for (int n = 0; n < M->n_nodes; n++) z[n] = z[n] + -0.5 * Z;
     }
 }
 
@@ -878,6 +912,7 @@ void oracle_step(oracle_case *o, int n_steps) {
             s[2] = t1[2] / t1[3];
             for (int m = 0; m < 4; m++) sq[m] += r[m] * r[m];
         }
+        if (o->n_mem > 0 && o->t % 5000 == 1) periodic_wrap(o);
         const double ref_mom = o->p.ref_rho * o->p.max_velocity;
         for (int m = 0; m < 4; m++) o->resid[m] = sqrt(sq[m] / o->nc) / (m == 0 ? o->p.ref_rho : ref_mom);
     }

@@ -237,6 +237,7 @@ struct ref_params {
     int time_stepping;     // globals.gpu_time_stepping: 1 local, 2 constant, 3 min, 4 talts (0 = 2)
     double pre_conditioned_gamma;  // get_cfl_device's gamma (0 = 1 / gamma_inv)
     int preconditioning;           // globals.preconditioning_active
+    int object_periodic;           // object_vec[0].periodic (check_periodic_object)
 };
 
 namespace {
@@ -518,6 +519,13 @@ extern "C" void ref_case_step(void *h, int n_steps) {
         add(nc, c->res_w.data(), c->fz.data());
         time_integration(nc, 0, 1, c->dtl.data(), c->t0.data(), c->t1.data(), c->soln.data(), c->res_rho.data(),
                          c->res_u.data(), c->res_v.data(), c->res_w.data(), delta_t, mode);
+        // gpu_solver::check_periodic_object (Solver_gpu.cu:1027-1029, 1277-1304): total<128> over
+        // n_node_Blocks = ceil(n / 128) blocks, host sum, add_double
+        if (p.has_rbc && t % 5000 == 1 && p.object_periodic) {
+            const double sum_add = block_tree_total(c->z.data(), c->n_nodes, (c->n_nodes + 127) / 128);
+            const double object_centre_z = sum_add / c->n_nodes;
+            if (object_centre_z > (D.origin_z + 0.75 * D.Z)) add_double(c->n_nodes, c->z.data(), (-0.5 * D.Z));
+        }
         // residual RMS (Solver_gpu.cu:1033-1046, residuals.cpp:114-133)
         int nblk = (nc + 127) / 128;
         std::vector<double> sq(nc);

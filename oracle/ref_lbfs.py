@@ -34,7 +34,7 @@ class RefParams(ctypes.Structure):
         ("internal_viscosity_ratio", ctypes.c_double), ("reference_length", ctypes.c_double),
         ("pivkin_length", ctypes.c_int), ("sphere_reference", ctypes.c_int), ("viscosity_period", ctypes.c_int),
         ("time_stepping", ctypes.c_int), ("pre_conditioned_gamma", ctypes.c_double),
-        ("preconditioning", ctypes.c_int),
+        ("preconditioning", ctypes.c_int), ("object_periodic", ctypes.c_int),
     ]
 
 

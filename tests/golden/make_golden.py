@@ -49,6 +49,7 @@ def ref_case(c):
                   "curvature_ratio", "volume_ratio", "internal_viscosity_ratio", "reference_length"):
             setattr(p, k, float(getattr(mb, k)))
         p.pivkin_length, p.sphere_reference = int(mb.pivkin_length), int(mb.sphere_reference)
+        p.object_periodic = int(bool(mb.periodic))
     rc = R.RefCase(rm, p, m.bc_rho_type, m.bc_vel_type, m.bc_values)
     rc.set_state(c.rho, c.u, c.v, c.w)
     if c.membranes:
@@ -129,6 +130,10 @@ def main():
     c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
     c.params = replace(c.params, time_stepping=_abi.LBFS_DT_MIN)
     step_fixture("step_shear_rbc_16_min.npz", c, 10)
+    # a periodic object above 0.75 Z: check_periodic_object moves it down by Z / 2 after step t = 1
+    step_fixture("step_shear_rbc_16_wrap.npz",
+                 cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2,
+                                 centre=(0.5, 0.5, 0.8), periodic_object=True), 4)
     # preconditioning: gamma = 2 in the relaxation, the interface and the
     # boundary faces' lattice equilibria, with local time stepping
     c = cases.poiseuille(n=6, ny=5, nz=4)

@@ -33,10 +33,10 @@ def test_library_exports_every_declared_symbol():
 def test_structs_match_header_sizes():
     # sizes of the descriptors as a C compiler lays them out (64-bit)
     from lbfs_b200 import _abi
-    assert ctypes.sizeof(_abi.MeshDesc) == 8 * 4 + 14 * 8 + 8 * 8 + 8 + 8 + 3 * 8
+    assert ctypes.sizeof(_abi.MeshDesc) == 8 * 4 + 14 * 8 + 8 * 8 + 8 + 8 + 3 * 8 + 8  # ... periodic_node
     assert ctypes.sizeof(_abi.GridDesc) == 8 + 8 * 8
     assert ctypes.sizeof(_abi.Params) == 4 * 8 + 3 * 8 + 4 * 8 + 4 * 4 + 8 + 8 + 8  # time stepping, gamma, precond.
-    assert ctypes.sizeof(_abi.RbcDesc) == 16 + 4 * 8 + 13 * 8 + 8 + 8
+    assert ctypes.sizeof(_abi.RbcDesc) == 16 + 4 * 8 + 13 * 8 + 8 + 8  # ... instance, periodic
 
 
 def test_struct_layout_matches_c_compiler(tmp_path):

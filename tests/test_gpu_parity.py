@@ -49,6 +49,8 @@ def fixture_case(golden, name):
         c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
         mb = c.membranes[0]
         mb.xyz_stress_free, mb.xyz_initial = g["xyz_stress_free"], g["xyz_initial"]
+    if "wrap" in name:  # a periodic object: check_periodic_object moves it at t = 1
+        c.membranes[0].periodic = True
     c.rho, c.u, c.v, c.w = g["rho0"], g["u0"], g["v0"], g["w0"]
     if "time_stepping" in g.files:
         c.params = replace(c.params, time_stepping=int(g["time_stepping"]), gamma_inv=float(g["gamma_inv"]),
@@ -58,7 +60,8 @@ def fixture_case(golden, name):
 
 FIXTURES = ["step_poiseuille_6x5x4.npz", "step_shear_rbc_16.npz", "step_poiseuille_6x5x4_local.npz",
             "step_poiseuille_6x5x4_talts.npz", "step_shear_rbc_16_min.npz", "step_plateau_rbc_16.npz",
-            "step_poiseuille_6x5x4_precond.npz", "step_foam_duct_8x6x5.npz", "step_foam_shear_rbc_16.npz"]
+            "step_poiseuille_6x5x4_precond.npz", "step_foam_duct_8x6x5.npz", "step_foam_shear_rbc_16.npz",
+            "step_shear_rbc_16_wrap.npz"]
 
 
 @pytest.mark.parametrize("name", FIXTURES)
@@ -163,6 +166,53 @@ def test_general_normal_faces_vs_oracle():
 def _set_general(d):
     d.axis_aligned = 0
     return d
+
+
+def test_periodic_duct_vs_oracle():
+    # type-3 ends: ghosts take the partner cell's state (K1) and gradients (boundary-face flux kernel)
+    compare_with_oracle(cases.poiseuille(n=10, ny=8, nz=6, periodic_x=True), 20)
+
+
+def test_periodic_jittered_duct_vs_oracle():
+    # general-normal faces everywhere, partners found on the moved centroids
+    compare_with_oracle(cases.poiseuille(n=10, ny=8, nz=6, periodic_x=True, jitter=0.15), 12)
+
+
+def test_periodic_channel_32_vs_oracle():
+    # the 32^3 body-force duct with periodic x and seeded +-1e-4 velocity perturbations
+    compare_with_oracle(cases.poiseuille(n=32, periodic_x=True), 6, fields=False)
+
+
+def test_periodic_duct_fp32_bulk_against_fp64():
+    a = make(cases.poiseuille(n=16, periodic_x=True))
+    b = make(cases.poiseuille(n=16, periodic_x=True, precision=_abi.LBFS_FP32_BULK))
+    a.step(40, graph=True)
+    b.step(40, graph=True)
+    sa, sb = a.state(), b.state()
+    assert rel_err(sb[0] - 1.0, sa[0] - 1.0) < 1e-3
+    for k in (1, 2, 3):
+        assert rel_err(sb[k], sa[k]) < FP32_RTOL, (k, rel_err(sb[k], sa[k]))
+    a.close()
+    b.close()
+
+
+def test_periodic_needs_partners_and_no_adjoint():
+    c = cases.poiseuille(n=6, ny=5, nz=4, periodic_x=True)
+    keep = c.mesh.periodic_node
+    c.mesh.periodic_node = None
+    with pytest.raises(_abi.LbfsError) as e:
+        make(c)
+    assert e.value.code == _abi.LBFS_ERR_ARG
+    c.mesh.periodic_node = keep.copy()
+    c.mesh.periodic_node[np.flatnonzero(c.mesh.bc_rho_type == 3)[0]] = c.mesh.n_cells  # not an interior cell
+    with pytest.raises(_abi.LbfsError):
+        make(c)
+    c.mesh.periodic_node = keep
+    s = make(c)
+    with pytest.raises(_abi.LbfsError) as e:
+        s.adjoint(2, weights=np.ones((c.mesh.n_cells, 3)))
+    assert e.value.code == _abi.LBFS_ERR_UNSUPPORTED
+    s.close()
 
 
 def test_peskin4_ibm_vs_oracle():
