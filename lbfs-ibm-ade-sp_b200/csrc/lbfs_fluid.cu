@@ -46,11 +46,10 @@ __device__ __forceinline__ Vec4<R> ghost_state(const FluidArgs<R> &a, int b, con
 }
 
 template <typename R, int TB>
-__global__ void __launch_bounds__(TB) k_cell_gradients(FluidArgs<R> a, int begin, int end) {
+__global__ void __launch_bounds__(TB, TB == 128 ? 5 : 1) k_cell_gradients(FluidArgs<R> a, int begin, int end) {
     const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= end) return;
     const Vec4<R> own = a.state[i];
-    R rr[3] = {0, 0, 0}, ru[3] = {0, 0, 0}, rv[3] = {0, 0, 0}, rw[3] = {0, 0, 0};
     int st[6];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
@@ -58,8 +57,11 @@ __global__ void __launch_bounds__(TB) k_cell_gradients(FluidArgs<R> a, int begin
         st[2 * q] = p.x;
         st[2 * q + 1] = p.y;
     }
-    const LsRec<R> ls = a.ls[i];
-    bool has_ghost = false;
+    const LsW<R> W = a.lsw[i];
+    GradRec<R> gr;
+    R *g = gr.g;
+#pragma unroll
+    for (int t = 0; t < 12; t++) g[t] = R(0);
 #pragma unroll
     for (int q = 0; q < 6; q++) {
         const int j = st[q];
@@ -68,62 +70,15 @@ __global__ void __launch_bounds__(TB) k_cell_gradients(FluidArgs<R> a, int begin
             s = a.state[j];
         } else {
             s = ghost_state(a, j - a.nc, own);
-            has_ghost = true;
         }
-        // add_LS_contributions, LBFS.cu:2051-2083
-        const R du = s.u - own.u, dv = s.v - own.v, dw = s.w - own.w, dr = s.rho - own.rho;
-        const R r0 = ls.rhs[3 * q], r1 = ls.rhs[3 * q + 1], r2 = ls.rhs[3 * q + 2];
-        rr[0] = rr[0] + r0 * dr; rr[1] = rr[1] + r1 * dr; rr[2] = rr[2] + r2 * dr;
-        ru[0] = ru[0] + r0 * du; ru[1] = ru[1] + r1 * du; ru[2] = ru[2] + r2 * du;
-        rv[0] = rv[0] + r0 * dv; rv[1] = rv[1] + r1 * dv; rv[2] = rv[2] + r2 * dv;
-        rw[0] = rw[0] + r0 * dw; rw[1] = rw[1] + r1 * dw; rw[2] = rw[2] + r2 * dw;
-    }
-    const R *L = ls.lhs;
-    GradRec<R> gr;
-    R *g = gr.g;
-    const R *rs[4] = {rr, ru, rv, rw};
+        // add_LS_contributions (LBFS.cu:2051-2083) with LHS^-1 folded in
+        const R d[4] = {s.rho - own.rho, s.u - own.u, s.v - own.v, s.w - own.w};
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-        g[3 * m + 0] = L[0] * rs[m][0] + L[1] * rs[m][1] + L[2] * rs[m][2];
-        g[3 * m + 1] = L[3] * rs[m][0] + L[4] * rs[m][1] + L[5] * rs[m][2];
-        g[3 * m + 2] = L[6] * rs[m][0] + L[7] * rs[m][1] + L[8] * rs[m][2];
+        for (int m = 0; m < 4; m++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) g[3 * m + r] = g[3 * m + r] + W.w[3 * q + r] * d[m];
     }
     reinterpret_cast<GradRec<R> *>(a.grad)[i] = gr;
-    if (!has_ghost) return;
-    // Ghost states and ghost gradients of this cell's boundary faces
-    // (get_bc_gradients, LBFS.cu:1941-2044).  A periodic component's ghost
-    // gradient is its partner's, which this launch may not have formed yet:
-    // the boundary-face flux kernel reads it from the partner and stores it
-    // here.
-    for (int q = 0; q < 6; q++) {
-        const int j = st[q];
-        if (j < a.nc) continue;
-        const int b = j - a.nc;
-        const Vec4<R> gs = ghost_state(a, b, own);
-        a.state[j] = gs;
-        const BcRec<R> r = a.bc_rec[b];
-        R gg[12];
-        const R d[4] = {gs.rho - own.rho, gs.u - own.u, gs.v - own.v, gs.w - own.w};
-        const bool dir_rho = a.bc_rho_type[b] == 1;
-        const bool dir_vel = a.bc_vel_type[b] != 2 && a.bc_vel_type[b] != 3;
-#pragma unroll
-        for (int m = 0; m < 4; m++) {
-            const bool dirichlet = (m == 0) ? dir_rho : dir_vel;
-            if (dirichlet) {
-                gg[3 * m + 0] = d[m] / r.dmag * r.dnx;
-                gg[3 * m + 1] = d[m] / r.dmag * r.dny;
-                gg[3 * m + 2] = d[m] / r.dmag * r.dnz;
-            } else {
-                gg[3 * m + 0] = g[3 * m + 0] * r.mx;
-                gg[3 * m + 1] = g[3 * m + 1] * r.my;
-                gg[3 * m + 2] = g[3 * m + 2] * r.mz;
-            }
-        }
-        GradRec<R> gro;
-#pragma unroll
-        for (int t = 0; t < 12; t++) gro.g[t] = gg[t];
-        reinterpret_cast<GradRec<R> *>(a.grad)[j] = gro;
-    }
 }
 
 // ------------------------------------------------------------------ K2 ----
@@ -296,35 +251,66 @@ __device__ __forceinline__ Vec4<R> axis_face_flux(const FluidArgs<R> &a, int f) 
 // General face: populate_lattice_macros (LBFS.cu:323-936).  Boundary faces
 // take the boundary branch except the face of the first ghost (LBFS.cu tests
 // neighbour > n_cells), which the host marks per instance in bc_branch.
+// Ghost of boundary face f (ghost cell g = its neighbour): its state
+// (update_unstructured_bcs, LBFS.cu:1843-1928) and its gradients
+// (get_bc_gradients, LBFS.cu:1933-2048): Dirichlet components the difference
+// to the owner over the owner-ghost distance along that direction, the others
+// the owner's gradient without its face-normal part; a periodic component
+// (type 3) the partner cell's gradient (gradients::Get_LS_Gradients,
+// gradients.cpp:428-440).  Formed here, once every cell's gradients exist,
+// and stored in the ghost's records for the fields and the adjoint.
+template <typename R>
+__device__ __forceinline__ void boundary_ghost(const FluidArgs<R> &a, int g, const Vec4<R> &own, const R (&go)[12],
+                                               Vec4<R> &gs, R (&gg)[12]) {
+    const int b = g - a.nc;
+    gs = ghost_state(a, b, own);
+    const BcRec<R> r = a.bc_rec[b];
+    const int rt = a.bc_rho_type[b], vt = a.bc_vel_type[b];
+    const R d[4] = {gs.rho - own.rho, gs.u - own.u, gs.v - own.v, gs.w - own.w};
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const bool dirichlet = (m == 0) ? rt == 1 : (vt != 2 && vt != 3);
+        if (dirichlet) {
+            gg[3 * m + 0] = d[m] / r.dmag * r.dnx;
+            gg[3 * m + 1] = d[m] / r.dmag * r.dny;
+            gg[3 * m + 2] = d[m] / r.dmag * r.dnz;
+        } else {
+            gg[3 * m + 0] = go[3 * m + 0] * r.mx;
+            gg[3 * m + 1] = go[3 * m + 1] * r.my;
+            gg[3 * m + 2] = go[3 * m + 2] * r.mz;
+        }
+    }
+    if (rt == 3 || vt == 3) {
+        R gp[12];
+        load_grad(a.grad + (size_t)12 * a.bc_periodic[b], gp);
+#pragma unroll
+        for (int t = 0; t < 12; t++)
+            if ((t < 3) ? rt == 3 : vt == 3) gg[t] = gp[t];
+    }
+    a.state[g] = gs;
+    GradRec<R> gr;
+#pragma unroll
+    for (int t = 0; t < 12; t++) gr.g[t] = gg[t];
+    reinterpret_cast<GradRec<R> *>(a.grad)[g] = gr;
+}
+
 template <typename R>
 __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int f, bool is_bc) {
     const int2 oc = __ldg(a.face_cells + f);
     const GenFace<R> geo = a.gen_face[a.axis_aligned ? f - a.ni : f];
-    const Vec4<R> s1 = a.state[oc.x], s2 = a.state[oc.y];
+    const Vec4<R> s1 = a.state[oc.x];
+    Vec4<R> s2;
     R g1[12], g2[12];
     load_grad(a.grad + (size_t)12 * oc.x, g1);
-    load_grad(a.grad + (size_t)12 * oc.y, g2);
+    if (is_bc) {
+        boundary_ghost(a, oc.y, s1, g1, s2, g2);
+    } else {
+        s2 = a.state[oc.y];
+        load_grad(a.grad + (size_t)12 * oc.y, g2);
+    }
     const R dt = geo.dt;
     const R S1[4] = {s1.rho, s1.u, s1.v, s1.w}, S2[4] = {s2.rho, s2.u, s2.v, s2.w};
     R pi[4], pn[4], p0[4], g3[12];
-    if (is_bc) {
-        // Periodic ghost (type 3): the partner's gradients (gradients::
-        // Get_LS_Gradients, gradients.cpp:428-440), complete now that every
-        // cell's gradients are formed; stored in the ghost's record too.
-        const int b = oc.y - a.nc;
-        const int rt = a.bc_rho_type[b], vt = a.bc_vel_type[b];
-        if (rt == 3 || vt == 3) {
-            R gp[12];
-            load_grad(a.grad + (size_t)12 * a.bc_periodic[b], gp);
-#pragma unroll
-            for (int t = 0; t < 12; t++)
-                if ((t < 3) ? rt == 3 : vt == 3) g2[t] = gp[t];
-            GradRec<R> gr;
-#pragma unroll
-            for (int t = 0; t < 12; t++) gr.g[t] = g2[t];
-            reinterpret_cast<GradRec<R> *>(a.grad)[oc.y] = gr;
-        }
-    }
     if (geo.bc_branch != R(0)) {
         const int b = oc.y - a.nc;
         const Vec4<R> bc = a.bc_val[b];

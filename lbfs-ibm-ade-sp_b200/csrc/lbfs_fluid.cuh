@@ -1,16 +1,20 @@
 // Fluid-side kernels of one LBFS time step (sm_100a).
 //
-//   K1 cell_gradients : ghost-cell update + least-squares cell gradients +
-//                       ghost gradients, one thread per interior cell.
-//                       Replaces update_unstructured_bcs (LBFS.cu:1843-1928),
-//                       get_interior_gradients (LBFS.cu:2177-2240) and
-//                       get_bc_gradients (LBFS.cu:1933-2048).
+//   K1 cell_gradients : least-squares cell gradients, one thread per interior
+//                       cell, the ghost states of its stencil formed in
+//                       registers.  Replaces get_interior_gradients
+//                       (LBFS.cu:2177-2240) and, for its own use,
+//                       update_unstructured_bcs (LBFS.cu:1843-1928).
 //   K2 face_flux      : D3Q15 reconstruction at the face lattice nodes,
 //                       equilibria, interface BGK relaxation and the face flux,
 //                       one thread per face, all in registers.  Replaces
 //                       calc_face_flux_x/_y/_z (LBFS.cu:2283-2569),
 //                       calc_face_flux (LBFS.cu:2574-2687) and calc_face_flux_bc
-//                       (LBFS.cu:2691-2810).
+//                       (LBFS.cu:2691-2810); the boundary-face thread also
+//                       forms and stores its ghost's state and gradients
+//                       (update_unstructured_bcs, get_bc_gradients,
+//                       LBFS.cu:1933-2048), which keeps that tail and its
+//                       registers out of K1.
 //   K3 cell_update    : deterministic gather of the face fluxes of each cell,
 //                       body + IBM force, forward-Euler update of soln_t1 and
 //                       of the primitive state, residual partial sums, status
@@ -111,6 +115,16 @@ template <typename R> struct alignas(16) LsRec {
     R pad;
 };
 
+// The same geometry folded for K1: per stencil entry q the gradient weights
+// W_q = LHS^-1 RHS_q (x, y, z), so that grad = sum_q W_q (s_q - s_i).  The
+// reference forms LHS^-1 (sum_q RHS_q (s_q - s_i)) (get_interior_gradients,
+// LBFS.cu:2177-2240): the same linear map with its products regrouped
+// (rounding differences of a few ulps), and 18 values per cell to load
+// instead of 27.
+template <typename R> struct alignas(16) LsW {
+    R w[18];
+};
+
 // Gradients of one cell: grad rho, grad u, grad v, grad w (x, y, z each).
 template <typename R> struct alignas(16) GradRec {
     R g[12];
@@ -129,7 +143,8 @@ template <typename R> struct FluidArgs {
     R *grad;                     // [12*(nc+nb)] rho(x,y,z) u(x,y,z) v(x,y,z) w(x,y,z)
     // K1 geometry
     const int2 *stencil;         // [3*nc] (6 stencil entries per cell)
-    const LsRec<R> *ls;          // [nc]
+    const LsRec<R> *ls;          // [nc] RHS and LHS^-1 (the adjoint's; null for FP32-bulk handles)
+    const LsW<R> *lsw;           // [nc] K1's folded weights
     const int *bc_rho_type, *bc_vel_type;
     const int *bc_periodic;      // [nb] partner cell of a type-3 ghost (Boundary_Conditions::periodic_node)
     const Vec4<R> *bc_val;       // [nb] (u, v, w, rho - rho0)

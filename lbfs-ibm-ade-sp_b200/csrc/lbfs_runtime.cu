@@ -193,11 +193,18 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     // K1 geometry
     std::vector<int2> stencil(3 * (size_t)nc);
     for (size_t q = 0; q < 3 * (size_t)nc; q++) stencil[q] = make_int2(m->gradient_stencil[2 * q], m->gradient_stencil[2 * q + 1]);
-    std::vector<LsRec<R>> ls(nc);
-    for (int i = 0; i < nc; i++) {
-        for (int q = 0; q < 18; q++) ls[i].rhs[q] = (R)m->rhs[18 * (size_t)i + q];
-        for (int q = 0; q < 9; q++) ls[i].lhs[q] = (R)m->lhs_inverse[9 * (size_t)i + q];
+    std::vector<LsRec<R>> ls(s->fp32 ? 0 : nc);  // the adjoint's (FP64 handles)
+    for (size_t i = 0; i < ls.size(); i++) {
+        for (int q = 0; q < 18; q++) ls[i].rhs[q] = (R)m->rhs[18 * i + q];
+        for (int q = 0; q < 9; q++) ls[i].lhs[q] = (R)m->lhs_inverse[9 * i + q];
         ls[i].pad = 0;
+    }
+    std::vector<LsW<R>> lsw(nc);  // W_q = LHS^-1 RHS_q, formed in FP64
+    for (int i = 0; i < nc; i++) {
+        const double *L = m->lhs_inverse + 9 * (size_t)i, *rh = m->rhs + 18 * (size_t)i;
+        for (int q = 0; q < 6; q++)
+            for (int r = 0; r < 3; r++)
+                lsw[i].w[3 * q + r] = (R)(L[3 * r] * rh[3 * q] + L[3 * r + 1] * rh[3 * q + 1] + L[3 * r + 2] * rh[3 * q + 2]);
     }
     std::vector<int> rt(nb), vt(nb), per(nb, 0);
     std::vector<Vec4<R>> bcv(nb);
@@ -299,7 +306,8 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     int rc = 0;
     int *d_rt, *d_vt, *d_per, *d_cf;
     int2 *d_stencil;
-    LsRec<R> *d_ls;
+    LsRec<R> *d_ls = nullptr;
+    LsW<R> *d_lsw;
     R *d_visc;
     Vec4<R> *d_bcv;
     BcRec<R> *d_bcr;
@@ -307,7 +315,8 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     AxisFace<R> *d_axf = nullptr;
     GenFace<R> *d_gen;
     double *d_vol, *d_ivol;
-    if ((rc = s->upload(&d_stencil, stencil)) || (rc = s->upload(&d_ls, ls)) ||
+    if ((rc = s->upload(&d_stencil, stencil)) || (rc = s->upload(&d_lsw, lsw)) ||
+        (!ls.empty() && (rc = s->upload(&d_ls, ls))) ||
         (rc = s->upload(&d_rt, rt)) || (rc = s->upload(&d_vt, vt)) || (rc = s->upload(&d_per, per)) ||
         (rc = s->upload(&d_bcv, bcv)) ||
         (rc = s->upload(&d_bcr, bcr)) || (rc = s->upload(&d_fcells, fcells)) || (rc = s->upload(&d_gen, gen)) ||
@@ -321,7 +330,7 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         if ((rc = s->upload(&d_cl, closure))) return rc;
         a.closure = d_cl;
     }
-    a.stencil = d_stencil; a.ls = d_ls; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt; a.bc_periodic = d_per;
+    a.stencil = d_stencil; a.ls = d_ls; a.lsw = d_lsw; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt; a.bc_periodic = d_per;
     a.bc_val = d_bcv; a.bc_rec = d_bcr; a.face_cells = d_fcells; a.axis_face = d_axf; a.gen_face = d_gen;
     a.visc_factor = d_visc; a.cell_faces = d_cf; a.cell_volume = d_vol; a.cell_inv_volume = d_ivol;
     Vec4<R> *d_state, *d_flux;
