@@ -114,13 +114,13 @@ def algorithmic_bytes(mesh, phase, fp64=True):
     R = 8 if fp64 else 4
     if phase == "flux":
         # per axis face: owner+neighbour ids 8, geometry (area, dt, t1, t2) 4R, flux out 4R;
-        # per bc face: ids 8, geometry 12R, bc types/values 8 + 4R, flux out 4R;
-        # per cell (interior and ghost): state 4R + 12 gradients 12R, visc factor R (interior)
-        return ni * (8 + 8 * R) + nb * (16 + 20 * R) + nc * (17 * R) + nb * (16 * R)
+        # per bc face: ids 8, geometry 12R, bc types/values 8 + 4R, bc record 9R, flux out 4R;
+        # per cell: state 4R + 12 gradients 12R, visc factor R; per ghost: state and gradients out 16R
+        return ni * (8 + 8 * R) + nb * (16 + 29 * R) + nc * (17 * R) + nb * (16 * R)
     if phase == "gradients":
-        # per cell: stencil 24, RHS 18R, LHS^-1 9R, state 4R, gradients out 12R;
-        # per ghost: bc record 9R + types 8 + values 4R, ghost state out 4R, ghost gradients out 12R
-        return nc * (24 + 43 * R) + nb * (8 + 29 * R)
+        # per cell: stencil 24, folded weights 18R, state 4R, gradients out 12R;
+        # per ghost: bc record 9R + types 8 + values 4R (ghost states formed in registers)
+        return nc * (24 + 34 * R) + nb * (8 + 13 * R)
     if phase == "update":
         # per cell: face list 24, volume 8, t1 in/out 64, state out 4R; each face flux read once 4R
         return nc * (96 + 4 * R) + nf * 4 * R

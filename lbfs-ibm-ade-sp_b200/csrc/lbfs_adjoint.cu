@@ -50,7 +50,8 @@ __device__ __forceinline__ void feq_grad(int k, double rho, double u, double v, 
 
 // Adjoint of interface_flux (FP64, rho0 = 0, qscale = 1): lo = adjoint of the
 // face flux (mass, momentum x, y, z); lfl += adjoint of the 15 reconstructed
-// equilibria.
+// equilibria.  The forward flux is (1 - tau) F_eq(rho, u) + tau F_fl with the
+// interface moments rho = sum fl, rho u = sum e fl.
 __device__ __forceinline__ void interface_flux_bwd(const double (&fl)[15], double tau, double area, int axis,
                                                    double nx, double ny, double nz, const double (&lo)[4],
                                                    double (&lfl)[15]) {
@@ -73,7 +74,7 @@ __device__ __forceinline__ void interface_flux_bwd(const double (&fl)[15], doubl
     for (int c = 0; c < 3; c++)
 #pragma unroll
         for (int j = 0; j < 4; j++) lF[c][j] = axis >= 0 ? (c == axis ? area * lo[j] : 0.0) : area * n[c] * lo[j];
-    double lrho = 0.0, lu[3] = {0, 0, 0};
+    // fr = (1 - tau) f + tau fl: the reconstructed populations' share
 #pragma unroll
     for (int k = 1; k < 15; k++) {
         const Dir3 e = dir3(k);
@@ -90,16 +91,27 @@ __device__ __forceinline__ void interface_flux_bwd(const double (&fl)[15], doubl
                 if (ee[q]) t += ee[q] * lF[c][1 + q];
             lfr += ee[c] * t;
         }
-        // fr = f - tau (f - fl) = (1 - tau) f + tau fl
-        const double lf = (1.0 - tau) * lfr;
         lfl[k] += tau * lfr;
-        double d[4];
-        feq_grad(k, rho, u[0], u[1], u[2], d);
-        lrho += lf * d[0];
-        lu[0] += lf * d[1];
-        lu[1] += lf * d[2];
-        lu[2] += lf * d[3];
     }
+    // the equilibrium's share, through the closed-form moments the forward
+    // kernel forms (rho u_c and rho (u_c u_m + d_cm / 3)), not 14 equilibria
+    const double keep = 1.0 - tau;
+    double lrho = 0.0, lu[3] = {0, 0, 0};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if (axis >= 0 && c != axis) continue;
+        lrho += lF[c][0] * u[c];
+        lu[c] += rho * lF[c][0];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            lrho += lF[c][1 + q] * (u[c] * u[q] + (q == c ? 1.0 / 3.0 : 0.0));
+            lu[c] += rho * lF[c][1 + q] * u[q];
+            lu[q] += rho * lF[c][1 + q] * u[c];
+        }
+    }
+    lrho *= keep;
+#pragma unroll
+    for (int c = 0; c < 3; c++) lu[c] *= keep;
     // u = m / rho
     const double lm[3] = {lu[0] * inv, lu[1] * inv, lu[2] * inv};
     lrho -= (lu[0] * u[0] + lu[1] * u[1] + lu[2] * u[2]) * inv;
@@ -133,15 +145,20 @@ struct FaceAdj {
     double s1[4], s2[4], g1[12], g2[12];
 };
 
-// One side of a face record: lambda of the side's state (4) and gradient (12).
+// One side of a face record: lambda of the side's state (4) and gradient (12),
+// 128 contiguous bytes; the owner sides of all faces, then the neighbour
+// sides, so that the per-cell gather (A2) reads whole records of neighbouring
+// faces.
+__device__ __forceinline__ double *face_side(const AdjointArgs &j, int f, int side) {
+    return j.lam_face + 16 * ((size_t)side * j.nf + f);
+}
 __device__ __forceinline__ void store_face_side(const AdjointArgs &j, int f, int side, const double (&ls)[4],
                                                 const double (&lg)[12]) {
-    double2 *o = reinterpret_cast<double2 *>(j.lam_face + 32 * (size_t)f);
-    double2 *os = o + (side == 0 ? 0 : 2), *og = o + (side == 0 ? 4 : 10);
-    os[0] = make_double2(ls[0], ls[1]);
-    os[1] = make_double2(ls[2], ls[3]);
+    double2 *o = reinterpret_cast<double2 *>(face_side(j, f, side));
+    o[0] = make_double2(ls[0], ls[1]);
+    o[1] = make_double2(ls[2], ls[3]);
 #pragma unroll
-    for (int t = 0; t < 6; t++) og[t] = make_double2(lg[2 * t], lg[2 * t + 1]);
+    for (int t = 0; t < 6; t++) o[2 + t] = make_double2(lg[2 * t], lg[2 * t + 1]);
 }
 
 // Axis-aligned interior face (axis_face_flux of the forward kernel): writes
@@ -465,17 +482,8 @@ __device__ __forceinline__ void face_flux_adjoint(const FluidArgs<double> &a, co
 }
 
 __device__ __forceinline__ void store_face(const AdjointArgs &j, int f, const FaceAdj &r) {
-    double2 *o = reinterpret_cast<double2 *>(j.lam_face + 32 * (size_t)f);
-#pragma unroll
-    for (int m = 0; m < 2; m++) {
-        o[m] = make_double2(r.s1[2 * m], r.s1[2 * m + 1]);
-        o[2 + m] = make_double2(r.s2[2 * m], r.s2[2 * m + 1]);
-    }
-#pragma unroll
-    for (int t = 0; t < 6; t++) {
-        o[4 + t] = make_double2(r.g1[2 * t], r.g1[2 * t + 1]);
-        o[10 + t] = make_double2(r.g2[2 * t], r.g2[2 * t + 1]);
-    }
+    store_face_side(j, f, 0, r.s1, r.g1);
+    store_face_side(j, f, 1, r.s2, r.g2);
 }
 
 __global__ void __launch_bounds__(128, 3) k_adj_flux_axis(FluidArgs<double> a, AdjointArgs j) {
@@ -515,14 +523,21 @@ __global__ void __launch_bounds__(128, 4) k_adj_cell(FluidArgs<double> a, Adjoin
     double ls[4] = {0, 0, 0, 0}, lg[12];
 #pragma unroll
     for (int t = 0; t < 12; t++) lg[t] = 0.0;
+    int cf[6];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const int2 p = __ldg(reinterpret_cast<const int2 *>(a.cell_faces) + 3 * i + q);
+        cf[2 * q] = p.x;
+        cf[2 * q + 1] = p.y;
+    }
 #pragma unroll
     for (int q = 0; q < 6; q++) {
-        const int e = a.cell_faces[6 * i + q];
+        const int e = cf[q];
         const int f = (e > 0 ? e : -e) - 1;
-        const double *r = j.lam_face + 32 * (size_t)f;
+        const double *r = face_side(j, f, e > 0 ? 0 : 1);
         double rs[4], rg[12];
-        load4(e > 0 ? r : r + 4, rs);
-        load12(e > 0 ? r + 8 : r + 20, rg);
+        load4(r, rs);
+        load12(r + 4, rg);
 #pragma unroll
         for (int m = 0; m < 4; m++) ls[m] += rs[m];
 #pragma unroll
@@ -550,7 +565,7 @@ __global__ void __launch_bounds__(128, 4) k_adj_cell(FluidArgs<double> a, Adjoin
         if (g < a.nc) continue;
         const int b = g - a.nc;
         const int f = a.ni + b;
-        const double *r = j.lam_face + 32 * (size_t)f;  // the boundary face: owner i, neighbour = ghost
+        const double *r = face_side(j, f, 1);  // the boundary face's ghost side (owner i, neighbour = ghost)
         const double *lbc = j.lam_bcv + 4 * (size_t)b;
         // Dirichlet boundary values seen by the face reconstruction
         const Vec4<double> bc = a.bc_val[b];
@@ -560,11 +575,11 @@ __global__ void __launch_bounds__(128, 4) k_adj_cell(FluidArgs<double> a, Adjoin
         const BcRec<double> br = a.bc_rec[b];
         const bool dir_rho = a.bc_rho_type[b] == 1, dir_vel = a.bc_vel_type[b] != 2;
 #pragma unroll
-        for (int m = 0; m < 4; m++) lgs[q][m] += r[4 + m];
+        for (int m = 0; m < 4; m++) lgs[q][m] += r[m];
         // ghost gradient (get_bc_gradients)
 #pragma unroll
         for (int m = 0; m < 4; m++) {
-            const double *lgg = r + 20 + 3 * m;
+            const double *lgg = r + 4 + 3 * m;
             const bool dirichlet = (m == 0) ? dir_rho : dir_vel;
             if (dirichlet) {
                 const double ld = (lgg[0] * br.dnx + lgg[1] * br.dny + lgg[2] * br.dnz) / br.dmag;
@@ -691,6 +706,26 @@ __global__ void k_adj_velocity_seed(FluidArgs<double> a, AdjointArgs j, const do
 }
 
 }  // namespace
+
+namespace {
+__global__ void __launch_bounds__(256) k_copy_list(CopyList l) {
+    const int q = blockIdx.y;
+    const double *src = l.src[q];
+    double *dst = l.dst[q];
+    const long long n = l.n[q];
+    const int stride = l.src_stride[q];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i * stride];
+}
+}  // namespace
+
+void launch_copy_list(const CopyList &l, cudaStream_t s) {
+    if (l.count <= 0) return;
+    long long most = 0;
+    for (int q = 0; q < l.count; q++) most = l.n[q] > most ? l.n[q] : most;
+    const int bx = (int)((most + 255) / 256 < 296 ? (most + 255) / 256 : 296);
+    k_copy_list<<<dim3(bx, l.count), 256, 0, s>>>(l);
+}
 
 void launch_adj_prim(const FluidArgs<double> &a, cudaStream_t s) {
     k_adj_prim<<<(a.nc + 255) / 256, 256, 0, s>>>(a);

@@ -11,7 +11,8 @@ namespace lbfs {
 struct AdjointArgs {
     double dt;                   // time-marching step
     double4 *lam_t1;             // [nc] adjoint of soln_t1 (mom x, y, z, mass)
-    double *lam_face;            // [32 nf] per face: owner state, neighbour state, owner grad, neighbour grad
+    double *lam_face;            // [2][nf][16] per side (owner, then neighbour) and face: state (4), grad (12)
+    int nf;                      // faces (the stride between the two sides)
     double *lam_bcv;             // [4 nb] Dirichlet boundary values seen by the boundary-face reconstruction
     double *lam_rs;              // [12 nc] lambda_R = LHS^-T lambda_grad per cell
     double *lam_state;           // [4 nc] state adjoint from the cell's faces, ghosts and stencil self terms
@@ -47,6 +48,27 @@ int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, cons
                         const InstanceGrid *instances, cudaStream_t s);
 
 void launch_adj_prim(const FluidArgs<double> &a, cudaStream_t s);
+
+// Up to kMaxCopyJobs device-to-device copies of doubles in one launch (the
+// per-step stores of the segment re-run): job q copies n[q] values,
+// dst[q][i] = src[q][i * src_stride[q]].
+constexpr int kMaxCopyJobs = 12;
+struct CopyList {
+    const double *src[kMaxCopyJobs];
+    double *dst[kMaxCopyJobs];
+    long long n[kMaxCopyJobs];
+    int src_stride[kMaxCopyJobs];
+    int count;
+    void add(const void *from, void *to, long long doubles, int stride = 1) {
+        if (doubles <= 0) return;
+        src[count] = static_cast<const double *>(from);
+        dst[count] = static_cast<double *>(to);
+        n[count] = doubles;
+        src_stride[count] = stride;
+        count++;
+    }
+};
+void launch_copy_list(const CopyList &l, cudaStream_t s);
 void launch_adj_velocity_seed(const FluidArgs<double> &a, const AdjointArgs &j, const double *weights, cudaStream_t s);
 int launch_adj_fluid(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
 // the phases of launch_adj_fluid: A1 on axis and on general faces (independent,

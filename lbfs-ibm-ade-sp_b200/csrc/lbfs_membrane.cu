@@ -37,6 +37,14 @@
 namespace lbfs {
 namespace {
 
+// Node sort: two int arrays of sort_capacity (bins, sorted list), then the bin
+// counts of a patch with at most kSortBinsSmem - 1 bins (larger patches count
+// in global memory).
+constexpr int kSortBinsSmem = 12288;
+size_t sort_smem_bytes(int sort_capacity) {
+    return (size_t)(sort_capacity > 0 ? sort_capacity : 1) * 2 * sizeof(int) + kSortBinsSmem * sizeof(int);
+}
+
 struct D3 {
     double x, y, z;
 };
@@ -656,6 +664,21 @@ __global__ void __launch_bounds__(128) k_mem_forces(MembraneArgs A) {
 // stencil weights and first x cell (recomputed from its position, so nothing
 // but the keys lives between the phases).  The last CTA of the launch writes
 // the prefix of patch cells over the membranes (the spread kernel's work list).
+// Spread records in sorted order: the node's stencil weights, first x cell and
+// index, and each node's sorted position.
+__device__ __forceinline__ void write_spread_records(const MembraneArgs &A, const MembraneConst &mc, const int *list) {
+    for (int e = threadIdx.x; e < mc.n_nodes; e += blockDim.x) {
+        const int n = mc.node0 + list[e];
+        SpreadRec rec;
+        for (int q = 0; q < 12; q++) rec.w[q] = A.node_w[12 * (size_t)n + q];
+        rec.b0 = A.node_base[3 * (size_t)n];
+        rec.node = n;
+        rec.pad[0] = rec.pad[1] = 0;
+        A.spread_rec[mc.node0 + e] = rec;
+        A.sorted_pos[n] = mc.node0 + e;
+    }
+}
+
 __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     extern __shared__ unsigned long long skeys[];  // 2 int arrays of sort_capacity: bins, sorted list
     __shared__ double shv[kMembraneThreads / 32][12];
@@ -756,6 +779,61 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     int *cursor = A.bin_cursor + (size_t)ms->patch_off + m;
     int *bins = reinterpret_cast<int *>(skeys);
     int *list = bins + A.sort_capacity;
+    if (nbins + 1 <= kSortBinsSmem) {
+        // the same counting sort with counts and cursors in shared memory
+        int *cnt = list + A.sort_capacity;
+        for (int b = threadIdx.x; b <= nbins; b += blockDim.x) cnt[b] = 0;
+        __syncthreads();
+        for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
+            const int *bb = A.node_base + 3 * (size_t)(mc.node0 + ln);
+            const int bin = (bb[0] - plo[0]) + bdim[0] * ((bb[1] - plo[1]) + bdim[1] * (bb[2] - plo[2]));
+            bins[ln] = bin;
+            atomicAdd(cnt + bin, 1);
+        }
+        __syncthreads();
+        {
+            __shared__ int cscan[kMembraneThreads];
+            const int count = nbins + 1;
+            const int per = (count + blockDim.x - 1) / blockDim.x;
+            const int b0 = min(count, (int)threadIdx.x * per), b1 = min(count, b0 + per);
+            int local = 0;
+            for (int b = b0; b < b1; b++) local += cnt[b];
+            cscan[threadIdx.x] = local;
+            __syncthreads();
+            for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+                const int x = threadIdx.x >= (unsigned)o ? cscan[threadIdx.x - o] : 0;
+                __syncthreads();
+                cscan[threadIdx.x] += x;
+                __syncthreads();
+            }
+            int run = cscan[threadIdx.x] - local;
+            for (int b = b0; b < b1; b++) {
+                const int c = cnt[b];
+                bin_start[b] = run;  // the spread's bin table
+                cnt[b] = run;        // cursor
+                run += c;
+            }
+        }
+        __syncthreads();
+        for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) list[atomicAdd(cnt + bins[ln], 1)] = ln;
+        __syncthreads();
+        // after placement cnt[b] is the end of bin b, i.e. the start of bin b + 1
+        for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
+            const int lo = b == 0 ? 0 : cnt[b - 1], hi = cnt[b];
+            for (int i = lo + 1; i < hi; i++) {
+                const int v = list[i];
+                int j = i - 1;
+                while (j >= lo && list[j] > v) {
+                    list[j + 1] = list[j];
+                    j--;
+                }
+                list[j + 1] = v;
+            }
+        }
+        __syncthreads();
+        write_spread_records(A, mc, list);
+        return;
+    }
     for (int b = threadIdx.x; b <= nbins; b += blockDim.x) bin_start[b] = 0;
     __syncthreads();
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
@@ -804,16 +882,7 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         }
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < mc.n_nodes; e += blockDim.x) {
-        const int n = mc.node0 + list[e];
-        SpreadRec rec;
-        for (int q = 0; q < 12; q++) rec.w[q] = A.node_w[12 * (size_t)n + q];
-        rec.b0 = A.node_base[3 * (size_t)n];
-        rec.node = n;
-        rec.pad[0] = rec.pad[1] = 0;
-        A.spread_rec[mc.node0 + e] = rec;
-        A.sorted_pos[n] = mc.node0 + e;
-    }
+    write_spread_records(A, mc, list);
 }
 
 // ---- M5: spread as a per-cell reduction over the sorted nodes -------------
@@ -1138,7 +1207,7 @@ __global__ void k_interior_viscosity(ViscArgs a) {
 }  // namespace
 
 void membrane_prepare(int sort_capacity) {
-    const size_t smem = (size_t)(sort_capacity > 0 ? sort_capacity : 1) * sizeof(unsigned long long);
+    const size_t smem = sort_smem_bytes(sort_capacity);
     cudaFuncSetAttribute(k_mem_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k_mem_forces<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
@@ -1176,7 +1245,7 @@ void launch_hi(void (*kernel)(Args...), dim3 grid, dim3 block, size_t smem, cuda
 
 int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, cudaEvent_t ev_advected,
                     cudaEvent_t ev_sorted) {
-    const size_t smem = (size_t)(a.sort_capacity > 0 ? a.sort_capacity : 1) * sizeof(unsigned long long);
+    const size_t smem = sort_smem_bytes(a.sort_capacity);
     const dim3 spring_grid((a.max_springs + 127) / 128, a.n_membranes);
     if (a.mode == kModeReference) {  // stress-free reference pass
         launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
@@ -1234,7 +1303,7 @@ void launch_membrane_forces(const MembraneArgs &a, cudaStream_t s) {
 }
 
 void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s) {
-    const size_t smem = (size_t)(a.sort_capacity > 0 ? a.sort_capacity : 1) * sizeof(unsigned long long);
+    const size_t smem = sort_smem_bytes(a.sort_capacity);
     launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, s, a);
 }
 

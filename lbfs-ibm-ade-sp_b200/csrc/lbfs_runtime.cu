@@ -1382,6 +1382,7 @@ int adj_prepare(lbfs_solver *s) {
     AdjointArgs &j = s->adj;
     const int nc = s->nc, nf = s->nf, nb = s->nb;
     int rc;
+    j.nf = nf;
     if ((rc = s->alloc(&j.lam_t1, nc)) || (rc = s->alloc(&j.lam_face, 32 * (size_t)nf)) ||
         (rc = s->alloc(&j.lam_bcv, 4 * (size_t)(nb > 0 ? nb : 1))) || (rc = s->alloc(&j.lam_rs, 12 * (size_t)nc)) ||
         (rc = s->alloc(&j.lam_state, 4 * (size_t)nc)) || (rc = s->alloc(&j.sigma_acc, nc)))
@@ -1724,27 +1725,46 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
             if ((rc = load_x(ck_x + (size_t)sg * xs))) return rc;
             launch_adjm_set_mad(ma, ck_m + (size_t)sg * M, st);
         }
+        // the stores of a step in one launch each (a dozen separate copies per
+        // step cost more than the copies themselves): before the first step
+        // t1, x and MAD; after step i its gradients, ghost states, x', node
+        // forces and scalars, and t1 and MAD of step i + 1
+        static_assert(sizeof(MembraneScalars) % sizeof(double) == 0, "MembraneScalars copied as doubles");
+        const int mad_stride = (int)(sizeof(MembraneScalars) / sizeof(double));
+        const double *mad_src = &ma.ms[0].MAD;
+        const int count = n1 - n0;
+        {
+            CopyList pre = {};
+            pre.add(a.t1, seg_t1, 4 * (long long)nc);
+            if (M > 0) {
+                pre.add(ma.x, seg_x, N);
+                pre.add(ma.y, seg_x + N, N);
+                pre.add(ma.z, seg_x + 2 * (size_t)N, N);
+                pre.add(mad_src, seg_m, M, mad_stride);
+            }
+            launch_copy_list(pre, st);
+        }
         for (int n = n0; n < n1; n++) {
             const size_t i = n - n0;
-            LBFS_CUDA(cudaMemcpyAsync(seg_t1 + i * nc, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
-            if (M > 0) {
-                if ((rc = save_x(seg_x + i * xs))) return rc;
-                launch_adjm_get_mad(ma, seg_m + i * M, st);
-            }
             s->t = t_start + n;
             if ((rc = run_one_step(s))) return rc;
-            LBFS_CUDA(cudaMemcpyAsync(seg_g + i * gsz, a.grad, sizeof(double) * gsz, cudaMemcpyDeviceToDevice, st));
-            if (s->nb > 0)
-                LBFS_CUDA(cudaMemcpyAsync(seg_h + i * s->nb, a.state + nc, sizeof(Vec4<double>) * s->nb,
-                                          cudaMemcpyDeviceToDevice, st));
+            CopyList post = {};
+            post.add(a.grad, seg_g + i * gsz, (long long)gsz);
+            post.add(a.state + nc, seg_h + i * s->nb, 4 * (long long)s->nb);
+            if ((int)i + 1 < count) post.add(a.t1, seg_t1 + (i + 1) * nc, 4 * (long long)nc);
             if (M > 0) {
-                if ((rc = save_x(seg_x + (i + 1) * xs))) return rc;
-                LBFS_CUDA(cudaMemcpyAsync(seg_f + i * xs, ma.fx, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
-                LBFS_CUDA(cudaMemcpyAsync(seg_f + i * xs + N, ma.fy, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
-                LBFS_CUDA(cudaMemcpyAsync(seg_f + i * xs + 2 * (size_t)N, ma.fz, sizeof(double) * N,
-                                          cudaMemcpyDeviceToDevice, st));
-                LBFS_CUDA(cudaMemcpyAsync(seg_s + i * M, ma.ms, sizeof(MembraneScalars) * M, cudaMemcpyDeviceToDevice, st));
+                double *xn1 = seg_x + (i + 1) * xs, *fi = seg_f + i * xs;
+                post.add(ma.x, xn1, N);
+                post.add(ma.y, xn1 + N, N);
+                post.add(ma.z, xn1 + 2 * (size_t)N, N);
+                post.add(ma.fx, fi, N);
+                post.add(ma.fy, fi + N, N);
+                post.add(ma.fz, fi + 2 * (size_t)N, N);
+                post.add(ma.ms, seg_s + i * M, (long long)(sizeof(MembraneScalars) / sizeof(double)) * M);
+                if ((int)i + 1 < count) post.add(mad_src, seg_m + (i + 1) * M, M, mad_stride);
             }
+            launch_copy_list(post, st);
+            LBFS_CUDA(cudaGetLastError());
         }
         return LBFS_OK;
     };
