@@ -17,7 +17,8 @@ OUT_DIR = os.path.join(HERE, "lbfs_b200", "_lib")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "liblbfs_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-CUDA_SOURCES = ["lbfs_fluid.cu", "lbfs_membrane.cu", "lbfs_runtime.cu", "lbfs_noalloc.cu", "lbfs_adjoint.cu", "lbfs_adjoint_mem.cu"]
+CUDA_SOURCES = ["lbfs_fluid.cu", "lbfs_membrane.cu", "lbfs_runtime.cu", "lbfs_noalloc.cu", "lbfs_adjoint.cu", "lbfs_adjoint_mem.cu",
+                "lbfs_mesh_gpu.cu"]
 HOST_SOURCES = ["host_setup.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]

@@ -20,6 +20,12 @@
 
 #include "lbfs_b200.h"
 #include "lbfs_internal.h"
+#include "lbfs_mesh_common.h"
+
+using lbfs::UniformDims;
+using lbfs::axis_vertices;
+using lbfs::jitter_unit;
+using lbfs::uniform_dims;
 
 namespace {
 
@@ -32,14 +38,10 @@ inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b
 inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline double mag(V3 a) { return std::sqrt(std::pow(a.x, 2) + std::pow(a.y, 2) + std::pow(a.z, 2)); }
 
-struct UniformDims {
-    int nx, ny, nz;
-    double dx, dy, dz;
-    int n_cells, n_faces, n_interior, n_bc, n_fx, n_fy, n_fz;
-};
+}  // namespace
 
 // unstructured_mesh::create_uniform_openfoam_mesh, unstructured_mesh.cpp:252-401
-UniformDims uniform_dims(double X, double Y, double Z, double dt) {
+lbfs::UniformDims lbfs::uniform_dims(double X, double Y, double Z, double dt) {
     UniformDims d;
     d.nx = (int)std::ceil(X / dt * 0.5);
     d.ny = (int)std::ceil(Y / dt * 0.5);
@@ -57,8 +59,6 @@ UniformDims uniform_dims(double X, double Y, double Z, double dt) {
     return d;
 }
 
-}  // namespace
-
 extern "C" int lbfs_mesh_uniform_counts(double X, double Y, double Z, double dt, int32_t *out) {
     if (!out || !(dt > 0) || !(X > 0) || !(Y > 0) || !(Z > 0)) return lbfs::set_error(LBFS_ERR_ARG, "bad domain");
     UniformDims d = uniform_dims(X, Y, Z, dt);
@@ -69,16 +69,6 @@ extern "C" int lbfs_mesh_uniform_counts(double X, double Y, double Z, double dt,
 }
 
 namespace {
-
-// Seeded uniform variate in [-1, 1) for (seed, vertex, axis): splitmix64 of
-// the combined key, top 53 bits.
-double jitter_unit(uint64_t seed, uint64_t vertex, int axis) {
-    uint64_t z = seed * 0x9E3779B97F4A7C15ull + vertex * 3 + (uint64_t)axis + 0x632BE59BD9B4E019ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    z = z ^ (z >> 31);
-    return (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
-}
 
 // How the generator places the vertices: the reference's mesh types
 // (unstructured_mesh.cpp:354-378) and the seeded jitter of interior vertices.
@@ -147,12 +137,10 @@ extern "C" int lbfs_mesh_build_jittered(double X, double Y, double Z, double dt,
                       gradient_stencil, lhs_inverse, rhs, bc_patch, delta_h, nullptr);
 }
 
-namespace {
-
 // Vertex coordinates along one axis of n cells (unstructured_mesh.cpp:290-378):
 // uniform, cosine-clustered, or the plateau function normalised to the length.
-std::vector<double> axis_vertices(int mesh_type, bool clustered, int n, double origin, double length, double step,
-                                  double ap, double bp) {
+std::vector<double> lbfs::axis_vertices(int mesh_type, bool clustered, int n, double origin, double length,
+                                        double step, double ap, double bp) {
     std::vector<double> v(n + 1);
     const double PI = std::acos(-1.0);  // globals.PI
     if (mesh_type == 4) {
@@ -170,6 +158,8 @@ std::vector<double> axis_vertices(int mesh_type, bool clustered, int n, double o
     }
     return v;
 }
+
+namespace {
 
 // Geometry and least-squares matrices of a hex mesh given as float vertices,
 // quadrilateral faces (4 vertex ids each, winding giving the owner -> neighbour

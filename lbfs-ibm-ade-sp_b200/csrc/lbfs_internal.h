@@ -11,6 +11,16 @@ namespace lbfs {
 // Thread-local last-error text behind lbfs_last_error; returns `code`.
 int set_error(int code, const std::string &msg);
 
+// Returns the error status of a failed CUDA runtime call from the enclosing
+// entry point (allocation failures as LBFS_ERR_NOMEM).
+#define LBFS_CUDA(call)                                                                                  \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            return lbfs::set_error(e_ == cudaErrorMemoryAllocation ? LBFS_ERR_NOMEM : LBFS_ERR_CUDA,     \
+                                   std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+    } while (0)
+
 // Largest membrane patch (cells of the IBM stencil's bounding box) a membrane
 // may cover; 48^3 cells covers a red cell of radius 8 cells deformed to twice
 // its diameter with the 4-point stencil margin.

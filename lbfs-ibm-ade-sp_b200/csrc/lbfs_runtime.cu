@@ -38,14 +38,6 @@ int set_error(int code, const std::string &msg) {
 
 using namespace lbfs;
 
-#define LBFS_CUDA(call)                                                                                  \
-    do {                                                                                                 \
-        cudaError_t e_ = (call);                                                                         \
-        if (e_ != cudaSuccess)                                                                           \
-            return set_error(e_ == cudaErrorMemoryAllocation ? LBFS_ERR_NOMEM : LBFS_ERR_CUDA,           \
-                             std::string(#call) + ": " + cudaGetErrorString(e_));                        \
-    } while (0)
-
 struct lbfs_solver {
     int device = 0;
     cudaStream_t stream = nullptr, stream2 = nullptr, stream3 = nullptr, stream4 = nullptr;

@@ -177,6 +177,12 @@ def lib():
                                                                                        ctypes.c_double, ctypes.c_uint64],
             "lbfs_mesh_openfoam_counts": [ctypes.c_char_p, _i32p],
             "lbfs_mesh_find_periodic_nodes": [ctypes.POINTER(MeshDesc), _f64p, _i32p],
+            "lbfs_mesh_build_gpu": [ctypes.c_double] * 4 + [_f64p, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                                                              ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                                              ctypes.c_double, ctypes.c_uint64, ctypes.c_int32,
+                                                              ctypes.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p,
+                                                              _f64p, _f64p, _f64p, _i32p, _f64p, _f64p, _i32p,
+                                                              _f64p, _f64p],
             "lbfs_mesh_import_openfoam": [ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                           ctypes.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
                                           _i32p, _f64p, _f64p, _i32p, ctypes.c_char_p, ctypes.c_int32],
@@ -236,5 +242,5 @@ EXPORTED = [
     "lbfs_residual_rms_noalloc", "lbfs_get_launch_shape", "lbfs_set_launch_shape", "lbfs_autotune",
     "lbfs_adjoint", "lbfs_checkpoint_size", "lbfs_checkpoint_save", "lbfs_checkpoint_load",
     "lbfs_mesh_build_jittered", "lbfs_mesh_build_rectilinear", "lbfs_mesh_write_openfoam", "lbfs_mesh_openfoam_counts",
-    "lbfs_mesh_import_openfoam", "lbfs_mesh_find_periodic_nodes",
+    "lbfs_mesh_import_openfoam", "lbfs_mesh_find_periodic_nodes", "lbfs_mesh_build_gpu",
 ]

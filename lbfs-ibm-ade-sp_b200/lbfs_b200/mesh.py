@@ -138,13 +138,14 @@ def uniform_counts(X, Y, Z, dt):
 
 
 def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_min=0.0, gradient="LS", jitter=0.0,
-                       seed=0, mesh_type=6, plateau_width=0.0, plateau_slope=0.0, closed_faces=True):
+                       seed=0, mesh_type=6, plateau_width=0.0, plateau_slope=0.0, closed_faces=True, device=None):
     """Mesh of ceil(X/(2 dt)) x ceil(Y/(2 dt)) x ceil(Z/(2 dt)) cells.  mesh_type 6 (uniform),
     7 / 5 (cosine-clustered in x, y / in x, y, z) and 4 (the plateau mesh of plateau_width,
     plateau_slope) are the reference generator's rectilinear meshes; with jitter > 0 every
     interior vertex of the uniform mesh moves by a seeded uniform offset of up to jitter x spacing
     per axis and the mesh is stepped through the general-normal flux (mesh_type 3); closed_faces=False
-    gives the reference importer's geometry of that mesh (lbfs_mesh_build_jittered)."""
+    gives the reference importer's geometry of that mesh (lbfs_mesh_build_jittered).  device = a
+    CUDA device index builds the same arrays on that GPU (lbfs_mesh_build_gpu)."""
     nc, nf, ni, nb, nfx, nfy, nfz, nt = uniform_counts(X, Y, Z, dt)
     owner = np.zeros(nf, np.int32)
     neighbour = np.zeros(nf, np.int32)
@@ -165,9 +166,17 @@ def build_uniform_mesh(X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), visc=0.1, fneq_m
             ctypes.byref(dh))
     hybrid = 1 if gradient == "hybrid" else 0
     grid = None
-    if mesh_type != 6:
-        if jitter > 0:
-            raise ValueError("jitter applies to the uniform mesh only")
+    if mesh_type != 6 and jitter > 0:
+        raise ValueError("jitter applies to the uniform mesh only")
+    if device is not None:
+        nx, ny, nz = (int(np.ceil(L / dt * 0.5)) for L in (X, Y, Z))
+        g = np.zeros(nx + ny + nz + 3)
+        _abi.check(_abi.lib().lbfs_mesh_build_gpu(X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, hybrid, int(mesh_type),
+                                                  float(plateau_width), float(plateau_slope), float(jitter), int(seed),
+                                                  1 if closed_faces else 0, int(device), *outs, _abi.ptr(g)))
+        if mesh_type != 6:
+            grid = (g[:nx + 1].copy(), g[nx + 1:nx + ny + 2].copy(), g[nx + ny + 2:].copy())
+    elif mesh_type != 6:
         nx, ny, nz = (int(np.ceil(L / dt * 0.5)) for L in (X, Y, Z))
         g = np.zeros(nx + ny + nz + 3)
         _abi.check(_abi.lib().lbfs_mesh_build_rectilinear(X, Y, Z, dt, _abi.ptr(org), visc, fneq_min, hybrid,
