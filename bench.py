@@ -444,7 +444,7 @@ def main():
         s.set_launch_shape(**fixed)
         shape = dict(s.launch_shape(), source="--launch-shape")
     else:
-        shape = s.autotune(reps=10)  # launch shape by whole-step timing (the library's autotuner)
+        shape = s.autotune(reps=40)  # launch shape by whole-step timing (the library's autotuner)
     s.set_profiling(1)  # events around each whole step only
     s.step(2, graph=True)
     s.synchronize()
@@ -533,7 +533,7 @@ def main():
         for x in (a, b):
             x.set_state(c.rho, c.u, c.v, c.w)
             x.step(2, graph=True)
-            x.autotune(reps=10)
+            x.autotune(reps=40)
             x.set_profiling(1)
         b.step(warmup, graph=True)
         a.step(warmup, graph=True)

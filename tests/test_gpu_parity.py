@@ -305,21 +305,25 @@ def test_fp32_bulk_against_fp64(builder):
 
 def test_pipelined_gradients_and_fluxes_are_bit_identical():
     """K1 -> K2 pipelined in chunks of cells on two streams (launch shape flux_chunks) gives the
-    same fields as the sequential step, bit for bit, at the benchmark size."""
+    same fields and residual norms as the sequential step, bit for bit, at the benchmark size."""
     c = cases.shear_rbc(n=64, level=3, radius_cells=8.0)
     out = []
-    for k in (1, 4):
+    for k in (1, 4, 8):
         s = make(c)
         s.set_launch_shape(flux_chunks=k)
         assert s.launch_shape()["flux_chunks"] == k
         s.keep_residuals(True)
         s.step(5, graph=True)
-        out.append((s.state(), s.nodes(), s.field(_abi.LBFS_FIELD_FACE_FLUX), s.field(_abi.LBFS_FIELD_RESIDUAL)))
+        out.append((s.state(), s.nodes(), s.field(_abi.LBFS_FIELD_FACE_FLUX), s.field(_abi.LBFS_FIELD_RESIDUAL),
+                    s.residuals()))
+        assert s.status() == 0
         s.close()
-    for a, b in zip(out[0][0], out[1][0]):
-        assert np.array_equal(a, b)
-    for x, y in zip(out[0][1:], out[1][1:]):
-        assert np.array_equal(x, y)
+    for o in out[1:]:
+        for a, b in zip(out[0][0], o[0]):
+            assert np.array_equal(a, b)
+        for x, y in zip(out[0][1:4], o[1:4]):
+            assert np.array_equal(x, y)
+        assert np.array_equal(o[4], out[0][4])
 
 
 def test_nonfinite_state_sets_status_flag():
