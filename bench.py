@@ -500,6 +500,13 @@ def main():
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": alg, "launch_ms": fluid[dom],
                 "timing": "per-kernel CUDA events, second timed pass of K steps with K1 and K2 not pipelined"}
+    # every fluid kernel against the same HBM peak (algorithmic bytes / event-timed duration)
+    kernel_roofline = {}
+    for ph, kn in (("gradients", "k_cell_gradients"), ("flux", "k_face_flux"), ("update", "k_cell_update")):
+        b_ = algorithmic_bytes(mesh, ph)
+        gbs = b_ / (fluid[ph] * 1e-3) / 1e9
+        kernel_roofline[kn] = {"algorithmic_bytes": b_, "ms": fluid[ph], "achieved_gbs": gbs,
+                               "frac": gbs / peaks["hbm_gbs"]}
 
     # end to end through the C ABI with page-locked host buffers
     e2e = None
@@ -597,6 +604,7 @@ def main():
             "launch_shape": shape,
             "clocks": clocks,
             "kernel_ms": phases,
+            "kernel_roofline": kernel_roofline,
             "rbc_node_steps_per_s": 642 * K * world / total_s,
             "fp32_bulk": fp32,
             "batched": batched,
