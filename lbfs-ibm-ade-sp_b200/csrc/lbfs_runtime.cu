@@ -1030,7 +1030,9 @@ extern "C" int lbfs_step_graph(lbfs_solver *s, int32_t n_steps) {
         cudaError_t e = cudaStreamEndCapture(s->stream, &g);
         if (rc) return rc;
         if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&s->graph, g, 0);
+        // keep the membrane kernels' launch priority inside the graph (without
+        // the flag every node runs at the priority of the stream it is launched into)
+        e = cudaGraphInstantiate(&s->graph, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
         s->graph_steps = 1;
