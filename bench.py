@@ -1,11 +1,13 @@
 #!/usr/bin/env python
 """Benchmark of the LBFS-IBM time step on B200.
 
-Workload (one GPU): wall-driven shear on a 64^3-cell uniform hex mesh stored as
-an unstructured face/cell list (262,144 cells, 798,720 faces), one red cell
-(level-3 icosphere: 642 nodes, 1,280 triangles, 1,920 springs, radius 8 cells,
-capillary number 0.1) with the 4-point Peskin IBM delta, plain FP64 -- the
-single-RBC shear configuration.  A "step" is one time step of the solver.
+Workload (one GPU): wall-driven shear on an n^3-cell uniform hex mesh stored as
+an unstructured face/cell list (default n = 64: 262,144 cells, 798,720 faces),
+one red cell (level-3 icosphere: 642 nodes, 1,280 triangles, 1,920 springs,
+radius 8 cells, capillary number 0.1) with the 4-point Peskin IBM delta, plain
+FP64 -- the single-RBC shear configuration.  A "step" is one time step of the
+solver.  hat2_value / hat2_e2e are the same workload on the reference's own
+2-point hat stencil, the like-for-like counterpart of the reference arm.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -35,9 +37,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "lbfs-ibm-ade-sp_b200"))
 
 METRIC = "Mcell-updates/s"
-WORKLOAD = ("shear_rbc: 64^3-cell uniform hex mesh as unstructured faces (262144 cells, 798720 faces), "
-            "wall shear (bc type 10), 1 red cell L3 icosphere (642 nodes, 1280 triangles, 1920 springs), "
-            "radius 8 cells, Ca 0.1, 4-point Peskin IBM, FP64")
+IBM_NAMES = {"peskin4": "4-point Peskin IBM", "hat2": "2-point hat IBM"}
+
+
+def workload(n, n_cells, n_faces, n_nodes, n_tris, n_springs, ibm="peskin4"):
+    """Name of the shear + red-cell workload at n^3 cells with its sizes."""
+    return (f"shear_rbc: {n}^3-cell uniform hex mesh as unstructured faces ({n_cells} cells, {n_faces} faces), "
+            f"wall shear (bc type 10), 1 red cell L3 icosphere ({n_nodes} nodes, {n_tris} triangles, "
+            f"{n_springs} springs), radius 8 cells, Ca 0.1, {IBM_NAMES[ibm]}, FP64")
 
 
 def parse():
@@ -48,6 +55,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=64, help="cells per axis")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-hat2", action="store_true", help="skip the run on the reference's 2-point hat stencil")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble section")
     ap.add_argument("--instances", type=int, default=64, help="instances of the batched ensemble")
@@ -127,18 +135,20 @@ def algorithmic_bytes(mesh, phase, fp64=True):
     return 0
 
 
-def read_traffic(kernel):
-    """DRAM bytes per launch from the committed ncu summary (profiles/dram_traffic.txt)."""
+def read_traffic(kernel, key):
+    """DRAM bytes per launch of `kernel` on the workload `key` (e.g. shear_rbc_64_fp64) from the
+    committed ncu summary profiles/dram_traffic.txt; None when that workload was not captured."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
         f = line.split()
-        if len(f) >= 2 and f[0] == kernel and not line.startswith("#"):
-            try:
-                return float(f[1])
-            except ValueError:
-                return None
+        if line.startswith("#") or len(f) < 3 or f[0] != kernel or f[1] != key:
+            continue
+        try:
+            return float(f[2])
+        except ValueError:
+            return None
     return None
 
 
@@ -152,45 +162,48 @@ def measured_peaks():
 
 def cpu_baseline_sample(n, budget_s=12.0, max_steps=200):
     """The reference's own kernels compiled for the host (oracle/_ref), serial,
-    on the same workload (its 2-point IBM; the reference has no 4-point kernel)."""
+    on the same workload with its 2-point IBM (the reference has no 4-point
+    kernel); inputs from the reference's own generator (oracle/ref_cases.py)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
     import ref_lbfs
-    from lbfs_b200 import _abi, cases
-    c = cases.shear_rbc(n=n, ibm_stencil=_abi.LBFS_IBM_HAT2)
-    if ref_lbfs.available():
-        from make_golden import ref_case
-        solver, kind = ref_case(c), "reference"
-    else:
-        from oracle_lbfs import OracleSolver
-        solver, kind = OracleSolver(c.mesh, c.params, c.membranes), "port"
-        solver.set_state(c.rho, c.u, c.v, c.w)
+    if not ref_lbfs.available():
+        return {"value": None, "unit": METRIC, "cores": 1, "kind": "reference",
+                "sample": "oracle/_ref/libref_lbfs.so was not built"}
+    import ref_cases
+    solver, n_cells, _ = ref_cases.shear_rbc(n=n)
     solver.step(1)
     t0, steps = time.perf_counter(), 0
     while steps < max_steps and time.perf_counter() - t0 < budget_s:
         solver.step(1)
         steps += 1
     dt = time.perf_counter() - t0
-    return {"value": c.mesh.n_cells * steps / dt / 1e6, "unit": METRIC, "cores": 1, "kind": kind,
-            "sample": f"{steps} steps of the {n}^3 + 1 red cell workload (2-point IBM), serial, {dt:.1f} s"}
+    solver.close()
+    return {"value": n_cells * steps / dt / 1e6, "unit": METRIC, "cores": 1, "kind": "reference",
+            "sample": f"{steps} steps of the {n}^3 + 1 red cell workload (2-point hat IBM), serial, {dt:.1f} s"}
 
 
 def _ref_worker(args):
+    """One reference instance: the workload built by the reference's own code
+    (oracle/ref_cases.py) and stepped by its kernels compiled for the host; this
+    process loads oracle/_ref/libref_lbfs.so and nothing of this repository's library."""
     n, steps, warmup = args
-    sys.path.insert(0, os.path.join(ROOT, "lbfs-ibm-ade-sp_b200"))
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
-    from lbfs_b200 import _abi, cases
-    from make_golden import ref_case
-    c = cases.shear_rbc(n=n, ibm_stencil=_abi.LBFS_IBM_HAT2)
-    rc = ref_case(c)
+    import ref_cases
+    rc, n_cells, _ = ref_cases.shear_rbc(n=n)
     rc.step(warmup)
     t0 = time.perf_counter()
     rc.step(steps)
-    return c.mesh.n_cells * steps, time.perf_counter() - t0
+    dt = time.perf_counter() - t0
+    rc.close()
+    return n_cells * steps, dt
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the step (its kernel sources
+    compiled for the host, oracle/_ref), one serial instance per host core, on
+    the benchmark workload with the reference's 2-point hat IBM (its uniform-mesh
+    kernels have no 4-point delta).  Same warm-up and timed steps as the CUDA arm
+    (steps capped at 200 so the run stays within minutes)."""
     if rank != 0:
         return 0
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -206,9 +219,8 @@ def run_reference(args, rank, world):
     except Exception:
         mem_procs = os.cpu_count() or 1
     procs = max(1, min(os.cpu_count() or 1, mem_procs))
-    # each "step" of this arm is one time step of every instance; bound the run to a few minutes
-    steps = max(1, min(args.steps, 60))
-    warmup = max(1, min(args.warmup, 3))
+    steps = max(1, min(args.steps, 200))
+    warmup = max(3, args.warmup)  # the CUDA arm's warm-up
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
@@ -217,14 +229,23 @@ def run_reference(args, rank, world):
     cells = sum(r[0] for r in res)
     slowest = max(r[1] for r in res)
     value = cells / slowest / 1e6
+    n = args.n
+    nc = n ** 3
+    nf = 3 * n * n * (n - 1) + 6 * n * n
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": world, "steps": steps,
         "warmup": warmup, "ms_per_step": slowest / steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD.replace("4-point Peskin", "2-point hat (the reference has no 4-point kernel)"),
-                   "instances": procs, "parallelism": f"{procs} independent host processes"},
+        "config": {"workload": workload(n, nc, nf, 642, 1280, 1920, ibm="hat2"), "cells": nc, "faces": nf,
+                   "membrane_nodes": 642, "ibm": "2-point hat",
+                   "ibm_note": "the reference's uniform-mesh IBM kernels (immersed_boundary_method.cu:14-97, "
+                               "947-1024) have only the 2-point hat stencil; the CUDA arm's headline uses the "
+                               "4-point Peskin delta and reports the 2-point hat run as hat2_value / hat2_e2e",
+                   "instances": procs, "parallelism": f"{procs} independent host processes, one instance each",
+                   "inputs": "built by the reference's own generator and lagrangian_object (oracle/ref_cases.py); "
+                             "no code of the CUDA arm is loaded"},
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "reference",
-                         "sample": f"{steps} steps x {procs} instances of the {args.n}^3 workload, "
+                         "sample": f"{steps} steps x {procs} instances of the {n}^3 workload, "
                                    f"reference kernels compiled for the host, one instance per core "
                                    f"(wall {wall:.1f} s incl. set-up)"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -435,6 +456,9 @@ def main():
     K = args.steps
     c = cases.shear_rbc(n=args.n)
     mesh = c.mesh
+    n_nodes = sum(m.n_nodes for m in c.membranes)
+    n_tris = sum(len(m.tris) for m in c.membranes)
+    n_springs = sum(len(m.springs) for m in c.membranes)
     s = GpuSolver(mesh, c.params, c.membranes, device=local_rank)
     s.set_state(c.rho, c.u, c.v, c.w)
     flush = torch.empty(512 * 2 ** 20, dtype=torch.uint8, device="cuda")  # 512 MB > 126 MB L2
@@ -495,7 +519,7 @@ def main():
     alg = algorithmic_bytes(mesh, dom)
     achieved = alg / (fluid[dom] * 1e-3) / 1e9
     kname = {"flux": "k_face_flux", "gradients": "k_cell_gradients", "update": "k_cell_update"}[dom]
-    traffic = read_traffic(kname)
+    traffic = read_traffic(kname, f"shear_rbc_{args.n}_fp64")
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": alg, "launch_ms": fluid[dom],
@@ -508,27 +532,53 @@ def main():
         kernel_roofline[kn] = {"algorithmic_bytes": b_, "ms": fluid[ph], "achieved_gbs": gbs,
                                "frac": gbs / peaks["hbm_gbs"]}
 
-    # end to end through the C ABI with page-locked host buffers
-    e2e = None
-    if not args.no_e2e:
+    def e2e_pass(h):
+        """End to end through the C ABI with page-locked host buffers: every step the
+        state goes host -> device, the step runs, the state comes back."""
         n = mesh.n_cells
         host = [torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
-        rho, u, v, w = s.state()
-        for h, a in zip(host, (rho, u, v, w)):
-            h[:] = a
-        s.set_profiling(False)
+        for hh, a in zip(host, h.state()):
+            hh[:] = a
+        h.set_profiling(False)
         Ke = min(K, 50)
         barrier()
         t0 = time.perf_counter()
         for _ in range(Ke):
-            _abi.check(_abi.lib().lbfs_set_state(s._h, *[_abi.ptr(h) for h in host]))
-            s.step(1, graph=True)
-            _abi.check(_abi.lib().lbfs_get_state(s._h, *[_abi.ptr(h) for h in host]))
+            _abi.check(_abi.lib().lbfs_set_state(h._h, *[_abi.ptr(x) for x in host]))
+            h.step(1, graph=True)
+            _abi.check(_abi.lib().lbfs_get_state(h._h, *[_abi.ptr(x) for x in host]))
         barrier()
         te = max_over_ranks(time.perf_counter() - t0, device="cuda")
-        e2e = {"value": n * Ke * world / te / 1e6, "unit": METRIC, "h2d_bytes_per_step": 4 * 8 * n,
-               "d2h_bytes_per_step": 4 * 8 * n, "steps": Ke, "timing": "host wall clock around set_state, step, "
-               "get_state (page-locked host arrays)"}
+        return {"value": n * Ke * world / te / 1e6, "unit": METRIC, "h2d_bytes_per_step": 4 * 8 * n,
+                "d2h_bytes_per_step": 4 * 8 * n, "steps": Ke, "timing": "host wall clock around set_state, step, "
+                "get_state (page-locked host arrays)"}
+
+    e2e = None if args.no_e2e else e2e_pass(s)
+
+    # the same workload on the reference's own IBM stencil (2-point hat): the like-for-like
+    # counterpart of the reference arm, which has no 4-point kernel
+    hat2 = None
+    if not args.no_hat2:
+        ch = cases.shear_rbc(n=args.n, ibm_stencil=_abi.LBFS_IBM_HAT2)
+        sh = GpuSolver(ch.mesh, ch.params, ch.membranes, device=local_rank)
+        sh.set_state(ch.rho, ch.u, ch.v, ch.w)
+        sh.step(warmup, graph=True)
+        sh.autotune(reps=40)
+        sh.set_profiling(1)
+        sh.step(2, graph=True)
+        acc = 0.0
+        barrier()
+        for k in range(K):
+            flush.fill_(k & 0xFF)
+            torch.cuda.synchronize()
+            sh.step(1, graph=True)
+            acc += sh.phase_times()[5]
+        barrier()
+        th = max_over_ranks(acc / 1e3, device="cuda")
+        hat2 = {"value": mesh.n_cells * K * world / th / 1e6, "ms_per_step": acc / K,
+                "e2e": None if args.no_e2e else e2e_pass(sh), "status_flags": sh.status(),
+                "workload": workload(args.n, mesh.n_cells, mesh.n_faces, n_nodes, n_tris, n_springs, ibm="hat2")}
+        sh.close()
 
     # FP32-bulk form on the same workload: throughput and field error against this FP64 run
     fp32 = None
@@ -594,7 +644,8 @@ def main():
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K, "warmup": warmup,
             "ms_per_step": t_step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cells": mesh.n_cells, "faces": mesh.n_faces, "membrane_nodes": 642,
+            "config": {"workload": workload(args.n, mesh.n_cells, mesh.n_faces, n_nodes, n_tris, n_springs),
+                       "cells": mesh.n_cells, "faces": mesh.n_faces, "membrane_nodes": n_nodes, "ibm": "4-point Peskin",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "flushed between timed steps (512 MB write)", "graph": "CUDA graph per step"},
             "roofline": roofline,
@@ -605,7 +656,10 @@ def main():
             "clocks": clocks,
             "kernel_ms": phases,
             "kernel_roofline": kernel_roofline,
-            "rbc_node_steps_per_s": 642 * K * world / total_s,
+            "rbc_node_steps_per_s": n_nodes * K * world / total_s,
+            "hat2_value": None if hat2 is None else hat2["value"],
+            "hat2_e2e": None if hat2 is None else hat2["e2e"],
+            "hat2": hat2,
             "fp32_bulk": fp32,
             "batched": batched,
             "adjoint": adjoint,

@@ -350,7 +350,10 @@ int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_every, cons
  * shared by every call, so calls that overlap on the GPU race -- serialise
  * them.  The first call on a device resolves the array's device address
  * (cudaGetSymbolAddress) and must come before any stream capture on that
- * device. */
+ * device.  The scratch is the CURRENT device's: `stream` must belong to the
+ * current device (LBFS_ERR_ARG otherwise).  The resolved address is kept for
+ * the life of the process; after cudaDeviceReset on a device, do not call
+ * this entry point on that device again in the same process. */
 #define LBFS_NOALLOC_MAX_BLOCKS 65536
 #define LBFS_NOALLOC_MAX_CELLS (LBFS_NOALLOC_MAX_BLOCKS * 256)
 int lbfs_residual_rms_noalloc(const double *d_res, int32_t n_cells, double ref_rho, double max_velocity,

@@ -43,7 +43,10 @@ struct NoallocScratch {
 
 // Address of g_noalloc_scratch on each device, resolved once per device with
 // that device current (the host-side symbol is only a stand-in, not a device
-// address).
+// address).  The table lives as long as the process: cudaDeviceReset (or any
+// other reset of a device's primary context) unloads the module, and the next
+// load may place the array elsewhere, so a caller that resets a device must
+// not call lbfs_residual_rms_noalloc on it afterwards in the same process.
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 double *g_noalloc_ptr[kMaxDevices] = {};
@@ -135,10 +138,20 @@ extern "C" int lbfs_residual_rms_noalloc(const double *d_res, int32_t n_cells, d
     if (blocks > LBFS_NOALLOC_MAX_BLOCKS)
         return set_error(LBFS_ERR_LIMIT, "lbfs_residual_rms_noalloc: n_cells exceeds LBFS_NOALLOC_MAX_CELLS (" +
                                              std::to_string((long long)LBFS_NOALLOC_MAX_CELLS) + ")");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (s) {
+        // the scratch address is the current device's: the stream must belong to it
+        int cur = 0, sdev = 0;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e == cudaSuccess) e = cudaStreamGetDevice(s, &sdev);
+        if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("stream device: ") + cudaGetErrorString(e));
+        if (sdev != cur)
+            return set_error(LBFS_ERR_ARG, "lbfs_residual_rms_noalloc: the stream belongs to device " +
+                                               std::to_string(sdev) + ", the current device is " + std::to_string(cur));
+    }
     NoallocScratch scratch;
     int rc = scratch_for_current_device(&scratch);
     if (rc) return rc;
-    cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(scratch.ticket, 0, sizeof(unsigned int), s);
     if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
     k_residual_rms_noalloc<<<(unsigned int)blocks, kNoallocThreads, 0, s>>>(d_res, n_cells, ref_rho,

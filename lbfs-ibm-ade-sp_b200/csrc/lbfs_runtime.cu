@@ -1023,13 +1023,16 @@ extern "C" int lbfs_step_graph(lbfs_solver *s, int32_t n_steps) {
     if (!s || n_steps < 0) return set_error(LBFS_ERR_ARG, "bad arguments");
     LBFS_CUDA(cudaSetDevice(s->device));
     if (!s->graph) {
-        cudaGraph_t g;
+        cudaGraph_t g = nullptr;
         LBFS_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
         int n = 0;
         int rc = enqueue(s, false, &n);
         cudaError_t e = cudaStreamEndCapture(s->stream, &g);
-        if (rc) return rc;
-        if (e != cudaSuccess) return set_error(LBFS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);  // a capture that ended but whose enqueue failed
+            if (rc) return rc;
+            return set_error(LBFS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        }
         // keep the membrane kernels' launch priority inside the graph (without
         // the flag every node runs at the priority of the stream it is launched into)
         e = cudaGraphInstantiate(&s->graph, g, cudaGraphInstantiateFlagUseNodePriority);

@@ -3,10 +3,11 @@
 # (read-only), with the host stubs in oracle/ref_stub/ and the driver
 # oracle/ref_driver.cpp.  Test infrastructure only: it produces the golden
 # vectors under tests/golden/ and the CPU timing of bench.py's reference arm.
-# Usage: oracle/build_ref.sh [REFERENCE_DIR]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_DIR]
+#   (default: $LBFS_REFERENCE_DIR, else /root/reference)
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${LBFS_REFERENCE_DIR:-/root/reference}}"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/LBFS.cu" ]; then
   echo "reference sources not found at $REF; skipping oracle/_ref" >&2

@@ -76,6 +76,14 @@ def spring_fixture(name, level):
     np.savez_compressed(os.path.join(HERE, name), nodes=nodes, tris=tris, ref_springs=spr, ref_tris=tri, ref_xyz=xyz)
 
 
+def icosphere_fixture():
+    """Unit level-3 icosphere (nodes, outward triangles): the red cell of the
+    reference arm's workload (oracle/ref_cases.py), which loads no code of this
+    repository."""
+    unit, tris = icosphere(3, 1.0)
+    np.savez_compressed(os.path.join(HERE, "icosphere_L3.npz"), unit_nodes=unit, tris=tris)
+
+
 def plateau_case():
     return cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_VANDERMONDE4, mesh_type=4,
                            plateau=(5.0, 0.3))
@@ -119,6 +127,7 @@ def main():
     spring_fixture("springs_L1.npz", 1)
     spring_fixture("springs_L2.npz", 2)
     spring_fixture("springs_L3.npz", 3)
+    icosphere_fixture()
     step_fixture("step_poiseuille_6x5x4.npz", cases.poiseuille(n=6, ny=5, nz=4), 20)
     step_fixture("step_shear_rbc_16.npz",
                  cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2), 10)

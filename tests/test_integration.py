@@ -7,10 +7,12 @@ import pytest
 
 from conftest import ROOT
 
-REF = "/root/reference"
+# the reference sources (read-only); LBFS_REFERENCE_DIR overrides the default location
+REF = os.environ.get("LBFS_REFERENCE_DIR", "/root/reference")
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "Solver_gpu.h")), reason="reference headers absent")
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "Solver_gpu.h")),
+                    reason=f"reference headers absent at {REF} (set LBFS_REFERENCE_DIR)")
 def test_drop_in_shim_compiles_against_reference_headers():
     src = os.path.join(ROOT, "lbfs-ibm-ade-sp_b200", "integration", "Solver_gpu_lbfs.cpp")
     cmd = ["g++", "-std=c++17", "-fsyntax-only", "-fpermissive", "-w", "-I", os.path.join(ROOT, "oracle", "ref_stub"),
