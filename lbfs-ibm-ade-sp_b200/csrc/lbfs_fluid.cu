@@ -83,101 +83,93 @@ __global__ void __launch_bounds__(TB, TB == 128 ? 5 : 1) k_cell_gradients(FluidA
 
 // ------------------------------------------------------------------ K2 ----
 
+// Density offset of the stored state: 0 in FP64 (a compile-time zero, so no
+// add is spent on it), rho0 in the FP32-bulk form.
+template <typename R> __device__ __forceinline__ R rho0_of(const FluidArgs<R> &a) {
+    if constexpr (sizeof(R) == 8) return R(0);
+    else return a.rho0;
+}
+
+// Lattice population divided by its weight, g_k = f_k / w_k, at a reconstructed
+// state L = (rho', u, v, w):  g = rho' + (rho' + rho0) X,
+// X = 3 e.u + q (4.5 (e.u)^2 - 1.5 |u|^2).  The reference's equilibrium
+// w_k rho (1 + X) (populate_feq_lattice_explicit, LBFS.cu:1041-1354; populate_feq,
+// LBFS.cu:940-1036 with the preconditioning factor q) with the weight applied
+// later, once per group of directions that share it.
+template <typename R>
+__device__ __forceinline__ R pop_g(const R (&L)[4], R eu, R rho0, R q) {
+    const R usq = L[1] * L[1] + L[2] * L[2] + L[3] * L[3];
+    const R X = R(3) * eu + q * (R(4.5) * eu * eu - R(1.5) * usq);
+    if constexpr (sizeof(R) == 8) return L[0] + L[0] * X;
+    else return L[0] + (L[0] + rho0) * X;
+}
+
+// Moments of the reconstructed lattice populations that the interface flux
+// needs: rho = sum f, m_c = sum e_c f, d_c = sum_{e_c != 0} f (= sum e_c e_c f),
+// o_xy, o_xz, o_yz = sum e_c e_m f.  Formed from sums and differences of
+// opposite directions (the D3Q15 set is symmetric), then weighted once per
+// group: a few dozen adds instead of one accumulation per direction and moment.
+template <typename R> struct LatMoments {
+    R rho, m[3], d[3], o[3];  // o: xy, xz, yz
+};
+template <typename R> __device__ __forceinline__ R o_of(const LatMoments<R> &M, int c, int q) {
+    // symmetric second moment e_c e_q for c != q
+    return (c + q == 1) ? M.o[0] : ((c + q == 2) ? M.o[1] : M.o[2]);
+}
+
+// Interface equilibrium, BGK relaxation towards the lattice populations and
+// the flux through the face: calculate_flux_at_interface (LBFS.cu:1462-1648)
+// and its axis-aligned forms (LBFS.cu:3648-4092).  The relaxed populations are
+// f_k - tau (f_k - fl_k), f_k the interface equilibrium, so the flux tensor is
+// (1 - tau) F_eq + tau F_fl, F_fl the moments of the lattice populations fl_k.
+// The D3Q15 weights make the equilibrium moments exact closed forms
+// (sum w e = 0, sum w e e = I / 3, sum w e e e e = (dd + dd + dd) / 9):
+//   sum_k e_c f_k = rho u_c = m_c,  sum_k e_c e_q f_k = q_s m_c m_q / rho + d_cq rho' / 3
+// (q_s the preconditioning factor; in the deviation form the d_cq term is
+// rho' / 3).  So the mass flux is m . n exactly, and the momentum flux is
+// formed from the six distinct second moments.  The reference sums the 15
+// equilibria explicitly; the closed form is the same quantity with fewer
+// roundings.  `axis` >= 0: only the face-normal component (axis-aligned faces,
+// n = e_axis); `axis` < 0: all three with the face normal.
+template <typename R>
+__device__ __forceinline__ Vec4<R> interface_flux(const LatMoments<R> &M, R rho0, R tau, R qscale, R area, int axis,
+                                                  R nx, R ny, R nz) {
+    const R rho_i = M.rho + rho0;
+    const R inv = R(1) / rho_i;
+    const R keep = R(1) - tau;
+    const R third = M.rho * R(1.0 / 3.0);
+    // relaxed second moment c, q
+    auto T = [&](int c, int q) -> R {
+        R eq = qscale * (M.m[c] * inv) * M.m[q];
+        R fl;
+        if (c == q) {
+            eq = eq + third;
+            fl = M.d[c];
+        } else {
+            fl = o_of(M, c, q);
+        }
+        return keep * eq + tau * fl;
+    };
+    Vec4<R> out;
+    if (axis >= 0) {
+        out.rho = M.m[axis] * area;
+        out.u = T(axis, 0) * area;
+        out.v = T(axis, 1) * area;
+        out.w = T(axis, 2) * area;
+    } else {
+        const R Txx = T(0, 0), Tyy = T(1, 1), Tzz = T(2, 2), Txy = T(0, 1), Txz = T(0, 2), Tyz = T(1, 2);
+        out.rho = (M.m[0] * nx + M.m[1] * ny + M.m[2] * nz) * area;
+        out.u = (Txx * nx + Txy * ny + Txz * nz) * area;
+        out.v = (Txy * nx + Tyy * ny + Tyz * nz) * area;
+        out.w = (Txz * nx + Tyz * ny + Tzz * nz) * area;
+    }
+    return out;
+}
+
 struct Dir {
     int ex, ey, ez;
 };
 __device__ __forceinline__ Dir dir_of(int k) { return {c_ex(k), c_ey(k), c_ez(k)}; }
-
-// Moments of the reconstructed populations, accumulated direction by
-// direction in the order k = 0..14 (the same sums and order as over a stored
-// fl[15], with 8-16 accumulators live instead of 15 populations).
-template <typename R> struct Moments {
-    R rho, m[3], F[3][4];  // F[c][.] over the directions crossing the face (c = axis, or all c)
-};
-template <typename R> __device__ __forceinline__ void moments_init(Moments<R> &M) {
-    M.rho = R(0);
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        M.m[c] = R(0);
-#pragma unroll
-        for (int j = 0; j < 4; j++) M.F[c][j] = R(0);
-    }
-}
-template <typename R>
-__device__ __forceinline__ void moments_add(Moments<R> &M, int k, R f, int axis) {
-    M.rho = (k == 0) ? f : M.rho + f;
-    if (k == 0) return;
-    const Dir e = dir_of(k);
-    if (e.ex) M.m[0] = (e.ex > 0) ? M.m[0] + f : M.m[0] - f;
-    if (e.ey) M.m[1] = (e.ey > 0) ? M.m[1] + f : M.m[1] - f;
-    if (e.ez) M.m[2] = (e.ez > 0) ? M.m[2] + f : M.m[2] - f;
-    if (axis == 0 && !e.ex) return;
-    if (axis == 1 && !e.ey) return;
-    if (axis == 2 && !e.ez) return;
-    const int ee[3] = {e.ex, e.ey, e.ez};
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        if (axis >= 0 && c != axis) continue;
-        if (!ee[c]) continue;
-        M.F[c][0] = (ee[c] > 0) ? M.F[c][0] + f : M.F[c][0] - f;
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-            if (!ee[q]) continue;
-            M.F[c][1 + q] = (ee[c] * ee[q] > 0) ? M.F[c][1 + q] + f : M.F[c][1 + q] - f;
-        }
-    }
-}
-
-// Interface equilibrium, BGK relaxation towards the lattice equilibria and
-// the flux through the face: calculate_flux_at_interface (LBFS.cu:1462-1648)
-// and its axis-aligned forms (LBFS.cu:3648-4092).  `axis` < 0 selects the
-// general three-component form with the face normal; otherwise only the
-// face-normal component is formed.
-//
-// The relaxed populations are f_k - tau (f_k - fl_k), f_k the interface
-// equilibrium, so the flux tensor is (1 - tau) F_eq + tau F_fl, F_fl the
-// first and second moments of the reconstructed fl_k over the directions
-// crossing the face and F_eq those of the equilibrium.  The D3Q15 weights
-// make the equilibrium moments exact closed forms (sum w e = 0,
-// sum w e e = I / 3, sum w e e e e = (dd + dd + dd) / 9):
-//   sum_k e_c f_k = rho u_c,  sum_k e_c e_m f_k = rho (q u_c u_m + d_cm / 3)
-// (q the preconditioning factor); in the deviation form (f' = f - w rho0)
-// the second moment's d_cm term is rho' / 3.  The reference sums the 15
-// equilibria explicitly; the closed form is the same quantity with fewer
-// roundings.
-template <typename R>
-__device__ __forceinline__ Vec4<R> interface_flux(Moments<R> &M, R rho0, R tau, R qscale, R area, int axis, R nx,
-                                                  R ny, R nz) {
-    const R rho_dev = M.rho;
-    const R rho_i = rho_dev + rho0;
-    const R inv = R(1) / rho_i;
-    const R u[3] = {inv * M.m[0], inv * M.m[1], inv * M.m[2]};
-    const R keep = R(1) - tau;
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        if (axis >= 0 && c != axis) continue;
-        M.F[c][0] = keep * (rho_i * u[c]) + tau * M.F[c][0];
-#pragma unroll
-        for (int m = 0; m < 3; m++) {
-            R eq = rho_i * (qscale * u[c] * u[m]);
-            if (m == c) eq = eq + rho_dev * R(1.0 / 3.0);
-            M.F[c][1 + m] = keep * eq + tau * M.F[c][1 + m];
-        }
-    }
-    Vec4<R> out;
-    if (axis >= 0) {
-        out.rho = M.F[axis][0] * area;
-        out.u = M.F[axis][1] * area;
-        out.v = M.F[axis][2] * area;
-        out.w = M.F[axis][3] * area;
-    } else {
-        out.rho = (M.F[0][0] * nx + M.F[1][0] * ny + M.F[2][0] * nz) * area;
-        out.u = (M.F[0][1] * nx + M.F[1][1] * ny + M.F[2][1] * nz) * area;
-        out.v = (M.F[0][2] * nx + M.F[1][2] * ny + M.F[2][2] * nz) * area;
-        out.w = (M.F[0][3] * nx + M.F[1][3] * ny + M.F[2][3] * nz) * area;
-    }
-    return out;
-}
 
 template <typename R> __device__ __forceinline__ void load_grad(const R *g, R (&o)[12]) {
     const GradRec<R> r = *reinterpret_cast<const GradRec<R> *>(g);
@@ -185,67 +177,113 @@ template <typename R> __device__ __forceinline__ void load_grad(const R *g, R (&
     for (int t = 0; t < 12; t++) o[t] = r.g[t];
 }
 
-// Axis-aligned face: populate_lattice_macros_uniform_{x,y,z} (LBFS.cu:2939-3644).
-// For direction k the lattice node sits at x_f - e_k dt; directions with
-// e_k[axis] = +1 extrapolate from the owner, -1 from the neighbour, 0 from the
-// face centre with the distance-weighted gradient.
-template <typename R, int axis>
+// The five directions of one side of an axis-A face: e_A = s (s = +1 owner
+// side, -1 neighbour side) with (e_B, e_C) in {(0,0), (+,+), (+,-), (-,+), (-,-)}
+// (B < C the other two axes).  populate_lattice_macros_uniform_{x,y,z}
+// (LBFS.cu:2939-3644): the lattice node sits at x_f - e dt and is extrapolated
+// from the side's cell: L = p - dt (e . g).  With a = p - s dt g_A,
+// b = dt g_B, c = dt g_C the four corners are (a -+ b) -+ c.  Returns the
+// side's weighted sums S = sum f, YB = sum e_B f, YC = sum e_C f.
+template <typename R, int A>
+__device__ __forceinline__ void axis_side(const R (&p)[4], const R (&g)[12], R s, R dt, R rho0, R &S, R &YB,
+                                          R &YC) {
+    constexpr int B = A == 0 ? 1 : 0, C = A == 2 ? 1 : 2;
+    R av[4], amb[4], apb[4], cv[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        av[m] = p[m] - s * dt * g[3 * m + A];
+        const R b = dt * g[3 * m + B];
+        cv[m] = dt * g[3 * m + C];
+        amb[m] = av[m] - b;  // e_B = +1
+        apb[m] = av[m] + b;  // e_B = -1
+    }
+    // e = (s e_A, e_B, e_C) in (A, B, C) order; e.u = s u_A + e_B u_B + e_C u_C
+    const R g0 = pop_g<R>(av, s * av[1 + A], rho0, R(1));
+    R Lc[4], gpp, gpm, gmp, gmm;
+#pragma unroll
+    for (int m = 0; m < 4; m++) Lc[m] = amb[m] - cv[m];
+    gpp = pop_g<R>(Lc, s * Lc[1 + A] + Lc[1 + B] + Lc[1 + C], rho0, R(1));
+#pragma unroll
+    for (int m = 0; m < 4; m++) Lc[m] = amb[m] + cv[m];
+    gpm = pop_g<R>(Lc, s * Lc[1 + A] + Lc[1 + B] - Lc[1 + C], rho0, R(1));
+#pragma unroll
+    for (int m = 0; m < 4; m++) Lc[m] = apb[m] - cv[m];
+    gmp = pop_g<R>(Lc, s * Lc[1 + A] - Lc[1 + B] + Lc[1 + C], rho0, R(1));
+#pragma unroll
+    for (int m = 0; m < 4; m++) Lc[m] = apb[m] + cv[m];
+    gmm = pop_g<R>(Lc, s * Lc[1 + A] - Lc[1 + B] - Lc[1 + C], rho0, R(1));
+    const R bp = gpp + gpm, bm = gmp + gmm, cp = gpp - gpm, cm = gmp - gmm;
+    constexpr R w_axis = R(1.0 / 9.0), w_corner = R(1.0 / 72.0);
+    S = w_axis * g0 + w_corner * (bp + bm);
+    YB = w_corner * (bp - bm);
+    YC = w_corner * (cp + cm);
+}
+
+// Axis-aligned interior face of axis A (calc_face_flux_x/_y/_z, LBFS.cu:2283-2569):
+// directions with e_A = +1 extrapolate from the owner, -1 from the neighbour,
+// 0 from the face centre with the distance-weighted gradient.
+template <typename R, int A>
 __device__ __forceinline__ Vec4<R> axis_face_flux(const FluidArgs<R> &a, int f) {
+    constexpr int B = A == 0 ? 1 : 0, C = A == 2 ? 1 : 2;
     const int2 oc = __ldg(a.face_cells + f);
     const AxisFace<R> geo = a.axis_face[f];
     const Vec4<R> s1 = a.state[oc.x], s2 = a.state[oc.y];
     R g1[12], g2[12];
     load_grad(a.grad + (size_t)12 * oc.x, g1);
     load_grad(a.grad + (size_t)12 * oc.y, g2);
+    const R rho0 = rho0_of(a);
     const R dt = geo.dt, t1 = geo.t1, t2 = geo.t2;
-    const R c = t2 - t1;
-    const R wa = fabs(t2 / c), wb = fabs(t1 / c);
+    const R ic = R(1) / (t2 - t1);
+    const R wa = fabs(t2 * ic), wb = fabs(t1 * ic);
     const R S1[4] = {s1.rho, s1.u, s1.v, s1.w}, S2[4] = {s2.rho, s2.u, s2.v, s2.w};
     R pi[4], pn[4], p0[4];
 #pragma unroll
     for (int m = 0; m < 4; m++) {
-        pi[m] = S1[m] - t1 * g1[3 * m + axis];
-        pn[m] = S2[m] - (t2 * g2[3 * m + axis]);
+        pi[m] = S1[m] - t1 * g1[3 * m + A];
+        pn[m] = S2[m] - t2 * g2[3 * m + A];
         p0[m] = (pi[m] + pn[m]) * R(0.5);
     }
-    constexpr int ob = axis == 0 ? 1 : 0;  // other axes in increasing order
-    constexpr int oc2 = axis == 2 ? 1 : 2;
-    Moments<R> M;
-    moments_init(M);
-#pragma unroll
-    for (int k = 0; k < 15; k++) {
-        const Dir e = dir_of(k);
-        const int ee[3] = {e.ex, e.ey, e.ez};
-        R L[4];
+    LatMoments<R> M;
+    R Sp, Bp, Cp, Sn, Bn, Cn;
+    axis_side<R, A>(pi, g1, R(1), dt, rho0, Sp, Bp, Cp);
+    axis_side<R, A>(pn, g2, R(-1), dt, rho0, Sn, Bn, Cn);
+    // centre directions (e_A = 0): rest, +-B, +-C, from p0 with gi = wa g1 + wb g2
+    R gz0, gbp, gbm, gcp, gcm;
+    {
+        R bv[4], cv[4], L[4];
 #pragma unroll
         for (int m = 0; m < 4; m++) {
-            R val;
-            if (ee[axis] > 0) {
-                val = pi[m] - g1[3 * m + axis] * dt;
-                if (ee[ob]) val = (ee[ob] > 0) ? val - g1[3 * m + ob] * dt : val + g1[3 * m + ob] * dt;
-                if (ee[oc2]) val = (ee[oc2] > 0) ? val - g1[3 * m + oc2] * dt : val + g1[3 * m + oc2] * dt;
-            } else if (ee[axis] < 0) {
-                val = pn[m] + g2[3 * m + axis] * dt;
-                if (ee[ob]) val = (ee[ob] > 0) ? val - g2[3 * m + ob] * dt : val + g2[3 * m + ob] * dt;
-                if (ee[oc2]) val = (ee[oc2] > 0) ? val - g2[3 * m + oc2] * dt : val + g2[3 * m + oc2] * dt;
-            } else {
-                val = p0[m];
-                if (ee[ob]) {
-                    const R gi = g1[3 * m + ob] * wa + g2[3 * m + ob] * wb;
-                    val = (ee[ob] > 0) ? val - gi * dt : val + gi * dt;
-                }
-                if (ee[oc2]) {
-                    const R gi = g1[3 * m + oc2] * wa + g2[3 * m + oc2] * wb;
-                    val = (ee[oc2] > 0) ? val - gi * dt : val + gi * dt;
-                }
-            }
-            L[m] = val;
+            bv[m] = dt * (g1[3 * m + B] * wa + g2[3 * m + B] * wb);
+            cv[m] = dt * (g1[3 * m + C] * wa + g2[3 * m + C] * wb);
         }
-        moments_add(M, k, feq_dev<R>(k, L[0], L[1], L[2], L[3], a.rho0, R(1)), axis);
+        gz0 = pop_g<R>(p0, R(0), rho0, R(1));
+#pragma unroll
+        for (int m = 0; m < 4; m++) L[m] = p0[m] - bv[m];
+        gbp = pop_g<R>(L, L[1 + B], rho0, R(1));
+#pragma unroll
+        for (int m = 0; m < 4; m++) L[m] = p0[m] + bv[m];
+        gbm = pop_g<R>(L, -L[1 + B], rho0, R(1));
+#pragma unroll
+        for (int m = 0; m < 4; m++) L[m] = p0[m] - cv[m];
+        gcp = pop_g<R>(L, L[1 + C], rho0, R(1));
+#pragma unroll
+        for (int m = 0; m < 4; m++) L[m] = p0[m] + cv[m];
+        gcm = pop_g<R>(L, -L[1 + C], rho0, R(1));
     }
+    constexpr R w_rest = R(2.0 / 9.0), w_axis = R(1.0 / 9.0);
+    const R Sz = w_rest * gz0 + w_axis * ((gbp + gbm) + (gcp + gcm));
+    const R Bz = w_axis * (gbp - gbm), Cz = w_axis * (gcp - gcm);
+    M.rho = (Sp + Sn) + Sz;
+    M.m[A] = Sp - Sn;
+    M.d[A] = Sp + Sn;
+    M.m[B] = (Bp + Bn) + Bz;
+    M.m[C] = (Cp + Cn) + Cz;
+    M.o[A + B - 1] = Bp - Bn;  // o index of the pair (A, B): xy 0, xz 1, yz 2
+    M.o[A + C - 1] = Cp - Cn;
+    M.d[B] = M.d[C] = M.o[B + C - 1] = R(0);  // not read by the axis-A flux
     const R vf = a.visc_factor[oc.x];
     const R tau = (a.testcase == 8) ? R(0) : (a.visc * vf * R(3) / dt * a.gamma_inv);
-    return interface_flux<R>(M, a.rho0, tau, R(1), geo.area, axis, 0, 0, 0);
+    return interface_flux<R>(M, rho0, tau, R(1), geo.area, A, 0, 0, 0);
 }
 
 // General face: populate_lattice_macros (LBFS.cu:323-936).  Boundary faces
@@ -299,6 +337,7 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
     const int2 oc = __ldg(a.face_cells + f);
     const GenFace<R> geo = a.gen_face[a.axis_aligned ? f - a.ni : f];
     const Vec4<R> s1 = a.state[oc.x];
+    const R rho0 = rho0_of(a);
     Vec4<R> s2;
     R g1[12], g2[12];
     load_grad(a.grad + (size_t)12 * oc.x, g1);
@@ -337,24 +376,28 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
         for (int t = 0; t < 12; t++) g3[t] = (g1[t] + g2[t]) * R(0.5);
     }
     // Upwind selection by the sign of n.e_k with the threshold 0.001 dt
-    // (LBFS.cu:351-352 override the sin(pi/14) arguments).
+    // (LBFS.cu:351-352 override the sin(pi/14) arguments).  Directions come in
+    // opposite pairs (k, k + 1): sum and difference of the pair's populations
+    // feed the moments.
     const R thr = R(0.001) * dt;
-    Moments<R> M;
-    moments_init(M);
-    moments_add(M, 0, feq_dev<R>(0, p0[0], p0[1], p0[2], p0[3], a.rho0, a.recon_q), -1);
+    const R q = a.recon_q;
+    const R g0 = pop_g<R>(p0, R(0), rho0, q);
+    R sax[3], dax[3];          // axis pairs (+e_c, -e_c): sum and difference
+    R sc, mcor[3], ocor[3];    // corner pairs: sum of sums; sum of e_c x difference; of e_c e_q x sum
 #pragma unroll
     for (int k = 1; k < 15; k += 2) {
-        const Dir e = dir_of(k);
+        const Dir e = dir_of(k);  // odd k: e_k; k + 1: -e_k
+        const int ee[3] = {e.ex, e.ey, e.ez};
         const R s = (k < 7) ? (e.ex ? geo.nx : (e.ey ? geo.ny : geo.nz))
                             : (R(e.ex) * geo.nx + R(e.ey) * geo.ny + R(e.ez) * geo.nz);
         // side of direction k and of its opposite k+1: 0 owner, 1 neighbour, 2 centre
         const int side_k = (s > thr) ? 0 : ((s < -thr) ? 1 : 2);
         const int side_o = (side_k == 2) ? 2 : 1 - side_k;
+        R gp[2];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const int kk = k + h;
             const int side = h ? side_o : side_k;
-            const int ee[3] = {h ? -e.ex : e.ex, h ? -e.ey : e.ey, h ? -e.ez : e.ez};
+            const int sg = h ? -1 : 1;
             R L[4];
 #pragma unroll
             for (int m = 0; m < 4; m++) {
@@ -363,16 +406,51 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
                 for (int d = 0; d < 3; d++) {
                     if (!ee[d]) continue;
                     const R gd = side == 0 ? g1[3 * m + d] : (side == 1 ? g2[3 * m + d] : g3[3 * m + d]);
-                    val = (ee[d] > 0) ? val - gd * dt : val + gd * dt;
+                    val = (sg * ee[d] > 0) ? val - gd * dt : val + gd * dt;
                 }
                 L[m] = val;
             }
-            moments_add(M, kk, feq_dev<R>(kk, L[0], L[1], L[2], L[3], a.rho0, a.recon_q), -1);
+            R eu = R(0);
+            bool first = true;
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                if (!ee[d]) continue;
+                const R ud = (sg * ee[d] > 0) ? L[1 + d] : -L[1 + d];
+                eu = first ? ud : eu + ud;
+                first = false;
+            }
+            gp[h] = pop_g<R>(L, eu, rho0, q);
         }
+        const R sig = gp[0] + gp[1], del = gp[0] - gp[1];
+        if (k < 7) {
+            const int c = e.ex ? 0 : (e.ey ? 1 : 2);
+            sax[c] = sig;
+            dax[c] = del;
+        } else if (k == 7) {  // (+,+,+): first corner pair
+            sc = sig;
+#pragma unroll
+            for (int d = 0; d < 3; d++) { mcor[d] = del; ocor[d] = sig; }
+        } else {
+            sc = sc + sig;
+#pragma unroll
+            for (int d = 0; d < 3; d++) mcor[d] = (ee[d] > 0) ? mcor[d] + del : mcor[d] - del;
+            ocor[0] = (ee[0] * ee[1] > 0) ? ocor[0] + sig : ocor[0] - sig;
+            ocor[1] = (ee[0] * ee[2] > 0) ? ocor[1] + sig : ocor[1] - sig;
+            ocor[2] = (ee[1] * ee[2] > 0) ? ocor[2] + sig : ocor[2] - sig;
+        }
+    }
+    constexpr R w_rest = R(2.0 / 9.0), w_axis = R(1.0 / 9.0), w_corner = R(1.0 / 72.0);
+    LatMoments<R> M;
+    M.rho = w_rest * g0 + w_axis * ((sax[0] + sax[1]) + sax[2]) + w_corner * sc;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        M.m[c] = w_axis * dax[c] + w_corner * mcor[c];
+        M.d[c] = w_axis * sax[c] + w_corner * sc;
+        M.o[c] = w_corner * ocor[c];
     }
     const R vf = is_bc ? R(1) : a.visc_factor[oc.x];
     const R tau = (a.testcase == 8) ? R(0) : (a.visc * vf * R(3) / dt * a.gamma_inv);
-    return interface_flux<R>(M, a.rho0, tau, a.gamma_inv, geo.area, -1, geo.nx, geo.ny, geo.nz);
+    return interface_flux<R>(M, rho0, tau, a.gamma_inv, geo.area, -1, geo.nx, geo.ny, geo.nz);
 }
 
 // Interior faces of an axis-aligned mesh: faces [0, nfx) x, [nfx, nfx+nfy) y,
@@ -390,6 +468,23 @@ __global__ void __launch_bounds__(TB, 640 / TB) k_face_flux(FluidArgs<R> a, Face
     else if (f < a.nfx + a.nfy) out = axis_face_flux<R, 1>(a, f);
     else out = axis_face_flux<R, 2>(a, f);
     a.flux[f] = out;
+}
+
+// Interior faces of an axis-aligned mesh, tile by tile: block b takes the
+// faces owned by the TB cells of tile tile0 + b -- the x, y and z faces whose
+// owner lies in the tile, three contiguous ranges of the face list
+// (tiles[3 t + axis] = first face of that axis owned by tile t) -- so the
+// tile's cell states and gradients come from DRAM once for all three axes
+// instead of once per axis sweep.  Warps take the x faces, then the y, then
+// the z faces: one axis per warp at a time.
+template <typename R, int TB>
+__global__ void __launch_bounds__(TB, 640 / TB) k_face_flux_tiles(FluidArgs<R> a, int tile0) {
+    const int *tp = a.flux_tiles + 3 * (tile0 + (int)blockIdx.x);
+    const int f0x = __ldg(tp), f0y = __ldg(tp + 1), f0z = __ldg(tp + 2);
+    const int f1x = __ldg(tp + 3), f1y = __ldg(tp + 4), f1z = __ldg(tp + 5);
+    for (int f = f0x + (int)threadIdx.x; f < f1x; f += TB) a.flux[f] = axis_face_flux<R, 0>(a, f);
+    for (int f = f0y + (int)threadIdx.x; f < f1y; f += TB) a.flux[f] = axis_face_flux<R, 1>(a, f);
+    for (int f = f0z + (int)threadIdx.x; f < f1z; f += TB) a.flux[f] = axis_face_flux<R, 2>(a, f);
 }
 
 // Boundary faces (always) and the interior faces of meshes that are not axis
@@ -627,7 +722,18 @@ template <typename R> void launch_fluid_flux_axis_ranges(const FluidArgs<R> &a, 
     else if (tb == 256) k_face_flux<R, 256><<<g, 256, 0, s>>>(a, r);
     else k_face_flux<R, 128><<<g, 128, 0, s>>>(a, r);
 }
+template <typename R> void launch_fluid_flux_tiles(const FluidArgs<R> &a, int tile0, int tile1, cudaStream_t s) {
+    const int g = tile1 - tile0;
+    if (!a.axis_aligned || g <= 0) return;
+    if (a.tb_flux == 64) k_face_flux_tiles<R, 64><<<g, 64, 0, s>>>(a, tile0);
+    else if (a.tb_flux == 256) k_face_flux_tiles<R, 256><<<g, 256, 0, s>>>(a, tile0);
+    else k_face_flux_tiles<R, 128><<<g, 128, 0, s>>>(a, tile0);
+}
 template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s) {
+    if (a.flux_tiles) {
+        launch_fluid_flux_tiles<R>(a, 0, a.n_tiles, s);
+        return;
+    }
     const FaceRanges r = {{0, a.nfx, a.nfx + a.nfy}, {a.nfx, a.nfy, a.ni - a.nfx - a.nfy}};
     launch_fluid_flux_axis_ranges<R>(a, r, s);
 }
@@ -681,6 +787,8 @@ template void launch_fluid_gradients_range<double>(const FluidArgs<double> &, in
 template void launch_fluid_gradients_range<float>(const FluidArgs<float> &, int, int, cudaStream_t);
 template void launch_fluid_flux_axis_ranges<double>(const FluidArgs<double> &, const FaceRanges &, cudaStream_t);
 template void launch_fluid_flux_axis_ranges<float>(const FluidArgs<float> &, const FaceRanges &, cudaStream_t);
+template void launch_fluid_flux_tiles<double>(const FluidArgs<double> &, int, int, cudaStream_t);
+template void launch_fluid_flux_tiles<float>(const FluidArgs<float> &, int, int, cudaStream_t);
 template void launch_fluid_cfl<float>(const FluidArgs<float> &, cudaStream_t);
 
 }  // namespace lbfs

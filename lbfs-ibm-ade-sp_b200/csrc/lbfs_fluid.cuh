@@ -155,6 +155,10 @@ template <typename R> struct FluidArgs {
     const GenFace<R> *gen_face;  // [nb] bc faces, or [nf] when not axis aligned (indexed by face)
     const R *visc_factor;        // [nc]
     Vec4<R> *flux;               // [nf]
+    // tiles of tb_flux cells for the face kernel: [3 (n_tiles + 1)], first face of each axis owned by
+    // a tile (null: faces not ordered by owner, the per-axis face ranges are used)
+    const int *flux_tiles;
+    int n_tiles;
     // K3
     const int *cell_faces;       // [6*nc] +(f+1) owner, -(f+1) neighbour
     const double *cell_volume;   // [nc]

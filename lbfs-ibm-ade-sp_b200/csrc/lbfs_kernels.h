@@ -16,6 +16,9 @@ template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStr
 // K1 over cells [begin, end) and K2 over up to three axis face ranges (the pipelined form)
 template <typename R> void launch_fluid_gradients_range(const FluidArgs<R> &a, int begin, int end, cudaStream_t s);
 template <typename R> void launch_fluid_flux_axis_ranges(const FluidArgs<R> &a, const FaceRanges &r, cudaStream_t s);
+// K2 over the faces owned by tiles [tile0, tile1) of a.flux_tiles (axis-aligned meshes whose faces are
+// ordered by owner within each axis)
+template <typename R> void launch_fluid_flux_tiles(const FluidArgs<R> &a, int tile0, int tile1, cudaStream_t s);
 template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s);
 template <typename R> void launch_fluid_flux_general(const FluidArgs<R> &a, cudaStream_t s);

@@ -49,6 +49,13 @@ struct lbfs_solver {
     int chunk_start[3] = {0, 0, 0}, chunk_count[3] = {0, 0, 0};
     std::vector<int> chunk_cell;
     std::vector<FaceRanges> chunk_faces;
+    // tiles of the face kernel (interior faces ordered by owner within each axis), one table per flux
+    // block size 64 / 128 / 256: tiles_h[b] = first face of each axis owned by tile t (3 ints per
+    // tile, n_tiles + 1 rows), tile_maxnb[b][t] = largest neighbour of the faces of tiles <= t
+    bool tiled = false;
+    std::vector<int> tiles_h[3], tile_maxnb[3];
+    int *d_tiles[3] = {};
+    std::vector<int> chunk_tile;  // K + 1 tile splits of the pipelined K2
     cudaEvent_t ev_chunk[kMaxFluxChunks] = {}, ev_flux = nullptr;
     cudaEvent_t ev_advected = nullptr, ev_sorted = nullptr;
     bool own_stream = true;
@@ -674,28 +681,85 @@ cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
 // non-decreasing neighbours (the generator's order; ensembles keep it): then
 // the faces whose neighbour lies below a split form a prefix of each range,
 // and the faces of chunk c need the gradients of chunks <= c only.
-void plan_chunks(lbfs_solver *s, const int *owner, const int *neighbour, int nfx, int nfy, int nfz) {
+//
+// Tiles of the face kernel need in addition owners that do not decrease within
+// each axis range (the generator's order; ensembles keep it): the faces owned
+// by a tile of cells are then a contiguous range of each axis.
+int plan_chunks(lbfs_solver *s, const int *owner, const int *neighbour, int nfx, int nfy, int nfz) {
     s->chunkable = false;
+    s->tiled = false;
     const int ni = s->ni, nc = s->nc;
-    if (ni == 0 || nc < 2 * kMaxFluxChunks * 256 || !owner) return;
+    if (ni == 0 || !owner) return LBFS_OK;
     const int start[3] = {0, nfx, nfx + nfy}, count[3] = {nfx, nfy, nfz};
+    bool ordered = true, owners_ordered = true;
     for (int ax = 0; ax < 3; ax++)
-        for (int f = start[ax]; f < start[ax] + count[ax]; f++)
-            if (!(owner[f] < neighbour[f]) || (f > start[ax] && neighbour[f] < neighbour[f - 1])) return;
+        for (int f = start[ax]; f < start[ax] + count[ax]; f++) {
+            if (!(owner[f] < neighbour[f]) || (f > start[ax] && neighbour[f] < neighbour[f - 1])) ordered = false;
+            if (f > start[ax] && owner[f] < owner[f - 1]) owners_ordered = false;
+        }
+    if (!ordered) return LBFS_OK;
+    if (owners_ordered) {
+        for (int b = 0; b < 3; b++) {
+            const int T = 64 << b, nt = (nc + T - 1) / T;
+            std::vector<int> &tt = s->tiles_h[b];
+            std::vector<int> &mx = s->tile_maxnb[b];
+            tt.assign(3 * (size_t)(nt + 1), 0);
+            mx.assign(nt, -1);
+            for (int ax = 0; ax < 3; ax++) {
+                const int *ow = owner + start[ax];
+                for (int t = 0; t <= nt; t++)
+                    tt[3 * (size_t)t + ax] =
+                        start[ax] + (int)(std::lower_bound(ow, ow + count[ax], (int)std::min<long long>((long long)t * T, nc)) - ow);
+            }
+            int run = -1;
+            for (int t = 0; t < nt; t++) {
+                for (int ax = 0; ax < 3; ax++) {
+                    const int f1 = tt[3 * (size_t)(t + 1) + ax];
+                    if (f1 > tt[3 * (size_t)t + ax]) run = std::max(run, neighbour[f1 - 1]);
+                }
+                mx[t] = run;
+            }
+            int rc = s->upload(&s->d_tiles[b], tt);
+            if (rc) return rc;
+        }
+        s->tiled = true;
+    }
+    if (nc < 2 * kMaxFluxChunks * 256) return LBFS_OK;
     s->chunkable = true;
     s->chunk_nb.assign(neighbour, neighbour + ni);
     for (int ax = 0; ax < 3; ax++) { s->chunk_start[ax] = start[ax]; s->chunk_count[ax] = count[ax]; }
+    return LBFS_OK;
+}
+
+// Face-kernel tiles of the current flux block size into the kernel arguments.
+template <typename R> void apply_tiles(lbfs_solver *s, FluidArgs<R> &a) {
+    const int b = a.tb_flux == 64 ? 0 : (a.tb_flux == 256 ? 2 : 1);
+    a.flux_tiles = s->tiled ? s->d_tiles[b] : nullptr;
+    a.n_tiles = s->tiled ? (int)s->tile_maxnb[b].size() : 0;
 }
 
 // Cell splits and face ranges for K chunks (chunk_cell has K + 1 entries).
 void set_chunks(lbfs_solver *s, int K) {
     if (!s->chunkable || K < 2) K = 1;
     s->flux_chunks = K;
+    if (s->fp32) apply_tiles<float>(s, s->f32);
+    else apply_tiles<double>(s, s->f64);
+    const int tb = s->fp32 ? s->f32.tb_flux : s->f64.tb_flux;
+    const std::vector<int> &mx = s->tile_maxnb[tb == 64 ? 0 : (tb == 256 ? 2 : 1)];
     // gradients and interior fluxes (K each), boundary fluxes, update; membrane kernels; CFL
     s->launches_per_step = 2 * K + 2 + (s->n_membranes > 0 ? (s->ma.force_cluster > 0 ? 4 : 6) : 0) + (dynamic_dt(s->params) ? 1 : 0);
     s->chunk_cell.assign(K + 1, 0);
     s->chunk_faces.assign(K, FaceRanges{});
     for (int c = 0; c <= K; c++) s->chunk_cell[c] = (int)((long long)s->nc * c / K);
+    // tiles of chunk c: those whose faces' neighbours all lie below the chunk's upper split
+    s->chunk_tile.assign(K + 1, 0);
+    if (s->tiled) {
+        const int nt = (int)mx.size();
+        for (int c = 1; c < K; c++)
+            s->chunk_tile[c] = std::max(s->chunk_tile[c - 1],
+                                        (int)(std::lower_bound(mx.begin(), mx.end(), s->chunk_cell[c]) - mx.begin()));
+        s->chunk_tile[K] = nt;
+    }
     if (K == 1) return;
     int prev[3] = {0, 0, 0};
     for (int c = 0; c < K; c++) {
@@ -732,11 +796,25 @@ struct PhaseMark {
 // the chunks before) are done, so the FP64-heavy fluxes of one chunk run beside
 // the load-latency-bound gradients of the next; the boundary faces (which read
 // ghost gradients) follow every K1, and the handle's stream joins the second.
+//
+// Unpipelined, the interior axis faces still run on the second stream beside
+// the boundary faces (a short kernel of long threads that would otherwise add
+// its whole latency after the axis faces).
 template <typename R> int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n) {
     const int K = a.axis_aligned ? s->flux_chunks : 1;
     if (K <= 1) {
         { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
-        { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
+        {
+            PhaseMark m(s, 2, s->stream);
+            if (a.axis_aligned) {
+                LBFS_CUDA(cudaEventRecord(s->ev_chunk[0], s->stream));
+                LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_chunk[0], 0));
+                launch_fluid_flux_axis<R>(a, s->stream4);
+                LBFS_CUDA(cudaEventRecord(s->ev_flux, s->stream4));
+            }
+            launch_fluid_flux_general<R>(a, s->stream);
+            if (a.axis_aligned) LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_flux, 0));
+        }
         *n += 2;
         return LBFS_OK;
     }
@@ -750,7 +828,8 @@ template <typename R> int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n)
     for (int c = 0; c < K; c++) {
         LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_chunk[c], 0));
         if (c == 0 && s->kernel_events) LBFS_CUDA(record_event(s->ev_phase[2][0], s->stream4));
-        launch_fluid_flux_axis_ranges<R>(a, s->chunk_faces[c], s->stream4);
+        if (a.flux_tiles) launch_fluid_flux_tiles<R>(a, s->chunk_tile[c], s->chunk_tile[c + 1], s->stream4);
+        else launch_fluid_flux_axis_ranges<R>(a, s->chunk_faces[c], s->stream4);
     }
     if (s->kernel_events) {
         LBFS_CUDA(record_event(s->ev_phase[2][1], s->stream4));
@@ -911,8 +990,9 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if (rc) return fail(rc);
     rc = s->fp32 ? setup_time_stepping<float>(s, mesh) : setup_time_stepping<double>(s, mesh);
     if (rc) return fail(rc);
-    if (mesh->axis_aligned)
-        plan_chunks(s, mesh->owner, mesh->neighbour, mesh->n_face_x, mesh->n_face_y, mesh->n_face_z);
+    if (mesh->axis_aligned &&
+        (rc = plan_chunks(s, mesh->owner, mesh->neighbour, mesh->n_face_x, mesh->n_face_y, mesh->n_face_z)))
+        return fail(rc);
     set_chunks(s, 1);
     *out = s;
     return LBFS_OK;
