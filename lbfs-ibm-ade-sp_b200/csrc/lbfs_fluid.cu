@@ -104,6 +104,23 @@ __device__ __forceinline__ R pop_g(const R (&L)[4], R eu, R rho0, R q) {
     else return L[0] + (L[0] + rho0) * X;
 }
 
+// FP32-bulk (deviation) form of pop_g at a reconstructed state written as
+// L = p0 + d, p0 the face-centre state and d the direction's small offset
+// from it.  The population's term 3 rho0 e.p0_u is large (the velocity
+// itself) and the same for every direction, so that summing the populations
+// over directions would cancel it and leave its FP32 rounding in the
+// cross-stream moments; it is left out here, and its moments (rho0 p0_u in
+// the first moment, zero in every other) are added once, exactly, by the
+// caller.  The rest is formed from small terms only:
+//   g~ = rho' (1 + X) + rho0 (3 e.d_u + q (4.5 (e.u)^2 - 1.5 |u|^2)).
+// eu = e.u at L, edu = e.d_u.
+__device__ __forceinline__ float pop_dev(const float (&L)[4], float eu, float edu, float rho0, float q) {
+    const float usq = L[1] * L[1] + L[2] * L[2] + L[3] * L[3];
+    const float Q = q * (4.5f * eu * eu - 1.5f * usq);
+    const float X = 3.0f * eu + Q;
+    return (L[0] + L[0] * X) + rho0 * (3.0f * edu + Q);
+}
+
 // Moments of the reconstructed lattice populations that the interface flux
 // needs: rho = sum f, m_c = sum e_c f, d_c = sum_{e_c != 0} f (= sum e_c e_c f),
 // o_xy, o_xz, o_yz = sum e_c e_m f.  Formed from sums and differences of
@@ -219,6 +236,44 @@ __device__ __forceinline__ void axis_side(const R (&p)[4], const R (&g)[12], R s
     YC = w_corner * (cp + cm);
 }
 
+// The same five directions in the deviation form: the side's offsets from
+// the face centre, d = s (hdp - dt g_A) -+ dt g_B -+ dt g_C (hdp half the
+// owner-neighbour difference of the reconstructed states), and L = p0 + d.
+template <int A>
+__device__ __forceinline__ void axis_side_dev(const float (&p0)[4], const float (&hdp)[4], const float (&g)[12],
+                                              float s, float dt, float rho0, float &S, float &YB, float &YC) {
+    constexpr int B = A == 0 ? 1 : 0, C = A == 2 ? 1 : 2;
+    float ad[4], amb[4], apb[4], cv[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        ad[m] = s * (hdp[m] - dt * g[3 * m + A]);
+        const float b = dt * g[3 * m + B];
+        cv[m] = dt * g[3 * m + C];
+        amb[m] = ad[m] - b;
+        apb[m] = ad[m] + b;
+    }
+    float L[4], d[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) L[m] = p0[m] + ad[m];
+    const float g0 = pop_dev(L, s * L[1 + A], s * ad[1 + A], rho0, 1.0f);
+    float gq[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float eb = (q < 2) ? 1.0f : -1.0f, ec = (q & 1) ? -1.0f : 1.0f;  // (+,+), (+,-), (-,+), (-,-)
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            d[m] = ((q < 2) ? amb[m] : apb[m]) - ec * cv[m];
+            L[m] = p0[m] + d[m];
+        }
+        gq[q] = pop_dev(L, s * L[1 + A] + eb * L[1 + B] + ec * L[1 + C], s * d[1 + A] + eb * d[1 + B] + ec * d[1 + C],
+                        rho0, 1.0f);
+    }
+    const float bp = gq[0] + gq[1], bm = gq[2] + gq[3], cp = gq[0] - gq[1], cm = gq[2] - gq[3];
+    S = (1.0f / 9.0f) * g0 + (1.0f / 72.0f) * (bp + bm);
+    YB = (1.0f / 72.0f) * (bp - bm);
+    YC = (1.0f / 72.0f) * (cp + cm);
+}
+
 // Axis-aligned interior face of axis A (calc_face_flux_x/_y/_z, LBFS.cu:2283-2569):
 // directions with e_A = +1 extrapolate from the owner, -1 from the neighbour,
 // 0 from the face centre with the distance-weighted gradient.
@@ -245,11 +300,40 @@ __device__ __forceinline__ Vec4<R> axis_face_flux(const FluidArgs<R> &a, int f) 
     }
     LatMoments<R> M;
     R Sp, Bp, Cp, Sn, Bn, Cn;
-    axis_side<R, A>(pi, g1, R(1), dt, rho0, Sp, Bp, Cp);
-    axis_side<R, A>(pn, g2, R(-1), dt, rho0, Sn, Bn, Cn);
+    if constexpr (sizeof(R) == 8) {
+        axis_side<R, A>(pi, g1, R(1), dt, rho0, Sp, Bp, Cp);
+        axis_side<R, A>(pn, g2, R(-1), dt, rho0, Sn, Bn, Cn);
+    } else {
+        // half the owner-neighbour difference, from the states' difference (exact for close values)
+        R hdp[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) hdp[m] = ((S1[m] - S2[m]) - (t1 * g1[3 * m + A] - t2 * g2[3 * m + A])) * R(0.5);
+        axis_side_dev<A>(p0, hdp, g1, 1.0f, dt, rho0, Sp, Bp, Cp);
+        axis_side_dev<A>(p0, hdp, g2, -1.0f, dt, rho0, Sn, Bn, Cn);
+    }
     // centre directions (e_A = 0): rest, +-B, +-C, from p0 with gi = wa g1 + wb g2
     R gz0, gbp, gbm, gcp, gcm;
-    {
+    if constexpr (sizeof(R) == 4) {
+        R bv[4], cv[4], L[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            bv[m] = dt * (g1[3 * m + B] * wa + g2[3 * m + B] * wb);
+            cv[m] = dt * (g1[3 * m + C] * wa + g2[3 * m + C] * wb);
+        }
+        gz0 = pop_dev(p0, R(0), R(0), rho0, R(1));
+#pragma unroll
+        for (int m = 0; m < 4; m++) L[m] = p0[m] - bv[m];
+        gbp = pop_dev(L, L[1 + B], -bv[1 + B], rho0, R(1));
+#pragma unroll
+        for (int m = 0; m < 4; m++) L[m] = p0[m] + bv[m];
+        gbm = pop_dev(L, -L[1 + B], -bv[1 + B], rho0, R(1));
+#pragma unroll
+        for (int m = 0; m < 4; m++) L[m] = p0[m] - cv[m];
+        gcp = pop_dev(L, L[1 + C], -cv[1 + C], rho0, R(1));
+#pragma unroll
+        for (int m = 0; m < 4; m++) L[m] = p0[m] + cv[m];
+        gcm = pop_dev(L, -L[1 + C], -cv[1 + C], rho0, R(1));
+    } else {
         R bv[4], cv[4], L[4];
 #pragma unroll
         for (int m = 0; m < 4; m++) {
@@ -281,6 +365,11 @@ __device__ __forceinline__ Vec4<R> axis_face_flux(const FluidArgs<R> &a, int f) 
     M.o[A + B - 1] = Bp - Bn;  // o index of the pair (A, B): xy 0, xz 1, yz 2
     M.o[A + C - 1] = Cp - Cn;
     M.d[B] = M.d[C] = M.o[B + C - 1] = R(0);  // not read by the axis-A flux
+    if constexpr (sizeof(R) == 4) {
+        // first moments of the left-out term 3 rho0 e.p0_u (pop_dev)
+#pragma unroll
+        for (int c = 0; c < 3; c++) M.m[c] = M.m[c] + rho0 * p0[1 + c];
+    }
     const R vf = a.visc_factor[oc.x];
     const R tau = (a.testcase == 8) ? R(0) : (a.visc * vf * R(3) / dt * a.gamma_inv);
     return interface_flux<R>(M, rho0, tau, R(1), geo.area, A, 0, 0, 0);
@@ -375,13 +464,27 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
 #pragma unroll
         for (int t = 0; t < 12; t++) g3[t] = (g1[t] + g2[t]) * R(0.5);
     }
+    // FP32 deviation form: offsets from the face centre (pop_dev); hdp is half
+    // the owner-neighbour difference of the reconstructed states
+    R hdp[4] = {R(0), R(0), R(0), R(0)};
+    if constexpr (sizeof(R) == 4) {
+        if (geo.bc_branch == R(0)) {
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                hdp[m] = ((S1[m] - S2[m]) - ((geo.t1x * g1[3 * m] + geo.t1y * g1[3 * m + 1] + geo.t1z * g1[3 * m + 2]) -
+                                             (geo.t2x * g2[3 * m] + geo.t2y * g2[3 * m + 1] + geo.t2z * g2[3 * m + 2]))) *
+                         R(0.5);
+        }
+    }
     // Upwind selection by the sign of n.e_k with the threshold 0.001 dt
     // (LBFS.cu:351-352 override the sin(pi/14) arguments).  Directions come in
     // opposite pairs (k, k + 1): sum and difference of the pair's populations
     // feed the moments.
     const R thr = R(0.001) * dt;
     const R q = a.recon_q;
-    const R g0 = pop_g<R>(p0, R(0), rho0, q);
+    R g0;
+    if constexpr (sizeof(R) == 4) g0 = pop_dev(p0, R(0), R(0), rho0, q);
+    else g0 = pop_g<R>(p0, R(0), rho0, q);
     R sax[3], dax[3];          // axis pairs (+e_c, -e_c): sum and difference
     R sc, mcor[3], ocor[3];    // corner pairs: sum of sums; sum of e_c x difference; of e_c e_q x sum
 #pragma unroll
@@ -398,28 +501,38 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
         for (int h = 0; h < 2; h++) {
             const int side = h ? side_o : side_k;
             const int sg = h ? -1 : 1;
-            R L[4];
+            R L[4], D[4];
 #pragma unroll
             for (int m = 0; m < 4; m++) {
-                R val = side == 0 ? pi[m] : (side == 1 ? pn[m] : p0[m]);
+                // FP64: the value itself; FP32: its offset from the face centre
+                R val;
+                if constexpr (sizeof(R) == 8) val = side == 0 ? pi[m] : (side == 1 ? pn[m] : p0[m]);
+                else val = side == 0 ? hdp[m] : (side == 1 ? -hdp[m] : R(0));
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
                     if (!ee[d]) continue;
                     const R gd = side == 0 ? g1[3 * m + d] : (side == 1 ? g2[3 * m + d] : g3[3 * m + d]);
                     val = (sg * ee[d] > 0) ? val - gd * dt : val + gd * dt;
                 }
-                L[m] = val;
+                if constexpr (sizeof(R) == 8) L[m] = val;
+                else { D[m] = val; L[m] = p0[m] + val; }
             }
-            R eu = R(0);
+            R eu = R(0), edu = R(0);
             bool first = true;
 #pragma unroll
             for (int d = 0; d < 3; d++) {
                 if (!ee[d]) continue;
-                const R ud = (sg * ee[d] > 0) ? L[1 + d] : -L[1 + d];
+                const bool pos = sg * ee[d] > 0;
+                const R ud = pos ? L[1 + d] : -L[1 + d];
                 eu = first ? ud : eu + ud;
+                if constexpr (sizeof(R) == 4) {
+                    const R dd = pos ? D[1 + d] : -D[1 + d];
+                    edu = first ? dd : edu + dd;
+                }
                 first = false;
             }
-            gp[h] = pop_g<R>(L, eu, rho0, q);
+            if constexpr (sizeof(R) == 4) gp[h] = pop_dev(L, eu, edu, rho0, q);
+            else gp[h] = pop_g<R>(L, eu, rho0, q);
         }
         const R sig = gp[0] + gp[1], del = gp[0] - gp[1];
         if (k < 7) {
@@ -447,6 +560,7 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
         M.m[c] = w_axis * dax[c] + w_corner * mcor[c];
         M.d[c] = w_axis * sax[c] + w_corner * sc;
         M.o[c] = w_corner * ocor[c];
+        if constexpr (sizeof(R) == 4) M.m[c] = M.m[c] + rho0 * p0[1 + c];  // the term pop_dev leaves out
     }
     const R vf = is_bc ? R(1) : a.visc_factor[oc.x];
     const R tau = (a.testcase == 8) ? R(0) : (a.visc * vf * R(3) / dt * a.gamma_inv);

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from conftest import has_gpu
-from helpers import rel_err
+from helpers import FP32_RTOL, rel_err
 
 
 def _small_ensemble(precision):
@@ -174,3 +174,35 @@ def test_checkpoint_rejects_foreign_blob():
     buf = ctypes.create_string_buffer(b"not a checkpoint" * 8)
     # argument checks run before any device work: a null handle is an argument error
     assert _abi.lib().lbfs_checkpoint_load(None, buf, len(buf)) == _abi.LBFS_ERR_ARG
+
+
+@pytest.mark.gpu
+def test_batched_fp32_bulk_within_bound_of_fp64():
+    """The batched workload itself (64 shear channels of 16^3-48^3 cells, 1-8 red cells each, FP32 bulk)
+    against the same ensemble in FP64 after 205 steps.  The velocity field within FP32_RTOL (1e-6):
+    max over cells of |u32 - u64| relative to the largest |u64|.  Each component relative to its own
+    largest magnitude within 5e-6: the cross-stream components are ~50x smaller than the stream
+    velocity, whose FP32 storage (rounding ~6e-11 at |u| ~ 1e-3, renewed every step from the FP64
+    accumulator) seeds noise of that absolute size in every component.  The density deviation from
+    rho0 within 1e-4 of its largest; red-cell nodes within 1e-9."""
+    import dataclasses
+
+    from lbfs_b200 import GpuSolver, _abi, cases
+    ce = cases.ensemble(n_instances=64, precision=_abi.LBFS_FP32_BULK)
+    p64 = dataclasses.replace(ce.params, precision=_abi.LBFS_FP64)
+    a = GpuSolver(ce.mesh, p64, ce.membranes)
+    b = GpuSolver(ce.mesh, ce.params, ce.membranes)
+    for s in (a, b):
+        s.set_state(ce.rho, ce.u, ce.v, ce.w)
+        s.step(205, graph=True)
+    sa, sb = a.state(), b.state()
+    mag = np.sqrt(sa[1] ** 2 + sa[2] ** 2 + sa[3] ** 2)
+    diff = np.sqrt((sb[1] - sa[1]) ** 2 + (sb[2] - sa[2]) ** 2 + (sb[3] - sa[3]) ** 2)
+    assert np.max(diff) / np.max(mag) < FP32_RTOL, np.max(diff) / np.max(mag)
+    errs = {k: rel_err(sb[i], sa[i]) for i, k in ((1, "u"), (2, "v"), (3, "w"))}
+    assert max(errs.values()) < 5e-6, errs
+    assert rel_err(sb[0] - 1.0, sa[0] - 1.0) < 1e-4
+    assert rel_err(b.nodes(), a.nodes()) < 1e-9
+    assert a.status() == 0 and b.status() == 0
+    a.close()
+    b.close()
