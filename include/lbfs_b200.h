@@ -169,12 +169,18 @@ typedef struct lbfs_rbc_desc {
     int32_t pivkin_length, sphere_reference;
     int32_t instance;               /* ensemble instance the membrane lives in (0 without an ensemble) */
     /* lagrangian_object::periodic (its XML key): at t % 5000 == 1, after the
-     * step's fluid update, a membrane whose mean node z exceeds
-     * origin_z + 0.75 Z moves by -0.5 Z in z (gpu_solver::check_periodic_object,
-     * Solver_gpu.cu:1027-1029, 1277-1304; the reference tests the mean of all
-     * objects' nodes together, here each membrane's own). */
+     * step's fluid update, nodes whose mean z exceeds origin_z + 0.75 Z move by
+     * -0.5 Z in z (gpu_solver::check_periodic_object, Solver_gpu.cu:1027-1029,
+     * 1277-1304).  0: never; LBFS_WRAP_OWN: this membrane by the mean of its own
+     * nodes; LBFS_WRAP_ALL (membrane 0 only, as the reference gates on
+     * object_vec[0].periodic): the mean over the nodes of every membrane of the
+     * handle together, and every membrane moves when it exceeds the bound -- the
+     * reference's behaviour with several objects. */
     int32_t periodic;
 } lbfs_rbc_desc;
+
+#define LBFS_WRAP_OWN 1
+#define LBFS_WRAP_ALL 2
 
 typedef struct lbfs_solver lbfs_solver;
 

@@ -84,8 +84,8 @@ struct MembraneArgs {
     int *cell_start;             // [n_membranes + 1] first spread cell of each membrane (prefix over patches)
     unsigned int *sort_ticket;   // membranes whose patch is known in this launch; zero between launches
     int spread_blocks;           // grid of the spread kernel (grid-stride over the tiles)
-    int force_cluster;           // 8 or 16: totals, spring and node forces as one cluster of that many
-                                 // CTAs per membrane (k_mem_forces); 0: three kernels
+    int force_cluster;           // 8 or 16: totals, node sort, spring and node forces as one cluster of that
+                                 // many CTAs per membrane (k_mem_step); 0: four kernels
     int *node_base;              // [3 total_nodes] first IBM stencil cell per axis at the current positions
     double *node_w;              // [12 total_nodes] 1D stencil weights per axis (4 slots) at the current positions
     int *sorted_pos;             // [total_nodes] position of each node in its membrane's sorted order

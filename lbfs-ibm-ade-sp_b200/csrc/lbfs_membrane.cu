@@ -6,6 +6,7 @@
 //   M4 k_mem_sort      (one CTA per membrane, on a side stream)      P5
 //   k_mem_totals       (one CTA per membrane: V, A)                  P1
 //   M5 k_mem_spread    (one warp per patch cell, all membranes)      P6
+//   k_mem_step         (one thread-block cluster per membrane)       P1-P5 in one launch
 //
 //   P0  IBM velocity interpolation at the nodes + explicit node advection
 //       (interpolate_velocities_on_nodes, immersed_boundary_method.cu:14-97;
@@ -574,88 +575,6 @@ __global__ void __launch_bounds__(128) k_mem_nodeforce(MembraneArgs A) {
     A.fz[n] = f[2];
 }
 
-// ---- M2+M3 fused: totals, spring forces, MAD and node forces of a step -------
-// One thread-block cluster of kForceCluster CTAs (8, or 16 where the device
-// allows non-portable cluster sizes) per membrane.  The CTAs
-// split the triangles, then the springs, then the nodes; the membrane-wide
-// sums (volume, area, then MAD) are the CTAs' block sums added in rank order
-// through distributed shared memory, so every CTA holds the same values.  The
-// cluster barriers (release / acquire at cluster scope) also publish the
-// per-spring contributions that the node gather of another CTA reads.  Node
-// forces are written in node order; the spread reads them through the node
-// index of its sorted record, so this kernel does not wait for the sort.
-template <int kForceCluster>
-__global__ void __launch_bounds__(128) k_mem_forces(MembraneArgs A) {
-    namespace cg = cooperative_groups;
-    cg::cluster_group cluster = cg::this_cluster();
-    __shared__ double sh[33];
-    __shared__ double part_va[2], part_mad[1];
-    const int m = blockIdx.y;
-    const int rank = (int)cluster.block_rank();
-    const int nth = kForceCluster * blockDim.x, tid = rank * blockDim.x + threadIdx.x;
-    const MembraneConst mc = A.mc[m];
-    MembraneScalars *ms = A.ms + m;
-    // volume and area (update_spring_network_tet_parameters + total<128>)
-    double pv = 0.0, pa = 0.0;
-    for (int lt = tid; lt < mc.n_tris; lt += nth) {
-        const int t = mc.tri0 + lt;
-        const int na = A.tri[3 * t], nb = A.tri[3 * t + 1], nc = A.tri[3 * t + 2];
-        const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]), c = d3(A.x[nc], A.y[nc], A.z[nc]);
-        const D3 normal = cross(b - a, c - a);
-        pv += dot(normal, tri_centroid(a, b, c)) / 6;
-        pa += sqrt(dot(normal, normal)) * 0.5;
-    }
-    const double bv = block_sum(pv, sh), ba = block_sum(pa, sh);
-    if (threadIdx.x == 0) { part_va[0] = bv; part_va[1] = ba; }
-    const double V0 = ms->V0, A0 = ms->A0, MADp = ms->MAD, MAD0p = ms->MAD0;
-    cluster.sync();
-    double V = 0.0, Ar = 0.0;
-    for (int r = 0; r < kForceCluster; r++) {
-        const double *p = cluster.map_shared_rank(part_va, r);
-        V += p[0];
-        Ar += p[1];
-    }
-    // spring forces (get_spring_forces_atomics) and the MAD terms of the first n_nodes springs
-    const double wr = mc.wlc_ratio;
-    const double sfc = (0.25 * wr * wr / ((wr - 1.0) * (wr - 1.0)) - 0.25 + 1.0 / wr);
-    const double vol_coef = -1 * mc.volume_modulus * (V / V0 - 1.0) / 6.0;
-    const double area_coef = -1 * mc.global_area_modulus * (Ar / A0 - 1.0);
-    const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (MADp - MAD0p) / A0;
-    const MembraneScalars cur = *ms;
-    double pm = 0.0;
-    for (int ls = tid; ls < mc.n_springs; ls += nth) {
-        const int sp = mc.spring0 + ls;
-        spring_forces(A, mc, cur, sp, false, sfc, vol_coef, area_coef, mad_coef);
-        if (ls < mc.n_nodes) pm += A.curv[sp] * (A.area[2 * sp] + A.area[2 * sp + 1]) * 1 / 3;
-    }
-    const double bm = block_sum(pm, sh);
-    if (threadIdx.x == 0) part_mad[0] = bm;
-    cluster.sync();
-    double mad = 0.0;
-    for (int r = 0; r < kForceCluster; r++) mad += *cluster.map_shared_rank(part_mad, r);
-    // node forces: each node's contributions in spring order
-    for (int ln = tid; ln < mc.n_nodes; ln += nth) {
-        const int n = mc.node0 + ln;
-        double f[3] = {0.0, 0.0, 0.0};
-        for (int e = A.inc_start[n]; e < A.inc_start[n + 1]; e++) {
-            const int code = __ldg(A.inc + e);
-            const double *o = A.contrib + 12 * (size_t)(code >> 2) + 3 * (code & 3);
-            f[0] += o[0]; f[1] += o[1]; f[2] += o[2];
-        }
-        A.fx[n] = f[0];
-        A.fy[n] = f[1];
-        A.fz[n] = f[2];
-    }
-    if (rank == 0 && threadIdx.x == 0) {
-        ms->Vc = V;
-        ms->Ac = Ar;
-        ms->V = V;
-        ms->A = Ar;
-        ms->MAD = mad / Ar;
-    }
-    cluster.sync();  // no CTA leaves while another may still read its shared memory
-}
-
 // ---- M4: node bounds, nodes sorted by stencil base cell, spread records -----
 // One CTA per membrane; needs only the advected positions, so it runs beside
 // M2.  Finds the patch (bounding box of the stencils), sorts (bin, node) keys
@@ -679,21 +598,24 @@ __device__ __forceinline__ void write_spread_records(const MembraneArgs &A, cons
     }
 }
 
-__global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
-    extern __shared__ unsigned long long skeys[];  // 2 int arrays of sort_capacity: bins, sorted list
+// Node bounds of a membrane for the patch and the sort: per thread over
+// nodes ln = first, first + stride, ... (min of positions, minus max of
+// positions, min and minus max of the first stencil cells), the range flag,
+// and whether every first cell is sane; then reduced over the CTA
+// (minima are exact, so any order gives the same result).  out[12] valid in
+// every thread on return.
+__device__ void node_bounds(const MembraneArgs &A, const MembraneConst &mc, int first, int stride, double *out,
+                            unsigned int *flag_out, int *sane_out) {
     __shared__ double shv[kMembraneThreads / 32][12];
-    __shared__ double red[12];
-    __shared__ bool last_sorted;
-    const int m = blockIdx.x;
-    const MembraneConst mc = A.mc[m];
-    MembraneScalars *ms = A.ms + m;
+    __shared__ unsigned int sflag;
+    __shared__ int ssane;
     const int S = stencil_width(A.ibm_stencil);
     const int gn[3] = {mc.gnx, mc.gny, mc.gnz};
     double v[12];
-    for (int c = 0; c < 3; c++) { v[c] = 1e300; v[3 + c] = 1e300; v[6 + c] = 1e300; v[9 + c] = 1e300; }
+    for (int c = 0; c < 12; c++) v[c] = 1e300;
     unsigned int range_flag = 0;
     bool base_range = true;
-    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
+    for (int ln = first; ln < mc.n_nodes; ln += stride) {
         const int n = mc.node0 + ln;
         const double p[3] = {A.x[n], A.y[n], A.z[n]};
         const int b[3] = {A.node_base[3 * (size_t)n], A.node_base[3 * (size_t)n + 1], A.node_base[3 * (size_t)n + 2]};
@@ -706,6 +628,7 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
             if (b[c] < -(1 << 19) || b[c] > (1 << 19)) base_range = false;
         }
     }
+    if (threadIdx.x == 0) { sflag = 0u; ssane = 1; }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < 12; q++) {
@@ -714,12 +637,30 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         if (lane == 0) shv[warp][q] = x;
     }
     __syncthreads();
+    if (range_flag) atomicOr(&sflag, range_flag);
+    if (!base_range) ssane = 0;
     if (threadIdx.x < 12) {
         double x = shv[0][threadIdx.x];
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) x = fmin(x, shv[w][threadIdx.x]);
-        red[threadIdx.x] = x;
+        shv[0][threadIdx.x] = x;
     }
     __syncthreads();
+    for (int q = 0; q < 12; q++) out[q] = shv[0][q];
+    *flag_out = sflag;
+    *sane_out = ssane;
+    __syncthreads();
+}
+
+// Patch of a membrane from its node bounds red[12], the prefix of patch
+// cells over the membranes (by the last of the n_sorters CTAs to get here),
+// and the counting sort of its nodes by stencil bin with the spread records;
+// one CTA.  `skeys` is the dynamic shared memory of sort_smem_bytes.
+__device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool bases_sane, unsigned int range_flag,
+                           int n_sorters, unsigned long long *skeys) {
+    __shared__ bool last_sorted;
+    const MembraneConst mc = A.mc[m];
+    MembraneScalars *ms = A.ms + m;
+    const int S = stencil_width(A.ibm_stencil);
     int plo[3], bdim[3], pdim[3];
     for (int c = 0; c < 3; c++) {
         plo[c] = (int)red[6 + c];
@@ -727,10 +668,9 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         pdim[c] = bdim[c] + S - 1;
     }
     const long long pcells = (long long)pdim[0] * pdim[1] * pdim[2];
-    const bool bases_sane = __syncthreads_and(base_range) != 0;
     const bool overflow = pcells > mc.patch_bound || mc.n_nodes == 0 || !bases_sane;
-    if (range_flag) atomicOr(A.flags, range_flag);
     if (threadIdx.x == 0) {
+        if (range_flag) atomicOr(A.flags, range_flag);
         for (int c = 0; c < 3; c++) {
             ms->bbox_lo[c] = red[c];
             ms->bbox_hi[c] = -red[3 + c];
@@ -740,14 +680,14 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
         ms->patch_cells = overflow ? 0 : (int)pcells;
         if (overflow) atomicOr(A.flags, LBFS_FLAG_IBM_RANGE);
         __threadfence();
-        last_sorted = atomicAdd(A.sort_ticket, 1u) == gridDim.x - 1;
+        last_sorted = atomicAdd(A.sort_ticket, 1u) == (unsigned)(n_sorters - 1);
     }
     __syncthreads();
     if (last_sorted) {
         // every patch is known: prefix of patch cells over the membranes
         __threadfence();
         __shared__ int scan[kMembraneThreads];
-        const int M = gridDim.x;
+        const int M = n_sorters;
         const int per = (M + blockDim.x - 1) / blockDim.x;
         const int m0 = min(M, (int)threadIdx.x * per), m1 = min(M, m0 + per);
         int local = 0;
@@ -779,96 +719,47 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     int *cursor = A.bin_cursor + (size_t)ms->patch_off + m;
     int *bins = reinterpret_cast<int *>(skeys);
     int *list = bins + A.sort_capacity;
-    if (nbins + 1 <= kSortBinsSmem) {
-        // the same counting sort with counts and cursors in shared memory
-        int *cnt = list + A.sort_capacity;
-        for (int b = threadIdx.x; b <= nbins; b += blockDim.x) cnt[b] = 0;
-        __syncthreads();
-        for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
-            const int *bb = A.node_base + 3 * (size_t)(mc.node0 + ln);
-            const int bin = (bb[0] - plo[0]) + bdim[0] * ((bb[1] - plo[1]) + bdim[1] * (bb[2] - plo[2]));
-            bins[ln] = bin;
-            atomicAdd(cnt + bin, 1);
-        }
-        __syncthreads();
-        {
-            __shared__ int cscan[kMembraneThreads];
-            const int count = nbins + 1;
-            const int per = (count + blockDim.x - 1) / blockDim.x;
-            const int b0 = min(count, (int)threadIdx.x * per), b1 = min(count, b0 + per);
-            int local = 0;
-            for (int b = b0; b < b1; b++) local += cnt[b];
-            cscan[threadIdx.x] = local;
-            __syncthreads();
-            for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-                const int x = threadIdx.x >= (unsigned)o ? cscan[threadIdx.x - o] : 0;
-                __syncthreads();
-                cscan[threadIdx.x] += x;
-                __syncthreads();
-            }
-            int run = cscan[threadIdx.x] - local;
-            for (int b = b0; b < b1; b++) {
-                const int c = cnt[b];
-                bin_start[b] = run;  // the spread's bin table
-                cnt[b] = run;        // cursor
-                run += c;
-            }
-        }
-        __syncthreads();
-        for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) list[atomicAdd(cnt + bins[ln], 1)] = ln;
-        __syncthreads();
-        // after placement cnt[b] is the end of bin b, i.e. the start of bin b + 1
-        for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
-            const int lo = b == 0 ? 0 : cnt[b - 1], hi = cnt[b];
-            for (int i = lo + 1; i < hi; i++) {
-                const int v = list[i];
-                int j = i - 1;
-                while (j >= lo && list[j] > v) {
-                    list[j + 1] = list[j];
-                    j--;
-                }
-                list[j + 1] = v;
-            }
-        }
-        __syncthreads();
-        write_spread_records(A, mc, list);
-        return;
-    }
-    for (int b = threadIdx.x; b <= nbins; b += blockDim.x) bin_start[b] = 0;
+    const bool in_smem = nbins + 1 <= kSortBinsSmem;
+    // counts and cursors in shared memory when the patch's bins fit, else in global memory
+    int *cnt = in_smem ? list + A.sort_capacity : bin_start;
+    for (int b = threadIdx.x; b <= nbins; b += blockDim.x) cnt[b] = 0;
     __syncthreads();
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
         const int *bb = A.node_base + 3 * (size_t)(mc.node0 + ln);
         const int bin = (bb[0] - plo[0]) + bdim[0] * ((bb[1] - plo[1]) + bdim[1] * (bb[2] - plo[2]));
         bins[ln] = bin;
-        atomicAdd(bin_start + bin, 1);
+        atomicAdd(cnt + bin, 1);
     }
     __syncthreads();
     {
-        __shared__ int bscan[kMembraneThreads];
+        __shared__ int cscan[kMembraneThreads];
         const int count = nbins + 1;
         const int per = (count + blockDim.x - 1) / blockDim.x;
         const int b0 = min(count, (int)threadIdx.x * per), b1 = min(count, b0 + per);
         int local = 0;
-        for (int b = b0; b < b1; b++) local += bin_start[b];
-        bscan[threadIdx.x] = local;
+        for (int b = b0; b < b1; b++) local += cnt[b];
+        cscan[threadIdx.x] = local;
         __syncthreads();
         for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-            const int x = threadIdx.x >= (unsigned)o ? bscan[threadIdx.x - o] : 0;
+            const int x = threadIdx.x >= (unsigned)o ? cscan[threadIdx.x - o] : 0;
             __syncthreads();
-            bscan[threadIdx.x] += x;
+            cscan[threadIdx.x] += x;
             __syncthreads();
         }
-        int run = bscan[threadIdx.x] - local;
+        int run = cscan[threadIdx.x] - local;
+        int *cur = in_smem ? cnt : cursor;
         for (int b = b0; b < b1; b++) {
-            const int c = bin_start[b];
-            bin_start[b] = run;
-            cursor[b] = run;
+            const int c = cnt[b];
+            bin_start[b] = run;  // the spread's bin table
+            cur[b] = run;        // placement cursor
             run += c;
         }
     }
     __syncthreads();
-    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) list[atomicAdd(cursor + bins[ln], 1)] = ln;
+    int *cur = in_smem ? cnt : cursor;
+    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) list[atomicAdd(cur + bins[ln], 1)] = ln;
     __syncthreads();
+    // each bin [bin_start[b], bin_start[b + 1]) in node-index order
     for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
         const int lo = bin_start[b], hi = bin_start[b + 1];
         for (int i = lo + 1; i < hi; i++) {
@@ -883,6 +774,126 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
     }
     __syncthreads();
     write_spread_records(A, mc, list);
+}
+
+__global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
+    extern __shared__ unsigned long long skeys[];  // 2 int arrays of sort_capacity: bins, sorted list
+    const int m = blockIdx.x;
+    double red[12];
+    unsigned int flag;
+    int sane;
+    node_bounds(A, A.mc[m], threadIdx.x, blockDim.x, red, &flag, &sane);
+    sort_patch(A, m, red, sane != 0, flag, gridDim.x, skeys);
+}
+
+// ---- the membrane step as one thread-block cluster per membrane -------------
+// Totals V, A and the node bounds (all CTAs, summed in rank order through
+// distributed shared memory), then the node sort and spread records (CTA rank
+// 0) beside the spring forces (ranks 1 ..), the MAD sum, and the node forces
+// (all CTAs).  Replaces k_mem_totals, k_mem_springs, k_mem_nodeforce and
+// k_mem_sort with one launch; the cluster barriers (release / acquire at
+// cluster scope) publish the per-spring contributions and the sorted records
+// between the phases.  Deterministic: every sum has a fixed order.
+constexpr int kStepThreads = 256;
+template <int CL>
+__global__ void __launch_bounds__(kStepThreads) k_mem_step(MembraneArgs A) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ unsigned long long sdyn[];  // the node sort's arrays (CTA rank 0)
+    __shared__ double sh[33];
+    __shared__ double part_va[2], part_mad[1], part_b[12];
+    __shared__ unsigned int part_flag;
+    __shared__ int part_sane;
+    const int m = blockIdx.y;
+    const int rank = (int)cluster.block_rank();
+    const int nth = CL * blockDim.x, tid = rank * blockDim.x + threadIdx.x;
+    const MembraneConst mc = A.mc[m];
+    MembraneScalars *ms = A.ms + m;
+    // volume and area (update_spring_network_tet_parameters + total<128>)
+    double pv = 0.0, pa = 0.0;
+    for (int lt = tid; lt < mc.n_tris; lt += nth) {
+        const int t = mc.tri0 + lt;
+        const int na = A.tri[3 * t], nb = A.tri[3 * t + 1], nc = A.tri[3 * t + 2];
+        const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]), c = d3(A.x[nc], A.y[nc], A.z[nc]);
+        const D3 normal = cross(b - a, c - a);
+        pv += dot(normal, tri_centroid(a, b, c)) / 6;
+        pa += sqrt(dot(normal, normal)) * 0.5;
+    }
+    const double bv = block_sum(pv, sh), ba = block_sum(pa, sh);
+    double bnd[12];
+    unsigned int bflag;
+    int bsane;
+    node_bounds(A, mc, tid, nth, bnd, &bflag, &bsane);
+    if (threadIdx.x == 0) {
+        part_va[0] = bv;
+        part_va[1] = ba;
+        for (int q = 0; q < 12; q++) part_b[q] = bnd[q];
+        part_flag = bflag;
+        part_sane = bsane;
+    }
+    const double V0 = ms->V0, A0 = ms->A0, MADp = ms->MAD, MAD0p = ms->MAD0;
+    cluster.sync();
+    double V = 0.0, Ar = 0.0;
+    for (int r = 0; r < CL; r++) {
+        const double *p = cluster.map_shared_rank(part_va, r);
+        V += p[0];
+        Ar += p[1];
+    }
+    double pm = 0.0;
+    if (rank == 0) {
+        // patch and node sort: the cluster's bounds (minima: any order)
+        double red[12];
+        unsigned int flag = 0;
+        int sane = 1;
+        for (int q = 0; q < 12; q++) red[q] = 1e300;
+        for (int r = 0; r < CL; r++) {
+            const double *p = cluster.map_shared_rank(part_b, r);
+            for (int q = 0; q < 12; q++) red[q] = fmin(red[q], p[q]);
+            flag |= *cluster.map_shared_rank(&part_flag, r);
+            sane &= *cluster.map_shared_rank(&part_sane, r);
+        }
+        sort_patch(A, m, red, sane != 0, flag, gridDim.y, sdyn);
+    } else {
+        // spring forces (get_spring_forces_atomics) and the MAD terms of the first n_nodes springs
+        const double wr = mc.wlc_ratio;
+        const double sfc = (0.25 * wr * wr / ((wr - 1.0) * (wr - 1.0)) - 0.25 + 1.0 / wr);
+        const double vol_coef = -1 * mc.volume_modulus * (V / V0 - 1.0) / 6.0;
+        const double area_coef = -1 * mc.global_area_modulus * (Ar / A0 - 1.0);
+        const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (MADp - MAD0p) / A0;
+        const MembraneScalars cur = *ms;
+        const int ns = (CL - 1) * blockDim.x;
+        for (int ls = tid - (int)blockDim.x; ls < mc.n_springs; ls += ns) {
+            const int sp = mc.spring0 + ls;
+            spring_forces(A, mc, cur, sp, false, sfc, vol_coef, area_coef, mad_coef);
+            if (ls < mc.n_nodes) pm += A.curv[sp] * (A.area[2 * sp] + A.area[2 * sp + 1]) * 1 / 3;
+        }
+    }
+    const double bm = block_sum(pm, sh);
+    if (threadIdx.x == 0) part_mad[0] = bm;
+    cluster.sync();
+    double mad = 0.0;
+    for (int r = 0; r < CL; r++) mad += *cluster.map_shared_rank(part_mad, r);
+    // node forces: each node's contributions in spring order
+    for (int ln = tid; ln < mc.n_nodes; ln += nth) {
+        const int n = mc.node0 + ln;
+        double f[3] = {0.0, 0.0, 0.0};
+        for (int e = A.inc_start[n]; e < A.inc_start[n + 1]; e++) {
+            const int code = __ldg(A.inc + e);
+            const double *o = A.contrib + 12 * (size_t)(code >> 2) + 3 * (code & 3);
+            f[0] += o[0]; f[1] += o[1]; f[2] += o[2];
+        }
+        A.fx[n] = f[0];
+        A.fy[n] = f[1];
+        A.fz[n] = f[2];
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+        ms->Vc = V;
+        ms->Ac = Ar;
+        ms->V = V;
+        ms->A = Ar;
+        ms->MAD = mad / Ar;
+    }
+    cluster.sync();  // no CTA leaves while another may still read its shared memory
 }
 
 // ---- M5: spread as a per-cell reduction over the sorted nodes -------------
@@ -1017,7 +1028,9 @@ __global__ void __launch_bounds__(kTotalsThreads) k_mem_energies(MembraneArgs A,
 }
 
 // ---- periodic object (gpu_solver::check_periodic_object, Solver_gpu.cu:1277-1304) ----
-// One CTA of 128 threads per membrane flagged periodic.  The mean z of its
+// One CTA of 128 threads per membrane flagged periodic (LBFS_WRAP_OWN), or
+// one CTA for all membranes together (LBFS_WRAP_ALL on membrane 0: the
+// reference's object_z array holds every object's nodes).  The mean z of the
 // nodes is summed as total<128> does (common_kernels.hpp:71-94: every 256
 // consecutive nodes tree-summed, stride 128 down to 1) with the chunk sums
 // added in order from 0, as the host adds the block partials; a mean above
@@ -1028,12 +1041,15 @@ __global__ void __launch_bounds__(128) k_mem_wrap(MembraneArgs A) {
     const int m = blockIdx.x;
     const MembraneConst &mc = A.mc[m];
     if (!mc.periodic) return;
+    const bool all = A.mc[0].periodic == LBFS_WRAP_ALL;
+    if (all && m > 0) return;  // membrane 0's CTA moves them all
+    const int n_nodes = all ? A.total_nodes : mc.n_nodes;
     const int t = threadIdx.x;
-    const double *z = A.z + mc.node0;
+    double *z = A.z + (all ? 0 : mc.node0);
     double sum = 0.0;
-    for (int s0 = 0; s0 < mc.n_nodes; s0 += 256) {
-        part[t] = s0 + t < mc.n_nodes ? z[s0 + t] : 0.0;
-        part[128 + t] = s0 + 128 + t < mc.n_nodes ? z[s0 + 128 + t] : 0.0;
+    for (int s0 = 0; s0 < n_nodes; s0 += 256) {
+        part[t] = s0 + t < n_nodes ? z[s0 + t] : 0.0;
+        part[128 + t] = s0 + 128 + t < n_nodes ? z[s0 + 128 + t] : 0.0;
         for (int stride = 128; stride >= 1; stride >>= 1) {
             __syncthreads();
             if (t < stride) part[t] += part[t + stride];
@@ -1042,11 +1058,11 @@ __global__ void __launch_bounds__(128) k_mem_wrap(MembraneArgs A) {
         if (t == 0) sum = sum + part[0];
         __syncthreads();
     }
-    if (t == 0) shift = sum / mc.n_nodes > mc.domain_z0 + 0.75 * mc.domain_Z;
+    if (t == 0) shift = sum / n_nodes > mc.domain_z0 + 0.75 * mc.domain_Z;
     __syncthreads();
     if (!shift) return;
     const double dz = -0.5 * mc.domain_Z;
-    for (int n = t; n < mc.n_nodes; n += blockDim.x) A.z[mc.node0 + n] = A.z[mc.node0 + n] + dz;
+    for (int n = t; n < n_nodes; n += blockDim.x) z[n] = z[n] + dz;
 }
 
 // ---- interior viscosity (update_interior_viscosities_plucker, immersed_boundary_method.cu:389-527) ----
@@ -1209,7 +1225,9 @@ __global__ void k_interior_viscosity(ViscArgs a) {
 void membrane_prepare(int sort_capacity) {
     const size_t smem = sort_smem_bytes(sort_capacity);
     cudaFuncSetAttribute(k_mem_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_mem_forces<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(k_mem_step<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_mem_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_mem_step<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 
 namespace {
@@ -1259,6 +1277,15 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     const int blocks = (a.total_nodes * 32 + 255) / 256;
     if (a.state_is_float) launch_hi(k_mem_advect<float>, dim3(blocks), dim3(256), 0, s, a);
     else launch_hi(k_mem_advect<double>, dim3(blocks), dim3(256), 0, s, a);
+    const dim3 spread_grid(a.spread_blocks);
+    if (a.force_cluster == 8 || a.force_cluster == 16) {
+        // totals, sort, spring and node forces as one cluster per membrane, then the spread
+        if (a.force_cluster == 16) launch_hi(k_mem_step<16>, dim3(16, a.n_membranes), dim3(kStepThreads), smem, s, a, 16);
+        else launch_hi(k_mem_step<8>, dim3(8, a.n_membranes), dim3(kStepThreads), smem, s, a, 8);
+        if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, spread_grid, dim3(256), 0, s, a);
+        else launch_hi(k_mem_spread<2>, spread_grid, dim3(256), 0, s, a);
+        return 3;
+    }
     // the node sort needs only the advected positions: side stream
     const bool side = s_side != nullptr && ev_advected != nullptr && ev_sorted != nullptr;
     if (side) {
@@ -1267,22 +1294,15 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     }
     launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, side ? s_side : s, a);
     if (side) cudaEventRecord(ev_sorted, s_side);
-    int n = 4;
-    if (a.force_cluster == 16) {
-        launch_hi(k_mem_forces<16>, dim3(16, a.n_membranes), dim3(128), 0, s, a, 16);
-    } else if (a.force_cluster == 8) {
-        launch_hi(k_mem_forces<8>, dim3(8, a.n_membranes), dim3(128), 0, s, a, 8);
-    } else {  // separate kernels: more CTAs for the springs, two more launches
-        launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a);
-        launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
-        launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
-        n = 6;
-    }
+    // separate kernels for the totals, the spring forces and the node forces
+    launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a);
+    launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
+    launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
+    const int n = 6;
     // the spread reads the sorted records and the node forces
     if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
-    const dim3 grid(a.spread_blocks);
-    if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
-    else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a);
+    if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, spread_grid, dim3(256), 0, s, a);
+    else launch_hi(k_mem_spread<2>, spread_grid, dim3(256), 0, s, a);
     return n;
 }
 

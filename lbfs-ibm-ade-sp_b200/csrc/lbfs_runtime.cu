@@ -525,10 +525,12 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         c.cell0 = g.cell0; c.gnx = g.nx; c.gny = g.ny; c.gnz = g.nz;
         for (int q = 0; q < 3; q++) c.gorigin[q] = gd.origin[q];
         c.gdx = gd.delta_x; c.gdh = gd.delta_h;
-        c.periodic = d.periodic ? 1 : 0;
+        if (d.periodic < 0 || d.periodic > LBFS_WRAP_ALL || (d.periodic == LBFS_WRAP_ALL && r > 0 && rbc[0].periodic != LBFS_WRAP_ALL))
+            return set_error(LBFS_ERR_ARG, "periodic: 0, LBFS_WRAP_OWN, or LBFS_WRAP_ALL on membrane 0 (it decides for all)");
+        c.periodic = rbc[0].periodic == LBFS_WRAP_ALL ? LBFS_WRAP_ALL : d.periodic;
         c.domain_z0 = gd.origin[2];
         c.domain_Z = gd.length[2];
-        if (d.periodic) s->wrap_membranes = true;
+        if (c.periodic) s->wrap_membranes = true;
         {
             // a patch of in-range stencils lies inside the instance's grid
             const int S = stencil_width(p.ibm_stencil);
@@ -747,7 +749,7 @@ void set_chunks(lbfs_solver *s, int K) {
     const int tb = s->fp32 ? s->f32.tb_flux : s->f64.tb_flux;
     const std::vector<int> &mx = s->tile_maxnb[tb == 64 ? 0 : (tb == 256 ? 2 : 1)];
     // gradients and interior fluxes (K each), boundary fluxes, update; membrane kernels; CFL
-    s->launches_per_step = 2 * K + 2 + (s->n_membranes > 0 ? (s->ma.force_cluster > 0 ? 4 : 6) : 0) + (dynamic_dt(s->params) ? 1 : 0);
+    s->launches_per_step = 2 * K + 2 + (s->n_membranes > 0 ? (s->ma.force_cluster > 0 ? 3 : 6) : 0) + (dynamic_dt(s->params) ? 1 : 0);
     s->chunk_cell.assign(K + 1, 0);
     s->chunk_faces.assign(K, FaceRanges{});
     for (int c = 0; c <= K; c++) s->chunk_cell[c] = (int)((long long)s->nc * c / K);

@@ -163,7 +163,9 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
             d.curvature_ratio = o.curvature_ratio; d.volume_ratio = o.volume_ratio;
             d.internal_viscosity_ratio = o.internal_viscosity_ratio; d.reference_length = o.reference_length;
             d.pivkin_length = o.pivkin_length; d.sphere_reference = o.sphere_reference;
-            d.periodic = object_vec[0].periodic;  // the reference's gate of check_periodic_object (Solver_gpu.cu:1027)
+            // the reference's gate of check_periodic_object (Solver_gpu.cu:1027): object 0's flag, one mean
+            // over every object's nodes, all objects moved together
+            d.periodic = object_vec[0].periodic ? LBFS_WRAP_ALL : 0;
             rbc.push_back(d);
         }
         for (size_t k = 0; k < rbc.size(); k++) {
@@ -179,7 +181,9 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
     lbfs_check(lbfs_set_state(s, rho.data(), u.data(), v.data(), w.data()), "lbfs_set_state");
 
     const int timesteps = (int)std::ceil(globals.simulation_length);
-    const int chunk = globals.output_step > 0 ? globals.output_step : 1;
+    // the reference tests convergence on the residuals after every step (Solver_gpu.cu:1206); with a
+    // tolerance the steps go one at a time, without one in chunks of output_step
+    const int chunk = globals.tolerance > 0 ? 1 : (globals.output_step > 0 ? globals.output_step : 1);
     for (int t = 0; t < timesteps; t += chunk) {
         const int n = std::min(chunk, timesteps - t);
         lbfs_check(lbfs_step_graph(s, n), "lbfs_step_graph");

@@ -48,6 +48,8 @@ LBFS_DT_LOCAL = 1
 LBFS_DT_CONSTANT = 2
 LBFS_DT_MIN = 3
 LBFS_DT_TALTS = 4
+LBFS_WRAP_OWN = 1
+LBFS_WRAP_ALL = 2
 
 LBFS_NOALLOC_MAX_BLOCKS = 65536
 LBFS_NOALLOC_MAX_CELLS = LBFS_NOALLOC_MAX_BLOCKS * 256

@@ -114,7 +114,7 @@ class Membrane:
     pivkin_length: bool = False
     sphere_reference: bool = True
     instance: int = 0  # ensemble instance the membrane lives in
-    periodic: bool = False  # lagrangian_object::periodic: the z wrap every 5000 steps
+    periodic: int = 0  # lagrangian_object::periodic, the z wrap every 5000 steps: 0, LBFS_WRAP_OWN or LBFS_WRAP_ALL
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -136,7 +136,7 @@ class Membrane:
         d.pivkin_length = int(bool(self.pivkin_length))
         d.sphere_reference = int(bool(self.sphere_reference))
         d.instance = int(self.instance)
-        d.periodic = int(bool(self.periodic))
+        d.periodic = int(self.periodic)
         return d
 
 

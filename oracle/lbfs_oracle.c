@@ -837,21 +837,30 @@ void oracle_get_state(const oracle_case *o, double *rho, double *u, double *v, d
  * periodic membrane: the mean node z as total<128> sums it (256 nodes per
  * block tree-summed, stride 128 down to 1; the block sums added in order
  * from 0), and a move by -0.5 Z when it exceeds origin_z + 0.75 Z. */
+static void wrap_nodes(double *z, int n_nodes, double z0, double Z) {
+    double sum = 0.0;
+    for (int s0 = 0; s0 < n_nodes; s0 += 256) {
+        double part[256];
+        for (int t = 0; t < 256; t++) part[t] = s0 + t < n_nodes ? z[s0 + t] : 0.0;
+        for (int stride = 128; stride >= 1; stride >>= 1)
+            for (int t = 0; t < stride; t++) part[t] += part[t + stride];
+        sum = sum + part[0];
+    }
+    if (sum / n_nodes > z0 + 0.75 * Z)
+        for (int n = 0; n < n_nodes; n++) z[n] = z[n] + -0.5 * Z;
+}
+
+/* LBFS_WRAP_ALL on membrane 0: as the reference (object_z holds every
+ * object's nodes), one mean over all membranes' nodes and one move of all. */
 static void periodic_wrap(oracle_case *o) {
     const double z0 = o->m.origin[2], Z = o->m.length[2];
+    if (o->n_mem > 0 && o->mem[0].d.periodic == LBFS_WRAP_ALL) {
+        wrap_nodes(o->z, o->N, z0, Z);
+        return;
+    }
     for (int r = 0; r < o->n_mem; r++) {
         const omem *M = o->mem + r;
-        if (!M->d.periodic) continue;
-        double *z = o->z + M->node0, sum = 0.0;
-        for (int s0 = 0; s0 < M->n_nodes; s0 += 256) {
-            double part[256];
-            for (int t = 0; t < 256; t++) part[t] = s0 + t < M->n_nodes ? z[s0 + t] : 0.0;
-            for (int stride = 128; stride >= 1; stride >>= 1)
-                for (int t = 0; t < stride; t++) part[t] += part[t + stride];
-            sum = sum + part[0];
-        }
-        if (sum / M->n_nodes > z0 + 0.75 * Z)
-            for (int n = 0; n < M->n_nodes; n++) z[n] = z[n] + -0.5 * Z;
+        if (M->d.periodic) wrap_nodes(o->z + M->node0, M->n_nodes, z0, Z);
     }
 }
 

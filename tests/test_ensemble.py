@@ -54,12 +54,14 @@ def test_concatenated_layout():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
-def test_ensemble_matches_separate_handles(precision):
+@pytest.mark.parametrize("precision,membrane_cluster", [(0, 0), (1, 0), (0, 8), (1, 16)],
+                         ids=["fp64", "fp32", "fp64_cluster8", "fp32_cluster16"])
+def test_ensemble_matches_separate_handles(precision, membrane_cluster):
     from lbfs_b200 import GpuSolver
     c = _small_ensemble(precision)
     steps = 12  # crosses the interior-viscosity update at t = 1
     with GpuSolver(c.mesh, c.params, c.membranes) as s:
+        s.set_launch_shape(membrane_cluster=membrane_cluster)
         s.set_state(c.rho, c.u, c.v, c.w)
         s.step(steps, graph=True)
         state = s.state()
@@ -69,6 +71,7 @@ def test_ensemble_matches_separate_handles(precision):
     node0 = 0
     for k, m in enumerate(c.info["members"]):
         with GpuSolver(m.mesh, m.params, m.membranes) as t:
+            t.set_launch_shape(membrane_cluster=membrane_cluster)
             t.set_state(m.rho, m.u, m.v, m.w)
             t.step(steps, graph=True)
             own = t.state()
@@ -90,7 +93,7 @@ def test_launch_shapes_do_not_change_fields():
               dict(gradient_threads=512, flux_threads=256, general_flux_threads=64, update_threads=128,
                    update_blocks=2368, spread_blocks=2368),
               dict(flux_chunks=2), dict(flux_chunks=8, gradient_threads=128),
-              dict(membrane_cluster=0), dict(membrane_cluster=16, flux_chunks=4)]
+              dict(membrane_cluster=0), dict(membrane_cluster=8), dict(membrane_cluster=16, flux_chunks=4)]
     out = []
     for sh in shapes:
         with GpuSolver(c.mesh, c.params, c.membranes) as s:

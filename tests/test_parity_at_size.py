@@ -141,9 +141,13 @@ def test_shear_rbc64_hat2_vs_reference():
 
 
 @pytest.mark.gpu
-def test_shear_rbc64_peskin4_vs_oracle():
+@pytest.mark.parametrize("membrane_cluster", [0, 8, 16])
+def test_shear_rbc64_peskin4_vs_oracle(membrane_cluster):
+    """membrane_cluster 0: the membrane step as separate kernels; 8 / 16: as one thread-block
+    cluster of that many CTAs per membrane (k_mem_step)."""
     c = cases.shear_rbc(n=64)  # the benchmark workload: 4-point Peskin delta
     s, o = _gpu(c), _oracle(c)
+    s.set_launch_shape(membrane_cluster=membrane_cluster)
     s.step(1)
     o.step(1)
     _check({name: (s.field(w), o.field(w)) for name, w in (

@@ -129,3 +129,74 @@ def test_oracle_periodic_ghosts_take_the_partner_values():
     np.testing.assert_array_equal(grad[m.n_cells + per], grad[pn])
     o.close()
     o2.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["own", "all"])
+def test_periodic_objects_wrap_modes_vs_oracle(mode):
+    """Two periodic red cells, one high in z (0.8 Z) and one lower (0.4 Z): with LBFS_WRAP_OWN only the
+    high one moves down by Z / 2 at t = 1 (its own mean is above 0.75 Z); with LBFS_WRAP_ALL on
+    membrane 0 -- the reference's check_periodic_object over all objects' nodes -- the joint mean is
+    below the bound and neither moves.  CUDA path and oracle agree to 1e-10."""
+    from helpers import FP64_RTOL, rel_err
+    from lbfs_b200 import GpuSolver, _abi, cases, red_cell
+    from oracle_lbfs import OracleSolver
+    c = cases.shear_rbc(n=16, level=1, radius_cells=2.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
+    first = c.membranes[0]
+    moduli = {k: getattr(first, k) for k in ("volume_modulus", "local_area_modulus", "global_area_modulus",
+                                             "shear_modulus", "global_bending_modulus", "wlc_ratio",
+                                             "internal_viscosity_ratio")}
+    X = c.mesh.X
+    flag = _abi.LBFS_WRAP_OWN if mode == "own" else _abi.LBFS_WRAP_ALL
+    c.membranes = [red_cell(1, 4.0, (0.3 * X, 0.5 * X, 0.8 * X), **moduli),
+                   red_cell(1, 4.0, (0.7 * X, 0.5 * X, 0.4 * X), **moduli)]
+    for m in c.membranes:
+        m.periodic = flag
+    s = GpuSolver(c.mesh, c.params, c.membranes)
+    o = OracleSolver(c.mesh, c.params, c.membranes)
+    z_before = []
+    for h in (s, o):
+        h.set_state(c.rho, c.u, c.v, c.w)
+    z_before = s.nodes()[:, 2].copy()
+    s.step(2)  # the wrap follows the fluid update of step t = 1
+    o.step(2)
+    z_gpu, z_ora = s.nodes()[:, 2], o.nodes()[:, 2]
+    assert rel_err(s.nodes(), o.nodes()) < FP64_RTOL
+    n0 = c.membranes[0].n_nodes
+    moved = z_before - z_gpu > 0.25 * X  # moved by Z / 2 (the advection moves nodes far less)
+    if mode == "own":
+        assert moved[:n0].all() and not moved[n0:].any()
+    else:
+        assert not moved.any()
+    for a, b in zip(s.state(), o.state()):
+        assert rel_err(a, b) < FP64_RTOL
+    s.close()
+    o.close()
+
+
+@pytest.mark.parametrize("mode", ["own", "all"])
+def test_oracle_periodic_object_wrap_modes(mode):
+    """The oracle's check_periodic_object: LBFS_WRAP_OWN moves each membrane by its own mean,
+    LBFS_WRAP_ALL (membrane 0) moves all membranes by the mean over all their nodes."""
+    from lbfs_b200 import red_cell
+    c = cases.shear_rbc(n=16, level=1, radius_cells=2.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
+    first = c.membranes[0]
+    moduli = {k: getattr(first, k) for k in ("volume_modulus", "local_area_modulus", "global_area_modulus",
+                                             "shear_modulus", "global_bending_modulus", "wlc_ratio",
+                                             "internal_viscosity_ratio")}
+    X = c.mesh.X
+    flag = _abi.LBFS_WRAP_OWN if mode == "own" else _abi.LBFS_WRAP_ALL
+    for zs, expect in (((0.8, 0.4), {"own": (True, False), "all": (False, False)}),
+                       ((0.8, 0.78), {"own": (True, True), "all": (True, True)})):
+        c.membranes = [red_cell(1, 4.0, (x * X, 0.5 * X, z * X), **moduli) for x, z in zip((0.3, 0.7), zs)]
+        for m in c.membranes:
+            m.periodic = flag
+        o = OracleSolver(c.mesh, c.params, c.membranes)
+        o.set_state(c.rho, c.u, c.v, c.w)
+        z0 = o.nodes()[:, 2].copy()
+        o.step(2)  # the wrap follows the fluid update of step t = 1
+        moved = z0 - o.nodes()[:, 2] > 0.25 * X
+        n0 = c.membranes[0].n_nodes
+        assert (bool(moved[:n0].all()), bool(moved[n0:].all())) == expect[mode], (zs, mode)
+        assert moved[:n0].all() or not moved[:n0].any()
+        o.close()
