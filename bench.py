@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--n", type=int, default=64, help="cells per axis")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-hat2", action="store_true", help="skip the run on the reference's 2-point hat stencil")
+    ap.add_argument("--no-reference-programs", action="store_true",
+                    help="reference arm: skip the reference's own GPU solver and CPU Solver programs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble section")
     ap.add_argument("--instances", type=int, default=64, help="instances of the batched ensemble")
@@ -216,6 +218,59 @@ def _ref_worker(args):
     return n_cells * steps, dt
 
 
+def _timed_program(program, make_deck, steps_pair, workdir, timeout=900):
+    """Per-step host wall time of one of the reference's programs (oracle/ref_program.cpp behind the
+    reference's set-up) from two runs of different step counts: the difference removes the set-up."""
+    t = {}
+    for n in steps_pair:
+        d = os.path.join(workdir, f"{os.path.basename(program)}_{n}")
+        deck, state, info = make_deck(d, n)
+        r = subprocess.run([program, deck, os.path.join(d, "run"), state], capture_output=True, text=True,
+                           timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"{os.path.basename(program)} exited {r.returncode}: {r.stderr[-300:]}")
+        t[n] = float(open(os.path.join(d, "run_run.txt")).read().split()[1])
+    n0, n1 = steps_pair
+    per = (t[n1] - t[n0]) / (n1 - n0)
+    return {"value": info["n_cells"] / per / 1e6, "unit": METRIC, "ms_per_step": per * 1e3,
+            "timing": f"host wall clock of the solver call at {n1} and {n0} steps, difference over {n1 - n0} steps",
+            "seconds": {str(k): v for k, v in t.items()}}
+
+
+def reference_programs():
+    """The reference's own GPU solver (Solver_gpu.cu and its kernels, unmodified, built for sm_100a with
+    relocatable device code: oracle/_ref/ref_gpu_program) and its CPU Solver (oracle/_ref/ref_cpu_program),
+    each behind the reference's program set-up reading an XML deck (oracle/ref_program.cpp,
+    oracle/ref_deck.py): the 64^3 shear + L3 red cell workload (its 2-point IBM) and the 32^3 duct."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_deck
+    gpu_prog = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_program")
+    cpu_prog = os.path.join(ROOT, "oracle", "_ref", "ref_cpu_program")
+    out = {}
+    with tempfile.TemporaryDirectory(prefix="refprog") as work:
+        shear = lambda d, n: ref_deck.shear_rbc_deck(d, n=64, steps=n, level=3, radius_cells=8.0)
+        duct = lambda d, n: ref_deck.poiseuille_deck(d, n=32, steps=n)
+        duct_cpu = lambda d, n: ref_deck.poiseuille_deck(d, n=32, steps=n, cpu_solver=True)
+        if os.path.exists(gpu_prog):
+            for name, mk, pair in (("shear_rbc64_hat2", shear, (50, 550)), ("poiseuille32", duct, (50, 1050))):
+                try:
+                    out.setdefault("reference_gpu", {})[name] = _timed_program(gpu_prog, mk, pair, work)
+                except Exception as exc:
+                    out.setdefault("reference_gpu", {})[name] = {"value": None, "error": str(exc)}
+            out["reference_gpu"]["what"] = ("the reference's Solver_gpu.cu time loop (every kernel followed by a "
+                                            "device synchronize, managed memory) built for sm_100a, 1 B200")
+        else:
+            out["reference_gpu"] = {"unavailable": "oracle/_ref/ref_gpu_program was not built"}
+        if os.path.exists(cpu_prog):
+            try:
+                out["reference_cpu_solver"] = dict(_timed_program(cpu_prog, duct_cpu, (3, 23), work), cores=1,
+                                                   what="Solver::General_Purpose_Solver_mk_i (Solver.cpp:88-587), "
+                                                        "serial, fluid only, on the 32^3 duct")
+            except Exception as exc:
+                out["reference_cpu_solver"] = {"value": None, "error": str(exc)}
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference's own CPU implementation of the step (its kernel sources
     compiled for the host, oracle/_ref), one serial instance per host core, on
@@ -268,6 +323,8 @@ def run_reference(args, rank, world):
                                    f"(wall {wall:.1f} s incl. set-up)"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_reference_programs:
+        line.update(reference_programs())
     print(json.dumps(line))
     return 0
 

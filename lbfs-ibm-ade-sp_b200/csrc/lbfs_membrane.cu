@@ -1165,10 +1165,12 @@ __global__ void k_interior_viscosity(ViscArgs a) {
     if (i >= a.nc) return;
     const int inst = a.cell_instance ? a.cell_instance[i] : 0;
     const InstanceGrid g = a.instances[inst];
-    if (i == g.cell0) return;  // the reference skips cell 0 (of its mesh)
+    // update_viscosities fills every cell with 1 before the ray test (fill_double, Solver_gpu.cu:2194):
+    // cells outside every membrane's box, and cell 0, which the test skips, end at 1
+    double out = 1.0;
     const D3 cc = d3(a.centroid[3 * i], a.centroid[3 * i + 1], a.centroid[3 * i + 2]);
     const double pi = acos(-1.0);
-    for (int m = g.mem0; m < g.mem1; m++) {
+    for (int m = g.mem0; m < g.mem1 && i != g.cell0; m++) {
         const MembraneScalars ms = a.ms[m];
         const MembraneConst mc = a.mc[m];
         const double dh = mc.gdh;
@@ -1216,8 +1218,9 @@ __global__ void k_interior_viscosity(ViscArgs a) {
         const double r = mc.internal_viscosity_ratio;
         const double factor = 2.0 * fmin(0.5, (min_distance * 0.5 / dh + 1.0 / pi * sin(pi * min_distance / dh) * 0.5));
         const double visc = inside ? (r + 1.0) + (r - 1.0) * factor : (r + 1.0) + (1.0 - r) * factor;
-        ((R *)a.visc_factor)[i] = (R)(visc * 0.5);
+        out = visc * 0.5;
     }
+    ((R *)a.visc_factor)[i] = (R)out;
 }
 
 }  // namespace

@@ -36,6 +36,11 @@ void lbfs_check(int rc, const char *what) {
 
 }  // namespace
 
+// The rest of the class as Solver_gpu.cu defines it (this file takes that
+// translation unit's place in a build): construction and destruction hold no state.
+gpu_solver::gpu_solver() {}
+gpu_solver::~gpu_solver() {}
+
 void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &soln, Boundary_Conditions &bcs,
                                              external_forces &source, global_variables &globals,
                                              domain_geometry &domain, initial_conditions &init_conds,

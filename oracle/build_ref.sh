@@ -19,7 +19,7 @@ mkdir -p "$OUT"
 CXXFLAGS="-std=c++17 -O2 -ffp-contract=off -fPIC -fpermissive -w -I$HERE/ref_stub -I$REF"
 HOST_SRC="unstructured_mesh Mesh global_variables domain_geometry initial_conditions vector_var gradients
           Boundary_Conditions Solution unstructured_bcs lagrangian_object tecplot_output quad_bcs quad_bcs_plus
-          post_processing residuals flux_var RungeKutta external_forces"
+          post_processing residuals flux_var RungeKutta external_forces preprocessor tinyxml2"
 KERNEL_SRC="LBFS immersed_boundary_method spring_network common_kernels"
 pids=()
 for f in $HOST_SRC; do
@@ -30,5 +30,42 @@ for f in $KERNEL_SRC; do
 done
 g++ $CXXFLAGS -c "$HERE/ref_driver.cpp" -o "$OUT/ref_driver.o" & pids+=($!)
 for p in "${pids[@]}"; do wait "$p"; done
-g++ -shared -o "$OUT/libref_lbfs.so" "$OUT"/*.o
+KERNEL_OBJ=""
+for f in $KERNEL_SRC; do KERNEL_OBJ="$KERNEL_OBJ $OUT/$f.o"; done
+HOST_OBJ=""
+for f in $HOST_SRC; do HOST_OBJ="$HOST_OBJ $OUT/$f.o"; done
+g++ -shared -o "$OUT/libref_lbfs.so" $HOST_OBJ $KERNEL_OBJ "$OUT/ref_driver.o"
 echo "built $OUT/libref_lbfs.so"
+
+# The drop-in program: the reference's own set-up (XML deck, preprocessor, mesh,
+# boundary conditions, lagrangian object; oracle/ref_program.cpp after
+# program::run) calling gpu_solver::General_Purpose_Solver_mk_i as linked from
+# the repository's drop-in (integration/Solver_gpu_lbfs.cpp) over liblbfs_b200.so
+# instead of the reference's Solver_gpu.cu.  Needs the library built first.
+ROOT="$(dirname "$HERE")"
+LIBDIR="$ROOT/lbfs-ibm-ade-sp_b200/lbfs_b200/_lib"
+if [ -f "$LIBDIR/liblbfs_b200.so" ]; then
+  mkdir -p "$OUT/dropin"
+  g++ $CXXFLAGS -I"$ROOT/include" -c "$HERE/ref_program.cpp" -o "$OUT/dropin/ref_program.o" &
+  p1=$!
+  g++ $CXXFLAGS -I"$ROOT/include" -c "$ROOT/lbfs-ibm-ade-sp_b200/integration/Solver_gpu_lbfs.cpp" \
+      -o "$OUT/dropin/Solver_gpu_lbfs.o" &
+  p2=$!
+  wait $p1; wait $p2
+  g++ -o "$OUT/dropin_program" "$OUT/dropin/ref_program.o" "$OUT/dropin/Solver_gpu_lbfs.o" $HOST_OBJ \
+      -L"$LIBDIR" -llbfs_b200 -Wl,-rpath,'$ORIGIN/../../lbfs-ibm-ade-sp_b200/lbfs_b200/_lib'
+  echo "built $OUT/dropin_program"
+else
+  echo "liblbfs_b200.so not built yet; skipping oracle/_ref/dropin_program" >&2
+fi
+
+# The reference's CPU solver behind the same set-up (Solver::General_Purpose_Solver_mk_i,
+# the BASELINE's CPU row): ref_program.cpp built with REF_CPU_SOLVER.
+mkdir -p "$OUT/cpu"
+g++ $CXXFLAGS -c "$REF/Solver.cpp" -o "$OUT/cpu/Solver.o" &
+p1=$!
+g++ $CXXFLAGS -DREF_CPU_SOLVER -c "$HERE/ref_program.cpp" -o "$OUT/cpu/ref_program.o" &
+p2=$!
+wait $p1; wait $p2
+g++ -o "$OUT/ref_cpu_program" "$OUT/cpu/ref_program.o" "$OUT/cpu/Solver.o" $HOST_OBJ
+echo "built $OUT/ref_cpu_program"

@@ -77,11 +77,13 @@ def spring_fixture(name, level):
 
 
 def icosphere_fixture():
-    """Unit level-3 icosphere (nodes, outward triangles): the red cell of the
-    reference arm's workload (oracle/ref_cases.py), which loads no code of this
+    """Unit level-2 and level-3 icospheres (nodes, outward triangles): the red
+    cells of the reference arm's workload and of the reference's own decks
+    (oracle/ref_cases.py, oracle/ref_deck.py), which load no code of this
     repository."""
-    unit, tris = icosphere(3, 1.0)
-    np.savez_compressed(os.path.join(HERE, "icosphere_L3.npz"), unit_nodes=unit, tris=tris)
+    for level in (2, 3):
+        unit, tris = icosphere(level, 1.0)
+        np.savez_compressed(os.path.join(HERE, f"icosphere_L{level}.npz"), unit_nodes=unit, tris=tris)
 
 
 def plateau_case():

@@ -191,3 +191,22 @@ def test_shear48_l4_vs_oracle():
     assert s.status() == 0
     s.close()
     o.close()
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_zero_initial_visc_factor_vs_reference():
+    """The reference reads visc_factor before its first interior-viscosity update (zero-filled managed
+    memory in an RBC run, what the C++ drop-in passes), and that update first sets every cell to 1
+    (update_viscosities, Solver_gpu.cu:2194): cells outside the membrane's box must end at 1, not at
+    the initial value.  16^3 shear + L2 cell, 10 steps across the update at t = 1."""
+    import dataclasses
+    c = cases.shear_rbc(n=16, level=2, radius_cells=3.0, ibm_stencil=_abi.LBFS_IBM_HAT2)
+    c.params = dataclasses.replace(c.params, visc_factor_initial=0.0)
+    s, rc = _gpu(c), _ref(c)
+    s.step(10, graph=True)
+    rc.step(10)
+    _final_vs_ref(s, rc, True)
+    assert np.count_nonzero(s.field(_abi.LBFS_FIELD_VISC) == 1.0) > c.mesh.n_cells // 2
+    s.close()
+    rc.close()
