@@ -329,17 +329,26 @@ def run_reference(args, rank, world):
     return 0
 
 
-def run_batched(args, K, warmup, flush, device, plain_fp64_value):
+def run_batched(args, K, warmup, flush, device, plain_fp64_value, rank=0, world=1):
     """Batched ensemble (independent shear channels of 16^3-48^3 cells with 1-8
     red cells each) in one handle, FP32 bulk and FP64, launch shapes autotuned;
-    plus the same instances as separate handles, one graph each."""
+    plus (one GPU) the same instances as separate handles, one graph each.  On
+    N GPUs the instances are sharded by cost (cells + red-cell nodes, longest
+    processing time first): each rank builds the ensemble of its own instances,
+    nothing crosses ranks on the data path, and the aggregate throughput is all
+    ranks' cells over the slowest rank's time (max over ranks)."""
     import dataclasses
 
     import numpy as np
     import torch
 
     from lbfs_b200 import GpuSolver, _abi, cases
-    ce = cases.ensemble(n_instances=args.instances, precision=_abi.LBFS_FP32_BULK)
+    from lbfs_b200.parallel import gather_objects, max_over_ranks, shard_instances
+    subset = None
+    if world > 1:
+        specs = cases.ensemble_specs(n_instances=args.instances)
+        subset = shard_instances([sp["cost"] for sp in specs], world)[rank]
+    ce = cases.ensemble(n_instances=args.instances, precision=_abi.LBFS_FP32_BULK, subset=subset)
     p64 = dataclasses.replace(ce.params, precision=_abi.LBFS_FP64)
     s32 = GpuSolver(ce.mesh, ce.params, ce.membranes, device=device)
     s64 = GpuSolver(ce.mesh, p64, ce.membranes, device=device)
@@ -365,9 +374,24 @@ def run_batched(args, K, warmup, flush, device, plain_fp64_value):
     s32.close()
     s64.close()
     nc, nodes = ce.mesh.n_cells, ce.info["nodes"]
+    members = ce.info["members"]
+    if world > 1:
+        # every rank: its shard's time; the job: all cells over the slowest rank
+        per_rank = gather_objects({"rank": rank, "instances": len(members), "cells": nc,
+                                   "value": nc * K / (t["fp32"] * 1e-3) / 1e6, "ms_per_step": t["fp32"] / K,
+                                   "rel_err_velocity_vs_fp64": err_field})
+        t_max = {k: max_over_ranks(v, device="cuda") for k, v in t.items()}
+        cells_all = sum(r["cells"] for r in per_rank)
+        val = {k: cells_all * K / (v * 1e-3) / 1e6 for k, v in t_max.items()}
+        return {"value": val["fp32"], "unit": METRIC, "dtype": "f32 bulk (f64 reductions, node integration)",
+                "instances": args.instances, "cells": cells_all, "n_gpus": world, "scaling": "strong",
+                "sharding": "instances by cost (cells + red-cell nodes), longest processing time first; "
+                            "no data-path collective", "per_rank": per_rank,
+                "ms_per_step": t_max["fp32"] / K, "fp64_value": val["fp64"],
+                "rel_err_velocity_vs_fp64": max(r["rel_err_velocity_vs_fp64"] for r in per_rank),
+                "status_flags": flags, "launch_shape_fp32": shapes["fp32"]}
     val = {k: nc * K / (v * 1e-3) / 1e6 for k, v in t.items()}
     # the same instances as separate handles (one graph each, their own streams)
-    members = ce.info["members"]
     Ks = min(K, 20)
     hs = []
     for m in members:
@@ -499,6 +523,16 @@ def run_adjoint(args, device):
                  "bending_modulus": (taylor(kb=1 + h) - taylor(kb=1 - h)) / (2 * h * scale["bending_modulus"]),
                  "velocity_scale": (taylor(su=1 + h) - taylor(su=1 - h)) / (2 * h)}
     rel = {h: {k: abs(g[k] - v) / abs(v) if v != 0 else None for k, v in d.items()} for h, d in fd.items()}
+    # the finite-difference noise floor of the wall-velocity derivative: its effect on J over the window is
+    # small, so central differences at small h sit in the rounding of J; sweep h and report the
+    # difference quotient's error against the adjoint at each h, with J's change at that h
+    j0 = taylor()
+    sweep = {}
+    for h in (1e-7, 1e-6, 1e-5, 1e-4, 1e-3):
+        jp, jm = taylor(su=1 + h), taylor(su=1 - h)
+        q = (jp - jm) / (2 * h)
+        sweep[f"{h:g}"] = {"fd": q, "rel_err_vs_adjoint": abs(g["velocity_scale"] - q) / abs(q) if q != 0 else None,
+                           "delta_J_over_J": abs(jp - jm) / abs(j0), "J_rounding_over_J": 2.2e-16 * 50}
     return {"workload": "48^3 shear channel (110592 cells), 1 red cell L4 icosphere (2562 nodes, 5120 triangles), "
                         f"radius 8 cells, Ca 0.1, 4-point Peskin IBM, FP64, {N} steps, checkpoint every {K}",
             "objective": "Taylor deformation (L - B)/(L + B) of the red cell in the x-y plane at the final step",
@@ -508,7 +542,11 @@ def run_adjoint(args, device):
             "reverse_over_forward": t[1] / (N * fwd_ms),
             "reverse_over_forward_note": "reverse sweep (segment recomputation + backward kernels) per step over "
                                          "one plain forward step (graph, device events)",
-            "fd_h1e-6": fd[1e-6], "rel_err_h1e-6": rel[1e-6], "fd_h1e-4": fd[1e-4], "rel_err_h1e-4": rel[1e-4]}
+            "fd_h1e-6": fd[1e-6], "rel_err_h1e-6": rel[1e-6], "fd_h1e-4": fd[1e-4], "rel_err_h1e-4": rel[1e-4],
+            "velocity_fd_sweep": sweep,
+            "velocity_fd_sweep_note": "central differences of J in the wall-velocity scale at relative steps h; "
+                                      "J_rounding_over_J is an estimate of J's own rounding (50 ulp), the floor "
+                                      "below which delta_J_over_J carries no digits"}
 
 
 def run_profile(args):
@@ -551,7 +589,7 @@ def main():
 
     torch.cuda.set_device(local_rank)
     if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
     warmup = max(3, args.warmup)
     K = args.steps
     c = cases.shear_rbc(n=args.n)
@@ -681,8 +719,9 @@ def main():
         sh.close()
 
     # FP32-bulk form on the same workload: throughput and field error against this FP64 run
+    # the sections below describe the forms on one GPU; a multi-GPU run reports the replicas and the sharded ensemble
     fp32 = None
-    if rank == 0:
+    if rank == 0 and world == 1:
         c32 = cases.shear_rbc(n=args.n, precision=_abi.LBFS_FP32_BULK)
         c64 = cases.shear_rbc(n=args.n)
         a, b = GpuSolver(mesh, c64.params, c64.membranes, device=local_rank), \
@@ -713,21 +752,20 @@ def main():
         b.close()
 
     batched = None
-    if rank == 0 and not args.no_batched:
-        try:
-            batched = run_batched(args, K, warmup, flush, local_rank, mesh.n_cells * K / (step_sum[5] * 1e-3) / 1e6)
-        except Exception as exc:
-            batched = {"value": None, "error": f"{type(exc).__name__}: {exc}"}
+    if not args.no_batched:
+        # on N GPUs every rank takes its shard of the instances (the collectives inside are taken by all ranks)
+        batched = run_batched(args, K, warmup, flush, local_rank, mesh.n_cells * K / (step_sum[5] * 1e-3) / 1e6,
+                              rank, world)
 
     precision = None
-    if rank == 0 and not args.no_precision:
+    if rank == 0 and world == 1 and not args.no_precision:
         try:
             precision = run_precision(args, local_rank)
         except Exception as exc:
             precision = {"error": f"{type(exc).__name__}: {exc}"}
 
     adjoint = None
-    if rank == 0 and not args.no_adjoint:
+    if rank == 0 and world == 1 and not args.no_adjoint:
         try:
             adjoint = run_adjoint(args, local_rank)
         except Exception as exc:

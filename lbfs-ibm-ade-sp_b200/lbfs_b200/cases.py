@@ -157,19 +157,13 @@ def shear_channel(n, n_rbc=1, level=2, radius_cells=3.0, shear_modulus=1e-5, cap
                  "shear_modulus": shear_modulus, "gamma_dot": gamma, "n_rbc": len(cells)})
 
 
-def ensemble(n_instances=64, seed=2024, n_range=(16, 48), rbc_range=(1, 8), levels=(2, 3),
-             shear_modulus_range=(2e-6, 2e-5), capillary_range=(0.05, 0.5), precision=_abi.LBFS_FP32_BULK,
-             ibm_stencil=_abi.LBFS_IBM_PESKIN4, tau=0.8, delta_t=0.5, radius_cells=None):
-    """Batched ensemble of independent shear channels: per instance a cube of n
-    cells per axis (n uniform in n_range), 1-8 red cells of a level drawn from
-    `levels`, shear modulus log-uniform and capillary number uniform in their
-    ranges.  Red-cell radius: n / 12 cells, at least 1.5 (unless given).
-    Returns a Case whose mesh is an EnsembleMesh and whose info['members'] holds
-    the stand-alone Case of every instance."""
-    from dataclasses import replace
-    from .ensemble import concatenate
+def ensemble_specs(n_instances=64, seed=2024, n_range=(16, 48), rbc_range=(1, 8), levels=(2, 3),
+                   shear_modulus_range=(2e-6, 2e-5), capillary_range=(0.05, 0.5), radius_cells=None):
+    """The seeded draws of the batched workload, one dict per instance (n, n_rbc, level, shear
+    modulus, capillary number, radius, seed) and its cost for sharding (cells + red-cell nodes,
+    n_rbc taken as drawn)."""
     rng = np.random.default_rng(seed)
-    members = []
+    specs = []
     for k in range(n_instances):
         n = int(rng.integers(n_range[0], n_range[1] + 1))
         n_rbc = int(rng.integers(rbc_range[0], rbc_range[1] + 1))
@@ -177,7 +171,32 @@ def ensemble(n_instances=64, seed=2024, n_range=(16, 48), rbc_range=(1, 8), leve
         gs = float(np.exp(rng.uniform(np.log(shear_modulus_range[0]), np.log(shear_modulus_range[1]))))
         ca = float(rng.uniform(*capillary_range))
         r = radius_cells if radius_cells is not None else max(1.5, n / 12.0)
-        members.append(shear_channel(n, n_rbc, level, r, gs, ca, seed=seed * 1000 + k, tau=tau, delta_t=delta_t,
+        specs.append(dict(n=n, n_rbc=n_rbc, level=level, shear_modulus=gs, capillary=ca, radius_cells=r,
+                          seed=seed * 1000 + k, cost=n ** 3 + n_rbc * (10 * 4 ** level + 2)))
+    return specs
+
+
+def ensemble(n_instances=64, seed=2024, n_range=(16, 48), rbc_range=(1, 8), levels=(2, 3),
+             shear_modulus_range=(2e-6, 2e-5), capillary_range=(0.05, 0.5), precision=_abi.LBFS_FP32_BULK,
+             ibm_stencil=_abi.LBFS_IBM_PESKIN4, tau=0.8, delta_t=0.5, radius_cells=None, subset=None):
+    """Batched ensemble of independent shear channels: per instance a cube of n
+    cells per axis (n uniform in n_range), 1-8 red cells of a level drawn from
+    `levels`, shear modulus log-uniform and capillary number uniform in their
+    ranges.  Red-cell radius: n / 12 cells, at least 1.5 (unless given).
+    subset: the indices of the instances to build (a rank's shard; every
+    instance is the same whatever the subset).  Returns a Case whose mesh is an
+    EnsembleMesh and whose info['members'] holds the stand-alone Case of every
+    built instance (info['indices'] their instance numbers)."""
+    from dataclasses import replace
+    from .ensemble import concatenate
+    specs = ensemble_specs(n_instances, seed, n_range, rbc_range, levels, shear_modulus_range, capillary_range,
+                           radius_cells)
+    indices = list(range(n_instances)) if subset is None else sorted(int(k) for k in subset)
+    members = []
+    for k in indices:
+        sp = specs[k]
+        members.append(shear_channel(sp["n"], sp["n_rbc"], sp["level"], sp["radius_cells"], sp["shear_modulus"],
+                                     sp["capillary"], seed=sp["seed"], tau=tau, delta_t=delta_t,
                                      precision=precision, ibm_stencil=ibm_stencil))
     mesh = concatenate([c.mesh for c in members])
     membranes = [replace(m, instance=k) for k, c in enumerate(members) for m in c.membranes]
@@ -185,7 +204,7 @@ def ensemble(n_instances=64, seed=2024, n_range=(16, 48), rbc_range=(1, 8), leve
     params = replace(p, max_velocity=max(c.params.max_velocity for c in members))
     cat = lambda name: np.ascontiguousarray(np.concatenate([getattr(c, name) for c in members]))
     return Case("ensemble", mesh, params, membranes, cat("rho"), cat("u"), cat("v"), cat("w"), None,
-                {"members": members, "n_instances": n_instances, "cells": int(mesh.n_cells),
+                {"members": members, "indices": indices, "n_instances": n_instances, "cells": int(mesh.n_cells),
                  "membranes": len(membranes), "nodes": int(sum(m.n_nodes for m in membranes))})
 
 

@@ -88,3 +88,61 @@ def test_shard_instances_balances_and_is_deterministic():
     assert sorted(sum(a, [])) == list(range(len(costs)))
     loads = [sum(costs[i] for i in s) for s in a]
     assert max(loads) <= 1.34 * (sum(costs) / 3)
+
+
+_ENS = dict(n_instances=6, seed=31, n_range=(8, 12), rbc_range=(1, 2), levels=(1, 2))
+
+
+def _ensemble_worker(rank, world, port, q):
+    """One rank of the sharded batched workload: its instances by cost (cells + red-cell nodes),
+    its own ensemble layout of just those, and each of its instances stepped (the oracle standing in
+    for the GPU), gathered by instance number."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "lbfs-ibm-ade-sp_b200"))
+    import torch.distributed as dist
+    from datetime import timedelta
+    from lbfs_b200 import cases
+    from lbfs_b200.parallel import gather_objects, shard_instances
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    specs = cases.ensemble_specs(**_ENS)
+    shard = shard_instances([s["cost"] for s in specs], world)[rank]
+    part = cases.ensemble(**_ENS, subset=shard)
+    layout = {k: (part.mesh.split(part.u)[j].copy(), m.membranes[0].xyz_initial.copy())
+              for j, (k, m) in enumerate(zip(part.info["indices"], part.info["members"]))}
+    stepped = {k: _run_instance(m, steps=2) for k, m in zip(part.info["indices"], part.info["members"])}
+    gathered = gather_objects((shard, layout, stepped))
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        q.put(gathered)
+
+
+def test_two_rank_sharded_ensemble_equals_single_process():
+    """Sharding the batched workload over 2 gloo ranks: the shards cover every instance once, each
+    rank's ensemble holds exactly its instances' meshes, states and red cells as the one-process
+    ensemble does, and stepping them gives the one-process numbers."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_lbfs
+    from lbfs_b200 import cases
+    oracle_lbfs.lib()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_ensemble_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    gathered = q.get(timeout=240)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    shards = [g[0] for g in gathered]
+    assert sorted(shards[0] + shards[1]) == list(range(_ENS["n_instances"]))
+    full = cases.ensemble(**_ENS)
+    u = full.mesh.split(full.u)
+    for shard, layout, stepped in gathered:
+        for k in shard:
+            assert np.array_equal(layout[k][0], u[k])
+            assert np.array_equal(layout[k][1], full.info["members"][k].membranes[0].xyz_initial)
+            assert stepped[k] == _run_instance(full.info["members"][k], steps=2)
