@@ -851,13 +851,38 @@ template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStr
     const FaceRanges r = {{0, a.nfx, a.nfx + a.nfy}, {a.nfx, a.nfy, a.ni - a.nfx - a.nfy}};
     launch_fluid_flux_axis_ranges<R>(a, r, s);
 }
+// Boundary faces of an axis-aligned mesh: a short launch of long threads (a
+// one-wave grid that forms ghost records and general-normal fluxes) that runs
+// beside the interior-face tiles on another stream.  Launched with the
+// device's greatest scheduling priority so that its blocks are placed first
+// and finish under the interior faces instead of after them (the step graph is
+// instantiated with per-node priorities).
+template <typename R, int TB> void launch_general(const FluidArgs<R> &a, int first, int g, cudaStream_t s, bool hi) {
+    if (!hi) {
+        k_face_flux_general<R, TB><<<g, TB, 0, s>>>(a, first);
+        return;
+    }
+    int lo = 0, top = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &top);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = top;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(g);
+    cfg.blockDim = dim3(TB);
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_face_flux_general<R, TB>, a, first);
+}
 template <typename R> void launch_fluid_flux_general(const FluidArgs<R> &a, cudaStream_t s) {
     const int first = a.axis_aligned ? a.ni : 0;
     if (a.nf <= first) return;
     const int tb = a.tb_gen, g = (a.nf - first + tb - 1) / tb;
-    if (tb == 64) k_face_flux_general<R, 64><<<g, 64, 0, s>>>(a, first);
-    else if (tb == 256) k_face_flux_general<R, 256><<<g, 256, 0, s>>>(a, first);
-    else k_face_flux_general<R, 128><<<g, 128, 0, s>>>(a, first);
+    const bool hi = a.axis_aligned != 0;  // boundary faces only: beside the interior-face kernel
+    if (tb == 64) launch_general<R, 64>(a, first, g, s, hi);
+    else if (tb == 256) launch_general<R, 256>(a, first, g, s, hi);
+    else launch_general<R, 128>(a, first, g, s, hi);
 }
 template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s) {
     launch_fluid_flux_axis<R>(a, s);

@@ -127,3 +127,30 @@ def test_dropin_program_matches_reference_kernels(workload):
         for k in range(4):
             assert rel_err(got[k], want[k]) < FP64_RTOL, (k, rel_err(got[k], want[k]))
         assert not np.array_equal(got, inp["state"])  # the solver stepped
+
+
+REF_GPU = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_program")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (os.path.exists(PROGRAM) and os.path.exists(REF_GPU)),
+                    reason="oracle/_ref/ref_gpu_program or dropin_program not built")
+@pytest.mark.parametrize("workload", ["shear_rbc16", "poiseuille12"])
+def test_reference_gpu_solver_matches_dropin(workload):
+    """The reference's own GPU solver (Solver_gpu.cu and its kernels built for sm_100a) and the drop-in,
+    each behind the same program set-up and deck, agree within FP64_RTOL after 10 steps."""
+    import ref_deck
+    with tempfile.TemporaryDirectory() as d:
+        if workload == "shear_rbc16":
+            deck, state, _ = ref_deck.shear_rbc_deck(d, n=16, steps=10, level=2, radius_cells=3.0)
+        else:
+            deck, state, _ = ref_deck.poiseuille_deck(d, n=12, steps=10)
+        out = {}
+        for name, prog in (("dropin", PROGRAM), ("reference", REF_GPU)):
+            r = subprocess.run([prog, deck, os.path.join(d, name), state], capture_output=True, text=True,
+                               timeout=600)
+            assert r.returncode == 0, (name, r.stderr[-2000:])
+            out[name] = np.fromfile(os.path.join(d, f"{name}_state.bin")).reshape(4, -1)
+        for k in range(4):
+            assert rel_err(out["dropin"][k], out["reference"][k]) < FP64_RTOL, (k, rel_err(out["dropin"][k],
+                                                                                           out["reference"][k]))
