@@ -127,6 +127,11 @@ def algorithmic_bytes(mesh, phase, fp64=True):
     reads or writes counted once), FP64 storage."""
     nc, nf, ni, nb = mesh.n_cells, mesh.n_faces, mesh.n_interior, mesh.n_bc
     R = 8 if fp64 else 4
+    if phase == "flux" and not getattr(mesh, "axis_aligned", True):
+        # general-normal faces: per interior face ids 8, geometry (area, dt, n, t1, t2, branch) 12R,
+        # flux out 4R; per bc face the same plus bc types/values 8 + 4R, bc record 9R, ghost state and
+        # gradients out 16R; per cell: state 4R + 12 gradients 12R, visc factor R
+        return ni * (8 + 16 * R) + nb * (16 + 45 * R) + nc * (17 * R)
     if phase == "flux":
         # per axis face: owner+neighbour ids 8, geometry (area, dt, t1, t2) 4R, flux out 4R;
         # per bc face: ids 8, geometry 12R, bc types/values 8 + 4R, bc record 9R, flux out 4R;
@@ -451,6 +456,23 @@ def run_precision(args, device):
                 t += s.phase_times()[5]
             runs[name] = (s.state(), s.nodes().reshape(-1, 3), s.status())
             out[name] = {"value": c.mesh.n_cells * (N - 3) / (t * 1e-3) / 1e6, "ms_per_step": t / (N - 3)}
+            # per-kernel events on a few more steps (after the compared ones): K1, the general-normal
+            # face fluxes (interior tiles + boundary faces beside them), K3 against the HBM peak
+            s.set_profiling(2)
+            s.step(2, graph=True)
+            acc = np.zeros(6)
+            for _ in range(10):
+                s.step(1, graph=True)
+                acc += s.phase_times()
+            peaks, _ = measured_peaks()
+            kr = {}
+            for i, (ph, kn) in ((1, ("gradients", "k_cell_gradients")), (2, ("flux", "k_face_flux_general")),
+                                (3, ("update", "k_cell_update"))):
+                ms = acc[i] / 10
+                b_ = algorithmic_bytes(c.mesh, ph, fp64=(name == "fp64"))
+                kr[kn] = {"algorithmic_bytes": b_, "ms": ms, "achieved_gbs": b_ / (ms * 1e-3) / 1e9,
+                          "frac": b_ / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"]}
+            out[name]["kernel_roofline"] = kr
         info = c.info
     (r64, x64, f64), (r32, x32, f32) = runs["fp64"], runs["fp32"]
     rel_inf = {k: float(np.max(np.abs(a - b)) / np.max(np.abs(b))) for k, a, b in zip("uvw", r32[1:], r64[1:])}

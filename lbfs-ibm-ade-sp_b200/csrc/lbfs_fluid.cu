@@ -438,7 +438,7 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
     }
     const R dt = geo.dt;
     const R S1[4] = {s1.rho, s1.u, s1.v, s1.w}, S2[4] = {s2.rho, s2.u, s2.v, s2.w};
-    R pi[4], pn[4], p0[4], g3[12];
+    R pi[4], pn[4], p0[4];
     if (geo.bc_branch != R(0)) {
         const int b = oc.y - a.nc;
         const Vec4<R> bc = a.bc_val[b];
@@ -453,7 +453,7 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
             pn[m] = p0[m];
         }
 #pragma unroll
-        for (int t = 0; t < 12; t++) { g3[t] = g2[t]; g1[t] = g2[t]; }
+        for (int t = 0; t < 12; t++) g1[t] = g2[t];
     } else {
 #pragma unroll
         for (int m = 0; m < 4; m++) {
@@ -461,8 +461,6 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
             pn[m] = S2[m] - (geo.t2x * g2[3 * m] + geo.t2y * g2[3 * m + 1] + geo.t2z * g2[3 * m + 2]);
             p0[m] = (pi[m] + pn[m]) * R(0.5);
         }
-#pragma unroll
-        for (int t = 0; t < 12; t++) g3[t] = (g1[t] + g2[t]) * R(0.5);
     }
     // FP32 deviation form: offsets from the face centre (pop_dev); hdp is half
     // the owner-neighbour difference of the reconstructed states
@@ -496,27 +494,48 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
         // side of direction k and of its opposite k+1: 0 owner, 1 neighbour, 2 centre
         const int side_k = (s > thr) ? 0 : ((s < -thr) ? 1 : 2);
         const int side_o = (side_k == 2) ? 2 : 1 - side_k;
+        (void)side_o;
+        // e . gradient per component from the owner (A), the neighbour (B) and the face centre
+        // (C, the mean gradient); direction k (+e) is extrapolated from side_k, its opposite (-e)
+        // from the other side (the centre for both): L = base -+ dt (e . g)
+        R Lp[4], Lm[4], Dp[4], Dm[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            R A = R(0), B = R(0);
+            bool first = true;
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                if (!ee[d]) continue;
+                const R ga = ee[d] > 0 ? g1[3 * m + d] : -g1[3 * m + d];
+                const R gb = ee[d] > 0 ? g2[3 * m + d] : -g2[3 * m + d];
+                A = first ? ga : A + ga;
+                B = first ? gb : B + gb;
+                first = false;
+            }
+            const R C = (A + B) * R(0.5);
+            const R Xp = side_k == 0 ? A : (side_k == 1 ? B : C);
+            const R Xm = side_k == 0 ? B : (side_k == 1 ? A : C);
+            if constexpr (sizeof(R) == 8) {
+                const R bp = side_k == 0 ? pi[m] : (side_k == 1 ? pn[m] : p0[m]);
+                const R bm = side_k == 0 ? pn[m] : (side_k == 1 ? pi[m] : p0[m]);
+                Lp[m] = bp - Xp * dt;
+                Lm[m] = bm + Xm * dt;
+            } else {
+                // FP32: offsets from the face centre (+hdp owner, -hdp neighbour, 0 centre)
+                const R bp = side_k == 0 ? hdp[m] : (side_k == 1 ? -hdp[m] : R(0));
+                const R bm = side_k == 0 ? -hdp[m] : (side_k == 1 ? hdp[m] : R(0));
+                Dp[m] = bp - Xp * dt;
+                Dm[m] = bm + Xm * dt;
+                Lp[m] = p0[m] + Dp[m];
+                Lm[m] = p0[m] + Dm[m];
+            }
+        }
         R gp[2];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const int side = h ? side_o : side_k;
+            const R(&L)[4] = h ? Lm : Lp;
+            const R(&D)[4] = h ? Dm : Dp;
             const int sg = h ? -1 : 1;
-            R L[4], D[4];
-#pragma unroll
-            for (int m = 0; m < 4; m++) {
-                // FP64: the value itself; FP32: its offset from the face centre
-                R val;
-                if constexpr (sizeof(R) == 8) val = side == 0 ? pi[m] : (side == 1 ? pn[m] : p0[m]);
-                else val = side == 0 ? hdp[m] : (side == 1 ? -hdp[m] : R(0));
-#pragma unroll
-                for (int d = 0; d < 3; d++) {
-                    if (!ee[d]) continue;
-                    const R gd = side == 0 ? g1[3 * m + d] : (side == 1 ? g2[3 * m + d] : g3[3 * m + d]);
-                    val = (sg * ee[d] > 0) ? val - gd * dt : val + gd * dt;
-                }
-                if constexpr (sizeof(R) == 8) L[m] = val;
-                else { D[m] = val; L[m] = p0[m] + val; }
-            }
             R eu = R(0), edu = R(0);
             bool first = true;
 #pragma unroll
@@ -599,6 +618,21 @@ __global__ void __launch_bounds__(TB, 640 / TB) k_face_flux_tiles(FluidArgs<R> a
     for (int f = f0x + (int)threadIdx.x; f < f1x; f += TB) a.flux[f] = axis_face_flux<R, 0>(a, f);
     for (int f = f0y + (int)threadIdx.x; f < f1y; f += TB) a.flux[f] = axis_face_flux<R, 1>(a, f);
     for (int f = f0z + (int)threadIdx.x; f < f1z; f += TB) a.flux[f] = axis_face_flux<R, 2>(a, f);
+}
+
+// Interior faces of a mesh that is not axis aligned (every face takes the
+// general-normal reconstruction), tile by tile as k_face_flux_tiles: block b
+// takes the faces owned by the TB cells of tile tile0 + b, in up to three
+// face ranges ordered by owner (the generator's x, y, z faces; an imported
+// mesh's internal faces, which OpenFOAM orders by owner, form one range).
+template <typename R, int TB>
+__global__ void __launch_bounds__(TB, 512 / TB) k_face_flux_general_tiles(FluidArgs<R> a, int tile0) {
+    const int *tp = a.flux_tiles + 3 * (tile0 + (int)blockIdx.x);
+#pragma unroll 1
+    for (int r = 0; r < 3; r++) {
+        const int f0 = __ldg(tp + r), f1 = __ldg(tp + 3 + r);
+        for (int f = f0 + (int)threadIdx.x; f < f1; f += TB) a.flux[f] = general_face_flux<R>(a, f, false);
+    }
 }
 
 // Boundary faces (always) and the interior faces of meshes that are not axis
@@ -838,13 +872,19 @@ template <typename R> void launch_fluid_flux_axis_ranges(const FluidArgs<R> &a, 
 }
 template <typename R> void launch_fluid_flux_tiles(const FluidArgs<R> &a, int tile0, int tile1, cudaStream_t s) {
     const int g = tile1 - tile0;
-    if (!a.axis_aligned || g <= 0) return;
+    if (g <= 0) return;
+    if (!a.axis_aligned) {
+        if (a.tb_gen == 64) k_face_flux_general_tiles<R, 64><<<g, 64, 0, s>>>(a, tile0);
+        else if (a.tb_gen == 256) k_face_flux_general_tiles<R, 256><<<g, 256, 0, s>>>(a, tile0);
+        else k_face_flux_general_tiles<R, 128><<<g, 128, 0, s>>>(a, tile0);
+        return;
+    }
     if (a.tb_flux == 64) k_face_flux_tiles<R, 64><<<g, 64, 0, s>>>(a, tile0);
     else if (a.tb_flux == 256) k_face_flux_tiles<R, 256><<<g, 256, 0, s>>>(a, tile0);
     else k_face_flux_tiles<R, 128><<<g, 128, 0, s>>>(a, tile0);
 }
 template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s) {
-    if (a.flux_tiles) {
+    if (a.flux_tiles) {  // interior faces by tiles (axis-aligned or general-normal kernel)
         launch_fluid_flux_tiles<R>(a, 0, a.n_tiles, s);
         return;
     }
@@ -876,10 +916,12 @@ template <typename R, int TB> void launch_general(const FluidArgs<R> &a, int fir
     cudaLaunchKernelEx(&cfg, k_face_flux_general<R, TB>, a, first);
 }
 template <typename R> void launch_fluid_flux_general(const FluidArgs<R> &a, cudaStream_t s) {
-    const int first = a.axis_aligned ? a.ni : 0;
+    // boundary faces only when the interior faces have a kernel of their own (axis faces, or tiles)
+    const bool bc_only = a.axis_aligned || a.flux_tiles;
+    const int first = bc_only ? a.ni : 0;
     if (a.nf <= first) return;
     const int tb = a.tb_gen, g = (a.nf - first + tb - 1) / tb;
-    const bool hi = a.axis_aligned != 0;  // boundary faces only: beside the interior-face kernel
+    const bool hi = bc_only;  // beside the interior-face kernel
     if (tb == 64) launch_general<R, 64>(a, first, g, s, hi);
     else if (tb == 256) launch_general<R, 256>(a, first, g, s, hi);
     else launch_general<R, 128>(a, first, g, s, hi);

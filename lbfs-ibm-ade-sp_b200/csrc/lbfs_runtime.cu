@@ -687,11 +687,20 @@ cudaError_t record_event(cudaEvent_t ev, cudaStream_t st) {
 // Tiles of the face kernel need in addition owners that do not decrease within
 // each axis range (the generator's order; ensembles keep it): the faces owned
 // by a tile of cells are then a contiguous range of each axis.
-int plan_chunks(lbfs_solver *s, const int *owner, const int *neighbour, int nfx, int nfy, int nfz) {
+//
+// Meshes that are not axis aligned take tiles too (their interior faces in the
+// general-normal kernel): the generator's face ranges when the x, y, z counts
+// cover the interior faces, else one range of all interior faces (an imported
+// polyMesh, whose internal faces OpenFOAM orders by owner); no chunking.
+int plan_chunks(lbfs_solver *s, const int *owner, const int *neighbour, int nfx, int nfy, int nfz, bool axis_aligned) {
     s->chunkable = false;
     s->tiled = false;
     const int ni = s->ni, nc = s->nc;
     if (ni == 0 || !owner) return LBFS_OK;
+    if (nfx < 0 || nfy < 0 || nfz < 0 || (long long)nfx + nfy + nfz != ni) {
+        if (axis_aligned) return LBFS_OK;
+        nfx = ni; nfy = 0; nfz = 0;
+    }
     const int start[3] = {0, nfx, nfx + nfy}, count[3] = {nfx, nfy, nfz};
     bool ordered = true, owners_ordered = true;
     for (int ax = 0; ax < 3; ax++)
@@ -699,7 +708,6 @@ int plan_chunks(lbfs_solver *s, const int *owner, const int *neighbour, int nfx,
             if (!(owner[f] < neighbour[f]) || (f > start[ax] && neighbour[f] < neighbour[f - 1])) ordered = false;
             if (f > start[ax] && owner[f] < owner[f - 1]) owners_ordered = false;
         }
-    if (!ordered) return LBFS_OK;
     if (owners_ordered) {
         for (int b = 0; b < 3; b++) {
             const int T = 64 << b, nt = (nc + T - 1) / T;
@@ -726,7 +734,7 @@ int plan_chunks(lbfs_solver *s, const int *owner, const int *neighbour, int nfx,
         }
         s->tiled = true;
     }
-    if (nc < 2 * kMaxFluxChunks * 256) return LBFS_OK;
+    if (!ordered || !axis_aligned || nc < 2 * kMaxFluxChunks * 256) return LBFS_OK;
     s->chunkable = true;
     s->chunk_nb.assign(neighbour, neighbour + ni);
     for (int ax = 0; ax < 3; ax++) { s->chunk_start[ax] = start[ax]; s->chunk_count[ax] = count[ax]; }
@@ -735,7 +743,8 @@ int plan_chunks(lbfs_solver *s, const int *owner, const int *neighbour, int nfx,
 
 // Face-kernel tiles of the current flux block size into the kernel arguments.
 template <typename R> void apply_tiles(lbfs_solver *s, FluidArgs<R> &a) {
-    const int b = a.tb_flux == 64 ? 0 : (a.tb_flux == 256 ? 2 : 1);
+    const int tb = a.axis_aligned ? a.tb_flux : a.tb_gen;  // the tile kernel's block size
+    const int b = tb == 64 ? 0 : (tb == 256 ? 2 : 1);
     a.flux_tiles = s->tiled ? s->d_tiles[b] : nullptr;
     a.n_tiles = s->tiled ? (int)s->tile_maxnb[b].size() : 0;
 }
@@ -746,7 +755,8 @@ void set_chunks(lbfs_solver *s, int K) {
     s->flux_chunks = K;
     if (s->fp32) apply_tiles<float>(s, s->f32);
     else apply_tiles<double>(s, s->f64);
-    const int tb = s->fp32 ? s->f32.tb_flux : s->f64.tb_flux;
+    const bool aa = s->fp32 ? s->f32.axis_aligned : s->f64.axis_aligned;
+    const int tb = s->fp32 ? (aa ? s->f32.tb_flux : s->f32.tb_gen) : (aa ? s->f64.tb_flux : s->f64.tb_gen);
     const std::vector<int> &mx = s->tile_maxnb[tb == 64 ? 0 : (tb == 256 ? 2 : 1)];
     // gradients and interior fluxes (K each), boundary fluxes, update; membrane kernels; CFL
     s->launches_per_step = 2 * K + 2 + (s->n_membranes > 0 ? (s->ma.force_cluster > 0 ? 3 : 6) : 0) + (dynamic_dt(s->params) ? 1 : 0);
@@ -808,14 +818,15 @@ template <typename R> int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n)
         { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
         {
             PhaseMark m(s, 2, s->stream);
-            if (a.axis_aligned) {
+            const bool fork = a.axis_aligned || a.flux_tiles;  // interior faces in their own kernel
+            if (fork) {
                 LBFS_CUDA(cudaEventRecord(s->ev_chunk[0], s->stream));
                 LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_chunk[0], 0));
                 launch_fluid_flux_axis<R>(a, s->stream4);
                 LBFS_CUDA(cudaEventRecord(s->ev_flux, s->stream4));
             }
             launch_fluid_flux_general<R>(a, s->stream);
-            if (a.axis_aligned) LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_flux, 0));
+            if (fork) LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_flux, 0));
         }
         *n += 2;
         return LBFS_OK;
@@ -992,8 +1003,8 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
     if (rc) return fail(rc);
     rc = s->fp32 ? setup_time_stepping<float>(s, mesh) : setup_time_stepping<double>(s, mesh);
     if (rc) return fail(rc);
-    if (mesh->axis_aligned &&
-        (rc = plan_chunks(s, mesh->owner, mesh->neighbour, mesh->n_face_x, mesh->n_face_y, mesh->n_face_z)))
+    if ((rc = plan_chunks(s, mesh->owner, mesh->neighbour, mesh->n_face_x, mesh->n_face_y, mesh->n_face_z,
+                          mesh->axis_aligned != 0)))
         return fail(rc);
     set_chunks(s, 1);
     *out = s;
