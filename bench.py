@@ -257,7 +257,7 @@ def reference_programs():
         duct = lambda d, n: ref_deck.poiseuille_deck(d, n=32, steps=n)
         duct_cpu = lambda d, n: ref_deck.poiseuille_deck(d, n=32, steps=n, cpu_solver=True)
         if os.path.exists(gpu_prog):
-            for name, mk, pair in (("shear_rbc64_hat2", shear, (50, 550)), ("poiseuille32", duct, (50, 1050))):
+            for name, mk, pair in (("shear_rbc64_hat2", shear, (50, 2050)), ("poiseuille32", duct, (50, 3050))):
                 try:
                     out.setdefault("reference_gpu", {})[name] = _timed_program(gpu_prog, mk, pair, work)
                 except Exception as exc:

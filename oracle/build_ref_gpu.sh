@@ -30,7 +30,7 @@ for f in $CU_SRC; do
   "$NVCC" -std=c++17 -O2 -rdc=true -gencode arch=compute_100a,code=sm_100a -maxrregcount=128 -w $INC \
       -c "$REF/$f.cu" -o "$OUT/$f.o" & pids+=($!)
 done
-g++ -std=c++17 -O2 -fpermissive -w $INC -c "$HERE/ref_program.cpp" -o "$OUT/ref_program.o" & pids+=($!)
+g++ -std=c++17 -O2 -fpermissive -w $INC -DREF_GPU_PROGRAM -c "$HERE/ref_program.cpp" -o "$OUT/ref_program.o" & pids+=($!)
 for p in "${pids[@]}"; do wait "$p"; done
 OBJ=""
 for f in $HOST_SRC $CU_SRC ref_program; do OBJ="$OBJ $OUT/$f.o"; done
