@@ -598,6 +598,38 @@ __device__ __forceinline__ void write_spread_records(const MembraneArgs &A, cons
     }
 }
 
+// Exclusive prefix sum of one int per thread over the CTA, and the CTA's
+// total: a shuffle scan within each warp, the warp totals scanned by warp 0,
+// two barriers (in place of a Hillis-Steele scan over the whole CTA, whose
+// 2 log2(threads) barriers dominated the node sort).
+__device__ int block_exclusive_scan(int v, int *total) {
+    __shared__ int warp_sum[kMembraneThreads / 32 + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = (blockDim.x + 31) >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < n_warps ? warp_sum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < n_warps) warp_sum[lane] = w;  // inclusive prefix of the warp totals
+    }
+    __syncthreads();
+    const int before = warp == 0 ? 0 : warp_sum[warp - 1];
+    *total = warp_sum[n_warps - 1];
+    const int r = before + x - v;
+    __syncthreads();  // warp_sum is reused by the next call
+    return r;
+}
+
 // Node bounds of a membrane for the patch and the sort: per thread over
 // nodes ln = first, first + stride, ... (min of positions, minus max of
 // positions, min and minus max of the first stencil cells), the range flag,
@@ -686,27 +718,19 @@ __device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool
     if (last_sorted) {
         // every patch is known: prefix of patch cells over the membranes
         __threadfence();
-        __shared__ int scan[kMembraneThreads];
         const int M = n_sorters;
         const int per = (M + blockDim.x - 1) / blockDim.x;
         const int m0 = min(M, (int)threadIdx.x * per), m1 = min(M, m0 + per);
         int local = 0;
         for (int q = m0; q < m1; q++) local += __ldcg(&A.ms[q].patch_cells);
-        scan[threadIdx.x] = local;
-        __syncthreads();
-        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-            const int x = threadIdx.x >= (unsigned)o ? scan[threadIdx.x - o] : 0;
-            __syncthreads();
-            scan[threadIdx.x] += x;
-            __syncthreads();
-        }
-        int run = scan[threadIdx.x] - local;
+        int total = 0;
+        int run = block_exclusive_scan(local, &total);
         for (int q = m0; q < m1; q++) {
             A.cell_start[q] = run;
             run += __ldcg(&A.ms[q].patch_cells);
         }
-        if (threadIdx.x == blockDim.x - 1) {
-            A.cell_start[M] = scan[threadIdx.x];
+        if (threadIdx.x == 0) {
+            A.cell_start[M] = total;
             *A.sort_ticket = 0u;
         }
     }
@@ -732,21 +756,13 @@ __device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool
     }
     __syncthreads();
     {
-        __shared__ int cscan[kMembraneThreads];
         const int count = nbins + 1;
         const int per = (count + blockDim.x - 1) / blockDim.x;
         const int b0 = min(count, (int)threadIdx.x * per), b1 = min(count, b0 + per);
         int local = 0;
         for (int b = b0; b < b1; b++) local += cnt[b];
-        cscan[threadIdx.x] = local;
-        __syncthreads();
-        for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-            const int x = threadIdx.x >= (unsigned)o ? cscan[threadIdx.x - o] : 0;
-            __syncthreads();
-            cscan[threadIdx.x] += x;
-            __syncthreads();
-        }
-        int run = cscan[threadIdx.x] - local;
+        int total_unused = 0;
+        int run = block_exclusive_scan(local, &total_unused);
         int *cur = in_smem ? cnt : cursor;
         for (int b = b0; b < b1; b++) {
             const int c = cnt[b];
