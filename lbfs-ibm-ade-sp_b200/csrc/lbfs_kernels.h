@@ -77,6 +77,7 @@ struct MembraneArgs {
     double *patch_force;         // [sum of patch_bound * 3], membrane m from cell ms[m].patch_off
     unsigned int *flags;
     int sort_capacity;           // power of two >= nodes of the largest membrane
+    int max_nodes;               // nodes of the largest membrane
     int total_nodes, total_springs;
     const int *spring_mem;       // [total_springs] membrane of each spring
     int *bin_start;              // [sum of (patch_bound + 1)] first sorted node of each bin, from patch_off + m
@@ -84,8 +85,8 @@ struct MembraneArgs {
     int *cell_start;             // [n_membranes + 1] first spread cell of each membrane (prefix over patches)
     unsigned int *sort_ticket;   // membranes whose patch is known in this launch; zero between launches
     int spread_blocks;           // grid of the spread kernel (grid-stride over the tiles)
-    int force_cluster;           // 8 or 16: totals, node sort, spring and node forces as one cluster of that
-                                 // many CTAs per membrane (k_mem_step); 0: four kernels
+    int force_cluster;           // 8 or 16: totals, node sort, spring and node forces as one cluster of
+                                 // that many CTAs per membrane (k_mem_step); 0: four kernels
     int *node_base;              // [3 total_nodes] first IBM stencil cell per axis at the current positions
     double *node_w;              // [12 total_nodes] 1D stencil weights per axis (4 slots) at the current positions
     int *sorted_pos;             // [total_nodes] position of each node in its membrane's sorted order
@@ -106,7 +107,10 @@ struct MembraneArgs {
 // points per axis of an IBM stencil
 __host__ __device__ constexpr int stencil_width(int ibm_stencil) { return ibm_stencil == 2 ? 2 : 4; }
 
-void membrane_prepare(int sort_capacity);
+// Shared-memory limits of the kernels for the largest membrane.
+void membrane_prepare(int sort_capacity, int max_nodes);
+// Whether membranes of max_nodes nodes fit the one-cluster-per-membrane step.
+bool membrane_cluster_fits(int max_nodes);
 // Enqueues the membrane kernels of the current mode on `s` (the node sort on
 // `s_side`, joined back before the spread, when the side stream and its two
 // events are given); returns the launch count.

@@ -23,7 +23,8 @@
 //   P4  MAD = sum over the first n_nodes springs of c (A1 + A2) / 3, / A
 //       (sum_product_curvature<128> + lagrangian_object::add_MAD).
 //   P5  nodes sorted by the Eulerian cell at the base of their IBM stencil
-//       (bitonic sort of (cell, node) keys in shared memory).
+//       (counting sort over the stencil bins of the membrane's patch, each
+//       bin's nodes in index order).
 //   P6  force spreading as a per-cell segmented reduction over the sorted
 //       nodes into a dense patch around the membrane (replaces
 //       spread_forces_on_structured_grid, :947-1024, and its CAS atomics).
@@ -58,8 +59,13 @@ __device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y
 __device__ __forceinline__ D3 cross(D3 a, D3 b) {
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
+// Divisions by constants and repeated divisors are products with the
+// reciprocal in the membrane kernels (an FP64 division is a dependent
+// sequence of about ten instructions, and the spring forces are a chain of
+// them): results differ from the reference's divisions by rounding only.
+constexpr double kThird = 1.0 / 3.0, kSixth = 1.0 / 6.0;
 __device__ __forceinline__ D3 tri_centroid(D3 a, D3 b, D3 c) {
-    return {(a.x + b.x + c.x) / 3, (a.y + b.y + c.y) / 3, (a.z + b.z + c.z) / 3};
+    return {(a.x + b.x + c.x) * kThird, (a.y + b.y + c.y) * kThird, (a.z + b.z + c.z) * kThird};
 }
 
 // Deterministic block reductions: warp shuffle tree, then the warp results
@@ -194,7 +200,7 @@ __device__ __forceinline__ void d_normals(D3 a, D3 b, D3 c, D3 normal, double *d
     dN[18] = 0.0;       dN[19] = b.z - a.z; dN[20] = a.y - b.y;
     dN[21] = a.z - b.z; dN[22] = 0.0;       dN[23] = b.x - a.x;
     dN[24] = b.y - a.y; dN[25] = a.x - b.x; dN[26] = 0.0;
-    normal = normal / 3.0;
+    normal = normal * kThird;
 #pragma unroll
     for (int s = 0; s < 3; s++) {
         dV[3 * s + 0] = normal.x + dN[9 * s + 1] * cen.y + dN[9 * s + 2] * cen.z;
@@ -204,7 +210,7 @@ __device__ __forceinline__ void d_normals(D3 a, D3 b, D3 c, D3 normal, double *d
 }
 // Projection of dN on the unit normal (get_d_norms, spring_network.cu:1419-1428).
 __device__ __forceinline__ void d_norms(double *dn, const double *dN, double norm, D3 normal) {
-    normal = normal / norm;
+    normal = normal * (1.0 / norm);
 #pragma unroll
     for (int i = 0; i < 9; i++) dn[i] = dN[3 * i] * normal.x + dN[3 * i + 1] * normal.y + dN[3 * i + 2] * normal.z;
 }
@@ -226,12 +232,22 @@ struct SpringGeom {
     double norm_1, norm_2, length;
 };
 
-__device__ void spring_forces(const MembraneArgs &A, const MembraneConst &mc, const MembraneScalars &ms, int s,
-                              bool initials, double sfc, double vol_coef, double area_coef, double mad_coef) {
-    const int na = A.spring[4 * s], nb = A.spring[4 * s + 1], ncn = A.spring[4 * s + 2], nd = A.spring[4 * s + 3];
-    const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]);
-    D3 c = d3(A.x[ncn], A.y[ncn], A.z[ncn]);
-    const D3 d = d3(A.x[nd], A.y[nd], A.z[nd]);
+// What one spring's force needs besides the positions of its nodes a, b, c, d:
+// the velocities of a and c, and its stress-free constants.
+struct SpringConst {
+    double area0_1, area0_2, curv0, contour, kspring;
+};
+__device__ __forceinline__ SpringConst spring_const(const MembraneArgs &A, int s) {
+    return {A.area0[2 * s], A.area0[2 * s + 1], A.curv0[s], A.contour[s], A.kspring[s]};
+}
+
+// One spring's contributions to its four nodes (o[12]: a, b, c, d), its two
+// triangle areas (doubled) and its curvature.  With `initials` the reference
+// areas are the current ones (the initial pass writes them first).
+__device__ __forceinline__ void spring_core(const MembraneConst &mc, D3 a, D3 b, D3 c, D3 d, D3 va, D3 vcn,
+                                            const SpringConst &k, bool initials, double sfc, double vol_coef,
+                                            double area_coef, double mad_coef, double *o, double &area_1,
+                                            double &area_2, double &curvature_out, double &angle_out) {
     const D3 l = c - a;
     double length = sqrt(dot(l, l));
     const D3 normal_a = cross(b - a, c - a), normal_b = cross(c - a, d - a);
@@ -256,26 +272,23 @@ __device__ void spring_forces(const MembraneArgs &A, const MembraneConst &mc, co
     const double angle_direction = dot(normal_a, centroid_2);
     double angle = acos(cos_angle);
     angle = ((angle_direction < 0) - (angle_direction > 0)) * angle;
-    if (initials) {
-        A.angle0[s] = angle;
-        A.area0[2 * s] = norm_1;
-        A.area0[2 * s + 1] = norm_2;
-    }
+    angle_out = angle;
     double d_angle_1[9], d_angle_2[9], d_angle[12];
     {
-        const D3 h = cross(normal_a / norm_1, l / length);
+        const double inv_n1 = 1.0 / norm_1, inv_n2 = 1.0 / norm_2, inv_len = 1.0 / length;
+        const D3 h = cross(normal_a * inv_n1, l * inv_len);
 #pragma unroll
         for (int j = 0; j < 9; j++)
-            d_angle_1[j] = -1 / norm_1 * (h.x * dN1[j * 3] + h.y * dN1[j * 3 + 1] + h.z * dN1[j * 3 + 2]);
-        const D3 h2 = cross(l / length, normal_b / norm_2);
+            d_angle_1[j] = -inv_n1 * (h.x * dN1[j * 3] + h.y * dN1[j * 3 + 1] + h.z * dN1[j * 3 + 2]);
+        const D3 h2 = cross(l * inv_len, normal_b * inv_n2);
 #pragma unroll
         for (int j = 0; j < 9; j++)
-            d_angle_2[j] = -1 / norm_2 * (h2.x * dN2[j * 3] + h2.y * dN2[j * 3 + 1] + h2.z * dN2[j * 3 + 2]);
+            d_angle_2[j] = -inv_n2 * (h2.x * dN2[j * 3] + h2.y * dN2[j * 3 + 1] + h2.z * dN2[j * 3 + 2]);
     }
     merge12(d_angle, d_angle_1, d_angle_2);
     c = c - a;
     length = sqrt(dot(c, c));
-    const D3 dL_ds = c / length;
+    const D3 dL_ds = c * (1.0 / length);
     double d_curve[12];
 #pragma unroll
     for (int j = 0; j < 12; j++) d_curve[j] = d_angle[j] * length;
@@ -288,9 +301,9 @@ __device__ void spring_forces(const MembraneArgs &A, const MembraneConst &mc, co
 
     D3 fa = {0, 0, 0}, fb = {0, 0, 0}, fc = {0, 0, 0}, fd = {0, 0, 0};
     // local + global area
-    double lac = -1 * mc.local_area_modulus * (norm_1 / A.area0[2 * s] - 1) + area_coef;
+    double lac = -1 * mc.local_area_modulus * (norm_1 / (initials ? norm_1 : k.area0_1) - 1) + area_coef;
     fb.x += lac * dn1[3]; fb.y += lac * dn1[4]; fb.z += lac * dn1[5];
-    lac = -1 * mc.local_area_modulus * (norm_2 / A.area0[2 * s + 1] - 1) + area_coef;
+    lac = -1 * mc.local_area_modulus * (norm_2 / (initials ? norm_2 : k.area0_2) - 1) + area_coef;
     fd.x += lac * dn2[3]; fd.y += lac * dn2[4]; fd.z += lac * dn2[5];
     // volume
     fa.x += vol_coef * d_volume[0]; fa.y += vol_coef * d_volume[1]; fa.z += vol_coef * d_volume[2];
@@ -299,19 +312,18 @@ __device__ void spring_forces(const MembraneArgs &A, const MembraneConst &mc, co
     fd.x += vol_coef * d_volume[9]; fd.y += vol_coef * d_volume[10]; fd.z += vol_coef * d_volume[11];
     // membrane viscosity (Osay form)
     {
-        const D3 va = d3(A.vx[na], A.vy[na], A.vz[na]);
-        const D3 vc = d3(A.vx[ncn], A.vy[ncn], A.vz[ncn]) - va;
-        const D3 visc = dL_ds * -1 * dot(dL_ds, vc) * 4 / sqrt(3.0) * mc.viscosity;
+        const D3 vc = vcn - va;
+        const D3 visc = dL_ds * (-dot(dL_ds, vc) * (4.0 / 1.7320508075688772) * mc.viscosity);  // 4 / sqrt(3)
         fc = fc + visc;
         fa = fa - visc;
     }
     // curvature and bending
-    const double spring_area_total = (norm_1 + norm_2) / 6.0;
-    A.area[2 * s] = norm_1;
-    A.area[2 * s + 1] = norm_2;
+    const double spring_area_total = (norm_1 + norm_2) * kSixth;
+    area_1 = norm_1;
+    area_2 = norm_2;
     const double curvature = angle * length / spring_area_total;
-    A.curv[s] = curvature;
-    const double c0 = A.curv0[s];
+    curvature_out = curvature;
+    const double c0 = k.curv0;
     const double lbc = -0.5 * mc.local_bending_modulus * (c0 - curvature) * (c0 - curvature);
     fa.x += lbc * d_area[0]; fa.y += lbc * d_area[1]; fa.z += lbc * d_area[2];
     fb.x += lbc * d_area[3]; fb.y += lbc * d_area[4]; fb.z += lbc * d_area[5];
@@ -323,15 +335,37 @@ __device__ void spring_forces(const MembraneArgs &A, const MembraneConst &mc, co
     fc.x += cc * d_curve[6]; fc.y += cc * d_curve[7]; fc.z += cc * d_curve[8];
     fd.x += cc * d_curve[9]; fd.y += cc * d_curve[10]; fd.z += cc * d_curve[11];
     // WLC stretching
-    const double sr = length / A.contour[s];
-    const double fcoef = -1 * A.kspring[s] * ((0.25 / ((1.0 - sr) * (1.0 - sr))) - 0.25 + sr - sfc);
+    const double sr = length / k.contour;
+    const double fcoef = -1 * k.kspring * ((0.25 / ((1.0 - sr) * (1.0 - sr))) - 0.25 + sr - sfc);
     fc = fc + dL_ds * fcoef;
     fa = fa - dL_ds * fcoef;
-    double *o = A.contrib + 12 * (size_t)s;
     o[0] = fa.x; o[1] = fa.y; o[2] = fa.z;
     o[3] = fb.x; o[4] = fb.y; o[5] = fb.z;
     o[6] = fc.x; o[7] = fc.y; o[8] = fc.z;
     o[9] = fd.x; o[10] = fd.y; o[11] = fd.z;
+}
+
+// Spring s from the node arrays: forces into contrib[12 s], areas and
+// curvature into area / curv; the initial pass also records the reference
+// angle and areas.
+__device__ void spring_forces(const MembraneArgs &A, const MembraneConst &mc, const MembraneScalars &ms, int s,
+                              bool initials, double sfc, double vol_coef, double area_coef, double mad_coef) {
+    const int na = A.spring[4 * s], nb = A.spring[4 * s + 1], ncn = A.spring[4 * s + 2], nd = A.spring[4 * s + 3];
+    const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]);
+    const D3 c = d3(A.x[ncn], A.y[ncn], A.z[ncn]), d = d3(A.x[nd], A.y[nd], A.z[nd]);
+    const D3 va = d3(A.vx[na], A.vy[na], A.vz[na]), vc = d3(A.vx[ncn], A.vy[ncn], A.vz[ncn]);
+    const SpringConst k = initials ? SpringConst{0.0, 0.0, A.curv0[s], A.contour[s], A.kspring[s]} : spring_const(A, s);
+    double area_1, area_2, curvature, angle;
+    spring_core(mc, a, b, c, d, va, vc, k, initials, sfc, vol_coef, area_coef, mad_coef, A.contrib + 12 * (size_t)s,
+                area_1, area_2, curvature, angle);
+    if (initials) {
+        A.angle0[s] = angle;
+        A.area0[2 * s] = area_1;
+        A.area0[2 * s + 1] = area_2;
+    }
+    A.area[2 * s] = area_1;
+    A.area[2 * s + 1] = area_2;
+    A.curv[s] = curvature;
 }
 
 // Stress-free reference pass: get_contour_lengths (spring_network.cu:516-604)
@@ -479,13 +513,27 @@ __global__ void __launch_bounds__(kTotalsThreads) k_mem_totals(MembraneArgs A) {
     const int m = blockIdx.x;
     const MembraneConst mc = A.mc[m];
     double pv = 0.0, pa = 0.0;
-    for (int lt = threadIdx.x; lt < mc.n_tris; lt += blockDim.x) {
-        const int t = mc.tri0 + lt;
-        const int na = A.tri[3 * t], nb = A.tri[3 * t + 1], nc = A.tri[3 * t + 2];
-        const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]), c = d3(A.x[nc], A.y[nc], A.z[nc]);
-        const D3 normal = cross(b - a, c - a);
-        pv += dot(normal, tri_centroid(a, b, c)) / 6;
-        pa += sqrt(dot(normal, normal)) * 0.5;
+    for (int l0 = threadIdx.x; l0 < mc.n_tris; l0 += 2 * blockDim.x) {  // two triangles' loads per round
+        int tn[2][3];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int t = mc.tri0 + (l0 + k * (int)blockDim.x < mc.n_tris ? l0 + k * (int)blockDim.x : 0);
+#pragma unroll
+            for (int q = 0; q < 3; q++) tn[k][q] = A.tri[3 * (size_t)t + q];
+        }
+        D3 p[2][3];
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) p[k][q] = d3(A.x[tn[k][q]], A.y[tn[k][q]], A.z[tn[k][q]]);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            if (l0 + k * (int)blockDim.x >= mc.n_tris) break;
+            const D3 a = p[k][0], b = p[k][1], c = p[k][2];
+            const D3 normal = cross(b - a, c - a);
+            pv += dot(normal, tri_centroid(a, b, c)) * kSixth;
+            pa += sqrt(dot(normal, normal)) * 0.5;
+        }
     }
     const double V = block_sum(pv, sh), Ar = block_sum(pa, sh);
     if (threadIdx.x == 0) {
@@ -586,15 +634,31 @@ __global__ void __launch_bounds__(128) k_mem_nodeforce(MembraneArgs A) {
 // Spread records in sorted order: the node's stencil weights, first x cell and
 // index, and each node's sorted position.
 __device__ __forceinline__ void write_spread_records(const MembraneArgs &A, const MembraneConst &mc, const int *list) {
-    for (int e = threadIdx.x; e < mc.n_nodes; e += blockDim.x) {
-        const int n = mc.node0 + list[e];
-        SpreadRec rec;
-        for (int q = 0; q < 12; q++) rec.w[q] = A.node_w[12 * (size_t)n + q];
-        rec.b0 = A.node_base[3 * (size_t)n];
-        rec.node = n;
-        rec.pad[0] = rec.pad[1] = 0;
-        A.spread_rec[mc.node0 + e] = rec;
-        A.sorted_pos[n] = mc.node0 + e;
+    // two records per round: all their loads are issued before the stores
+    for (int e0 = threadIdx.x; e0 < mc.n_nodes; e0 += 2 * blockDim.x) {
+        SpreadRec rec[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int e = e0 + k * blockDim.x;
+            const int n = mc.node0 + list[e < mc.n_nodes ? e : 0];
+            const double2 *w = reinterpret_cast<const double2 *>(A.node_w + 12 * (size_t)n);
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                const double2 x = __ldcg(w + q);
+                rec[k].w[2 * q] = x.x;
+                rec[k].w[2 * q + 1] = x.y;
+            }
+            rec[k].b0 = __ldcg(A.node_base + 3 * (size_t)n);
+            rec[k].node = n;
+            rec[k].pad[0] = rec[k].pad[1] = 0;
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int e = e0 + k * blockDim.x;
+            if (e >= mc.n_nodes) break;
+            A.spread_rec[mc.node0 + e] = rec[k];
+            A.sorted_pos[rec[k].node] = mc.node0 + e;
+        }
     }
 }
 
@@ -636,30 +700,27 @@ __device__ int block_exclusive_scan(int v, int *total) {
 // and whether every first cell is sane; then reduced over the CTA
 // (minima are exact, so any order gives the same result).  out[12] valid in
 // every thread on return.
-__device__ void node_bounds(const MembraneArgs &A, const MembraneConst &mc, int first, int stride, double *out,
-                            unsigned int *flag_out, int *sane_out) {
+// One node's position p and first stencil cells b into the running bounds v[12].
+__device__ __forceinline__ void bounds_add(double (&v)[12], const double (&p)[3], const int (&b)[3], int S,
+                                           const MembraneConst &mc, unsigned int &range_flag, bool &base_range) {
+    const int gn[3] = {mc.gnx, mc.gny, mc.gnz};
+    for (int c = 0; c < 3; c++) {
+        v[c] = fmin(v[c], p[c]);            // lower bound
+        v[3 + c] = fmin(v[3 + c], -p[c]);   // minus upper bound
+        v[6 + c] = fmin(v[6 + c], (double)b[c]);
+        v[9 + c] = fmin(v[9 + c], -(double)b[c]);
+        if (b[c] < 0 || b[c] + S > gn[c]) range_flag = LBFS_FLAG_IBM_RANGE;
+        if (b[c] < -(1 << 19) || b[c] > (1 << 19)) base_range = false;
+    }
+}
+
+// The threads' bounds v[12], range flags and sanity reduced over the CTA;
+// out[12] valid in every thread on return.
+__device__ void bounds_reduce(const double (&v)[12], unsigned int range_flag, bool base_range, double *out,
+                              unsigned int *flag_out, int *sane_out) {
     __shared__ double shv[kMembraneThreads / 32][12];
     __shared__ unsigned int sflag;
     __shared__ int ssane;
-    const int S = stencil_width(A.ibm_stencil);
-    const int gn[3] = {mc.gnx, mc.gny, mc.gnz};
-    double v[12];
-    for (int c = 0; c < 12; c++) v[c] = 1e300;
-    unsigned int range_flag = 0;
-    bool base_range = true;
-    for (int ln = first; ln < mc.n_nodes; ln += stride) {
-        const int n = mc.node0 + ln;
-        const double p[3] = {A.x[n], A.y[n], A.z[n]};
-        const int b[3] = {A.node_base[3 * (size_t)n], A.node_base[3 * (size_t)n + 1], A.node_base[3 * (size_t)n + 2]};
-        for (int c = 0; c < 3; c++) {
-            v[c] = fmin(v[c], p[c]);            // lower bound
-            v[3 + c] = fmin(v[3 + c], -p[c]);   // minus upper bound
-            v[6 + c] = fmin(v[6 + c], (double)b[c]);
-            v[9 + c] = fmin(v[9 + c], -(double)b[c]);
-            if (b[c] < 0 || b[c] + S > gn[c]) range_flag = LBFS_FLAG_IBM_RANGE;
-            if (b[c] < -(1 << 19) || b[c] > (1 << 19)) base_range = false;
-        }
-    }
     if (threadIdx.x == 0) { sflag = 0u; ssane = 1; }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -681,6 +742,32 @@ __device__ void node_bounds(const MembraneArgs &A, const MembraneConst &mc, int 
     *flag_out = sflag;
     *sane_out = ssane;
     __syncthreads();
+}
+
+__device__ void node_bounds(const MembraneArgs &A, const MembraneConst &mc, int first, int stride, double *out,
+                            unsigned int *flag_out, int *sane_out) {
+    const int S = stencil_width(A.ibm_stencil);
+    double v[12];
+    for (int c = 0; c < 12; c++) v[c] = 1e300;
+    unsigned int range_flag = 0;
+    bool base_range = true;
+    // four nodes per round: their loads are issued together
+    for (int l0 = first; l0 < mc.n_nodes; l0 += 4 * stride) {
+        double p[4][3];
+        int b[4][3];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int ln = l0 + k * stride;
+            const int n = mc.node0 + (ln < mc.n_nodes ? ln : 0);
+            p[k][0] = A.x[n]; p[k][1] = A.y[n]; p[k][2] = A.z[n];
+            b[k][0] = A.node_base[3 * (size_t)n]; b[k][1] = A.node_base[3 * (size_t)n + 1];
+            b[k][2] = A.node_base[3 * (size_t)n + 2];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (l0 + k * stride < mc.n_nodes) bounds_add(v, p[k], b[k], S, mc, range_flag, base_range);
+    }
+    bounds_reduce(v, range_flag, base_range, out, flag_out, sane_out);
 }
 
 // Patch of a membrane from its node bounds red[12], the prefix of patch
@@ -748,11 +835,23 @@ __device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool
     int *cnt = in_smem ? list + A.sort_capacity : bin_start;
     for (int b = threadIdx.x; b <= nbins; b += blockDim.x) cnt[b] = 0;
     __syncthreads();
-    for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) {
-        const int *bb = A.node_base + 3 * (size_t)(mc.node0 + ln);
-        const int bin = (bb[0] - plo[0]) + bdim[0] * ((bb[1] - plo[1]) + bdim[1] * (bb[2] - plo[2]));
-        bins[ln] = bin;
-        atomicAdd(cnt + bin, 1);
+    for (int l0 = threadIdx.x; l0 < mc.n_nodes; l0 += 4 * blockDim.x) {  // four nodes' loads per round
+        int bb[4][3];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int ln = l0 + k * blockDim.x;
+            const int *src = A.node_base + 3 * (size_t)(mc.node0 + (ln < mc.n_nodes ? ln : 0));
+#pragma unroll
+            for (int q = 0; q < 3; q++) bb[k][q] = __ldcg(src + q);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int ln = l0 + k * blockDim.x;
+            if (ln >= mc.n_nodes) break;
+            const int bin = (bb[k][0] - plo[0]) + bdim[0] * ((bb[k][1] - plo[1]) + bdim[1] * (bb[k][2] - plo[2]));
+            bins[ln] = bin;
+            atomicAdd(cnt + bin, 1);
+        }
     }
     __syncthreads();
     {
@@ -760,12 +859,13 @@ __device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool
         const int per = (count + blockDim.x - 1) / blockDim.x;
         const int b0 = min(count, (int)threadIdx.x * per), b1 = min(count, b0 + per);
         int local = 0;
-        for (int b = b0; b < b1; b++) local += cnt[b];
+        // global counts were formed by atomics: L2 loads
+        for (int b = b0; b < b1; b++) local += in_smem ? cnt[b] : __ldcg(cnt + b);
         int total_unused = 0;
         int run = block_exclusive_scan(local, &total_unused);
         int *cur = in_smem ? cnt : cursor;
         for (int b = b0; b < b1; b++) {
-            const int c = cnt[b];
+            const int c = in_smem ? cnt[b] : __ldcg(cnt + b);
             bin_start[b] = run;  // the spread's bin table
             cur[b] = run;        // placement cursor
             run += c;
@@ -775,9 +875,11 @@ __device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool
     int *cur = in_smem ? cnt : cursor;
     for (int ln = threadIdx.x; ln < mc.n_nodes; ln += blockDim.x) list[atomicAdd(cur + bins[ln], 1)] = ln;
     __syncthreads();
-    // each bin [bin_start[b], bin_start[b + 1]) in node-index order
+    // each bin in node-index order; after the placement cur[b] is the end of
+    // bin b, the start of bin b + 1
     for (int b = threadIdx.x; b < nbins; b += blockDim.x) {
-        const int lo = bin_start[b], hi = bin_start[b + 1];
+        const int lo = b == 0 ? 0 : (in_smem ? cur[b - 1] : __ldcg(cur + b - 1));
+        const int hi = in_smem ? cur[b] : __ldcg(cur + b);  // global cursors were moved by atomics
         for (int i = lo + 1; i < hi; i++) {
             const int v = list[i];
             int j = i - 1;
@@ -803,113 +905,181 @@ __global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
 }
 
 // ---- the membrane step as one thread-block cluster per membrane -------------
-// Totals V, A and the node bounds (all CTAs, summed in rank order through
-// distributed shared memory), then the node sort and spread records (CTA rank
-// 0) beside the spring forces (ranks 1 ..), the MAD sum, and the node forces
-// (all CTAs).  Replaces k_mem_totals, k_mem_springs, k_mem_nodeforce and
-// k_mem_sort with one launch; the cluster barriers (release / acquire at
-// cluster scope) publish the per-spring contributions and the sorted records
-// between the phases.  Deterministic: every sum has a fixed order.
-constexpr int kStepThreads = 256;
-template <int CL>
-__global__ void __launch_bounds__(kStepThreads) k_mem_step(MembraneArgs A) {
+// After the advection kernel, one cluster of CL CTAs of TPB threads per
+// membrane does the work of k_mem_totals, k_mem_springs, k_mem_nodeforce and
+// k_mem_sort (four launches whose phases are each a few dependent memory round
+// trips, so that the launches and the waits between them set the chain's
+// length); the spread follows.
+//  rank 0: node bounds, the patch, the node sort and the spread records.
+//  ranks 1..: every node position into shared memory, V and A over all
+//     triangles (each CTA the same fixed-order sum, so they agree bit for
+//     bit), the spring forces and the MAD terms.
+//  -- cluster barrier (release / acquire): contributions and MAD partials
+//  all: MAD, the node forces in spring order.
+// Every sum has a fixed order that does not depend on the membrane's place in
+// an ensemble.  Shared memory: step_smem_bytes.
+constexpr int kStepMaxNodes = 8192;  // 24 bytes of shared memory per node
+constexpr int kStepThreads = 128;
+
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+template <int CL, int TPB>
+__global__ void __launch_bounds__(TPB) k_mem_step(MembraneArgs A) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
-    extern __shared__ unsigned long long sdyn[];  // the node sort's arrays (CTA rank 0)
+    extern __shared__ unsigned long long sdyn[];  // rank 0: the node sort's arrays; ranks 1..: node positions
     __shared__ double sh[33];
-    __shared__ double part_va[2], part_mad[1], part_b[12];
-    __shared__ unsigned int part_flag;
-    __shared__ int part_sane;
+    __shared__ double part_va[2], part_mad[1], mad_all;
     const int m = blockIdx.y;
     const int rank = (int)cluster.block_rank();
-    const int nth = CL * blockDim.x, tid = rank * blockDim.x + threadIdx.x;
+    const int nth = CL * TPB, tid = rank * TPB + threadIdx.x;
     const MembraneConst mc = A.mc[m];
     MembraneScalars *ms = A.ms + m;
-    // volume and area (update_spring_network_tet_parameters + total<128>)
-    double pv = 0.0, pa = 0.0;
-    for (int lt = tid; lt < mc.n_tris; lt += nth) {
-        const int t = mc.tri0 + lt;
-        const int na = A.tri[3 * t], nb = A.tri[3 * t + 1], nc = A.tri[3 * t + 2];
-        const D3 a = d3(A.x[na], A.y[na], A.z[na]), b = d3(A.x[nb], A.y[nb], A.z[nb]), c = d3(A.x[nc], A.y[nc], A.z[nc]);
-        const D3 normal = cross(b - a, c - a);
-        pv += dot(normal, tri_centroid(a, b, c)) / 6;
-        pa += sqrt(dot(normal, normal)) * 0.5;
-    }
-    const double bv = block_sum(pv, sh), ba = block_sum(pa, sh);
-    double bnd[12];
-    unsigned int bflag;
-    int bsane;
-    node_bounds(A, mc, tid, nth, bnd, &bflag, &bsane);
-    if (threadIdx.x == 0) {
-        part_va[0] = bv;
-        part_va[1] = ba;
-        for (int q = 0; q < 12; q++) part_b[q] = bnd[q];
-        part_flag = bflag;
-        part_sane = bsane;
-    }
-    const double V0 = ms->V0, A0 = ms->A0, MADp = ms->MAD, MAD0p = ms->MAD0;
-    cluster.sync();
-    double V = 0.0, Ar = 0.0;
-    for (int r = 0; r < CL; r++) {
-        const double *p = cluster.map_shared_rank(part_va, r);
-        V += p[0];
-        Ar += p[1];
-    }
     double pm = 0.0;
     if (rank == 0) {
-        // patch and node sort: the cluster's bounds (minima: any order)
         double red[12];
-        unsigned int flag = 0;
-        int sane = 1;
-        for (int q = 0; q < 12; q++) red[q] = 1e300;
-        for (int r = 0; r < CL; r++) {
-            const double *p = cluster.map_shared_rank(part_b, r);
-            for (int q = 0; q < 12; q++) red[q] = fmin(red[q], p[q]);
-            flag |= *cluster.map_shared_rank(&part_flag, r);
-            sane &= *cluster.map_shared_rank(&part_sane, r);
-        }
+        unsigned int flag;
+        int sane;
+        node_bounds(A, mc, threadIdx.x, TPB, red, &flag, &sane);
         sort_patch(A, m, red, sane != 0, flag, gridDim.y, sdyn);
     } else {
+        // this thread's first spring (ls0), its nodes, constants and end velocities
+        const int spring_stride = (CL - 1) * TPB;
+        const int ls0 = tid - TPB;
+        int sn[4] = {0, 0, 0, 0};
+        SpringConst sk{};
+        D3 va{0.0, 0.0, 0.0}, vc{0.0, 0.0, 0.0};
+        if (ls0 < mc.n_springs) {
+            const int sp = mc.spring0 + ls0;
+#pragma unroll
+            for (int q = 0; q < 4; q++) sn[q] = A.spring[4 * (size_t)sp + q];
+            sk = spring_const(A, sp);
+            va = d3(A.vx[sn[0]], A.vy[sn[0]], A.vz[sn[0]]);
+            vc = d3(A.vx[sn[2]], A.vy[sn[2]], A.vz[sn[2]]);
+        }
+        {   // the incidence table for the node forces into L2 meanwhile
+            const char *i0 = reinterpret_cast<const char *>(A.inc + mc.inc0);
+            const char *i1 = reinterpret_cast<const char *>(A.inc + mc.inc0 + 4 * (size_t)mc.n_springs);
+            for (const char *p = i0 + 128 * (size_t)(tid - TPB); p < i1; p += 128 * (size_t)(nth - TPB)) prefetch_l2(p);
+        }
+        const double V0 = ms->V0, A0 = ms->A0, MADp = ms->MAD, MAD0p = ms->MAD0;
+        double *px = reinterpret_cast<double *>(sdyn), *py = px + mc.n_nodes, *pz = py + mc.n_nodes;
+#pragma unroll 4
+        for (int ln = threadIdx.x; ln < mc.n_nodes; ln += TPB) {
+            const int n = mc.node0 + ln;
+            px[ln] = A.x[n];
+            py[ln] = A.y[n];
+            pz[ln] = A.z[n];
+        }
+        __syncthreads();
+        // volume and area (update_spring_network_tet_parameters + total<128>)
+        double pv = 0.0, pa = 0.0;
+        for (int l0 = threadIdx.x; l0 < mc.n_tris; l0 += 4 * TPB) {  // four triangles' indices per round
+            int tn[4][3];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int t = mc.tri0 + (l0 + k * TPB < mc.n_tris ? l0 + k * TPB : 0);
+#pragma unroll
+                for (int q = 0; q < 3; q++) tn[k][q] = A.tri[3 * (size_t)t + q] - mc.node0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (l0 + k * TPB >= mc.n_tris) break;
+                const int na = tn[k][0], nb = tn[k][1], nc = tn[k][2];
+                const D3 a = d3(px[na], py[na], pz[na]), b = d3(px[nb], py[nb], pz[nb]), c = d3(px[nc], py[nc], pz[nc]);
+                const D3 normal = cross(b - a, c - a);
+                pv += dot(normal, tri_centroid(a, b, c)) * kSixth;
+                pa += sqrt(dot(normal, normal)) * 0.5;
+            }
+        }
+        const double V = block_sum(pv, sh), Ar = block_sum(pa, sh);
+        if (threadIdx.x == 0) {
+            part_va[0] = V;
+            part_va[1] = Ar;
+        }
         // spring forces (get_spring_forces_atomics) and the MAD terms of the first n_nodes springs
         const double wr = mc.wlc_ratio;
         const double sfc = (0.25 * wr * wr / ((wr - 1.0) * (wr - 1.0)) - 0.25 + 1.0 / wr);
         const double vol_coef = -1 * mc.volume_modulus * (V / V0 - 1.0) / 6.0;
         const double area_coef = -1 * mc.global_area_modulus * (Ar / A0 - 1.0);
         const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (MADp - MAD0p) / A0;
-        const MembraneScalars cur = *ms;
-        const int ns = (CL - 1) * blockDim.x;
-        for (int ls = tid - (int)blockDim.x; ls < mc.n_springs; ls += ns) {
+        for (int ls = ls0; ls < mc.n_springs; ls += spring_stride) {
             const int sp = mc.spring0 + ls;
-            spring_forces(A, mc, cur, sp, false, sfc, vol_coef, area_coef, mad_coef);
-            if (ls < mc.n_nodes) pm += A.curv[sp] * (A.area[2 * sp] + A.area[2 * sp + 1]) * 1 / 3;
+            if (ls != ls0) {  // springs past the first pass: loaded now
+#pragma unroll
+                for (int q = 0; q < 4; q++) sn[q] = A.spring[4 * (size_t)sp + q];
+                sk = spring_const(A, sp);
+                va = d3(A.vx[sn[0]], A.vy[sn[0]], A.vz[sn[0]]);
+                vc = d3(A.vx[sn[2]], A.vy[sn[2]], A.vz[sn[2]]);
+            }
+            const int la = sn[0] - mc.node0, lb = sn[1] - mc.node0, lc = sn[2] - mc.node0, ld = sn[3] - mc.node0;
+            double area_1, area_2, curvature, angle;
+            spring_core(mc, d3(px[la], py[la], pz[la]), d3(px[lb], py[lb], pz[lb]), d3(px[lc], py[lc], pz[lc]),
+                        d3(px[ld], py[ld], pz[ld]), va, vc, sk, false, sfc, vol_coef, area_coef, mad_coef,
+                        A.contrib + 12 * (size_t)sp, area_1, area_2, curvature, angle);
+            A.area[2 * sp] = area_1;
+            A.area[2 * sp + 1] = area_2;
+            A.curv[sp] = curvature;
+            if (ls < mc.n_nodes) pm += curvature * (area_1 + area_2) * 1 / 3;
         }
     }
     const double bm = block_sum(pm, sh);
     if (threadIdx.x == 0) part_mad[0] = bm;
     cluster.sync();
-    double mad = 0.0;
-    for (int r = 0; r < CL; r++) mad += *cluster.map_shared_rank(part_mad, r);
+
+    // MAD: one warp reads the CL partials (lane r from rank r) and adds them in rank order
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const double v = lane < CL ? *cluster.map_shared_rank(part_mad, lane) : 0.0;
+        double mad = 0.0;
+        for (int r = 0; r < CL; r++) mad += __shfl_sync(0xffffffffu, v, r);
+        if (lane == 0) mad_all = mad;
+    }
     // node forces: each node's contributions in spring order
     for (int ln = tid; ln < mc.n_nodes; ln += nth) {
         const int n = mc.node0 + ln;
         double f[3] = {0.0, 0.0, 0.0};
-        for (int e = A.inc_start[n]; e < A.inc_start[n + 1]; e++) {
-            const int code = __ldg(A.inc + e);
-            const double *o = A.contrib + 12 * (size_t)(code >> 2) + 3 * (code & 3);
-            f[0] += o[0]; f[1] += o[1]; f[2] += o[2];
+        const int e0 = A.inc_start[n], e1 = A.inc_start[n + 1];
+        for (int c0 = e0; c0 < e1; c0 += 8) {
+            int code[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) code[q] = (c0 + q < e1) ? __ldg(A.inc + c0 + q) : -1;
+            double d[8][3];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (code[q] >= 0) {  // written by other CTAs of this launch: L2 loads
+                    const double *o = A.contrib + 12 * (size_t)(code[q] >> 2) + 3 * (code[q] & 3);
+                    d[q][0] = __ldcg(o);
+                    d[q][1] = __ldcg(o + 1);
+                    d[q][2] = __ldcg(o + 2);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (code[q] >= 0) { f[0] += d[q][0]; f[1] += d[q][1]; f[2] += d[q][2]; }
         }
         A.fx[n] = f[0];
         A.fy[n] = f[1];
         A.fz[n] = f[2];
     }
+    __syncthreads();
     if (rank == 0 && threadIdx.x == 0) {
+        const double *va = cluster.map_shared_rank(part_va, 1);  // V and A as every rank 1.. formed them
+        const double V = va[0], Ar = va[1];
         ms->Vc = V;
         ms->Ac = Ar;
         ms->V = V;
         ms->A = Ar;
-        ms->MAD = mad / Ar;
+        ms->MAD = mad_all / Ar;
     }
     cluster.sync();  // no CTA leaves while another may still read its shared memory
+}
+
+size_t step_smem_bytes(int sort_capacity, int max_nodes) {
+    const size_t sort = sort_smem_bytes(sort_capacity), pos = 3 * sizeof(double) * (size_t)(max_nodes > 0 ? max_nodes : 1);
+    return sort > pos ? sort : pos;
 }
 
 // ---- M5: spread as a per-cell reduction over the sorted nodes -------------
@@ -1241,12 +1411,22 @@ __global__ void k_interior_viscosity(ViscArgs a) {
 
 }  // namespace
 
-void membrane_prepare(int sort_capacity) {
+namespace {
+template <int CL, int TPB> void prepare_step(int smem) {
+    cudaFuncSetAttribute(k_mem_step<CL, TPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (CL > 8) cudaFuncSetAttribute(k_mem_step<CL, TPB>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+}  // namespace
+
+bool membrane_cluster_fits(int max_nodes) { return max_nodes <= kStepMaxNodes; }
+
+void membrane_prepare(int sort_capacity, int max_nodes) {
     const size_t smem = sort_smem_bytes(sort_capacity);
     cudaFuncSetAttribute(k_mem_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_mem_step<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_mem_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_mem_step<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (!membrane_cluster_fits(max_nodes)) return;
+    const int fs = (int)step_smem_bytes(sort_capacity, max_nodes);
+    prepare_step<8, kStepThreads>(fs);
+    prepare_step<16, kStepThreads>(fs);
 }
 
 namespace {
@@ -1299,8 +1479,10 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     const dim3 spread_grid(a.spread_blocks);
     if (a.force_cluster == 8 || a.force_cluster == 16) {
         // totals, sort, spring and node forces as one cluster per membrane, then the spread
-        if (a.force_cluster == 16) launch_hi(k_mem_step<16>, dim3(16, a.n_membranes), dim3(kStepThreads), smem, s, a, 16);
-        else launch_hi(k_mem_step<8>, dim3(8, a.n_membranes), dim3(kStepThreads), smem, s, a, 8);
+        const size_t fs = step_smem_bytes(a.sort_capacity, a.max_nodes);
+        const dim3 grid(a.force_cluster, a.n_membranes), block(kStepThreads);
+        if (a.force_cluster == 16) launch_hi(k_mem_step<16, kStepThreads>, grid, block, fs, s, a, 16);
+        else launch_hi(k_mem_step<8, kStepThreads>, grid, block, fs, s, a, 8);
         if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, spread_grid, dim3(256), 0, s, a);
         else launch_hi(k_mem_spread<2>, spread_grid, dim3(256), 0, s, a);
         return 3;

@@ -556,7 +556,8 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     }
     while (cap < maxn) cap <<= 1;
     ma.sort_capacity = cap;
-    membrane_prepare(cap);
+    ma.max_nodes = maxn;
+    membrane_prepare(cap, maxn);
     // node -> (spring, slot) incidence in spring order
     const int N = s->total_nodes, S = s->total_springs;
     std::vector<int> inc_start(N + 1, 0), inc(4 * (size_t)S);
@@ -1449,6 +1450,9 @@ extern "C" int lbfs_set_launch_shape(lbfs_solver *s, const lbfs_launch_shape *sh
     if (!s || !shape) return set_error(LBFS_ERR_ARG, "null argument");
     int rc = check_shape(*shape);
     if (rc) return rc;
+    if (shape->membrane_cluster != 0 && s->n_membranes > 0 && !membrane_cluster_fits(s->ma.max_nodes))
+        return set_error(LBFS_ERR_ARG, "launch shape: membrane_cluster 8 or 16 holds membranes of at most 8192 "
+                                       "nodes in shared memory");
     if (s->fp32) shape_to_args<float>(s, *shape);
     else shape_to_args<double>(s, *shape);
     drop_graph(s);
@@ -2142,7 +2146,8 @@ int autotune_steps(lbfs_solver *s, int reps, lbfs_launch_shape *out, bool fp32) 
         {&lbfs_launch_shape::spread_blocks,
          membranes ? std::vector<int>{148, 296, 592, 1184, 2368} : std::vector<int>{}},
         {&lbfs_launch_shape::flux_chunks, s->chunkable ? std::vector<int>{1, 2, 4, 8} : std::vector<int>{}},
-        {&lbfs_launch_shape::membrane_cluster, membranes ? std::vector<int>{0, 8, 16} : std::vector<int>{}},
+        {&lbfs_launch_shape::membrane_cluster,
+         membranes && membrane_cluster_fits(s->ma.max_nodes) ? std::vector<int>{0, 8, 16} : std::vector<int>{}},
     };
     lbfs_launch_shape cur = fp32 ? args_to_shape<float>(s) : args_to_shape<double>(s);
     double best = 0;
