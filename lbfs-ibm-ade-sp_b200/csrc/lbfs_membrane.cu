@@ -68,6 +68,15 @@ __device__ __forceinline__ D3 tri_centroid(D3 a, D3 b, D3 c) {
     return {(a.x + b.x + c.x) * kThird, (a.y + b.y + c.y) * kThird, (a.z + b.z + c.z) * kThird};
 }
 
+// Programmatic dependent launch: a kernel of the membrane chain lets the next
+// one be scheduled as soon as all its CTAs have started (pdl_trigger), and the
+// next one, launched with the programmatic-serialization attribute, waits in
+// pdl_wait until this grid has completed and its writes are visible; what it
+// does before the wait reads only data no kernel of the step writes.  Without
+// the attribute the wait returns at once.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Deterministic block reductions: warp shuffle tree, then the warp results
 // in warp order by one thread.  `sh` holds 33 doubles.
 __device__ double block_sum(double v, double *sh) {
@@ -440,6 +449,7 @@ __global__ void __launch_bounds__(256) k_mem_tables(MembraneArgs A) {
 // ---- M1: IBM interpolation + advection, one warp per node ----------------
 template <typename R>
 __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
+    pdl_trigger();
     const int lane = threadIdx.x & 31;
     const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (n >= A.total_nodes) return;
@@ -510,8 +520,10 @@ __global__ void __launch_bounds__(256) k_mem_advect(MembraneArgs A) {
 constexpr int kTotalsThreads = 512;
 __global__ void __launch_bounds__(kTotalsThreads) k_mem_totals(MembraneArgs A) {
     __shared__ double sh[33];
+    pdl_trigger();
     const int m = blockIdx.x;
     const MembraneConst mc = A.mc[m];
+    pdl_wait();
     double pv = 0.0, pa = 0.0;
     for (int l0 = threadIdx.x; l0 < mc.n_tris; l0 += 2 * blockDim.x) {  // two triangles' loads per round
         int tn[2][3];
@@ -545,6 +557,8 @@ __global__ void __launch_bounds__(kTotalsThreads) k_mem_totals(MembraneArgs A) {
 __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
     __shared__ double sh[33];
     __shared__ bool last_block;
+    pdl_trigger();
+    pdl_wait();
     const int m = blockIdx.y;
     const MembraneConst mc = A.mc[m];
     const int first = blockIdx.x * blockDim.x;
@@ -598,6 +612,8 @@ __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
 
 // ---- M3: node forces, one thread per node, contributions in spring order ----
 __global__ void __launch_bounds__(128) k_mem_nodeforce(MembraneArgs A) {
+    pdl_trigger();
+    pdl_wait();
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.total_nodes) return;
     double f[3] = {0.0, 0.0, 0.0};
@@ -937,11 +953,14 @@ __global__ void __launch_bounds__(TPB) k_mem_step(MembraneArgs A) {
     const int nth = CL * TPB, tid = rank * TPB + threadIdx.x;
     const MembraneConst mc = A.mc[m];
     MembraneScalars *ms = A.ms + m;
+    // no early trigger: the spread behind it is a full-GPU grid whose waiting
+    // blocks would hold SMs the fluid kernels use; it launches at completion
     double pm = 0.0;
     if (rank == 0) {
         double red[12];
         unsigned int flag;
         int sane;
+        pdl_wait();
         node_bounds(A, mc, threadIdx.x, TPB, red, &flag, &sane);
         sort_patch(A, m, red, sane != 0, flag, gridDim.y, sdyn);
     } else {
@@ -951,11 +970,14 @@ __global__ void __launch_bounds__(TPB) k_mem_step(MembraneArgs A) {
         int sn[4] = {0, 0, 0, 0};
         SpringConst sk{};
         D3 va{0.0, 0.0, 0.0}, vc{0.0, 0.0, 0.0};
-        if (ls0 < mc.n_springs) {
+        if (ls0 < mc.n_springs) {  // spring tables: not written during a step
             const int sp = mc.spring0 + ls0;
 #pragma unroll
             for (int q = 0; q < 4; q++) sn[q] = A.spring[4 * (size_t)sp + q];
             sk = spring_const(A, sp);
+        }
+        pdl_wait();  // the advected positions and velocities
+        if (ls0 < mc.n_springs) {
             va = d3(A.vx[sn[0]], A.vy[sn[0]], A.vz[sn[0]]);
             vc = d3(A.vx[sn[2]], A.vy[sn[2]], A.vz[sn[2]]);
         }
@@ -1091,6 +1113,7 @@ size_t step_smem_bytes(int sort_capacity, int max_nodes) {
 // the loads of one contribution do not wait on each other.
 template <int S>
 __global__ void __launch_bounds__(256) k_mem_spread(MembraneArgs A) {
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int M = A.n_membranes;
     const int total = __ldg(A.cell_start + M);
@@ -1435,19 +1458,24 @@ namespace {
 // stream, so its blocks are placed ahead of pending fluid blocks.
 template <typename... Args>
 void launch_hi(void (*kernel)(Args...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const MembraneArgs &a,
-               int cluster_x = 0) {
+               int cluster_x = 0, bool after_kernel = false) {
     int lo = 0, hi = 0;
     cudaDeviceGetStreamPriorityRange(&lo, &hi);
-    cudaLaunchAttribute attr[2];
+    cudaLaunchAttribute attr[3];
     attr[0].id = cudaLaunchAttributePriority;
     attr[0].val.priority = hi;
     int n_attr = 1;
     if (cluster_x > 0) {  // thread-block clusters of cluster_x CTAs along x
-        attr[1].id = cudaLaunchAttributeClusterDimension;
-        attr[1].val.clusterDim.x = cluster_x;
-        attr[1].val.clusterDim.y = 1;
-        attr[1].val.clusterDim.z = 1;
-        n_attr = 2;
+        attr[n_attr].id = cudaLaunchAttributeClusterDimension;
+        attr[n_attr].val.clusterDim.x = cluster_x;
+        attr[n_attr].val.clusterDim.y = 1;
+        attr[n_attr].val.clusterDim.z = 1;
+        n_attr++;
+    }
+    if (after_kernel) {  // directly behind a kernel of the chain on the same stream: programmatic launch
+        attr[n_attr].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[n_attr].val.programmaticStreamSerializationAllowed = 1;
+        n_attr++;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
@@ -1481,10 +1509,10 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
         // totals, sort, spring and node forces as one cluster per membrane, then the spread
         const size_t fs = step_smem_bytes(a.sort_capacity, a.max_nodes);
         const dim3 grid(a.force_cluster, a.n_membranes), block(kStepThreads);
-        if (a.force_cluster == 16) launch_hi(k_mem_step<16, kStepThreads>, grid, block, fs, s, a, 16);
-        else launch_hi(k_mem_step<8, kStepThreads>, grid, block, fs, s, a, 8);
-        if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, spread_grid, dim3(256), 0, s, a);
-        else launch_hi(k_mem_spread<2>, spread_grid, dim3(256), 0, s, a);
+        if (a.force_cluster == 16) launch_hi(k_mem_step<16, kStepThreads>, grid, block, fs, s, a, 16, true);
+        else launch_hi(k_mem_step<8, kStepThreads>, grid, block, fs, s, a, 8, true);
+        if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, spread_grid, dim3(256), 0, s, a, 0, true);
+        else launch_hi(k_mem_spread<2>, spread_grid, dim3(256), 0, s, a, 0, true);
         return 3;
     }
     // the node sort needs only the advected positions: side stream
@@ -1496,9 +1524,9 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, side ? s_side : s, a);
     if (side) cudaEventRecord(ev_sorted, s_side);
     // separate kernels for the totals, the spring forces and the node forces
-    launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a);
-    launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a);
-    launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a);
+    launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a, 0, true);
+    launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a, 0, true);
+    launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a, 0, true);
     const int n = 6;
     // the spread reads the sorted records and the node forces
     if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
