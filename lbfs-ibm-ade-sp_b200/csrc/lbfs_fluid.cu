@@ -47,6 +47,7 @@ __device__ __forceinline__ Vec4<R> ghost_state(const FluidArgs<R> &a, int b, con
 
 template <typename R, int TB>
 __global__ void __launch_bounds__(TB, TB == 128 ? 5 : 1) k_cell_gradients(FluidArgs<R> a, int begin, int end) {
+    pdl_trigger();  // the interior-face kernel may be scheduled behind the last wave
     const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= end) return;
     const Vec4<R> own = a.state[i];
@@ -612,9 +613,11 @@ __global__ void __launch_bounds__(TB, 640 / TB) k_face_flux(FluidArgs<R> a, Face
 // the z faces: one axis per warp at a time.
 template <typename R, int TB>
 __global__ void __launch_bounds__(TB, 640 / TB) k_face_flux_tiles(FluidArgs<R> a, int tile0) {
+    pdl_trigger();
     const int *tp = a.flux_tiles + 3 * (tile0 + (int)blockIdx.x);
     const int f0x = __ldg(tp), f0y = __ldg(tp + 1), f0z = __ldg(tp + 2);
     const int f1x = __ldg(tp + 3), f1y = __ldg(tp + 4), f1z = __ldg(tp + 5);
+    pdl_wait();  // the gradients
     for (int f = f0x + (int)threadIdx.x; f < f1x; f += TB) a.flux[f] = axis_face_flux<R, 0>(a, f);
     for (int f = f0y + (int)threadIdx.x; f < f1y; f += TB) a.flux[f] = axis_face_flux<R, 1>(a, f);
     for (int f = f0z + (int)threadIdx.x; f < f1z; f += TB) a.flux[f] = axis_face_flux<R, 2>(a, f);
@@ -627,6 +630,8 @@ __global__ void __launch_bounds__(TB, 640 / TB) k_face_flux_tiles(FluidArgs<R> a
 // mesh's internal faces, which OpenFOAM orders by owner, form one range).
 template <typename R, int TB>
 __global__ void __launch_bounds__(TB, 512 / TB) k_face_flux_general_tiles(FluidArgs<R> a, int tile0) {
+    pdl_trigger();
+    pdl_wait();  // the gradients
     const int *tp = a.flux_tiles + 3 * (tile0 + (int)blockIdx.x);
 #pragma unroll 1
     for (int r = 0; r < 3; r++) {
@@ -698,6 +703,7 @@ template <typename R, int TB>
 __global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
     __shared__ double sh[4][TB / 32];
     __shared__ bool last_block;
+    pdl_wait();  // the face fluxes
     double sq[4] = {0, 0, 0, 0};
     unsigned int flag = 0;
     // the step: constant, or the minimum per-cell step, or each cell's own (LBFS_DT_LOCAL)
@@ -870,22 +876,42 @@ template <typename R> void launch_fluid_flux_axis_ranges(const FluidArgs<R> &a, 
     else if (tb == 256) k_face_flux<R, 256><<<g, 256, 0, s>>>(a, r);
     else k_face_flux<R, 128><<<g, 128, 0, s>>>(a, r);
 }
-template <typename R> void launch_fluid_flux_tiles(const FluidArgs<R> &a, int tile0, int tile1, cudaStream_t s) {
+// A launch with the programmatic-serialization attribute when `pdl` (the
+// kernel directly behind the kernel whose output it reads, on the same stream).
+template <typename... KArgs, typename... Args>
+void launch_maybe_pdl(void (*kernel)(KArgs...), int g, int tb, cudaStream_t s, bool pdl, Args... args) {
+    if (!pdl) {
+        kernel<<<g, tb, 0, s>>>(args...);
+        return;
+    }
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(g);
+    cfg.blockDim = dim3(tb);
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+template <typename R>
+void launch_fluid_flux_tiles(const FluidArgs<R> &a, int tile0, int tile1, cudaStream_t s, bool pdl) {
     const int g = tile1 - tile0;
     if (g <= 0) return;
     if (!a.axis_aligned) {
-        if (a.tb_gen == 64) k_face_flux_general_tiles<R, 64><<<g, 64, 0, s>>>(a, tile0);
-        else if (a.tb_gen == 256) k_face_flux_general_tiles<R, 256><<<g, 256, 0, s>>>(a, tile0);
-        else k_face_flux_general_tiles<R, 128><<<g, 128, 0, s>>>(a, tile0);
+        if (a.tb_gen == 64) launch_maybe_pdl(k_face_flux_general_tiles<R, 64>, g, 64, s, pdl, a, tile0);
+        else if (a.tb_gen == 256) launch_maybe_pdl(k_face_flux_general_tiles<R, 256>, g, 256, s, pdl, a, tile0);
+        else launch_maybe_pdl(k_face_flux_general_tiles<R, 128>, g, 128, s, pdl, a, tile0);
         return;
     }
-    if (a.tb_flux == 64) k_face_flux_tiles<R, 64><<<g, 64, 0, s>>>(a, tile0);
-    else if (a.tb_flux == 256) k_face_flux_tiles<R, 256><<<g, 256, 0, s>>>(a, tile0);
-    else k_face_flux_tiles<R, 128><<<g, 128, 0, s>>>(a, tile0);
+    if (a.tb_flux == 64) launch_maybe_pdl(k_face_flux_tiles<R, 64>, g, 64, s, pdl, a, tile0);
+    else if (a.tb_flux == 256) launch_maybe_pdl(k_face_flux_tiles<R, 256>, g, 256, s, pdl, a, tile0);
+    else launch_maybe_pdl(k_face_flux_tiles<R, 128>, g, 128, s, pdl, a, tile0);
 }
-template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s) {
+template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s, bool pdl) {
     if (a.flux_tiles) {  // interior faces by tiles (axis-aligned or general-normal kernel)
-        launch_fluid_flux_tiles<R>(a, 0, a.n_tiles, s);
+        launch_fluid_flux_tiles<R>(a, 0, a.n_tiles, s, pdl);
         return;
     }
     const FaceRanges r = {{0, a.nfx, a.nfx + a.nfy}, {a.nfx, a.nfy, a.ni - a.nfx - a.nfy}};
@@ -930,11 +956,11 @@ template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t
     launch_fluid_flux_axis<R>(a, s);
     launch_fluid_flux_general<R>(a, s);
 }
-template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s) {
+template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s, bool pdl) {
     const int tb = a.tb_update, g = k3_grid(a);
-    if (tb == 128) k_cell_update<R, 128><<<g, 128, 0, s>>>(a);
-    else if (tb == 512) k_cell_update<R, 512><<<g, 512, 0, s>>>(a);
-    else k_cell_update<R, 256><<<g, 256, 0, s>>>(a);
+    if (tb == 128) launch_maybe_pdl(k_cell_update<R, 128>, g, 128, s, pdl, a);
+    else if (tb == 512) launch_maybe_pdl(k_cell_update<R, 512>, g, 512, s, pdl, a);
+    else launch_maybe_pdl(k_cell_update<R, 256>, g, 256, s, pdl, a);
 }
 
 template <typename R> void launch_fluid_cfl(const FluidArgs<R> &a, cudaStream_t s) {
@@ -955,21 +981,21 @@ template void launch_unpack_state<float>(const FluidArgs<float> &, double *, cud
 
 template void launch_fluid_gradients<double>(const FluidArgs<double> &, cudaStream_t);
 template void launch_fluid_flux<double>(const FluidArgs<double> &, cudaStream_t);
-template void launch_fluid_flux_axis<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_flux_axis<double>(const FluidArgs<double> &, cudaStream_t, bool);
 template void launch_fluid_flux_general<double>(const FluidArgs<double> &, cudaStream_t);
-template void launch_fluid_flux_axis<float>(const FluidArgs<float> &, cudaStream_t);
+template void launch_fluid_flux_axis<float>(const FluidArgs<float> &, cudaStream_t, bool);
 template void launch_fluid_flux_general<float>(const FluidArgs<float> &, cudaStream_t);
-template void launch_fluid_update<double>(const FluidArgs<double> &, cudaStream_t);
+template void launch_fluid_update<double>(const FluidArgs<double> &, cudaStream_t, bool);
 template void launch_fluid_gradients<float>(const FluidArgs<float> &, cudaStream_t);
 template void launch_fluid_flux<float>(const FluidArgs<float> &, cudaStream_t);
-template void launch_fluid_update<float>(const FluidArgs<float> &, cudaStream_t);
+template void launch_fluid_update<float>(const FluidArgs<float> &, cudaStream_t, bool);
 template void launch_fluid_cfl<double>(const FluidArgs<double> &, cudaStream_t);
 template void launch_fluid_gradients_range<double>(const FluidArgs<double> &, int, int, cudaStream_t);
 template void launch_fluid_gradients_range<float>(const FluidArgs<float> &, int, int, cudaStream_t);
 template void launch_fluid_flux_axis_ranges<double>(const FluidArgs<double> &, const FaceRanges &, cudaStream_t);
 template void launch_fluid_flux_axis_ranges<float>(const FluidArgs<float> &, const FaceRanges &, cudaStream_t);
-template void launch_fluid_flux_tiles<double>(const FluidArgs<double> &, int, int, cudaStream_t);
-template void launch_fluid_flux_tiles<float>(const FluidArgs<float> &, int, int, cudaStream_t);
+template void launch_fluid_flux_tiles<double>(const FluidArgs<double> &, int, int, cudaStream_t, bool);
+template void launch_fluid_flux_tiles<float>(const FluidArgs<float> &, int, int, cudaStream_t, bool);
 template void launch_fluid_cfl<float>(const FluidArgs<float> &, cudaStream_t);
 
 }  // namespace lbfs

@@ -77,6 +77,15 @@ __device__ __forceinline__ R feq_dev(int k, R rho, R u, R v, R w, R rho0, R qsca
     return lattice_w<R>(k) * (rho + (rho + rho0) * X);
 }
 
+// Programmatic dependent launch: a kernel lets the next one on its stream be
+// scheduled as soon as all its CTAs have started (pdl_trigger), and the next
+// one, launched with the programmatic-serialization attribute, waits in
+// pdl_wait until this grid has completed and its writes are visible; before the
+// wait it touches nothing a kernel of the step writes.  Without the attribute
+// the wait returns at once.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 }  // namespace lbfs
 
 namespace lbfs {

@@ -18,11 +18,15 @@ template <typename R> void launch_fluid_gradients_range(const FluidArgs<R> &a, i
 template <typename R> void launch_fluid_flux_axis_ranges(const FluidArgs<R> &a, const FaceRanges &r, cudaStream_t s);
 // K2 over the faces owned by tiles [tile0, tile1) of a.flux_tiles (axis-aligned meshes whose faces are
 // ordered by owner within each axis)
-template <typename R> void launch_fluid_flux_tiles(const FluidArgs<R> &a, int tile0, int tile1, cudaStream_t s);
+template <typename R>
+void launch_fluid_flux_tiles(const FluidArgs<R> &a, int tile0, int tile1, cudaStream_t s, bool pdl = false);
 template <typename R> void launch_fluid_flux(const FluidArgs<R> &a, cudaStream_t s);
-template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s);
+// pdl: launched with the programmatic-serialization attribute, directly behind
+// the gradient kernel on the same stream
+template <typename R> void launch_fluid_flux_axis(const FluidArgs<R> &a, cudaStream_t s, bool pdl = false);
 template <typename R> void launch_fluid_flux_general(const FluidArgs<R> &a, cudaStream_t s);
-template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s);
+// pdl: launched with the programmatic-serialization attribute behind the face kernels
+template <typename R> void launch_fluid_update(const FluidArgs<R> &a, cudaStream_t s, bool pdl = false);
 // per-cell step and its minimum (time stepping other than constant)
 template <typename R> void launch_fluid_cfl(const FluidArgs<R> &a, cudaStream_t s);
 // stage = 4 planes of n_cells doubles (rho, u, v, w); pack also resets soln_t1

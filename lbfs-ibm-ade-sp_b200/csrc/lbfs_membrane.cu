@@ -68,15 +68,6 @@ __device__ __forceinline__ D3 tri_centroid(D3 a, D3 b, D3 c) {
     return {(a.x + b.x + c.x) * kThird, (a.y + b.y + c.y) * kThird, (a.z + b.z + c.z) * kThird};
 }
 
-// Programmatic dependent launch: a kernel of the membrane chain lets the next
-// one be scheduled as soon as all its CTAs have started (pdl_trigger), and the
-// next one, launched with the programmatic-serialization attribute, waits in
-// pdl_wait until this grid has completed and its writes are visible; what it
-// does before the wait reads only data no kernel of the step writes.  Without
-// the attribute the wait returns at once.
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
 // Deterministic block reductions: warp shuffle tree, then the warp results
 // in warp order by one thread.  `sh` holds 33 doubles.
 __device__ double block_sum(double v, double *sh) {

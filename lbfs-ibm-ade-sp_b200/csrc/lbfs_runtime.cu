@@ -810,9 +810,12 @@ struct PhaseMark {
 // the load-latency-bound gradients of the next; the boundary faces (which read
 // ghost gradients) follow every K1, and the handle's stream joins the second.
 //
-// Unpipelined, the interior axis faces still run on the second stream beside
-// the boundary faces (a short kernel of long threads that would otherwise add
-// its whole latency after the axis faces).
+// Unpipelined, the boundary faces (a short kernel of long threads that would
+// otherwise add its whole latency after the interior faces) run on the second
+// stream beside the interior faces, which follow the gradients on the
+// handle's stream as a programmatic dependent launch (their CTAs are placed
+// behind the gradients' last wave and wait there for its results) unless
+// per-kernel events sit between the two.
 template <typename R> int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n) {
     const int K = a.axis_aligned ? s->flux_chunks : 1;
     if (K <= 1) {
@@ -823,11 +826,13 @@ template <typename R> int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n)
             if (fork) {
                 LBFS_CUDA(cudaEventRecord(s->ev_chunk[0], s->stream));
                 LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_chunk[0], 0));
-                launch_fluid_flux_axis<R>(a, s->stream4);
+                launch_fluid_flux_general<R>(a, s->stream4);
                 LBFS_CUDA(cudaEventRecord(s->ev_flux, s->stream4));
+                launch_fluid_flux_axis<R>(a, s->stream, !s->kernel_events);
+                LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_flux, 0));
+            } else {
+                launch_fluid_flux_general<R>(a, s->stream);
             }
-            launch_fluid_flux_general<R>(a, s->stream);
-            if (fork) LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_flux, 0));
         }
         *n += 2;
         return LBFS_OK;
@@ -886,7 +891,8 @@ template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *la
         int rc = enqueue_k1_k2<R>(s, a, &n);
         if (rc) return rc;
     }
-    { PhaseMark m(s, 3, s->stream); launch_fluid_update<R>(a, s->stream); }
+    // behind the face kernels as a programmatic dependent launch (its wait also covers the joined streams)
+    { PhaseMark m(s, 3, s->stream); launch_fluid_update<R>(a, s->stream, !s->kernel_events); }
     n += 1;
     if (s->profiling) {
         LBFS_CUDA(record_event(s->ev_phase[5][1], s->stream));
