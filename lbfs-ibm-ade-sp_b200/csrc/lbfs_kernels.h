@@ -117,9 +117,10 @@ void membrane_prepare(int sort_capacity, int max_nodes);
 bool membrane_cluster_fits(int max_nodes);
 // Enqueues the membrane kernels of the current mode on `s` (the node sort on
 // `s_side`, joined back before the spread, when the side stream and its two
-// events are given); returns the launch count.
+// events are given); returns the launch count.  without_spread: everything
+// but the spread, which the caller launches (launch_membrane_spread).
 int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side = nullptr,
-                    cudaEvent_t ev_advected = nullptr, cudaEvent_t ev_sorted = nullptr);
+                    cudaEvent_t ev_advected = nullptr, cudaEvent_t ev_sorted = nullptr, bool without_spread = false);
 
 // Per membrane, the y-z binning of its triangles for the interior test: bins
 // of size >= every triangle's y-z extent and >= 4 delta_h over the membrane's

@@ -1480,7 +1480,7 @@ void launch_hi(void (*kernel)(Args...), dim3 grid, dim3 block, size_t smem, cuda
 }  // namespace
 
 int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, cudaEvent_t ev_advected,
-                    cudaEvent_t ev_sorted) {
+                    cudaEvent_t ev_sorted, bool without_spread) {
     const size_t smem = sort_smem_bytes(a.sort_capacity);
     const dim3 spring_grid((a.max_springs + 127) / 128, a.n_membranes);
     if (a.mode == kModeReference) {  // stress-free reference pass
@@ -1502,6 +1502,7 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
         const dim3 grid(a.force_cluster, a.n_membranes), block(kStepThreads);
         if (a.force_cluster == 16) launch_hi(k_mem_step<16, kStepThreads>, grid, block, fs, s, a, 16, true);
         else launch_hi(k_mem_step<8, kStepThreads>, grid, block, fs, s, a, 8, true);
+        if (without_spread) return 2;
         if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, spread_grid, dim3(256), 0, s, a, 0, true);
         else launch_hi(k_mem_spread<2>, spread_grid, dim3(256), 0, s, a, 0, true);
         return 3;
@@ -1521,6 +1522,7 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     const int n = 6;
     // the spread reads the sorted records and the node forces
     if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
+    if (without_spread) return n - 1;
     if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, spread_grid, dim3(256), 0, s, a);
     else launch_hi(k_mem_spread<2>, spread_grid, dim3(256), 0, s, a);
     return n;

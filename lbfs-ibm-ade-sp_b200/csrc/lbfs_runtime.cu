@@ -816,7 +816,19 @@ struct PhaseMark {
 // handle's stream as a programmatic dependent launch (their CTAs are placed
 // behind the gradients' last wave and wait there for its results) unless
 // per-kernel events sit between the two.
-template <typename R> int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n) {
+//
+// spread_here: the membrane chain (on its own stream, recorded in ev_join)
+// left its spread out; it runs on the boundary-face stream after the boundary
+// faces, so the cell update depends on two kernels, the interior faces (a
+// programmatic edge, which lets it be placed behind their last wave) and that
+// stream's last one, as without membranes.  With the membrane stream joined to
+// the handle's stream directly the update started only after the interior
+// faces had finished.
+template <typename R> bool spread_with_faces(const lbfs_solver *s, const FluidArgs<R> &a) {
+    const int K = a.axis_aligned ? s->flux_chunks : 1;
+    return s->n_membranes > 0 && K <= 1 && (a.axis_aligned || a.flux_tiles) && !s->kernel_events;
+}
+template <typename R> int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n, bool spread_here) {
     const int K = a.axis_aligned ? s->flux_chunks : 1;
     if (K <= 1) {
         { PhaseMark m(s, 1, s->stream); launch_fluid_gradients<R>(a, s->stream); }
@@ -827,6 +839,11 @@ template <typename R> int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n)
                 LBFS_CUDA(cudaEventRecord(s->ev_chunk[0], s->stream));
                 LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_chunk[0], 0));
                 launch_fluid_flux_general<R>(a, s->stream4);
+                if (spread_here) {
+                    LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_join, 0));
+                    launch_membrane_spread(s->ma, s->stream4);
+                    *n += 1;
+                }
                 LBFS_CUDA(cudaEventRecord(s->ev_flux, s->stream4));
                 launch_fluid_flux_axis<R>(a, s->stream, !s->kernel_events);
                 LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_flux, 0));
@@ -879,16 +896,20 @@ template <typename R> int enqueue_step(lbfs_solver *s, bool visc_update, int *la
             { PhaseMark m(s, 2, s->stream); launch_fluid_flux<R>(a, s->stream); }
             n += 3;
         } else {
+            const bool spread_here = spread_with_faces<R>(s, a);
             LBFS_CUDA(cudaEventRecord(s->ev_fork, s->stream));
             LBFS_CUDA(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
-            { PhaseMark m(s, 0, s->stream2); n += launch_membrane(s->ma, s->stream2, s->stream3, s->ev_advected, s->ev_sorted); }
+            {
+                PhaseMark m(s, 0, s->stream2);
+                n += launch_membrane(s->ma, s->stream2, s->stream3, s->ev_advected, s->ev_sorted, spread_here);
+            }
             LBFS_CUDA(cudaEventRecord(s->ev_join, s->stream2));
-            int rc = enqueue_k1_k2<R>(s, a, &n);
+            int rc = enqueue_k1_k2<R>(s, a, &n, spread_here);
             if (rc) return rc;
-            LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
+            if (!spread_here) LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
         }
     } else {
-        int rc = enqueue_k1_k2<R>(s, a, &n);
+        int rc = enqueue_k1_k2<R>(s, a, &n, false);
         if (rc) return rc;
     }
     // behind the face kernels as a programmatic dependent launch (its wait also covers the joined streams)
