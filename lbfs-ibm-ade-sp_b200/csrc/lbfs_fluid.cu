@@ -610,9 +610,10 @@ __global__ void __launch_bounds__(TB, 640 / TB) k_face_flux(FluidArgs<R> a, Face
 // (tiles[3 t + axis] = first face of that axis owned by tile t) -- so the
 // tile's cell states and gradients come from DRAM once for all three axes
 // instead of once per axis sweep.  Warps take the x faces, then the y, then
-// the z faces: one axis per warp at a time.
+// the z faces: one axis per warp at a time.  Load-latency bound: FP64 fits 96
+// registers (20 warps per SM; at 80 it spills), FP32 64 (32 warps per SM).
 template <typename R, int TB>
-__global__ void __launch_bounds__(TB, 640 / TB) k_face_flux_tiles(FluidArgs<R> a, int tile0) {
+__global__ void __launch_bounds__(TB, (sizeof(R) == 4 ? 1024 : 640) / TB) k_face_flux_tiles(FluidArgs<R> a, int tile0) {
     pdl_trigger();
     const int *tp = a.flux_tiles + 3 * (tile0 + (int)blockIdx.x);
     const int f0x = __ldg(tp), f0y = __ldg(tp + 1), f0z = __ldg(tp + 2);
@@ -628,8 +629,9 @@ __global__ void __launch_bounds__(TB, 640 / TB) k_face_flux_tiles(FluidArgs<R> a
 // takes the faces owned by the TB cells of tile tile0 + b, in up to three
 // face ranges ordered by owner (the generator's x, y, z faces; an imported
 // mesh's internal faces, which OpenFOAM orders by owner, form one range).
+// FP64 at 128 registers (16 warps per SM; fewer spill), FP32 at 80 (24).
 template <typename R, int TB>
-__global__ void __launch_bounds__(TB, 512 / TB) k_face_flux_general_tiles(FluidArgs<R> a, int tile0) {
+__global__ void __launch_bounds__(TB, (sizeof(R) == 4 ? 768 : 512) / TB) k_face_flux_general_tiles(FluidArgs<R> a, int tile0) {
     pdl_trigger();
     pdl_wait();  // the gradients
     const int *tp = a.flux_tiles + 3 * (tile0 + (int)blockIdx.x);
