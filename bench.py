@@ -690,7 +690,8 @@ def main():
         b_ = algorithmic_bytes(mesh, ph)
         gbs = b_ / (fluid[ph] * 1e-3) / 1e9
         kernel_roofline[kn] = {"algorithmic_bytes": b_, "ms": fluid[ph], "achieved_gbs": gbs,
-                               "frac": gbs / peaks["hbm_gbs"]}
+                               "frac": gbs / peaks["hbm_gbs"],
+                               "traffic": read_traffic(kn, f"shear_rbc_{args.n}_fp64")}
 
     def e2e_pass(h):
         """End to end through the C ABI with page-locked host buffers: every step the
