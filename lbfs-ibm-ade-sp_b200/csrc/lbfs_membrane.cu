@@ -514,23 +514,29 @@ __global__ void __launch_bounds__(kTotalsThreads) k_mem_totals(MembraneArgs A) {
     pdl_trigger();
     const int m = blockIdx.x;
     const MembraneConst mc = A.mc[m];
-    pdl_wait();
-    double pv = 0.0, pa = 0.0;
-    for (int l0 = threadIdx.x; l0 < mc.n_tris; l0 += 2 * blockDim.x) {  // two triangles' loads per round
-        int tn[2][3];
+    // four triangles per round; the first round's indices (constant) are loaded
+    // before the wait for the advected positions
+    int tn[4][3];
+    auto load_tris = [&](int l0) {
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < 4; k++) {
             const int t = mc.tri0 + (l0 + k * (int)blockDim.x < mc.n_tris ? l0 + k * (int)blockDim.x : 0);
 #pragma unroll
             for (int q = 0; q < 3; q++) tn[k][q] = A.tri[3 * (size_t)t + q];
         }
-        D3 p[2][3];
+    };
+    load_tris(threadIdx.x);
+    pdl_wait();
+    double pv = 0.0, pa = 0.0;
+    for (int l0 = threadIdx.x; l0 < mc.n_tris; l0 += 4 * blockDim.x) {
+        if (l0 != (int)threadIdx.x) load_tris(l0);
+        D3 p[4][3];
 #pragma unroll
-        for (int k = 0; k < 2; k++)
+        for (int k = 0; k < 4; k++)
 #pragma unroll
             for (int q = 0; q < 3; q++) p[k][q] = d3(A.x[tn[k][q]], A.y[tn[k][q]], A.z[tn[k][q]]);
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < 4; k++) {
             if (l0 + k * (int)blockDim.x >= mc.n_tris) break;
             const D3 a = p[k][0], b = p[k][1], c = p[k][2];
             const D3 normal = cross(b - a, c - a);
@@ -549,7 +555,6 @@ __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
     __shared__ double sh[33];
     __shared__ bool last_block;
     pdl_trigger();
-    pdl_wait();
     const int m = blockIdx.y;
     const MembraneConst mc = A.mc[m];
     const int first = blockIdx.x * blockDim.x;
@@ -562,6 +567,16 @@ __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
     }
     MembraneScalars *ms = A.ms + m;
     const bool initials = A.mode == kModeInitial;
+    // the spring's nodes and stress-free constants (not written during a step)
+    // before the wait for the totals and the advected positions
+    int sn[4] = {0, 0, 0, 0};
+    SpringConst sk{};
+    if (ls < mc.n_springs && !initials) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) sn[q] = A.spring[4 * (size_t)s + q];
+        sk = spring_const(A, s);
+    }
+    pdl_wait();
     const double V = ms->Vc, Ar = ms->Ac;  // k_mem_totals of this launch sequence
     const double V0 = initials ? V * mc.volume_ratio : ms->V0;
     const double A0 = initials ? Ar : ms->A0;
@@ -573,8 +588,20 @@ __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
     const double mad_coef = -1 * 2.0 * mc.global_bending_modulus * (MADp - MAD0p) / A0;
     double pm = 0.0;
     if (ls < mc.n_springs) {
-        MembraneScalars cur = *ms;
-        spring_forces(A, mc, cur, s, initials, sfc, vol_coef, area_coef, mad_coef);
+        if (initials) {
+            MembraneScalars cur = *ms;
+            spring_forces(A, mc, cur, s, initials, sfc, vol_coef, area_coef, mad_coef);
+        } else {
+            const D3 a = d3(A.x[sn[0]], A.y[sn[0]], A.z[sn[0]]), b = d3(A.x[sn[1]], A.y[sn[1]], A.z[sn[1]]);
+            const D3 c = d3(A.x[sn[2]], A.y[sn[2]], A.z[sn[2]]), d = d3(A.x[sn[3]], A.y[sn[3]], A.z[sn[3]]);
+            const D3 va = d3(A.vx[sn[0]], A.vy[sn[0]], A.vz[sn[0]]), vc = d3(A.vx[sn[2]], A.vy[sn[2]], A.vz[sn[2]]);
+            double area_1, area_2, curvature, angle;
+            spring_core(mc, a, b, c, d, va, vc, sk, false, sfc, vol_coef, area_coef, mad_coef, A.contrib + 12 * (size_t)s,
+                        area_1, area_2, curvature, angle);
+            A.area[2 * s] = area_1;
+            A.area[2 * s + 1] = area_2;
+            A.curv[s] = curvature;
+        }
         if (ls < mc.n_nodes) pm = A.curv[s] * (A.area[2 * s] + A.area[2 * s + 1]) * 1 / 3;
     }
     const double part = block_sum(pm, sh);
@@ -604,25 +631,30 @@ __global__ void __launch_bounds__(128) k_mem_springs(MembraneArgs A) {
 // ---- M3: node forces, one thread per node, contributions in spring order ----
 __global__ void __launch_bounds__(128) k_mem_nodeforce(MembraneArgs A) {
     pdl_trigger();
-    pdl_wait();
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.total_nodes) return;
-    double f[3] = {0.0, 0.0, 0.0};
+    // the node's incidence (constant) before the wait for the spring kernel's contributions
     const int e0 = A.inc_start[n], e1 = A.inc_start[n + 1];
-    for (int c0 = e0; c0 < e1; c0 += 8) {
-        int code[8];
+    int code[16];
 #pragma unroll
-        for (int q = 0; q < 8; q++) code[q] = (c0 + q < e1) ? __ldg(A.inc + c0 + q) : -1;
-        double d[8][3];
+    for (int q = 0; q < 16; q++) code[q] = (e0 + q < e1) ? __ldg(A.inc + e0 + q) : -1;
+    pdl_wait();
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int c0 = e0; c0 < e1; c0 += 16) {
+        if (c0 != e0) {
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
+            for (int q = 0; q < 16; q++) code[q] = (c0 + q < e1) ? __ldg(A.inc + c0 + q) : -1;
+        }
+        double d[16][3];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
             if (code[q] >= 0) {
                 const double *o = A.contrib + 12 * (size_t)(code[q] >> 2) + 3 * (code[q] & 3);
                 d[q][0] = o[0]; d[q][1] = o[1]; d[q][2] = o[2];
             }
         }
 #pragma unroll
-        for (int q = 0; q < 8; q++)
+        for (int q = 0; q < 16; q++)
             if (code[q] >= 0) { f[0] += d[q][0]; f[1] += d[q][1]; f[2] += d[q][2]; }
     }
     A.fx[n] = f[0];
