@@ -933,7 +933,10 @@ __device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool
     write_spread_records(A, mc, list);
 }
 
-__global__ void __launch_bounds__(kMembraneThreads) k_mem_sort(MembraneArgs A) {
+// 256 threads: the sort runs on a side stream beside the fluid kernels, off
+// the critical path, and a 1024-thread CTA held a whole SM for its 17 us.
+constexpr int kSortThreads = 256;
+__global__ void __launch_bounds__(kSortThreads) k_mem_sort(MembraneArgs A) {
     extern __shared__ unsigned long long skeys[];  // 2 int arrays of sort_capacity: bins, sorted list
     const int m = blockIdx.x;
     double red[12];
@@ -1545,7 +1548,7 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
         cudaEventRecord(ev_advected, s);
         cudaStreamWaitEvent(s_side, ev_advected, 0);
     }
-    launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, side ? s_side : s, a);
+    launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kSortThreads), smem, side ? s_side : s, a);
     if (side) cudaEventRecord(ev_sorted, s_side);
     // separate kernels for the totals, the spring forces and the node forces
     launch_hi(k_mem_totals, dim3(a.n_membranes), dim3(kTotalsThreads), 0, s, a, 0, true);
@@ -1578,7 +1581,7 @@ void launch_membrane_forces(const MembraneArgs &a, cudaStream_t s) {
 
 void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s) {
     const size_t smem = sort_smem_bytes(a.sort_capacity);
-    launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kMembraneThreads), smem, s, a);
+    launch_hi(k_mem_sort, dim3(a.n_membranes), dim3(kSortThreads), smem, s, a);
 }
 
 void launch_membrane_energies(const MembraneArgs &a, double *out, cudaStream_t s) {
