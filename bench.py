@@ -714,7 +714,33 @@ def main():
                 "d2h_bytes_per_step": 4 * 8 * n, "steps": Ke, "timing": "host wall clock around set_state, step, "
                 "get_state (page-locked host arrays)"}
 
+    def e2e_run(h, steps=100):
+        """End to end the way the reference's own loop uses its solver (Solver_gpu.cu's time loop
+        behind General_Purpose_Solver_mk_i): the state host -> device once, every step followed by
+        the device -> host read of its residual norms (the convergence check), the state back once;
+        host wall clock over the whole call, page-locked host arrays."""
+        n = mesh.n_cells
+        host = [torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+        for hh, a in zip(host, h.state()):
+            hh[:] = a
+        h.set_profiling(False)
+        res = torch.empty(4, dtype=torch.float64, pin_memory=True).numpy()
+        barrier()
+        t0 = time.perf_counter()
+        _abi.check(_abi.lib().lbfs_set_state(h._h, *[_abi.ptr(x) for x in host]))
+        for _ in range(steps):
+            h.step(1, graph=True)
+            _abi.check(_abi.lib().lbfs_get_residuals(h._h, _abi.ptr(res)))
+        _abi.check(_abi.lib().lbfs_get_state(h._h, *[_abi.ptr(x) for x in host]))
+        barrier()
+        te = max_over_ranks(time.perf_counter() - t0, device="cuda")
+        return {"value": n * steps * world / te / 1e6, "unit": METRIC, "h2d_bytes_per_step": 4 * 8 * n / steps,
+                "d2h_bytes_per_step": 4 * 8 * n / steps + 4 * 8, "steps": steps,
+                "timing": "host wall clock around set_state, then per step step + get_residuals (4 doubles), "
+                          "then get_state (page-locked host arrays)"}
+
     e2e = None if args.no_e2e else e2e_pass(s)
+    e2e_reference_loop = None if args.no_e2e else e2e_run(s)
 
     # the same workload on the reference's own IBM stencil (2-point hat): the like-for-like
     # counterpart of the reference arm, which has no 4-point kernel
@@ -737,7 +763,8 @@ def main():
         barrier()
         th = max_over_ranks(acc / 1e3, device="cuda")
         hat2 = {"value": mesh.n_cells * K * world / th / 1e6, "ms_per_step": acc / K,
-                "e2e": None if args.no_e2e else e2e_pass(sh), "status_flags": sh.status(),
+                "e2e": None if args.no_e2e else e2e_pass(sh),
+                "e2e_reference_loop": None if args.no_e2e else e2e_run(sh), "status_flags": sh.status(),
                 "workload": workload(args.n, mesh.n_cells, mesh.n_faces, n_nodes, n_tris, n_springs, ibm="hat2")}
         sh.close()
 
@@ -813,6 +840,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "e2e_reference_loop": e2e_reference_loop,
             "gpu_launches": launches_per_step * K,
             "launch_shape": shape,
             "clocks": clocks,
