@@ -122,6 +122,27 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def axis_geometry_uniform(mesh):
+    """Whether every interior face of each axis has the same (area, dt, t1, t2), as the library
+    checks at create (then the interior-face kernel takes the geometry from its parameters)."""
+    import numpy as np
+    if not getattr(mesh, "axis_aligned", True):
+        return False
+    ni, nfx, nfy = mesh.n_interior, mesh.n_face_x, mesh.n_face_y
+    own, nb = np.asarray(mesh.owner)[:ni], np.asarray(mesh.neighbour)[:ni]
+    cen, fc = np.asarray(mesh.cell_centroid).reshape(-1, 3), np.asarray(mesh.face_centroid).reshape(-1, 3)
+    area, sdt = np.asarray(mesh.face_area)[:ni], np.asarray(mesh.streaming_dt)[:ni]
+    for ax, (a, b) in enumerate(((0, nfx), (nfx, nfx + nfy), (nfx + nfy, ni))):
+        if b <= a:
+            continue
+        t1 = cen[own[a:b], ax] - fc[a:b, ax]
+        t2 = cen[nb[a:b], ax] - fc[a:b, ax]
+        for v in (area[a:b], sdt[a:b], t1, t2):
+            if not np.all(v == v[0]):
+                return False
+    return True
+
+
 def algorithmic_bytes(mesh, phase, fp64=True):
     """Bytes each kernel must move once per launch (every array element it
     reads or writes counted once), FP64 storage."""
@@ -135,8 +156,11 @@ def algorithmic_bytes(mesh, phase, fp64=True):
     if phase == "flux":
         # per axis face: owner+neighbour ids 8, geometry (area, dt, t1, t2) 4R, flux out 4R;
         # per bc face: ids 8, geometry 12R, bc types/values 8 + 4R, bc record 9R, flux out 4R;
-        # per cell: state 4R + 12 gradients 12R, visc factor R; per ghost: state and gradients out 16R
-        return ni * (8 + 8 * R) + nb * (16 + 29 * R) + nc * (17 * R) + nb * (16 * R)
+        # per cell: state 4R + 12 gradients 12R, visc factor R; per ghost: state and gradients out 16R.
+        # On a mesh whose faces of each axis share one geometry the kernel reads it from its
+        # parameters: no per-face geometry
+        geo = 0 if axis_geometry_uniform(mesh) else 4 * R
+        return ni * (8 + 4 * R + geo) + nb * (16 + 29 * R) + nc * (17 * R) + nb * (16 * R)
     if phase == "gradients":
         # per cell: stencil 24, folded weights 18R, state 4R, gradients out 12R;
         # per ghost: bc record 9R + types 8 + values 4R (ghost states formed in registers)

@@ -282,15 +282,24 @@ template <typename R, int A>
 __device__ __forceinline__ Vec4<R> axis_face_flux(const FluidArgs<R> &a, int f) {
     constexpr int B = A == 0 ? 1 : 0, C = A == 2 ? 1 : 2;
     const int2 oc = __ldg(a.face_cells + f);
-    const AxisFace<R> geo = a.axis_face[f];
+    AxisFace<R> geo;
+    R wa, wb;
+    if (a.axis_uniform) {
+        geo = {a.axis_geo[A][0], a.axis_geo[A][1], a.axis_geo[A][2], a.axis_geo[A][3]};
+        wa = a.axis_wa[A];
+        wb = a.axis_wb[A];
+    } else {
+        geo = a.axis_face[f];
+        const R ic = R(1) / (geo.t2 - geo.t1);
+        wa = fabs(geo.t2 * ic);
+        wb = fabs(geo.t1 * ic);
+    }
     const Vec4<R> s1 = a.state[oc.x], s2 = a.state[oc.y];
     R g1[12], g2[12];
     load_grad(a.grad + (size_t)12 * oc.x, g1);
     load_grad(a.grad + (size_t)12 * oc.y, g2);
     const R rho0 = rho0_of(a);
     const R dt = geo.dt, t1 = geo.t1, t2 = geo.t2;
-    const R ic = R(1) / (t2 - t1);
-    const R wa = fabs(t2 * ic), wb = fabs(t1 * ic);
     const R S1[4] = {s1.rho, s1.u, s1.v, s1.w}, S2[4] = {s2.rho, s2.u, s2.v, s2.w};
     R pi[4], pn[4], p0[4];
 #pragma unroll

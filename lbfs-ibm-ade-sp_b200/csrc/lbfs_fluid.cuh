@@ -161,6 +161,14 @@ template <typename R> struct FluidArgs {
     // K2 geometry
     const int2 *face_cells;      // [nf] owner, neighbour
     const AxisFace<R> *axis_face;  // [ni] when axis_aligned
+    // axis_uniform: every interior face of an axis has the same geometry (the
+    // generator's uniform meshes, also across ensemble instances of one
+    // spacing), checked bit for bit at create; the interior-face kernels then
+    // take it from here instead of reading axis_face, with the owner/neighbour
+    // interpolation weights |t2 / (t2 - t1)|, |t1 / (t2 - t1)| formed once
+    int axis_uniform;
+    R axis_geo[3][4];            // per axis: area, dt, t1, t2
+    R axis_wa[3], axis_wb[3];
     const GenFace<R> *gen_face;  // [nb] bc faces, or [nf] when not axis aligned (indexed by face)
     const R *visc_factor;        // [nc]
     Vec4<R> *flux;               // [nf]

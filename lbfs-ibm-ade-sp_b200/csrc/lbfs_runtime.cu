@@ -323,6 +323,24 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         (rc = s->upload(&d_visc, visc)))
         return rc;
     if (a.axis_aligned && (rc = s->upload(&d_axf, axf))) return rc;
+    // one geometry per axis (bit for bit) on the generator's uniform meshes
+    a.axis_uniform = 0;
+    if (a.axis_aligned && ni > 0) {
+        const int first[3] = {0, a.nfx, a.nfx + a.nfy}, count[3] = {a.nfx, a.nfy, ni - a.nfx - a.nfy};
+        bool uniform = true;
+        for (int ax = 0; ax < 3 && uniform; ax++) {
+            if (count[ax] == 0) continue;
+            const AxisFace<R> &r = axf[first[ax]];
+            for (int f = first[ax]; f < first[ax] + count[ax] && uniform; f++)
+                uniform = std::memcmp(&axf[f], &r, sizeof(AxisFace<R>)) == 0;
+            if (!uniform) break;
+            a.axis_geo[ax][0] = r.area; a.axis_geo[ax][1] = r.dt; a.axis_geo[ax][2] = r.t1; a.axis_geo[ax][3] = r.t2;
+            const R ic = R(1) / (r.t2 - r.t1);  // as the kernel forms it (IEEE division and product)
+            a.axis_wa[ax] = std::fabs(r.t2 * ic);
+            a.axis_wb[ax] = std::fabs(r.t1 * ic);
+        }
+        a.axis_uniform = uniform ? 1 : 0;
+    }
     a.closure = nullptr;
     if (!closure.empty()) {
         double *d_cl;
