@@ -143,6 +143,17 @@ def axis_geometry_uniform(mesh):
     return True
 
 
+def ls_weights_coded(mesh):
+    """Whether the folded least-squares weights W_q = LHS^-1 RHS_q of all cells take at most 8
+    distinct vectors, as the library checks at create (then the gradient kernel reads a 3-bit code
+    per stencil slot instead of the weights)."""
+    import numpy as np
+    L = np.asarray(mesh.lhs_inverse).reshape(-1, 3, 3)
+    rh = np.asarray(mesh.rhs).reshape(-1, 6, 3)
+    W = (L[:, None, :, 0] * rh[:, :, None, 0] + L[:, None, :, 1] * rh[:, :, None, 1]) + L[:, None, :, 2] * rh[:, :, None, 2]
+    return len(np.unique(W.reshape(-1, 3), axis=0)) <= 8
+
+
 def algorithmic_bytes(mesh, phase, fp64=True):
     """Bytes each kernel must move once per launch (every array element it
     reads or writes counted once), FP64 storage."""
@@ -162,9 +173,11 @@ def algorithmic_bytes(mesh, phase, fp64=True):
         geo = 0 if axis_geometry_uniform(mesh) else 4 * R
         return ni * (8 + 4 * R + geo) + nb * (16 + 29 * R) + nc * (17 * R) + nb * (16 * R)
     if phase == "gradients":
-        # per cell: stencil 24, folded weights 18R, state 4R, gradients out 12R;
+        # per cell: stencil 24, folded weights 18R (or their 3-bit codes, 4, on a mesh with at most 8
+        # distinct weight vectors), state 4R, gradients out 12R;
         # per ghost: bc record 9R + types 8 + values 4R (ghost states formed in registers)
-        return nc * (24 + 34 * R) + nb * (8 + 13 * R)
+        w = 4 if ls_weights_coded(mesh) else 18 * R
+        return nc * (24 + 16 * R + w) + nb * (8 + 13 * R)
     if phase == "update":
         # per cell: face list 24, volume 8, t1 in/out 64, state out 4R; each face flux read once 4R
         return nc * (96 + 4 * R) + nf * 4 * R

@@ -58,7 +58,23 @@ __global__ void __launch_bounds__(TB, TB == 128 ? 5 : 1) k_cell_gradients(FluidA
         st[2 * q] = p.x;
         st[2 * q + 1] = p.y;
     }
-    const LsW<R> W = a.lsw[i];
+    LsW<R> W;
+    if (a.lsw_code) {  // the weights from the per-mesh table by the cell's six 3-bit codes
+        const unsigned code = __ldg(a.lsw_code + i);
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            const unsigned k = (code >> (3 * q)) & 7u;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                R v = a.lsw_tab[0][r];
+#pragma unroll
+                for (unsigned t = 1; t < 8; t++) v = (k == t) ? a.lsw_tab[t][r] : v;
+                W.w[3 * q + r] = v;
+            }
+        }
+    } else {
+        W = a.lsw[i];
+    }
     GradRec<R> gr;
     R *g = gr.g;
 #pragma unroll

@@ -154,6 +154,12 @@ template <typename R> struct FluidArgs {
     const int2 *stencil;         // [3*nc] (6 stencil entries per cell)
     const LsRec<R> *ls;          // [nc] RHS and LHS^-1 (the adjoint's; null for FP32-bulk handles)
     const LsW<R> *lsw;           // [nc] K1's folded weights
+    // Meshes whose per-slot weight vectors W_q take at most 8 distinct values
+    // (the generator's uniform meshes: +-1/(4 dx) along one axis, in a
+    // per-cell order): each cell's six vectors as 3-bit indices into lsw_tab,
+    // checked bit for bit at create (null: read lsw)
+    const unsigned *lsw_code;    // [nc]
+    R lsw_tab[8][3];
     const int *bc_rho_type, *bc_vel_type;
     const int *bc_periodic;      // [nb] partner cell of a type-3 ghost (Boundary_Conditions::periodic_node)
     const Vec4<R> *bc_val;       // [nb] (u, v, w, rho - rho0)

@@ -205,6 +205,25 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
             for (int r = 0; r < 3; r++)
                 lsw[i].w[3 * q + r] = (R)(L[3 * r] * rh[3 * q] + L[3 * r + 1] * rh[3 * q + 1] + L[3 * r + 2] * rh[3 * q + 2]);
     }
+    // at most 8 distinct weight vectors over all cells and slots: 3-bit codes per slot
+    std::vector<unsigned> lcode(nc);
+    int n_tab = 0;
+    bool coded = nc > 0;
+    for (int i = 0; i < nc && coded; i++) {
+        unsigned c = 0;
+        for (int q = 0; q < 6 && coded; q++) {
+            const R *v = lsw[i].w + 3 * q;
+            int k = 0;
+            while (k < n_tab && std::memcmp(a.lsw_tab[k], v, 3 * sizeof(R)) != 0) k++;
+            if (k == n_tab) {
+                if (n_tab == 8) { coded = false; break; }
+                std::memcpy(a.lsw_tab[n_tab++], v, 3 * sizeof(R));
+            }
+            c |= (unsigned)k << (3 * q);
+        }
+        lcode[i] = c;
+    }
+    for (int k = n_tab; k < 8; k++) a.lsw_tab[k][0] = a.lsw_tab[k][1] = a.lsw_tab[k][2] = R(0);
     std::vector<int> rt(nb), vt(nb), per(nb, 0);
     std::vector<Vec4<R>> bcv(nb);
     std::vector<BcRec<R>> bcr(nb);
@@ -346,6 +365,12 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         double *d_cl;
         if ((rc = s->upload(&d_cl, closure))) return rc;
         a.closure = d_cl;
+    }
+    a.lsw_code = nullptr;
+    if (coded) {
+        unsigned *d_code;
+        if ((rc = s->upload(&d_code, lcode))) return rc;
+        a.lsw_code = d_code;
     }
     a.stencil = d_stencil; a.ls = d_ls; a.lsw = d_lsw; a.bc_rho_type = d_rt; a.bc_vel_type = d_vt; a.bc_periodic = d_per;
     a.bc_val = d_bcv; a.bc_rec = d_bcr; a.face_cells = d_fcells; a.axis_face = d_axf; a.gen_face = d_gen;
