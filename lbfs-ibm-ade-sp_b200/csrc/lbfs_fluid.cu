@@ -730,7 +730,31 @@ template <typename R, int TB>
 __global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
     __shared__ double sh[4][TB / 32];
     __shared__ bool last_block;
+    // one instance with few membranes: its grid and the membranes' patches cached per block,
+    // with each patch's first and last linear cell (cells outside skip the i, j, k split)
+    __shared__ int s_grid[6];                 // cell0, nx, ny, nz, mem0, mem1
+    __shared__ int s_patch[kK3PatchCache][10];  // lo[3], dim[3], cells, off, first, last linear cell
     pdl_wait();  // the face fluxes
+    const bool cached = a.n_membranes > 0 && a.n_membranes <= kK3PatchCache && !a.cell_instance;
+    if (cached) {
+        const InstanceGrid g0 = reinterpret_cast<const InstanceGrid *>(a.instances)[0];
+        if (threadIdx.x == 0) {
+            s_grid[0] = g0.cell0; s_grid[1] = g0.nx; s_grid[2] = g0.ny; s_grid[3] = g0.nz;
+            s_grid[4] = g0.mem0; s_grid[5] = g0.mem1;
+        }
+        const MembraneScalars *ms = (const MembraneScalars *)a.membrane_scalars;
+        if ((int)threadIdx.x < a.n_membranes) {
+            const MembraneScalars &q = ms[threadIdx.x];
+            int *e = s_patch[threadIdx.x];
+            for (int c = 0; c < 3; c++) { e[c] = q.patch_lo[c]; e[3 + c] = q.patch_dim[c]; }
+            e[6] = q.patch_cells;
+            e[7] = q.patch_off;
+            e[8] = q.patch_lo[0] + g0.nx * (q.patch_lo[1] + g0.ny * q.patch_lo[2]);
+            e[9] = (q.patch_lo[0] + q.patch_dim[0] - 1) +
+                   g0.nx * ((q.patch_lo[1] + q.patch_dim[1] - 1) + g0.ny * (q.patch_lo[2] + q.patch_dim[2] - 1));
+        }
+        __syncthreads();
+    }
     double sq[4] = {0, 0, 0, 0};
     unsigned int flag = 0;
     // the step: constant, or the minimum per-cell step, or each cell's own (LBFS_DT_LOCAL)
@@ -761,7 +785,22 @@ __global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
             for (int m = 0; m < 3; m++) r[1 + m] = r[1 + m] + __ldg(a.closure + 3 * (size_t)i + m);
         }
         double fx = a.force[0], fy = a.force[1], fz = a.force[2];
-        if (a.n_membranes > 0) {
+        if (cached) {
+            const int li = i - s_grid[0];
+            for (int m = s_grid[4]; m < s_grid[5]; m++) {
+                const int *e = s_patch[m];
+                if (e[6] <= 0 || li < e[8] || li > e[9]) continue;
+                const int nx = s_grid[1], ny = s_grid[2];
+                const int ci = li % nx, cj = (li / nx) % ny, ck = li / (nx * ny);
+                const int px = ci - e[0], py = cj - e[1], pz = ck - e[2];
+                if (px >= 0 && py >= 0 && pz >= 0 && px < e[3] && py < e[4] && pz < e[5]) {
+                    const double *pf = a.patch_force + ((size_t)e[7] + (px + e[3] * (py + e[4] * pz))) * 3;
+                    fx = fx + pf[0];
+                    fy = fy + pf[1];
+                    fz = fz + pf[2];
+                }
+            }
+        } else if (a.n_membranes > 0) {
             const int inst = a.cell_instance ? __ldg(a.cell_instance + i) : 0;
             const InstanceGrid g = reinterpret_cast<const InstanceGrid *>(a.instances)[inst];
             const int li = i - g.cell0;

@@ -10,6 +10,7 @@ namespace lbfs {
 
 constexpr int kK3MaxBlocks = 148 * 8;      // default grid cap of the cell update (grid-stride)
 constexpr int kSpreadMaxBlocks = 148 * 8;  // default spread grid cap (grid-stride over the tiles)
+constexpr int kK3PatchCache = 32;          // membranes whose patches the cell update caches per block
 constexpr int kK3BlocksLimit = LBFS_MAX_UPDATE_BLOCKS;  // partial-sum slots allocated for the update
 
 template <typename R> void launch_fluid_gradients(const FluidArgs<R> &a, cudaStream_t s);
