@@ -42,14 +42,6 @@ enum MembraneMode : int {
     kModeStep = 2,       // one time step: interpolate, advect, forces, spread
 };
 
-// A node as the spread reads it, in sorted order: 1D stencil weights per axis,
-// first stencil cell (b[0..2]) and the node index (b[3]).
-struct alignas(16) SpreadRec {
-    double w[12];  // 1D stencil weights of a node, x then y then z (4 slots per axis)
-    int b0;        // first stencil cell along x
-    int node;      // the node (global index): the spread reads its force in node order
-    int pad[2];
-};
 
 
 
@@ -94,8 +86,7 @@ struct MembraneArgs {
                                  // that many CTAs per membrane (k_mem_step); 0: four kernels
     int *node_base;              // [3 total_nodes] first IBM stencil cell per axis at the current positions
     double *node_w;              // [12 total_nodes] 1D stencil weights per axis (4 slots) at the current positions
-    int *sorted_pos;             // [total_nodes] position of each node in its membrane's sorted order
-    SpreadRec *spread_rec;       // [total_nodes] nodes in (bin, node) order (scratch)
+    int *sorted_node;            // [total_nodes] each membrane's nodes in (bin, node) order, from node0
     // LBFS_IBM_VANDERMONDE4 (rectilinear meshes, one instance): per axis the
     // vertex coordinates [n + 1] and the centroid coordinate of each cell row [n]
     // (centroid[i].x, centroid[j nx].y, centroid[k nx ny].z), and the cell volumes

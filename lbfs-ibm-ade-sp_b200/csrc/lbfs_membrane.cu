@@ -661,43 +661,17 @@ __global__ void __launch_bounds__(128) k_mem_nodeforce(MembraneArgs A) {
     A.fz[n] = f[2];
 }
 
-// ---- M4: node bounds, nodes sorted by stencil base cell, spread records -----
+// ---- M4: node bounds, nodes sorted by stencil base cell ---------------------
 // One CTA per membrane; needs only the advected positions, so it runs beside
-// M2.  Finds the patch (bounding box of the stencils), sorts (bin, node) keys
-// in shared memory, writes for every bin b of the patch the first sorted
-// position whose bin is >= b, and for every sorted position the node's
-// stencil weights and first x cell (recomputed from its position, so nothing
-// but the keys lives between the phases).  The last CTA of the launch writes
-// the prefix of patch cells over the membranes (the spread kernel's work list).
-// Spread records in sorted order: the node's stencil weights, first x cell and
-// index, and each node's sorted position.
-__device__ __forceinline__ void write_spread_records(const MembraneArgs &A, const MembraneConst &mc, const int *list) {
-    // two records per round: all their loads are issued before the stores
-    for (int e0 = threadIdx.x; e0 < mc.n_nodes; e0 += 2 * blockDim.x) {
-        SpreadRec rec[2];
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const int e = e0 + k * blockDim.x;
-            const int n = mc.node0 + list[e < mc.n_nodes ? e : 0];
-            const double2 *w = reinterpret_cast<const double2 *>(A.node_w + 12 * (size_t)n);
-#pragma unroll
-            for (int q = 0; q < 6; q++) {
-                const double2 x = __ldcg(w + q);
-                rec[k].w[2 * q] = x.x;
-                rec[k].w[2 * q + 1] = x.y;
-            }
-            rec[k].b0 = __ldcg(A.node_base + 3 * (size_t)n);
-            rec[k].node = n;
-            rec[k].pad[0] = rec[k].pad[1] = 0;
-        }
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const int e = e0 + k * blockDim.x;
-            if (e >= mc.n_nodes) break;
-            A.spread_rec[mc.node0 + e] = rec[k];
-            A.sorted_pos[rec[k].node] = mc.node0 + e;
-        }
-    }
+// M2.  Finds the patch (bounding box of the stencils), counts the nodes per
+// stencil bin in shared memory, writes for every bin b of the patch the first
+// sorted position whose bin is >= b, and the nodes in (bin, node) order.  The
+// last CTA of the launch writes the prefix of patch cells over the membranes
+// (the spread kernel's work list).
+// The membrane's nodes in sorted order (global node indices): the spread reads
+// each contribution's stencil weights and force through it.
+__device__ __forceinline__ void write_sorted_nodes(const MembraneArgs &A, const MembraneConst &mc, const int *list) {
+    for (int e = threadIdx.x; e < mc.n_nodes; e += blockDim.x) A.sorted_node[mc.node0 + e] = mc.node0 + list[e];
 }
 
 // Exclusive prefix sum of one int per thread over the CTA, and the CTA's
@@ -810,8 +784,7 @@ __device__ void node_bounds(const MembraneArgs &A, const MembraneConst &mc, int 
 
 // Patch of a membrane from its node bounds red[12], the prefix of patch
 // cells over the membranes (by the last of the n_sorters CTAs to get here),
-// and the counting sort of its nodes by stencil bin with the spread records;
-// one CTA.  `skeys` is the dynamic shared memory of sort_smem_bytes.
+// and the counting sort of its nodes by stencil bin; one CTA.  `skeys` is the dynamic shared memory of sort_smem_bytes.
 __device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool bases_sane, unsigned int range_flag,
                            int n_sorters, unsigned long long *skeys) {
     __shared__ bool last_sorted;
@@ -929,12 +902,10 @@ __device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool
         }
     }
     __syncthreads();
-    write_spread_records(A, mc, list);
+    write_sorted_nodes(A, mc, list);
 }
 
-// 256 threads: the sort runs on a side stream beside the fluid kernels, off
-// the critical path, and a 1024-thread CTA held a whole SM for its 17 us.
-constexpr int kSortThreads = 256;
+constexpr int kSortThreads = kMembraneThreads;
 __global__ void __launch_bounds__(kSortThreads) k_mem_sort(MembraneArgs A) {
     extern __shared__ unsigned long long skeys[];  // 2 int arrays of sort_capacity: bins, sorted list
     const int m = blockIdx.x;
@@ -951,7 +922,7 @@ __global__ void __launch_bounds__(kSortThreads) k_mem_sort(MembraneArgs A) {
 // k_mem_sort (four launches whose phases are each a few dependent memory round
 // trips, so that the launches and the waits between them set the chain's
 // length); the spread follows.
-//  rank 0: node bounds, the patch, the node sort and the spread records.
+//  rank 0: node bounds, the patch and the node sort.
 //  ranks 1..: every node position into shared memory, V and A over all
 //     triangles (each CTA the same fixed-order sum, so they agree bit for
 //     bit), the spring forces and the MAD terms.
@@ -1183,7 +1154,7 @@ __global__ void __launch_bounds__(256) k_mem_spread(MembraneArgs A) {
             if (lane >= o) end += x;
         }
         const int count = __shfl_sync(0xffffffffu, end, S * S - 1);
-        const SpreadRec *rec = A.spread_rec + mc.node0;
+        const int *sorted = A.sorted_node + mc.node0;
 
         double inv3 = 1 / mc.gdx / mc.gdx / mc.gdx;
         if (A.ibm_stencil == LBFS_IBM_VANDERMONDE4) {
@@ -1205,10 +1176,11 @@ __global__ void __launch_bounds__(256) k_mem_spread(MembraneArgs A) {
             const int r_lo = __shfl_sync(0xffffffffu, lo, r);
             if (q < count) {
                 const int e = r_lo + q - (r_end - r_len);
-                const SpreadRec &w = rec[e];
-                const double3 F = make_double3(__ldg(A.fx + w.node), __ldg(A.fy + w.node), __ldg(A.fz + w.node));
-                const double wy = w.w[4 + S - 1 - r % S], wz = w.w[8 + S - 1 - r / S];
-                const double wx = w.w[ci - w.b0];
+                const int node = __ldg(sorted + e);
+                const double *w = A.node_w + 12 * (size_t)node;
+                const double3 F = make_double3(__ldg(A.fx + node), __ldg(A.fy + node), __ldg(A.fz + node));
+                const double wy = __ldg(w + 4 + S - 1 - r % S), wz = __ldg(w + 8 + S - 1 - r / S);
+                const double wx = __ldg(w + ci - __ldg(A.node_base + 3 * (size_t)node));
                 f[0] += F.x * wx * wy * wz * inv3;
                 f[1] += F.y * wx * wy * wz * inv3;
                 f[2] += F.z * wx * wy * wz * inv3;
@@ -1554,7 +1526,7 @@ int launch_membrane(const MembraneArgs &a, cudaStream_t s, cudaStream_t s_side, 
     launch_hi(k_mem_springs, spring_grid, dim3(128), 0, s, a, 0, true);
     launch_hi(k_mem_nodeforce, dim3((a.total_nodes + 127) / 128), dim3(128), 0, s, a, 0, true);
     const int n = 6;
-    // the spread reads the sorted records and the node forces
+    // the spread reads the sorted node list and the node forces
     if (side) cudaStreamWaitEvent(s, ev_sorted, 0);
     if (without_spread) return n - 1;
     if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, spread_grid, dim3(256), 0, s, a);

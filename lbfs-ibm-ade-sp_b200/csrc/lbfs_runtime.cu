@@ -657,7 +657,7 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
         (rc = s->alloc(&ma.bin_start, (size_t)total_patch + n_rbc)) ||
         (rc = s->alloc(&ma.bin_cursor, (size_t)total_patch + n_rbc)) ||
         (rc = s->alloc(&ma.cell_start, (size_t)n_rbc + 1)) || (rc = s->alloc(&ma.sort_ticket, 1)) ||
-        (rc = s->alloc(&ma.spread_rec, (size_t)N)) || (rc = s->upload(&ma.sorted_pos, identity)) ||
+        (rc = s->upload(&ma.sorted_node, identity)) ||
         (rc = s->alloc(&ma.node_base, 3 * (size_t)N)) ||
         (rc = s->alloc(&ma.node_w, 12 * (size_t)N)) ||
         (rc = s->alloc(&ma.mad_partials, (size_t)n_rbc * kMaxSpringBlocks)) ||
@@ -1623,10 +1623,10 @@ int adjm_prepare(lbfs_solver *s) {
     std::vector<int> identity(N);
     for (int n = 0; n < N; n++) identity[n] = n;
     MembraneScalars *ms2;
-    if ((rc = s->alloc(&ms2, M)) || (rc = s->alloc(&mb.spread_rec, N)) ||
+    if ((rc = s->alloc(&ms2, M)) ||
         (rc = s->alloc(&mb.bin_start, (size_t)s->total_patch + M)) || (rc = s->alloc(&mb.cell_start, (size_t)M + 1)) ||
         (rc = s->alloc(&mb.bin_cursor, (size_t)s->total_patch + M)) ||
-        (rc = s->alloc(&mb.sort_ticket, 1)) || (rc = s->upload(&mb.sorted_pos, identity)) ||
+        (rc = s->alloc(&mb.sort_ticket, 1)) || (rc = s->upload(&mb.sorted_node, identity)) ||
         (rc = s->alloc(&mb.fx, N)) || (rc = s->alloc(&mb.fy, N)) || (rc = s->alloc(&mb.fz, N)) ||
         (rc = s->alloc(&mb.patch_force, 3 * (size_t)s->total_patch)) ||
         (rc = s->alloc(&mb.node_base, 3 * (size_t)N)) || (rc = s->alloc(&mb.node_w, 12 * (size_t)N)))
