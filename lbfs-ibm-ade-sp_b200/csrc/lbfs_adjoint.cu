@@ -167,7 +167,9 @@ template <int axis>
 __device__ __forceinline__ void axis_face_bwd(const FluidArgs<double> &a, const AdjointArgs &j, int f,
                                               const double (&lo)[4]) {
     const int2 oc = __ldg(a.face_cells + f);
-    const AxisFace<double> geo = a.axis_face[f];
+    AxisFace<double> geo;
+    if (a.axis_uniform) geo = {a.axis_geo[axis][0], a.axis_geo[axis][1], a.axis_geo[axis][2], a.axis_geo[axis][3]};
+    else geo = a.axis_face[f];
     const Vec4<double> s1 = a.state[oc.x], s2 = a.state[oc.y];
     double g1[12], g2[12];
     load12(a.grad + 12 * (size_t)oc.x, g1);
@@ -511,6 +513,15 @@ __global__ void __launch_bounds__(128) k_adj_flux_general(FluidArgs<double> a, A
     }
 }
 
+// RHS vector k, component c, of a mesh with coded least-squares geometry (selects: k is not a
+// compile-time index into the parameter table)
+__device__ __forceinline__ double rhs_of(const FluidArgs<double> &a, unsigned k, int c) {
+    double v = a.ls_rhs_tab[0][c];
+#pragma unroll
+    for (unsigned t = 1; t < 8; t++) v = (k == t) ? a.ls_rhs_tab[t][c] : v;
+    return v;
+}
+
 // A2: per cell.  lambda of the cell's state and gradient from its faces; its
 // ghost cells (boundary faces) back through the ghost gradient and the ghost
 // state; lambda_R = LHS^-T lambda_grad for the stencil; the self term of the
@@ -594,7 +605,20 @@ __global__ void __launch_bounds__(128, 4) k_adj_cell(FluidArgs<double> a, Adjoin
         (void)G;
     }
     // lambda_R[m][col] = sum_row LHS[row][col] lambda_grad[m][row]
-    const LsRec<double> L = a.ls[i];
+    LsRec<double> L;
+    if (a.ls_coded) {  // one LHS^-1, RHS vectors by the cell's codes
+        const unsigned code = __ldg(a.lsw_code + i);
+#pragma unroll
+        for (int t = 0; t < 9; t++) L.lhs[t] = a.ls_lhs[t];
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            const unsigned k = (code >> (3 * q)) & 7u;
+#pragma unroll
+            for (int c = 0; c < 3; c++) L.rhs[3 * q + c] = rhs_of(a, k, c);
+        }
+    } else {
+        L = a.ls[i];
+    }
     double lr[12];
 #pragma unroll
     for (int m = 0; m < 4; m++)
@@ -653,7 +677,15 @@ __global__ void __launch_bounds__(128) k_adj_gather(FluidArgs<double> a, Adjoint
     for (int e = j.tst_start[c]; e < j.tst_start[c + 1]; e++) {
         const int code = j.tst[e];
         const int i = code >> 3, q = code & 7;
-        const double *r = a.ls[i].rhs + 3 * q;
+        double r[3];
+        if (a.ls_coded) {
+            const unsigned k = (__ldg(a.lsw_code + i) >> (3 * q)) & 7u;
+#pragma unroll
+            for (int c = 0; c < 3; c++) r[c] = rhs_of(a, k, c);
+        } else {
+            const double *rr = a.ls[i].rhs + 3 * q;
+            r[0] = rr[0]; r[1] = rr[1]; r[2] = rr[2];
+        }
         double lr[12];
         load12(j.lam_rs + 12 * (size_t)i, lr);
 #pragma unroll

@@ -160,6 +160,11 @@ template <typename R> struct FluidArgs {
     // checked bit for bit at create (null: read lsw)
     const unsigned *lsw_code;    // [nc]
     R lsw_tab[8][3];
+    // ls_coded (FP64 handles, with lsw_code): every cell has the same LHS^-1 (ls_lhs) and its RHS
+    // vectors are ls_rhs_tab[k] for the same codes; the adjoint reads these instead of ls
+    int ls_coded;
+    R ls_lhs[9];
+    R ls_rhs_tab[8][3];
     const int *bc_rho_type, *bc_vel_type;
     const int *bc_periodic;      // [nb] partner cell of a type-3 ghost (Boundary_Conditions::periodic_node)
     const Vec4<R> *bc_val;       // [nb] (u, v, w, rho - rho0)

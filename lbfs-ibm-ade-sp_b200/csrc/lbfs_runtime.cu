@@ -224,6 +224,27 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         lcode[i] = c;
     }
     for (int k = n_tab; k < 8; k++) a.lsw_tab[k][0] = a.lsw_tab[k][1] = a.lsw_tab[k][2] = R(0);
+    // the adjoint's LHS^-1 and RHS by the same codes: one LHS^-1 for all cells, one RHS vector per code
+    a.ls_coded = 0;
+    if (coded && !ls.empty()) {
+        bool ok = true, seen[8] = {false, false, false, false, false, false, false, false};
+        std::memcpy(a.ls_lhs, ls[0].lhs, 9 * sizeof(R));
+        for (int i = 0; i < nc && ok; i++) {
+            ok = std::memcmp(ls[i].lhs, a.ls_lhs, 9 * sizeof(R)) == 0;
+            for (int q = 0; q < 6 && ok; q++) {
+                const unsigned k = (lcode[i] >> (3 * q)) & 7u;
+                if (!seen[k]) {
+                    std::memcpy(a.ls_rhs_tab[k], ls[i].rhs + 3 * q, 3 * sizeof(R));
+                    seen[k] = true;
+                } else {
+                    ok = std::memcmp(a.ls_rhs_tab[k], ls[i].rhs + 3 * q, 3 * sizeof(R)) == 0;
+                }
+            }
+        }
+        for (int k = 0; k < 8; k++)
+            if (!seen[k]) a.ls_rhs_tab[k][0] = a.ls_rhs_tab[k][1] = a.ls_rhs_tab[k][2] = R(0);
+        a.ls_coded = ok ? 1 : 0;
+    }
     std::vector<int> rt(nb), vt(nb), per(nb, 0);
     std::vector<Vec4<R>> bcv(nb);
     std::vector<BcRec<R>> bcr(nb);
