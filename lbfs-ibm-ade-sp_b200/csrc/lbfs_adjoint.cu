@@ -489,6 +489,7 @@ __device__ __forceinline__ void store_face(const AdjointArgs &j, int f, const Fa
 }
 
 __global__ void __launch_bounds__(128, 3) k_adj_flux_axis(FluidArgs<double> a, AdjointArgs j) {
+    pdl_trigger();
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= a.ni) return;
     double lo[4];
@@ -529,6 +530,8 @@ __device__ __forceinline__ double rhs_of(const FluidArgs<double> &a, unsigned k,
 // boundary-velocity scale sigma (every boundary velocity value times sigma)
 // is added to sigma_acc[cell].
 __global__ void __launch_bounds__(128, 4) k_adj_cell(FluidArgs<double> a, AdjointArgs j) {
+    pdl_trigger();
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nc) return;
     double ls[4] = {0, 0, 0, 0}, lg[12];
@@ -669,6 +672,7 @@ __global__ void __launch_bounds__(128, 4) k_adj_cell(FluidArgs<double> a, Adjoin
 // A3: per cell.  lambda_state += transposed-stencil gather of lambda_R and the
 // IBM interpolation term; lambda_t1 += d primitive / d t1 ^T lambda_state.
 __global__ void __launch_bounds__(128) k_adj_gather(FluidArgs<double> a, AdjointArgs j) {
+    pdl_wait();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= a.nc) return;
     double ls[4];
@@ -776,12 +780,31 @@ void launch_adj_flux_general(const FluidArgs<double> &a, const AdjointArgs &j, c
     if (a.nf > first) k_adj_flux_general<<<(a.nf - first + 127) / 128, 128, 0, s>>>(a, j, first);
 }
 
-void launch_adj_cells(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
-    k_adj_cell<<<(a.nc + 127) / 128, 128, 0, s>>>(a, j);
+// pdl: a programmatic dependent launch directly behind the kernel it follows on the stream
+template <typename... KArgs, typename... Args>
+void launch_adj_kernel(void (*kernel)(KArgs...), int g, int tb, cudaStream_t s, bool pdl, Args... args) {
+    if (!pdl) {
+        kernel<<<g, tb, 0, s>>>(args...);
+        return;
+    }
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(g);
+    cfg.blockDim = dim3(tb);
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
-void launch_adj_gather(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
-    k_adj_gather<<<(a.nc + 127) / 128, 128, 0, s>>>(a, j);
+void launch_adj_cells(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s, bool pdl) {
+    launch_adj_kernel(k_adj_cell, (a.nc + 127) / 128, 128, s, pdl, a, j);
+}
+
+void launch_adj_gather(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s, bool pdl) {
+    launch_adj_kernel(k_adj_gather, (a.nc + 127) / 128, 128, s, pdl, a, j);
 }
 
 int launch_adj_fluid(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {

@@ -75,7 +75,8 @@ int launch_adj_fluid(const FluidArgs<double> &a, const AdjointArgs &j, cudaStrea
 // disjoint face records), A2 after both, A3 after A2 and the membrane part
 void launch_adj_flux_axis(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
 void launch_adj_flux_general(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
-void launch_adj_cells(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
-void launch_adj_gather(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s);
+// pdl: launched as a programmatic dependent launch behind the kernel before it on the stream
+void launch_adj_cells(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s, bool pdl = false);
+void launch_adj_gather(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s, bool pdl = false);
 
 }  // namespace lbfs

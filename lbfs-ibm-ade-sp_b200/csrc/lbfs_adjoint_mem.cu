@@ -248,6 +248,7 @@ __device__ __forceinline__ StencilD stencil_d(int stencil, const MembraneConst &
 
 // ---- B1: spread adjoint at x' -------------------------------------------------
 __global__ void __launch_bounds__(256) k_adjm_spread(MembraneArgs A, MemAdjArgs J) {
+    pdl_trigger();
     const int lane = threadIdx.x & 31;
     const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (n >= A.total_nodes) return;
@@ -294,6 +295,8 @@ constexpr int kDirs = 17;   // 12 coordinates, V, A, MAD_n, G_s, k_b
 constexpr int kPasses = 13; // the 12 coordinate directions in dual numbers, then one value pass for the 5 scalars
 
 __global__ void __launch_bounds__(128) k_adjm_springs(MembraneArgs A, MemAdjArgs J) {
+    pdl_trigger();
+    pdl_wait();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
     if (s >= A.total_springs) return;
@@ -351,6 +354,8 @@ __global__ void __launch_bounds__(128) k_adjm_springs(MembraneArgs A, MemAdjArgs
 // ---- B3: per-membrane sums ----------------------------------------------------
 __global__ void __launch_bounds__(1024) k_adjm_reduce(MembraneArgs A, MemAdjArgs J) {
     __shared__ double sh[32][5];
+    pdl_trigger();
+    pdl_wait();
     const int m = blockIdx.x;
     const MembraneConst &mc = A.mc[m];
     double v[5] = {0, 0, 0, 0, 0};
@@ -382,6 +387,8 @@ __global__ void __launch_bounds__(1024) k_adjm_reduce(MembraneArgs A, MemAdjArgs
 
 // ---- B4: node gather of the spring and totals adjoints -------------------------
 __global__ void __launch_bounds__(128) k_adjm_nodes(MembraneArgs A, MemAdjArgs J) {
+    pdl_trigger();
+    pdl_wait();
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.total_nodes) return;
     const int m = A.node_mem[n];
@@ -421,6 +428,8 @@ __global__ void __launch_bounds__(128) k_adjm_nodes(MembraneArgs A, MemAdjArgs J
 // ---- B5: advection adjoint at x_n -------------------------------------------------
 template <typename R>
 __global__ void __launch_bounds__(256) k_adjm_advect(MembraneArgs A, MemAdjArgs J) {
+    pdl_trigger();
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int n = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (n >= A.total_nodes) return;
@@ -463,6 +472,7 @@ __global__ void __launch_bounds__(256) k_adjm_advect(MembraneArgs A, MemAdjArgs 
 // Cells' velocity adjoint from the patches of the second spread.
 __global__ void __launch_bounds__(256) k_adjm_cells(MemAdjArgs J, int nc, const int *cell_instance,
                                                      const InstanceGrid *instances) {
+    pdl_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nc) return;
     const int inst = cell_instance ? cell_instance[i] : 0;
@@ -515,17 +525,34 @@ void launch_adj_membrane_sort(const MemAdjArgs &J, cudaStream_t s) {
 
 // Membrane part of one backward step, after launch_adj_membrane_sort: A holds
 // the step's x', node forces, totals and MAD_{n+1}.
+// Each kernel after the first directly behind its predecessor on the stream,
+// as a programmatic dependent launch (it waits in pdl_wait for the
+// predecessor's results).
+template <typename... KArgs, typename... Args>
+void launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 int launch_adj_membrane(const MembraneArgs &A, const MemAdjArgs &J, int nc, const int *cell_instance,
                         const InstanceGrid *instances, cudaStream_t s) {
     const int node_blocks = (A.total_nodes * 32 + 255) / 256;
     k_adjm_spread<<<node_blocks, 256, 0, s>>>(A, J);
-    k_adjm_springs<<<dim3((A.total_springs + 127) / 128, kPasses), 128, 0, s>>>(A, J);
-    k_adjm_reduce<<<A.n_membranes, 1024, 0, s>>>(A, J);
-    k_adjm_nodes<<<(A.total_nodes + 127) / 128, 128, 0, s>>>(A, J);
-    if (A.state_is_float) k_adjm_advect<float><<<node_blocks, 256, 0, s>>>(A, J);
-    else k_adjm_advect<double><<<node_blocks, 256, 0, s>>>(A, J);
+    launch_chained(k_adjm_springs, dim3((A.total_springs + 127) / 128, kPasses), dim3(128), s, A, J);
+    launch_chained(k_adjm_reduce, dim3(A.n_membranes), dim3(1024), s, A, J);
+    launch_chained(k_adjm_nodes, dim3((A.total_nodes + 127) / 128), dim3(128), s, A, J);
+    if (A.state_is_float) launch_chained(k_adjm_advect<float>, dim3(node_blocks), dim3(256), s, A, J);
+    else launch_chained(k_adjm_advect<double>, dim3(node_blocks), dim3(256), s, A, J);
     launch_membrane_spread(J.mb, s);
-    k_adjm_cells<<<(nc + 255) / 256, 256, 0, s>>>(J, nc, cell_instance, instances);
+    launch_chained(k_adjm_cells, dim3((nc + 255) / 256), dim3(256), s, J, nc, cell_instance, instances);
     return 7;
 }
 

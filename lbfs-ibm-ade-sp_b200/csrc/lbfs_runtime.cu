@@ -2008,9 +2008,11 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
             LBFS_CUDA(cudaEventRecord(ev_gen, rs.g));
             launch_adj_flux_axis(ab, j, rs.f);
             LBFS_CUDA(cudaStreamWaitEvent(rs.f, ev_gen, 0));
-            launch_adj_cells(ab, j, rs.f);
+            // A2 and A3 behind A1 and A2 as programmatic dependent launches (their other
+            // dependency, the boundary faces / the membrane backward, is one kernel each)
+            launch_adj_cells(ab, j, rs.f, a.axis_aligned && a.ni > 0);
             if (M > 0) LBFS_CUDA(cudaStreamWaitEvent(rs.f, ev_mem, 0));
-            launch_adj_gather(ab, j, rs.f);
+            launch_adj_gather(ab, j, rs.f, true);
             LBFS_CUDA(cudaGetLastError());
         }
         return LBFS_OK;
