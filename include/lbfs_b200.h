@@ -322,7 +322,11 @@ int lbfs_checkpoint_load(lbfs_solver *s, const void *buf, uint64_t bytes);
  * (and, with membranes, node positions and MAD) every `checkpoint_every`
  * steps, evaluates the objective on the final state, then sweeps backwards
  * segment by segment: each segment is recomputed from its checkpoint and the
- * discrete adjoint of every step is applied in reverse.  FP64 handles without
+ * discrete adjoint of every step is applied in reverse.  When every segment's
+ * per-step intermediates fit in half the free device memory (at most
+ * LBFS_ADJOINT_MEMORY_MB MiB if that environment variable is set; 0 forces the
+ * recomputation), the forward sweep keeps them and the reverse sweep
+ * recomputes nothing; the results are the same bit for bit.  FP64 handles without
  * preconditioning.  On return the handle holds the final forward state and
  * the step counter has advanced by n_steps.
  *   J        objective value

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdint>
 #include <initializer_list>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -1752,16 +1753,36 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     const size_t xs = 3 * (size_t)N;  // positions of one step: x, y, z planes
     cudaStream_t st = s->stream;
     DevBuf ck, st0, fin_t1, fin_state, wts, ckx, ckm, finx, finm, bst;
-    // segment storage, two sets: the re-run of one segment fills one set while
-    // the backward sweep of the next later segment reads the other
+    // segment storage: per step t1, the gradients and ghost states of its K1,
+    // x', node forces, membrane scalars and MAD.  Two sets, the re-run of one
+    // segment filling one while the backward sweep of the next later segment
+    // reads the other; or, when every segment's set fits in half the free
+    // device memory (at most LBFS_ADJOINT_MEMORY_MB if that is set), one set per
+    // segment, filled by the forward sweep itself, and the reverse sweep
+    // re-runs nothing (the same kernels on the same inputs: the same results).
     struct SegStore {
         DevBuf t1, g, h, x, f, s, m;
-    } segbuf[2];
-    const int n_sets = n_ck > 1 ? 2 : 1;
-    LBFS_CUDA(cudaMalloc(&ck.p, sizeof(double4) * (size_t)nc * n_ck));
-    // per step of a segment: t1, the gradients and ghost states of its K1
+    };
     const size_t gsz = 12 * (size_t)nt;
     const size_t nbx = s->nb > 0 ? s->nb : 1;
+    const size_t set_bytes = (sizeof(double4) * (size_t)nc + sizeof(double) * gsz + sizeof(Vec4<double>) * nbx) * K +
+                             (M > 0 ? sizeof(double) * xs * (2 * (size_t)K + 1) +
+                                          (sizeof(MembraneScalars) + sizeof(double)) * (size_t)M * K
+                                    : 0);
+    bool store_all = false;
+    if (n_ck > 1) {
+        size_t free_b = 0, total_b = 0;
+        LBFS_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        size_t budget = free_b / 2;
+        if (const char *mb = std::getenv("LBFS_ADJOINT_MEMORY_MB")) {
+            const long long v = std::atoll(mb);
+            budget = std::min(budget, v > 0 ? (size_t)v << 20 : (size_t)0);
+        }
+        store_all = set_bytes * (size_t)n_ck <= budget;
+    }
+    const int n_sets = store_all ? n_ck : (n_ck > 1 ? 2 : 1);
+    std::vector<SegStore> segbuf(n_sets);
+    LBFS_CUDA(cudaMalloc(&ck.p, sizeof(double4) * (size_t)nc * n_ck));
     for (int b = 0; b < n_sets; b++) {
         SegStore &q = segbuf[b];
         LBFS_CUDA(cudaMalloc(&q.t1.p, sizeof(double4) * (size_t)nc * K));
@@ -1828,19 +1849,91 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     const long long t_start = s->t;
     cudaEvent_t e0, e1, e2;
     cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
+    // run segment sg from the handle's state into segment set b, keeping each
+    // step's inputs (t1, x, MAD) and what its backward reads (gradients, ghost
+    // states, x', node forces, membrane scalars); on the handle's stream
+    auto record = [&](int sg, int b) -> int {
+        SegStore &q = segbuf[b];
+        double4 *seg_t1 = (double4 *)q.t1.p;
+        double *seg_g = (double *)q.g.p, *seg_x = (double *)q.x.p, *seg_f = (double *)q.f.p, *seg_m = (double *)q.m.p;
+        Vec4<double> *seg_h = (Vec4<double> *)q.h.p;
+        MembraneScalars *seg_s = (MembraneScalars *)q.s.p;
+        const int n0 = sg * K, n1 = std::min(n_steps, n0 + K);
+        int rc;
+        // the stores of a step in one launch each (a dozen separate copies per
+        // step cost more than the copies themselves): before the first step
+        // t1, x and MAD; after step i its gradients, ghost states, x', node
+        // forces and scalars, and t1 and MAD of step i + 1
+        static_assert(sizeof(MembraneScalars) % sizeof(double) == 0, "MembraneScalars copied as doubles");
+        const int mad_stride = (int)(sizeof(MembraneScalars) / sizeof(double));
+        const double *mad_src = &ma.ms[0].MAD;
+        const int count = n1 - n0;
+        {
+            CopyList pre = {};
+            pre.add(a.t1, seg_t1, 4 * (long long)nc);
+            if (M > 0) {
+                pre.add(ma.x, seg_x, N);
+                pre.add(ma.y, seg_x + N, N);
+                pre.add(ma.z, seg_x + 2 * (size_t)N, N);
+                pre.add(mad_src, seg_m, M, mad_stride);
+            }
+            launch_copy_list(pre, st);
+        }
+        for (int n = n0; n < n1; n++) {
+            const size_t i = n - n0;
+            s->t = t_start + n;
+            if ((rc = run_one_step(s))) return rc;
+            CopyList post = {};
+            post.add(a.grad, seg_g + i * gsz, (long long)gsz);
+            post.add(a.state + nc, seg_h + i * s->nb, 4 * (long long)s->nb);
+            if ((int)i + 1 < count) post.add(a.t1, seg_t1 + (i + 1) * nc, 4 * (long long)nc);
+            if (M > 0) {
+                double *xn1 = seg_x + (i + 1) * xs, *fi = seg_f + i * xs;
+                post.add(ma.x, xn1, N);
+                post.add(ma.y, xn1 + N, N);
+                post.add(ma.z, xn1 + 2 * (size_t)N, N);
+                post.add(ma.fx, fi, N);
+                post.add(ma.fy, fi + N, N);
+                post.add(ma.fz, fi + 2 * (size_t)N, N);
+                post.add(ma.ms, seg_s + i * M, (long long)(sizeof(MembraneScalars) / sizeof(double)) * M);
+                if ((int)i + 1 < count) post.add(mad_src, seg_m + (i + 1) * M, M, mad_stride);
+            }
+            launch_copy_list(post, st);
+            LBFS_CUDA(cudaGetLastError());
+        }
+        return LBFS_OK;
+    };
+    // the same from segment sg's checkpoint (the two-set form of the reverse sweep)
+    auto rerun = [&](int sg, int b) -> int {
+        const int n0 = sg * K;
+        int rc;
+        LBFS_CUDA(cudaMemcpyAsync(a.t1, ck_t1 + (size_t)sg * nc, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
+        if (n0 == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
+        else launch_adj_prim(a, st);
+        if (M > 0) {
+            if ((rc = load_x(ck_x + (size_t)sg * xs))) return rc;
+            launch_adjm_set_mad(ma, ck_m + (size_t)sg * M, st);
+        }
+        return record(sg, b);
+    };
     // ---- forward sweep with checkpoints
     LBFS_CUDA(cudaMemcpyAsync(st0.p, a.state, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
     LBFS_CUDA(cudaMemsetAsync(a.flags, 0, sizeof(unsigned int), st));
     cudaEventRecord(e0, st);
-    for (int n = 0; n < n_steps; n++) {
-        if (n % K == 0) {
-            LBFS_CUDA(cudaMemcpyAsync(ck_t1 + (size_t)(n / K) * nc, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
-            if (M > 0) {
-                if ((rc = save_x(ck_x + (size_t)(n / K) * xs))) return rc;
-                launch_adjm_get_mad(ma, ck_m + (size_t)(n / K) * M, st);
+    if (store_all) {
+        for (int sg = 0; sg < n_ck; sg++)
+            if ((rc = record(sg, sg))) return rc;
+    } else {
+        for (int n = 0; n < n_steps; n++) {
+            if (n % K == 0) {
+                LBFS_CUDA(cudaMemcpyAsync(ck_t1 + (size_t)(n / K) * nc, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
+                if (M > 0) {
+                    if ((rc = save_x(ck_x + (size_t)(n / K) * xs))) return rc;
+                    launch_adjm_get_mad(ma, ck_m + (size_t)(n / K) * M, st);
+                }
             }
+            if ((rc = run_one_step(s))) return rc;
         }
-        if ((rc = run_one_step(s))) return rc;
     }
     cudaEventRecord(e1, st);
     LBFS_CUDA(cudaMemcpyAsync(fin_t1.p, a.t1, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
@@ -1892,81 +1985,20 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     // ---- reverse sweep
     j.lam_u_ibm = M > 0 ? mj.lam_u_ibm : nullptr;
     mj.lam_t1 = j.lam_t1;
-    // re-run segment sg from its checkpoint into segment set b, keeping each
-    // step's inputs (t1, x, MAD) and what its backward reads (gradients, ghost
-    // states, x', node forces, membrane scalars); on the handle's stream
-    auto rerun = [&](int sg, int b) -> int {
-        SegStore &q = segbuf[b];
-        double4 *seg_t1 = (double4 *)q.t1.p;
-        double *seg_g = (double *)q.g.p, *seg_x = (double *)q.x.p, *seg_f = (double *)q.f.p, *seg_m = (double *)q.m.p;
-        Vec4<double> *seg_h = (Vec4<double> *)q.h.p;
-        MembraneScalars *seg_s = (MembraneScalars *)q.s.p;
-        const int n0 = sg * K, n1 = std::min(n_steps, n0 + K);
-        int rc;
-        LBFS_CUDA(cudaMemcpyAsync(a.t1, ck_t1 + (size_t)sg * nc, sizeof(double4) * nc, cudaMemcpyDeviceToDevice, st));
-        if (n0 == 0) LBFS_CUDA(cudaMemcpyAsync(a.state, st0.p, sizeof(Vec4<double>) * nt, cudaMemcpyDeviceToDevice, st));
-        else launch_adj_prim(a, st);
-        if (M > 0) {
-            if ((rc = load_x(ck_x + (size_t)sg * xs))) return rc;
-            launch_adjm_set_mad(ma, ck_m + (size_t)sg * M, st);
-        }
-        // the stores of a step in one launch each (a dozen separate copies per
-        // step cost more than the copies themselves): before the first step
-        // t1, x and MAD; after step i its gradients, ghost states, x', node
-        // forces and scalars, and t1 and MAD of step i + 1
-        static_assert(sizeof(MembraneScalars) % sizeof(double) == 0, "MembraneScalars copied as doubles");
-        const int mad_stride = (int)(sizeof(MembraneScalars) / sizeof(double));
-        const double *mad_src = &ma.ms[0].MAD;
-        const int count = n1 - n0;
-        {
-            CopyList pre = {};
-            pre.add(a.t1, seg_t1, 4 * (long long)nc);
-            if (M > 0) {
-                pre.add(ma.x, seg_x, N);
-                pre.add(ma.y, seg_x + N, N);
-                pre.add(ma.z, seg_x + 2 * (size_t)N, N);
-                pre.add(mad_src, seg_m, M, mad_stride);
-            }
-            launch_copy_list(pre, st);
-        }
-        for (int n = n0; n < n1; n++) {
-            const size_t i = n - n0;
-            s->t = t_start + n;
-            if ((rc = run_one_step(s))) return rc;
-            CopyList post = {};
-            post.add(a.grad, seg_g + i * gsz, (long long)gsz);
-            post.add(a.state + nc, seg_h + i * s->nb, 4 * (long long)s->nb);
-            if ((int)i + 1 < count) post.add(a.t1, seg_t1 + (i + 1) * nc, 4 * (long long)nc);
-            if (M > 0) {
-                double *xn1 = seg_x + (i + 1) * xs, *fi = seg_f + i * xs;
-                post.add(ma.x, xn1, N);
-                post.add(ma.y, xn1 + N, N);
-                post.add(ma.z, xn1 + 2 * (size_t)N, N);
-                post.add(ma.fx, fi, N);
-                post.add(ma.fy, fi + N, N);
-                post.add(ma.fz, fi + 2 * (size_t)N, N);
-                post.add(ma.ms, seg_s + i * M, (long long)(sizeof(MembraneScalars) / sizeof(double)) * M);
-                if ((int)i + 1 < count) post.add(mad_src, seg_m + (i + 1) * M, M, mad_stride);
-            }
-            launch_copy_list(post, st);
-            LBFS_CUDA(cudaGetLastError());
-        }
-        return LBFS_OK;
-    };
     // backward sweep of segment sg from segment set b.  The kernels read the
     // stored intermediates in place (their own FluidArgs / MembraneArgs), so
     // nothing of the handle's live buffers is touched and the next re-run
     // overlaps it.  Per step: setup (state of step n) on sf; the membrane
     // backward on sm and the general faces on sg_, beside the axis faces and
     // A2 on sf; A3 (which updates lam_t1) after all of them.
-    auto backward = [&](int sg, int b) -> int {
+    auto backward = [&](int sg, int b, cudaEvent_t ready) -> int {
         SegStore &q = segbuf[b];
         double4 *seg_t1 = (double4 *)q.t1.p;
         double *seg_g = (double *)q.g.p, *seg_x = (double *)q.x.p, *seg_f = (double *)q.f.p, *seg_m = (double *)q.m.p;
         Vec4<double> *seg_h = (Vec4<double> *)q.h.p;
         MembraneScalars *seg_s = (MembraneScalars *)q.s.p;
         const int n0 = sg * K, n1 = std::min(n_steps, n0 + K);
-        if (M > 0) LBFS_CUDA(cudaStreamWaitEvent(rs.m, ev_rerun[b], 0));
+        if (M > 0) LBFS_CUDA(cudaStreamWaitEvent(rs.m, ready, 0));
         for (int n = n1 - 1; n >= n0; n--) {
             const size_t i = n - n0;
             FluidArgs<double> ab = a;
@@ -2019,6 +2051,12 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
     };
     LBFS_CUDA(cudaEventRecord(ev_start, st));
     LBFS_CUDA(cudaStreamWaitEvent(rs.f, ev_start, 0));
+    if (store_all) {  // every segment recorded by the forward sweep
+        LBFS_CUDA(cudaEventRecord(ev_rerun[0], st));
+        for (int sg = n_ck - 1; sg >= 0; sg--)
+            if ((rc = backward(sg, sg, ev_rerun[0]))) return rc;
+        LBFS_CUDA(cudaEventRecord(ev_back[0], rs.f));
+    } else {
     if ((rc = rerun(n_ck - 1, (n_ck - 1) % n_sets))) return rc;
     LBFS_CUDA(cudaEventRecord(ev_rerun[(n_ck - 1) % n_sets], st));
     for (int sg = n_ck - 1; sg >= 0; sg--) {
@@ -2031,8 +2069,9 @@ extern "C" int lbfs_adjoint(lbfs_solver *s, int32_t n_steps, int32_t checkpoint_
         }
         const int b = sg % n_sets;
         LBFS_CUDA(cudaStreamWaitEvent(rs.f, ev_rerun[b], 0));
-        if ((rc = backward(sg, b))) return rc;
+        if ((rc = backward(sg, b, ev_rerun[b]))) return rc;
         LBFS_CUDA(cudaEventRecord(ev_back[b], rs.f));
+    }
     }
     LBFS_CUDA(cudaStreamWaitEvent(st, ev_back[0], 0));
     cudaEventRecord(e2, st);

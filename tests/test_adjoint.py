@@ -116,6 +116,38 @@ def test_membrane_adjoint_matches_finite_differences():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("objective", ["taylor", "velocity"])
+def test_stored_trajectory_equals_segment_reruns(objective, monkeypatch):
+    """The adjoint keeps every segment's intermediates from the forward sweep when they fit
+    (the default here), or re-runs each segment from its checkpoint (LBFS_ADJOINT_MEMORY_MB=0):
+    the same kernels on the same inputs, so J and the gradients agree bit for bit, and the
+    handle ends in the same state."""
+    from lbfs_b200 import GpuSolver
+    c = _rbc_case()
+    steps, K = 20, 6
+    weights = np.random.default_rng(5).uniform(-1, 1, (c.mesh.n_cells, 3))
+    out = []
+    for budget in (None, "0"):
+        if budget is None:
+            monkeypatch.delenv("LBFS_ADJOINT_MEMORY_MB", raising=False)
+        else:
+            monkeypatch.setenv("LBFS_ADJOINT_MEMORY_MB", budget)
+        with GpuSolver(c.mesh, c.params, c.membranes) as s:
+            s.set_state(c.rho, c.u, c.v, c.w)
+            if objective == "taylor":
+                J, g, _ = s.adjoint(steps, K, membrane=0)
+            else:
+                J, g, _ = s.adjoint(steps, K, weights=weights)
+            out.append((J, g, s.state(), s.nodes()))
+    (Ja, ga, sa, na), (Jb, gb, sb, nb) = out
+    assert Ja == Jb
+    assert ga == gb
+    for x, y in zip(sa, sb):
+        assert np.array_equal(x, y)
+    assert np.array_equal(na, nb)
+
+
+@pytest.mark.gpu
 def test_coupled_adjoint_velocity_objective():
     """Velocity objective with a red cell in the flow: the fluid adjoint runs
     through the IBM coupling (spread and interpolation transposes, springs)."""
