@@ -207,9 +207,11 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
                 lsw[i].w[3 * q + r] = (R)(L[3 * r] * rh[3 * q] + L[3 * r + 1] * rh[3 * q + 1] + L[3 * r + 2] * rh[3 * q + 2]);
     }
     // at most 8 distinct weight vectors over all cells and slots: 3-bit codes per slot
+    // (LBFS_GENERIC_GEOMETRY set: never, nor one geometry per axis below; a diagnostic switch)
+    const bool generic = std::getenv("LBFS_GENERIC_GEOMETRY") != nullptr;
     std::vector<unsigned> lcode(nc);
     int n_tab = 0;
-    bool coded = nc > 0;
+    bool coded = nc > 0 && !generic;
     for (int i = 0; i < nc && coded; i++) {
         unsigned c = 0;
         for (int q = 0; q < 6 && coded; q++) {
@@ -366,7 +368,7 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     if (a.axis_aligned && (rc = s->upload(&d_axf, axf))) return rc;
     // one geometry per axis (bit for bit) on the generator's uniform meshes
     a.axis_uniform = 0;
-    if (a.axis_aligned && ni > 0) {
+    if (a.axis_aligned && ni > 0 && !generic) {
         const int first[3] = {0, a.nfx, a.nfx + a.nfy}, count[3] = {a.nfx, a.nfy, ni - a.nfx - a.nfy};
         bool uniform = true;
         for (int ax = 0; ax < 3 && uniform; ax++) {
