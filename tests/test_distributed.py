@@ -146,3 +146,66 @@ def test_two_rank_sharded_ensemble_equals_single_process():
             assert np.array_equal(layout[k][0], u[k])
             assert np.array_equal(layout[k][1], full.info["members"][k].membranes[0].xyz_initial)
             assert stepped[k] == _run_instance(full.info["members"][k], steps=2)
+
+
+_ENS_GPU = dict(n_instances=6, seed=17, n_range=(10, 14), rbc_range=(1, 2), levels=(1, 2), radius_cells=1.5)
+
+
+def _gpu_ensemble_worker(rank, world, port, q):
+    """One rank of the sharded batched workload on the GPU: its shard of instances as one ensemble
+    handle, stepped in a graph; the ranks share nothing on the data path (gloo carries only the
+    max-over-ranks time and the gathered results), so none of their kernels waits on another's."""
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "lbfs-ibm-ade-sp_b200"))
+    import torch.distributed as dist
+    from datetime import timedelta
+    from lbfs_b200 import GpuSolver, cases
+    from lbfs_b200.parallel import gather_objects, max_over_ranks, shard_instances
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    specs = cases.ensemble_specs(**_ENS_GPU)
+    shard = shard_instances([s["cost"] for s in specs], world)[rank]
+    part = cases.ensemble(**_ENS_GPU, subset=shard)
+    with GpuSolver(part.mesh, part.params, part.membranes, device=0) as s:
+        s.set_state(part.rho, part.u, part.v, part.w)
+        s.step(8, graph=True)
+        state = s.state()
+        status = s.status()
+    per = {k: [part.mesh.split(a)[j].copy() for a in state] for j, k in enumerate(part.info["indices"])}
+    t = max_over_ranks(10.0 + rank)
+    gathered = gather_objects((shard, per, status))
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        q.put((t, gathered))
+
+
+@pytest.mark.gpu
+def test_two_rank_sharded_ensemble_on_gpu_equals_single_process():
+    """The sharded batched path with real GPU handles: two gloo ranks (both on the one GPU of this
+    run) each step their shard; every instance's state equals, bit for bit, the same instance in the
+    one-process ensemble handle."""
+    from lbfs_b200 import GpuSolver, cases
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gpu_ensemble_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    t, gathered = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert t == 11.0
+    shards = [g[0] for g in gathered]
+    assert sorted(shards[0] + shards[1]) == list(range(_ENS_GPU["n_instances"]))
+    assert all(g[2] == 0 for g in gathered)
+    full = cases.ensemble(**_ENS_GPU)
+    with GpuSolver(full.mesh, full.params, full.membranes) as s:
+        s.set_state(full.rho, full.u, full.v, full.w)
+        s.step(8, graph=True)
+        ref = [full.mesh.split(a) for a in s.state()]
+    for shard, per, _ in gathered:
+        for k in shard:
+            for c in range(4):
+                assert np.array_equal(per[k][c], ref[c][k]), (k, c)
