@@ -474,6 +474,20 @@ int lbfs_mesh_import_openfoam(const char *dir, double visc, double fneq_min, int
                               double *face_normal, double *face_centroid, double *streaming_dt, double *cell_volume,
                               double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse, double *rhs,
                               int32_t *bc_patch, char *names, int32_t names_len);
+/* lbfs_mesh_import_openfoam with the geometry and least-squares matrices
+ * formed on GPU `device`: the file is read on the host as above, then one
+ * thread per face forms the face geometry and one per cell gathers its six
+ * faces in increasing face index (the order of the host routine's face loop)
+ * for the volume, centroid and LS sums, so every array equals
+ * lbfs_mesh_import_openfoam's bit for bit.  Rejects (LBFS_ERR_ARG) a face
+ * whose neighbour is its owner and a cell without six faces.  Device memory
+ * is allocated for the build and released before it returns. */
+int lbfs_mesh_import_openfoam_gpu(const char *dir, double visc, double fneq_min, int32_t gradient_hybrid,
+                                  int32_t closed_faces, int32_t device, int32_t *owner, int32_t *neighbour,
+                                  double *face_area, double *face_normal, double *face_centroid,
+                                  double *streaming_dt, double *cell_volume, double *cell_centroid,
+                                  int32_t *gradient_stencil, double *lhs_inverse, double *rhs, int32_t *bc_patch,
+                                  char *names, int32_t names_len);
 
 /* Spring connectivity of a closed triangulated membrane, in the order the
  * reference's Osay reader produces it (lagrangian_object.cpp:238-481).

@@ -7,6 +7,7 @@
 // Compiled with -ffp-contract=off so every multiply and add rounds on its own,
 // as the reference's host code does; the geometry is then bit-identical.
 #include <algorithm>
+#include <cerrno>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -512,6 +513,75 @@ std::vector<std::string> list_entries(const std::vector<std::string> &lines) {
     return out;
 }
 
+// A polyMesh file read whole, with the [begin, end) offsets of its list's
+// entries (delimited as list_entries does).  The large lists (points, faces,
+// owner, neighbour) are parsed from it with strtof / strtol, which read a
+// well-formed entry as the stream extractions of the reference's reader do.
+struct FoamText {
+    std::string text;
+    std::vector<std::pair<size_t, size_t>> entries;
+    std::string buf;  // the entry being parsed, NUL-terminated
+    const char *entry(size_t k) {
+        buf.assign(text, entries[k].first, entries[k].second - entries[k].first);
+        return buf.c_str();
+    }
+    // Line `k` (0-based) of the file, without its newline; empty past the end.
+    std::string line(int k) const {
+        size_t b = 0;
+        for (int i = 0; i < k && b < text.size(); i++) {
+            const size_t e = text.find('\n', b);
+            b = e == std::string::npos ? text.size() : e + 1;
+        }
+        const size_t e = std::min(text.find('\n', b), text.size());
+        return b < text.size() ? text.substr(b, e - b) : std::string();
+    }
+};
+
+bool read_foam_text(const std::string &path, FoamText &t) {
+    std::FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return false;
+    char chunk[1 << 16];
+    size_t n;
+    while ((n = std::fread(chunk, 1, sizeof chunk, f)) > 0) t.text.append(chunk, n);
+    std::fclose(f);
+    bool start = false;
+    for (size_t b = 0; b < t.text.size();) {
+        size_t e = t.text.find('\n', b);
+        if (e == std::string::npos) e = t.text.size();
+        const char c = e > b ? t.text[b] : 0;
+        if (c == ')') start = false;
+        if (start && e > b) t.entries.push_back({b, e});
+        if (c == '(') start = true;
+        b = e + 1;
+    }
+    return true;
+}
+
+// One int from p (leading blanks skipped, as the stream extraction does);
+// false when nothing was read or it does not fit an int.
+bool parse_int(const char *&p, int &v) {
+    char *end = nullptr;
+    errno = 0;
+    const long r = std::strtol(p, &end, 10);
+    if (end == p || errno == ERANGE || r < std::numeric_limits<int>::min() || r > std::numeric_limits<int>::max())
+        return false;
+    v = (int)r;
+    p = end;
+    return true;
+}
+
+// One float from p, read as float (unstructured_mesh.h:59): false when
+// nothing was read or the value overflows a float.
+bool parse_float(const char *&p, float &v) {
+    char *end = nullptr;
+    errno = 0;
+    const float r = std::strtof(p, &end);
+    if (end == p || !std::isfinite(r)) return false;
+    v = r;
+    p = end;
+    return true;
+}
+
 struct FoamMesh {
     int n_points = 0, n_cells = 0, n_faces = 0, n_internal = 0;
     std::vector<float> x, y, z;
@@ -526,10 +596,10 @@ struct FoamMesh {
 // unstructured_mesh.cpp:670-941; import_openfoam_BC_tags, :2533-2608).
 int read_foam(const std::string &dir0, FoamMesh &m, bool header_only) {
     const std::string dir = dir0.empty() || dir0.back() == '/' ? dir0 : dir0 + "/";
-    std::vector<std::string> own;
-    if (!read_lines(dir + "owner", own)) return lbfs::set_error(LBFS_ERR_ARG, "cannot open " + dir + "owner");
-    if (own.size() < 13) return lbfs::set_error(LBFS_ERR_ARG, "owner: no header note on line 13");
-    const std::string &note = own[12];
+    FoamText own;
+    if (!read_foam_text(dir + "owner", own)) return lbfs::set_error(LBFS_ERR_ARG, "cannot open " + dir + "owner");
+    const std::string note = own.line(12);
+    if (note.empty()) return lbfs::set_error(LBFS_ERR_ARG, "owner: no header note on line 13");
     auto field = [&](const char *key, int &v) {
         const size_t p = note.find(key);
         if (p == std::string::npos) return false;
@@ -563,42 +633,42 @@ int read_foam(const std::string &dir0, FoamMesh &m, bool header_only) {
     if (nbf != m.n_faces - m.n_internal)
         return lbfs::set_error(LBFS_ERR_ARG, "boundary: patch face counts do not add up to the boundary faces");
     if (header_only) return LBFS_OK;
-    std::vector<std::string> pts, fcs, nbr;
-    if (!read_lines(dir + "points", pts) || !read_lines(dir + "faces", fcs) || !read_lines(dir + "neighbour", nbr))
+    FoamText P, F, N;
+    if (!read_foam_text(dir + "points", P) || !read_foam_text(dir + "faces", F) ||
+        !read_foam_text(dir + "neighbour", N))
         return lbfs::set_error(LBFS_ERR_ARG, "cannot open points, faces or neighbour in " + dir);
-    const std::vector<std::string> P = list_entries(pts), F = list_entries(fcs), O = list_entries(own),
-                                   N = list_entries(nbr);
-    if ((int)P.size() != m.n_points || (int)F.size() != m.n_faces || (int)O.size() != m.n_faces ||
-        (int)N.size() != m.n_internal)
+    FoamText &O = own;
+    if ((int)P.entries.size() != m.n_points || (int)F.entries.size() != m.n_faces ||
+        (int)O.entries.size() != m.n_faces || (int)N.entries.size() != m.n_internal)
         return lbfs::set_error(LBFS_ERR_ARG, "polyMesh lists do not match the owner file's header note");
     m.x.resize(m.n_points); m.y.resize(m.n_points); m.z.resize(m.n_points);
     for (int i = 0; i < m.n_points; i++) {
-        std::istringstream is(P[i]);
-        is.ignore(1);  // '('; the coordinates are read as float (unstructured_mesh.h:59)
-        if (!(is >> m.x[i] >> m.y[i] >> m.z[i])) return lbfs::set_error(LBFS_ERR_ARG, "points: bad entry");
+        const char *p = P.entry(i) + 1;  // past '('; the coordinates are read as float (unstructured_mesh.h:59)
+        if (!parse_float(p, m.x[i]) || !parse_float(p, m.y[i]) || !parse_float(p, m.z[i]))
+            return lbfs::set_error(LBFS_ERR_ARG, "points: bad entry");
     }
     m.fv.resize(4 * (size_t)m.n_faces);
     for (int f = 0; f < m.n_faces; f++) {
-        std::istringstream is(F[f]);
+        const char *p = F.entry(f);
         int n = 0;
-        is >> n;
-        if (n != 4) return lbfs::set_error(LBFS_ERR_UNSUPPORTED, "faces: quadrilaterals only (hexahedral cells)");
-        is.ignore(1);
+        if (!parse_int(p, n) || n != 4)
+            return lbfs::set_error(LBFS_ERR_UNSUPPORTED, "faces: quadrilaterals only (hexahedral cells)");
+        if (*p) p++;  // '('
         for (int q = 0; q < 4; q++) {
-            if (!(is >> m.fv[4 * f + q]) || m.fv[4 * f + q] < 0 || m.fv[4 * f + q] >= m.n_points)
+            if (!parse_int(p, m.fv[4 * f + q]) || m.fv[4 * f + q] < 0 || m.fv[4 * f + q] >= m.n_points)
                 return lbfs::set_error(LBFS_ERR_ARG, "faces: bad vertex index");
         }
     }
     m.owner.resize(m.n_faces);
     m.neighbour.assign(m.n_faces, 0);
     for (int f = 0; f < m.n_faces; f++) {
-        std::istringstream is(O[f]);
-        if (!(is >> m.owner[f]) || m.owner[f] < 0 || m.owner[f] >= m.n_cells)
+        const char *p = O.entry(f);
+        if (!parse_int(p, m.owner[f]) || m.owner[f] < 0 || m.owner[f] >= m.n_cells)
             return lbfs::set_error(LBFS_ERR_ARG, "owner: bad cell index");
     }
     for (int f = 0; f < m.n_internal; f++) {
-        std::istringstream is(N[f]);
-        if (!(is >> m.neighbour[f]) || m.neighbour[f] < 0 || m.neighbour[f] >= m.n_cells)
+        const char *p = N.entry(f);
+        if (!parse_int(p, m.neighbour[f]) || m.neighbour[f] < 0 || m.neighbour[f] >= m.n_cells)
             return lbfs::set_error(LBFS_ERR_ARG, "neighbour: bad cell index");
     }
     return LBFS_OK;
@@ -713,6 +783,34 @@ extern "C" int lbfs_mesh_import_openfoam(const char *dir, double visc, double fn
     return mesh_geometry(m.n_cells, m.n_faces, m.n_internal, m.x.data(), m.y.data(), m.z.data(), m.fv.data(), owner,
                          neighbour, visc, fneq_min, gradient_hybrid, closed_faces != 0, face_area, face_normal,
                          face_centroid, streaming_dt, cell_volume, cell_centroid, gradient_stencil, lhs_inverse, rhs);
+}
+
+extern "C" int lbfs_mesh_import_openfoam_gpu(const char *dir, double visc, double fneq_min, int32_t gradient_hybrid,
+                                             int32_t closed_faces, int32_t device, int32_t *owner, int32_t *neighbour,
+                                             double *face_area, double *face_normal, double *face_centroid,
+                                             double *streaming_dt, double *cell_volume, double *cell_centroid,
+                                             int32_t *gradient_stencil, double *lhs_inverse, double *rhs,
+                                             int32_t *bc_patch, char *names, int32_t names_len) {
+    if (!dir || !owner || !neighbour || !face_area || !face_normal || !face_centroid || !streaming_dt ||
+        !cell_volume || !cell_centroid || !gradient_stencil || !lhs_inverse || !rhs || !bc_patch)
+        return lbfs::set_error(LBFS_ERR_ARG, "null argument");
+    FoamMesh m;
+    int rc = read_foam(dir, m, false);
+    if (rc) return rc;
+    std::copy(m.owner.begin(), m.owner.end(), owner);
+    std::copy(m.neighbour.begin(), m.neighbour.end(), neighbour);
+    int b = 0;
+    for (size_t p = 0; p < m.patch_faces.size(); p++)
+        for (int q = 0; q < m.patch_faces[p]; q++) bc_patch[b++] = (int32_t)p;
+    if (names && names_len > 0) {
+        std::string all;
+        for (const std::string &n : m.patch_names) all += n + "\n";
+        std::snprintf(names, (size_t)names_len, "%s", all.c_str());
+    }
+    return lbfs::mesh_geometry_gpu(device, m.n_points, m.n_cells, m.n_faces, m.n_internal, m.x.data(), m.y.data(),
+                                   m.z.data(), m.fv.data(), owner, neighbour, visc, fneq_min, gradient_hybrid,
+                                   closed_faces != 0, face_area, face_normal, face_centroid, streaming_dt,
+                                   cell_volume, cell_centroid, gradient_stencil, lhs_inverse, rhs);
 }
 
 // Periodic partners (Boundary_Conditions::assign_boundary_conditions,

@@ -21,6 +21,16 @@ int set_error(int code, const std::string &msg);
                                    std::string(#call) + ": " + cudaGetErrorString(e_));                  \
     } while (0)
 
+// Geometry and least-squares matrices of a hex mesh given as lists (float
+// vertices, four vertex ids per face, owner per face, neighbour per interior
+// face; boundary neighbours are written as their ghosts) built on GPU
+// `device` (lbfs_mesh_gpu.cu): the host routine's arrays bit for bit.
+int mesh_geometry_gpu(int device, int np, int nc, int nf, int ni, const float *vx, const float *vy, const float *vz,
+                      const int *fv, const int32_t *owner, int32_t *neighbour, double visc, double fneq_min,
+                      int32_t gradient_hybrid, bool closed_faces, double *face_area, double *face_normal,
+                      double *face_centroid, double *streaming_dt, double *cell_volume, double *cell_centroid,
+                      int32_t *gradient_stencil, double *lhs_inverse, double *rhs);
+
 // Largest membrane patch (cells of the IBM stencil's bounding box) a membrane
 // may cover; 48^3 cells covers a red cell of radius 8 cells deformed to twice
 // its diameter with the 4-point stencil margin.

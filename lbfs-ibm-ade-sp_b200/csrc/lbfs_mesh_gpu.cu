@@ -6,7 +6,9 @@
 // -ffp-contract=off, and glibc's pow(x, 2) equals x * x, so the arrays come
 // out bit for bit those of lbfs_mesh_build_rectilinear / _jittered.  Sums over
 // a cell's faces, which the host accumulates face by face, are gathered per
-// cell in increasing face order.
+// cell in increasing face order.  Imported meshes (an OpenFOAM polyMesh) take
+// the same kernels with their topology from lists instead of the generator's
+// closed forms: the arrays of lbfs_mesh_import_openfoam bit for bit.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -148,16 +150,34 @@ __device__ void face_topology(const MeshDims &m, int f, int (&v)[4], int &own, i
     }
 }
 
+// Topology of an imported mesh (device arrays): four vertex ids per face in
+// winding order, the owner of every face, the neighbour of every interior
+// face; cell_face / cell_count receive each cell's faces (six slots per cell,
+// in arrival order) from k_mesh_cell_faces.
+struct FaceLists {
+    const int *fv, *owner, *neighbour;
+    int *cell_face, *cell_count;
+};
+
 // Per face: owner / neighbour (ghost nc + f - ni for boundary faces), area,
 // centroid, normal and streaming dt (unstructured_mesh.cpp:1592-1692), and
 // for the cells' sums the two triangles' volumes, the face's triangle-area
-// sum and its area-weighted centroid sum.
-__global__ void k_mesh_faces(MeshDims m, const float *vx, const float *vy, const float *vz, int *owner,
+// sum and its area-weighted centroid sum.  kList: the topology from L (an
+// imported mesh), otherwise the generator's.
+template <bool kList>
+__global__ void k_mesh_faces(MeshDims m, FaceLists L, const float *vx, const float *vy, const float *vz, int *owner,
                              int *neighbour, double *face_area, double *face_normal, double *face_centroid,
                              double *streaming_dt, double *tvol, double *tarea, double *tcen) {
     for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < m.nf; f += gridDim.x * blockDim.x) {
         int v[4], own, nb;
-        face_topology(m, f, v, own, nb);
+        if (kList) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) v[q] = L.fv[4 * (size_t)f + q];
+            own = L.owner[f];
+            nb = f < m.ni ? L.neighbour[f] : -1;
+        } else {
+            face_topology(m, f, v, own, nb);
+        }
         owner[f] = own;
         neighbour[f] = f < m.ni ? nb : m.nc + f - m.ni;
         D3 nd[4];
@@ -232,14 +252,47 @@ __device__ void cell_faces(const MeshDims &m, int c, int (&face)[6], int (&other
         }
 }
 
+// Each face of an imported mesh into the slot lists of its owner and (interior
+// faces) its neighbour.  The host has checked that every cell has six faces;
+// the slot bound keeps the writes inside the lists regardless.
+__global__ void k_mesh_cell_faces(MeshDims m, FaceLists L) {
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < m.nf; f += gridDim.x * blockDim.x) {
+        const int o = L.owner[f];
+        int s = atomicAdd(&L.cell_count[o], 1);
+        if (s < 6) L.cell_face[6 * (size_t)o + s] = f;
+        if (f < m.ni) {
+            const int n = L.neighbour[f];
+            s = atomicAdd(&L.cell_count[n], 1);
+            if (s < 6) L.cell_face[6 * (size_t)n + s] = f;
+        }
+    }
+}
+
 // Per interior cell: volume (signed tet volumes, + as owner, - as neighbour),
 // the area-weighted centroid, and its stencil (sorted faces, other cells).
-__global__ void k_mesh_cells(MeshDims m, const int *owner, const double *tvol, const double *tarea,
-                             const double *tcen, double *cell_volume, double *cell_centroid, int *stencil,
-                             int *stencil_face) {
+// kList: the cell's faces from L's slots, sorted by face index (the order of
+// the host's face loop), the other cell from owner / neighbour (neighbour
+// already holds the ghost of a boundary face).
+template <bool kList>
+__global__ void k_mesh_cells(MeshDims m, FaceLists L, const int *owner, const int *neighbour, const double *tvol,
+                             const double *tarea, const double *tcen, double *cell_volume, double *cell_centroid,
+                             int *stencil, int *stencil_face) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < m.nc; c += gridDim.x * blockDim.x) {
         int face[6], other[6];
-        cell_faces(m, c, face, other);
+        if (kList) {
+#pragma unroll
+            for (int q = 0; q < 6; q++) face[q] = L.cell_face[6 * (size_t)c + q];
+            for (int a = 1; a < 6; a++)  // insertion sort by face index
+                for (int b = a; b > 0 && face[b] < face[b - 1]; b--) {
+                    const int t = face[b];
+                    face[b] = face[b - 1];
+                    face[b - 1] = t;
+                }
+#pragma unroll
+            for (int q = 0; q < 6; q++) other[q] = owner[face[q]] == c ? neighbour[face[q]] : owner[face[q]];
+        } else {
+            cell_faces(m, c, face, other);
+        }
         double vol = 0.0, csum = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
 #pragma unroll
         for (int q = 0; q < 6; q++) {
@@ -362,7 +415,7 @@ struct Scratch {
     template <typename T> int get(T **out, size_t n) {
         void *q = nullptr;
         cudaError_t e = cudaMalloc(&q, (n > 0 ? n : 1) * sizeof(T));
-        if (e != cudaSuccess) return set_error(LBFS_ERR_NOMEM, std::string("lbfs_mesh_build_gpu: ") + cudaGetErrorString(e));
+        if (e != cudaSuccess) return set_error(LBFS_ERR_NOMEM, std::string("mesh build on the GPU: ") + cudaGetErrorString(e));
         p.push_back(q);
         *out = static_cast<T *>(q);
         return LBFS_OK;
@@ -445,9 +498,11 @@ extern "C" int lbfs_mesh_build_gpu(double X, double Y, double Z, double dt, cons
     LBFS_CUDA(cudaMemcpy(day, ay.data(), sizeof(double) * ay.size(), cudaMemcpyHostToDevice));
     LBFS_CUDA(cudaMemcpy(daz, az.data(), sizeof(double) * az.size(), cudaMemcpyHostToDevice));
     k_mesh_vertices<<<grid_for((long long)nv), 256>>>(m, dax, day, daz, vx, vy, vz);
-    k_mesh_faces<<<grid_for((long long)nf), 256>>>(m, vx, vy, vz, d_owner, d_nb, d_area, d_normal, d_fcen, d_sdt, tvol,
-                                                   tarea, tcen);
-    k_mesh_cells<<<grid_for((long long)nc), 256>>>(m, d_owner, tvol, tarea, tcen, d_vol, d_cen, d_st, d_stf);
+    const FaceLists none = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    k_mesh_faces<false><<<grid_for((long long)nf), 256>>>(m, none, vx, vy, vz, d_owner, d_nb, d_area, d_normal, d_fcen,
+                                                          d_sdt, tvol, tarea, tcen);
+    k_mesh_cells<false><<<grid_for((long long)nc), 256>>>(m, none, d_owner, d_nb, tvol, tarea, tcen, d_vol, d_cen, d_st,
+                                                          d_stf);
     k_mesh_ghosts<<<grid_for((long long)(nf - m.ni)), 256>>>(m, d_owner, d_fcen, d_vol, d_cen);
     k_mesh_ls<<<grid_for((long long)nc), 256>>>(m, d_owner, d_area, d_normal, d_fcen, d_vol, d_cen, d_st, d_stf,
                                                 d_lhs, d_rhs);
@@ -464,5 +519,85 @@ extern "C" int lbfs_mesh_build_gpu(double X, double Y, double Z, double dt, cons
     LBFS_CUDA(cudaMemcpy(gradient_stencil, d_st, sizeof(int) * 6 * nc, cudaMemcpyDeviceToHost));
     LBFS_CUDA(cudaMemcpy(lhs_inverse, d_lhs, sizeof(double) * 9 * nc, cudaMemcpyDeviceToHost));
     LBFS_CUDA(cudaMemcpy(rhs, d_rhs, sizeof(double) * 18 * nc, cudaMemcpyDeviceToHost));
+    return LBFS_OK;
+}
+
+// The geometry of a hex mesh given as lists, on GPU `device`: the kernels
+// above with the topology from the lists, so every array equals the host
+// routine's (host_setup.cpp mesh_geometry) bit for bit.  The host has
+// checked the indices (vertices < np, cells < nc); this checks that no face
+// has its owner as neighbour and that every cell has six faces, as the host
+// routine's stencil check does.
+int lbfs::mesh_geometry_gpu(int device, int np, int nc, int nf, int ni, const float *vx, const float *vy,
+                            const float *vz, const int *fv, const int32_t *owner, int32_t *neighbour, double visc,
+                            double fneq_min, int32_t gradient_hybrid, bool closed_faces, double *face_area,
+                            double *face_normal, double *face_centroid, double *streaming_dt, double *cell_volume,
+                            double *cell_centroid, int32_t *gradient_stencil, double *lhs_inverse, double *rhs) {
+    if (np <= 0 || nc <= 0 || ni < 0 || ni > nf) return set_error(LBFS_ERR_ARG, "mesh_geometry_gpu: bad sizes");
+    {
+        std::vector<int> count(nc, 0);
+        for (int f = 0; f < nf; f++) {
+            count[owner[f]]++;
+            if (f < ni) {
+                if (neighbour[f] == owner[f]) return set_error(LBFS_ERR_ARG, "face with its owner as neighbour");
+                count[neighbour[f]]++;
+            }
+        }
+        for (int c = 0; c < nc; c++)
+            if (count[c] != 6) return set_error(LBFS_ERR_ARG, "hex cell without 6 stencil entries");
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_error(LBFS_ERR_CUDA, "no CUDA device: this library has no CPU path");
+    if (device < 0 || device >= ndev) return set_error(LBFS_ERR_ARG, "bad device index");
+    LBFS_CUDA(cudaSetDevice(device));
+    MeshDims m = {};
+    m.nc = nc; m.nf = nf; m.ni = ni;
+    m.closed_faces = closed_faces ? 1 : 0;
+    m.hybrid = gradient_hybrid ? 1 : 0;
+    m.reference_dt = visc * 3 / 1.0 / fneq_min;  // pre_conditioned_gamma = 1, as the host routine
+    const size_t unc = nc, unf = nf, nt = unc + (unf - ni);
+    Scratch S;
+    double *d_area, *d_normal, *d_fcen, *d_sdt, *d_vol, *d_cen, *d_lhs, *d_rhs, *tvol, *tarea, *tcen;
+    float *d_vx, *d_vy, *d_vz;
+    int *d_fv, *d_own_in, *d_nb_in, *d_owner, *d_nb, *d_st, *d_stf, *d_cf, *d_cc;
+    int rc;
+    if ((rc = S.get(&d_vx, np)) || (rc = S.get(&d_vy, np)) || (rc = S.get(&d_vz, np)) || (rc = S.get(&d_fv, 4 * unf)) ||
+        (rc = S.get(&d_own_in, unf)) || (rc = S.get(&d_nb_in, (size_t)ni)) || (rc = S.get(&d_owner, unf)) ||
+        (rc = S.get(&d_nb, unf)) || (rc = S.get(&d_area, unf)) || (rc = S.get(&d_normal, 3 * unf)) ||
+        (rc = S.get(&d_fcen, 3 * unf)) || (rc = S.get(&d_sdt, unf)) || (rc = S.get(&tvol, 2 * unf)) ||
+        (rc = S.get(&tarea, unf)) || (rc = S.get(&tcen, 3 * unf)) || (rc = S.get(&d_vol, nt)) ||
+        (rc = S.get(&d_cen, 3 * nt)) || (rc = S.get(&d_st, 6 * unc)) || (rc = S.get(&d_stf, 6 * unc)) ||
+        (rc = S.get(&d_lhs, 9 * unc)) || (rc = S.get(&d_rhs, 18 * unc)) || (rc = S.get(&d_cf, 6 * unc)) ||
+        (rc = S.get(&d_cc, unc)))
+        return rc;
+    LBFS_CUDA(cudaMemcpy(d_vx, vx, sizeof(float) * np, cudaMemcpyHostToDevice));
+    LBFS_CUDA(cudaMemcpy(d_vy, vy, sizeof(float) * np, cudaMemcpyHostToDevice));
+    LBFS_CUDA(cudaMemcpy(d_vz, vz, sizeof(float) * np, cudaMemcpyHostToDevice));
+    LBFS_CUDA(cudaMemcpy(d_fv, fv, sizeof(int) * 4 * unf, cudaMemcpyHostToDevice));
+    LBFS_CUDA(cudaMemcpy(d_own_in, owner, sizeof(int) * unf, cudaMemcpyHostToDevice));
+    if (ni > 0) LBFS_CUDA(cudaMemcpy(d_nb_in, neighbour, sizeof(int) * ni, cudaMemcpyHostToDevice));
+    LBFS_CUDA(cudaMemset(d_cc, 0, sizeof(int) * unc));
+    const FaceLists L = {d_fv, d_own_in, d_nb_in, d_cf, d_cc};
+    k_mesh_faces<true><<<grid_for((long long)nf), 256>>>(m, L, d_vx, d_vy, d_vz, d_owner, d_nb, d_area, d_normal, d_fcen,
+                                                         d_sdt, tvol, tarea, tcen);
+    k_mesh_cell_faces<<<grid_for((long long)nf), 256>>>(m, L);
+    k_mesh_cells<true><<<grid_for((long long)nc), 256>>>(m, L, d_owner, d_nb, tvol, tarea, tcen, d_vol, d_cen, d_st,
+                                                         d_stf);
+    if (nf > ni) k_mesh_ghosts<<<grid_for((long long)(nf - ni)), 256>>>(m, d_owner, d_fcen, d_vol, d_cen);
+    k_mesh_ls<<<grid_for((long long)nc), 256>>>(m, d_owner, d_area, d_normal, d_fcen, d_vol, d_cen, d_st, d_stf,
+                                                d_lhs, d_rhs);
+    LBFS_CUDA(cudaGetLastError());
+    LBFS_CUDA(cudaDeviceSynchronize());
+    LBFS_CUDA(cudaMemcpy(neighbour, d_nb, sizeof(int) * unf, cudaMemcpyDeviceToHost));
+    LBFS_CUDA(cudaMemcpy(face_area, d_area, sizeof(double) * unf, cudaMemcpyDeviceToHost));
+    LBFS_CUDA(cudaMemcpy(face_normal, d_normal, sizeof(double) * 3 * unf, cudaMemcpyDeviceToHost));
+    LBFS_CUDA(cudaMemcpy(face_centroid, d_fcen, sizeof(double) * 3 * unf, cudaMemcpyDeviceToHost));
+    LBFS_CUDA(cudaMemcpy(streaming_dt, d_sdt, sizeof(double) * unf, cudaMemcpyDeviceToHost));
+    LBFS_CUDA(cudaMemcpy(cell_volume, d_vol, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    LBFS_CUDA(cudaMemcpy(cell_centroid, d_cen, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost));
+    LBFS_CUDA(cudaMemcpy(gradient_stencil, d_st, sizeof(int) * 6 * unc, cudaMemcpyDeviceToHost));
+    LBFS_CUDA(cudaMemcpy(lhs_inverse, d_lhs, sizeof(double) * 9 * unc, cudaMemcpyDeviceToHost));
+    LBFS_CUDA(cudaMemcpy(rhs, d_rhs, sizeof(double) * 18 * unc, cudaMemcpyDeviceToHost));
     return LBFS_OK;
 }

@@ -188,6 +188,10 @@ def lib():
             "lbfs_mesh_import_openfoam": [ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                           ctypes.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
                                           _i32p, _f64p, _f64p, _i32p, ctypes.c_char_p, ctypes.c_int32],
+            "lbfs_mesh_import_openfoam_gpu": [ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_int32,
+                                              ctypes.c_int32, ctypes.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p,
+                                              _f64p, _f64p, _f64p, _i32p, _f64p, _f64p, _i32p, ctypes.c_char_p,
+                                              ctypes.c_int32],
             "lbfs_mesh_build_rectilinear": [ctypes.c_double] * 4 + [_f64p, ctypes.c_double, ctypes.c_double,
                                                                       ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                                                       ctypes.c_double, _i32p, _i32p, _f64p, _f64p,
@@ -245,4 +249,5 @@ EXPORTED = [
     "lbfs_adjoint", "lbfs_checkpoint_size", "lbfs_checkpoint_save", "lbfs_checkpoint_load",
     "lbfs_mesh_build_jittered", "lbfs_mesh_build_rectilinear", "lbfs_mesh_write_openfoam", "lbfs_mesh_openfoam_counts",
     "lbfs_mesh_import_openfoam", "lbfs_mesh_find_periodic_nodes", "lbfs_mesh_build_gpu",
+    "lbfs_mesh_import_openfoam_gpu",
 ]

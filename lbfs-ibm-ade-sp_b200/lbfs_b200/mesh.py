@@ -204,11 +204,13 @@ def write_openfoam(directory, X, Y, Z, dt=1.0, origin=(0.0, 0.0, 0.0), mesh_type
                                                    float(jitter), int(seed)))
 
 
-def import_openfoam(directory, dt=1.0, visc=0.1, fneq_min=0.0, gradient="LS", closed_faces=False, delta_h=None):
+def import_openfoam(directory, dt=1.0, visc=0.1, fneq_min=0.0, gradient="LS", closed_faces=False, delta_h=None,
+                    device=None):
     """Read an OpenFOAM polyMesh of hexahedra as the reference's importer does (mesh_type 3: every face
     takes the general-normal flux).  The IBM grid is the mesh's bounding box with cells of 2 dt
     (cell order must be lexicographic for the IBM, as in the reference); delta_h defaults to
-    min(0.1, dt)."""
+    min(0.1, dt).  device = a CUDA device index forms the geometry and least-squares arrays on that
+    GPU (lbfs_mesh_import_openfoam_gpu; the same arrays bit for bit)."""
     d = str(directory).encode()
     c = (ctypes.c_int32 * 6)()
     _abi.check(_abi.lib().lbfs_mesh_openfoam_counts(d, c))
@@ -227,10 +229,14 @@ def import_openfoam(directory, dt=1.0, visc=0.1, fneq_min=0.0, gradient="LS", cl
     rhs = np.zeros((nc, 6, 3))
     patch = np.zeros(nb, np.int32)
     names = ctypes.create_string_buffer(64 * (n_patches + 1) + 64)
-    _abi.check(_abi.lib().lbfs_mesh_import_openfoam(
-        d, visc, fneq_min, 1 if gradient == "hybrid" else 0, 1 if closed_faces else 0, _abi.iptr(owner),
-        _abi.iptr(neighbour), _abi.ptr(area), _abi.ptr(normal), _abi.ptr(fcen), _abi.ptr(sdt), _abi.ptr(vol),
-        _abi.ptr(ccen), _abi.iptr(stencil), _abi.ptr(lhs), _abi.ptr(rhs), _abi.iptr(patch), names, len(names)))
+    head = (d, visc, fneq_min, 1 if gradient == "hybrid" else 0, 1 if closed_faces else 0)
+    outs = (_abi.iptr(owner), _abi.iptr(neighbour), _abi.ptr(area), _abi.ptr(normal), _abi.ptr(fcen), _abi.ptr(sdt),
+            _abi.ptr(vol), _abi.ptr(ccen), _abi.iptr(stencil), _abi.ptr(lhs), _abi.ptr(rhs), _abi.iptr(patch), names,
+            len(names))
+    if device is None:
+        _abi.check(_abi.lib().lbfs_mesh_import_openfoam(*head, *outs))
+    else:
+        _abi.check(_abi.lib().lbfs_mesh_import_openfoam_gpu(*head, int(device), *outs))
     patch_names = tuple(names.value.decode().split())
     # bounding box of the boundary face centroids: the box the IBM grid covers
     bf = fcen[ni:]

@@ -1,12 +1,16 @@
-"""The generator's meshes built on the GPU (lbfs_mesh_build_gpu) against the
-host builder, whose arrays are pinned bit for bit on the reference's own
-generator (tests/test_setup_golden.py): every array equal, bit for bit."""
+"""The generator's meshes built on the GPU (lbfs_mesh_build_gpu) and imported
+polyMesh files whose geometry is formed on the GPU (lbfs_mesh_import_openfoam_gpu)
+against the host builder and importer, whose arrays are pinned bit for bit on the
+reference's own generator and importer (tests/test_setup_golden.py): every
+array equal, bit for bit."""
+import os
 import time
 
 import numpy as np
 import pytest
 
-from lbfs_b200 import build_uniform_mesh
+from conftest import ROOT
+from lbfs_b200 import build_uniform_mesh, import_openfoam, write_openfoam
 
 pytestmark = pytest.mark.gpu
 
@@ -49,3 +53,33 @@ def test_gpu_mesh_128_jittered():
     t2 = time.perf_counter()
     same(g, h)
     print(f"128^3 jittered mesh: GPU build {t1 - t0:.3f} s, host build {t2 - t1:.3f} s")
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(gradient="hybrid", visc=0.07, fneq_min=0.05), dict(closed_faces=True)],
+                         ids=["LS", "hybrid", "closed"])
+def test_gpu_import_equals_host_import(kw):
+    d = os.path.join(ROOT, "tests", "golden", "polymesh_jitter_8x6x5")
+    g = import_openfoam(d, device=0, **kw)
+    h = import_openfoam(d, **kw)
+    same(g, h)
+    assert g.patch_names == h.patch_names
+
+
+@pytest.mark.parametrize("kw", [dict(jitter=0.15, seed=3), dict(mesh_type=7)], ids=["jitter", "cosine7"])
+def test_gpu_import_written_meshes(tmp_path, kw):
+    write_openfoam(tmp_path, 40.0, 30.0, 24.0, 1.0, origin=(1.0, 0.0, -2.0), **kw)
+    for hybrid in (False, True):
+        grad = "hybrid" if hybrid else "LS"
+        same(import_openfoam(tmp_path, gradient=grad, device=0), import_openfoam(tmp_path, gradient=grad))
+
+
+def test_gpu_import_64_jittered(tmp_path):
+    # 64^3 cells, jitter 0.1: the file read is shared, the geometry differs in where it runs
+    write_openfoam(tmp_path, 128.0, 128.0, 128.0, 1.0, jitter=0.1, seed=1313)
+    t0 = time.perf_counter()
+    g = import_openfoam(tmp_path, device=0)
+    t1 = time.perf_counter()
+    h = import_openfoam(tmp_path)
+    t2 = time.perf_counter()
+    same(g, h)
+    print(f"64^3 jittered polyMesh: import with GPU geometry {t1 - t0:.3f} s, host geometry {t2 - t1:.3f} s")

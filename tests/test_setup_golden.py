@@ -101,3 +101,22 @@ def test_openfoam_import_rejects_bad_headers(tmp_path):
     (tmp_path / "owner").write_text("\n".join(lines))
     with pytest.raises(LbfsError):
         import_openfoam(tmp_path)
+
+
+@pytest.mark.parametrize("defect", ["cell_with_7_faces", "owner_is_neighbour"])
+def test_openfoam_gpu_import_rejects_bad_topology(tmp_path, defect):
+    """The GPU geometry's topology checks run on the host before any device work."""
+    from lbfs_b200 import LbfsError, import_openfoam, write_openfoam
+    write_openfoam(tmp_path, 8.0, 6.0, 10.0, 1.0)
+    name = "owner" if defect == "cell_with_7_faces" else "neighbour"
+    lines = (tmp_path / name).read_text().split("\n")
+    start = lines.index("(") + 1
+    if defect == "cell_with_7_faces":  # the last (boundary) face handed to cell 0
+        end = lines.index(")")
+        lines[end - 1] = "0"
+    else:  # face 0's neighbour set to its owner
+        own = (tmp_path / "owner").read_text().split("\n")
+        lines[start] = own[own.index("(") + 1]
+    (tmp_path / name).write_text("\n".join(lines))
+    with pytest.raises(LbfsError, match="6 stencil entries|owner as neighbour"):
+        import_openfoam(tmp_path, device=0)
