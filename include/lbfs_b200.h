@@ -453,6 +453,24 @@ int lbfs_mesh_build_gpu(double X, double Y, double Z, double dt, const double *o
                         double *streaming_dt, double *cell_volume, double *cell_centroid, int32_t *gradient_stencil,
                         double *lhs_inverse, double *rhs, int32_t *bc_patch, double *delta_h, double *grid_xyz);
 
+/* Slab decomposition of one mesh over several handles (one per GPU): each
+ * handle holds a slab of z planes plus halo planes of its neighbours' cells,
+ * and between steps the halo planes are refreshed from the neighbours (the
+ * reference has no multi-GPU path; its step is Solver_gpu.cu:749-1021 on one
+ * device).  lbfs_halo_bytes: bytes of the buffer for n_cells cells.
+ * lbfs_halo_pack / lbfs_halo_unpack copy the state records and the FP64
+ * accumulators (soln_t1) of interior cells [first_cell, first_cell + n_cells)
+ * to / from the DEVICE buffer `d_buf` on the handle's stream, device to
+ * device, without synchronising (order NCCL or peer copies on the same
+ * stream, lbfs_set_stream).  lbfs_set_ibm_window confines the IBM patches of
+ * the handle's membranes to z cells [z_lo, z_hi) of its grid: a patch that
+ * leaves the window spreads nothing and raises LBFS_FLAG_IBM_RANGE, so a
+ * membrane cannot reach a halo plane unnoticed. */
+int lbfs_halo_bytes(lbfs_solver *s, int32_t n_cells, uint64_t *bytes);
+int lbfs_halo_pack(lbfs_solver *s, int32_t first_cell, int32_t n_cells, void *d_buf);
+int lbfs_halo_unpack(lbfs_solver *s, int32_t first_cell, int32_t n_cells, const void *d_buf);
+int lbfs_set_ibm_window(lbfs_solver *s, int32_t z_lo, int32_t z_hi);
+
 /* Periodic partners (Boundary_Conditions::assign_boundary_conditions,
  * Boundary_Conditions.cpp:417-432): for every ghost b whose rho or velocity
  * type is 3, out[b] = the interior cell whose centroid is nearest to the

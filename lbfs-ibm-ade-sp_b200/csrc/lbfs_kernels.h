@@ -98,6 +98,9 @@ struct MembraneArgs {
     const int *node_mem;         // [total_nodes] membrane of each node
     double *mad_partials;        // [n_membranes * kMaxSpringBlocks] (scratch)
     unsigned int *mad_ticket;    // [n_membranes], zero between launches
+    // IBM window along z (lbfs_set_ibm_window): a patch whose z cells leave
+    // [ibm_z_lo, ibm_z_hi) of its grid is an IBM range error (whole grid by default)
+    int ibm_z_lo, ibm_z_hi;
 };
 
 // points per axis of an IBM stencil

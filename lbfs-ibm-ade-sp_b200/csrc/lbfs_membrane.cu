@@ -798,7 +798,8 @@ __device__ void sort_patch(const MembraneArgs &A, int m, const double *red, bool
         pdim[c] = bdim[c] + S - 1;
     }
     const long long pcells = (long long)pdim[0] * pdim[1] * pdim[2];
-    const bool overflow = pcells > mc.patch_bound || mc.n_nodes == 0 || !bases_sane;
+    const bool overflow = pcells > mc.patch_bound || mc.n_nodes == 0 || !bases_sane || plo[2] < A.ibm_z_lo ||
+                          plo[2] + pdim[2] > A.ibm_z_hi;
     if (threadIdx.x == 0) {
         if (range_flag) atomicOr(A.flags, range_flag);
         for (int c = 0; c < 3; c++) {

@@ -647,6 +647,8 @@ int setup_membranes(lbfs_solver *s, const lbfs_mesh_desc *m, const lbfs_rbc_desc
     s->total_patch = total_patch;
     // one warp per patch cell, 8 warps a block, grid-stride
     ma.spread_blocks = (int)std::max<long long>(1, std::min<long long>((total_patch + 7) / 8, kSpreadMaxBlocks));
+    ma.ibm_z_lo = 0;
+    ma.ibm_z_hi = INT32_MAX;
     int rc = 0;
     std::vector<int> spring_mem(S), node_mem(N), identity(N);
     for (int n = 0; n < N; n++) identity[n] = n;
@@ -1442,6 +1444,64 @@ extern "C" int lbfs_get_time_step(lbfs_solver *s, double *delta_t) {
     LBFS_CUDA(cudaSetDevice(s->device));
     LBFS_CUDA(cudaMemcpyAsync(delta_t, d, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    return LBFS_OK;
+}
+
+// Slab decomposition: the state records and FP64 accumulators of a range of
+// cells, copied device to device on the handle's stream (no synchronisation),
+// so a caller can move halo planes between handles with NCCL or peer copies
+// on that stream.  Layout of the buffer: the n_cells state records, then the
+// n_cells accumulators.
+namespace {
+size_t state_record_bytes(const lbfs_solver *s) { return s->fp32 ? sizeof(Vec4<float>) : sizeof(Vec4<double>); }
+int halo_range(const lbfs_solver *s, int32_t first_cell, int32_t n_cells, const void *buf) {
+    if (!s || !buf) return set_error(LBFS_ERR_ARG, "null argument");
+    if (first_cell < 0 || n_cells < 0 || (long long)first_cell + n_cells > (long long)s->nc)
+        return set_error(LBFS_ERR_ARG, "halo cells outside the interior cells");
+    return LBFS_OK;
+}
+}  // namespace
+
+extern "C" int lbfs_halo_bytes(lbfs_solver *s, int32_t n_cells, uint64_t *bytes) {
+    if (!s || !bytes || n_cells < 0) return set_error(LBFS_ERR_ARG, "bad argument");
+    *bytes = (uint64_t)n_cells * (state_record_bytes(s) + sizeof(double4));
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_halo_pack(lbfs_solver *s, int32_t first_cell, int32_t n_cells, void *d_out) {
+    int rc = halo_range(s, first_cell, n_cells, d_out);
+    if (rc || n_cells == 0) return rc;
+    LBFS_CUDA(cudaSetDevice(s->device));
+    const size_t rb = state_record_bytes(s), n = (size_t)n_cells;
+    const char *state = s->fp32 ? (const char *)s->f32.state : (const char *)s->f64.state;
+    const double4 *t1 = s->fp32 ? s->f32.t1 : s->f64.t1;
+    char *out = static_cast<char *>(d_out);
+    LBFS_CUDA(cudaMemcpyAsync(out, state + rb * first_cell, rb * n, cudaMemcpyDeviceToDevice, s->stream));
+    LBFS_CUDA(cudaMemcpyAsync(out + rb * n, t1 + first_cell, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s->stream));
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_halo_unpack(lbfs_solver *s, int32_t first_cell, int32_t n_cells, const void *d_in) {
+    int rc = halo_range(s, first_cell, n_cells, d_in);
+    if (rc || n_cells == 0) return rc;
+    LBFS_CUDA(cudaSetDevice(s->device));
+    const size_t rb = state_record_bytes(s), n = (size_t)n_cells;
+    char *state = s->fp32 ? (char *)s->f32.state : (char *)s->f64.state;
+    double4 *t1 = s->fp32 ? s->f32.t1 : s->f64.t1;
+    const char *in = static_cast<const char *>(d_in);
+    LBFS_CUDA(cudaMemcpyAsync(state + rb * first_cell, in, rb * n, cudaMemcpyDeviceToDevice, s->stream));
+    LBFS_CUDA(cudaMemcpyAsync(t1 + first_cell, in + rb * n, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s->stream));
+    return LBFS_OK;
+}
+
+extern "C" int lbfs_set_ibm_window(lbfs_solver *s, int32_t z_lo, int32_t z_hi) {
+    if (!s) return set_error(LBFS_ERR_ARG, "null handle");
+    if (z_lo < 0 || z_hi <= z_lo) return set_error(LBFS_ERR_ARG, "IBM window must satisfy 0 <= z_lo < z_hi");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    LBFS_CUDA(cudaStreamSynchronize(s->stream));
+    s->ma.ibm_z_lo = z_lo;
+    s->ma.ibm_z_hi = z_hi;
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
     return LBFS_OK;
 }
 

@@ -181,6 +181,25 @@ class GpuSolver:
     def set_stream(self, stream_ptr):
         _abi.check(_abi.lib().lbfs_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 
+    # -- slab decomposition -----------------------------------------------------
+    def halo_bytes(self, n_cells):
+        """Bytes of a halo buffer for n_cells cells (state records, then FP64 accumulators)."""
+        b = ctypes.c_uint64()
+        _abi.check(_abi.lib().lbfs_halo_bytes(self._h, int(n_cells), ctypes.byref(b)))
+        return b.value
+
+    def halo_pack(self, first_cell, n_cells, device_ptr):
+        """Copy cells [first_cell, first_cell + n_cells) into a device buffer (on the handle's stream)."""
+        _abi.check(_abi.lib().lbfs_halo_pack(self._h, int(first_cell), int(n_cells), ctypes.c_void_p(device_ptr)))
+
+    def halo_unpack(self, first_cell, n_cells, device_ptr):
+        """Overwrite cells [first_cell, first_cell + n_cells) from a device buffer (on the handle's stream)."""
+        _abi.check(_abi.lib().lbfs_halo_unpack(self._h, int(first_cell), int(n_cells), ctypes.c_void_p(device_ptr)))
+
+    def set_ibm_window(self, z_lo, z_hi):
+        """Confine the membranes' IBM patches to z cells [z_lo, z_hi) of the grid (else LBFS_FLAG_IBM_RANGE)."""
+        _abi.check(_abi.lib().lbfs_set_ibm_window(self._h, int(z_lo), int(z_hi)))
+
     def launch_shape(self):
         """Current launch shape as a dict (block sizes, grid caps)."""
         sh = _abi.LaunchShape()
