@@ -157,7 +157,8 @@ def assign_membranes(membranes, bounds, nz, origin_z, dz, stencil):
 
 
 class SlabSolver:
-    """One rank's handle on its slab: the step, then the halo exchange through `exchange`."""
+    """One rank's handle on its slab, with the pack and unpack of its halo planes; an exchange
+    (TorchExchange, LocalExchange) moves the planes between slabs after every step."""
 
     def __init__(self, slab, params, membranes=(), device=0):
         if params.time_stepping not in (0, _abi.LBFS_DT_CONSTANT):
@@ -214,6 +215,7 @@ class LocalExchange:
         self.slabs, self.device = slabs, device
 
     def __call__(self):
+        import torch
         sent = []
         for s in self.slabs:
             sent.append(s.pack(self.device))
@@ -222,7 +224,6 @@ class LocalExchange:
             bufs = s.recv_buffers(self.device)
             for peer in bufs:
                 bufs[peer].copy_(sent[r + peer][-peer])
-            import torch
             torch.cuda.synchronize(self.device)
             s.unpack(bufs)
             s.solver.synchronize()
