@@ -300,6 +300,10 @@ typedef struct lbfs_launch_shape {
     int32_t membrane_cluster;       /* 8 or 16: a membrane's totals, spring and node forces as one
                                        thread-block cluster of that many CTAs; 0: three kernels.  It
                                        changes the summation order of V, A and MAD (rounding only) */
+    int32_t membrane_after_k1;      /* 1: in a captured step the membrane kernels start once every block
+                                       of the gradient kernel has begun (a programmatic edge from its
+                                       launch-completion port) instead of beside it from the step's
+                                       start; 0: from the step's start.  Order only: results unchanged */
     double time_us[5];              /* autotune: [0] mean step time of the chosen shape (us) */
 } lbfs_launch_shape;
 int lbfs_get_launch_shape(lbfs_solver *s, lbfs_launch_shape *shape);

@@ -116,7 +116,7 @@ class LaunchShape(ctypes.Structure):
         ("gradient_threads", ctypes.c_int32), ("flux_threads", ctypes.c_int32),
         ("general_flux_threads", ctypes.c_int32), ("update_threads", ctypes.c_int32),
         ("update_blocks", ctypes.c_int32), ("spread_blocks", ctypes.c_int32), ("flux_chunks", ctypes.c_int32), ("membrane_cluster", ctypes.c_int32),
-        ("time_us", ctypes.c_double * 5),
+        ("membrane_after_k1", ctypes.c_int32), ("time_us", ctypes.c_double * 5),
     ]
 
 

@@ -326,6 +326,29 @@ def test_pipelined_gradients_and_fluxes_are_bit_identical():
         assert np.array_equal(o[4], out[0][4])
 
 
+@pytest.mark.parametrize("precision,cluster,chunks", [(0, 0, 1), (1, 0, 1), (0, 8, 1), (0, 0, 4)],
+                         ids=["fp64", "fp32", "fp64_cluster8", "fp64_chunks4"])
+def test_membranes_behind_the_gradient_launch_are_bit_identical(precision, cluster, chunks):
+    """Launch shape membrane_after_k1: in a captured step the membrane kernels start behind the
+    gradient kernel's launch completion instead of beside it from the step's start; the order changes,
+    the results do not (graph steps, several per graph, and eager steps in between)."""
+    c = cases.shear_rbc(n=32, level=2, radius_cells=5.0, precision=precision)
+    out = []
+    for after in (0, 1):
+        s = make(c)
+        s.set_launch_shape(membrane_after_k1=after, membrane_cluster=cluster, flux_chunks=chunks)
+        assert s.launch_shape()["membrane_after_k1"] == after
+        s.step(3, graph=True)
+        s.step(1)
+        s.step(4, graph=True)
+        out.append((s.state(), s.nodes(), s.residuals()))
+        assert s.status() == 0
+        s.close()
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
+
+
 def test_nonfinite_state_sets_status_flag():
     c = cases.poiseuille(n=8)
     c.u = c.u.copy()
