@@ -150,7 +150,9 @@ void launch_membrane_tables(const MembraneArgs &a, cudaStream_t s);
 void launch_membrane_forces(const MembraneArgs &a, cudaStream_t s);
 // single phases of the membrane chain (autotuner): node sort + patches, spread
 void launch_membrane_sort(const MembraneArgs &a, cudaStream_t s);
-void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s);
+// programmatic: launched behind the membrane kernel before it on the same stream (its CTAs placed
+// behind that kernel's last wave)
+void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s, bool programmatic = false);
 // per membrane the local area, local bending and spring energy sums, out[3 n_membranes]
 void launch_membrane_energies(const MembraneArgs &a, double *out, cudaStream_t s);
 // check_periodic_object for the membranes flagged periodic (after a step's fluid update)

@@ -1564,10 +1564,10 @@ void launch_membrane_wrap(const MembraneArgs &a, cudaStream_t s) {
     if (a.n_membranes > 0) k_mem_wrap<<<a.n_membranes, 128, 0, s>>>(a);
 }
 
-void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s) {
+void launch_membrane_spread(const MembraneArgs &a, cudaStream_t s, bool programmatic) {
     const dim3 grid(a.spread_blocks);
-    if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a);
-    else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a);
+    if (stencil_width(a.ibm_stencil) == 4) launch_hi(k_mem_spread<4>, grid, dim3(256), 0, s, a, 0, programmatic);
+    else launch_hi(k_mem_spread<2>, grid, dim3(256), 0, s, a, 0, programmatic);
 }
 
 void launch_interior_viscosity(const ViscArgs &a, cudaStream_t s) {

@@ -60,7 +60,7 @@ struct lbfs_solver {
     std::vector<int> tiles_h[3], tile_maxnb[3];
     int *d_tiles[3] = {};
     std::vector<int> chunk_tile;  // K + 1 tile splits of the pipelined K2
-    cudaEvent_t ev_chunk[kMaxFluxChunks] = {}, ev_flux = nullptr;
+    cudaEvent_t ev_chunk[kMaxFluxChunks] = {}, ev_flux = nullptr, ev_bnd = nullptr;
     cudaEvent_t ev_advected = nullptr, ev_sorted = nullptr;
     bool own_stream = true;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -902,7 +902,12 @@ template <typename R> bool spread_with_faces(const lbfs_solver *s, const FluidAr
 }
 //
 // after_k1 (may be null): enqueued right behind the gradient launch (the last
-// chunk's), before anything that waits for the membrane stream.
+// chunk's), before anything that waits for the membrane stream.  With it and
+// spread_here, the spread instead follows the membrane kernels on their own
+// stream as a programmatic launch, joined by the boundary faces (which then
+// end long before the membrane kernels): the cell update still has one other
+// dependency, and the spread starts behind the last membrane kernel's last
+// wave instead of a launch after it.
 template <typename R>
 int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n, bool spread_here,
                   const std::function<int()> *after_k1 = nullptr) {
@@ -920,12 +925,20 @@ int enqueue_k1_k2(lbfs_solver *s, FluidArgs<R> &a, int *n, bool spread_here,
                 LBFS_CUDA(cudaEventRecord(s->ev_chunk[0], s->stream));
                 LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_chunk[0], 0));
                 launch_fluid_flux_general<R>(a, s->stream4);
-                if (spread_here) {
-                    LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_join, 0));
-                    launch_membrane_spread(s->ma, s->stream4);
+                if (spread_here && after_k1) {
+                    LBFS_CUDA(cudaEventRecord(s->ev_bnd, s->stream4));
+                    LBFS_CUDA(cudaStreamWaitEvent(s->stream2, s->ev_bnd, 0));
+                    launch_membrane_spread(s->ma, s->stream2, true);
                     *n += 1;
+                    LBFS_CUDA(cudaEventRecord(s->ev_flux, s->stream2));
+                } else {
+                    if (spread_here) {
+                        LBFS_CUDA(cudaStreamWaitEvent(s->stream4, s->ev_join, 0));
+                        launch_membrane_spread(s->ma, s->stream4);
+                        *n += 1;
+                    }
+                    LBFS_CUDA(cudaEventRecord(s->ev_flux, s->stream4));
                 }
-                LBFS_CUDA(cudaEventRecord(s->ev_flux, s->stream4));
                 launch_fluid_flux_axis<R>(a, s->stream, !s->kernel_events);
                 LBFS_CUDA(cudaStreamWaitEvent(s->stream, s->ev_flux, 0));
             } else {
@@ -1080,6 +1093,7 @@ void free_all(lbfs_solver *s) {
     if (s->stream3) cudaStreamDestroy(s->stream3);
     if (s->stream4) cudaStreamDestroy(s->stream4);
     if (s->ev_flux) cudaEventDestroy(s->ev_flux);
+    if (s->ev_bnd) cudaEventDestroy(s->ev_bnd);
     for (cudaEvent_t e : s->ev_chunk)
         if (e) cudaEventDestroy(e);
     if (s->stream2) cudaStreamDestroy(s->stream2);
@@ -1136,6 +1150,7 @@ extern "C" int lbfs_create(const lbfs_mesh_desc *mesh, const lbfs_params *params
         cudaStreamCreateWithPriority(&s->stream3, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->stream4, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_flux, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_bnd, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_advected, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_sorted, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
