@@ -762,14 +762,19 @@ __global__ void __launch_bounds__(TB) k_cell_update(FluidArgs<R> a) {
     const double dt_all = (a.time_stepping == LBFS_DT_MIN || a.time_stepping == LBFS_DT_TALTS) ? __ldcg(a.dt_min)
                                                                                                  : a.delta_t;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.nc; i += gridDim.x * blockDim.x) {
-        const double iv = __ldg(a.cell_inv_volume + i);  // 1 / volume: products instead of 24 divisions
+        // 1 / volume: products instead of 24 divisions
+        const double iv = a.inv_volume_uniform ? a.inv_volume_all : __ldg(a.cell_inv_volume + i);
         double r[4] = {0, 0, 0, 0};  // rho, u, v, w
         int cfl[6];
+        if (a.grid_faces) {  // the structured mesh's faces, formed (no dependent load before the fluxes)
+            grid_cell_faces(i, a.grid_n[0], a.grid_n[1], a.grid_n[2], cfl);
+        } else {
 #pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const int2 p = __ldg(reinterpret_cast<const int2 *>(a.cell_faces) + 3 * i + q);
-            cfl[2 * q] = p.x;
-            cfl[2 * q + 1] = p.y;
+            for (int q = 0; q < 3; q++) {
+                const int2 p = __ldg(reinterpret_cast<const int2 *>(a.cell_faces) + 3 * i + q);
+                cfl[2 * q] = p.x;
+                cfl[2 * q + 1] = p.y;
+            }
         }
 #pragma unroll
         for (int q = 0; q < 6; q++) {

@@ -139,6 +139,39 @@ template <typename R> struct alignas(16) GradRec {
     R g[12];
 };
 
+// The six faces of cell c of the generator's structured mesh of nx x ny x nz
+// cells (x, y, z interior faces in the generator's loop order, then the
+// patches left, right, bottom, top, back, front; unstructured_mesh.cpp:415-664)
+// in increasing face index, signed as the cell update's face table: +(f + 1)
+// where the cell owns face f, -(f + 1) where it is the face's neighbour.
+__host__ __device__ inline void grid_cell_faces(int c, int nx, int ny, int nz, int (&cf)[6]) {
+    const int i = c % nx, j = (c / nx) % ny, k = c / (nx * ny);
+    const int nfx = (nx - 1) * ny * nz, nfy = nx * (ny - 1) * nz, nfz = nx * ny * (nz - 1);
+    const int nyz = ny * nz, nxz = nx * nz;
+    const int bl = nfx + nfy + nfz, br = bl + nyz, bb = br + nyz, bt = bb + nxz, bk = bt + nxz, bf = bk + nx * ny;
+    int f[6], sg[6];
+    f[0] = i > 0 ? (i - 1) + (nx - 1) * (j + ny * k) : bl + j + ny * k;
+    sg[0] = i > 0 ? -1 : 1;
+    f[1] = i < nx - 1 ? i + (nx - 1) * (j + ny * k) : br + j + ny * k;
+    sg[1] = 1;
+    f[2] = j > 0 ? nfx + i + nx * ((j - 1) + (ny - 1) * k) : bb + i + nx * k;
+    sg[2] = j > 0 ? -1 : 1;
+    f[3] = j < ny - 1 ? nfx + i + nx * (j + (ny - 1) * k) : bt + i + nx * k;
+    sg[3] = 1;
+    f[4] = k > 0 ? nfx + nfy + i + nx * (j + ny * (k - 1)) : bk + i + nx * j;
+    sg[4] = k > 0 ? -1 : 1;
+    f[5] = k < nz - 1 ? nfx + nfy + i + nx * (j + ny * k) : bf + i + nx * j;
+    sg[5] = 1;
+    for (int a = 1; a < 6; a++)  // insertion sort by face index
+        for (int b = a; b > 0 && f[b] < f[b - 1]; b--) {
+            const int tf = f[b], ts = sg[b];
+            f[b] = f[b - 1]; sg[b] = sg[b - 1];
+            f[b - 1] = tf; sg[b - 1] = ts;
+        }
+#pragma unroll
+    for (int q = 0; q < 6; q++) cf[q] = sg[q] * (f[q] + 1);
+}
+
 template <typename R> struct FluidArgs {
     int nc, nf, ni, nb, nfx, nfy, nfz, axis_aligned;
     int testcase;
@@ -189,6 +222,12 @@ template <typename R> struct FluidArgs {
     int n_tiles;
     // K3
     const int *cell_faces;       // [6*nc] +(f+1) owner, -(f+1) neighbour
+    // grid_faces: the mesh is the generator's structured mesh of grid_n cells (one instance) and its
+    // face table is grid_cell_faces's, checked entry for entry at create: K3 forms each cell's faces
+    // instead of loading them.  inv_volume_uniform: every cell has the same 1 / volume (bitwise).
+    int grid_faces, grid_n[3];
+    int inv_volume_uniform;
+    double inv_volume_all;
     const double *cell_volume;   // [nc]
     const double *cell_inv_volume;  // [nc] 1 / cell_volume
     // FP32 bulk on meshes whose cell faces do not close: per cell the momentum

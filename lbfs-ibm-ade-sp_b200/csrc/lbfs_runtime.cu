@@ -387,6 +387,37 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
         }
         a.axis_uniform = uniform ? 1 : 0;
     }
+    // K3 on the generator's structured meshes (one instance): the face table in closed form when it
+    // equals the table entry for entry, and one 1 / volume when every cell has it
+    a.grid_faces = 0;
+    a.inv_volume_uniform = 0;
+    if (a.axis_aligned && !generic && m->n_instances == 0 && m->delta_x > 0) {
+        int n3[3];
+        bool dims = true;
+        for (int d = 0; d < 3; d++) {
+            const double q = m->length[d] / m->delta_x;
+            n3[d] = (int)std::llround(q);
+            dims = dims && n3[d] > 0 && std::fabs(q - n3[d]) < 1e-9 * q;
+        }
+        dims = dims && (long long)n3[0] * n3[1] * n3[2] == nc && (long long)(n3[0] - 1) * n3[1] * n3[2] == a.nfx &&
+               (long long)n3[0] * (n3[1] - 1) * n3[2] == a.nfy;
+        bool same = dims;
+        for (int c = 0; c < nc && same; c++) {
+            int g[6];
+            grid_cell_faces(c, n3[0], n3[1], n3[2], g);
+            same = std::memcmp(g, &cf[6 * (size_t)c], sizeof g) == 0;
+        }
+        if (same) {
+            a.grid_faces = 1;
+            for (int d = 0; d < 3; d++) a.grid_n[d] = n3[d];
+        }
+        bool one = nc > 0;
+        for (int c = 1; c < nc && one; c++) one = std::memcmp(&inv_vol[c], &inv_vol[0], sizeof(double)) == 0;
+        if (one) {
+            a.inv_volume_uniform = 1;
+            a.inv_volume_all = inv_vol[0];
+        }
+    }
     a.closure = nullptr;
     if (!closure.empty()) {
         double *d_cl;
