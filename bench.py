@@ -700,6 +700,7 @@ def main():
     import numpy as np
     import torch
     import torch.distributed as dist
+    import ctypes
     from datetime import timedelta
 
     from lbfs_b200 import GpuSolver, _abi, cases
@@ -837,8 +838,34 @@ def main():
                 "timing": "host wall clock around set_state, then per step step + get_residuals (4 doubles), "
                           "then get_state (page-locked host arrays)"}
 
+    def e2e_device_loop(h, steps=100):
+        """The reference's loop through lbfs_step_until: the state host -> device once, the steps with
+        the convergence test of every step on the device (a CUDA graph while node; tolerance 0, so all
+        `steps` run), the last residual norms and the state back once; host wall clock."""
+        n = mesh.n_cells
+        host = [torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for _ in range(4)]
+        for hh, a in zip(host, h.state()):
+            hh[:] = a
+        h.set_profiling(False)
+        h.step_until(2, 0.0)  # the loop graph built outside the timed region
+        res = torch.empty(4, dtype=torch.float64, pin_memory=True).numpy()
+        done = ctypes.c_int32()
+        barrier()
+        t0 = time.perf_counter()
+        _abi.check(_abi.lib().lbfs_set_state(h._h, *[_abi.ptr(x) for x in host]))
+        _abi.check(_abi.lib().lbfs_step_until(h._h, steps, 0.0, ctypes.byref(done), _abi.ptr(res)))
+        _abi.check(_abi.lib().lbfs_get_state(h._h, *[_abi.ptr(x) for x in host]))
+        barrier()
+        te = max_over_ranks(time.perf_counter() - t0, device="cuda")
+        assert done.value == steps
+        return {"value": n * steps * world / te / 1e6, "unit": METRIC, "h2d_bytes_per_step": 4 * 8 * n / steps,
+                "d2h_bytes_per_step": (4 * 8 * n + 4 * 8) / steps, "steps": steps,
+                "timing": "host wall clock around set_state, lbfs_step_until (convergence test on the device "
+                          "after every step), get_state (page-locked host arrays)"}
+
     e2e = None if args.no_e2e else e2e_pass(s)
     e2e_reference_loop = None if args.no_e2e else e2e_run(s)
+    e2e_device_loop_value = None if args.no_e2e else e2e_device_loop(s)
 
     # the same workload on the reference's own IBM stencil (2-point hat): the like-for-like
     # counterpart of the reference arm, which has no 4-point kernel
@@ -863,7 +890,8 @@ def main():
         th = max_over_ranks(acc / 1e3, device="cuda")
         hat2 = {"value": mesh.n_cells * K * world / th / 1e6, "ms_per_step": acc / K,
                 "e2e": None if args.no_e2e else e2e_pass(sh),
-                "e2e_reference_loop": None if args.no_e2e else e2e_run(sh), "status_flags": sh.status(),
+                "e2e_reference_loop": None if args.no_e2e else e2e_run(sh),
+                "e2e_device_loop": None if args.no_e2e else e2e_device_loop(sh), "status_flags": sh.status(),
                 "workload": workload(args.n, mesh.n_cells, mesh.n_faces, n_nodes, n_tris, n_springs, ibm="hat2")}
         sh.close()
 
@@ -940,7 +968,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "e2e_reference_loop": e2e_reference_loop,
+            "e2e_reference_loop": e2e_reference_loop, "e2e_device_loop": e2e_device_loop_value,
             "gpu_launches": launches_per_step * K,
             "launch_shape": shape,
             "clocks": clocks,

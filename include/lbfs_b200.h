@@ -206,6 +206,18 @@ int lbfs_step(lbfs_solver *s, int32_t n_steps);
 /* Same, with the per-step work replayed from a CUDA graph captured on first use. */
 int lbfs_step_graph(lbfs_solver *s, int32_t n_steps);
 int lbfs_synchronize(lbfs_solver *s);
+/* The reference's time loop with its convergence test (Solver_gpu.cu:1206-1208:
+ * stop after the first step whose residual norms, as lbfs_get_residuals gives
+ * them, have their maximum below `tolerance`) and the drop-in's divergence test
+ * (stop once LBFS_FLAG_NONFINITE or LBFS_FLAG_RHO_RANGE is set), for at most
+ * max_steps steps.  The tests run on the device: the steps between
+ * interior-viscosity updates and object wraps are one launch of a CUDA graph
+ * whose while node repeats the step and a one-thread check kernel, so no host
+ * round trip separates two steps (those special steps, and every step while
+ * profiling, go one at a time with the tests on the host).  *steps_done gets
+ * the number of steps taken, residuals[4] (may be null) the last step's norms.
+ * Results equal lbfs_step_graph + lbfs_get_residuals step by step. */
+int lbfs_step_until(lbfs_solver *s, int32_t max_steps, double tolerance, int32_t *steps_done, double *residuals);
 
 /* Use a caller stream (a cudaStream_t) instead of the solver's own. */
 int lbfs_set_stream(lbfs_solver *s, void *cuda_stream);

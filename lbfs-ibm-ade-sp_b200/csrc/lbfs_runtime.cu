@@ -81,6 +81,10 @@ struct lbfs_solver {
     long long t = 0;  // time-step counter (the reference's loop index)
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
+    // lbfs_step_until: one graph whose while node repeats the step and a convergence check
+    cudaGraphExec_t loop_graph = nullptr;
+    bool loop_unavailable = false;  // the loop graph could not be built (steps go one at a time)
+    struct UntilState *d_until = nullptr;
     int launches_per_step = 0;
     // per-kernel timing: start/stop events per phase (membrane, gradients, flux, update, viscosity)
     bool profiling = false;    // step events (level >= 1)
@@ -121,10 +125,47 @@ struct lbfs_solver {
     }
 };
 
+// Device record of lbfs_step_until's loop: steps taken in this launch, their limit, the tolerance,
+// the last step's residual norms and why the loop stopped (0 limit, 1 converged, 2 diverged).
+struct UntilState {
+    int count, limit, stop, pad;
+    double tol;
+    double res[4];
+};
+
 namespace {
 
 // time stepping other than constant (lbfs_params.time_stepping 1, 3, 4)
 bool dynamic_dt(const lbfs_params &p) { return p.time_stepping != 0 && p.time_stepping != LBFS_DT_CONSTANT; }
+
+// The cached graphs of a step hold the launch shape, the stream and the kernel arguments: dropped
+// whenever one of those changes.
+void drop_step_graphs(lbfs_solver *s) {
+    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+    if (s->loop_graph) { cudaGraphExecDestroy(s->loop_graph); s->loop_graph = nullptr; }
+}
+
+// The convergence test of the reference's loop (Solver_gpu.cu:1206-1208:
+// convergence_residual.max_error() < tolerance) on the step's residual norms,
+// formed as lbfs_get_residuals forms them, and the drop-in's divergence test
+// (non-finite state or density out of range); sets the while node's condition.
+__global__ void k_until_check(cudaGraphConditionalHandle h, UntilState *u, const double *sums, const unsigned int *flags,
+                              double nc, double ref_rho, double ref_mom) {
+    if (threadIdx.x != 0) return;
+    double r[4];
+    for (int k = 0; k < 4; k++) {
+        r[k] = sqrt(sums[k] / nc) / (k == 0 ? ref_rho : ref_mom);
+        u->res[k] = r[k];
+    }
+    const double m01 = r[0] < r[1] ? r[1] : r[0], m23 = r[2] < r[3] ? r[3] : r[2];  // std::max
+    const double mx = m01 < m23 ? m23 : m01;
+    const bool converged = mx < u->tol;
+    const bool diverged = (*flags & (LBFS_FLAG_NONFINITE | LBFS_FLAG_RHO_RANGE)) != 0u;
+    const int c = u->count + 1;
+    u->count = c;
+    u->stop = converged ? 1 : (diverged ? 2 : 0);
+    cudaGraphSetConditional(h, (!converged && !diverged && c < u->limit) ? 1u : 0u);
+}
 
 // Device buffer freed when it leaves scope (temporary storage).
 struct DevBuf {
@@ -1119,6 +1160,7 @@ int after_step(lbfs_solver *s) {
 
 void free_all(lbfs_solver *s) {
     if (s->graph) cudaGraphExecDestroy(s->graph);
+    if (s->loop_graph) cudaGraphExecDestroy(s->loop_graph);
     for (int p = 0; p < kPhases; p++)
         for (int e = 0; e < 2; e++)
             if (s->ev_phase[p][e]) cudaEventDestroy(s->ev_phase[p][e]);
@@ -1230,7 +1272,7 @@ extern "C" int lbfs_set_stream(lbfs_solver *s, void *stream) {
     if (s->own_stream) cudaStreamDestroy(s->stream);
     s->stream = (cudaStream_t)stream;
     s->own_stream = false;
-    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+    drop_step_graphs(s);
     return LBFS_OK;
 }
 
@@ -1286,7 +1328,7 @@ extern "C" int lbfs_set_profiling(lbfs_solver *s, int32_t on) {
     s->profiling = on != 0;
     s->kernel_events = on >= 2;
     for (int p = 0; p < kPhases; p++) s->phase_recorded[p] = false;
-    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+    drop_step_graphs(s);
     return LBFS_OK;
 }
 
@@ -1349,6 +1391,102 @@ extern "C" int lbfs_step_graph(lbfs_solver *s, int32_t n_steps) {
         if (int rc = after_step(s)) return rc;
         s->t++;
     }
+    return LBFS_OK;
+}
+
+namespace {
+// The loop graph of lbfs_step_until: a while node whose body is one regular step (as the step graph
+// captures it) followed by k_until_check.  Returns LBFS_OK with s->loop_unavailable set when the
+// driver refuses the body (the caller then steps one graph at a time).
+int build_loop_graph(lbfs_solver *s) {
+    if (!s->d_until) {
+        int rc = s->alloc(&s->d_until, 1);
+        if (rc) return rc;
+    }
+    cudaGraph_t loop = nullptr;
+    LBFS_CUDA(cudaGraphCreate(&loop, 0));
+    cudaGraphConditionalHandle h;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, loop, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, loop, nullptr, 0, &p);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(loop);
+        cudaGetLastError();
+        s->loop_unavailable = true;
+        return LBFS_OK;
+    }
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    LBFS_CUDA(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int n = 0;
+    int rc = enqueue(s, false, &n);
+    if (!rc) {
+        const double ref_mom = s->params.ref_rho * s->params.max_velocity;
+        k_until_check<<<1, 32, 0, s->stream>>>(h, s->d_until, s->fp32 ? s->f32.residual_sums : s->f64.residual_sums,
+                                               s->fp32 ? s->f32.flags : s->f64.flags, (double)s->nc, s->params.ref_rho,
+                                               ref_mom);
+    }
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(s->stream, &captured);
+    if (rc) {
+        cudaGraphDestroy(loop);
+        return rc;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&s->loop_graph, loop, cudaGraphInstantiateFlagUseNodePriority);
+    cudaGraphDestroy(loop);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        s->loop_graph = nullptr;
+        s->loop_unavailable = true;
+    }
+    return LBFS_OK;
+}
+}  // namespace
+
+extern "C" int lbfs_step_until(lbfs_solver *s, int32_t max_steps, double tolerance, int32_t *steps_done,
+                               double *residuals) {
+    if (!s || max_steps < 0 || !steps_done) return set_error(LBFS_ERR_ARG, "bad arguments");
+    LBFS_CUDA(cudaSetDevice(s->device));
+    int done = 0, stop = 0;
+    double res[4] = {0.0, 0.0, 0.0, 0.0};
+    const bool loop_ok = !s->profiling && !s->loop_unavailable;
+    while (done < max_steps && !stop) {
+        // regular steps ahead (no interior-viscosity update, no object wrap): one launch of the loop graph
+        int chunk = 0;
+        while (loop_ok && done + chunk < max_steps && !visc_due(s, s->t + chunk) && !wrap_due(s, s->t + chunk)) chunk++;
+        if (chunk > 0 && !s->loop_graph) {
+            int rc = build_loop_graph(s);
+            if (rc) return rc;
+        }
+        if (chunk > 0 && s->loop_graph) {
+            UntilState u = {0, chunk, 0, 0, tolerance, {0.0, 0.0, 0.0, 0.0}};
+            LBFS_CUDA(cudaMemcpyAsync(s->d_until, &u, sizeof u, cudaMemcpyHostToDevice, s->stream));
+            LBFS_CUDA(cudaGraphLaunch(s->loop_graph, s->stream));
+            LBFS_CUDA(cudaMemcpyAsync(&u, s->d_until, sizeof u, cudaMemcpyDeviceToHost, s->stream));
+            LBFS_CUDA(cudaStreamSynchronize(s->stream));
+            s->t += u.count;
+            done += u.count;
+            for (int k = 0; k < 4; k++) res[k] = u.res[k];
+            stop = u.stop;
+            continue;
+        }
+        // one step through the step graph (or its interior-viscosity form) and the same tests on the host
+        int rc = lbfs_step_graph(s, 1);
+        if (rc) return rc;
+        if ((rc = lbfs_get_residuals(s, res))) return rc;
+        uint32_t flags = 0;
+        if ((rc = lbfs_status(s, &flags))) return rc;
+        done++;
+        const double mx = std::max(std::max(res[0], res[1]), std::max(res[2], res[3]));
+        stop = mx < tolerance ? 1 : ((flags & (LBFS_FLAG_NONFINITE | LBFS_FLAG_RHO_RANGE)) ? 2 : 0);
+    }
+    *steps_done = done;
+    if (residuals)
+        for (int k = 0; k < 4; k++) residuals[k] = res[k];
     return LBFS_OK;
 }
 
@@ -1608,7 +1746,7 @@ extern "C" int lbfs_set_ibm_window(lbfs_solver *s, int32_t z_lo, int32_t z_hi) {
     LBFS_CUDA(cudaStreamSynchronize(s->stream));
     s->ma.ibm_z_lo = z_lo;
     s->ma.ibm_z_hi = z_hi;
-    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+    drop_step_graphs(s);
     return LBFS_OK;
 }
 
@@ -1623,7 +1761,7 @@ extern "C" int lbfs_keep_residuals(lbfs_solver *s, int32_t on) {
     double *p = on ? s->d_res_out : nullptr;
     s->f64.res_out = p;
     s->f32.res_out = p;
-    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+    drop_step_graphs(s);
     return LBFS_OK;
 }
 
@@ -1698,7 +1836,7 @@ int check_shape(const lbfs_launch_shape &sh) {
 }
 
 void drop_graph(lbfs_solver *s) {
-    if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; s->graph_steps = 0; }
+    drop_step_graphs(s);
 }
 
 int autotune_steps(lbfs_solver *s, int reps, lbfs_launch_shape *out, bool fp32);

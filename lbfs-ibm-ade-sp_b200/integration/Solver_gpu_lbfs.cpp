@@ -187,9 +187,21 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
 
     const int timesteps = (int)std::ceil(globals.simulation_length);
     // the reference tests convergence on the residuals after every step (Solver_gpu.cu:1206); with a
-    // tolerance the steps go one at a time, without one in chunks of output_step
-    const int chunk = globals.tolerance > 0 ? 1 : (globals.output_step > 0 ? globals.output_step : 1);
-    for (int t = 0; t < timesteps; t += chunk) {
+    // tolerance the library runs that test on the device after every step (lbfs_step_until), without
+    // one the steps go in chunks of output_step
+    if (globals.tolerance > 0) {
+        int32_t done = 0;
+        double rms[4];
+        lbfs_check(lbfs_step_until(s, timesteps, globals.tolerance, &done, rms), "lbfs_step_until");
+        uint32_t flags = 0;
+        lbfs_check(lbfs_status(s, &flags), "lbfs_status");
+        if (flags & (LBFS_FLAG_NONFINITE | LBFS_FLAG_RHO_RANGE)) {
+            std::fprintf(stderr, "lbfs_b200: solution diverged (flags %u) at step %d\n", flags, done);
+            std::exit(-1);
+        }
+    }
+    const int chunk = globals.output_step > 0 ? globals.output_step : 1;
+    for (int t = 0; globals.tolerance <= 0 && t < timesteps; t += chunk) {
         const int n = std::min(chunk, timesteps - t);
         lbfs_check(lbfs_step_graph(s, n), "lbfs_step_graph");
         double rms[4];
@@ -200,8 +212,6 @@ void gpu_solver::General_Purpose_Solver_mk_i(unstructured_mesh &Mesh, Solution &
             std::fprintf(stderr, "lbfs_b200: solution diverged (flags %u) at step %d\n", flags, t + n);
             std::exit(-1);
         }
-        const double max_error = std::max(std::max(rms[0], rms[1]), std::max(rms[2], rms[3]));
-        if (max_error < globals.tolerance) break;  // convergence test, Solver_gpu.cu:1206
     }
     lbfs_check(lbfs_get_state(s, rho.data(), u.data(), v.data(), w.data()), "lbfs_get_state");
     for (int i = 0; i < nc; i++) soln.update(rho[i], u[i], v[i], w[i], i);

@@ -199,6 +199,7 @@ def lib():
                                                                       _f64p, _i32p, _f64p, _f64p],
             "lbfs_rbc_build_springs": [ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int32, _i32p, _i32p],
             "lbfs_residual_rms_noalloc": [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, vp, vp],
+            "lbfs_step_until": [vp, ctypes.c_int32, ctypes.c_double, ctypes.POINTER(ctypes.c_int32), _f64p],
             "lbfs_halo_bytes": [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)],
             "lbfs_halo_pack": [vp, ctypes.c_int32, ctypes.c_int32, vp],
             "lbfs_halo_unpack": [vp, ctypes.c_int32, ctypes.c_int32, vp],
@@ -253,5 +254,5 @@ EXPORTED = [
     "lbfs_adjoint", "lbfs_checkpoint_size", "lbfs_checkpoint_save", "lbfs_checkpoint_load",
     "lbfs_mesh_build_jittered", "lbfs_mesh_build_rectilinear", "lbfs_mesh_write_openfoam", "lbfs_mesh_openfoam_counts",
     "lbfs_mesh_import_openfoam", "lbfs_mesh_find_periodic_nodes", "lbfs_mesh_build_gpu",
-    "lbfs_mesh_import_openfoam_gpu", "lbfs_halo_bytes", "lbfs_halo_pack", "lbfs_halo_unpack", "lbfs_set_ibm_window",
+    "lbfs_mesh_import_openfoam_gpu", "lbfs_step_until", "lbfs_halo_bytes", "lbfs_halo_pack", "lbfs_halo_unpack", "lbfs_set_ibm_window",
 ]

@@ -111,6 +111,14 @@ class GpuSolver:
     def synchronize(self):
         _abi.check(_abi.lib().lbfs_synchronize(self._h))
 
+    def step_until(self, max_steps, tolerance):
+        """Up to max_steps steps, stopping after the first whose largest residual norm is below
+        tolerance (or once the state diverged), the tests on the device.  Returns (steps, residuals)."""
+        n = ctypes.c_int32()
+        res = np.zeros(4)
+        _abi.check(_abi.lib().lbfs_step_until(self._h, int(max_steps), float(tolerance), ctypes.byref(n), _abi.ptr(res)))
+        return n.value, res
+
     # -- diagnostics ----------------------------------------------------------
     def nodes(self, which=_abi.LBFS_NODES_POSITION):
         out = np.zeros((self.total_nodes, 3))

@@ -58,7 +58,8 @@ def _seeded_state(n, seed, u0_of_y=None, dt=1.0):
     return np.concatenate([np.full(nc, 1.0), u, v, w])
 
 
-def poiseuille_deck(directory, n=32, steps=20, u_centre=0.01, seed=1234, tau=0.8, delta_t=0.5, cpu_solver=False):
+def poiseuille_deck(directory, n=32, steps=20, u_centre=0.01, seed=1234, tau=0.8, delta_t=0.5, cpu_solver=False,
+                    tolerance=0.0):
     """The body-force-driven square duct on n^3 cells without a red cell (testcase 2): no-slip walls in y
     and z (velocity type dirichlet), zero-gradient x ends, force along x for a centreline speed u_centre
     (series solution of the square duct); the seeded +-1e-4 velocity perturbation.  cpu_solver selects
@@ -78,6 +79,7 @@ def poiseuille_deck(directory, n=32, steps=20, u_centre=0.01, seed=1234, tau=0.8
     bcs = "".join([_bc("left", "neumann", "neumann"), _bc("right", "neumann", "neumann")] +
                   [_bc(p, "dirichlet", "neumann") for p in ("bottom", "top", "back", "front")])
     deck = _deck(directory, L, dt, steps, delta_t, mach=u_centre, visc=visc, testcase=2, force=force, bcs=bcs,
+                 tolerance=tolerance,
                  obj=(f"<name>dummy</name><num_nodes>{len(unit)}</num_nodes><radius>2.0</radius><depth>0.0</depth>"
                       f"<stiffness>0.0</stiffness><centre_x>{0.5 * L!r}</centre_x><centre_y>{0.5 * L!r}</centre_y>"
                       f"<centre_z>{0.5 * L!r}</centre_z><type>spring_network</type><mesh_file>{sf_path}</mesh_file>"
@@ -93,7 +95,8 @@ def poiseuille_deck(directory, n=32, steps=20, u_centre=0.01, seed=1234, tau=0.8
     return deck_path, state_path, {"n_cells": n ** 3, "steps": steps, "visc": visc, "force": force}
 
 
-def _deck(directory, L, dt, steps, delta_t, mach, visc, testcase, force, bcs, obj, gpu_solver=1, output_step=None):
+def _deck(directory, L, dt, steps, delta_t, mach, visc, testcase, force, bcs, obj, gpu_solver=1, output_step=None,
+          tolerance=0.0):
     zero3 = "<x>0.0</x><y>0.0</y><z>0.0</z>"
     quad = "".join(f"<{side}><rho>1.0</rho><u>0.0</u><v>0.0</v><vel_type>dirichlet</vel_type>"
                    f"<rho_type>neumann</rho_type></{side}>" for side in ("west", "east", "north", "south"))
@@ -101,7 +104,7 @@ def _deck(directory, L, dt, steps, delta_t, mach, visc, testcase, force, bcs, ob
     return (
         "<lbfs>"
         "<global_variables>"
-        f"<tolerance>0.0</tolerance><pre_condition_gamma>1.0</pre_condition_gamma>"
+        f"<tolerance>{tolerance!r}</tolerance><pre_condition_gamma>1.0</pre_condition_gamma>"
         f"<simulation_length>{steps}</simulation_length><time_marching_step>{delta_t!r}</time_marching_step>"
         f"<reynolds_no>{reynolds!r}</reynolds_no><mach_no>{mach!r}</mach_no>"
         f"<simulation_name>case</simulation_name><output_directory>{os.path.join(directory, 'out')}/</output_directory>"

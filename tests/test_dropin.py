@@ -135,16 +135,20 @@ REF_GPU = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_program")
 @pytest.mark.gpu
 @pytest.mark.skipif(not (os.path.exists(PROGRAM) and os.path.exists(REF_GPU)),
                     reason="oracle/_ref/ref_gpu_program or dropin_program not built")
-@pytest.mark.parametrize("workload", ["shear_rbc16", "poiseuille12"])
+@pytest.mark.parametrize("workload", ["shear_rbc16", "poiseuille12", "poiseuille12_tolerance"])
 def test_reference_gpu_solver_matches_dropin(workload):
     """The reference's own GPU solver (Solver_gpu.cu and its kernels built for sm_100a) and the drop-in,
-    each behind the same program set-up and deck, agree within FP64_RTOL after 10 steps."""
+    each behind the same program set-up and deck, agree within FP64_RTOL after 10 steps.  With a
+    tolerance in the deck (one no step meets) the drop-in runs its time loop through lbfs_step_until,
+    the convergence test on the device after every step."""
     import ref_deck
     with tempfile.TemporaryDirectory() as d:
         if workload == "shear_rbc16":
             deck, state, _ = ref_deck.shear_rbc_deck(d, n=16, steps=10, level=2, radius_cells=3.0)
-        else:
+        elif workload == "poiseuille12":
             deck, state, _ = ref_deck.poiseuille_deck(d, n=12, steps=10)
+        else:
+            deck, state, _ = ref_deck.poiseuille_deck(d, n=12, steps=10, tolerance=1e-30)
         out = {}
         for name, prog in (("dropin", PROGRAM), ("reference", REF_GPU)):
             r = subprocess.run([prog, deck, os.path.join(d, name), state], capture_output=True, text=True,

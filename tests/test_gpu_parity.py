@@ -349,6 +349,48 @@ def test_membranes_behind_the_gradient_launch_are_bit_identical(precision, clust
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
 
 
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+def test_step_until_matches_the_host_loop(precision):
+    """lbfs_step_until runs the reference's convergence test on the device (a CUDA graph while node
+    repeating the step and a check kernel): it stops at the same step as a host loop of single graph
+    steps reading the residual norms after each, with the same state and norms, bit for bit; with no
+    tolerance it runs every step; a non-finite state stops it after one step."""
+    c = cases.shear_rbc(n=32, level=2, radius_cells=5.0, precision=precision)
+    s = make(c)
+    errs = []
+    for _ in range(40):
+        s.step(1, graph=True)
+        errs.append(float(np.max(s.residuals())))
+    s.close()
+    tol = errs[24] * (1.0 + 1e-12)
+    expected = next(i for i, e in enumerate(errs) if e < tol) + 1
+    a, b = make(c), make(c)
+    n, res = a.step_until(40, tol)
+    assert n == expected
+    for _ in range(expected):
+        b.step(1, graph=True)
+    assert np.array_equal(res, b.residuals())
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.nodes(), b.nodes())
+    n2, _ = a.step_until(7, 0.0)  # no tolerance: all seven
+    b.step(7, graph=True)
+    assert n2 == 7
+    for x, y in zip(a.state(), b.state()):
+        assert np.array_equal(x, y)
+    a.close()
+    b.close()
+    d = make(c)
+    d.step(2, graph=True)
+    rho, u, v, w = d.state()
+    u = u.copy()
+    u[123] = np.nan
+    d.set_state(rho, u, v, w)
+    n3, _ = d.step_until(10, 1e-30)
+    assert n3 == 1 and d.status() & _abi.LBFS_FLAG_NONFINITE
+    d.close()
+
+
 def test_nonfinite_state_sets_status_flag():
     c = cases.poiseuille(n=8)
     c.u = c.u.copy()
