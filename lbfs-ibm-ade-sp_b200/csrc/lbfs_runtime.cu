@@ -1421,7 +1421,13 @@ int build_loop_graph(lbfs_solver *s) {
         return LBFS_OK;
     }
     cudaGraph_t body = p.conditional.phGraph_out[0];
-    LBFS_CUDA(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    e = cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(loop);
+        cudaGetLastError();
+        s->loop_unavailable = true;
+        return LBFS_OK;
+    }
     int n = 0;
     int rc = enqueue(s, false, &n);
     if (!rc) {
