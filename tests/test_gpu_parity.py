@@ -349,14 +349,22 @@ def test_membranes_behind_the_gradient_launch_are_bit_identical(precision, clust
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
 
 
-@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
-def test_step_until_matches_the_host_loop(precision):
+@pytest.mark.parametrize("precision,shape", [(0, {}), (1, {}), (0, {"membrane_cluster": 8, "membrane_after_k1": 1})],
+                         ids=["fp64", "fp32", "fp64_cluster8_after_k1"])
+def test_step_until_matches_the_host_loop(precision, shape):
     """lbfs_step_until runs the reference's convergence test on the device (a CUDA graph while node
     repeating the step and a check kernel): it stops at the same step as a host loop of single graph
     steps reading the residual norms after each, with the same state and norms, bit for bit; with no
     tolerance it runs every step; a non-finite state stops it after one step."""
     c = cases.shear_rbc(n=32, level=2, radius_cells=5.0, precision=precision)
-    s = make(c)
+
+    def make_shaped(case):
+        h = make(case)
+        if shape:
+            h.set_launch_shape(**shape)
+        return h
+
+    s = make_shaped(c)
     errs = []
     for _ in range(40):
         s.step(1, graph=True)
@@ -364,7 +372,7 @@ def test_step_until_matches_the_host_loop(precision):
     s.close()
     tol = errs[24] * (1.0 + 1e-12)
     expected = next(i for i, e in enumerate(errs) if e < tol) + 1
-    a, b = make(c), make(c)
+    a, b = make_shaped(c), make_shaped(c)
     n, res = a.step_until(40, tol)
     assert n == expected
     for _ in range(expected):
@@ -380,7 +388,7 @@ def test_step_until_matches_the_host_loop(precision):
         assert np.array_equal(x, y)
     a.close()
     b.close()
-    d = make(c)
+    d = make_shaped(c)
     d.step(2, graph=True)
     rho, u, v, w = d.state()
     u = u.copy()
