@@ -349,14 +349,17 @@ def test_membranes_behind_the_gradient_launch_are_bit_identical(precision, clust
     assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][2], out[1][2])
 
 
-@pytest.mark.parametrize("precision,shape", [(0, {}), (1, {}), (0, {"membrane_cluster": 8, "membrane_after_k1": 1})],
-                         ids=["fp64", "fp32", "fp64_cluster8_after_k1"])
-def test_step_until_matches_the_host_loop(precision, shape):
+@pytest.mark.parametrize("precision,shape,period", [(0, {}, 10000), (1, {}, 10000),
+                                                   (0, {"membrane_cluster": 8, "membrane_after_k1": 1}, 10000),
+                                                   (0, {}, 7)],
+                         ids=["fp64", "fp32", "fp64_cluster8_after_k1", "fp64_viscosity_every_7"])
+def test_step_until_matches_the_host_loop(precision, shape, period):
     """lbfs_step_until runs the reference's convergence test on the device (a CUDA graph while node
     repeating the step and a check kernel): it stops at the same step as a host loop of single graph
     steps reading the residual norms after each, with the same state and norms, bit for bit; with no
     tolerance it runs every step; a non-finite state stops it after one step."""
     c = cases.shear_rbc(n=32, level=2, radius_cells=5.0, precision=precision)
+    c.params.viscosity_period = period  # 7: an interior-viscosity step (one at a time) between every six
 
     def make_shaped(case):
         h = make(case)
