@@ -499,6 +499,30 @@ __global__ void __launch_bounds__(128, 3) k_adj_flux_axis(FluidArgs<double> a, A
     else axis_face_bwd<2>(a, j, f, lo);
 }
 
+// A1 over the forward step's face tiles (k_face_flux_tiles): block b takes the x, y and z faces owned
+// by the cells of tile tile0 + b, so the tile's cells are read once for the three axes.  Each face's
+// adjoint is written to that face's own records, so the results do not depend on the mapping.
+template <int TB>
+__global__ void __launch_bounds__(TB, 384 / TB) k_adj_flux_axis_tiles(FluidArgs<double> a, AdjointArgs j) {
+    pdl_trigger();
+    const int *tp = a.flux_tiles + 3 * (int)blockIdx.x;
+    const int f0x = __ldg(tp), f0y = __ldg(tp + 1), f0z = __ldg(tp + 2);
+    const int f1x = __ldg(tp + 3), f1y = __ldg(tp + 4), f1z = __ldg(tp + 5);
+    double lo[4];
+    for (int f = f0x + (int)threadIdx.x; f < f1x; f += TB) {
+        face_flux_adjoint(a, j, f, lo);
+        axis_face_bwd<0>(a, j, f, lo);
+    }
+    for (int f = f0y + (int)threadIdx.x; f < f1y; f += TB) {
+        face_flux_adjoint(a, j, f, lo);
+        axis_face_bwd<1>(a, j, f, lo);
+    }
+    for (int f = f0z + (int)threadIdx.x; f < f1z; f += TB) {
+        face_flux_adjoint(a, j, f, lo);
+        axis_face_bwd<2>(a, j, f, lo);
+    }
+}
+
 __global__ void __launch_bounds__(128) k_adj_flux_general(FluidArgs<double> a, AdjointArgs j, int first) {
     const int f = first + blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= a.nf) return;
@@ -780,7 +804,14 @@ void launch_adj_velocity_seed(const FluidArgs<double> &a, const AdjointArgs &j, 
 }
 
 void launch_adj_flux_axis(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
-    if (a.axis_aligned && a.ni > 0) k_adj_flux_axis<<<(a.ni + 127) / 128, 128, 0, s>>>(a, j);
+    if (!a.axis_aligned || a.ni == 0) return;
+    if (a.flux_tiles && a.n_tiles > 0) {  // the forward's tiles (block size tb_flux)
+        if (a.tb_flux == 64) k_adj_flux_axis_tiles<64><<<a.n_tiles, 64, 0, s>>>(a, j);
+        else if (a.tb_flux == 256) k_adj_flux_axis_tiles<256><<<a.n_tiles, 256, 0, s>>>(a, j);
+        else k_adj_flux_axis_tiles<128><<<a.n_tiles, 128, 0, s>>>(a, j);
+        return;
+    }
+    k_adj_flux_axis<<<(a.ni + 127) / 128, 128, 0, s>>>(a, j);
 }
 
 void launch_adj_flux_general(const FluidArgs<double> &a, const AdjointArgs &j, cudaStream_t s) {
