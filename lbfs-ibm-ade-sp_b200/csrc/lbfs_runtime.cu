@@ -1459,9 +1459,9 @@ extern "C" int lbfs_step_until(lbfs_solver *s, int32_t max_steps, double toleran
     LBFS_CUDA(cudaSetDevice(s->device));
     int done = 0, stop = 0;
     double res[4] = {0.0, 0.0, 0.0, 0.0};
-    const bool loop_ok = !s->profiling && !s->loop_unavailable;
     while (done < max_steps && !stop) {
         // regular steps ahead (no interior-viscosity update, no object wrap): one launch of the loop graph
+        const bool loop_ok = !s->profiling && !s->loop_unavailable;
         int chunk = 0;
         while (loop_ok && done + chunk < max_steps && !visc_due(s, s->t + chunk) && !wrap_due(s, s->t + chunk)) chunk++;
         if (chunk > 0 && !s->loop_graph) {
