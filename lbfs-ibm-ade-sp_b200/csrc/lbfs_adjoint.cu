@@ -588,15 +588,11 @@ __global__ void __launch_bounds__(128, 4) k_adj_cell(FluidArgs<double> a, Adjoin
     const Vec4<double> own = a.state[i];
     const double O[4] = {own.rho, own.u, own.v, own.w};
     int st[6];
-    if (a.grid_stencil) {
-        grid_cell_stencil(i, a.grid_n[0], a.grid_n[1], a.grid_n[2], st);
-    } else {
 #pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const int2 p = a.stencil[3 * i + q];
-            st[2 * q] = p.x;
-            st[2 * q + 1] = p.y;
-        }
+    for (int q = 0; q < 3; q++) {
+        const int2 p = a.stencil[3 * i + q];
+        st[2 * q] = p.x;
+        st[2 * q + 1] = p.y;
     }
     // ghosts: lambda of the ghost state collected here, then taken back to own
     double lgs[6][4];

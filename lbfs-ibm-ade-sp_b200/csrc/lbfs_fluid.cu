@@ -52,15 +52,11 @@ __global__ void __launch_bounds__(TB, TB == 128 ? 5 : 1) k_cell_gradients(FluidA
     if (i >= end) return;
     const Vec4<R> own = a.state[i];
     int st[6];
-    if (a.grid_stencil) {  // the structured mesh's stencil, formed (no dependent load before the states)
-        grid_cell_stencil(i, a.grid_n[0], a.grid_n[1], a.grid_n[2], st);
-    } else {
 #pragma unroll
-        for (int q = 0; q < 3; q++) {
-            const int2 p = __ldg(a.stencil + 3 * i + q);
-            st[2 * q] = p.x;
-            st[2 * q + 1] = p.y;
-        }
+    for (int q = 0; q < 3; q++) {
+        const int2 p = __ldg(a.stencil + 3 * i + q);
+        st[2 * q] = p.x;
+        st[2 * q + 1] = p.y;
     }
     LsW<R> W;
     if (a.lsw_code) {  // the weights from the per-mesh table by the cell's six 3-bit codes

@@ -172,22 +172,6 @@ __host__ __device__ inline void grid_cell_faces(int c, int nx, int ny, int nz, i
     for (int q = 0; q < 6; q++) cf[q] = sg[q] * (f[q] + 1);
 }
 
-// The gradient stencil of that cell: the cell across each of its faces in the
-// same order (the neighbour or owner of an interior face, the ghost
-// n_cells + f - n_interior of a boundary face f).
-__host__ __device__ inline void grid_cell_stencil(int c, int nx, int ny, int nz, int (&st)[6]) {
-    int cf[6];
-    grid_cell_faces(c, nx, ny, nz, cf);
-    const int nxy = nx * ny, nc = nxy * nz;
-    const int nfx = (nx - 1) * ny * nz, nfy = nx * (ny - 1) * nz, ni = nfx + nfy + nx * ny * (nz - 1);
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-        const int f = (cf[q] > 0 ? cf[q] : -cf[q]) - 1;
-        const int step = f < nfx ? 1 : (f < nfx + nfy ? nx : nxy);
-        st[q] = f >= ni ? nc + f - ni : (cf[q] > 0 ? c + step : c - step);
-    }
-}
-
 template <typename R> struct FluidArgs {
     int nc, nf, ni, nb, nfx, nfy, nfz, axis_aligned;
     int testcase;
@@ -242,7 +226,6 @@ template <typename R> struct FluidArgs {
     // face table is grid_cell_faces's, checked entry for entry at create: K3 forms each cell's faces
     // instead of loading them.  inv_volume_uniform: every cell has the same 1 / volume (bitwise).
     int grid_faces, grid_n[3];
-    int grid_stencil;            // K1: the stencil in closed form (grid_cell_stencil, checked likewise)
     int inv_volume_uniform;
     double inv_volume_all;
     const double *cell_volume;   // [nc]

@@ -431,7 +431,6 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
     // K3 on the generator's structured meshes (one instance): the face table in closed form when it
     // equals the table entry for entry, and one 1 / volume when every cell has it
     a.grid_faces = 0;
-    a.grid_stencil = 0;
     a.inv_volume_uniform = 0;
     if (a.axis_aligned && !generic && m->n_instances == 0 && m->delta_x > 0) {
         int n3[3];
@@ -449,16 +448,10 @@ template <typename R> int setup_fluid(lbfs_solver *s, const lbfs_mesh_desc *m) {
             grid_cell_faces(c, n3[0], n3[1], n3[2], g);
             same = std::memcmp(g, &cf[6 * (size_t)c], sizeof g) == 0;
         }
-        bool same_st = dims;
-        for (int c = 0; c < nc && same_st; c++) {
-            int g[6];
-            grid_cell_stencil(c, n3[0], n3[1], n3[2], g);
-            same_st = std::memcmp(g, &m->gradient_stencil[6 * (size_t)c], sizeof g) == 0;
-        }
-        if (same || same_st)
+        if (same) {
+            a.grid_faces = 1;
             for (int d = 0; d < 3; d++) a.grid_n[d] = n3[d];
-        a.grid_faces = same ? 1 : 0;
-        a.grid_stencil = same_st ? 1 : 0;
+        }
         bool one = nc > 0;
         for (int c = 1; c < nc && one; c++) one = std::memcmp(&inv_vol[c], &inv_vol[0], sizeof(double)) == 0;
         if (one) {
