@@ -517,69 +517,88 @@ __device__ __forceinline__ Vec4<R> general_face_flux(const FluidArgs<R> &a, int 
         const int ee[3] = {e.ex, e.ey, e.ez};
         const R s = (k < 7) ? (e.ex ? geo.nx : (e.ey ? geo.ny : geo.nz))
                             : (R(e.ex) * geo.nx + R(e.ey) * geo.ny + R(e.ez) * geo.nz);
-        // side of direction k and of its opposite k+1: 0 owner, 1 neighbour, 2 centre
-        const int side_k = (s > thr) ? 0 : ((s < -thr) ? 1 : 2);
-        const int side_o = (side_k == 2) ? 2 : 1 - side_k;
-        (void)side_o;
-        // e . gradient per component from the owner (A), the neighbour (B) and the face centre
-        // (C, the mean gradient); direction k (+e) is extrapolated from side_k, its opposite (-e)
-        // from the other side (the centre for both): L = base -+ dt (e . g)
-        R Lp[4], Lm[4], Dp[4], Dm[4];
+        // Upwind sides.  With sg = -1 where n.e < -thr and +1 otherwise, the population of
+        // direction sg e comes from the owner and that of -sg e from the neighbour, each
+        // extrapolated along its own direction: Lo = p_owner - sg dt (e . g_owner),
+        // Ln = p_neighbour + sg dt (e . g_neighbour).  Where |n.e| <= thr (cen) both come from
+        // the face centre with the mean gradient C (sg = +1: +e at Lo, -e at Ln).  Only warps
+        // with such a lane take the selects; in the others the side is a sign of dt.
+        const bool neg = s < -thr, cen = !(s > thr) && !neg;
+        const R sg = neg ? R(-1) : R(1);
+        const R sdt = sg * dt;
+        R A[4], B[4];  // e . gradient per component, owner (A) and neighbour (B)
 #pragma unroll
         for (int m = 0; m < 4; m++) {
-            R A = R(0), B = R(0);
             bool first = true;
 #pragma unroll
             for (int d = 0; d < 3; d++) {
                 if (!ee[d]) continue;
                 const R ga = ee[d] > 0 ? g1[3 * m + d] : -g1[3 * m + d];
                 const R gb = ee[d] > 0 ? g2[3 * m + d] : -g2[3 * m + d];
-                A = first ? ga : A + ga;
-                B = first ? gb : B + gb;
+                A[m] = first ? ga : A[m] + ga;
+                B[m] = first ? gb : B[m] + gb;
                 first = false;
             }
-            const R C = (A + B) * R(0.5);
-            const R Xp = side_k == 0 ? A : (side_k == 1 ? B : C);
-            const R Xm = side_k == 0 ? B : (side_k == 1 ? A : C);
-            if constexpr (sizeof(R) == 8) {
-                const R bp = side_k == 0 ? pi[m] : (side_k == 1 ? pn[m] : p0[m]);
-                const R bm = side_k == 0 ? pn[m] : (side_k == 1 ? pi[m] : p0[m]);
-                Lp[m] = bp - Xp * dt;
-                Lm[m] = bm + Xm * dt;
-            } else {
-                // FP32: offsets from the face centre (+hdp owner, -hdp neighbour, 0 centre)
-                const R bp = side_k == 0 ? hdp[m] : (side_k == 1 ? -hdp[m] : R(0));
-                const R bm = side_k == 0 ? -hdp[m] : (side_k == 1 ? hdp[m] : R(0));
-                Dp[m] = bp - Xp * dt;
-                Dm[m] = bm + Xm * dt;
-                Lp[m] = p0[m] + Dp[m];
-                Lm[m] = p0[m] + Dm[m];
+        }
+        R Lo[4], Ln[4], Do[4], Dn[4];
+        if (__any_sync(__activemask(), cen)) {
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                const R C = (A[m] + B[m]) * R(0.5);
+                const R Xo = cen ? C : A[m], Xn = cen ? C : B[m];
+                if constexpr (sizeof(R) == 8) {
+                    Lo[m] = (cen ? p0[m] : pi[m]) - sdt * Xo;
+                    Ln[m] = (cen ? p0[m] : pn[m]) + sdt * Xn;
+                } else {
+                    // FP32: offsets from the face centre (+hdp owner, -hdp neighbour, 0 centre)
+                    Do[m] = (cen ? R(0) : hdp[m]) - sdt * Xo;
+                    Dn[m] = (cen ? R(0) : -hdp[m]) + sdt * Xn;
+                    Lo[m] = p0[m] + Do[m];
+                    Ln[m] = p0[m] + Dn[m];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                if constexpr (sizeof(R) == 8) {
+                    Lo[m] = pi[m] - sdt * A[m];
+                    Ln[m] = pn[m] + sdt * B[m];
+                } else {
+                    Do[m] = hdp[m] - sdt * A[m];
+                    Dn[m] = -hdp[m] + sdt * B[m];
+                    Lo[m] = p0[m] + Do[m];
+                    Ln[m] = p0[m] + Dn[m];
+                }
             }
         }
-        R gp[2];
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const R(&L)[4] = h ? Lm : Lp;
-            const R(&D)[4] = h ? Dm : Dp;
-            const int sg = h ? -1 : 1;
-            R eu = R(0), edu = R(0);
+        // e . u at both states (and e . d, FP32); the owner's direction is sg e, the neighbour's -sg e
+        R Eo, En, Edo = R(0), Edn = R(0);
+        {
             bool first = true;
 #pragma unroll
             for (int d = 0; d < 3; d++) {
                 if (!ee[d]) continue;
-                const bool pos = sg * ee[d] > 0;
-                const R ud = pos ? L[1 + d] : -L[1 + d];
-                eu = first ? ud : eu + ud;
+                const R uo = ee[d] > 0 ? Lo[1 + d] : -Lo[1 + d], un = ee[d] > 0 ? Ln[1 + d] : -Ln[1 + d];
+                Eo = first ? uo : Eo + uo;
+                En = first ? un : En + un;
                 if constexpr (sizeof(R) == 4) {
-                    const R dd = pos ? D[1 + d] : -D[1 + d];
-                    edu = first ? dd : edu + dd;
+                    const R dO = ee[d] > 0 ? Do[1 + d] : -Do[1 + d], dN = ee[d] > 0 ? Dn[1 + d] : -Dn[1 + d];
+                    Edo = first ? dO : Edo + dO;
+                    Edn = first ? dN : Edn + dN;
                 }
                 first = false;
             }
-            if constexpr (sizeof(R) == 4) gp[h] = pop_dev(L, eu, edu, rho0, q);
-            else gp[h] = pop_g<R>(L, eu, rho0, q);
         }
-        const R sig = gp[0] + gp[1], del = gp[0] - gp[1];
+        R go, gn;
+        if constexpr (sizeof(R) == 4) {
+            go = pop_dev(Lo, sg * Eo, sg * Edo, rho0, q);
+            gn = pop_dev(Ln, -sg * En, -sg * Edn, rho0, q);
+        } else {
+            go = pop_g<R>(Lo, sg * Eo, rho0, q);
+            gn = pop_g<R>(Ln, -sg * En, rho0, q);
+        }
+        // the pair's sum and its (+e) - (-e) difference
+        const R sig = go + gn, del = sg * (go - gn);
         if (k < 7) {
             const int c = e.ex ? 0 : (e.ey ? 1 : 2);
             sax[c] = sig;
