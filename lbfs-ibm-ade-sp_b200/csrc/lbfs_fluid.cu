@@ -673,9 +673,10 @@ __global__ void __launch_bounds__(TB, (sizeof(R) == 4 ? 1024 : 640) / TB) k_face
 // takes the faces owned by the TB cells of tile tile0 + b, in up to three
 // face ranges ordered by owner (the generator's x, y, z faces; an imported
 // mesh's internal faces, which OpenFOAM orders by owner, form one range).
-// FP64 at 128 registers (16 warps per SM; fewer spill), FP32 at 80 (24).
+// FP64 at 128 registers (16 warps per SM; at 96 it spills 1.4 KB a thread), FP32 at 64 (32 warps
+// per SM, 44 B spilled; 6 % faster than at 80 registers and 24 warps).
 template <typename R, int TB>
-__global__ void __launch_bounds__(TB, (sizeof(R) == 4 ? 768 : 512) / TB) k_face_flux_general_tiles(FluidArgs<R> a, int tile0) {
+__global__ void __launch_bounds__(TB, (sizeof(R) == 4 ? 1024 : 512) / TB) k_face_flux_general_tiles(FluidArgs<R> a, int tile0) {
     pdl_trigger();
     pdl_wait();  // the gradients
     const int *tp = a.flux_tiles + 3 * (tile0 + (int)blockIdx.x);
