@@ -154,6 +154,52 @@ def ls_weights_coded(mesh):
     return len(np.unique(W.reshape(-1, 3), axis=0)) <= 8
 
 
+def cell_update_closed_forms(mesh):
+    """(faces, volume): whether the cell update forms each cell's six faces in closed form instead
+    of reading its face list, and takes one 1 / volume from its parameters instead of one per cell,
+    as the library checks at create.  The faces: an axis-aligned single mesh of the generator's
+    structured layout (cell = i + nx (j + ny k)) whose face table -- per cell its faces in increasing
+    order, +(f + 1) where it owns f, -(f + 1) where it is f's neighbour -- equals the closed form
+    entry for entry.  The volume: every cell's 1 / volume the same, bit for bit."""
+    import numpy as np
+    inv = 1.0 / np.asarray(mesh.cell_volume, dtype=np.float64)[:mesh.n_cells]  # compared as the library does
+    same_volume = bool(mesh.n_cells > 0 and np.all(inv == inv[0]))
+    if not getattr(mesh, "axis_aligned", True) or mesh.delta_x <= 0:
+        return False, same_volume
+    q = [L / mesh.delta_x for L in (mesh.X, mesh.Y, mesh.Z)]
+    n = [int(round(v)) for v in q]
+    if any(m <= 0 or abs(v - m) >= 1e-9 * v for v, m in zip(q, n)):
+        return False, same_volume
+    nx, ny, nz = n
+    nc, nf, ni = mesh.n_cells, mesh.n_faces, mesh.n_interior
+    if nx * ny * nz != nc or (nx - 1) * ny * nz != mesh.n_face_x or nx * (ny - 1) * nz != mesh.n_face_y:
+        return False, same_volume
+    cells = np.concatenate([np.asarray(mesh.owner)[:nf], np.asarray(mesh.neighbour)[:ni]]).astype(np.int64)
+    faces = np.concatenate([np.arange(nf), np.arange(ni)])
+    signed = np.concatenate([np.arange(nf) + 1, -(np.arange(ni) + 1)])
+    if cells.min() < 0 or cells.max() >= nc or np.any(np.bincount(cells, minlength=nc) != 6):
+        return False, same_volume
+    table = signed[np.lexsort((faces, cells))].reshape(nc, 6)
+    c = np.arange(nc)
+    i, j, k = c % nx, (c // nx) % ny, c // (nx * ny)
+    nfx, nfy, nfz = (nx - 1) * ny * nz, nx * (ny - 1) * nz, nx * ny * (nz - 1)
+    bl = nfx + nfy + nfz
+    br, bb = bl + ny * nz, bl + 2 * ny * nz
+    bt, bk = bb + nx * nz, bb + 2 * nx * nz
+    bf = bk + nx * ny
+    f = np.stack([np.where(i > 0, (i - 1) + (nx - 1) * (j + ny * k), bl + j + ny * k),
+                  np.where(i < nx - 1, i + (nx - 1) * (j + ny * k), br + j + ny * k),
+                  np.where(j > 0, nfx + i + nx * ((j - 1) + (ny - 1) * k), bb + i + nx * k),
+                  np.where(j < ny - 1, nfx + i + nx * (j + (ny - 1) * k), bt + i + nx * k),
+                  np.where(k > 0, nfx + nfy + i + nx * (j + ny * (k - 1)), bk + i + nx * j),
+                  np.where(k < nz - 1, nfx + nfy + i + nx * (j + ny * k), bf + i + nx * j)], axis=1)
+    sg = np.stack([np.where(i > 0, -1, 1), np.ones(nc, np.int64), np.where(j > 0, -1, 1),
+                   np.ones(nc, np.int64), np.where(k > 0, -1, 1), np.ones(nc, np.int64)], axis=1)
+    o = np.argsort(f, axis=1, kind="stable")
+    closed = np.take_along_axis(sg * (f + 1), o, axis=1)
+    return bool(np.array_equal(table, closed)), same_volume
+
+
 def algorithmic_bytes(mesh, phase, fp64=True):
     """Bytes each kernel must move once per launch (every array element it
     reads or writes counted once), FP64 storage."""
@@ -179,8 +225,11 @@ def algorithmic_bytes(mesh, phase, fp64=True):
         w = 4 if ls_weights_coded(mesh) else 18 * R
         return nc * (24 + 16 * R + w) + nb * (8 + 13 * R)
     if phase == "update":
-        # per cell: face list 24, volume 8, t1 in/out 64, state out 4R; each face flux read once 4R
-        return nc * (96 + 4 * R) + nf * 4 * R
+        # per cell: face list 24, volume 8, t1 in/out 64, state out 4R; each face flux read once 4R.
+        # The face list is formed in closed form on the generator's structured meshes, and one
+        # 1 / volume comes from the parameters when every cell has it: neither is read then
+        faces, volume = cell_update_closed_forms(mesh)
+        return nc * ((0 if faces else 24) + (0 if volume else 8) + 64 + 4 * R) + nf * 4 * R
     return 0
 
 
