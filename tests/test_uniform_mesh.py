@@ -61,3 +61,30 @@ def test_generator_mesh_is_uniform():
     assert bench.axis_geometry_uniform(c.mesh) and bench.ls_weights_coded(c.mesh)
     j = cases.jittered_channel(n=8)
     assert not bench.axis_geometry_uniform(j.mesh) and not bench.ls_weights_coded(j.mesh)
+
+
+def test_cell_update_closed_form_faces():
+    """CPU: the bench counts K3's face list only where the library reads it.  The uniform
+    generator's mesh matches the closed-form face list entry for entry; a jittered mesh (not axis
+    aligned) and a uniform mesh whose table no longer matches (one interior face with owner and
+    neighbour swapped) do not, and then the 24 B per cell of the list are counted."""
+    import copy
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    from lbfs_b200 import cases
+    c = cases.shear_rbc(n=12, level=1, radius_cells=2.0)
+    faces, _ = bench.cell_update_closed_forms(c.mesh)
+    assert faces
+    nc = c.mesh.n_cells
+    full = bench.algorithmic_bytes(c.mesh, "update")
+    assert full == nc * (8 + 64 + 32) + c.mesh.n_faces * 32 or full == nc * (64 + 32) + c.mesh.n_faces * 32
+    j = cases.jittered_channel(n=8)
+    assert not bench.cell_update_closed_forms(j.mesh)[0]
+    m = copy.copy(c.mesh)
+    m.owner, m.neighbour = np.array(c.mesh.owner, copy=True), np.array(c.mesh.neighbour, copy=True)
+    f = c.mesh.n_face_x // 2
+    m.owner[f], m.neighbour[f] = c.mesh.neighbour[f], c.mesh.owner[f]
+    assert not bench.cell_update_closed_forms(m)[0]
+    assert bench.algorithmic_bytes(m, "update") == full + 24 * nc
